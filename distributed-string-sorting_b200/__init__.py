@@ -1,0 +1,358 @@
+"""dsss_b200 — Python front-end over libdsss (the C ABI in include/dsss.h).
+
+Every call goes through the shared library with ctypes; torch is used only for
+device memory and streams.  Importing fails loudly when libdsss.so is missing:
+there is no CPU fallback for any entry point.
+
+The directory name is not a Python identifier; load it with ``load_package()``
+from ``__graft_entry__`` (which registers it as ``dsss_b200``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdsss.so")
+
+DSSS_OK = 0
+ERRORS = {-22: "EINVAL", -12: "ENOMEM", -110: "ETIMEDOUT", -5: "EDEVICE", -95: "ENOTSUP"}
+SAMPLER_NUM_STRINGS = 0
+SAMPLER_INDEXED_NUM_STRINGS = 2
+FLAG_LOCAL_LCP = 1
+PAD = 64  # bytes of zero padding behind device arenas (the ABI asks for >= 32)
+
+
+class DsssError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Arena(ctypes.Structure):
+    _fields_ = [("chars", ctypes.c_void_p), ("char_bytes", ctypes.c_uint64), ("offsets", ctypes.c_void_p),
+                ("lengths", ctypes.c_void_p), ("n", ctypes.c_uint64)]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("sampler", ctypes.c_uint32), ("sampling_factor", ctypes.c_uint32),
+                ("small_sort_max", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
+
+
+class PdResult(ctypes.Structure):
+    _fields_ = [("local_order", ctypes.c_void_p), ("local_lcp", ctypes.c_void_p), ("dp", ctypes.c_void_p),
+                ("intervals", ctypes.c_void_p), ("perm_index", ctypes.c_void_p), ("perm_pe", ctypes.c_void_p),
+                ("merged_lcp", ctypes.c_void_p), ("recv_counts", ctypes.c_void_p)]
+
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_U32 = ctypes.c_uint32
+_I = ctypes.c_int
+_SIGS = {
+    "dsss_ctx_create": (_I, [_I, _U64, ctypes.POINTER(_P)]),
+    "dsss_ctx_destroy": (_I, [_P]),
+    "dsss_ctx_scratch_bytes": (_U64, [_P]),
+    "dsss_last_error": (ctypes.c_char_p, []),
+    "dsss_abi_version": (_I, []),
+    "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
+    "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
+                               _P]),
+    "dsss_local_sort_lcp": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), _P, _P, _P]),
+    "dsss_dp_prefixes": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _U32, _P, _P]),
+    "dsss_prefix_hash": (_I, [ctypes.POINTER(Arena), _P, _U64, _U32, _P, _P]),
+    "dsss_partition": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, ctypes.POINTER(Opts), _P, _P]),
+    "dsss_adjacent_lcp": (_I, [_P, ctypes.POINTER(Arena), _P, _U64, _P, _P]),
+    "dsss_gen_dn": (_I, [_U64, _U32, _U32, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P]),
+    "dsss_gen_markov_text": (_I, [_U64, ctypes.c_double, _U64, _P]),
+    "dsss_gen_suffixes": (_I, [_U64, _U32, _P, _P]),
+    "dsss_gen_request": (_I, [_U64, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded libdsss (raises if the library was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run build() (python build.py) first")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def check(rc: int):
+    if rc != DSSS_OK:
+        raise DsssError(rc, lib().dsss_last_error().decode(errors="replace"))
+
+
+def _ptr(a) -> Optional[int]:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+# ------------------------------------------------------------------ inputs --
+@dataclass
+class HostStrings:
+    """Strings in host memory: chars (uint8, padded), offsets (uint64), lengths (uint32)."""
+    chars: np.ndarray
+    offsets: np.ndarray
+    lengths: np.ndarray
+    char_bytes: int
+
+    @property
+    def n(self) -> int:
+        return int(self.offsets.shape[0])
+
+    def get(self, i: int) -> bytes:
+        o, l = int(self.offsets[i]), int(self.lengths[i])
+        return self.chars[o:o + l].tobytes()
+
+    def arena(self) -> Arena:
+        return Arena(_ptr(self.chars), self.char_bytes, _ptr(self.offsets), _ptr(self.lengths), self.n)
+
+
+def _alloc_host(nbytes: int, dtype, pinned: bool):
+    if pinned:
+        import torch
+        t = torch.empty(nbytes // np.dtype(dtype).itemsize, dtype=_TORCH_DT[np.dtype(dtype)], pin_memory=True)
+        return t.numpy()
+    return np.empty(nbytes // np.dtype(dtype).itemsize, dtype=dtype)
+
+
+def _torch_dt():
+    import torch
+    return {np.dtype(np.uint8): torch.uint8, np.dtype(np.uint32): torch.uint32, np.dtype(np.uint64): torch.uint64}
+
+
+class _LazyDT(dict):
+    def __missing__(self, k):
+        self.update(_torch_dt())
+        return dict.__getitem__(self, k)
+
+
+_TORCH_DT = _LazyDT()
+
+
+def gen_dn(n: int, length: int, k: int, seed: int = 1, long_len: int = 0, long_k: int = 0, frac_long: float = 0.0,
+           pinned: bool = False) -> HostStrings:
+    """D/N-ratio strings (see dsss_gen_dn); each string is followed by a NUL."""
+    cb = ctypes.c_uint64(0)
+    check(lib().dsss_gen_dn(n, length, k, long_len, long_k, frac_long, seed, None, None, None, ctypes.byref(cb)))
+    total = cb.value
+    chars = _alloc_host(total + PAD, np.uint8, pinned)
+    offs = _alloc_host(max(n, 1) * 8, np.uint64, pinned)[:n]
+    lens = _alloc_host(max(n, 1) * 4, np.uint32, pinned)[:n]
+    check(lib().dsss_gen_dn(n, length, k, long_len, long_k, frac_long, seed, _ptr(chars), _ptr(offs), _ptr(lens),
+                            ctypes.byref(cb)))
+    chars[total:] = 0
+    return HostStrings(chars, offs, lens, total)
+
+
+def gen_suffix_strings(text_len: int, max_len: int = 256, seed: int = 1, copy_prob: float = 0.01,
+                       pinned: bool = False) -> HostStrings:
+    """All suffixes of a seeded order-3 Markov ACGT text, truncated to max_len."""
+    chars = _alloc_host(text_len + PAD, np.uint8, pinned)
+    check(lib().dsss_gen_markov_text(text_len, copy_prob, seed, _ptr(chars)))
+    chars[text_len:] = 0
+    offs = _alloc_host(max(text_len, 1) * 8, np.uint64, pinned)[:text_len]
+    lens = _alloc_host(max(text_len, 1) * 4, np.uint32, pinned)[:text_len]
+    check(lib().dsss_gen_suffixes(text_len, max_len, _ptr(offs), _ptr(lens)))
+    return HostStrings(chars, offs, lens, text_len)
+
+
+def gen_request(n: int, seed: int, min_len: int = 8, max_len: int = 256, zipf_s: float = 1.2,
+                pinned: bool = False) -> HostStrings:
+    cb = ctypes.c_uint64(0)
+    check(lib().dsss_gen_request(n, min_len, max_len, zipf_s, seed, None, None, None, ctypes.byref(cb)))
+    total = cb.value
+    chars = _alloc_host(total + PAD, np.uint8, pinned)
+    offs = _alloc_host(max(n, 1) * 8, np.uint64, pinned)[:n]
+    lens = _alloc_host(max(n, 1) * 4, np.uint32, pinned)[:n]
+    check(lib().dsss_gen_request(n, min_len, max_len, zipf_s, seed, _ptr(chars), _ptr(offs), _ptr(lens),
+                                 ctypes.byref(cb)))
+    chars[total:] = 0
+    return HostStrings(chars, offs, lens, total)
+
+
+def from_bytes_list(strs) -> HostStrings:
+    """Arena of Python byte strings laid out back to back with NULs."""
+    n = len(strs)
+    lens = np.array([len(s) for s in strs], dtype=np.uint32)
+    offs = np.zeros(n, dtype=np.uint64)
+    if n:
+        offs[1:] = np.cumsum(lens.astype(np.uint64) + 1)[:-1]
+    total = int(lens.astype(np.uint64).sum()) + n
+    chars = np.zeros(total + PAD, dtype=np.uint8)
+    for i, s in enumerate(strs):
+        o = int(offs[i])
+        chars[o:o + len(s)] = np.frombuffer(s, dtype=np.uint8)
+    return HostStrings(chars, offs, lens, total)
+
+
+def equal_parts(n: int, p: int) -> np.ndarray:
+    """PE boundaries of p contiguous slices with equal string counts."""
+    return np.array([q * n // p for q in range(p + 1)], dtype=np.uint64)
+
+
+# ------------------------------------------------------------------ device --
+class DeviceStrings:
+    """A device copy of HostStrings (torch tensors; chars padded with zeros)."""
+
+    def __init__(self, hs: HostStrings, device="cuda"):
+        import torch
+        self.chars = torch.from_numpy(hs.chars).to(device)
+        self.offsets = torch.from_numpy(hs.offsets.view(np.int64)).to(device)
+        self.lengths = torch.from_numpy(hs.lengths.view(np.int32)).to(device)
+        self.char_bytes = hs.char_bytes
+        self.n = hs.n
+
+    def arena(self) -> Arena:
+        return Arena(self.chars.data_ptr(), self.char_bytes, self.offsets.data_ptr(), self.lengths.data_ptr(), self.n)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Context:
+    """Owns the library's reusable device scratch (one per host thread)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().dsss_ctx_create(device, hbm_budget, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().dsss_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(lib().dsss_ctx_scratch_bytes(self.h))
+
+
+def _opts(sampler=0, sampling_factor=2, small_sort_max=0, flags=0) -> Opts:
+    return Opts(sampler, sampling_factor, small_sort_max, flags)
+
+
+def _empty(n, dtype="int32", device="cuda"):
+    import torch
+    return torch.empty(max(n, 1), dtype=getattr(torch, dtype), device=device)
+
+
+def pd_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, sampler: int = 0, merged_lcp: bool = True,
+            local_lcp: bool = False, small_sort_max: int = 0, stream=None, out=None):
+    """DistributedPrefixDoublingSort::sort on the device.  Returns a dict of
+    torch tensors (device) plus host numpy intervals / recv_counts."""
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    if out is None:
+        out = dict(local_order=_empty(n), dp=_empty(n), perm_index=_empty(n), perm_pe=_empty(n),
+                   merged_lcp=_empty(n) if merged_lcp else None, local_lcp=_empty(n) if local_lcp else None,
+                   intervals=np.zeros(p * p, dtype=np.uint64), recv_counts=np.zeros(p, dtype=np.uint64))
+    res = PdResult(_ptr(out["local_order"]), _ptr(out["local_lcp"]), _ptr(out["dp"]), _ptr(out["intervals"]),
+                   _ptr(out["perm_index"]), _ptr(out["perm_pe"]), _ptr(out["merged_lcp"]), _ptr(out["recv_counts"]))
+    a = ds.arena()
+    o = _opts(sampler, 2, small_sort_max, FLAG_LOCAL_LCP if local_lcp else 0)
+    check(lib().dsss_pd_sort(ctx.h, ctypes.byref(a), p, _ptr(pb), ctypes.byref(o), ctypes.byref(res),
+                             _stream_ptr(stream)))
+    out["part_begin"] = pb
+    return out
+
+
+def pd_sort_host(ctx: Context, hs: HostStrings, p: int, part_begin=None, sampler: int = 0, merged_lcp: bool = True,
+                 out=None, pinned: bool = False, stream=None):
+    """The same path with host buffers (copies in and out inside the call)."""
+    n = hs.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    if out is None:
+        mk = (lambda: _alloc_host(max(n, 1) * 4, np.uint32, pinned)[:max(n, 1)])
+        out = dict(local_order=mk(), dp=mk(), perm_index=mk(), perm_pe=mk(), merged_lcp=mk() if merged_lcp else None,
+                   local_lcp=None, intervals=np.zeros(p * p, dtype=np.uint64), recv_counts=np.zeros(p, dtype=np.uint64))
+    res = PdResult(_ptr(out["local_order"]), None, _ptr(out["dp"]), _ptr(out["intervals"]), _ptr(out["perm_index"]),
+                   _ptr(out["perm_pe"]), _ptr(out["merged_lcp"]), _ptr(out["recv_counts"]))
+    a = hs.arena()
+    o = _opts(sampler)
+    check(lib().dsss_pd_sort_host(ctx.h, ctypes.byref(a), p, _ptr(pb), ctypes.byref(o), ctypes.byref(res),
+                                  _stream_ptr(stream)))
+    out["part_begin"] = pb
+    return out
+
+
+def local_sort_lcp(ctx: Context, ds: DeviceStrings, p: int = 1, part_begin=None, small_sort_max: int = 0,
+                   stream=None):
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    order, lcp = _empty(n), _empty(n)
+    o = _opts(small_sort_max=small_sort_max)
+    check(lib().dsss_local_sort_lcp(ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), ctypes.byref(o), _ptr(order),
+                                    _ptr(lcp), _stream_ptr(stream)))
+    return order[:n], lcp[:n]
+
+
+def dp_prefixes(ctx: Context, ds: DeviceStrings, order, lcp, p: int = 1, part_begin=None, max_rounds: int = 64,
+                stream=None):
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    dp = _empty(n)
+    counts = np.zeros(max_rounds, dtype=np.uint64)
+    rounds = ctypes.c_uint32(0)
+    check(lib().dsss_dp_prefixes(ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), _ptr(order), _ptr(lcp), _ptr(dp),
+                                 _ptr(counts), max_rounds, ctypes.byref(rounds), _stream_ptr(stream)))
+    return dp[:n], counts[:rounds.value]
+
+
+def prefix_hash(ds: DeviceStrings, ids, depth: int, stream=None):
+    import torch
+    m = int(ids.shape[0])
+    out = torch.empty(max(m, 1), dtype=torch.int64, device=ids.device)
+    check(lib().dsss_prefix_hash(ctypes.byref(ds.arena()), _ptr(ids), m, depth, _ptr(out), _stream_ptr(stream)))
+    return out[:m]
+
+
+def partition(ctx: Context, ds: DeviceStrings, order, dp, p: int, part_begin=None, sampler: int = 0, stream=None):
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    iv = np.zeros(p * p, dtype=np.uint64)
+    o = _opts(sampler)
+    check(lib().dsss_partition(ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), _ptr(order), _ptr(dp), ctypes.byref(o),
+                               _ptr(iv), _stream_ptr(stream)))
+    return iv.reshape(p, p)
+
+
+def adjacent_lcp(ctx: Context, ds: DeviceStrings, order, stream=None):
+    m = int(order.shape[0])
+    out = _empty(m)
+    check(lib().dsss_adjacent_lcp(ctx.h, ctypes.byref(ds.arena()), _ptr(order), m, _ptr(out), _stream_ptr(stream)))
+    return out[:m]

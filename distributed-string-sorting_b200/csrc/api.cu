@@ -1,0 +1,386 @@
+// C ABI entry points: the full prefix-doubling path and one entry per stage.
+//
+// The full path (dsss_pd_sort) is laid out for one GPU holding every PE:
+//   1. one string sort of all n strings (K3, LCP as by-product);
+//   2. distinguishing-prefix rounds over that global order (K1/K2) — the
+//      result per string does not depend on the PE split;
+//   3. stable multisplit by PE of the global order gives each PE's local sorted
+//      order (a subsequence of a sorted sequence is sorted), i.e. exactly what
+//      radixsort_CI3 produces per PE (prefix_doubling.hpp:228);
+//   4. partition (K5) on those local orders;
+//   5. every string's bucket follows from its PE and local index; a stable
+//      multisplit of the global order by bucket is each receiving PE's merged
+//      sequence — what AllToAllStringImplPrefixDoubling + choose_merge deliver
+//      (prefix_doubling.hpp:254-281) — with (local index, PE) as the
+//      permutation (:282-290) and merged LCPs taken from the global LCPs.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "dp.cuh"
+#include "internal.cuh"
+#include "partition.cuh"
+#include "strsort.cuh"
+#include "util.cuh"
+
+namespace dsss {
+
+static int check_parts(uint32_t p, const uint64_t* pb, uint64_t n) {
+    if (p == 0) return fail(DSSS_EINVAL, "p must be >= 1");
+    if (!pb) return fail(DSSS_EINVAL, "part_begin is NULL");
+    if (pb[0] != 0 || pb[p] != n) return fail(DSSS_EINVAL, "part_begin must start at 0 and end at n");
+    for (uint32_t q = 0; q < p; ++q)
+        if (pb[q + 1] < pb[q]) return fail(DSSS_EINVAL, "part_begin must be non-decreasing");
+    return DSSS_OK;
+}
+
+static ArenaDev view(const dsss_arena* a) { return ArenaDev{a->chars, a->offsets, a->lengths, a->n}; }
+
+static uint32_t factor_of(const dsss_opts* o) { return (o && o->sampling_factor) ? o->sampling_factor : 2; }
+static uint32_t sampler_of(const dsss_opts* o) { return o ? o->sampler : DSSS_SAMPLER_NUM_STRINGS; }
+static uint32_t smallmax_of(const dsss_opts* o) { return o ? o->small_sort_max : 0; }
+
+__global__ void k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p, uint32_t* pe) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t s = ord[g];
+    uint32_t lo = 0, hi = p;  // last q with pb[q] <= s
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (pb[mid] <= s) lo = mid;
+        else hi = mid;
+    }
+    pe[g] = lo;
+}
+
+__global__ void k_to_local(const uint32_t* ord, const uint32_t* dpg, const uint32_t* pe, const uint32_t* dest,
+                           const uint64_t* pb, uint64_t n, uint32_t* local_order, uint32_t* dp_local,
+                           uint32_t* g2l) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t d = dest[g];
+    local_order[d] = ord[g];
+    dp_local[d] = dpg[g];
+    g2l[g] = d - (uint32_t)pb[pe[g]];
+}
+
+__global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p, uint64_t n,
+                            uint32_t* bucket) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint64_t* b = bounds + (uint64_t)pe[g] * (p + 1);
+    const uint64_t li = g2l[g];
+    uint32_t lo = 0, hi = p;  // last r with b[r] <= li (b[0] = 0, b[p] = n_q > li)
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (b[mid] <= li) lo = mid;
+        else hi = mid;
+    }
+    bucket[g] = lo;
+}
+
+__global__ void k_perm(const uint32_t* opos, const uint32_t* g2l, const uint32_t* pe, uint64_t n, uint32_t* perm_index,
+                       uint32_t* perm_pe, uint32_t* out2g) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t o = opos[g];
+    perm_index[o] = g2l[g];
+    perm_pe[o] = pe[g];
+    out2g[o] = (uint32_t)g;
+}
+
+__global__ void k_merged_lcp(const uint32_t* out2g, const uint32_t* lcpg, const uint64_t* recv_begin, uint32_t p,
+                             uint64_t n, uint32_t* merged) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    uint32_t lo = 0, hi = p;  // is o the first string of some PE's merged run?
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (recv_begin[mid] <= o) lo = mid;
+        else hi = mid;
+    }
+    bool first = false;
+    for (uint32_t r = lo; r < p && recv_begin[r] <= o; ++r)
+        if (recv_begin[r] == o) { first = true; break; }
+    if (first) { merged[o] = 0; return; }
+    const uint32_t g = out2g[o], gp = out2g[o - 1];
+    uint32_t l = 0xFFFFFFFFu;
+    for (uint32_t x = gp + 1; x <= g; ++x) l = min(l, lcpg[x]);  // LCP over the skipped run
+    merged[o] = l;
+}
+
+__global__ void k_zero_starts(uint32_t* a, const uint64_t* pb, uint32_t p) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < p && pb[q] < pb[q + 1]) a[pb[q]] = 0;
+}
+
+struct PdLayout {
+    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *opos, *out2g, *nlong;
+    uint64_t *pb, *bounds, *recv_begin;
+    void* ms;
+    SortLayout sort;
+    DpLayout dp;
+    PartitionLayout part;
+};
+
+static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t p, uint32_t factor, uint32_t small_max) {
+    uint64_t N = n ? n : 1;
+    L.ord = c.take<uint32_t>(N);
+    L.lcp = c.take<uint32_t>(N);
+    L.dpg = c.take<uint32_t>(N);
+    L.pe = c.take<uint32_t>(N);
+    L.g2l = c.take<uint32_t>(N);
+    L.tmp = c.take<uint32_t>(N);
+    L.opos = c.take<uint32_t>(N);
+    L.out2g = c.take<uint32_t>(N);
+    L.nlong = c.take<uint32_t>(1);
+    L.pb = c.take<uint64_t>(p + 1);
+    L.bounds = c.take<uint64_t>((uint64_t)p * (p + 1));
+    L.recv_begin = c.take<uint64_t>(p + 1);
+    L.ms = c.take<unsigned char>(multisplit_scratch_bytes(N, p));
+    layout_sort(c, L.sort, N, 1, small_max);
+    layout_dp(c, L.dp, N);
+    layout_partition(c, L.part, N, p, factor);
+}
+
+static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* pb, const dsss_opts* opts,
+                       dsss_pd_result* out, cudaStream_t st) {
+    DSSS_TRY(check_arena(in));
+    DSSS_TRY(check_parts(p, pb, in->n));
+    if (!out || !out->local_order || !out->recv_counts) return fail(DSSS_EINVAL, "result arrays missing");
+    if (p > 1 && (!out->dp || !out->intervals || !out->perm_index || !out->perm_pe))
+        return fail(DSSS_EINVAL, "result arrays missing");
+    if (p > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "p > %u PEs per GPU is not supported", MAX_SPLIT_BUCKETS);
+    const uint64_t n = in->n;
+    const uint32_t factor = factor_of(opts), smax = smallmax_of(opts);
+    const bool want_local_lcp = opts && (opts->flags & DSSS_FLAG_LOCAL_LCP) && out->local_lcp;
+    Carve sz(nullptr);
+    PdLayout L;
+    layout_pd(sz, L, n, p, factor, smax);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_pd(c, L, n, p, factor, smax);
+    uint32_t* pin = (uint32_t*)ctx->pin;
+    const ArenaDev a = view(in);
+    if (n == 0) {
+        for (uint32_t r = 0; r < p; ++r) out->recv_counts[r] = 0;
+        if (p > 1)
+            for (uint64_t k = 0; k < (uint64_t)p * p; ++k) out->intervals[k] = 0;
+        return DSSS_OK;
+    }
+    // 1. one sort of all strings
+    uint64_t all[2] = {0, n};
+    DSSS_TRY(sort_strings(L.sort, a, n, 1, all, nullptr, L.ord, L.lcp, smax, pin, st));
+    if (p == 1) {  // prefix_doubling.hpp:236: one PE sorts locally and returns no permutation
+        DSSS_CUDA(cudaMemcpyAsync(out->local_order, L.ord, n * 4, cudaMemcpyDeviceToDevice, st));
+        if (want_local_lcp) DSSS_CUDA(cudaMemcpyAsync(out->local_lcp, L.lcp, n * 4, cudaMemcpyDeviceToDevice, st));
+        out->recv_counts[0] = 0;
+        return DSSS_OK;
+    }
+    // 2. distinguishing prefixes over the global order
+    DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st));
+    // 3. local orders per PE
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe);
+    DSSS_TRY(multisplit(L.pe, n, p, L.tmp, L.ms, st));
+    k_to_local<<<grid_for(n, 256), 256, 0, st>>>(L.ord, L.dpg, L.pe, L.tmp, L.pb, n, out->local_order, out->dp,
+                                                L.g2l);
+    DSSS_CUDA(cudaGetLastError());
+    // 4. partition
+    DSSS_TRY(partition_pes(L.part, ctx, a, p, pb, out->local_order, out->dp, sampler_of(opts), factor,
+                           out->intervals, st));
+    // 5. buckets and the merged sequences
+    std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), recv(p + 1, 0);
+    for (uint32_t q = 0; q < p; ++q) {
+        bounds[(uint64_t)q * (p + 1)] = 0;
+        for (uint32_t r = 0; r < p; ++r) {
+            uint64_t v = out->intervals[(uint64_t)q * p + r];
+            bounds[(uint64_t)q * (p + 1) + r + 1] = bounds[(uint64_t)q * (p + 1) + r] + v;
+            recv[r + 1] += v;
+        }
+    }
+    for (uint32_t r = 0; r < p; ++r) {
+        out->recv_counts[r] = recv[r + 1];
+        recv[r + 1] += recv[r];
+    }
+    DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp);
+    DSSS_TRY(multisplit(L.tmp, n, p, L.opos, L.ms, st));
+    k_perm<<<grid_for(n, 256), 256, 0, st>>>(L.opos, L.g2l, L.pe, n, out->perm_index, out->perm_pe, L.out2g);
+    if (out->merged_lcp)
+        k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->merged_lcp);
+    if (want_local_lcp) {
+        DSSS_TRY(adjacent_lcp(a, out->local_order, n, out->local_lcp, L.tmp, L.nlong, st));
+        k_zero_starts<<<grid_for(p, 128), 128, 0, st>>>(out->local_lcp, L.pb, p);
+    }
+    DSSS_CUDA(cudaGetLastError());
+    // The host vectors above were copied asynchronously; finish before they go.
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    return DSSS_OK;
+}
+
+}  // namespace dsss
+
+using namespace dsss;
+
+extern "C" {
+
+int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, const dsss_opts* opts,
+                 dsss_pd_result* out, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    return pd_sort_dev(ctx, in, p, part_begin, opts, out, (cudaStream_t)stream);
+}
+
+int dsss_local_sort_lcp(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                        const dsss_opts* opts, uint32_t* order, uint32_t* lcp, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    DSSS_TRY(check_arena(in));
+    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (in->n && (!order || !lcp)) return fail(DSSS_EINVAL, "order/lcp is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t smax = smallmax_of(opts);
+    Carve sz(nullptr);
+    SortLayout L;
+    layout_sort(sz, L, in->n, p, smax);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_sort(c, L, in->n, p, smax);
+    return sort_strings(L, view(in), in->n, p, part_begin, nullptr, order, lcp, smax, (uint32_t*)ctx->pin, st);
+}
+
+int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                     const uint32_t* order, const uint32_t* lcp, uint32_t* dp, uint64_t* round_counts,
+                     uint32_t max_rounds, uint32_t* rounds, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    DSSS_TRY(check_arena(in));
+    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (in->n && (!order || !lcp || !dp)) return fail(DSSS_EINVAL, "order/lcp/dp is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    Carve sz(nullptr);
+    DpLayout L;
+    layout_dp(sz, L, in->n);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_dp(c, L, in->n);
+    // The PE split needs no extra handling: every PE's first LCP is 0, so no
+    // string is an LCP duplicate of the previous PE's last one.
+    return dp_rounds(L, view(in), in->n, order, lcp, dp, round_counts, max_rounds, rounds, (uint32_t*)ctx->pin,
+                     (cudaStream_t)stream);
+}
+
+int dsss_prefix_hash(const dsss_arena* in, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* hash,
+                     dsss_stream_t stream) {
+    DSSS_TRY(check_arena(in));
+    if (m && (!ids || !hash)) return fail(DSSS_EINVAL, "ids/hash is NULL");
+    return prefix_hash(view(in), ids, m, depth, hash, (cudaStream_t)stream);
+}
+
+int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                   const uint32_t* order, const uint32_t* dp, const dsss_opts* opts, uint64_t* intervals,
+                   dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    DSSS_TRY(check_arena(in));
+    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (!intervals || (in->n && (!order || !dp))) return fail(DSSS_EINVAL, "order/dp/intervals is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    const uint32_t factor = factor_of(opts);
+    Carve sz(nullptr);
+    PartitionLayout L;
+    layout_partition(sz, L, in->n, p, factor);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    Carve c(ctx->ws);
+    layout_partition(c, L, in->n, p, factor);
+    return partition_pes(L, ctx, view(in), p, part_begin, order, dp, sampler_of(opts), factor, intervals,
+                         (cudaStream_t)stream);
+}
+
+int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
+                      dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    DSSS_TRY(check_arena(in));
+    if (m && (!order || !lcp)) return fail(DSSS_EINVAL, "order/lcp is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    Carve sz(nullptr);
+    sz.take<uint32_t>(m + 1);
+    sz.take<uint32_t>(1);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    Carve c(ctx->ws);
+    uint32_t* longq = c.take<uint32_t>(m + 1);
+    uint32_t* nlong = c.take<uint32_t>(1);
+    return adjacent_lcp(view(in), order, m, lcp, longq, nlong, (cudaStream_t)stream);
+}
+
+// Host-memory variant: device copies of the arena and results live in a
+// second context buffer so repeated calls reuse it.
+int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                      const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    if (!in) return fail(DSSS_EINVAL, "arena is NULL");
+    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (!out) return fail(DSSS_EINVAL, "result is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t n = in->n;
+    const bool llcp = opts && (opts->flags & DSSS_FLAG_LOCAL_LCP) && out->local_lcp;
+    auto plan = [&](Carve& c, dsss_arena& da, dsss_pd_result& dr) {
+        uint8_t* chars = c.take<uint8_t>(in->char_bytes + 64);
+        uint64_t* off = c.take<uint64_t>(n ? n : 1);
+        uint32_t* len = c.take<uint32_t>(n ? n : 1);
+        da = dsss_arena{chars, in->char_bytes, off, len, n};
+        dr = *out;
+        dr.local_order = c.take<uint32_t>(n ? n : 1);
+        dr.local_lcp = llcp ? c.take<uint32_t>(n ? n : 1) : nullptr;
+        dr.dp = c.take<uint32_t>(n ? n : 1);
+        dr.perm_index = c.take<uint32_t>(n ? n : 1);
+        dr.perm_pe = c.take<uint32_t>(n ? n : 1);
+        dr.merged_lcp = out->merged_lcp ? c.take<uint32_t>(n ? n : 1) : nullptr;
+    };
+    Carve sz(nullptr);
+    dsss_arena da;
+    dsss_pd_result dr;
+    plan(sz, da, dr);
+    // The io buffer sits in front of the pipeline's own scratch.
+    Carve pdsz(nullptr);
+    PdLayout PL;
+    layout_pd(pdsz, PL, n, p, factor_of(opts), smallmax_of(opts));
+    const uint64_t io_bytes = (sz.used + 255) & ~255ull;
+    DSSS_TRY(ensure_ws(ctx, io_bytes + pdsz.used));
+    Carve c(ctx->ws);
+    plan(c, da, dr);
+    if (in->char_bytes) DSSS_CUDA(cudaMemcpyAsync((void*)da.chars, in->chars, in->char_bytes, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemsetAsync((uint8_t*)da.chars + in->char_bytes, 0, 64, st));
+    if (n) {
+        DSSS_CUDA(cudaMemcpyAsync((void*)da.offsets, in->offsets, n * 8, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync((void*)da.lengths, in->lengths, n * 4, cudaMemcpyHostToDevice, st));
+    }
+    // Run the device path on the scratch behind the io block.
+    Ctx sub = *ctx;
+    sub.ws = (char*)ctx->ws + io_bytes;
+    sub.ws_cap = ctx->ws_cap - io_bytes;
+    sub.budget = 0;
+    int rc = pd_sort_dev(&sub, &da, p, part_begin, opts, &dr, st);
+    ctx->pin = sub.pin;
+    ctx->pin_cap = sub.pin_cap;
+    if (rc != DSSS_OK) return rc;
+    if (n) {
+        DSSS_CUDA(cudaMemcpyAsync(out->local_order, dr.local_order, n * 4, cudaMemcpyDeviceToHost, st));
+        if (llcp) DSSS_CUDA(cudaMemcpyAsync(out->local_lcp, dr.local_lcp, n * 4, cudaMemcpyDeviceToHost, st));
+        if (p > 1) {
+            DSSS_CUDA(cudaMemcpyAsync(out->dp, dr.dp, n * 4, cudaMemcpyDeviceToHost, st));
+            DSSS_CUDA(cudaMemcpyAsync(out->perm_index, dr.perm_index, n * 4, cudaMemcpyDeviceToHost, st));
+            DSSS_CUDA(cudaMemcpyAsync(out->perm_pe, dr.perm_pe, n * 4, cudaMemcpyDeviceToHost, st));
+            if (out->merged_lcp)
+                DSSS_CUDA(cudaMemcpyAsync(out->merged_lcp, dr.merged_lcp, n * 4, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    return DSSS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,203 @@
+// Context, error reporting, scratch management and the device-wide scan.
+#include <cstdarg>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace dsss {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int ensure_ws(Ctx* c, uint64_t bytes) {
+    if (bytes <= c->ws_cap) return DSSS_OK;
+    if (c->budget && bytes > c->budget)
+        return fail(DSSS_ENOMEM, "scratch of %llu bytes exceeds the context budget of %llu bytes",
+                    (unsigned long long)bytes, (unsigned long long)c->budget);
+    if (c->ws) {
+        DSSS_CUDA(cudaDeviceSynchronize());
+        DSSS_CUDA(cudaFree(c->ws));
+        c->ws = nullptr;
+        c->ws_cap = 0;
+    }
+    uint64_t want = bytes + bytes / 8;  // headroom so slightly larger calls reuse it
+    if (c->budget && want > c->budget) want = bytes;
+    cudaError_t e = cudaMalloc(&c->ws, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->ws = nullptr;
+        return fail(DSSS_ENOMEM, "cudaMalloc of %llu scratch bytes failed: %s", (unsigned long long)want,
+                    cudaGetErrorString(e));
+    }
+    c->ws_cap = want;
+    return DSSS_OK;
+}
+
+int ensure_pin(Ctx* c, uint64_t bytes) {
+    if (bytes <= c->pin_cap) return DSSS_OK;
+    if (c->pin) {
+        DSSS_CUDA(cudaFreeHost(c->pin));
+        c->pin = nullptr;
+        c->pin_cap = 0;
+    }
+    uint64_t want = bytes < 4096 ? 4096 : bytes * 2;
+    DSSS_CUDA(cudaMallocHost(&c->pin, want));
+    c->pin_cap = want;
+    return DSSS_OK;
+}
+
+int check_arena(const dsss_arena* a) {
+    if (!a) return fail(DSSS_EINVAL, "arena is NULL");
+    if (a->n && (!a->chars || !a->offsets || !a->lengths))
+        return fail(DSSS_EINVAL, "arena with n = %llu has a NULL array", (unsigned long long)a->n);
+    if (a->n >= (1ull << 32)) return fail(DSSS_EINVAL, "n = %llu exceeds 2^32-1 strings", (unsigned long long)a->n);
+    if (((uintptr_t)a->chars & 7) != 0) return fail(DSSS_EINVAL, "arena chars must be 8-byte aligned");
+    return DSSS_OK;
+}
+
+// ----------------------------------------------------- exclusive scan u32 ----
+// Three passes: per-tile sums, a single-CTA scan of the sums, per-tile scan.
+constexpr int SCAN_NT = 512, SCAN_IPT = 8, SCAN_TILE = SCAN_NT * SCAN_IPT;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) sh[lane] = s;
+    }
+    __syncthreads();
+    uint32_t base = w ? sh[w - 1] : 0;
+    if (total) *total = sh[nw - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+__global__ void scan_tile_sums(const uint32_t* in, uint64_t n, uint32_t* sums) {
+    __shared__ uint32_t sh[32];
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint32_t s = 0;
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + (uint64_t)k * SCAN_NT + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint32_t tot;
+    block_excl_scan(s, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void scan_sums(uint32_t* sums, uint64_t m, uint32_t* total) {
+    __shared__ uint32_t sh[32];
+    uint32_t carry = 0;
+    for (uint64_t b = 0; b < m; b += SCAN_NT) {
+        uint64_t i = b + threadIdx.x;
+        uint32_t v = i < m ? sums[i] : 0;
+        uint32_t tot;
+        uint32_t ex = block_excl_scan(v, sh, &tot);
+        if (i < m) sums[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void scan_tiles(const uint32_t* in, uint32_t* out, uint64_t n, const uint32_t* sums) {
+    __shared__ uint32_t sh[32];
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_IPT;
+    uint32_t v[SCAN_IPT];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        s += v[k];
+    }
+    uint32_t ex = block_excl_scan(s, sh, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+}
+
+uint64_t scan_scratch_bytes(uint64_t n) { return ((n + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(uint32_t); }
+
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total, void* scratch,
+                       cudaStream_t st) {
+    uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    uint32_t* sums = (uint32_t*)scratch;
+    if (n == 0) {
+        if (total) DSSS_CUDA(cudaMemsetAsync(total, 0, sizeof(uint32_t), st));
+        return DSSS_OK;
+    }
+    scan_tile_sums<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, n, sums);
+    scan_sums<<<1, SCAN_NT, 0, st>>>(sums, tiles, total);
+    scan_tiles<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, out, n, sums);
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+}  // namespace dsss
+
+using namespace dsss;
+
+extern "C" {
+
+int dsss_ctx_create(int device, uint64_t hbm_budget_bytes, dsss_ctx** out) {
+    if (!out) return fail(DSSS_EINVAL, "out is NULL");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(DSSS_EDEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count) return fail(DSSS_EINVAL, "device %d out of range (%d devices)", device, count);
+    DSSS_CUDA(cudaSetDevice(device));
+    dsss_ctx* c = new dsss_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    *out = c;
+    return DSSS_OK;
+}
+
+int dsss_ctx_destroy(dsss_ctx* c) {
+    if (!c) return DSSS_OK;
+    if (c->ws) cudaFree(c->ws);
+    if (c->pin) cudaFreeHost(c->pin);
+    delete c;
+    return DSSS_OK;
+}
+
+uint64_t dsss_ctx_scratch_bytes(const dsss_ctx* c) { return c ? c->ws_cap : 0; }
+
+const char* dsss_last_error(void) { return g_err; }
+
+int dsss_abi_version(void) { return DSSS_ABI_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,30 @@
+// Distinguishing-prefix rounds (K1/K2); see dp.cu.
+#pragma once
+#include "internal.cuh"
+
+namespace dsss {
+
+struct DpLayout {
+    uint32_t* cand[2];
+    uint32_t* flag;
+    uint32_t* pos;
+    uint32_t* slot;
+    unsigned long long* tkeys;
+    uint8_t* tdup;
+    uint64_t slots;
+    uint32_t* counters;
+    unsigned char* scan;
+};
+
+void layout_dp(Carve& c, DpLayout& L, uint64_t n);
+
+// order/lcp: strings in sorted order per PE (lcp 0 at every PE start); dp[i]
+// receives the distinguishing-prefix length of the string at position i.
+int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
+              uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
+              cudaStream_t st);
+
+int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out,
+                cudaStream_t st);
+
+}  // namespace dsss

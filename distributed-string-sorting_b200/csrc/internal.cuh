@@ -1,0 +1,243 @@
+// Shared internals of libdsss: context, error reporting, scratch carving and
+// the device helpers every kernel uses (big-endian 8-byte key loads, XXH64).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/dsss.h"
+
+namespace dsss {
+
+// ---------------------------------------------------------------- errors ----
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+
+#define DSSS_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::dsss::fail(DSSS_EDEVICE, "%s:%d %s: %s", __FILE__, __LINE__, #call,    \
+                                cudaGetErrorString(e_));                                  \
+    } while (0)
+
+#define DSSS_TRY(expr)             \
+    do {                           \
+        int r_ = (expr);           \
+        if (r_ != DSSS_OK) return r_; \
+    } while (0)
+
+// --------------------------------------------------------------- context ----
+struct Ctx {
+    int device = 0;
+    uint64_t budget = 0;     // 0 = unlimited
+    void* ws = nullptr;      // device scratch, grown on demand
+    uint64_t ws_cap = 0;
+    void* pin = nullptr;     // pinned host staging for small read-backs
+    uint64_t pin_cap = 0;
+};
+
+// Bump allocator over the context scratch.  Run a layout twice: first with
+// sizing = true to learn the total, then for real after ensure_ws().
+struct Carve {
+    char* base;
+    uint64_t used = 0;
+    bool sizing;
+    explicit Carve(void* b) : base((char*)b), sizing(b == nullptr) {}
+    template <typename T>
+    T* take(uint64_t count) {
+        used = (used + 255) & ~255ull;
+        T* p = sizing ? nullptr : (T*)(base + used);
+        used += count * sizeof(T);
+        return p;
+    }
+};
+
+int ensure_ws(Ctx* c, uint64_t bytes);
+int ensure_pin(Ctx* c, uint64_t bytes);
+
+// ------------------------------------------------------------ arena view ----
+struct ArenaDev {
+    const uint8_t* chars;
+    const uint64_t* off;
+    const uint32_t* len;
+    uint64_t n;
+};
+
+int check_arena(const dsss_arena* a);
+
+// --------------------------------------------------------- device helpers ----
+__device__ __forceinline__ uint64_t bswap64(uint64_t x) {
+    uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+    return ((uint64_t)__byte_perm(lo, 0, 0x0123) << 32) | (uint64_t)__byte_perm(hi, 0, 0x0123);
+}
+
+// 8 bytes at an arbitrary address as a little-endian word, from two aligned
+// 8-byte loads.  Reads up to 15 bytes past p; the arena contract pads 32.
+__device__ __forceinline__ uint64_t load_le8(const uint8_t* p) {
+    uintptr_t a = (uintptr_t)p;
+    const unsigned long long* q = (const unsigned long long*)(a & ~(uintptr_t)7);
+    unsigned sh = (unsigned)(a & 7) * 8;
+    uint64_t lo = __ldg(q);
+    if (sh == 0) return lo;
+    uint64_t hi = __ldg(q + 1);
+    return (lo >> sh) | (hi << (64 - sh));
+}
+
+// Bytes [depth, depth+8) of a string as a big-endian key; bytes at or past
+// the string's length are 0 (the NUL terminator and beyond), so unsigned key
+// order is the reference's byte-wise string order (scmp, stringtools.hpp:128).
+__device__ __forceinline__ uint64_t key8(const uint8_t* chars, uint64_t off, uint32_t len,
+                                         uint32_t depth) {
+    if (depth >= len) return 0;
+    uint64_t v = load_le8(chars + off + depth);
+    uint32_t rem = len - depth;
+    if (rem < 8) v &= (1ull << (rem * 8)) - 1;
+    return bswap64(v);
+}
+
+// Index (0..7) of the first zero byte of a big-endian key, or 8 if none.
+__device__ __forceinline__ uint32_t zero_byte(uint64_t k) {
+    const uint64_t m = 0x7F7F7F7F7F7F7F7Full;
+    // Exact per-byte zero test (no borrow between bytes): 0x80 in each zero byte.
+    uint64_t z = ~(((k & m) + m) | k | m);
+    return z ? (uint32_t)(__clzll(z) >> 3) : 8u;
+}
+
+// LCP in bytes of two keys that differ.
+__device__ __forceinline__ uint32_t key_lcp(uint64_t a, uint64_t b) {
+    return (uint32_t)(__clzll(a ^ b) >> 3);
+}
+
+// --------------------------------------------------------------- XXH64 ----
+// XXH64, seed 0, of m bytes at p: the published algorithm as the reference's
+// streaming port computes it (hash/xxhash.hpp:327-350, 516-660), including the
+// port's "total_len > 32" choice of the four-lane merge (xxhash.hpp:608).
+namespace xxh {
+constexpr uint64_t P1 = 11400714785074694791ULL, P2 = 14029467366897019727ULL,
+                   P3 = 1609587929392839161ULL, P4 = 9650029242287828579ULL,
+                   P5 = 2870177450012600261ULL;
+__device__ __forceinline__ uint64_t rotl(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+__device__ __forceinline__ uint64_t round(uint64_t acc, uint64_t in) {
+    acc += in * P2;
+    acc = rotl(acc, 31);
+    return acc * P1;
+}
+__device__ __forceinline__ uint64_t merge(uint64_t acc, uint64_t v) {
+    v = round(0, v);
+    acc ^= v;
+    return acc * P1 + P4;
+}
+}  // namespace xxh
+
+// Streams little-endian 8-byte words from an unaligned start with one aligned
+// 16-byte load per two words.
+struct WordStream {
+    const uint4* q;
+    unsigned sh;
+    uint64_t w0, w1, w2;  // w0 current aligned word, w1/w2 buffered
+    int buffered;         // words buffered after w0
+    __device__ __forceinline__ explicit WordStream(const uint8_t* p) {
+        uintptr_t a = (uintptr_t)p;
+        sh = (unsigned)(a & 7) * 8;
+        uintptr_t wa = a & ~(uintptr_t)7;           // first aligned word
+        q = (const uint4*)(wa & ~(uintptr_t)15);
+        uint4 v = __ldg(q++);
+        uint64_t lo = ((uint64_t)v.y << 32) | v.x, hi = ((uint64_t)v.w << 32) | v.z;
+        if (wa & 8) { w0 = hi; buffered = 0; }
+        else { w0 = lo; w1 = hi; buffered = 1; }
+    }
+    __device__ __forceinline__ uint64_t next_aligned() {
+        if (buffered == 0) {
+            uint4 v = __ldg(q++);
+            w1 = ((uint64_t)v.y << 32) | v.x;
+            w2 = ((uint64_t)v.w << 32) | v.z;
+            buffered = 2;
+        }
+        uint64_t r = w1;
+        w1 = w2;
+        --buffered;
+        return r;
+    }
+    __device__ __forceinline__ uint64_t next() {
+        uint64_t lo = w0;
+        uint64_t hi = next_aligned();
+        w0 = hi;
+        return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+    }
+};
+
+__device__ __forceinline__ uint64_t xxh64_dev(const uint8_t* p, uint32_t m) {
+    using namespace xxh;
+    WordStream ws(p);
+    uint64_t v1 = P1 + P2, v2 = P2, v3 = 0, v4 = 0 - P1;
+    uint32_t rem = m;
+    if (m >= 32) {
+        do {
+            v1 = round(v1, ws.next());
+            v2 = round(v2, ws.next());
+            v3 = round(v3, ws.next());
+            v4 = round(v4, ws.next());
+            rem -= 32;
+        } while (rem >= 32);
+    }
+    uint64_t h;
+    if (m > 32) {
+        h = rotl(v1, 1) + rotl(v2, 7) + rotl(v3, 12) + rotl(v4, 18);
+        h = merge(h, v1);
+        h = merge(h, v2);
+        h = merge(h, v3);
+        h = merge(h, v4);
+    } else {
+        h = v3 + P5;
+    }
+    h += m;
+    while (rem >= 8) {
+        h ^= round(0, ws.next());
+        h = rotl(h, 27) * P1 + P4;
+        rem -= 8;
+    }
+    if (rem) {
+        uint64_t w = ws.next();  // bytes past m are ignored
+        if (rem >= 4) {
+            h ^= (uint64_t)(uint32_t)w * P1;
+            h = rotl(h, 23) * P2 + P3;
+            w >>= 32;
+            rem -= 4;
+        }
+        while (rem) {
+            h ^= (w & 0xff) * P5;
+            h = rotl(h, 11) * P1;
+            w >>= 8;
+            --rem;
+        }
+    }
+    h ^= h >> 33;
+    h *= P2;
+    h ^= h >> 29;
+    h *= P3;
+    h ^= h >> 32;
+    return h;
+}
+
+// XXHasher::hash with bloomFilterSize = UINT64_MAX (bloomfilter.hpp:1094-1102, :1135).
+__device__ __forceinline__ uint64_t filter_hash(uint64_t h) { return h == ~0ull ? 0 : h; }
+
+// ------------------------------------------------------------ utilities ----
+// Exclusive scan of u32 values; writes the total to *total (device).
+// Scratch: scan_scratch_bytes(n).
+uint64_t scan_scratch_bytes(uint64_t n);
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total, void* scratch,
+                       cudaStream_t st);
+
+inline unsigned grid_for(uint64_t n, unsigned block) {
+    uint64_t g = (n + block - 1) / block;
+    return (unsigned)(g ? g : 1);
+}
+
+}  // namespace dsss
+
+struct dsss_ctx : dsss::Ctx {};

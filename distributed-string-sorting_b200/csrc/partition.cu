@@ -1,0 +1,174 @@
+// K5 — splitter sampling and partitioning: computePartition for the
+// distinguishing-prefix path (src/sorter/distributed/misc.hpp:531-587, indexed
+// variant :650-708).
+//   sample  : per PE, nr = min(factor*(p-1), n_q) strings at local index
+//             floor(i * (n_q / (nr+1))) in double arithmetic, each truncated to
+//             min(length, dp) (samplingStrategies.hpp:57-89, 148-184);
+//   sort    : the gathered sample with the string sort of strsort.cu, ties in
+//             input order, i.e. by (PE, index) — the order IndexStringComparator
+//             (misc.hpp:38-54) imposes and that RQuick's result has;
+//   choose  : nr' = min(p-1, total) splitters at every (total/(nr'+1))-th
+//             sorted sample (getSplitters, misc.hpp:89-135 / 137-189);
+//   search  : per (PE, splitter) the reference's binary search over the PE's
+//             sorted strings, which returns the first probe that compares
+//             equal (binarySearch misc.hpp:310-333, binarySearchIndexed :347-374).
+#include <algorithm>
+#include <vector>
+
+#include "internal.cuh"
+#include "partition.cuh"
+#include "strsort.cuh"
+
+namespace dsss {
+
+__global__ void k_sample_gather(ArenaDev a, const uint32_t* local_order, const uint32_t* dp,
+                                const uint64_t* sample_lp, uint64_t m, uint64_t* soff, uint32_t* slen) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint64_t lp = sample_lp[j];
+    const uint32_t s = local_order[lp];
+    soff[j] = a.off[s];
+    slen[j] = min(a.len[s], dp[lp]);
+}
+
+// Sign of the byte-wise comparison of two strings (scmp, stringtools.hpp:128-136).
+__device__ __forceinline__ int str_cmp(const uint8_t* chars, uint64_t oa, uint32_t la, uint64_t ob, uint32_t lb) {
+    for (uint32_t d = 0;; d += 8) {
+        uint64_t x = key8(chars, oa, la, d), y = key8(chars, ob, lb, d);
+        if (x != y) return x < y ? -1 : 1;
+        if (zero_byte(x) < 8) return 0;
+    }
+}
+
+__global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint64_t* pb, uint32_t p,
+                            uint32_t nspl, const uint64_t* spl_off, const uint32_t* spl_len,
+                            const uint64_t* spl_index, int indexed, uint64_t* pos) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)p * nspl) return;
+    const uint32_t q = (uint32_t)(t / nspl), k = (uint32_t)(t % nspl);
+    const uint64_t base = pb[q];
+    uint64_t left = 0, right = pb[q + 1] - base;
+    const uint64_t so = spl_off[k];
+    const uint32_t sl = spl_len[k];
+    while (left != right) {
+        const uint64_t d = (right - left) / 2;
+        const uint32_t s = local_order[base + left + d];
+        int res = str_cmp(a.chars, a.off[s], a.len[s], so, sl);
+        if (res == 0 && indexed) {
+            // indexStringCompare (misc.hpp:335-345): equal bytes compare by the
+            // global index, as int64 narrowed to int.
+            res = (int)(int32_t)(uint32_t)((left + d + base) - spl_index[k]);
+        }
+        if (res < 0) {
+            left = left + d + 1;
+        } else if (res == 0) {
+            pos[t] = left + d;
+            return;
+        } else {
+            right = left + d;
+        }
+    }
+    pos[t] = left;
+}
+
+uint64_t partition_scratch_bytes(uint64_t n, uint32_t p, uint32_t factor) {
+    Carve c(nullptr);
+    PartitionLayout L;
+    layout_partition(c, L, n, p, factor);
+    return c.used;
+}
+
+static uint64_t max_samples(uint64_t n, uint32_t p, uint32_t factor) {
+    return std::min<uint64_t>((uint64_t)factor * (p ? p - 1 : 0) * p, n) + 1;
+}
+
+void layout_partition(Carve& c, PartitionLayout& L, uint64_t n, uint32_t p, uint32_t factor) {
+    uint64_t S = max_samples(n, p, factor);
+    L.cap = S;
+    L.sample_lp = c.take<uint64_t>(S);
+    L.soff = c.take<uint64_t>(S);
+    L.slen = c.take<uint32_t>(S);
+    L.sorted = c.take<uint32_t>(S);
+    L.slcp = c.take<uint32_t>(S);
+    L.spl_off = c.take<uint64_t>(p);
+    L.spl_len = c.take<uint32_t>(p);
+    L.spl_index = c.take<uint64_t>(p);
+    L.pos = c.take<uint64_t>((uint64_t)p * p + 1);
+    L.pb = c.take<uint64_t>(p + 1);
+    layout_sort(c, L.sort, S, 1, 0);
+}
+
+int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_t p, const uint64_t* pb,
+                  const uint32_t* local_order, const uint32_t* dp, uint32_t sampler, uint32_t factor,
+                  uint64_t* intervals, cudaStream_t st) {
+    const bool indexed = sampler == DSSS_SAMPLER_INDEXED_NUM_STRINGS;
+    // sample positions (host, double arithmetic as getNumberSplitter/sample_splitters)
+    std::vector<uint64_t> lp, sindex;
+    for (uint32_t q = 0; q < p; ++q) {
+        const uint64_t nq = pb[q + 1] - pb[q];
+        const uint64_t nr = std::min<uint64_t>((uint64_t)factor * (p - 1), nq);
+        const double dist = (double)nq / (double)(nr + 1);
+        for (uint64_t i = 1; i <= nr; ++i) {
+            const uint64_t idx = (uint64_t)((double)i * dist);
+            lp.push_back(pb[q] + idx);
+            sindex.push_back(pb[q] + idx);
+        }
+    }
+    const uint64_t S = lp.size();
+    if (S > L.cap) return fail(DSSS_EINVAL, "partition: sample larger than planned");
+    const uint64_t nspl = std::min<uint64_t>(p - 1, S);
+    if (nspl == 0) {
+        for (uint32_t q = 0; q < p; ++q)
+            for (uint32_t r = 0; r < p; ++r) intervals[(uint64_t)q * p + r] = r == 0 ? pb[q + 1] - pb[q] : 0;
+        return DSSS_OK;
+    }
+    DSSS_TRY(ensure_pin(ctx, S * 16 + 64 + (uint64_t)p * p * 8));
+    uint64_t* hpin = (uint64_t*)ctx->pin;
+    std::copy(lp.begin(), lp.end(), hpin);
+    DSSS_CUDA(cudaMemcpyAsync(L.sample_lp, hpin, S * 8, cudaMemcpyHostToDevice, st));
+    k_sample_gather<<<grid_for(S, 256), 256, 0, st>>>(a, local_order, dp, L.sample_lp, S, L.soff, L.slen);
+    DSSS_CUDA(cudaGetLastError());
+    ArenaDev sa{a.chars, L.soff, L.slen, S};
+    uint64_t one[2] = {0, S};
+    // sort_strings synchronises on st before reading its counts back, so the
+    // sample positions copied above are consumed before hpin is reused.
+    DSSS_TRY(sort_strings(L.sort, sa, S, 1, one, nullptr, L.sorted, L.slcp, 0, (uint32_t*)hpin, st));
+    uint32_t* hsorted = (uint32_t*)hpin;
+    uint64_t* hoff = (uint64_t*)(hpin + (S + 1) / 2 + 1);
+    uint32_t* hlen = (uint32_t*)(hoff + S);
+    DSSS_CUDA(cudaMemcpyAsync(hsorted, L.sorted, S * 4, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaMemcpyAsync(hoff, L.soff, S * 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaMemcpyAsync(hlen, L.slen, S * 4, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    const uint64_t sd = S / (nspl + 1);
+    std::vector<uint64_t> so(nspl), si(nspl), pbv(pb, pb + p + 1);
+    std::vector<uint32_t> sl(nspl);
+    for (uint64_t k = 1; k <= nspl; ++k) {
+        const uint32_t sid = hsorted[k * sd];
+        so[k - 1] = hoff[sid];
+        sl[k - 1] = hlen[sid];
+        si[k - 1] = sindex[sid];
+    }
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_off, so.data(), nspl * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_len, sl.data(), nspl * 4, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_index, si.data(), nspl * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pbv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    k_binsearch<<<grid_for((uint64_t)p * nspl, 128), 128, 0, st>>>(a, local_order, L.pb, p, (uint32_t)nspl, L.spl_off,
+                                                                  L.spl_len, L.spl_index, indexed ? 1 : 0, L.pos);
+    DSSS_CUDA(cudaGetLastError());
+    std::vector<uint64_t> pos((uint64_t)p * nspl);
+    DSSS_CUDA(cudaMemcpyAsync(pos.data(), L.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    // compute_interval_binary (misc.hpp:376-395): differences of the positions
+    for (uint32_t q = 0; q < p; ++q) {
+        uint64_t prev = 0;
+        for (uint32_t r = 0; r < p; ++r) {
+            uint64_t cur = r < nspl ? pos[(uint64_t)q * nspl + r] : pb[q + 1] - pb[q];
+            intervals[(uint64_t)q * p + r] = cur - prev;
+            prev = cur;
+        }
+    }
+    return DSSS_OK;
+}
+
+}  // namespace dsss

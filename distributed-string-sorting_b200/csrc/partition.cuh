@@ -1,0 +1,31 @@
+// Splitter sampling and partitioning (K5); see partition.cu.
+#pragma once
+#include "internal.cuh"
+#include "strsort.cuh"
+
+namespace dsss {
+
+struct PartitionLayout {
+    uint64_t cap;
+    uint64_t* sample_lp;
+    uint64_t* soff;
+    uint32_t* slen;
+    uint32_t* sorted;
+    uint32_t* slcp;
+    uint64_t* spl_off;
+    uint32_t* spl_len;
+    uint64_t* spl_index;
+    uint64_t* pos;
+    uint64_t* pb;
+    SortLayout sort;
+};
+
+void layout_partition(Carve& c, PartitionLayout& L, uint64_t n, uint32_t p, uint32_t factor);
+
+// local_order: per PE the string ids in sorted order; dp: their distinguishing
+// prefixes (same positions).  intervals (host, p*p): strings PE q sends to PE r.
+int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_t p, const uint64_t* pb,
+                  const uint32_t* local_order, const uint32_t* dp, uint32_t sampler, uint32_t factor,
+                  uint64_t* intervals, cudaStream_t st);
+
+}  // namespace dsss

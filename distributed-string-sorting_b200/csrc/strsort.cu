@@ -1,0 +1,644 @@
+// K3 — segmented MSD string sort with LCP output, the role radixsort_CI3
+// plays per PE in the reference (tlx/sort/strings/radix_sort.hpp:861-884,
+// called at src/sorter/distributed/prefix_doubling.hpp:228).
+//
+// Elements are string ids; every segment is sorted independently (a PE's
+// strings, or the whole set).  Large segments (> small_max) are refined by
+// MSD passes over 8-byte big-endian key chunks:
+//   prefix   : common prefix of the segment (compare each string with the
+//              first one), so a segment's key starts at its first differing byte;
+//   keys/diff: gather the 8-byte key at that depth, OR of (key ^ key0) tells
+//              which key byte is the first to differ;
+//   hist     : warp-aggregated 256-bin histogram of that byte per 4096-element tile;
+//   scan     : per segment, bucket starts and per-tile offsets (chunked);
+//   scatter  : stable scatter of ids (and keys of children that stay large).
+// Children of size <= small_max finish in one CTA (small_sort): bitonic sort
+// of (group, key, id) in shared memory, tie groups re-keyed 8 bytes deeper
+// until every group is a single string or byte-identical strings.
+// LCPs are written where they become known: depth + first differing byte at
+// every bucket / group boundary, the length for byte-identical neighbours.
+// Ties between byte-identical strings keep ascending id order.
+#include <algorithm>
+
+#include "internal.cuh"
+#include "strsort.cuh"
+
+namespace dsss {
+
+constexpr int LT_NT = 256, LT_IPT = 16, LT_TILE = LT_NT * LT_IPT;
+constexpr int CHUNK_TILES = 32;
+constexpr uint32_t PREFIX_CAP = 256;
+constexpr uint32_t F_PARITY = 1u, F_KEYS = 2u;
+
+struct Seg {
+    uint32_t start, size, depth, flags;
+    uint32_t newdepth;
+    uint32_t first_digit;
+    unsigned long long diff;
+};
+
+constexpr int NBINS = 4;
+__host__ __device__ constexpr int bin_cap(int b) { return b == 0 ? 32 : b == 1 ? 256 : b == 2 ? 1024 : 4096; }
+__device__ __forceinline__ int bin_of(uint32_t size) {
+    return size <= 32 ? 0 : size <= 256 ? 1 : size <= 1024 ? 2 : 3;
+}
+
+// Counters block (device): [0] n_large_next, [1..4] n_small per bin,
+// [8] total tiles, [9] total chunks.
+struct SortState {
+    ArenaDev a;
+    uint32_t* ord[2];
+    unsigned long long* key[2];
+    uint32_t* ord_out;
+    uint32_t* lcp_out;
+    Seg* large[2];
+    Seg* small[NBINS];
+    uint32_t* tile0;
+    uint32_t* chunk0;
+    uint32_t* tmp_counts;
+    uint32_t* tile_hist;
+    uint32_t* chunk_pre;
+    uint32_t* bucket;  // 257 per large segment
+    uint32_t* counters;
+    uint32_t small_max;
+    uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
+};
+
+__device__ __forceinline__ uint32_t find_seg(const uint32_t* first, uint32_t nseg, uint32_t t) {
+    // last s with first[s] <= t
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (first[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void push_small(const SortState& S, uint32_t start, uint32_t size, uint32_t depth,
+                                           uint32_t parity) {
+    int b = bin_of(size);
+    uint32_t slot = atomicAdd(&S.counters[1 + b], 1u);
+    Seg s;
+    s.start = start;
+    s.size = size;
+    s.depth = depth;
+    s.flags = parity;
+    s.newdepth = 0xFFFFFFFFu;
+    s.first_digit = 0;
+    s.diff = 0;
+    S.small[b][slot] = s;
+}
+
+__device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_t start, uint32_t size,
+                                           uint32_t depth, uint32_t flags) {
+    uint32_t slot = atomicAdd(&S.counters[0], 1u);
+    Seg s;
+    s.start = start;
+    s.size = size;
+    s.depth = depth;
+    s.flags = flags;
+    s.newdepth = 0xFFFFFFFFu;
+    s.first_digit = 0;
+    s.diff = 0;
+    dst[slot] = s;
+}
+
+// ------------------------------------------------------------------ init ----
+__global__ void k_init_ids(uint32_t* ord, const uint32_t* in, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ord[i] = in ? in[i] : (uint32_t)i;
+}
+
+__global__ void k_init_segs(SortState S, const uint64_t* pb, uint32_t p) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p) return;
+    uint32_t start = (uint32_t)pb[q], size = (uint32_t)(pb[q + 1] - pb[q]);
+    if (size == 0) return;
+    S.lcp_out[start] = 0;
+    if (size == 1) {
+        S.ord_out[start] = S.ord[0][start];
+        return;
+    }
+    if (size > S.small_max) push_large(S, S.large[0], start, size, 0, 0);
+    else push_small(S, start, size, 0, 0);
+}
+
+// --------------------------------------------------------- tile indexing ----
+__global__ void k_tile_counts(const Seg* segs, uint32_t nseg, uint32_t* tiles, uint32_t* chunks) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    uint32_t t = (segs[s].size + LT_TILE - 1) / LT_TILE;
+    tiles[s] = t;
+    chunks[s] = (t + CHUNK_TILES - 1) / CHUNK_TILES;
+}
+
+// ---------------------------------------------------------------- prefix ----
+__global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32_t nseg) {
+    const uint32_t t = blockIdx.x;
+    if (t >= S.counters[8]) return;
+    const uint32_t si = find_seg(S.tile0, nseg, t);
+    Seg& sg = segs[si];
+    if (sg.flags & F_KEYS) return;
+    const uint32_t par = sg.flags & F_PARITY;
+    const uint32_t* ord = S.ord[par];
+    const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
+    const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    const uint32_t d0 = sg.depth, cap = d0 + PREFIX_CAP;
+    const uint32_t s0 = ord[sg.start];
+    const uint64_t off0 = S.a.off[s0];
+    const uint32_t len0 = S.a.len[s0];
+    uint32_t mn = 0xFFFFFFFFu;
+    for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
+        uint32_t s = ord[i];
+        uint64_t off = S.a.off[s];
+        uint32_t len = S.a.len[s];
+        uint32_t d = d0, l;
+        for (;;) {
+            uint64_t x = key8(S.a.chars, off, len, d), y = key8(S.a.chars, off0, len0, d);
+            if (x != y) { l = d + key_lcp(x, y); break; }
+            uint32_t z = zero_byte(x);
+            if (z < 8) { l = d + z; break; }
+            d += 8;
+            if (d >= cap) { l = cap; break; }
+        }
+        mn = min(mn, l);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    if ((threadIdx.x & 31) == 0 && mn != 0xFFFFFFFFu) atomicMin(&sg.newdepth, mn);
+}
+
+// ------------------------------------------------------------- keys/diff ----
+__global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uint32_t nseg) {
+    const uint32_t t = blockIdx.x;
+    if (t >= S.counters[8]) return;
+    const uint32_t si = find_seg(S.tile0, nseg, t);
+    Seg& sg = segs[si];
+    const uint32_t par = sg.flags & F_PARITY;
+    const bool valid = sg.flags & F_KEYS;
+    const uint32_t depth = valid ? sg.depth : sg.newdepth;
+    const uint32_t* ord = S.ord[par];
+    unsigned long long* key = S.key[par];
+    const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
+    const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    uint64_t k0;
+    if (valid) {
+        k0 = key[sg.start];
+    } else {
+        uint32_t s0 = ord[sg.start];
+        k0 = key8(S.a.chars, S.a.off[s0], S.a.len[s0], depth);
+    }
+    uint64_t df = 0;
+    for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
+        uint64_t k;
+        if (valid) {
+            k = key[i];
+        } else {
+            uint32_t s = ord[i];
+            k = key8(S.a.chars, S.a.off[s], S.a.len[s], depth);
+            key[i] = k;
+        }
+        df |= k ^ k0;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(0xffffffffu, df, o);
+    if ((threadIdx.x & 31) == 0 && df) atomicOr(&sg.diff, (unsigned long long)df);
+}
+
+// ------------------------------------------------------------------ hist ----
+__device__ __forceinline__ uint32_t digit_of(uint64_t k, uint32_t shift) { return (uint32_t)(k >> shift) & 0xFFu; }
+
+__global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, uint32_t nseg) {
+    __shared__ uint32_t hist[256];
+    const uint32_t t = blockIdx.x;
+    if (t >= S.counters[8]) return;
+    const uint32_t si = find_seg(S.tile0, nseg, t);
+    const Seg sg = segs[si];
+    if (sg.diff == 0) return;
+    const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
+    const unsigned long long* key = S.key[sg.flags & F_PARITY];
+    hist[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
+    const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = tb + (threadIdx.x & ~31u); base < te; base += LT_NT) {
+        uint32_t i = base + lane;
+        uint32_t d = i < te ? digit_of(key[i], shift) : 0x100u + lane;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    S.tile_hist[(uint64_t)t * 256 + threadIdx.x] = hist[threadIdx.x];
+}
+
+// ------------------------------------------------------------ chunk sums ----
+__global__ void k_chunk_sum(SortState S, const Seg* segs, uint32_t nseg) {
+    const uint32_t c = blockIdx.x;
+    if (c >= S.counters[9]) return;
+    const uint32_t si = find_seg(S.chunk0, nseg, c);
+    const Seg sg = segs[si];
+    if (sg.diff == 0) return;
+    const uint32_t ntiles = (sg.size + LT_TILE - 1) / LT_TILE;
+    const uint32_t t0 = S.tile0[si] + (c - S.chunk0[si]) * CHUNK_TILES;
+    const uint32_t t1 = min(S.tile0[si] + ntiles, t0 + CHUNK_TILES);
+    uint32_t s = 0;
+    for (uint32_t t = t0; t < t1; ++t) s += S.tile_hist[(uint64_t)t * 256 + threadIdx.x];
+    S.chunk_pre[(uint64_t)c * 256 + threadIdx.x] = s;
+}
+
+// ----------------------------------------------------------- segment scan ----
+__global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32_t nseg, Seg* next) {
+    __shared__ uint32_t sh[32];
+    __shared__ uint32_t s_first;
+    const uint32_t si = blockIdx.x;
+    Seg& sg = segs[si];
+    const uint32_t par = sg.flags & F_PARITY;
+    const uint32_t depth = (sg.flags & F_KEYS) ? sg.depth : sg.newdepth;
+    const uint32_t d = threadIdx.x;
+    if (sg.diff == 0) {
+        // Every key equal: byte-identical strings if the key holds the end,
+        // else look 8 bytes deeper.
+        const uint64_t k0 = S.key[par][sg.start];
+        const uint32_t z = zero_byte(k0);
+        if (z < 8) {
+            const uint32_t* ord = S.ord[par];
+            for (uint32_t i = threadIdx.x; i < sg.size; i += blockDim.x) {
+                S.ord_out[sg.start + i] = ord[sg.start + i];
+                if (i) S.lcp_out[sg.start + i] = depth + z;
+            }
+        } else if (threadIdx.x == 0) {
+            push_large(S, next, sg.start, sg.size, depth + 8, par);
+        }
+        return;
+    }
+    const uint32_t b = (uint32_t)(__clzll(sg.diff) >> 3);
+    const uint32_t c0 = S.chunk0[si];
+    const uint32_t ntiles = (sg.size + LT_TILE - 1) / LT_TILE;
+    const uint32_t nch = (ntiles + CHUNK_TILES - 1) / CHUNK_TILES;
+    uint32_t run = 0;
+    for (uint32_t c = 0; c < nch; ++c) {
+        uint64_t idx = (uint64_t)(c0 + c) * 256 + d;
+        uint32_t v = S.chunk_pre[idx];
+        S.chunk_pre[idx] = run;
+        run += v;
+    }
+    const uint32_t total = run;
+    // block exclusive scan over the 256 digits
+    const int lane = d & 31, w = d >> 5;
+    uint32_t x = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    if (d == 0) s_first = 256;
+    __syncthreads();
+    uint32_t wb = 0;
+    for (int k = 0; k < w; ++k) wb += sh[k];
+    const uint32_t excl = wb + x - total;
+    if (total) atomicMin(&s_first, d);
+    uint32_t* bk = S.bucket + (uint64_t)si * 257;
+    bk[d] = sg.start + excl;
+    if (d == 255) bk[256] = sg.start + sg.size;
+    __syncthreads();
+    if (d == 0) {
+        sg.first_digit = s_first;
+        sg.depth = depth;
+    }
+    if (total >= 2 && d != 0) {
+        const uint32_t cs = sg.start + excl;
+        if (total > S.small_max) push_large(S, next, cs, total, depth, (par ^ 1u) | F_KEYS);
+        else push_small(S, cs, total, depth + b + 1, par ^ 1u);
+    }
+}
+
+// --------------------------------------------------------------- scatter ----
+__global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs, uint32_t nseg) {
+    __shared__ uint32_t base[256];
+    __shared__ uint32_t bstart[257];
+    __shared__ uint32_t wcnt[LT_NT / 32][256];
+    const uint32_t t = blockIdx.x;
+    if (t >= S.counters[8]) return;
+    const uint32_t si = find_seg(S.tile0, nseg, t);
+    const Seg sg = segs[si];
+    if (sg.diff == 0) return;
+    const uint32_t par = sg.flags & F_PARITY;
+    const uint32_t b = (uint32_t)(__clzll(sg.diff) >> 3);
+    const uint32_t shift = 56 - 8 * b;
+    const uint32_t depth = sg.depth;
+    const uint32_t tloc = t - S.tile0[si];
+    const uint32_t c = S.chunk0[si] + tloc / CHUNK_TILES;
+    const uint32_t tfirst = t - tloc % CHUNK_TILES;
+    {
+        const uint32_t d = threadIdx.x;
+        const uint32_t* bk = S.bucket + (uint64_t)si * 257;
+        uint32_t o = bk[d] + S.chunk_pre[(uint64_t)c * 256 + d];
+        for (uint32_t u = tfirst; u < t; ++u) o += S.tile_hist[(uint64_t)u * 256 + d];
+        base[d] = o;
+        bstart[d] = bk[d];
+        if (d == 0) bstart[256] = bk[256];
+#pragma unroll
+        for (int w = 0; w < LT_NT / 32; ++w) wcnt[w][d] = 0;
+    }
+    __syncthreads();
+    const uint32_t* ord = S.ord[par];
+    const unsigned long long* key = S.key[par];
+    uint32_t* ord_dst = S.ord[par ^ 1u];
+    unsigned long long* key_dst = S.key[par ^ 1u];
+    const uint32_t tb = sg.start + tloc * LT_TILE;
+    const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t wb = tb + (uint32_t)w * 32 * LT_IPT;
+    uint64_t k[LT_IPT];
+    uint32_t rk[LT_IPT];
+#pragma unroll
+    for (int j = 0; j < LT_IPT; ++j) {
+        uint32_t i = wb + j * 32 + lane;
+        k[j] = i < te ? key[i] : 0;
+        uint32_t dg = i < te ? digit_of(k[j], shift) : 0x100u + lane;
+        uint32_t peers = __match_any_sync(0xffffffffu, dg);
+        uint32_t r = __popc(peers & ((1u << lane) - 1));
+        uint32_t prev = dg < 256 ? wcnt[w][dg] : 0;
+        __syncwarp();
+        if (dg < 256 && lane == __ffs(peers) - 1) wcnt[w][dg] = prev + __popc(peers);
+        __syncwarp();
+        rk[j] = prev + r;
+    }
+    __syncthreads();
+    {
+        const uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int ww = 0; ww < LT_NT / 32; ++ww) {
+            uint32_t v = wcnt[ww][d];
+            wcnt[ww][d] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < LT_IPT; ++j) {
+        uint32_t i = wb + j * 32 + lane;
+        if (i >= te) continue;
+        uint32_t dg = digit_of(k[j], shift);
+        uint32_t dest = base[dg] + wcnt[w][dg] + rk[j];
+        uint32_t o = ord[i];
+        uint32_t bs = bstart[dg], cnt = bstart[dg + 1] - bs;
+        if (dg == 0 || cnt == 1) {
+            S.ord_out[dest] = o;
+            if (dg == 0 && dest != bs) S.lcp_out[dest] = depth + b;
+        } else {
+            ord_dst[dest] = o;
+            if (cnt > S.small_max) key_dst[dest] = k[j];
+        }
+        if (dest == bs && dg != sg.first_digit) S.lcp_out[dest] = depth + b;
+    }
+}
+
+// ------------------------------------------------------------ small sort ----
+template <int CAP, int NT>
+__global__ void __launch_bounds__(NT) k_small_sort(SortState S, const Seg* segs, uint32_t nseg) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* sk = (unsigned long long*)smem;
+    uint32_t* so = (uint32_t*)(sk + CAP);
+    uint32_t* sg = so + CAP;
+    uint32_t* sd = sg + CAP;
+    uint32_t* rs = sd + CAP;
+    __shared__ uint32_t shm[32];
+    __shared__ int s_unres;
+    constexpr int IPT = CAP / NT;
+    const uint32_t bi = blockIdx.x;
+    if (bi >= nseg) return;
+    const Seg seg = segs[bi];
+    const uint32_t start = seg.start, size = seg.size;
+    const uint32_t* src = S.ord[seg.flags & F_PARITY];
+    for (uint32_t i = threadIdx.x; i < CAP; i += NT) {
+        if (i < size) {
+            uint32_t o = src[start + i];
+            so[i] = o;
+            sd[i] = seg.depth;
+            sg[i] = 0;
+            sk[i] = key8(S.a.chars, S.a.off[o], S.a.len[o], seg.depth);
+        } else {
+            so[i] = 0xFFFFFFFFu;
+            sg[i] = 0xFFFFFFFFu;
+            sk[i] = ~0ull;
+            sd[i] = 0;
+        }
+    }
+    __syncthreads();
+    for (;;) {
+        // bitonic sort by (group, key, id)
+        for (uint32_t kk = 2; kk <= (uint32_t)CAP; kk <<= 1) {
+            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < (uint32_t)CAP / 2; i += NT) {
+                    uint32_t a = 2 * j * (i / j) + (i % j), bb = a + j;
+                    bool asc = (a & kk) == 0;
+                    uint32_t ga = sg[a], gb = sg[bb];
+                    uint64_t ka = sk[a], kb = sk[bb];
+                    uint32_t oa = so[a], ob = so[bb];
+                    bool bless = gb < ga || (gb == ga && (kb < ka || (kb == ka && ob < oa)));
+                    if (bless == asc) {
+                        sg[a] = gb; sg[bb] = ga;
+                        sk[a] = kb; sk[bb] = ka;
+                        so[a] = ob; so[bb] = oa;
+                        uint32_t t2 = sd[a]; sd[a] = sd[bb]; sd[bb] = t2;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // run heads: a new (group, key) starts; boundaries inside a group get their LCP.
+        uint32_t carry = 0;  // 1 + last head index in this thread's range, 0 = none
+        const uint32_t ib = threadIdx.x * IPT;
+#pragma unroll 1
+        for (int j = 0; j < IPT; ++j) {
+            uint32_t i = ib + j;
+            if (i >= size) break;
+            bool head = i == 0 || sg[i] != sg[i - 1];
+            if (!head) {
+                if (sk[i] != sk[i - 1]) {
+                    head = true;
+                    S.lcp_out[start + i] = sd[i] + key_lcp(sk[i], sk[i - 1]);
+                } else {
+                    uint32_t z = zero_byte(sk[i]);
+                    if (z < 8) S.lcp_out[start + i] = sd[i] + z;  // byte-identical neighbours
+                }
+            }
+            if (head) carry = i + 1;
+        }
+        // exclusive max-scan of carries across threads
+        {
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            uint32_t x = carry;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x = max(x, y);
+            }
+            if (lane == 31) shm[w] = x;
+            if (threadIdx.x == 0) s_unres = 0;
+            __syncthreads();
+            uint32_t inc = 0;
+            for (int k2 = 0; k2 < w; ++k2) inc = max(inc, shm[k2]);
+            uint32_t prev_lane = __shfl_up_sync(0xffffffffu, x, 1);
+            if (lane > 0) inc = max(inc, prev_lane);
+            carry = inc;  // 1 + last head before this thread's range
+        }
+        for (int j = 0; j < IPT; ++j) {
+            uint32_t i = ib + j;
+            if (i >= size) break;
+            bool head = i == 0 || sg[i] != sg[i - 1] || sk[i] != sk[i - 1];
+            if (head) carry = i + 1;
+            rs[i] = carry - 1;
+        }
+        __syncthreads();
+        int unres = 0;
+        for (int j = 0; j < IPT; ++j) {
+            uint32_t i = ib + j;
+            if (i >= size) break;
+            uint32_t r = rs[i];
+            bool multi = (i > 0 && rs[i - 1] == r) || (i + 1 < size && rs[i + 1] == r);
+            if (multi && zero_byte(sk[i]) == 8) {
+                unres = 1;
+                sd[i] += 8;
+                uint32_t o = so[i];
+                sk[i] = key8(S.a.chars, S.a.off[o], S.a.len[o], sd[i]);
+            }
+        }
+        __syncthreads();
+        for (int j = 0; j < IPT; ++j) {
+            uint32_t i = ib + j;
+            if (i >= size) break;
+            sg[i] = rs[i];
+        }
+        if (unres) s_unres = 1;
+        __syncthreads();
+        if (!s_unres) break;
+    }
+    for (uint32_t i = threadIdx.x; i < size; i += NT) S.ord_out[start + i] = so[i];
+}
+
+template <int CAP, int NT>
+static int launch_small(const SortState& S, const Seg* segs, uint32_t n, cudaStream_t st) {
+    if (!n) return DSSS_OK;
+    constexpr size_t shm = (size_t)CAP * (8 + 4 * 4);
+    static bool configured = false;
+    if (!configured) {
+        DSSS_CUDA(cudaFuncSetAttribute(k_small_sort<CAP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        configured = true;
+    }
+    k_small_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n);
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+// ------------------------------------------------------------------ host ----
+static uint32_t clamp_small_max(uint32_t m) {
+    return (m == 0 || m > (uint32_t)bin_cap(NBINS - 1)) ? (uint32_t)bin_cap(NBINS - 1) : (m < 2 ? 2 : m);
+}
+
+void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small_max) {
+    small_max = clamp_small_max(small_max);
+    uint64_t N = n ? n : 1;
+    L.ord[0] = c.take<uint32_t>(N);
+    L.ord[1] = c.take<uint32_t>(N);
+    L.key[0] = c.take<unsigned long long>(N);
+    L.key[1] = c.take<unsigned long long>(N);
+    L.cap_large = N / (small_max + 1) + p + 1;
+    L.cap_small = N / 2 + p + 1;
+    L.cap_tiles = N / LT_TILE + L.cap_large + 1;
+    L.cap_chunks = L.cap_tiles / CHUNK_TILES + L.cap_large + 1;
+    L.large[0] = c.take<unsigned char>(L.cap_large * sizeof(Seg));
+    L.large[1] = c.take<unsigned char>(L.cap_large * sizeof(Seg));
+    for (int b = 0; b < NBINS; ++b) L.small[b] = c.take<unsigned char>(L.cap_small * sizeof(Seg));
+    L.tile0 = c.take<uint32_t>(L.cap_large);
+    L.chunk0 = c.take<uint32_t>(L.cap_large);
+    L.tmp_counts = c.take<uint32_t>(2 * L.cap_large);
+    L.tile_hist = c.take<uint32_t>(L.cap_tiles * 256);
+    L.chunk_pre = c.take<uint32_t>(L.cap_chunks * 256);
+    L.bucket = c.take<uint32_t>(L.cap_large * 257);
+    L.counters = c.take<uint32_t>(16);
+    L.pb = c.take<uint64_t>(p + 1);
+    L.scan = c.take<unsigned char>(scan_scratch_bytes(L.cap_large));
+    L.pin = nullptr;
+}
+
+int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p, const uint64_t* pb_host,
+                 const uint32_t* ids_in, uint32_t* ord_out, uint32_t* lcp_out, uint32_t small_max,
+                 uint32_t* pin, cudaStream_t st) {
+    if (n == 0) return DSSS_OK;
+    SortState S;
+    S.a = a;
+    S.ord[0] = L.ord[0];
+    S.ord[1] = L.ord[1];
+    S.key[0] = L.key[0];
+    S.key[1] = L.key[1];
+    S.ord_out = ord_out;
+    S.lcp_out = lcp_out;
+    Seg* large[2] = {(Seg*)L.large[0], (Seg*)L.large[1]};
+    for (int b = 0; b < NBINS; ++b) S.small[b] = (Seg*)L.small[b];
+    S.tile0 = L.tile0;
+    S.chunk0 = L.chunk0;
+    S.tmp_counts = L.tmp_counts;
+    S.tile_hist = L.tile_hist;
+    S.chunk_pre = L.chunk_pre;
+    S.bucket = L.bucket;
+    S.counters = L.counters;
+    S.small_max = clamp_small_max(small_max);
+    S.cap_large = L.cap_large;
+    S.cap_small = L.cap_small;
+    S.cap_tiles = L.cap_tiles;
+    S.cap_chunks = L.cap_chunks;
+
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb_host, (p + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
+    k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n);
+    S.large[0] = large[0];
+    S.large[1] = large[1];
+    k_init_segs<<<grid_for(p, 128), 128, 0, st>>>(S, L.pb, p);
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    uint32_t nlarge = pin[0];
+    int cur = 0;
+    uint32_t guard = 0;
+    while (nlarge) {
+        if (++guard > (1u << 24)) return fail(DSSS_EDEVICE, "string sort made no progress");
+        Seg* segs = large[cur];
+        Seg* next = large[cur ^ 1];
+        // tile / chunk indexing
+        k_tile_counts<<<grid_for(nlarge, 256), 256, 0, st>>>(segs, nlarge, S.tmp_counts, S.tmp_counts + L.cap_large);
+        DSSS_TRY(exclusive_scan_u32(S.tmp_counts, S.tile0, nlarge, S.counters + 8, L.scan, st));
+        DSSS_TRY(exclusive_scan_u32(S.tmp_counts + L.cap_large, S.chunk0, nlarge, S.counters + 9, L.scan, st));
+        DSSS_CUDA(cudaMemsetAsync(S.counters, 0, sizeof(uint32_t), st));  // n_large_next
+        // upper bounds for the grids (kernels exit past the real counts)
+        uint64_t max_tiles = std::min<uint64_t>(L.cap_tiles, n / LT_TILE + nlarge + 1);
+        uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
+        S.large[0] = segs;
+        k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
+        k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
+        k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
+        k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge);
+        k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next);
+        k_scatter<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
+        DSSS_CUDA(cudaGetLastError());
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        nlarge = pin[0];
+        if (nlarge > L.cap_large) return fail(DSSS_EDEVICE, "string sort: large-segment list overflow");
+        cur ^= 1;
+    }
+    for (int b = 0; b < NBINS; ++b)
+        if (pin[1 + b] > L.cap_small) return fail(DSSS_EDEVICE, "string sort: small-segment list overflow");
+    DSSS_TRY((launch_small<32, 32>(S, S.small[0], pin[1], st)));
+    DSSS_TRY((launch_small<256, 128>(S, S.small[1], pin[2], st)));
+    DSSS_TRY((launch_small<1024, 256>(S, S.small[2], pin[3], st)));
+    DSSS_TRY((launch_small<4096, 512>(S, S.small[3], pin[4], st)));
+    return DSSS_OK;
+}
+
+}  // namespace dsss

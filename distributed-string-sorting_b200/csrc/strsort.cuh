@@ -1,0 +1,38 @@
+// Segmented MSD string sort with LCP output (K3); see strsort.cu.
+#pragma once
+#include "internal.cuh"
+
+namespace dsss {
+
+struct SortLayout {
+    uint32_t* ord[2];
+    unsigned long long* key[2];
+    unsigned char* large[2];
+    unsigned char* small[4];
+    uint32_t* tile0;
+    uint32_t* chunk0;
+    uint32_t* tmp_counts;
+    uint32_t* tile_hist;
+    uint32_t* chunk_pre;
+    uint32_t* bucket;
+    uint32_t* counters;
+    uint64_t* pb;
+    unsigned char* scan;
+    uint32_t* pin;
+    uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
+};
+
+constexpr uint32_t SORT_SMALL_MAX_DEFAULT = 4096;
+
+// Scratch layout for sorting up to n strings in up to p segments.
+void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small_max);
+
+// Sorts ids (ids_in[i], or i when ids_in is NULL) within the segments
+// [pb[q], pb[q+1]) by the bytes of their strings.  ord_out gets the sorted ids,
+// lcp_out[i] the LCP with position i-1 (0 at segment starts).  pin: pinned
+// host buffer of >= 16 u32 for count read-backs (the call synchronises on st).
+int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p, const uint64_t* pb_host,
+                 const uint32_t* ids_in, uint32_t* ord_out, uint32_t* lcp_out, uint32_t small_max,
+                 uint32_t* pin, cudaStream_t st);
+
+}  // namespace dsss

@@ -1,0 +1,174 @@
+// K4 adjacent LCP and the stable multisplit used for PE / bucket projections.
+#include <algorithm>
+
+#include "internal.cuh"
+#include "util.cuh"
+
+namespace dsss {
+
+// ---------------------------------------------------------- adjacent LCP ----
+// calc_lcp of sorted neighbours (strings/stringtools.hpp:158-166).  One thread
+// per pair compares 8-byte big-endian chunks; pairs still equal after
+// WARP_AFTER bytes are finished by a whole warp, 32 chunks (256 bytes) per
+// step with a ballot over the lanes.
+constexpr uint32_t WARP_AFTER = 64;
+
+__device__ __forceinline__ uint32_t lcp_thread(const ArenaDev& a, uint32_t s, uint32_t t, uint32_t from,
+                                               uint32_t limit, bool* done) {
+    const uint64_t os = a.off[s], ot = a.off[t];
+    const uint32_t ls = a.len[s], lt = a.len[t];
+    for (uint32_t d = from;; d += 8) {
+        if (d >= limit) { *done = false; return d; }
+        uint64_t x = key8(a.chars, os, ls, d), y = key8(a.chars, ot, lt, d);
+        if (x != y) { *done = true; return d + key_lcp(x, y); }
+        uint32_t z = zero_byte(x);
+        if (z < 8) { *done = true; return d + z; }
+    }
+}
+
+__global__ void k_adjacent_lcp(ArenaDev a, const uint32_t* order, uint64_t m, uint32_t* lcp, uint32_t* longq,
+                               uint32_t* nlong) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    if (i == 0) { lcp[0] = 0; return; }
+    bool done;
+    uint32_t l = lcp_thread(a, order[i - 1], order[i], 0, WARP_AFTER, &done);
+    if (done) lcp[i] = l;
+    else longq[atomicAdd(nlong, 1u)] = (uint32_t)i;
+}
+
+__global__ void k_adjacent_lcp_warp(ArenaDev a, const uint32_t* order, const uint32_t* longq,
+                                    const uint32_t* nlong, uint32_t* lcp) {
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = *nlong;
+    for (uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wid < total; wid += nw) {
+        const uint32_t i = longq[wid];
+        const uint32_t s = order[i - 1], t = order[i];
+        const uint64_t os = a.off[s], ot = a.off[t];
+        const uint32_t ls = a.len[s], lt = a.len[t];
+        for (uint32_t d = WARP_AFTER;; d += 256) {
+            uint32_t dd = d + 8 * lane;
+            uint64_t x = key8(a.chars, os, ls, dd), y = key8(a.chars, ot, lt, dd);
+            uint32_t stop = x != y ? 1u : (zero_byte(x) < 8 ? 1u : 0u);
+            uint32_t bal = __ballot_sync(0xffffffffu, stop);
+            if (bal) {
+                int first = __ffs(bal) - 1;
+                if (lane == first) lcp[i] = dd + (x != y ? key_lcp(x, y) : zero_byte(x));
+                break;
+            }
+        }
+    }
+}
+
+int adjacent_lcp(const ArenaDev& a, const uint32_t* order, uint64_t m, uint32_t* lcp, uint32_t* longq,
+                 uint32_t* nlong, cudaStream_t st) {
+    if (m == 0) return DSSS_OK;
+    DSSS_CUDA(cudaMemsetAsync(nlong, 0, sizeof(uint32_t), st));
+    k_adjacent_lcp<<<grid_for(m, 256), 256, 0, st>>>(a, order, m, lcp, longq, nlong);
+    k_adjacent_lcp_warp<<<(unsigned)std::min<uint64_t>(grid_for(m * 32, 256), 148 * 16), 256, 0, st>>>(a, order, longq,
+                                                                                                  nlong, lcp);
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+// ------------------------------------------------------------ multisplit ----
+// Stable partition of n elements by bucket id b(i) < P: dest[i] = (elements of
+// buckets < b) + (elements of bucket b before i).  Histograms are stored
+// bucket-major per tile, so one flat exclusive scan yields every tile's
+// starting offset per bucket.
+constexpr int MS_NT = 256, MS_IPT = 16, MS_TILE = MS_NT * MS_IPT;
+
+__global__ void __launch_bounds__(MS_NT) k_ms_hist(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles,
+                                                  uint32_t* hist) {
+    extern __shared__ uint32_t h[];
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) h[b] = 0;
+    __syncthreads();
+    const uint64_t tb = (uint64_t)blockIdx.x * MS_TILE;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = tb + (threadIdx.x & ~31u); base < tb + MS_TILE; base += MS_NT) {
+        uint64_t i = base + lane;
+        uint32_t d = i < n ? bucket[i] : 0xFFFFFFFFu - lane;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (i < n && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) hist[(uint64_t)b * tiles + blockIdx.x] = h[b];
+}
+
+__global__ void __launch_bounds__(MS_NT) k_ms_scatter(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles,
+                                                     const uint32_t* off, uint32_t* dest) {
+    extern __shared__ uint32_t sm[];
+    uint32_t* base = sm;           // P
+    uint32_t* wcnt = sm + P;       // (MS_NT/32) x P
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) {
+        base[b] = off[(uint64_t)b * tiles + blockIdx.x];
+        for (int w = 0; w < MS_NT / 32; ++w) wcnt[w * P + b] = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t wb = (uint64_t)blockIdx.x * MS_TILE + (uint64_t)w * 32 * MS_IPT;
+    uint32_t rk[MS_IPT];
+    uint32_t bk[MS_IPT];
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        uint64_t i = wb + j * 32 + lane;
+        uint32_t d = i < n ? bucket[i] : 0xFFFFFFFFu - lane;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t r = __popc(peers & ((1u << lane) - 1));
+        uint32_t prev = i < n ? wcnt[w * P + d] : 0;
+        __syncwarp();
+        if (i < n && lane == __ffs(peers) - 1) wcnt[w * P + d] = prev + __popc(peers);
+        __syncwarp();
+        rk[j] = prev + r;
+        bk[j] = d;
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) {
+        uint32_t run = 0;
+        for (int ww = 0; ww < MS_NT / 32; ++ww) {
+            uint32_t v = wcnt[ww * P + b];
+            wcnt[ww * P + b] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        uint64_t i = wb + j * 32 + lane;
+        if (i < n) dest[i] = base[bk[j]] + wcnt[w * P + bk[j]] + rk[j];
+    }
+}
+
+uint64_t multisplit_scratch_bytes(uint64_t n, uint32_t P) {
+    uint64_t tiles = (n + MS_TILE - 1) / MS_TILE;
+    if (!tiles) tiles = 1;
+    uint64_t cells = tiles * P;
+    return 2 * ((cells * 4 + 255) & ~255ull) + ((scan_scratch_bytes(cells) + 255) & ~255ull) + 256;
+}
+
+int multisplit(const uint32_t* bucket, uint64_t n, uint32_t P, uint32_t* dest, void* scratch, cudaStream_t st) {
+    if (n == 0) return DSSS_OK;
+    if (P == 0 || P > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "multisplit supports 1..%u buckets", MAX_SPLIT_BUCKETS);
+    uint64_t tiles = (n + MS_TILE - 1) / MS_TILE;
+    uint64_t cells = tiles * P;
+    if (cells >= (1ull << 32)) return fail(DSSS_ENOTSUP, "multisplit: too many tiles x buckets");
+    Carve c(scratch);
+    uint32_t* hist = c.take<uint32_t>(cells);
+    uint32_t* off = c.take<uint32_t>(cells);
+    void* sc = c.take<unsigned char>(scan_scratch_bytes(cells));
+    size_t sh1 = P * sizeof(uint32_t), sh2 = (size_t)P * (1 + MS_NT / 32) * sizeof(uint32_t);
+    static bool configured = false;
+    if (!configured) {
+        DSSS_CUDA(cudaFuncSetAttribute(k_ms_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(MAX_SPLIT_BUCKETS * (1 + MS_NT / 32) * sizeof(uint32_t))));
+        configured = true;
+    }
+    k_ms_hist<<<(unsigned)tiles, MS_NT, sh1, st>>>(bucket, n, P, tiles, hist);
+    DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
+    k_ms_scatter<<<(unsigned)tiles, MS_NT, sh2, st>>>(bucket, n, P, tiles, off, dest);
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+}  // namespace dsss

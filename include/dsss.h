@@ -1,0 +1,188 @@
+/*
+ * dsss.h — C ABI of the B200 prefix-doubling string sorter.
+ *
+ * The reference (bingmann/distributed-string-sorting) exposes its hot path as
+ * compile-time C++ policies; each entry point below replaces one of those
+ * seams and cites the reference interface it stands in for.  One GPU holds
+ * all p "PEs" (processing elements, the reference's MPI ranks) as contiguous
+ * partitions of one string arena; the reference's all-to-all exchanges become
+ * on-device scatters.
+ *
+ * Conventions
+ *  - Strings live in an arena: bytes `chars`, per-string `offsets` (u64) and
+ *    `lengths` (u32).  A string is chars[offsets[i] .. offsets[i]+lengths[i]);
+ *    it must not contain byte 0 (the reference's strings are NUL-terminated,
+ *    stringset.hpp:674-840).  Strings may overlap (suffix arrays).  Device
+ *    arenas must be 8-byte aligned and readable 32 bytes past the last string
+ *    byte (kernels use aligned vector loads); the *_host entry points pad for
+ *    the caller.
+ *  - PEs are contiguous index ranges: PE q owns strings [part_begin[q],
+ *    part_begin[q+1]) (host array of p+1 entries, part_begin[0] = 0,
+ *    part_begin[p] = n), like the reference's per-rank input slices.
+ *  - n < 2^32 strings per call.  Index outputs are u32.
+ *  - Return value: DSSS_OK (0) or a negative error code; dsss_last_error()
+ *    gives a message for the calling thread.  The reference aborts instead
+ *    (e.g. bloomfilter.hpp:595-600, merging.hpp:119-120).
+ *  - Device entry points take device pointers and run on `stream`; they
+ *    return after enqueuing, except where a size is needed on the host (the
+ *    DP round loop and the partition step read small counts back).
+ *  - A context owns reusable device scratch; use one context per host thread.
+ */
+#ifndef DSSS_H
+#define DSSS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSSS_ABI_VERSION 1
+
+#define DSSS_OK 0
+#define DSSS_EINVAL (-22)
+#define DSSS_ENOMEM (-12)
+#define DSSS_ETIMEDOUT (-110)
+#define DSSS_EDEVICE (-5)
+#define DSSS_ENOTSUP (-95)
+
+/* cudaStream_t without including CUDA headers (same underlying type). */
+typedef struct CUstream_st* dsss_stream_t;
+
+typedef struct dsss_ctx dsss_ctx;
+
+typedef struct dsss_arena {
+    const uint8_t* chars;    /* string bytes */
+    uint64_t char_bytes;     /* bytes in chars that strings may reference */
+    const uint64_t* offsets; /* [n] */
+    const uint32_t* lengths; /* [n] */
+    uint64_t n;
+} dsss_arena;
+
+/* Sampling policy of computePartition (samplingStrategies.hpp). */
+#define DSSS_SAMPLER_NUM_STRINGS 0         /* SampleSplittersNumStringsPolicy :19-90 */
+#define DSSS_SAMPLER_INDEXED_NUM_STRINGS 2 /* SampleIndexedSplittersNumStringsPolicy :106-186 */
+
+typedef struct dsss_opts {
+    uint32_t sampler;         /* DSSS_SAMPLER_* (prefix_doubling.cpp:359, default 0) */
+    uint32_t sampling_factor; /* splitters per PE = factor*(p-1); the PD path uses 2 (prefix_doubling.hpp:251) */
+    uint32_t small_sort_max;  /* string-sort knob: segments up to this size finish in one CTA (0 = default) */
+    uint32_t flags;           /* DSSS_FLAG_* */
+} dsss_opts;
+
+#define DSSS_FLAG_LOCAL_LCP 1u /* dsss_pd_sort also writes local_lcp (costs one compare pass) */
+
+/* Outputs of the full path, all device arrays of n entries unless noted.
+ * NULL optional outputs are skipped. */
+typedef struct dsss_pd_result {
+    uint32_t* local_order;   /* per PE, the input index of each locally sorted string */
+    uint32_t* local_lcp;     /* optional: LCP in local order, 0 at each PE start */
+    uint32_t* dp;            /* distinguishing-prefix length per string, local order */
+    uint64_t* intervals;     /* HOST [p*p]: strings PE q sends to PE r at [q*p + r] */
+    uint32_t* perm_index;    /* merged output of PE 0, PE 1, ...: index into sender's local order */
+    uint32_t* perm_pe;       /* ... and the sender PE */
+    uint32_t* merged_lcp;    /* optional: LCP of merged neighbours, 0 at each PE start */
+    uint64_t* recv_counts;   /* HOST [p]: merged strings per PE */
+} dsss_pd_result;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* hbm_budget_bytes: cap on scratch the context may hold (0 = no cap). */
+int dsss_ctx_create(int device, uint64_t hbm_budget_bytes, dsss_ctx** out);
+int dsss_ctx_destroy(dsss_ctx* ctx);
+/* Scratch bytes currently held by the context. */
+uint64_t dsss_ctx_scratch_bytes(const dsss_ctx* ctx);
+const char* dsss_last_error(void);
+int dsss_abi_version(void);
+
+/* ---- full path ---------------------------------------------------------- */
+
+/* DistributedPrefixDoublingSort<...>::sort (src/sorter/distributed/prefix_doubling.hpp:200-295):
+ * local sort, distinguishing prefixes, partition, exchange, merge, and the
+ * (stringIndex, PEIndex) permutation (:282-290).  As in the reference, p == 1
+ * stops after the local sort (:236): recv_counts[0] = 0, dp/perm untouched.
+ * Byte-identical strings merge in (sender PE, local index) order; the
+ * reference's loser tree orders them by tournament history instead. */
+int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                 const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream);
+
+/* Same with every array in host memory; copies in and out inside the call. */
+int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                      const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream);
+
+/* ---- stages (one per reference seam) ------------------------------------ */
+
+/* tlx::sort_strings_detail::radixsort_CI3(StringLcpPtr, 0, 0)
+ * (tlx/sort/strings/radix_sort.hpp:861-884), called per PE at prefix_doubling.hpp:228:
+ * sorts each PE's strings, order[i] = input index, lcp[i] = LCP with i-1 in
+ * the same PE (0 at each PE start). */
+int dsss_local_sort_lcp(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                        const dsss_opts* opts, uint32_t* order, uint32_t* lcp, dsss_stream_t stream);
+
+/* computeDistinguishingPrefixes<StringPtr, AllToAllHashesNaive>
+ * (prefix_doubling.hpp:156-198) over BloomFilter::filter rounds
+ * (bloomfilter.hpp:1415-1556): order/lcp are a local sort per PE (as
+ * dsss_local_sort_lcp writes them); dp[i] is the DP length of the string at
+ * local position i.  Exact 64-bit dedup of XXH64 prefix hashes mod 2^64-1,
+ * depths 8, 24, 40, 72, ...  round_counts (host, may be NULL) receives the
+ * candidate count after each round, up to max_rounds entries; *rounds the
+ * number of rounds run. */
+int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                     const uint32_t* order, const uint32_t* lcp, uint32_t* dp,
+                     uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds,
+                     dsss_stream_t stream);
+
+/* XXHasher::hash(str, depth, UINT64_MAX) (bloomfilter.hpp:1094-1102) over
+ * xxh::hash_state_t<64> (hash/xxhash.hpp:508-706) for strings ids[0..m):
+ * hash[j] = XXH64(seed 0) of the first min(depth, len) bytes of string ids[j]
+ * (the whole string when shorter), mod 2^64-1. */
+int dsss_prefix_hash(const dsss_arena* in, const uint32_t* ids, uint64_t m, uint32_t depth,
+                     uint64_t* hash, dsss_stream_t stream);
+
+/* computePartition<Sampler>(ptr, 2, dp) (misc.hpp:531-587, indexed :650-708):
+ * regular DP-truncated samples per PE, sorted, p-1 splitters, binary search
+ * per PE.  order/dp as dsss_dp_prefixes uses them; intervals (HOST, p*p) as in
+ * dsss_pd_result. */
+int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                   const uint32_t* order, const uint32_t* dp, const dsss_opts* opts,
+                   uint64_t* intervals, dsss_stream_t stream);
+
+/* calc_lcp of sorted neighbours (strings/stringtools.hpp:158-166): lcp[i] =
+ * LCP(string order[i-1], string order[i]) for i >= 1, lcp[0] = 0. */
+int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
+                      dsss_stream_t stream);
+
+/* ---- synthetic inputs (host) --------------------------------------------- */
+
+/* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),
+ * seeded and reproducible: string i is (k - d) 'A's, the d base-26 digits
+ * ('A' = 0) of pi(i) for a seeded permutation pi of [0, n), then uniform
+ * 'A'-'Z' up to its length; d = ceil(log26 n).  A seeded fraction frac_long of
+ * the strings uses (len_long, k_long) instead of (len_short, k_short).
+ * Layout: strings back to back, each followed by one NUL.
+ * Call with chars == NULL to get *char_bytes only. */
+int dsss_gen_dn(uint64_t n, uint32_t len_short, uint32_t k_short, uint32_t len_long, uint32_t k_long,
+                double frac_long, uint64_t seed, uint8_t* chars, uint64_t* offsets, uint32_t* lengths,
+                uint64_t* char_bytes);
+
+/* Text over {A,C,G,T} from a seeded order-3 Markov source; each position the
+ * source emits starts, with probability copy_prob, a copy of 1-4 KiB from an
+ * earlier offset.  text gets text_len bytes. */
+int dsss_gen_markov_text(uint64_t text_len, double copy_prob, uint64_t seed, uint8_t* text);
+
+/* All suffixes of a text of text_len bytes, truncated to max_len bytes:
+ * offsets[i] = i, lengths[i] = min(max_len, text_len - i). */
+int dsss_gen_suffixes(uint64_t text_len, uint32_t max_len, uint64_t* offsets, uint32_t* lengths);
+
+/* One serving request: n strings, lengths Zipf(s) on [min_len, max_len],
+ * bytes uniform 0x21-0x7E after a shared per-request prefix of length
+ * uniform in [0, len/2].  Layout as dsss_gen_dn. */
+int dsss_gen_request(uint64_t n, uint32_t min_len, uint32_t max_len, double zipf_s, uint64_t seed,
+                     uint8_t* chars, uint64_t* offsets, uint32_t* lengths, uint64_t* char_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSSS_H */

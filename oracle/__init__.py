@@ -1,0 +1,252 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrappers over oracle/liboracle.so (the CPU restatement of the
+reference's prefix-doubling path, oracle/oracle.cpp) and, where built, the
+pieces of the reference compiled from its own sources (oracle/_ref/).  Only
+tests/, __graft_entry__.smoke() and bench.py's CPU baseline legs may use this
+package, and only as the checker or the timed CPU baseline; the product never
+calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF = os.path.join(HERE, "_ref", "libref.so")
+REF_DP = os.path.join(HERE, "_ref", "libref_dp.so")
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_U32 = ctypes.c_uint32
+_I = ctypes.c_int
+
+_lib = None
+_ref = None
+_ref_dp = None
+
+
+def build():
+    """Compiles liboracle.so (and oracle/_ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        L.oracle_xxh64.restype = _U64
+        L.oracle_xxh64.argtypes = [_P, _U64]
+        L.oracle_local_sort.restype = None
+        L.oracle_local_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P]
+        L.oracle_dp.restype = None
+        L.oracle_dp.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _P, _P, _U32, _P]
+        L.oracle_partition.restype = None
+        L.oracle_partition.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _U32, _I, _P]
+        L.oracle_exchange.restype = _I
+        L.oracle_exchange.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.oracle_merge.restype = _I
+        L.oracle_merge.argtypes = [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P, _P]
+        L.oracle_pd_sort.restype = _I
+        L.oracle_pd_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF)
+
+
+def ref_dp_available() -> bool:
+    return os.path.exists(REF_DP)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(REF)
+        L.ref_xxh64.restype = _U64
+        L.ref_xxh64.argtypes = [_P, _U64]
+        L.ref_radixsort_ci3.restype = _I
+        L.ref_radixsort_ci3.argtypes = [_P, _U64, _U64, _P, _P]
+        L.ref_lcp_merge.restype = _I
+        L.ref_lcp_merge.argtypes = [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P, _P]
+        _ref = L
+    return _ref
+
+
+def ref_dp():
+    global _ref_dp
+    if _ref_dp is None:
+        L = ctypes.CDLL(REF_DP)
+        L.ref_dp_single_pe.restype = _I
+        L.ref_dp_single_pe.argtypes = [_P, _U64, _U64, _P, _P, _P]
+        _ref_dp = L
+    return _ref_dp
+
+
+def _p(a):
+    return a.ctypes.data if a is not None else None
+
+
+class Strings:
+    """Host strings for the oracle: chars (uint8 with >= 8 bytes of slack), offsets, lengths."""
+
+    def __init__(self, chars, offsets, lengths):
+        self.chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self.lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+        self.n = int(self.offsets.shape[0])
+
+    @classmethod
+    def from_host(cls, hs):
+        return cls(hs.chars, hs.offsets, hs.lengths)
+
+    def args(self):
+        return (_p(self.chars), _p(self.offsets), _p(self.lengths), self.n)
+
+    def get(self, i):
+        o, l = int(self.offsets[i]), int(self.lengths[i])
+        return self.chars[o:o + l].tobytes()
+
+    def raw(self, ids=None):
+        """NUL-terminated back-to-back layout (the reference's raw string vector)."""
+        ids = range(self.n) if ids is None else ids
+        return b"".join(self.get(int(i)) + b"\0" for i in ids)
+
+
+def xxh64(data: bytes) -> int:
+    buf = np.frombuffer(data + b"\0" * 16, dtype=np.uint8)
+    return int(lib().oracle_xxh64(_p(buf), len(data)))
+
+
+def local_sort(s: Strings, pb):
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    order = np.zeros(max(s.n, 1), np.uint64)
+    lcp = np.zeros(max(s.n, 1), np.uint64)
+    lib().oracle_local_sort(*s.args(), len(pb) - 1, _p(pb), _p(order), _p(lcp))
+    return order[:s.n], lcp[:s.n]
+
+
+def dp_rounds(s: Strings, pb, order, lcp, max_rounds=64):
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    order = np.ascontiguousarray(order, dtype=np.uint64)
+    lcp = np.ascontiguousarray(lcp, dtype=np.uint64)
+    dp = np.zeros(max(s.n, 1), np.uint64)
+    counts = np.zeros(max_rounds, np.uint64)
+    rounds = ctypes.c_uint32(0)
+    lib().oracle_dp(*s.args(), len(pb) - 1, _p(pb), _p(order), _p(lcp), _p(dp), _p(counts), max_rounds,
+                    ctypes.byref(rounds))
+    return dp[:s.n], counts[:rounds.value]
+
+
+def partition(s: Strings, pb, order, dp, indexed=False, factor=2):
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    iv = np.zeros(p * p, np.uint64)
+    order = np.ascontiguousarray(order, np.uint64)
+    dp = np.ascontiguousarray(dp, np.uint64)
+    lib().oracle_partition(*s.args(), p, _p(pb), _p(order), _p(dp), factor, 1 if indexed else 0, _p(iv))
+    return iv.reshape(p, p)
+
+
+def exchange(s: Strings, pb, order, lcp, dp, intervals):
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    keep = [np.ascontiguousarray(x, np.uint64).ravel() for x in (order, lcp, dp, intervals)]
+    args = (*s.args(), p, _p(pb), *(_p(x) for x in keep))
+    tot = ctypes.c_uint64(0)
+    lib().oracle_exchange(*args, ctypes.byref(tot), None, None, None, None, None, None, None)
+    n = s.n
+    out = dict(chars=np.zeros(tot.value + 1, np.uint8), char_begin=np.zeros(p + 1, np.uint64),
+               lcp=np.zeros(max(n, 1), np.uint64), index=np.zeros(max(n, 1), np.uint64),
+               pe=np.zeros(max(n, 1), np.uint64), counts=np.zeros(p * p, np.uint64), offsets=np.zeros(p * p, np.uint64))
+    lib().oracle_exchange(*args, ctypes.byref(tot), _p(out["chars"]), _p(out["char_begin"]), _p(out["lcp"]),
+                          _p(out["index"]), _p(out["pe"]), _p(out["counts"]), _p(out["offsets"]))
+    out["chars"] = out["chars"][:tot.value]
+    for k in ("lcp", "index", "pe"):
+        out[k] = out[k][:n]
+    out["counts"] = out["counts"].reshape(p, p)
+    out["offsets"] = out["offsets"].reshape(p, p)
+    return out
+
+
+def merge(chars, lcps, counts, offsets):
+    """The oracle's loser-tree merge of one PE's receive container."""
+    chars = np.ascontiguousarray(chars, np.uint8)
+    lcps = np.ascontiguousarray(lcps, np.uint64)
+    n = lcps.size
+    p = len(counts)
+    o = [np.zeros(max(n, 1), np.uint64) for _ in range(4)]
+    counts = np.ascontiguousarray(counts, np.uint64)
+    offsets = np.ascontiguousarray(offsets, np.uint64)
+    rc = lib().oracle_merge(_p(chars), chars.size, _p(lcps), n, p, _p(counts), _p(offsets), *(_p(x) for x in o))
+    assert rc == 0, rc
+    return tuple(x[:n] for x in o)
+
+
+def pd_sort(s: Strings, pb, indexed=False):
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    n = s.n
+    z = lambda: np.zeros(max(n, 1), np.uint64)
+    o = dict(order=z(), lcp=z(), dp=z(), intervals=np.zeros(p * p, np.uint64), perm_index=z(), perm_pe=z(),
+             merged_lcp=z(), old_lcp=z(), recv_counts=np.zeros(p, np.uint64))
+    rc = lib().oracle_pd_sort(*s.args(), p, _p(pb), 1 if indexed else 0, _p(o["order"]), _p(o["lcp"]), _p(o["dp"]),
+                              _p(o["intervals"]), _p(o["perm_index"]), _p(o["perm_pe"]), _p(o["merged_lcp"]),
+                              _p(o["old_lcp"]), _p(o["recv_counts"]))
+    assert rc == 0
+    for k in ("order", "lcp", "dp", "perm_index", "perm_pe", "merged_lcp", "old_lcp"):
+        o[k] = o[k][:n]
+    o["intervals"] = o["intervals"].reshape(p, p)
+    return o
+
+
+# ------------------------------------------------------------ reference ----
+def ref_xxh64(data: bytes) -> int:
+    buf = np.frombuffer(data + b"\0", dtype=np.uint8)
+    return int(ref().ref_xxh64(_p(buf), len(data)))
+
+
+def ref_local_sort(strs):
+    """radixsort_CI3 of the reference on a list of byte strings: (order, lcp)."""
+    raw = np.frombuffer(b"".join(x + b"\0" for x in strs) + b"\0", dtype=np.uint8)
+    n = len(strs)
+    order = np.zeros(max(n, 1), np.uint64)
+    lcp = np.zeros(max(n, 1), np.uint64)
+    rc = ref().ref_radixsort_ci3(_p(raw), raw.size - 1, n, _p(order), _p(lcp))
+    assert rc == 0, rc
+    return order[:n], lcp[:n]
+
+
+def ref_dp_single_pe(strs):
+    """The reference's own computeDistinguishingPrefixes on one PE: (order, lcp, dp)."""
+    raw = np.frombuffer(b"".join(x + b"\0" for x in strs) + b"\0", dtype=np.uint8)
+    n = len(strs)
+    order = np.zeros(max(n, 1), np.uint64)
+    lcp = np.zeros(max(n, 1), np.uint64)
+    dp = np.zeros(max(n, 1), np.uint64)
+    rc = ref_dp().ref_dp_single_pe(_p(raw), raw.size - 1, n, _p(order), _p(lcp), _p(dp))
+    assert rc == 0, rc
+    return order[:n], lcp[:n], dp[:n]
+
+
+def ref_lcp_merge(chars, lcps, recv_counts, recv_offsets):
+    """LcpStringLoserTree_ of the reference on one PE's receive container."""
+    chars = np.ascontiguousarray(chars, np.uint8)
+    lcps = np.ascontiguousarray(lcps, np.uint64)
+    n = lcps.size
+    p = len(recv_counts)
+    o = [np.zeros(max(n, 1), np.uint64) for _ in range(4)]
+    recv_counts = np.ascontiguousarray(recv_counts, np.uint64)
+    recv_offsets = np.ascontiguousarray(recv_offsets, np.uint64)
+    rc = ref().ref_lcp_merge(_p(chars), chars.size, _p(lcps), n, p, _p(recv_counts), _p(recv_offsets),
+                             *(_p(x) for x in o))
+    assert rc == 0, rc
+    return tuple(x[:n] for x in o)
