@@ -1,0 +1,297 @@
+"""Benchmark of the prefix-doubling string sort (one JSON line on stdout).
+
+Default workload (N=1): 32,000,000 strings of 200 bytes over 'A'-'Z', D/N 0.25
+(44 'A's + 6 base-26 digits of a seeded permutation + 150 random letters),
+split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
+
+  value     strings/s with the input resident in HBM (device-timed, max over ranks)
+  e2e       the same metric through dsss_pd_sort_host: pinned host input copied
+            in, results copied out, inside the timed region
+  roofline  the string sort (K3, the dominant stage) against HBM: algorithmic
+            bytes D + 20 n (SURVEY 8(d) B_sort, D = sum of DP lengths) over the
+            summed CUDA-event durations of its launches
+  cpu_baseline  the oracle port of the reference path on the host
+
+--impl reference times the CPU port of the reference path (oracle/) on all
+host cores: one independent sort of a 1e6-string sample of the same rule per
+thread, throughput = strings / wall time.
+Under torchrun (N > 1) every rank sorts its own instance (weak scaling; the
+cross-GPU exchange is not used by this benchmark).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (n, len, k, p, description)
+    "dn32m": (32_000_000, 200, 50, 64, "32e6 strings x 200 B, D/N 0.25, p = 64 PEs"),
+    "dn1m": (1_000_000, 100, 50, 4, "1e6 strings x 100 B, D/N 0.5, p = 4 PEs"),
+    "dn100m": (100_000_000, 100, 50, 64, "1e8 strings x 100 B, D/N 0.5, p = 64 PEs"),
+}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1].split()[0]))
+                mx.append(float(c[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_port(n_sample, L, k, p, seed):
+    """Oracle port, one thread, on a bounded sample of the workload."""
+    import __graft_entry__
+    import oracle
+    d = __graft_entry__.load_package()
+    hs = d.gen_dn(n_sample, L, k, seed=seed)
+    s = oracle.Strings.from_host(hs)
+    t = time.perf_counter()
+    oracle.pd_sort(s, d.equal_parts(hs.n, p))
+    return hs.n / (time.perf_counter() - t)
+
+
+def run_reference(args, cfg):
+    """--impl reference: the CPU port of the reference path on all host threads."""
+    import __graft_entry__
+    import oracle
+    d = __graft_entry__.load_package()
+    n, L, k, p, desc = cfg
+    threads = os.cpu_count() or 1
+    sample = 1_000_000
+    inputs = [d.gen_dn(sample, L, k, seed=100 + t) for t in range(threads)]
+    strs = [oracle.Strings.from_host(h) for h in inputs]
+    pb = d.equal_parts(sample, p)
+    oracle.lib()
+
+    def step():
+        ths = [threading.Thread(target=oracle.pd_sort, args=(s, pb)) for s in strs]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    sec = sum(times) / len(times)
+    value = threads * sample / sec
+    line = {
+        "impl": "reference", "metric": "strings/s", "value": value, "unit": "strings/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded D/N generator)",
+        "config": {"workload": desc, "n": n, "len": L, "p": p, "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "strings/s", "cores": threads, "kind": "port",
+                         "sample": f"{threads} independent sorts of 1e6 strings of the same rule, p = {p}"},
+        "e2e": {"value": value, "unit": "strings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="dn32m", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+
+    import torch
+    import __graft_entry__
+    d = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    n, L, k, p, desc = cfg
+    hs = d.gen_dn(n, L, k, seed=1 + rank, pinned=not args.no_e2e)
+    ds = d.DeviceStrings(hs, f"cuda:{local}")
+    ctx = d.Context(local)
+    stream = torch.cuda.current_stream()
+    out = None
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        out = d.pd_sort(ctx, ds, p, out=out)
+    torch.cuda.synchronize()
+
+    # timed region: K steps, device events on the launching stream
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = d.pd_sort(ctx, ds, p, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+
+    # per-kernel events (a second pass of the same K steps with timing on)
+    ctx.set_timing(True)
+    for _ in range(args.steps):
+        out = d.pd_sort(ctx, ds, p, out=out)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    kernels = {k2: v for k2, v in kt.items() if not k2.startswith("stage:")}
+    stages = {k2[6:]: v[1] / args.steps for k2, v in kt.items() if k2.startswith("stage:")}
+    launches_per_step = sum(v[0] for v in kernels.values()) / args.steps
+    sort_kernels = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
+                    "k_scatter", "k_small_sort", "scan_")
+    # sort launches of the partition's sample sort are tiny; all sort-kernel time counts
+    sort_ms = sum(v[1] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps
+    sort_launches = sum(v[0] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps
+
+    dp = out["dp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
+    D = int(dp.sum())
+    algo_bytes = D + 20 * n
+    peak, peak_kind = read_peaks()
+    achieved = algo_bytes / (sort_ms * 1e-3) / 1e9
+    char_bytes = int(hs.lengths.astype(np.uint64).sum()) + n
+    value = n * world / (ms * 1e-3)
+
+    # e2e through the host entry point
+    e2e = None
+    if not args.no_e2e:
+        hout = None
+        for _ in range(1):
+            hout = d.pd_sort_host(ctx, hs, p, out=hout, pinned=True)
+        barrier()
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        for _ in range(args.steps):
+            hout = d.pd_sort_host(ctx, hs, p, out=hout, pinned=True)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        ems = h0.elapsed_time(h1) / args.steps
+        if dist is not None:
+            t = torch.tensor([ems], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        h2d = hs.char_bytes + d.PAD + n * 12
+        d2h = n * 4 * 5 + p * p * 8
+        e2e = {"value": n * world / (ems * 1e-3), "unit": "strings/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = min(n, 8_000_000)
+        cpu = {"value": cpu_baseline_port(sample, L, k, p, seed=1), "unit": "strings/s", "cores": 1, "kind": "port",
+               "sample": f"{sample} strings of the same rule, p = {p}, oracle port single-threaded"}
+
+    if rank == 0:
+        line = {
+            "metric": "strings/s", "value": value, "unit": "strings/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded D/N generator)",
+            "config": {"workload": desc, "n": n, "len": L, "k": k, "p": p, "char_bytes": char_bytes,
+                       "l2": "inputs of %.2f GB > L2 (126 MB), no flush" % (char_bytes / 1e9),
+                       "parallelism": "one GPU holds all p PEs" if world == 1 else
+                       f"{world} ranks, one instance each (weak)"},
+            "char_gbs": char_bytes / (ms * 1e-3) / 1e9 * world,
+            "roofline": {"bound": "hbm", "kernel": "string sort K3 (all launches of the sort stage)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None, "algo_bytes": algo_bytes,
+                         "algo_formula": "D + 20 n", "sort_ms": sort_ms, "sort_launches": sort_launches},
+            "stages_ms": stages,
+            "kernels_ms": {k2: round(v[1] / args.steps, 4) for k2, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -58,6 +58,8 @@ _SIGS = {
     "dsss_ctx_destroy": (_I, [_P]),
     "dsss_ctx_scratch_bytes": (_U64, [_P]),
     "dsss_last_error": (ctypes.c_char_p, []),
+    "dsss_ctx_set_timing": (_I, [_P, _I]),
+    "dsss_ctx_kernel_times": (_I, [_P, ctypes.c_char_p, _U64]),
     "dsss_abi_version": (_I, []),
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
@@ -260,6 +262,20 @@ class Context:
     @property
     def scratch_bytes(self) -> int:
         return int(lib().dsss_ctx_scratch_bytes(self.h))
+
+    def set_timing(self, on: bool):
+        """Per-kernel CUDA-event timing of every launch this context makes."""
+        check(lib().dsss_ctx_set_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        """{kernel: (launches, total_ms)} for the launches timed since set_timing(True)."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        check(lib().dsss_ctx_kernel_times(self.h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, k, ms = line.split()
+            out[name] = (int(k), float(ms))
+        return out
 
 
 def _opts(sampler=0, sampling_factor=2, small_sort_max=0, flags=0) -> Opts:

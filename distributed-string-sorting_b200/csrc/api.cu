@@ -59,6 +59,7 @@ __global__ void k_to_local(const uint32_t* ord, const uint32_t* dpg, const uint3
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const uint32_t d = dest[g];
+    if (d >= n) return;
     local_order[d] = ord[g];
     dp_local[d] = dpg[g];
     g2l[g] = d - (uint32_t)pb[pe[g]];
@@ -84,6 +85,7 @@ __global__ void k_perm(const uint32_t* opos, const uint32_t* g2l, const uint32_t
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const uint32_t o = opos[g];
+    if (o >= n) return;
     perm_index[o] = g2l[g];
     perm_pe[o] = pe[g];
     out2g[o] = (uint32_t)g;
@@ -171,7 +173,10 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     }
     // 1. one sort of all strings
     uint64_t all[2] = {0, n};
-    DSSS_TRY(sort_strings(L.sort, a, n, 1, all, nullptr, L.ord, L.lcp, smax, pin, st));
+    {
+        StageTimer t("stage:sort", st);
+        DSSS_TRY(sort_strings(L.sort, a, n, 1, all, nullptr, L.ord, L.lcp, smax, pin, st));
+    }
     if (p == 1) {  // prefix_doubling.hpp:236: one PE sorts locally and returns no permutation
         DSSS_CUDA(cudaMemcpyAsync(out->local_order, L.ord, n * 4, cudaMemcpyDeviceToDevice, st));
         if (want_local_lcp) DSSS_CUDA(cudaMemcpyAsync(out->local_lcp, L.lcp, n * 4, cudaMemcpyDeviceToDevice, st));
@@ -179,17 +184,26 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         return DSSS_OK;
     }
     // 2. distinguishing prefixes over the global order
-    DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st));
+    {
+        StageTimer t("stage:dp", st);
+        DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st));
+    }
     // 3. local orders per PE
+    StageTimer t_local("stage:local", st);
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe);
+    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe));
     DSSS_TRY(multisplit(L.pe, n, p, L.tmp, L.ms, st));
-    k_to_local<<<grid_for(n, 256), 256, 0, st>>>(L.ord, L.dpg, L.pe, L.tmp, L.pb, n, out->local_order, out->dp,
-                                                L.g2l);
+    DSSS_LAUNCH("k_to_local", st, k_to_local<<<grid_for(n, 256), 256, 0, st>>>(L.ord, L.dpg, L.pe, L.tmp, L.pb, n, out->local_order, out->dp,
+                                                L.g2l));
     DSSS_CUDA(cudaGetLastError());
+    t_local.end();
     // 4. partition
-    DSSS_TRY(partition_pes(L.part, ctx, a, p, pb, out->local_order, out->dp, sampler_of(opts), factor,
-                           out->intervals, st));
+    {
+        StageTimer t("stage:partition", st);
+        DSSS_TRY(partition_pes(L.part, ctx, a, p, pb, out->local_order, out->dp, sampler_of(opts), factor,
+                               out->intervals, st));
+    }
+    StageTimer t_merge("stage:merge", st);
     // 5. buckets and the merged sequences
     std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), recv(p + 1, 0);
     for (uint32_t q = 0; q < p; ++q) {
@@ -206,14 +220,14 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     }
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp);
+    DSSS_LAUNCH("k_bucket_of", st, k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp));
     DSSS_TRY(multisplit(L.tmp, n, p, L.opos, L.ms, st));
-    k_perm<<<grid_for(n, 256), 256, 0, st>>>(L.opos, L.g2l, L.pe, n, out->perm_index, out->perm_pe, L.out2g);
+    DSSS_LAUNCH("k_perm", st, k_perm<<<grid_for(n, 256), 256, 0, st>>>(L.opos, L.g2l, L.pe, n, out->perm_index, out->perm_pe, L.out2g));
     if (out->merged_lcp)
-        k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->merged_lcp);
+        DSSS_LAUNCH("k_merged_lcp", st, k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->merged_lcp));
     if (want_local_lcp) {
         DSSS_TRY(adjacent_lcp(a, out->local_order, n, out->local_lcp, L.tmp, L.nlong, st));
-        k_zero_starts<<<grid_for(p, 128), 128, 0, st>>>(out->local_lcp, L.pb, p);
+        DSSS_LAUNCH("k_zero_starts", st, k_zero_starts<<<grid_for(p, 128), 128, 0, st>>>(out->local_lcp, L.pb, p));
     }
     DSSS_CUDA(cudaGetLastError());
     // The host vectors above were copied asynchronously; finish before they go.
@@ -230,6 +244,7 @@ extern "C" {
 int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, const dsss_opts* opts,
                  dsss_pd_result* out, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     DSSS_CUDA(cudaSetDevice(ctx->device));
     return pd_sort_dev(ctx, in, p, part_begin, opts, out, (cudaStream_t)stream);
 }
@@ -237,6 +252,7 @@ int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t
 int dsss_local_sort_lcp(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                         const dsss_opts* opts, uint32_t* order, uint32_t* lcp, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     DSSS_TRY(check_arena(in));
     DSSS_TRY(check_parts(p, part_begin, in->n));
     if (in->n && (!order || !lcp)) return fail(DSSS_EINVAL, "order/lcp is NULL");
@@ -257,6 +273,7 @@ int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint
                      const uint32_t* order, const uint32_t* lcp, uint32_t* dp, uint64_t* round_counts,
                      uint32_t max_rounds, uint32_t* rounds, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     DSSS_TRY(check_arena(in));
     DSSS_TRY(check_parts(p, part_begin, in->n));
     if (in->n && (!order || !lcp || !dp)) return fail(DSSS_EINVAL, "order/lcp/dp is NULL");
@@ -285,6 +302,7 @@ int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64
                    const uint32_t* order, const uint32_t* dp, const dsss_opts* opts, uint64_t* intervals,
                    dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     DSSS_TRY(check_arena(in));
     DSSS_TRY(check_parts(p, part_begin, in->n));
     if (!intervals || (in->n && (!order || !dp))) return fail(DSSS_EINVAL, "order/dp/intervals is NULL");
@@ -303,6 +321,7 @@ int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64
 int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
                       dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     DSSS_TRY(check_arena(in));
     if (m && (!order || !lcp)) return fail(DSSS_EINVAL, "order/lcp is NULL");
     DSSS_CUDA(cudaSetDevice(ctx->device));
@@ -321,6 +340,7 @@ int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order
 int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                       const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
     if (!in) return fail(DSSS_EINVAL, "arena is NULL");
     DSSS_TRY(check_parts(p, part_begin, in->n));
     if (!out) return fail(DSSS_EINVAL, "result is NULL");

@@ -7,6 +7,38 @@
 namespace dsss {
 
 static thread_local char g_err[512] = "";
+thread_local KernelTimes* g_times = nullptr;
+
+cudaEvent_t KernelTimes::get() {
+    if (pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+}
+
+void KernelTimes::fold() {
+    for (auto& p : pending) {
+        float ms = 0;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            size_t k = 0;
+            while (k < names.size() && names[k] != p.name) ++k;
+            if (k == names.size()) {
+                names.emplace_back(p.name);
+                total_ms.push_back(0);
+                launches.push_back(0);
+            }
+            total_ms[k] += ms;
+            launches[k] += 1;
+        }
+        pool.push_back(p.a);
+        pool.push_back(p.b);
+    }
+    pending.clear();
+}
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -156,9 +188,9 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* 
         if (total) DSSS_CUDA(cudaMemsetAsync(total, 0, sizeof(uint32_t), st));
         return DSSS_OK;
     }
-    scan_tile_sums<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, n, sums);
-    scan_sums<<<1, SCAN_NT, 0, st>>>(sums, tiles, total);
-    scan_tiles<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, out, n, sums);
+    DSSS_LAUNCH("scan_tile_sums", st, scan_tile_sums<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, n, sums));
+    DSSS_LAUNCH("scan_sums", st, scan_sums<<<1, SCAN_NT, 0, st>>>(sums, tiles, total));
+    DSSS_LAUNCH("scan_tiles", st, scan_tiles<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, out, n, sums));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }
@@ -186,8 +218,40 @@ int dsss_ctx_create(int device, uint64_t hbm_budget_bytes, dsss_ctx** out) {
     return DSSS_OK;
 }
 
+int dsss_ctx_set_timing(dsss_ctx* c, int on) {
+    if (!c) return fail(DSSS_EINVAL, "ctx is NULL");
+    if (!c->times) c->times = new KernelTimes();
+    c->times->on = on != 0;
+    if (on) {
+        c->times->names.clear();
+        c->times->total_ms.clear();
+        c->times->launches.clear();
+    }
+    return DSSS_OK;
+}
+
+int dsss_ctx_kernel_times(dsss_ctx* c, char* buf, uint64_t len) {
+    if (!c || !buf || !len) return fail(DSSS_EINVAL, "ctx/buf is NULL");
+    buf[0] = 0;
+    if (!c->times) return DSSS_OK;
+    c->times->fold();
+    uint64_t used = 0;
+    for (size_t k = 0; k < c->times->names.size(); ++k) {
+        int w = snprintf(buf + used, len - used, "%s %llu %.6f\n", c->times->names[k].c_str(),
+                         (unsigned long long)c->times->launches[k], c->times->total_ms[k]);
+        if (w < 0 || (uint64_t)w >= len - used) return fail(DSSS_EINVAL, "buffer too small");
+        used += (uint64_t)w;
+    }
+    return DSSS_OK;
+}
+
 int dsss_ctx_destroy(dsss_ctx* c) {
     if (!c) return DSSS_OK;
+    if (c->times) {
+        c->times->fold();
+        for (auto e : c->times->pool) cudaEventDestroy(e);
+        delete c->times;
+    }
     if (c->ws) cudaFree(c->ws);
     if (c->pin) cudaFreeHost(c->pin);
     delete c;

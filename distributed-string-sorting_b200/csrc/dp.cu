@@ -132,11 +132,11 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         uint64_t slots = table_slots(m);
         DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-        k_dp_round<<<grid_for(m, 256), 256, 0, st>>>(a, order, lcp, cand, m, (uint32_t)depth, dp, L.flag, L.slot,
-                                                    L.tkeys, L.tdup, (uint32_t)(slots - 1), L.counters + 1);
-        k_dp_query<<<grid_for(m, 256), 256, 0, st>>>(m, L.flag, L.slot, L.tdup);
+        DSSS_LAUNCH("k_dp_round", st, k_dp_round<<<grid_for(m, 256), 256, 0, st>>>(a, order, lcp, cand, m, (uint32_t)depth, dp, L.flag, L.slot,
+                                                    L.tkeys, L.tdup, (uint32_t)(slots - 1), L.counters + 1));
+        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid_for(m, 256), 256, 0, st>>>(m, L.flag, L.slot, L.tdup));
         DSSS_TRY(exclusive_scan_u32(L.flag, L.pos, m, L.counters, L.scan, st));
-        k_compact<<<grid_for(m, 256), 256, 0, st>>>(cand, m, L.flag, L.pos, L.cand[cur]);
+        DSSS_LAUNCH("k_compact", st, k_compact<<<grid_for(m, 256), 256, 0, st>>>(cand, m, L.flag, L.pos, L.cand[cur]));
         DSSS_CUDA(cudaGetLastError());
         DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
@@ -156,7 +156,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
 int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out,
                 cudaStream_t st) {
     if (m == 0) return DSSS_OK;
-    k_prefix_hash<<<grid_for(m, 256), 256, 0, st>>>(a, ids, m, depth, out);
+    DSSS_LAUNCH("k_prefix_hash", st, k_prefix_hash<<<grid_for(m, 256), 256, 0, st>>>(a, ids, m, depth, out));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }

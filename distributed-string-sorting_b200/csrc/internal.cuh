@@ -31,6 +31,21 @@ int fail(int code, const char* fmt, ...);
     } while (0)
 
 // --------------------------------------------------------------- context ----
+// Per-kernel timing: when a context has timing on, every launch made through
+// DSSS_LAUNCH inside its calls is bracketed by CUDA events on the launching
+// stream; durations are folded into per-name totals when the call finishes.
+struct KernelTimes {
+    bool on = false;
+    struct Pending { const char* name; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::string> names;
+    std::vector<double> total_ms;
+    std::vector<uint64_t> launches;
+    cudaEvent_t get();
+    void fold();  // after the stream has been synchronised
+};
+
 struct Ctx {
     int device = 0;
     uint64_t budget = 0;     // 0 = unlimited
@@ -38,7 +53,45 @@ struct Ctx {
     uint64_t ws_cap = 0;
     void* pin = nullptr;     // pinned host staging for small read-backs
     uint64_t pin_cap = 0;
+    KernelTimes* times = nullptr;
 };
+
+// The context whose call is running on this thread (for launch timing).
+extern thread_local KernelTimes* g_times;
+struct ActiveCtx {
+    KernelTimes* prev;
+    explicit ActiveCtx(Ctx* c) : prev(g_times) { g_times = (c && c->times && c->times->on) ? c->times : nullptr; }
+    ~ActiveCtx() { g_times = prev; }
+};
+
+// Brackets a stage (several launches and host read-backs) the same way.
+struct StageTimer {
+    KernelTimes* kt;
+    const char* name;
+    cudaEvent_t a = nullptr;
+    cudaStream_t st;
+    StageTimer(const char* nm, cudaStream_t s) : kt(g_times), name(nm), st(s) {
+        if (kt) { a = kt->get(); cudaEventRecord(a, st); }
+    }
+    void end() {
+        if (kt) {
+            cudaEvent_t b = kt->get();
+            cudaEventRecord(b, st);
+            kt->pending.push_back({name, a, b});
+            kt = nullptr;
+        }
+    }
+    ~StageTimer() { end(); }
+};
+
+#define DSSS_LAUNCH(name, st, ...)                                          \
+    do {                                                                    \
+        ::dsss::KernelTimes* kt_ = ::dsss::g_times;                         \
+        cudaEvent_t a_ = nullptr, b_ = nullptr;                             \
+        if (kt_) { a_ = kt_->get(); b_ = kt_->get(); cudaEventRecord(a_, st); } \
+        __VA_ARGS__;                                                        \
+        if (kt_) { cudaEventRecord(b_, st); kt_->pending.push_back({name, a_, b_}); } \
+    } while (0)
 
 // Bump allocator over the context scratch.  Run a layout twice: first with
 // sizing = true to learn the total, then for real after ensure_ws().

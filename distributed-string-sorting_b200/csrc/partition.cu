@@ -126,7 +126,7 @@ int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_
     uint64_t* hpin = (uint64_t*)ctx->pin;
     std::copy(lp.begin(), lp.end(), hpin);
     DSSS_CUDA(cudaMemcpyAsync(L.sample_lp, hpin, S * 8, cudaMemcpyHostToDevice, st));
-    k_sample_gather<<<grid_for(S, 256), 256, 0, st>>>(a, local_order, dp, L.sample_lp, S, L.soff, L.slen);
+    DSSS_LAUNCH("k_sample_gather", st, k_sample_gather<<<grid_for(S, 256), 256, 0, st>>>(a, local_order, dp, L.sample_lp, S, L.soff, L.slen));
     DSSS_CUDA(cudaGetLastError());
     ArenaDev sa{a.chars, L.soff, L.slen, S};
     uint64_t one[2] = {0, S};
@@ -153,8 +153,8 @@ int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_
     DSSS_CUDA(cudaMemcpyAsync(L.spl_len, sl.data(), nspl * 4, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.spl_index, si.data(), nspl * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pbv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    k_binsearch<<<grid_for((uint64_t)p * nspl, 128), 128, 0, st>>>(a, local_order, L.pb, p, (uint32_t)nspl, L.spl_off,
-                                                                  L.spl_len, L.spl_index, indexed ? 1 : 0, L.pos);
+    DSSS_LAUNCH("k_binsearch", st, k_binsearch<<<grid_for((uint64_t)p * nspl, 128), 128, 0, st>>>(a, local_order, L.pb, p, (uint32_t)nspl, L.spl_off,
+                                                                  L.spl_len, L.spl_index, indexed ? 1 : 0, L.pos));
     DSSS_CUDA(cudaGetLastError());
     std::vector<uint64_t> pos((uint64_t)p * nspl);
     DSSS_CUDA(cudaMemcpyAsync(pos.data(), L.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st));

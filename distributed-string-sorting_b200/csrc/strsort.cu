@@ -44,7 +44,7 @@ __device__ __forceinline__ int bin_of(uint32_t size) {
 }
 
 // Counters block (device): [0] n_large_next, [1..4] n_small per bin,
-// [8] total tiles, [9] total chunks.
+// [8] total tiles, [9] total chunks, [10] error flag (a guard tripped).
 struct SortState {
     ArenaDev a;
     uint32_t* ord[2];
@@ -79,6 +79,10 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
                                            uint32_t parity) {
     int b = bin_of(size);
     uint32_t slot = atomicAdd(&S.counters[1 + b], 1u);
+    if (slot >= S.cap_small) {
+        atomicExch(&S.counters[10], 1u);
+        return;
+    }
     Seg s;
     s.start = start;
     s.size = size;
@@ -93,6 +97,10 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
 __device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_t start, uint32_t size,
                                            uint32_t depth, uint32_t flags) {
     uint32_t slot = atomicAdd(&S.counters[0], 1u);
+    if (slot >= S.cap_large) {
+        atomicExch(&S.counters[10], 1u);
+        return;
+    }
     Seg s;
     s.start = start;
     s.size = size;
@@ -385,6 +393,10 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
         if (i >= te) continue;
         uint32_t dg = digit_of(k[j], shift);
         uint32_t dest = base[dg] + wcnt[w][dg] + rk[j];
+        if (dest < bstart[dg] || dest >= bstart[dg + 1]) {  // never taken when the counts agree
+            atomicExch(&S.counters[10], 1u);
+            continue;
+        }
         uint32_t o = ord[i];
         uint32_t bs = bstart[dg], cnt = bstart[dg + 1] - bs;
         if (dg == 0 || cnt == 1) {
@@ -531,7 +543,7 @@ static int launch_small(const SortState& S, const Seg* segs, uint32_t n, cudaStr
         DSSS_CUDA(cudaFuncSetAttribute(k_small_sort<CAP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         configured = true;
     }
-    k_small_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n);
+    DSSS_LAUNCH(CAP == 32 ? "k_small_sort32" : CAP == 256 ? "k_small_sort256" : CAP == 1024 ? "k_small_sort1024" : "k_small_sort4096", st, k_small_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }
@@ -596,10 +608,10 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
 
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb_host, (p + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
-    k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n);
+    DSSS_LAUNCH("k_init_ids", st, k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n));
     S.large[0] = large[0];
     S.large[1] = large[1];
-    k_init_segs<<<grid_for(p, 128), 128, 0, st>>>(S, L.pb, p);
+    DSSS_LAUNCH("k_init_segs", st, k_init_segs<<<grid_for(p, 128), 128, 0, st>>>(S, L.pb, p));
     DSSS_CUDA(cudaGetLastError());
     DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
@@ -611,7 +623,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         Seg* segs = large[cur];
         Seg* next = large[cur ^ 1];
         // tile / chunk indexing
-        k_tile_counts<<<grid_for(nlarge, 256), 256, 0, st>>>(segs, nlarge, S.tmp_counts, S.tmp_counts + L.cap_large);
+        DSSS_LAUNCH("k_tile_counts", st, k_tile_counts<<<grid_for(nlarge, 256), 256, 0, st>>>(segs, nlarge, S.tmp_counts, S.tmp_counts + L.cap_large));
         DSSS_TRY(exclusive_scan_u32(S.tmp_counts, S.tile0, nlarge, S.counters + 8, L.scan, st));
         DSSS_TRY(exclusive_scan_u32(S.tmp_counts + L.cap_large, S.chunk0, nlarge, S.counters + 9, L.scan, st));
         DSSS_CUDA(cudaMemsetAsync(S.counters, 0, sizeof(uint32_t), st));  // n_large_next
@@ -619,16 +631,17 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         uint64_t max_tiles = std::min<uint64_t>(L.cap_tiles, n / LT_TILE + nlarge + 1);
         uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
         S.large[0] = segs;
-        k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
-        k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
-        k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
-        k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge);
-        k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next);
-        k_scatter<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge);
+        DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_hist", st, k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_seg_scan", st, k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next));
+        DSSS_LAUNCH("k_scatter", st, k_scatter<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_CUDA(cudaGetLastError());
         DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
         nlarge = pin[0];
+        if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
         if (nlarge > L.cap_large) return fail(DSSS_EDEVICE, "string sort: large-segment list overflow");
         cur ^= 1;
     }

@@ -65,9 +65,9 @@ int adjacent_lcp(const ArenaDev& a, const uint32_t* order, uint64_t m, uint32_t*
                  uint32_t* nlong, cudaStream_t st) {
     if (m == 0) return DSSS_OK;
     DSSS_CUDA(cudaMemsetAsync(nlong, 0, sizeof(uint32_t), st));
-    k_adjacent_lcp<<<grid_for(m, 256), 256, 0, st>>>(a, order, m, lcp, longq, nlong);
-    k_adjacent_lcp_warp<<<(unsigned)std::min<uint64_t>(grid_for(m * 32, 256), 148 * 16), 256, 0, st>>>(a, order, longq,
-                                                                                                  nlong, lcp);
+    DSSS_LAUNCH("k_adjacent_lcp", st, k_adjacent_lcp<<<grid_for(m, 256), 256, 0, st>>>(a, order, m, lcp, longq, nlong));
+    DSSS_LAUNCH("k_adjacent_lcp_warp", st, k_adjacent_lcp_warp<<<(unsigned)std::min<uint64_t>(grid_for(m * 32, 256), 148 * 16), 256, 0, st>>>(a, order, longq,
+                                                                                                  nlong, lcp));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }
@@ -136,7 +136,10 @@ __global__ void __launch_bounds__(MS_NT) k_ms_scatter(const uint32_t* bucket, ui
 #pragma unroll
     for (int j = 0; j < MS_IPT; ++j) {
         uint64_t i = wb + j * 32 + lane;
-        if (i < n) dest[i] = base[bk[j]] + wcnt[w * P + bk[j]] + rk[j];
+        if (i < n) {
+            uint32_t d = base[bk[j]] + wcnt[w * P + bk[j]] + rk[j];
+            dest[i] = d < n ? d : 0xFFFFFFFFu;  // out-of-range marks a count mismatch; users check
+        }
     }
 }
 
@@ -164,9 +167,9 @@ int multisplit(const uint32_t* bucket, uint64_t n, uint32_t P, uint32_t* dest, v
                                        (int)(MAX_SPLIT_BUCKETS * (1 + MS_NT / 32) * sizeof(uint32_t))));
         configured = true;
     }
-    k_ms_hist<<<(unsigned)tiles, MS_NT, sh1, st>>>(bucket, n, P, tiles, hist);
+    DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, sh1, st>>>(bucket, n, P, tiles, hist));
     DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
-    k_ms_scatter<<<(unsigned)tiles, MS_NT, sh2, st>>>(bucket, n, P, tiles, off, dest);
+    DSSS_LAUNCH("k_ms_scatter", st, k_ms_scatter<<<(unsigned)tiles, MS_NT, sh2, st>>>(bucket, n, P, tiles, off, dest));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }

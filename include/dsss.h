@@ -94,6 +94,11 @@ int dsss_ctx_destroy(dsss_ctx* ctx);
 /* Scratch bytes currently held by the context. */
 uint64_t dsss_ctx_scratch_bytes(const dsss_ctx* ctx);
 const char* dsss_last_error(void);
+/* Per-kernel timing (CUDA events around every launch of the calls made with
+ * this context, on the launching stream).  on != 0 clears the totals. */
+int dsss_ctx_set_timing(dsss_ctx* ctx, int on);
+/* Lines "kernel launches total_ms" for the launches timed so far. */
+int dsss_ctx_kernel_times(dsss_ctx* ctx, char* buf, uint64_t len);
 int dsss_abi_version(void);
 
 /* ---- full path ---------------------------------------------------------- */
