@@ -1,0 +1,204 @@
+// K6 — on-device bucket scatter: AllToAllStringImplPrefixDoubling::alltoallv
+// (src/mpi/alltoall.hpp:910-1008) with EmptyPrefixDoublingLcpByteEncoderMemCpy
+// (src/mpi/byte_encoder.hpp:139-171) for p PEs that share one GPU.
+//
+// PE r's receive container holds, in source-PE order, the r-th interval of
+// every PE (intervals[q*p + r] strings of PE q's local order).  Each string
+// contributes bytes [lcp', dp) and a NUL, where lcp' is its local LCP except
+// 0 at the first string of every non-empty interval (setLcpAtStartOfInterval,
+// alltoall.hpp:396-404); its tag is (index in the sender's local order,
+// sender PE) (InitPolicy<IndexPEIndex>, strings/stringcontainer.hpp:127-158).
+//
+// One thread per string computes its receive slot arithmetically (no sort:
+// slots follow from the interval table), a scan turns byte counts into
+// offsets, and a copy kernel gathers the bytes — warp-cooperative for long
+// strings.
+#include <vector>
+
+#include "exchange.cuh"
+#include "internal.cuh"
+
+namespace dsss {
+
+__global__ void k_recv_slots(ArenaDev a, const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp,
+                             const uint64_t* pb, const uint64_t* bounds, const uint64_t* slot_base, uint32_t p,
+                             uint64_t n, uint32_t* cnt, uint32_t* rlcp, uint32_t* rindex, uint32_t* rpe,
+                             uint32_t* rsrc, uint32_t* err) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    uint32_t lo = 0, hi = p;  // PE of local position g: last q with pb[q] <= g
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (pb[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t q = lo;
+    const uint64_t i = g - pb[q];
+    const uint64_t* b = bounds + (uint64_t)q * (p + 1);
+    lo = 0;
+    hi = p;  // bucket: last r with b[r] <= i
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (b[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t r = lo;
+    const uint32_t l = i == b[r] ? 0u : lcp[g];
+    const uint32_t d = dp[g];
+    if (d < l) {  // a DP shorter than the LCP cannot come from a consistent local sort
+        atomicExch(err, 1u);
+        return;
+    }
+    const uint64_t o = slot_base[(uint64_t)r * p + q] + (i - b[r]);
+    if (o >= n) {
+        atomicExch(err, 1u);
+        return;
+    }
+    cnt[o] = d - l + 1;
+    rlcp[o] = l;
+    rindex[o] = (uint32_t)i;
+    rpe[o] = q;
+    rsrc[o] = local_order[g];
+}
+
+__global__ void k_sum_u32(const uint32_t* v, uint64_t n, unsigned long long* total) {
+    unsigned long long s = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        s += v[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(total, s);
+}
+
+// Copies bytes [lcp, lcp + cnt - 1) of each source string and a NUL.  Strings
+// up to 64 bytes: one thread; longer: one warp (queued).
+constexpr uint32_t COPY_THREAD_MAX = 64;
+
+__device__ __forceinline__ void copy_bytes(uint8_t* dst, const uint8_t* src, uint32_t m) {
+    uint32_t k = 0;
+    for (; k + 8 <= m; k += 8) {
+        uint64_t w = load_le8(src + k);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) dst[k + b] = (uint8_t)(w >> (8 * b));
+    }
+    for (; k < m; ++k) dst[k] = src[k];
+}
+
+__global__ void k_recv_copy(ArenaDev a, uint64_t n, const uint32_t* cnt, const uint32_t* cstart, const uint32_t* rlcp,
+                            const uint32_t* rsrc, uint8_t* out, uint32_t* longq, uint32_t* nlong) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const uint32_t m = cnt[o] - 1;
+    uint8_t* dst = out + cstart[o];
+    dst[m] = 0;
+    if (m > COPY_THREAD_MAX) {
+        longq[atomicAdd(nlong, 1u)] = (uint32_t)o;
+        return;
+    }
+    const uint32_t s = rsrc[o];
+    copy_bytes(dst, a.chars + a.off[s] + rlcp[o], m);
+}
+
+__global__ void k_recv_copy_warp(ArenaDev a, const uint32_t* cnt, const uint32_t* cstart, const uint32_t* rlcp,
+                                 const uint32_t* rsrc, uint8_t* out, const uint32_t* longq, const uint32_t* nlong) {
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = *nlong;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += nw) {
+        const uint32_t o = longq[w];
+        const uint32_t m = cnt[o] - 1;
+        const uint8_t* src = a.chars + a.off[rsrc[o]] + rlcp[o];
+        uint8_t* dst = out + cstart[o];
+        for (uint32_t k = lane; k < m; k += 32) dst[k] = src[k];
+    }
+}
+
+void layout_exchange(Carve& c, ExchangeLayout& L, uint64_t n, uint32_t p) {
+    uint64_t N = n ? n : 1;
+    L.cnt = c.take<uint32_t>(N);
+    L.cstart = c.take<uint32_t>(N);
+    L.src = c.take<uint32_t>(N);
+    L.longq = c.take<uint32_t>(N);
+    L.counters = c.take<uint32_t>(4);
+    L.total64 = c.take<unsigned long long>(1);
+    L.pb = c.take<uint64_t>(p + 1);
+    L.bounds = c.take<uint64_t>((uint64_t)p * (p + 1));
+    L.slot_base = c.take<uint64_t>((uint64_t)p * p);
+    L.scan = c.take<unsigned char>(scan_scratch_bytes(N));
+}
+
+int bucket_scatter(const ExchangeLayout& L, const ArenaDev& a, uint32_t p, const uint64_t* pb,
+                   const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, const uint64_t* intervals,
+                   uint64_t* char_total, uint8_t* recv_chars, uint64_t recv_capacity, uint64_t* recv_char_begin,
+                   uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe, uint64_t* recv_counts,
+                   uint64_t* recv_offsets, uint32_t* pin, cudaStream_t st) {
+    const uint64_t n = pb[p];
+    // interval bounds per sender, receive slots per (receiver, sender)
+    std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), slot((uint64_t)p * p), rbeg(p + 1, 0);
+    for (uint32_t q = 0; q < p; ++q) {
+        bounds[(uint64_t)q * (p + 1)] = 0;
+        uint64_t tot = 0;
+        for (uint32_t r = 0; r < p; ++r) {
+            tot += intervals[(uint64_t)q * p + r];
+            bounds[(uint64_t)q * (p + 1) + r + 1] = tot;
+        }
+        if (tot != pb[q + 1] - pb[q]) return fail(DSSS_EINVAL, "intervals of PE %u do not add up to its size", q);
+    }
+    for (uint32_t r = 0; r < p; ++r) {
+        uint64_t run = rbeg[r];
+        for (uint32_t q = 0; q < p; ++q) {
+            slot[(uint64_t)r * p + q] = run;
+            if (recv_counts) recv_counts[(uint64_t)r * p + q] = intervals[(uint64_t)q * p + r];
+            if (recv_offsets) recv_offsets[(uint64_t)r * p + q] = bounds[(uint64_t)q * (p + 1) + r];
+            run += intervals[(uint64_t)q * p + r];
+        }
+        rbeg[r + 1] = run;
+    }
+    if (n == 0) {
+        *char_total = 0;
+        if (recv_char_begin)
+            for (uint32_t r = 0; r <= p; ++r) recv_char_begin[r] = 0;
+        return DSSS_OK;
+    }
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 4 * sizeof(uint32_t), st));
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.slot_base, slot.data(), slot.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_LAUNCH("k_recv_slots", st,
+                k_recv_slots<<<grid_for(n, 256), 256, 0, st>>>(a, local_order, lcp, dp, L.pb, L.bounds, L.slot_base,
+                                                              p, n, L.cnt, recv_lcp, recv_index, recv_pe, L.src,
+                                                              L.counters + 2));
+    DSSS_TRY(exclusive_scan_u32(L.cnt, L.cstart, n, L.counters, L.scan, st));
+    DSSS_CUDA(cudaMemsetAsync(L.total64, 0, 8, st));
+    DSSS_LAUNCH("k_sum_u32", st, k_sum_u32<<<148 * 4, 256, 0, st>>>(L.cnt, n, L.total64));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaMemcpyAsync(pin + 4, L.total64, 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[2]) return fail(DSSS_EINVAL, "dp shorter than lcp: order/lcp/dp are not a local sort");
+    const uint64_t total64 = *(const uint64_t*)(pin + 4);
+    if (total64 >= (1ull << 32)) return fail(DSSS_ENOTSUP, "receive containers over 4 GiB per call");
+    *char_total = pin[0];
+    if (recv_char_begin) {
+        std::vector<uint32_t> cs(p + 1);
+        for (uint32_t r = 0; r < p; ++r) {
+            if (rbeg[r] < n) DSSS_CUDA(cudaMemcpyAsync(&cs[r], L.cstart + rbeg[r], 4, cudaMemcpyDeviceToHost, st));
+            else cs[r] = pin[0];
+        }
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        for (uint32_t r = 0; r < p; ++r) recv_char_begin[r] = cs[r];
+        recv_char_begin[p] = pin[0];
+    }
+    if (!recv_chars) return DSSS_OK;
+    if (recv_capacity < *char_total) return fail(DSSS_EINVAL, "receive buffer of %llu bytes < %llu needed",
+                                                 (unsigned long long)recv_capacity, (unsigned long long)*char_total);
+    DSSS_LAUNCH("k_recv_copy", st,
+                k_recv_copy<<<grid_for(n, 256), 256, 0, st>>>(a, n, L.cnt, L.cstart, recv_lcp, L.src, recv_chars,
+                                                             L.longq, L.counters + 1));
+    DSSS_LAUNCH("k_recv_copy_warp", st,
+                k_recv_copy_warp<<<148 * 8, 256, 0, st>>>(a, L.cnt, L.cstart, recv_lcp, L.src, recv_chars, L.longq,
+                                                         L.counters + 1));
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+}  // namespace dsss
