@@ -8,7 +8,8 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   e2e       the same metric through dsss_pd_sort_host: pinned host input copied
             in, results copied out, inside the timed region
   roofline  the string sort (K3, the dominant stage) against HBM: algorithmic
-            bytes D + 20 n (SURVEY 8(d) B_sort, D = sum of DP lengths) over the
+            bytes D + 20 n (D = sum of DP lengths: each distinguishing byte read
+            once, 8 B id read + 8 B id write + 4 B LCP write per string) over the
             summed CUDA-event durations of its launches
   cpu_baseline  the oracle port of the reference path on the host
 
@@ -64,7 +65,7 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
@@ -151,7 +152,7 @@ def run_reference(args, cfg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="dn32m", choices=sorted(CONFIGS))

@@ -1,0 +1,67 @@
+"""The C++ policy adaptors (include/dsss_policies.hpp) as a reference caller
+would use them: a small C++ program linked against libdsss.so, checked
+against the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from inputs import random_strings, with_duplicates
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def prog(dsss, tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "pd_sort_main")
+    pkg = os.path.dirname(dsss.LIB_PATH)
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "cpp", "pd_sort_main.cpp"), "-o", exe, "-L", pkg, "-ldsss",
+           "-Wl,-rpath," + pkg, "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64"]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def run(prog, per_pe, sampler=0):
+    lines = [str(len(per_pe))]
+    for strs in per_pe:
+        lines.append(str(len(strs)))
+        lines += [s.hex() if s else "-" for s in strs]
+    out = subprocess.run([prog, str(sampler)], input="\n".join(lines), capture_output=True, text=True, check=True)
+    res = {}
+    for line in out.stdout.splitlines():
+        parts = line.split()
+        res.setdefault(parts[0], {})[int(parts[1]) if parts[0] not in ("ci3order", "ci3lcp") else 0] = \
+            parts[2:] if parts[0] not in ("ci3order", "ci3lcp") else parts[1:]
+    return res
+
+
+@pytest.mark.parametrize("sampler", [0, 2])
+def test_policies_match_oracle(prog, orc, dsss, sampler):
+    p = 4
+    strs = with_duplicates(random_strings(2000, 1, 20, b"ABCDE", 77), 0.1, 78)
+    per_pe = [strs[q * 500:(q + 1) * 500] for q in range(p)]
+    res = run(prog, per_pe, sampler)
+    hs = dsss.from_bytes_list(strs)
+    r = orc.pd_sort(orc.Strings.from_host(hs), dsss.equal_parts(len(strs), p), indexed=sampler == 2)
+    n = len(strs)
+    order = np.concatenate([np.array(res["order"][q], np.uint64) + q * 500 for q in range(p)])
+    assert np.array_equal(order, r["order"])
+    dp = np.concatenate([np.array(res["dp"][q], np.uint64) for q in range(p)])
+    assert np.array_equal(dp, r["dp"])
+    iv = np.array([[int(x) for x in res["intervals"][q]] for q in range(p)], np.uint64)
+    assert np.array_equal(iv, r["intervals"])
+    perm = [tuple(map(int, x.split(":"))) for q in range(p) for x in res["perm"][q]]
+    ref = list(zip(r["perm_index"].tolist(), r["perm_pe"].tolist()))
+    # identical strings may differ in label order only; compare strings and label sets
+    def s_of(i, q):
+        return strs[q * 500 + int(r["order"][q * 500 + i]) - q * 500]
+    assert [s_of(i, q) for i, q in perm] == [s_of(i, q) for i, q in ref]
+    assert sorted(perm) == sorted(ref)
+    lcp = np.concatenate([np.array(res["lcp"][q], np.uint64) for q in range(p)])
+    assert np.array_equal(lcp, r["merged_lcp"])
+    ro, rl = orc.local_sort(orc.Strings.from_host(dsss.from_bytes_list(per_pe[0])), np.array([0, 500], np.uint64))
+    assert [int(x) for x in res["ci3order"][0]] == ro.tolist()
+    assert [int(x) for x in res["ci3lcp"][0]] == rl.tolist()
