@@ -69,6 +69,7 @@ _SIGS = {
     "dsss_prefix_hash": (_I, [ctypes.POINTER(Arena), _P, _U64, _U32, _P, _P]),
     "dsss_partition": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, ctypes.POINTER(Opts), _P, _P]),
     "dsss_adjacent_lcp": (_I, [_P, ctypes.POINTER(Arena), _P, _U64, _P, _P]),
+    "dsss_adjacent_lcp_noalloc": (_I, [ctypes.POINTER(Arena), _P, _U64, _P, _P]),
     "dsss_gen_dn": (_I, [_U64, _U32, _U32, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P]),
     "dsss_gen_markov_text": (_I, [_U64, ctypes.c_double, _U64, _P]),
     "dsss_gen_suffixes": (_I, [_U64, _U32, _P, _P]),
@@ -365,6 +366,14 @@ def partition(ctx: Context, ds: DeviceStrings, order, dp, p: int, part_begin=Non
     check(lib().dsss_partition(ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), _ptr(order), _ptr(dp), ctypes.byref(o),
                                _ptr(iv), _stream_ptr(stream)))
     return iv.reshape(p, p)
+
+
+def adjacent_lcp_noalloc(ds: DeviceStrings, order, lcp, stream=None):
+    """dsss_adjacent_lcp_noalloc: writes into the caller's lcp tensor and
+    allocates nothing (see include/dsss.h)."""
+    m = int(order.shape[0])
+    check(lib().dsss_adjacent_lcp_noalloc(ctypes.byref(ds.arena()), _ptr(order), m, _ptr(lcp), _stream_ptr(stream)))
+    return lcp
 
 
 def adjacent_lcp(ctx: Context, ds: DeviceStrings, order, stream=None):

@@ -158,6 +158,22 @@ int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64
 int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
                       dsss_stream_t stream);
 
+/* No counterpart in the reference (which never runs on a GPU): dsss_adjacent_lcp
+ * for callers that must not allocate device memory — code running inside
+ * another framework's memory pool, where a raw cudaMalloc bypasses the pool
+ * and can fail once the pool holds the free memory, and latency-critical
+ * loops that cannot take the device-wide synchronisation of cudaMalloc /
+ * cudaFree.  Same result as dsss_adjacent_lcp; no context, no allocation.
+ * Its scratch is a static device array of 16 MiB + 256 B that every GPU
+ * loading the library holds until the process exits, so m <= 4,194,304
+ * strings per call (larger m returns DSSS_EINVAL).  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) with the
+ * device current; make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
+int dsss_adjacent_lcp_noalloc(const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
+                              dsss_stream_t stream);
+
 /* ---- synthetic inputs (host) --------------------------------------------- */
 
 /* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),
