@@ -38,6 +38,7 @@ CONFIGS = {
     # name: (n, len, k, p, description)
     "dn32m": (32_000_000, 200, 50, 64, "32e6 strings x 200 B, D/N 0.25, p = 64 PEs"),
     "dn1m": (1_000_000, 100, 50, 4, "1e6 strings x 100 B, D/N 0.5, p = 4 PEs"),
+    "dn8m": (8_000_000, 200, 50, 64, "8e6 strings x 200 B, D/N 0.25, p = 64 PEs (profiling size)"),
     "dn100m": (100_000_000, 100, 50, 64, "1e8 strings x 100 B, D/N 0.5, p = 64 PEs"),
 }
 
@@ -224,7 +225,7 @@ def main():
     stages = {k2[6:]: v[1] / args.steps for k2, v in kt.items() if k2.startswith("stage:")}
     launches_per_step = sum(v[0] for v in kernels.values()) / args.steps
     sort_kernels = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
-                    "k_scatter", "k_small_sort", "scan_")
+                    "k_scatter", "k_seg_sort", "k_warp_segs", "scan_")
     # sort launches of the partition's sample sort are tiny; all sort-kernel time counts
     sort_ms = sum(v[1] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps
     sort_launches = sum(v[0] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps

@@ -53,18 +53,6 @@ __global__ void k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uin
     pe[g] = lo;
 }
 
-__global__ void k_to_local(const uint32_t* ord, const uint32_t* dpg, const uint32_t* pe, const uint32_t* dest,
-                           const uint64_t* pb, uint64_t n, uint32_t* local_order, uint32_t* dp_local,
-                           uint32_t* g2l) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const uint32_t d = dest[g];
-    if (d >= n) return;
-    local_order[d] = ord[g];
-    dp_local[d] = dpg[g];
-    g2l[g] = d - (uint32_t)pb[pe[g]];
-}
-
 __global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p, uint64_t n,
                             uint32_t* bucket) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -78,17 +66,6 @@ __global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint6
         else hi = mid;
     }
     bucket[g] = lo;
-}
-
-__global__ void k_perm(const uint32_t* opos, const uint32_t* g2l, const uint32_t* pe, uint64_t n, uint32_t* perm_index,
-                       uint32_t* perm_pe, uint32_t* out2g) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const uint32_t o = opos[g];
-    if (o >= n) return;
-    perm_index[o] = g2l[g];
-    perm_pe[o] = pe[g];
-    out2g[o] = (uint32_t)g;
 }
 
 __global__ void k_merged_lcp(const uint32_t* out2g, const uint32_t* lcpg, const uint64_t* recv_begin, uint32_t p,
@@ -117,7 +94,8 @@ __global__ void k_zero_starts(uint32_t* a, const uint64_t* pb, uint32_t p) {
 }
 
 struct PdLayout {
-    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *opos, *out2g, *nlong;
+    ulonglong2* handles;
+    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *out2g, *nlong, *err;
     uint64_t *pb, *bounds, *recv_begin;
     void* ms;
     SortLayout sort;
@@ -127,15 +105,16 @@ struct PdLayout {
 
 static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t p, uint32_t factor, uint32_t small_max) {
     uint64_t N = n ? n : 1;
+    L.handles = c.take<ulonglong2>(N);
     L.ord = c.take<uint32_t>(N);
     L.lcp = c.take<uint32_t>(N);
     L.dpg = c.take<uint32_t>(N);
     L.pe = c.take<uint32_t>(N);
     L.g2l = c.take<uint32_t>(N);
     L.tmp = c.take<uint32_t>(N);
-    L.opos = c.take<uint32_t>(N);
     L.out2g = c.take<uint32_t>(N);
     L.nlong = c.take<uint32_t>(1);
+    L.err = c.take<uint32_t>(1);
     L.pb = c.take<uint64_t>(p + 1);
     L.bounds = c.take<uint64_t>((uint64_t)p * (p + 1));
     L.recv_begin = c.take<uint64_t>(p + 1);
@@ -163,14 +142,17 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     DSSS_TRY(ensure_pin(ctx, 4096));
     Carve c(ctx->ws);
     layout_pd(c, L, n, p, factor, smax);
-    uint32_t* pin = (uint32_t*)ctx->pin;
-    const ArenaDev a = view(in);
+    uint32_t* pin = (uint32_t*)ctx->pin;  // re-read after any call that may grow it
+    ArenaDev a = view(in);
     if (n == 0) {
         for (uint32_t r = 0; r < p; ++r) out->recv_counts[r] = 0;
         if (p > 1)
             for (uint64_t k = 0; k < (uint64_t)p * p; ++k) out->intervals[k] = 0;
         return DSSS_OK;
     }
+    make_handles(a, L.handles, st);
+    a.h = L.handles;
+    DSSS_CUDA(cudaMemsetAsync(L.err, 0, sizeof(uint32_t), st));
     // 1. one sort of all strings
     uint64_t all[2] = {0, n};
     {
@@ -192,9 +174,12 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     StageTimer t_local("stage:local", st);
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
     DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe));
-    DSSS_TRY(multisplit(L.pe, n, p, L.tmp, L.ms, st));
-    DSSS_LAUNCH("k_to_local", st, k_to_local<<<grid_for(n, 256), 256, 0, st>>>(L.ord, L.dpg, L.pe, L.tmp, L.pb, n, out->local_order, out->dp,
-                                                L.g2l));
+    {
+        // local order and DP per PE: out[dest] = (string id, dp); g2l = rank inside the PE
+        const uint32_t* in[2] = {L.ord, L.dpg};
+        uint32_t* outs[2] = {out->local_order, out->dp};
+        DSSS_TRY(multisplit_payload(L.pe, n, p, 2, in, outs, L.g2l, L.err, L.ms, st));
+    }
     DSSS_CUDA(cudaGetLastError());
     t_local.end();
     // 4. partition
@@ -221,8 +206,12 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
     DSSS_LAUNCH("k_bucket_of", st, k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp));
-    DSSS_TRY(multisplit(L.tmp, n, p, L.opos, L.ms, st));
-    DSSS_LAUNCH("k_perm", st, k_perm<<<grid_for(n, 256), 256, 0, st>>>(L.opos, L.g2l, L.pe, n, out->perm_index, out->perm_pe, L.out2g));
+    {
+        // merged sequences: (index in sender's local order, sender PE, global position)
+        const uint32_t* in[3] = {L.g2l, L.pe, nullptr};
+        uint32_t* outs[3] = {out->perm_index, out->perm_pe, L.out2g};
+        DSSS_TRY(multisplit_payload(L.tmp, n, p, 3, in, outs, nullptr, L.err, L.ms, st));
+    }
     if (out->merged_lcp)
         DSSS_LAUNCH("k_merged_lcp", st, k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->merged_lcp));
     if (want_local_lcp) {
@@ -231,7 +220,10 @@ static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     }
     DSSS_CUDA(cudaGetLastError());
     // The host vectors above were copied asynchronously; finish before they go.
+    pin = (uint32_t*)ctx->pin;  // the partition step may have grown the staging buffer
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[0]) return fail(DSSS_EDEVICE, "pd sort: internal consistency guard tripped");
     return DSSS_OK;
 }
 
@@ -261,12 +253,17 @@ int dsss_local_sort_lcp(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const u
     const uint32_t smax = smallmax_of(opts);
     Carve sz(nullptr);
     SortLayout L;
+    sz.take<ulonglong2>(in->n ? in->n : 1);
     layout_sort(sz, L, in->n, p, smax);
     DSSS_TRY(ensure_ws(ctx, sz.used));
     DSSS_TRY(ensure_pin(ctx, 4096));
     Carve c(ctx->ws);
+    ulonglong2* h = c.take<ulonglong2>(in->n ? in->n : 1);
     layout_sort(c, L, in->n, p, smax);
-    return sort_strings(L, view(in), in->n, p, part_begin, nullptr, order, lcp, smax, (uint32_t*)ctx->pin, st);
+    ArenaDev a = view(in);
+    make_handles(a, h, st);
+    a.h = h;
+    return sort_strings(L, a, in->n, p, part_begin, nullptr, order, lcp, smax, (uint32_t*)ctx->pin, st);
 }
 
 int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
@@ -280,14 +277,19 @@ int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint
     DSSS_CUDA(cudaSetDevice(ctx->device));
     Carve sz(nullptr);
     DpLayout L;
+    sz.take<ulonglong2>(in->n ? in->n : 1);
     layout_dp(sz, L, in->n);
     DSSS_TRY(ensure_ws(ctx, sz.used));
     DSSS_TRY(ensure_pin(ctx, 4096));
     Carve c(ctx->ws);
+    ulonglong2* h = c.take<ulonglong2>(in->n ? in->n : 1);
     layout_dp(c, L, in->n);
+    ArenaDev a = view(in);
+    make_handles(a, h, (cudaStream_t)stream);
+    a.h = h;
     // The PE split needs no extra handling: every PE's first LCP is 0, so no
     // string is an LCP duplicate of the previous PE's last one.
-    return dp_rounds(L, view(in), in->n, order, lcp, dp, round_counts, max_rounds, rounds, (uint32_t*)ctx->pin,
+    return dp_rounds(L, a, in->n, order, lcp, dp, round_counts, max_rounds, rounds, (uint32_t*)ctx->pin,
                      (cudaStream_t)stream);
 }
 

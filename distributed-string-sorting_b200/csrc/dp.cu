@@ -2,8 +2,8 @@
 // src/sorter/distributed/prefix_doubling.hpp:156-198, over BloomFilter::filter,
 // src/sorter/distributed/bloomfilter.hpp:1415-1556).
 //
-// Round at depth d over the current candidates (positions in sorted order,
-// ascending), one thread per candidate (K1):
+// Round at depth d, one thread per sorted position, candidates marked in a
+// state byte array (K1):
 //   - length < d                       -> dp = length, retired (EOS, :1183-1186);
 //   - previous position is a candidate and lcp >= d
 //                                      -> dp = d, stays a candidate (LCP-local
@@ -17,7 +17,7 @@
 // range-partitioned all-to-all (:529-546, :558-656, :662-765).  Whether a
 // prefix hash is shared with another candidate does not depend on which PE
 // holds either string, so one table over all PEs gives the same survivors.
-// Survivors are compacted in position order into the next candidate list.
+// The hash table is sized by the number of strings hashed in the round.
 #include "internal.cuh"
 #include "dp.cuh"
 
@@ -25,31 +25,70 @@ namespace dsss {
 
 constexpr unsigned long long EMPTY_KEY = ~0ull;  // never a filter hash (mod 2^64-1)
 constexpr uint32_t NO_SLOT = 0xFFFFFFFFu;
+constexpr unsigned FULLM = 0xffffffffu;
 
-__device__ __forceinline__ uint32_t cand_at(const uint32_t* cand, uint32_t j) { return cand ? cand[j] : j; }
+// Candidate state per sorted position: st[i] = 1 while string i is a candidate.
+// kind[i] after classification: 0 retired or not a candidate, 1 LCP-local
+// duplicate (stays), 2 hashed (stays iff its hash is shared), 3 hashed root
+// (stays; its hash is still inserted so others can collide with it).
 
-__global__ void k_dp_round(ArenaDev a, const uint32_t* order, const uint32_t* lcp, const uint32_t* cand,
-                           uint32_t m, uint32_t depth, uint32_t* dp, uint32_t* flag, uint32_t* slot,
-                           unsigned long long* tkeys, uint8_t* tdup, uint32_t mask, uint32_t* err) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= m) return;
-    const uint32_t i = cand_at(cand, j);
-    const uint32_t s = order[i];
-    const uint32_t L = a.len[s];
-    if (depth > L) {
-        dp[i] = L;
-        flag[j] = 0;
-        slot[j] = NO_SLOT;
-        return;
+__global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_t* lens) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) lens[i] = a.len[order[i]];  // the 4-byte array caches better than 16-byte handles
+}
+
+// Adds the block's number of true flags to *ctr with one atomic per block
+// (blockDim.x == 256, called by every thread of the block).
+__device__ __forceinline__ void block_count(uint32_t* ctr, bool flag) {
+    __shared__ uint32_t part[8];
+    const uint32_t b = __ballot_sync(FULLM, flag);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += part[w];
+        if (t) atomicAdd(ctr, t);
     }
-    dp[i] = depth;
-    if (j > 0 && cand_at(cand, j - 1) == i - 1 && lcp[i] >= depth) {
-        flag[j] = 1;
-        slot[j] = NO_SLOT;
-        return;
+    __syncthreads();
+}
+
+__global__ void k_dp_classify(const uint8_t* st, int all, const uint32_t* lens, const uint32_t* lcp, uint64_t n,
+                              uint32_t depth, uint32_t* dp, uint8_t* st_next, uint8_t* kind, uint32_t* counters) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool hashed = false, stays = false;
+    if (i < n) {
+        uint8_t k = 0, nx = 0;
+        if (all || st[i]) {
+            const uint32_t L = lens[i];
+            if (depth > L) {
+                dp[i] = L;  // end of string before the depth (EOS)
+            } else {
+                dp[i] = depth;
+                if (i > 0 && (all || st[i - 1]) && lcp[i] >= depth) {
+                    k = 1;
+                    nx = 1;
+                } else {
+                    const bool root = i + 1 < n && (all || st[i + 1]) && lcp[i + 1] >= depth;
+                    k = root ? 3 : 2;
+                    nx = root ? 1 : 0;
+                    hashed = true;
+                }
+            }
+        }
+        kind[i] = k;
+        st_next[i] = nx;
+        stays = nx != 0;
     }
-    const bool root = j + 1 < m && cand_at(cand, j + 1) == i + 1 && lcp[i + 1] >= depth;
-    const unsigned long long h = filter_hash(xxh64_dev(a.chars + a.off[s], depth));
+    block_count(counters + 0, hashed);
+    block_count(counters + 1, stays);
+}
+
+__global__ void k_dp_hash(ArenaDev a, const uint32_t* order, const uint8_t* kind, uint64_t n, uint32_t depth,
+                          unsigned long long* tkeys, uint8_t* tdup, uint32_t mask, uint32_t* slot, uint32_t* err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    const unsigned long long h = filter_hash(xxh64_dev(a.chars + a.off[order[i]], depth));
     uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
     // Linear probing; the table always has free slots, so a free or matching
     // slot is reached within mask + 1 probes.
@@ -59,7 +98,7 @@ __global__ void k_dp_round(ArenaDev a, const uint32_t* order, const uint32_t* lc
             sl = NO_SLOT;
             break;
         }
-        unsigned long long prev = atomicCAS(&tkeys[sl], EMPTY_KEY, h);
+        const unsigned long long prev = atomicCAS(&tkeys[sl], EMPTY_KEY, h);
         if (prev == EMPTY_KEY) break;
         if (prev == h) {
             tdup[sl] = 1;
@@ -67,29 +106,28 @@ __global__ void k_dp_round(ArenaDev a, const uint32_t* order, const uint32_t* lc
         }
         sl = (sl + 1) & mask;
     }
-    flag[j] = root ? 1 : 2;
-    slot[j] = sl;
+    slot[i] = sl;
 }
 
-__global__ void k_dp_query(uint32_t m, uint32_t* flag, const uint32_t* slot, const uint8_t* tdup) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= m) return;
-    if (flag[j] == 2) flag[j] = (slot[j] != NO_SLOT && tdup[slot[j]]) ? 1 : 0;
-}
-
-__global__ void k_compact(const uint32_t* cand, uint32_t m, const uint32_t* flag, const uint32_t* pos,
-                          uint32_t* next) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= m) return;
-    if (flag[j]) next[pos[j]] = cand_at(cand, j);
+__global__ void k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup, uint64_t n,
+                           uint8_t* st_next, uint32_t* counters) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool stays = false;
+    if (i < n && kind[i] == 2) {
+        const uint32_t sl = slot[i];
+        stays = sl != NO_SLOT && tdup[sl];
+        st_next[i] = stays ? 1 : 0;
+    }
+    block_count(counters + 1, stays);
 }
 
 __global__ void k_prefix_hash(ArenaDev a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out) {
     const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= m) return;
-    const uint32_t s = ids[j];
-    const uint32_t L = a.len[s];
-    out[j] = filter_hash(xxh64_dev(a.chars + a.off[s], depth < L ? depth : L));
+    uint64_t off;
+    uint32_t L;
+    str_of(a, ids[j], off, L);
+    out[j] = filter_hash(xxh64_dev(a.chars + off, depth < L ? depth : L));
 }
 
 // Power-of-two table with at most two keys per three slots.
@@ -101,16 +139,15 @@ static uint64_t table_slots(uint64_t n) {
 
 void layout_dp(Carve& c, DpLayout& L, uint64_t n) {
     uint64_t N = n ? n : 1;
-    L.cand[0] = c.take<uint32_t>(N);
-    L.cand[1] = c.take<uint32_t>(N);
-    L.flag = c.take<uint32_t>(N);
-    L.pos = c.take<uint32_t>(N);
+    L.st[0] = c.take<uint8_t>(N);
+    L.st[1] = c.take<uint8_t>(N);
+    L.kind = c.take<uint8_t>(N);
+    L.lens = c.take<uint32_t>(N);
     L.slot = c.take<uint32_t>(N);
     L.slots = table_slots(N);
     L.tkeys = c.take<unsigned long long>(L.slots);
     L.tdup = c.take<uint8_t>(L.slots);
     L.counters = c.take<uint32_t>(8);
-    L.scan = c.take<unsigned char>(scan_scratch_bytes(N));
 }
 
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
@@ -121,32 +158,39 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         if (rounds) *rounds = 0;
         return DSSS_OK;
     }
-    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
-    const uint32_t* cand = nullptr;  // round 0: every position
-    uint32_t m = (uint32_t)n;
+    const unsigned grid = grid_for(n, 256);
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens));
     int cur = 0;
     const uint64_t start = 8;
     uint64_t depth = start;
     for (uint64_t i = start * 2;; i *= 2) {
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
-        uint64_t slots = table_slots(m);
-        DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
-        DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-        DSSS_LAUNCH("k_dp_round", st, k_dp_round<<<grid_for(m, 256), 256, 0, st>>>(a, order, lcp, cand, m, (uint32_t)depth, dp, L.flag, L.slot,
-                                                    L.tkeys, L.tdup, (uint32_t)(slots - 1), L.counters + 1));
-        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid_for(m, 256), 256, 0, st>>>(m, L.flag, L.slot, L.tdup));
-        DSSS_TRY(exclusive_scan_u32(L.flag, L.pos, m, L.counters, L.scan, st));
-        DSSS_LAUNCH("k_compact", st, k_compact<<<grid_for(m, 256), 256, 0, st>>>(cand, m, L.flag, L.pos, L.cand[cur]));
-        DSSS_CUDA(cudaGetLastError());
-        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
+        DSSS_LAUNCH("k_dp_classify", st,
+                    k_dp_classify<<<grid, 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
+                                                       L.st[cur ^ 1], L.kind, L.counters));
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
-        if (pin[1]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table overflow");
-        m = pin[0];
+        const uint32_t hashed = pin[0];
+        if (hashed) {
+            const uint64_t slots = table_slots(hashed);
+            DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+            DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
+            DSSS_LAUNCH("k_dp_hash", st,
+                        k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
+                                                       (uint32_t)(slots - 1), L.slot, L.counters + 2));
+            DSSS_LAUNCH("k_dp_query", st,
+                        k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
+            DSSS_CUDA(cudaGetLastError());
+            DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            DSSS_CUDA(cudaStreamSynchronize(st));
+            if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table overflow");
+        }
+        const uint32_t m = pin[1];
         if (round_counts && r < max_rounds) round_counts[r] = m;
         ++r;
-        if (m == 0) break;
-        cand = L.cand[cur];
         cur ^= 1;
+        if (m == 0) break;
         depth = start + i;
     }
     if (rounds) *rounds = r;

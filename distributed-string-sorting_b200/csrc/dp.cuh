@@ -5,15 +5,14 @@
 namespace dsss {
 
 struct DpLayout {
-    uint32_t* cand[2];
-    uint32_t* flag;
-    uint32_t* pos;
+    uint8_t* st[2];
+    uint8_t* kind;
+    uint32_t* lens;
     uint32_t* slot;
     unsigned long long* tkeys;
     uint8_t* tdup;
     uint64_t slots;
     uint32_t* counters;
-    unsigned char* scan;
 };
 
 void layout_dp(Carve& c, DpLayout& L, uint64_t n);

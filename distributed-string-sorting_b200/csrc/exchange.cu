@@ -95,8 +95,10 @@ __global__ void k_recv_copy(ArenaDev a, uint64_t n, const uint32_t* cnt, const u
         longq[atomicAdd(nlong, 1u)] = (uint32_t)o;
         return;
     }
-    const uint32_t s = rsrc[o];
-    copy_bytes(dst, a.chars + a.off[s] + rlcp[o], m);
+    uint64_t off;
+    uint32_t len;
+    str_of(a, rsrc[o], off, len);
+    copy_bytes(dst, a.chars + off + rlcp[o], m);
 }
 
 __global__ void k_recv_copy_warp(ArenaDev a, const uint32_t* cnt, const uint32_t* cstart, const uint32_t* rlcp,
@@ -107,7 +109,10 @@ __global__ void k_recv_copy_warp(ArenaDev a, const uint32_t* cnt, const uint32_t
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += nw) {
         const uint32_t o = longq[w];
         const uint32_t m = cnt[o] - 1;
-        const uint8_t* src = a.chars + a.off[rsrc[o]] + rlcp[o];
+        uint64_t off;
+        uint32_t len;
+        str_of(a, rsrc[o], off, len);
+        const uint8_t* src = a.chars + off + rlcp[o];
         uint8_t* dst = out + cstart[o];
         for (uint32_t k = lane; k < m; k += 32) dst[k] = src[k];
     }

@@ -118,7 +118,25 @@ struct ArenaDev {
     const uint64_t* off;
     const uint32_t* len;
     uint64_t n;
+    // Optional interleaved (offset, length) per string: one 16-byte load (one
+    // memory sector) per random lookup instead of two.
+    const ulonglong2* h = nullptr;
 };
+
+// Offset and length of string s.
+__device__ __forceinline__ void str_of(const ArenaDev& a, uint32_t s, uint64_t& off, uint32_t& len) {
+    if (a.h) {
+        const ulonglong2 v = __ldg(&a.h[s]);
+        off = v.x;
+        len = (uint32_t)v.y;
+    } else {
+        off = a.off[s];
+        len = a.len[s];
+    }
+}
+
+// Builds the interleaved handle array for strings [0, n).
+void make_handles(const ArenaDev& a, ulonglong2* h, cudaStream_t st);
 
 int check_arena(const dsss_arena* a);
 
@@ -150,6 +168,13 @@ __device__ __forceinline__ uint64_t key8(const uint8_t* chars, uint64_t off, uin
     uint32_t rem = len - depth;
     if (rem < 8) v &= (1ull << (rem * 8)) - 1;
     return bswap64(v);
+}
+
+__device__ __forceinline__ uint64_t key8_of(const ArenaDev& a, uint32_t s, uint32_t depth) {
+    uint64_t off;
+    uint32_t len;
+    str_of(a, s, off, len);
+    return key8(a.chars, off, len, depth);
 }
 
 // Index (0..7) of the first zero byte of a big-endian key, or 8 if none.

@@ -26,9 +26,11 @@ __global__ void k_sample_gather(ArenaDev a, const uint32_t* local_order, const u
     const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= m) return;
     const uint64_t lp = sample_lp[j];
-    const uint32_t s = local_order[lp];
-    soff[j] = a.off[s];
-    slen[j] = min(a.len[s], dp[lp]);
+    uint64_t off;
+    uint32_t len;
+    str_of(a, local_order[lp], off, len);
+    soff[j] = off;
+    slen[j] = min(len, dp[lp]);
 }
 
 // Sign of the byte-wise comparison of two strings (scmp, stringtools.hpp:128-136).
@@ -52,8 +54,10 @@ __global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint6
     const uint32_t sl = spl_len[k];
     while (left != right) {
         const uint64_t d = (right - left) / 2;
-        const uint32_t s = local_order[base + left + d];
-        int res = str_cmp(a.chars, a.off[s], a.len[s], so, sl);
+        uint64_t off;
+        uint32_t len;
+        str_of(a, local_order[base + left + d], off, len);
+        int res = str_cmp(a.chars, off, len, so, sl);
         if (res == 0 && indexed) {
             // indexStringCompare (misc.hpp:335-345): equal bytes compare by the
             // global index, as int64 narrowed to int.

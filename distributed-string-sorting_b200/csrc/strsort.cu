@@ -76,7 +76,7 @@ __device__ __forceinline__ uint32_t find_seg(const uint32_t* first, uint32_t nse
 }
 
 __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, uint32_t size, uint32_t depth,
-                                           uint32_t parity) {
+                                           uint32_t flags) {
     int b = bin_of(size);
     uint32_t slot = atomicAdd(&S.counters[1 + b], 1u);
     if (slot >= S.cap_small) {
@@ -87,7 +87,7 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
     s.start = start;
     s.size = size;
     s.depth = depth;
-    s.flags = parity;
+    s.flags = flags;
     s.newdepth = 0xFFFFFFFFu;
     s.first_digit = 0;
     s.diff = 0;
@@ -154,21 +154,46 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
     const uint32_t d0 = sg.depth, cap = d0 + PREFIX_CAP;
     const uint32_t s0 = ord[sg.start];
-    const uint64_t off0 = S.a.off[s0];
-    const uint32_t len0 = S.a.len[s0];
+    uint64_t off0;
+    uint32_t len0;
+    str_of(S.a, s0, off0, len0);
     uint32_t mn = 0xFFFFFFFFu;
     for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
-        uint32_t s = ord[i];
-        uint64_t off = S.a.off[s];
-        uint32_t len = S.a.len[s];
+        uint64_t off;
+        uint32_t len;
+        str_of(S.a, ord[i], off, len);
         uint32_t d = d0, l;
         for (;;) {
-            uint64_t x = key8(S.a.chars, off, len, d), y = key8(S.a.chars, off0, len0, d);
-            if (x != y) { l = d + key_lcp(x, y); break; }
-            uint32_t z = zero_byte(x);
-            if (z < 8) { l = d + z; break; }
-            d += 8;
-            if (d >= cap) { l = cap; break; }
+            // 16 bytes per step: two independent 8-byte compares
+            uint64_t x[2], y[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                x[q] = key8(S.a.chars, off, len, d + 8 * q);
+                y[q] = key8(S.a.chars, off0, len0, d + 8 * q);
+            }
+            bool done = false;
+            l = d + 16;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (!done) {
+                    if (x[q] != y[q]) {
+                        l = d + 8 * q + key_lcp(x[q], y[q]);
+                        done = true;
+                    } else {
+                        const uint32_t z = zero_byte(x[q]);
+                        if (z < 8) {
+                            l = d + 8 * q + z;
+                            done = true;
+                        }
+                    }
+                }
+            }
+            if (done) break;
+            d += 16;
+            if (d >= cap) {
+                l = d;
+                break;
+            }
         }
         mn = min(mn, l);
     }
@@ -195,19 +220,39 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
         k0 = key[sg.start];
     } else {
         uint32_t s0 = ord[sg.start];
-        k0 = key8(S.a.chars, S.a.off[s0], S.a.len[s0], depth);
+        k0 = key8_of(S.a, s0, depth);
     }
     uint64_t df = 0;
-    for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
-        uint64_t k;
-        if (valid) {
-            k = key[i];
-        } else {
-            uint32_t s = ord[i];
-            k = key8(S.a.chars, S.a.off[s], S.a.len[s], depth);
-            key[i] = k;
+    if (valid) {
+        for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) df |= key[i] ^ k0;
+    } else {
+        // four independent gathers in flight per thread
+        for (uint32_t i0 = tb + threadIdx.x; i0 < te; i0 += 4 * LT_NT) {
+            uint32_t s[4];
+            uint64_t off[4];
+            uint32_t len[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t i = i0 + q * LT_NT;
+                s[q] = i < te ? ord[i] : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t i = i0 + q * LT_NT;
+                off[q] = 0;
+                len[q] = 0;
+                if (i < te) str_of(S.a, s[q], off[q], len[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t i = i0 + q * LT_NT;
+                if (i < te) {
+                    const uint64_t k = key8(S.a.chars, off[q], len[q], depth);
+                    key[i] = k;
+                    df |= k ^ k0;
+                }
+            }
         }
-        df |= k ^ k0;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(0xffffffffu, df, o);
@@ -318,16 +363,28 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
     }
     if (total >= 2 && d != 0) {
         const uint32_t cs = sg.start + excl;
+        // children keep the parent's keys: their first b+1 key bytes are now common
         if (total > S.small_max) push_large(S, next, cs, total, depth, (par ^ 1u) | F_KEYS);
-        else push_small(S, cs, total, depth + b + 1, par ^ 1u);
+        else push_small(S, cs, total, depth, (par ^ 1u) | F_KEYS);
     }
 }
 
 // --------------------------------------------------------------- scatter ----
+// Ranks are stable within the tile (warp-aggregated per digit); the tile is
+// first reordered by digit in shared memory so that the global writes of each
+// digit's run are contiguous.
+constexpr size_t SCATTER_SMEM = (size_t)LT_TILE * (8 + 4 + 1);
+
 __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs, uint32_t nseg) {
+    extern __shared__ __align__(16) unsigned char sm_scatter[];
+    unsigned long long* skey = (unsigned long long*)sm_scatter;
+    uint32_t* sord = (uint32_t*)(skey + LT_TILE);
+    uint8_t* sdig = (uint8_t*)(sord + LT_TILE);
     __shared__ uint32_t base[256];
     __shared__ uint32_t bstart[257];
+    __shared__ uint32_t tloff[256];
     __shared__ uint32_t wcnt[LT_NT / 32][256];
+    __shared__ uint32_t wsum[LT_NT / 32];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -358,18 +415,25 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
     unsigned long long* key_dst = S.key[par ^ 1u];
     const uint32_t tb = sg.start + tloc * LT_TILE;
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    const uint32_t tn = te - tb;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t wb = tb + (uint32_t)w * 32 * LT_IPT;
     uint64_t k[LT_IPT];
+    uint32_t o[LT_IPT];
     uint32_t rk[LT_IPT];
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
-        uint32_t i = wb + j * 32 + lane;
+        const uint32_t i = wb + j * 32 + lane;
         k[j] = i < te ? key[i] : 0;
-        uint32_t dg = i < te ? digit_of(k[j], shift) : 0x100u + lane;
-        uint32_t peers = __match_any_sync(0xffffffffu, dg);
-        uint32_t r = __popc(peers & ((1u << lane) - 1));
-        uint32_t prev = dg < 256 ? wcnt[w][dg] : 0;
+        o[j] = i < te ? ord[i] : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < LT_IPT; ++j) {
+        const uint32_t i = wb + j * 32 + lane;
+        const uint32_t dg = i < te ? digit_of(k[j], shift) : 0x100u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+        const uint32_t r = __popc(peers & ((1u << lane) - 1));
+        const uint32_t prev = dg < 256 ? wcnt[w][dg] : 0;
         __syncwarp();
         if (dg < 256 && lane == __ffs(peers) - 1) wcnt[w][dg] = prev + __popc(peers);
         __syncwarp();
@@ -377,173 +441,366 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
     }
     __syncthreads();
     {
+        // exclusive over warps per digit, then over digits within the tile
         const uint32_t d = threadIdx.x;
         uint32_t run = 0;
 #pragma unroll
         for (int ww = 0; ww < LT_NT / 32; ++ww) {
-            uint32_t v = wcnt[ww][d];
+            const uint32_t v = wcnt[ww][d];
             wcnt[ww][d] = run;
             run += v;
         }
+        uint32_t x = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        uint32_t wpre = 0;
+        for (int ww = 0; ww < w; ++ww) wpre += wsum[ww];
+        tloff[d] = wpre + x - run;
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
-        uint32_t i = wb + j * 32 + lane;
+        const uint32_t i = wb + j * 32 + lane;
         if (i >= te) continue;
-        uint32_t dg = digit_of(k[j], shift);
-        uint32_t dest = base[dg] + wcnt[w][dg] + rk[j];
-        if (dest < bstart[dg] || dest >= bstart[dg + 1]) {  // never taken when the counts agree
+        const uint32_t dg = digit_of(k[j], shift);
+        const uint32_t lp = tloff[dg] + wcnt[w][dg] + rk[j];
+        if (lp >= tn) {  // never taken when the counts agree
             atomicExch(&S.counters[10], 1u);
             continue;
         }
-        uint32_t o = ord[i];
-        uint32_t bs = bstart[dg], cnt = bstart[dg + 1] - bs;
+        skey[lp] = k[j];
+        sord[lp] = o[j];
+        sdig[lp] = (uint8_t)dg;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < tn; x += LT_NT) {
+        const uint32_t dg = sdig[x];
+        const uint32_t dest = base[dg] + (x - tloff[dg]);
+        const uint32_t bs = bstart[dg], cnt = bstart[dg + 1] - bs;
+        if (dest < bs || dest >= bs + cnt) {  // never taken when the counts agree
+            atomicExch(&S.counters[10], 1u);
+            continue;
+        }
+        const uint32_t oo = sord[x];
         if (dg == 0 || cnt == 1) {
-            S.ord_out[dest] = o;
+            S.ord_out[dest] = oo;
             if (dg == 0 && dest != bs) S.lcp_out[dest] = depth + b;
         } else {
-            ord_dst[dest] = o;
-            if (cnt > S.small_max) key_dst[dest] = k[j];
+            ord_dst[dest] = oo;
+            key_dst[dest] = skey[x];
         }
         if (dest == bs && dg != sg.first_digit) S.lcp_out[dest] = depth + b;
     }
 }
 
 // ------------------------------------------------------------ small sort ----
+// Segments of 2..small_max strings finish inside one CTA (the tail the MSD
+// passes hand over, like the reference's insertion-sort / multikey tail):
+//  - buckets of up to 32 strings: one warp, a bitonic network across the 32
+//    lanes on (group, key, id); groups of equal keys are re-keyed 8 bytes
+//    deeper until each group is one string or byte-identical strings;
+//  - larger buckets: an MSD pass in shared memory on the first key byte that
+//    differs inside the bucket (warp-aggregated histogram, scan, stable
+//    scatter); children go on a shared-memory stack or to the warp list.
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ bool lt3(uint32_t g1, uint64_t k1, uint32_t o1, uint32_t g2, uint64_t k2, uint32_t o2) {
+    return g1 < g2 || (g1 == g2 && (k1 < k2 || (k1 == k2 && o1 < o2)));
+}
+
+// Lane i < size holds (key at `depth`, id).  On return lane i holds the i-th
+// smallest; lcp[lane] (lanes 1..size-1) gets the LCP with the predecessor.
+__device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint32_t depth, uint64_t& key,
+                                          uint32_t& id, uint32_t* lcp) {
+    const int lane = threadIdx.x & 31;
+    const bool valid = (uint32_t)lane < size;
+    uint32_t grp = valid ? 0u : 0xFFFFFFFFu;
+    uint32_t dep = depth;
+    if (!valid) {
+        key = ~0ull;
+        id = 0xFFFFFFFFu;
+    }
+    for (;;) {
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const uint32_t pg = __shfl_xor_sync(FULL, grp, j);
+                const uint64_t pk = __shfl_xor_sync(FULL, key, j);
+                const uint32_t po = __shfl_xor_sync(FULL, id, j);
+                const uint32_t pd = __shfl_xor_sync(FULL, dep, j);
+                const bool want_min = ((lane & k) == 0) == ((lane & j) == 0);
+                const bool take = want_min ? lt3(pg, pk, po, grp, key, id) : lt3(grp, key, id, pg, pk, po);
+                if (take) {
+                    grp = pg;
+                    key = pk;
+                    id = po;
+                    dep = pd;
+                }
+            }
+        }
+        const uint32_t qg = __shfl_up_sync(FULL, grp, 1);
+        const uint64_t qk = __shfl_up_sync(FULL, key, 1);
+        const bool head = lane == 0 || qg != grp || qk != key;
+        if (valid && lane > 0 && qg == grp) {
+            if (qk != key) {
+                lcp[lane] = dep + key_lcp(key, qk);
+            } else {
+                const uint32_t z = zero_byte(key);
+                if (z < 8) lcp[lane] = dep + z;  // byte-identical neighbours
+            }
+        }
+        const uint32_t heads = __ballot_sync(FULL, head);
+        const uint32_t rs = 31u - __clz(heads & ((2u << lane) - 1u));
+        const bool next_head = lane == 31 ? true : ((heads >> (lane + 1)) & 1u) != 0;
+        const bool multi = !head || (!next_head && (uint32_t)(lane + 1) < size);
+        const bool unres = valid && multi && zero_byte(key) == 8;
+        if (valid) grp = rs;
+        if (!__any_sync(FULL, unres)) break;
+        if (unres) {
+            dep += 8;
+            key = key8_of(a, id, dep);
+        }
+    }
+}
+
+// Segments of 2..32 strings: one warp each, four per CTA.
+__global__ void __launch_bounds__(128) k_warp_segs(SortState S, const Seg* segs, uint32_t nseg) {
+    const uint32_t si = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (si >= nseg) return;
+    const int lane = threadIdx.x & 31;
+    const Seg seg = segs[si];
+    const uint32_t* src = S.ord[seg.flags & F_PARITY];
+    uint32_t id = 0;
+    uint64_t key = 0;
+    if ((uint32_t)lane < seg.size) {
+        id = src[seg.start + lane];
+        key = (seg.flags & F_KEYS) ? S.key[seg.flags & F_PARITY][seg.start + lane]
+                                   : key8_of(S.a, id, seg.depth);
+    }
+    warp_sort(S.a, seg.size, seg.depth, key, id, S.lcp_out + seg.start);
+    if ((uint32_t)lane < seg.size) S.ord_out[seg.start + lane] = id;
+}
+
+template <int CAP>
+constexpr size_t seg_sort_smem() {
+    return (size_t)CAP * (8 + 8 + 4 + 4 + 4) + (size_t)(CAP / 2) * 3 * 4 * 2;
+}
+
 template <int CAP, int NT>
-__global__ void __launch_bounds__(NT) k_small_sort(SortState S, const Seg* segs, uint32_t nseg) {
+__global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg) {
+    constexpr int NW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* sk = (unsigned long long*)smem;
-    uint32_t* so = (uint32_t*)(sk + CAP);
-    uint32_t* sg = so + CAP;
-    uint32_t* sd = sg + CAP;
-    uint32_t* rs = sd + CAP;
-    __shared__ uint32_t shm[32];
-    __shared__ int s_unres;
-    constexpr int IPT = CAP / NT;
+    unsigned long long* tk = sk + CAP;
+    uint32_t* so = (uint32_t*)(tk + CAP);
+    uint32_t* to = so + CAP;
+    uint32_t* pk = to + CAP;  // digit << 24 | rank within the warp's chunk
+    uint32_t* stk = pk + CAP;  // (start, size, depth) of buckets > 32
+    uint32_t* wl = stk + 3 * (CAP / 2);  // (start, size, depth) of buckets <= 32
+    __shared__ uint32_t hist[256], bstart[256];
+    __shared__ uint32_t wcnt[NW][256];
+    __shared__ uint32_t s_top, s_nw, s_cur[3];
+    __shared__ unsigned long long s_diff;
     const uint32_t bi = blockIdx.x;
     if (bi >= nseg) return;
     const Seg seg = segs[bi];
     const uint32_t start = seg.start, size = seg.size;
     const uint32_t* src = S.ord[seg.flags & F_PARITY];
-    for (uint32_t i = threadIdx.x; i < CAP; i += NT) {
-        if (i < size) {
-            uint32_t o = src[start + i];
-            so[i] = o;
-            sd[i] = seg.depth;
-            sg[i] = 0;
-            sk[i] = key8(S.a.chars, S.a.off[o], S.a.len[o], seg.depth);
-        } else {
-            so[i] = 0xFFFFFFFFu;
-            sg[i] = 0xFFFFFFFFu;
-            sk[i] = ~0ull;
-            sd[i] = 0;
+    uint32_t* lcp = S.lcp_out + start;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (seg.flags & F_KEYS) {
+        const unsigned long long* ksrc = S.key[seg.flags & F_PARITY];
+        for (uint32_t i = threadIdx.x; i < size; i += NT) {
+            so[i] = src[start + i];
+            sk[i] = ksrc[start + i];
         }
+    } else {
+        for (uint32_t i = threadIdx.x; i < size; i += NT) {
+            const uint32_t o = src[start + i];
+            so[i] = o;
+            sk[i] = key8_of(S.a, o, seg.depth);
+        }
+    }
+    if (threadIdx.x == 0) {
+        s_top = 0;
+        s_nw = 0;
+        uint32_t* dst = size <= 32 ? wl : stk;
+        dst[0] = 0;
+        dst[1] = size;
+        dst[2] = seg.depth;
+        if (size <= 32) s_nw = 1;
+        else s_top = 1;
+        s_diff = 0;
     }
     __syncthreads();
     for (;;) {
-        // bitonic sort by (group, key, id)
-        for (uint32_t kk = 2; kk <= (uint32_t)CAP; kk <<= 1) {
-            for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = threadIdx.x; i < (uint32_t)CAP / 2; i += NT) {
-                    uint32_t a = 2 * j * (i / j) + (i % j), bb = a + j;
-                    bool asc = (a & kk) == 0;
-                    uint32_t ga = sg[a], gb = sg[bb];
-                    uint64_t ka = sk[a], kb = sk[bb];
-                    uint32_t oa = so[a], ob = so[bb];
-                    bool bless = gb < ga || (gb == ga && (kb < ka || (kb == ka && ob < oa)));
-                    if (bless == asc) {
-                        sg[a] = gb; sg[bb] = ga;
-                        sk[a] = kb; sk[bb] = ka;
-                        so[a] = ob; so[bb] = oa;
-                        uint32_t t2 = sd[a]; sd[a] = sd[bb]; sd[bb] = t2;
-                    }
-                }
-                __syncthreads();
+        if (threadIdx.x == 0) {
+            if (s_top) {
+                --s_top;
+                s_cur[0] = stk[3 * s_top];
+                s_cur[1] = stk[3 * s_top + 1];
+                s_cur[2] = stk[3 * s_top + 2];
+            } else {
+                s_cur[1] = 0;
             }
         }
-        // run heads: a new (group, key) starts; boundaries inside a group get their LCP.
-        uint32_t carry = 0;  // 1 + last head index in this thread's range, 0 = none
-        const uint32_t ib = threadIdx.x * IPT;
-#pragma unroll 1
-        for (int j = 0; j < IPT; ++j) {
-            uint32_t i = ib + j;
-            if (i >= size) break;
-            bool head = i == 0 || sg[i] != sg[i - 1];
-            if (!head) {
-                if (sk[i] != sk[i - 1]) {
-                    head = true;
-                    S.lcp_out[start + i] = sd[i] + key_lcp(sk[i], sk[i - 1]);
-                } else {
-                    uint32_t z = zero_byte(sk[i]);
-                    if (z < 8) S.lcp_out[start + i] = sd[i] + z;  // byte-identical neighbours
+        __syncthreads();
+        const uint32_t bs = s_cur[0], bn = s_cur[1], dep = s_cur[2];
+        if (bn == 0) break;
+        const uint64_t k0 = sk[bs];
+        uint64_t df = 0;
+        for (uint32_t i = threadIdx.x; i < bn; i += NT) df |= sk[bs + i] ^ k0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(FULL, df, o);
+        if (lane == 0 && df) atomicOr(&s_diff, (unsigned long long)df);
+        __syncthreads();
+        df = s_diff;
+        if (df == 0) {
+            const uint32_t z = zero_byte(k0);
+            if (z < 8) {
+                for (uint32_t i = threadIdx.x + 1; i < bn; i += NT) lcp[bs + i] = dep + z;
+            } else {
+                for (uint32_t i = threadIdx.x; i < bn; i += NT) {
+                    const uint32_t o = so[bs + i];
+                    sk[bs + i] = key8_of(S.a, o, dep + 8);
+                }
+                if (threadIdx.x == 0) {
+                    stk[3 * s_top] = bs;
+                    stk[3 * s_top + 1] = bn;
+                    stk[3 * s_top + 2] = dep + 8;
+                    ++s_top;
                 }
             }
-            if (head) carry = i + 1;
+            __syncthreads();
+            if (threadIdx.x == 0) s_diff = 0;
+            __syncthreads();
+            continue;
         }
-        // exclusive max-scan of carries across threads
-        {
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            uint32_t x = carry;
+        const uint32_t b = (uint32_t)(__clzll(df) >> 3);
+        const uint32_t shift = 56 - 8 * b;
+        for (uint32_t x = threadIdx.x; x < NW * 256; x += NT) (&wcnt[0][0])[x] = 0;
+        __syncthreads();
+        // stable ranks: warp w owns the contiguous chunk [w*cs, min((w+1)*cs, bn))
+        const uint32_t cs = ((bn + NW - 1) / NW + 31) & ~31u;
+        const uint32_t ce = min((uint32_t)(w + 1) * cs, bn);
+        for (uint32_t base = (uint32_t)w * cs; base < ce; base += 32) {
+            const uint32_t i = base + lane;
+            const bool v = i < ce;
+            const uint32_t d = v ? digit_of(sk[bs + i], shift) : 0x100u + lane;
+            const uint32_t peers = __match_any_sync(FULL, d);
+            const uint32_t r = __popc(peers & ((1u << lane) - 1u));
+            const uint32_t prev = v ? wcnt[w][d] : 0u;
+            __syncwarp();
+            if (v && lane == __ffs(peers) - 1) wcnt[w][d] = prev + __popc(peers);
+            __syncwarp();
+            if (v) pk[bs + i] = (d << 24) | (prev + r);
+        }
+        __syncthreads();
+        for (uint32_t d = threadIdx.x; d < 256; d += NT) {
+            uint32_t run = 0;
+#pragma unroll
+            for (int ww = 0; ww < NW; ++ww) {
+                const uint32_t v = wcnt[ww][d];
+                wcnt[ww][d] = run;
+                run += v;
+            }
+            hist[d] = run;
+        }
+        __syncthreads();
+        if (w == 0) {  // exclusive scan of the 256 digit totals, 8 per lane
+            uint32_t v[8], sum = 0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                v[t] = hist[lane * 8 + t];
+                sum += v[t];
+            }
+            uint32_t x = sum;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x = max(x, y);
+                const uint32_t y = __shfl_up_sync(FULL, x, o);
+                if (lane >= o) x += y;
             }
-            if (lane == 31) shm[w] = x;
-            if (threadIdx.x == 0) s_unres = 0;
-            __syncthreads();
-            uint32_t inc = 0;
-            for (int k2 = 0; k2 < w; ++k2) inc = max(inc, shm[k2]);
-            uint32_t prev_lane = __shfl_up_sync(0xffffffffu, x, 1);
-            if (lane > 0) inc = max(inc, prev_lane);
-            carry = inc;  // 1 + last head before this thread's range
-        }
-        for (int j = 0; j < IPT; ++j) {
-            uint32_t i = ib + j;
-            if (i >= size) break;
-            bool head = i == 0 || sg[i] != sg[i - 1] || sk[i] != sk[i - 1];
-            if (head) carry = i + 1;
-            rs[i] = carry - 1;
-        }
-        __syncthreads();
-        int unres = 0;
-        for (int j = 0; j < IPT; ++j) {
-            uint32_t i = ib + j;
-            if (i >= size) break;
-            uint32_t r = rs[i];
-            bool multi = (i > 0 && rs[i - 1] == r) || (i + 1 < size && rs[i + 1] == r);
-            if (multi && zero_byte(sk[i]) == 8) {
-                unres = 1;
-                sd[i] += 8;
-                uint32_t o = so[i];
-                sk[i] = key8(S.a.chars, S.a.off[o], S.a.len[o], sd[i]);
+            uint32_t ex = x - sum;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                bstart[lane * 8 + t] = ex;
+                ex += v[t];
             }
         }
         __syncthreads();
-        for (int j = 0; j < IPT; ++j) {
-            uint32_t i = ib + j;
-            if (i >= size) break;
-            sg[i] = rs[i];
+        for (uint32_t i = threadIdx.x; i < bn; i += NT) {
+            const uint32_t x = pk[bs + i];
+            const uint32_t d = x >> 24;
+            const uint32_t dest = bstart[d] + wcnt[i / cs][d] + (x & 0xFFFFFFu);
+            if (dest >= bn) {  // never taken when the counts agree
+                atomicExch(&S.counters[10], 1u);
+                continue;
+            }
+            tk[bs + dest] = sk[bs + i];
+            to[bs + dest] = so[bs + i];
         }
-        if (unres) s_unres = 1;
         __syncthreads();
-        if (!s_unres) break;
+        for (uint32_t i = threadIdx.x; i < bn; i += NT) {
+            sk[bs + i] = tk[bs + i];
+            so[bs + i] = to[bs + i];
+        }
+        for (uint32_t d = threadIdx.x; d < 256; d += NT) {
+            const uint32_t cnt = hist[d];
+            if (!cnt) continue;
+            const uint32_t c0 = bs + bstart[d];
+            if (c0 != bs) lcp[c0] = dep + b;  // boundary to the previous non-empty bucket
+            if (d == 0) {  // strings that end here: byte-identical
+                for (uint32_t k = 1; k < cnt; ++k) lcp[c0 + k] = dep + b;
+            } else if (cnt >= 2) {
+                uint32_t* dst;
+                uint32_t slot;
+                if (cnt <= 32) {
+                    slot = atomicAdd(&s_nw, 1u);
+                    dst = wl + 3 * slot;
+                } else {
+                    slot = atomicAdd(&s_top, 1u);
+                    dst = stk + 3 * slot;
+                }
+                dst[0] = c0;
+                dst[1] = cnt;
+                dst[2] = dep;
+            }
+        }
+        if (threadIdx.x == 0) s_diff = 0;
+        __syncthreads();
     }
+    const uint32_t nwl = s_nw;
+    for (uint32_t e = w; e < nwl; e += NW) {
+        const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1], wd = wl[3 * e + 2];
+        uint64_t key = 0;
+        uint32_t id = 0;
+        if ((uint32_t)lane < wn) {
+            key = sk[ws + lane];
+            id = so[ws + lane];
+        }
+        warp_sort(S.a, wn, wd, key, id, lcp + ws);
+        if ((uint32_t)lane < wn) so[ws + lane] = id;
+    }
+    __syncthreads();
     for (uint32_t i = threadIdx.x; i < size; i += NT) S.ord_out[start + i] = so[i];
 }
 
 template <int CAP, int NT>
-static int launch_small(const SortState& S, const Seg* segs, uint32_t n, cudaStream_t st) {
+static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, const char* name, cudaStream_t st) {
     if (!n) return DSSS_OK;
-    constexpr size_t shm = (size_t)CAP * (8 + 4 * 4);
+    constexpr size_t shm = seg_sort_smem<CAP>();
     static bool configured = false;
     if (!configured) {
-        DSSS_CUDA(cudaFuncSetAttribute(k_small_sort<CAP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        DSSS_CUDA(cudaFuncSetAttribute(k_seg_sort<CAP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         configured = true;
     }
-    DSSS_LAUNCH(CAP == 32 ? "k_small_sort32" : CAP == 256 ? "k_small_sort256" : CAP == 1024 ? "k_small_sort1024" : "k_small_sort4096", st, k_small_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n));
+    DSSS_LAUNCH(name, st, k_seg_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }
@@ -606,6 +863,11 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.cap_tiles = L.cap_tiles;
     S.cap_chunks = L.cap_chunks;
 
+    static bool scatter_configured = false;
+    if (!scatter_configured) {
+        DSSS_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SCATTER_SMEM));
+        scatter_configured = true;
+    }
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb_host, (p + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     DSSS_LAUNCH("k_init_ids", st, k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n));
@@ -636,7 +898,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         DSSS_LAUNCH("k_hist", st, k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_seg_scan", st, k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next));
-        DSSS_LAUNCH("k_scatter", st, k_scatter<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_scatter", st, k_scatter<<<(unsigned)max_tiles, LT_NT, SCATTER_SMEM, st>>>(S, segs, nlarge));
         DSSS_CUDA(cudaGetLastError());
         DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
@@ -647,10 +909,16 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     }
     for (int b = 0; b < NBINS; ++b)
         if (pin[1 + b] > L.cap_small) return fail(DSSS_EDEVICE, "string sort: small-segment list overflow");
-    DSSS_TRY((launch_small<32, 32>(S, S.small[0], pin[1], st)));
-    DSSS_TRY((launch_small<256, 128>(S, S.small[1], pin[2], st)));
-    DSSS_TRY((launch_small<1024, 256>(S, S.small[2], pin[3], st)));
-    DSSS_TRY((launch_small<4096, 512>(S, S.small[3], pin[4], st)));
+    if (pin[1]) {
+        DSSS_LAUNCH("k_warp_segs", st, k_warp_segs<<<(pin[1] + 3) / 4, 128, 0, st>>>(S, S.small[0], pin[1]));
+        DSSS_CUDA(cudaGetLastError());
+    }
+    DSSS_TRY((launch_seg_sort<256, 128>(S, S.small[1], pin[2], "k_seg_sort256", st)));
+    DSSS_TRY((launch_seg_sort<1024, 256>(S, S.small[2], pin[3], "k_seg_sort1024", st)));
+    DSSS_TRY((launch_seg_sort<4096, 256>(S, S.small[3], pin[4], "k_seg_sort4096", st)));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
     return DSSS_OK;
 }
 

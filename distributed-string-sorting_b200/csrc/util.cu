@@ -15,8 +15,10 @@ constexpr uint32_t WARP_AFTER = 64;
 
 __device__ __forceinline__ uint32_t lcp_thread(const ArenaDev& a, uint32_t s, uint32_t t, uint32_t from,
                                                uint32_t limit, bool* done) {
-    const uint64_t os = a.off[s], ot = a.off[t];
-    const uint32_t ls = a.len[s], lt = a.len[t];
+    uint64_t os, ot;
+    uint32_t ls, lt;
+    str_of(a, s, os, ls);
+    str_of(a, t, ot, lt);
     for (uint32_t d = from;; d += 8) {
         if (d >= limit) { *done = false; return d; }
         uint64_t x = key8(a.chars, os, ls, d), y = key8(a.chars, ot, lt, d);
@@ -45,8 +47,10 @@ __global__ void k_adjacent_lcp_warp(ArenaDev a, const uint32_t* order, const uin
     for (uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wid < total; wid += nw) {
         const uint32_t i = longq[wid];
         const uint32_t s = order[i - 1], t = order[i];
-        const uint64_t os = a.off[s], ot = a.off[t];
-        const uint32_t ls = a.len[s], lt = a.len[t];
+        uint64_t os, ot;
+        uint32_t ls, lt;
+        str_of(a, s, os, ls);
+        str_of(a, t, ot, lt);
         for (uint32_t d = WARP_AFTER;; d += 256) {
             uint32_t dd = d + 8 * lane;
             uint64_t x = key8(a.chars, os, ls, dd), y = key8(a.chars, ot, lt, dd);
@@ -70,6 +74,15 @@ int adjacent_lcp(const ArenaDev& a, const uint32_t* order, uint64_t m, uint32_t*
                                                                                                   nlong, lcp));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
+}
+
+__global__ void k_make_handles(ArenaDev a, ulonglong2* h) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n) h[i] = make_ulonglong2(a.off[i], a.len[i]);
+}
+
+void make_handles(const ArenaDev& a, ulonglong2* h, cudaStream_t st) {
+    if (a.n) DSSS_LAUNCH("k_make_handles", st, k_make_handles<<<grid_for(a.n, 256), 256, 0, st>>>(a, h));
 }
 
 // ------------------------------------------------------------ multisplit ----
@@ -141,6 +154,159 @@ __global__ void __launch_bounds__(MS_NT) k_ms_scatter(const uint32_t* bucket, ui
             dest[i] = d < n ? d : 0xFFFFFFFFu;  // out-of-range marks a count mismatch; users check
         }
     }
+}
+
+// Same partition, carrying NPAY u32 payload columns: out_k[dest(i)] = in_k[i]
+// (in_k == NULL carries i itself), rank_out[i] = position of i inside its
+// bucket.  The tile is reordered by bucket in shared memory first, so global
+// writes of each bucket's run are contiguous.
+struct Payload {
+    const uint32_t* in[3];
+    uint32_t* out[3];
+};
+
+template <int NPAY>
+constexpr size_t msp_smem(uint32_t P) {
+    return (size_t)MS_TILE * (4 * NPAY + 2) + (size_t)P * 4 * (3 + MS_NT / 32);
+}
+
+template <int NPAY>
+__global__ void __launch_bounds__(MS_NT) k_ms_scatter_pay(const uint32_t* bucket, uint64_t n, uint32_t P,
+                                                         uint64_t tiles, const uint32_t* off, Payload pl,
+                                                         uint32_t* rank_out, uint32_t* err) {
+    extern __shared__ __align__(16) uint32_t smp[];
+    uint32_t* spay = smp;                                   // NPAY x MS_TILE
+    uint16_t* sbk = (uint16_t*)(smp + NPAY * MS_TILE);      // MS_TILE
+    uint32_t* base = (uint32_t*)(sbk + MS_TILE);            // P
+    uint32_t* b0 = base + P;                                 // P
+    uint32_t* tloff = b0 + P;                                // P
+    uint32_t* wcnt = tloff + P;                              // (MS_NT/32) x P
+    __shared__ uint32_t wsum[MS_NT / 32];
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) {
+        base[b] = off[(uint64_t)b * tiles + blockIdx.x];
+        b0[b] = off[(uint64_t)b * tiles];
+#pragma unroll
+        for (int w = 0; w < MS_NT / 32; ++w) wcnt[w * P + b] = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t tb = (uint64_t)blockIdx.x * MS_TILE;
+    const uint32_t tn = (uint32_t)min((uint64_t)MS_TILE, n - tb);
+    const uint64_t wb = tb + (uint64_t)w * 32 * MS_IPT;
+    uint32_t rk[MS_IPT], bk[MS_IPT];
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        const uint64_t i = wb + j * 32 + lane;
+        const uint32_t d = i < n ? bucket[i] : 0xFFFFFFFFu - lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t r = __popc(peers & ((1u << lane) - 1));
+        const uint32_t prev = i < n ? wcnt[w * P + d] : 0;
+        __syncwarp();
+        if (i < n && lane == __ffs(peers) - 1) wcnt[w * P + d] = prev + __popc(peers);
+        __syncwarp();
+        rk[j] = prev + r;
+        bk[j] = d;
+    }
+    __syncthreads();
+    // exclusive over warps per bucket, then over buckets within the tile
+    // (each thread a contiguous run of buckets, block scan of the run sums)
+    const uint32_t per = (P + MS_NT - 1) / MS_NT;
+    const uint32_t c0 = min(P, threadIdx.x * per), c1 = min(P, c0 + per);
+    uint32_t sum = 0;
+    for (uint32_t b = c0; b < c1; ++b) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int ww = 0; ww < MS_NT / 32; ++ww) {
+            const uint32_t v = wcnt[ww * P + b];
+            wcnt[ww * P + b] = run;
+            run += v;
+        }
+        tloff[b] = run;
+        sum += run;
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t run = x - sum;
+    for (int ww = 0; ww < w; ++ww) run += wsum[ww];
+    for (uint32_t b = c0; b < c1; ++b) {
+        const uint32_t v = tloff[b];
+        tloff[b] = run;
+        run += v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        const uint64_t i = wb + j * 32 + lane;
+        if (i >= n) continue;
+        const uint32_t d = bk[j];
+        const uint32_t lp = tloff[d] + wcnt[w * P + d] + rk[j];
+        if (lp >= tn) {  // never taken when the counts agree
+            atomicExch(err, 1u);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < NPAY; ++k) spay[k * MS_TILE + lp] = pl.in[k] ? pl.in[k][i] : (uint32_t)i;
+        sbk[lp] = (uint16_t)d;
+        if (rank_out) rank_out[i] = base[d] + wcnt[w * P + d] + rk[j] - b0[d];
+    }
+    __syncthreads();
+    for (uint32_t xx = threadIdx.x; xx < tn; xx += MS_NT) {
+        const uint32_t d = sbk[xx];
+        const uint64_t dest = (uint64_t)base[d] + (xx - tloff[d]);
+        if (dest >= n) {
+            atomicExch(err, 1u);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < NPAY; ++k) pl.out[k][dest] = spay[k * MS_TILE + xx];
+    }
+}
+
+template <int NPAY>
+static int launch_ms_pay(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles, const uint32_t* off,
+                         const Payload& pl, uint32_t* rank_out, uint32_t* err, cudaStream_t st) {
+    static uint32_t configured_p = 0;
+    const size_t sm = msp_smem<NPAY>(P);
+    if (configured_p < P) {
+        DSSS_CUDA(cudaFuncSetAttribute(k_ms_scatter_pay<NPAY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)msp_smem<NPAY>(MAX_SPLIT_BUCKETS)));
+        configured_p = MAX_SPLIT_BUCKETS;
+    }
+    DSSS_LAUNCH("k_ms_scatter_pay", st,
+                k_ms_scatter_pay<NPAY><<<(unsigned)tiles, MS_NT, sm, st>>>(bucket, n, P, tiles, off, pl, rank_out, err));
+    return DSSS_OK;
+}
+
+int multisplit_payload(const uint32_t* bucket, uint64_t n, uint32_t P, int npay, const uint32_t* const* in,
+                       uint32_t* const* out, uint32_t* rank_out, uint32_t* err, void* scratch, cudaStream_t st) {
+    if (n == 0) return DSSS_OK;
+    if (P == 0 || P > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "multisplit supports 1..%u buckets", MAX_SPLIT_BUCKETS);
+    if (npay < 1 || npay > 3) return fail(DSSS_EINVAL, "multisplit: 1 to 3 payload columns");
+    const uint64_t tiles = (n + MS_TILE - 1) / MS_TILE;
+    const uint64_t cells = tiles * P;
+    if (cells >= (1ull << 32)) return fail(DSSS_ENOTSUP, "multisplit: too many tiles x buckets");
+    Carve c(scratch);
+    uint32_t* hist = c.take<uint32_t>(cells);
+    uint32_t* off = c.take<uint32_t>(cells);
+    void* sc = c.take<unsigned char>(scan_scratch_bytes(cells));
+    Payload pl;
+    for (int k = 0; k < 3; ++k) {
+        pl.in[k] = k < npay ? in[k] : nullptr;
+        pl.out[k] = k < npay ? out[k] : nullptr;
+    }
+    DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, P * sizeof(uint32_t), st>>>(bucket, n, P, tiles, hist));
+    DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
+    if (npay == 1) DSSS_TRY(launch_ms_pay<1>(bucket, n, P, tiles, off, pl, rank_out, err, st));
+    else if (npay == 2) DSSS_TRY(launch_ms_pay<2>(bucket, n, P, tiles, off, pl, rank_out, err, st));
+    else DSSS_TRY(launch_ms_pay<3>(bucket, n, P, tiles, off, pl, rank_out, err, st));
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
 }
 
 uint64_t multisplit_scratch_bytes(uint64_t n, uint32_t P) {
