@@ -67,6 +67,10 @@ _SIGS = {
     "dsss_local_sort_lcp": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), _P, _P, _P]),
     "dsss_dp_prefixes": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "dsss_prefix_hash": (_I, [ctypes.POINTER(Arena), _P, _U64, _U32, _P, _P]),
+    "dsss_dp_round": (_I, [_P, ctypes.POINTER(Arena), _P, _P, _P, _U64, _U32, _P, _P, _P, _P]),
+    "dsss_bucket_scatter": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _P, _U64, _P, _P, _P, _P, _P,
+                                 _P, _P, _P, _P]),
+    "dsss_lcp_merge": (_I, [_P, _P, _U64, _P, _P, _U64, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dsss_partition": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, ctypes.POINTER(Opts), _P, _P]),
     "dsss_adjacent_lcp": (_I, [_P, ctypes.POINTER(Arena), _P, _U64, _P, _P]),
     "dsss_adjacent_lcp_noalloc": (_I, [ctypes.POINTER(Arena), _P, _U64, _P, _P]),
@@ -348,6 +352,52 @@ def dp_prefixes(ctx: Context, ds: DeviceStrings, order, lcp, p: int = 1, part_be
     check(lib().dsss_dp_prefixes(ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), _ptr(order), _ptr(lcp), _ptr(dp),
                                  _ptr(counts), max_rounds, ctypes.byref(rounds), _stream_ptr(stream)))
     return dp[:n], counts[:rounds.value]
+
+
+def dp_round(ctx: Context, ds: DeviceStrings, order, lcp, candidates, depth: int, results, stream=None):
+    """One BloomFilter::filter round (dsss_dp_round): returns (next positions, count)."""
+    n = ds.n
+    nxt = _empty(n)
+    m = 0 if candidates is None else int(candidates.shape[0])
+    mn = np.zeros(1, dtype=np.uint64)
+    check(lib().dsss_dp_round(ctx.h, ctypes.byref(ds.arena()), _ptr(order), _ptr(lcp), _ptr(candidates), m, depth,
+                              _ptr(results), _ptr(nxt), _ptr(mn), _stream_ptr(stream)))
+    return nxt[:int(mn[0])], int(mn[0])
+
+
+def bucket_scatter(ctx: Context, ds: DeviceStrings, p: int, local_order, lcp, dp, intervals, part_begin=None,
+                   stream=None):
+    """dsss_bucket_scatter: every PE's receive container, back to back."""
+    import torch
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    iv = np.ascontiguousarray(np.asarray(intervals, dtype=np.uint64).ravel())
+    total = np.zeros(1, np.uint64)
+    cbeg = np.zeros(p + 1, np.uint64)
+    counts = np.zeros(p * p, np.uint64)
+    offs = np.zeros(p * p, np.uint64)
+    cstart, rl, ri, rp = _empty(n), _empty(n), _empty(n), _empty(n)
+    args = [ctx.h, ctypes.byref(ds.arena()), p, _ptr(pb), _ptr(local_order), _ptr(lcp), _ptr(dp), _ptr(iv)]
+    check(lib().dsss_bucket_scatter(*args, None, 0, _ptr(total), _ptr(cbeg), None, _ptr(rl), _ptr(ri), _ptr(rp),
+                                    _ptr(counts), _ptr(offs), _stream_ptr(stream)))
+    chars = torch.zeros(int(total[0]) + PAD, dtype=torch.uint8, device=ds.chars.device)
+    check(lib().dsss_bucket_scatter(*args, _ptr(chars), int(total[0]) + PAD, _ptr(total), _ptr(cbeg), _ptr(cstart),
+                                    _ptr(rl), _ptr(ri), _ptr(rp), _ptr(counts), _ptr(offs), _stream_ptr(stream)))
+    return dict(chars=chars, char_total=int(total[0]), char_begin=cbeg, char_start=cstart[:n], lcp=rl[:n],
+                index=ri[:n], pe=rp[:n], counts=counts.reshape(p, p), offsets=offs.reshape(p, p))
+
+
+def lcp_merge(ctx: Context, chars, char_bytes: int, lcp, counts, offsets=None, char_start=None, stream=None):
+    """dsss_lcp_merge over nrecv x p source runs (counts/offsets shaped (nrecv, p))."""
+    counts = np.ascontiguousarray(np.asarray(counts, dtype=np.uint64))
+    nrecv, p = counts.shape
+    offs = None if offsets is None else np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+    n = int(lcp.shape[0])
+    out = dict(order=_empty(n), merged_lcp=_empty(n), old_lcp=_empty(n), perm_index=_empty(n), perm_pe=_empty(n))
+    check(lib().dsss_lcp_merge(ctx.h, _ptr(chars), char_bytes, _ptr(char_start), _ptr(lcp), n, nrecv, p, _ptr(counts),
+                               _ptr(offs), _ptr(out["order"]), _ptr(out["merged_lcp"]), _ptr(out["old_lcp"]),
+                               _ptr(out["perm_index"]), _ptr(out["perm_pe"]), _stream_ptr(stream)))
+    return {k: v[:n] for k, v in out.items()}
 
 
 def prefix_hash(ds: DeviceStrings, ids, depth: int, stream=None):

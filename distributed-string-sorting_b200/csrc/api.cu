@@ -18,7 +18,9 @@
 #include <vector>
 
 #include "dp.cuh"
+#include "exchange.cuh"
 #include "internal.cuh"
+#include "merge.cuh"
 #include "partition.cuh"
 #include "strsort.cuh"
 #include "util.cuh"
@@ -291,6 +293,71 @@ int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint
     // string is an LCP duplicate of the previous PE's last one.
     return dp_rounds(L, a, in->n, order, lcp, dp, round_counts, max_rounds, rounds, (uint32_t*)ctx->pin,
                      (cudaStream_t)stream);
+}
+
+int dsss_dp_round(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, const uint32_t* lcp,
+                  const uint32_t* candidates, uint64_t m, uint32_t depth, uint32_t* results, uint32_t* next,
+                  uint64_t* m_next, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    DSSS_TRY(check_arena(in));
+    if (!m_next) return fail(DSSS_EINVAL, "m_next is NULL");
+    if (in->n && (!order || !lcp || !results || !next)) return fail(DSSS_EINVAL, "order/lcp/results/next is NULL");
+    if (candidates && m > in->n) return fail(DSSS_EINVAL, "more candidates than strings");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    Carve sz(nullptr);
+    DpRoundLayout R;
+    layout_dp_round(sz, R, in->n);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_dp_round(c, R, in->n);
+    return dp_one_round(R, view(in), in->n, order, lcp, candidates, m, depth, results, next, m_next,
+                        (uint32_t*)ctx->pin, (cudaStream_t)stream);
+}
+
+int dsss_bucket_scatter(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                        const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, const uint64_t* intervals,
+                        uint8_t* recv_chars, uint64_t recv_capacity, uint64_t* char_total, uint64_t* recv_char_begin,
+                        uint32_t* recv_char_start, uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe,
+                        uint64_t* recv_counts, uint64_t* recv_offsets, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    DSSS_TRY(check_arena(in));
+    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (!intervals || !char_total) return fail(DSSS_EINVAL, "intervals/char_total is NULL");
+    if (in->n && (!local_order || !lcp || !dp || !recv_lcp || !recv_index || !recv_pe))
+        return fail(DSSS_EINVAL, "input or per-string output array is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    Carve sz(nullptr);
+    ExchangeLayout L;
+    layout_exchange(sz, L, in->n, p);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_exchange(c, L, in->n, p);
+    DSSS_TRY(bucket_scatter(L, view(in), p, part_begin, local_order, lcp, dp, intervals, char_total, recv_chars,
+                            recv_capacity, recv_char_begin, recv_lcp, recv_index, recv_pe, recv_counts, recv_offsets,
+                            (uint32_t*)ctx->pin, st));
+    if (recv_char_start && in->n)
+        DSSS_CUDA(cudaMemcpyAsync(recv_char_start, L.cstart, in->n * 4, cudaMemcpyDeviceToDevice, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    return DSSS_OK;
+}
+
+int dsss_lcp_merge(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes, const uint32_t* recv_char_start,
+                   const uint32_t* recv_lcp, uint64_t n, uint32_t nrecv, uint32_t p, const uint64_t* recv_counts,
+                   const uint64_t* recv_offsets, uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp,
+                   uint32_t* perm_index, uint32_t* perm_pe, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    if (nrecv == 0 || p == 0 || !recv_counts) return fail(DSSS_EINVAL, "nrecv/p/recv_counts missing");
+    if (n && (!recv_chars || !recv_lcp || !order)) return fail(DSSS_EINVAL, "recv_chars/recv_lcp/order is NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    int rc = lcp_merge(ctx, recv_chars, char_bytes, recv_char_start, recv_lcp, n, nrecv, p, recv_counts, recv_offsets,
+                       order, merged_lcp, old_lcp, perm_index, perm_pe, (cudaStream_t)stream);
+    return rc;
 }
 
 int dsss_prefix_hash(const dsss_arena* in, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* hash,

@@ -178,7 +178,96 @@ __global__ void scan_tiles(const uint32_t* in, uint32_t* out, uint64_t n, const 
     }
 }
 
-uint64_t scan_scratch_bytes(uint64_t n) { return ((n + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(uint32_t); }
+uint64_t scan_scratch_bytes(uint64_t n) { return ((n + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(uint64_t); }
+
+// 64-bit variant (values summed in u64).
+__device__ __forceinline__ uint64_t block_excl_scan64(uint64_t v, uint64_t* sh, uint64_t* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint64_t s = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) sh[lane] = s;
+    }
+    __syncthreads();
+    uint64_t base = w ? sh[w - 1] : 0;
+    if (total) *total = sh[nw - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+__global__ void scan64_tile_sums(const uint32_t* in, uint64_t n, uint64_t* sums) {
+    __shared__ uint64_t sh[32];
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint64_t s = 0;
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + (uint64_t)k * SCAN_NT + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint64_t tot;
+    block_excl_scan64(s, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void scan64_sums(uint64_t* sums, uint64_t m, uint64_t* total) {
+    __shared__ uint64_t sh[32];
+    uint64_t carry = 0;
+    for (uint64_t b = 0; b < m; b += SCAN_NT) {
+        uint64_t i = b + threadIdx.x;
+        uint64_t v = i < m ? sums[i] : 0;
+        uint64_t tot;
+        uint64_t ex = block_excl_scan64(v, sh, &tot);
+        if (i < m) sums[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void scan64_tiles(const uint32_t* in, uint64_t* out, uint64_t n, const uint64_t* sums) {
+    __shared__ uint64_t sh[32];
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_IPT;
+    uint32_t v[SCAN_IPT];
+    uint64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        s += v[k];
+    }
+    uint64_t ex = block_excl_scan64(s, sh, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; ++k) {
+        uint64_t i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+}
+
+int exclusive_scan_u32_to_u64(const uint32_t* in, uint64_t* out, uint64_t n, uint64_t* total, void* scratch,
+                              cudaStream_t st) {
+    uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    uint64_t* sums = (uint64_t*)scratch;
+    if (n == 0) {
+        if (total) DSSS_CUDA(cudaMemsetAsync(total, 0, sizeof(uint64_t), st));
+        return DSSS_OK;
+    }
+    DSSS_LAUNCH("scan64_tile_sums", st, scan64_tile_sums<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, n, sums));
+    DSSS_LAUNCH("scan64_sums", st, scan64_sums<<<1, SCAN_NT, 0, st>>>(sums, tiles, total));
+    DSSS_LAUNCH("scan64_tiles", st, scan64_tiles<<<(unsigned)tiles, SCAN_NT, 0, st>>>(in, out, n, sums));
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
 
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total, void* scratch,
                        cudaStream_t st) {

@@ -197,6 +197,78 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
     return DSSS_OK;
 }
 
+__global__ void k_cand_to_state(const uint32_t* cand, uint64_t m, uint64_t n, uint8_t* st, uint32_t* err) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint32_t i = cand[j];
+    if (i >= n || (j > 0 && cand[j - 1] >= i)) {  // positions must be ascending and in range
+        atomicExch(err, 1u);
+        return;
+    }
+    st[i] = 1;
+}
+
+__global__ void k_state_flags(const uint8_t* st, uint64_t n, uint32_t* flag) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = st[i];
+}
+
+__global__ void k_state_compact(const uint32_t* flag, const uint32_t* pos, uint64_t n, uint32_t* out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && flag[i]) out[pos[i]] = (uint32_t)i;
+}
+
+void layout_dp_round(Carve& c, DpRoundLayout& R, uint64_t n) {
+    layout_dp(c, R.dp, n);
+    const uint64_t N = n ? n : 1;
+    R.flag = c.take<uint32_t>(N);
+    R.pos = c.take<uint32_t>(N);
+    R.total = c.take<uint32_t>(2);
+    R.scan = c.take<unsigned char>(scan_scratch_bytes(N));
+}
+
+int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
+                 const uint32_t* cand, uint64_t m, uint32_t depth, uint32_t* dp, uint32_t* next, uint64_t* m_next,
+                 uint32_t* pin, cudaStream_t st) {
+    const DpLayout& L = R.dp;
+    *m_next = 0;
+    if (n == 0) return DSSS_OK;
+    const unsigned grid = grid_for(n, 256);
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens));
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
+    const bool all = cand == nullptr;
+    if (!all) {
+        DSSS_CUDA(cudaMemsetAsync(L.st[0], 0, n, st));
+        if (m) DSSS_LAUNCH("k_cand_to_state", st,
+                           k_cand_to_state<<<grid_for(m, 256), 256, 0, st>>>(cand, m, n, L.st[0], L.counters + 3));
+    }
+    DSSS_LAUNCH("k_dp_classify", st,
+                k_dp_classify<<<grid, 256, 0, st>>>(L.st[0], all, L.lens, lcp, n, depth, dp, L.st[1], L.kind,
+                                                   L.counters));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[3]) return fail(DSSS_EINVAL, "candidates must be ascending positions below n");
+    if (pin[0]) {
+        const uint64_t slots = table_slots(pin[0]);
+        DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+        DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
+        DSSS_LAUNCH("k_dp_hash", st,
+                    k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
+                                                   L.slot, L.counters + 2));
+        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
+    }
+    DSSS_LAUNCH("k_state_flags", st, k_state_flags<<<grid, 256, 0, st>>>(L.st[1], n, R.flag));
+    DSSS_TRY(exclusive_scan_u32(R.flag, R.pos, n, R.total, R.scan, st));
+    DSSS_LAUNCH("k_state_compact", st, k_state_compact<<<grid, 256, 0, st>>>(R.flag, R.pos, n, next));
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaMemcpyAsync(pin + 4, R.total, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table overflow");
+    *m_next = pin[4];
+    return DSSS_OK;
+}
+
 int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out,
                 cudaStream_t st) {
     if (m == 0) return DSSS_OK;

@@ -23,6 +23,23 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
               cudaStream_t st);
 
+struct DpRoundLayout {
+    DpLayout dp;
+    uint32_t* flag;
+    uint32_t* pos;
+    uint32_t* total;
+    unsigned char* scan;
+};
+
+void layout_dp_round(Carve& c, DpRoundLayout& R, uint64_t n);
+
+// One BloomFilter::filter round: cand (ascending sorted positions, or NULL for
+// every position, the first round) at depth; dp[c] written for each
+// candidate; next receives the surviving positions, *m_next their count.
+int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
+                 const uint32_t* cand, uint64_t m, uint32_t depth, uint32_t* dp, uint32_t* next, uint64_t* m_next,
+                 uint32_t* pin, cudaStream_t st);
+
 int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out,
                 cudaStream_t st);
 

@@ -310,6 +310,9 @@ __device__ __forceinline__ uint64_t filter_hash(uint64_t h) { return h == ~0ull 
 uint64_t scan_scratch_bytes(uint64_t n);
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total, void* scratch,
                        cudaStream_t st);
+// Exclusive scan of u32 values into u64 sums (same scratch size).
+int exclusive_scan_u32_to_u64(const uint32_t* in, uint64_t* out, uint64_t n, uint64_t* total, void* scratch,
+                              cudaStream_t st);
 
 inline unsigned grid_for(uint64_t n, unsigned block) {
     uint64_t g = (n + block - 1) / block;

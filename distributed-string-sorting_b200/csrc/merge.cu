@@ -1,0 +1,457 @@
+// K7 — merge of receive containers: choose_merge / LcpStringLoserTree_
+// (src/sorter/distributed/merging.hpp:66-123, src/merge/bingmann-lcp_losertree.hpp:203-480)
+// on strings delivered prefix-compressed by the PD exchange (each string holds
+// bytes [lcp, dp) of its DP prefix; lcp is relative to the previous string of
+// the same source run, 0 at run starts).
+//
+//   1. string starts: from the NUL layout when the caller has no start table;
+//   2. prefix decompression (the role of StringLcpContainer::extendPrefix,
+//      strings/stringcontainer.hpp:248-333): bytes [0, lcp) of string o are
+//      bytes of the nearest earlier string with a smaller LCP, found in
+//      O(log n) on a min-tree over the LCP array, recursively;
+//   3. merge rounds: runs are merged pairwise (log2 of the run count rounds)
+//      with merge-path partitioning (each thread finds its diagonal split by
+//      binary search, then merges 8 outputs serially); the serial merge keeps
+//      the LCP of both run heads with the last output, so characters are only
+//      compared when those LCPs are equal, and then only from that depth on.
+// Byte-identical strings keep run order (lower source PE first).
+#include <algorithm>
+#include <vector>
+
+#include "internal.cuh"
+#include "merge.cuh"
+
+namespace dsss {
+
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+constexpr int MG_NT = 256, MG_VT = 8, MG_TILE = MG_NT * MG_VT;
+
+__global__ void k_start_flags(const uint8_t* chars, uint64_t bytes, uint32_t* flag) {
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < bytes) flag[b] = (b == 0 || chars[b - 1] == 0) ? 1u : 0u;
+}
+
+__global__ void k_start_compact(const uint32_t* flag, const uint32_t* pos, uint64_t bytes, uint64_t n,
+                                uint32_t* start, uint32_t* err) {
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bytes || !flag[b]) return;
+    if (pos[b] >= n) {
+        atomicExch(err, 1u);
+        return;
+    }
+    start[pos[b]] = (uint32_t)b;
+}
+
+__global__ void k_full_len(const uint32_t* start, const uint32_t* lcp, uint64_t n, uint64_t bytes, uint32_t* flen,
+                           uint32_t* err) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const uint64_t b = start[o];
+    const uint64_t e = o + 1 < n ? start[o + 1] : bytes;
+    if (b >= bytes || e <= b || e > bytes) {  // starts must increase inside the buffer
+        atomicExch(err, 1u);
+        flen[o] = lcp[o];
+        return;
+    }
+    flen[o] = lcp[o] + (uint32_t)(e - b - 1);
+}
+
+__global__ void k_min_level(const uint32_t* prev, uint64_t nprev, uint32_t* cur, uint64_t ncur) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncur) return;
+    const uint32_t a = prev[2 * i];
+    const uint32_t b = 2 * i + 1 < nprev ? prev[2 * i + 1] : NONE32;
+    cur[i] = min(a, b);
+}
+
+struct MinTree {
+    const uint32_t* lv[40];
+    uint64_t sz[40];
+    int levels;
+};
+
+// Nearest j < o with lcp[j] < v, or NONE32.
+__device__ uint32_t prev_smaller(const MinTree& t, uint64_t o, uint32_t v) {
+    uint64_t i = o;
+    for (int l = 0; l < t.levels; ++l) {
+        if ((i & 1) && t.lv[l][i - 1] < v) {
+            uint64_t k = i - 1;
+            for (int m = l; m > 0; --m) {
+                const uint64_t r = 2 * k + 1;
+                k = (r < t.sz[m - 1] && t.lv[m - 1][r] < v) ? r : 2 * k;
+            }
+            return (uint32_t)k;
+        }
+        i >>= 1;
+    }
+    return NONE32;
+}
+
+__global__ void k_extend(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, MinTree tree, uint64_t n,
+                         const uint64_t* foff, const uint32_t* flen, uint8_t* full, uint32_t* err) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    uint8_t* dst = full + foff[o];
+    const uint32_t l0 = lcp[o];
+    if (flen[o] < l0) {
+        atomicExch(err, 1u);
+        return;
+    }
+    const uint32_t own = flen[o] - l0;
+    const uint8_t* src = chars + start[o];
+    for (uint32_t k = 0; k < own; ++k) dst[l0 + k] = src[k];
+    uint32_t need = l0;
+    uint64_t cur = o;
+    while (need > 0) {
+        const uint32_t j = prev_smaller(tree, cur, need);
+        if (j == NONE32) {  // a run must start with LCP 0
+            atomicExch(err, 1u);
+            return;
+        }
+        const uint32_t lj = lcp[j];
+        if (need - lj > flen[j] - lj) {  // the LCP claims more bytes than string j holds
+            atomicExch(err, 1u);
+            return;
+        }
+        const uint8_t* sj = chars + start[j];
+        for (uint32_t x = lj; x < need; ++x) dst[x] = sj[x - lj];
+        need = lj;
+        cur = j;
+    }
+}
+
+// ------------------------------------------------------------------ merge ----
+struct MergeJob {
+    uint32_t a_beg, a_len, b_beg, b_len, out_beg, tile0;
+};
+
+struct FullView {
+    const uint8_t* full;
+    const uint64_t* foff;
+    const uint32_t* flen;
+};
+
+// Compares strings x and y from depth h (their first h bytes are equal):
+// returns <0, 0, >0 and the LCP through *l.
+__device__ __forceinline__ int cmp_from(const FullView& f, uint32_t x, uint32_t y, uint32_t h, uint32_t* l) {
+    const uint64_t ox = f.foff[x], oy = f.foff[y];
+    const uint32_t lx = f.flen[x], ly = f.flen[y];
+    for (uint32_t d = h;; d += 8) {
+        const uint64_t a = key8(f.full, ox, lx, d), b = key8(f.full, oy, ly, d);
+        if (a != b) {
+            *l = d + key_lcp(a, b);
+            return a < b ? -1 : 1;
+        }
+        const uint32_t z = zero_byte(a);
+        if (z < 8) {
+            *l = d + z;
+            return 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MG_NT) k_merge_round(FullView f, const MergeJob* jobs, uint32_t njobs,
+                                                       const uint32_t* ids_in, const uint32_t* lcp_in,
+                                                       uint32_t* ids_out, uint32_t* lcp_out) {
+    __shared__ uint32_t s_job;
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = njobs;  // last job with tile0 <= blockIdx.x
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (jobs[mid].tile0 <= blockIdx.x) lo = mid;
+            else hi = mid;
+        }
+        s_job = lo;
+    }
+    __syncthreads();
+    const MergeJob J = jobs[s_job];
+    const uint32_t total = J.a_len + J.b_len;
+    const uint32_t diag = (blockIdx.x - J.tile0) * MG_TILE + threadIdx.x * MG_VT;
+    if (diag >= total) return;
+    const uint32_t* A = ids_in + J.a_beg;
+    const uint32_t* B = ids_in + J.b_beg;
+    const uint32_t* LA = lcp_in + J.a_beg;
+    const uint32_t* LB = lcp_in + J.b_beg;
+    // merge path: i = number of A elements among the first diag outputs (A first on ties)
+    uint32_t lo = diag > J.b_len ? diag - J.b_len : 0, hi = min(diag, J.a_len);
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        uint32_t l;
+        if (cmp_from(f, A[mid], B[diag - 1 - mid], 0, &l) <= 0) lo = mid + 1;
+        else hi = mid;
+    }
+    uint32_t i = lo, j = diag - lo;
+    // LCPs of both heads with the last output before this thread's range
+    uint32_t ha = 0, hb = 0;
+    if (diag > 0) {
+        bool last_a;
+        if (j == 0) last_a = true;
+        else if (i == 0) last_a = false;
+        else {
+            uint32_t l;
+            last_a = cmp_from(f, A[i - 1], B[j - 1], 0, &l) > 0;
+        }
+        const uint32_t last = last_a ? A[i - 1] : B[j - 1];
+        uint32_t l;
+        if (i < J.a_len) {
+            if (last_a) ha = LA[i];
+            else {
+                cmp_from(f, A[i], last, 0, &l);
+                ha = l;
+            }
+        }
+        if (j < J.b_len) {
+            if (!last_a) hb = LB[j];
+            else {
+                cmp_from(f, B[j], last, 0, &l);
+                hb = l;
+            }
+        }
+    }
+    uint32_t* out_id = ids_out + J.out_beg;
+    uint32_t* out_l = lcp_out + J.out_beg;
+    for (uint32_t k = 0; k < MG_VT && diag + k < total; ++k) {
+        bool take_a;
+        uint32_t h;
+        if (i >= J.a_len) {
+            take_a = false;
+            h = hb;
+        } else if (j >= J.b_len) {
+            take_a = true;
+            h = ha;
+        } else if (ha > hb) {
+            take_a = true;
+            h = ha;
+        } else if (hb > ha) {
+            take_a = false;
+            h = hb;
+        } else {
+            uint32_t l;
+            h = ha;
+            take_a = cmp_from(f, A[i], B[j], h, &l) <= 0;
+            if (take_a) hb = l;
+            else ha = l;
+        }
+        if (take_a) {
+            out_id[diag + k] = A[i];
+            out_l[diag + k] = h;
+            ++i;
+            ha = i < J.a_len ? LA[i] : 0;
+        } else {
+            out_id[diag + k] = B[j];
+            out_l[diag + k] = h;
+            ++j;
+            hb = j < J.b_len ? LB[j] : 0;
+        }
+    }
+}
+
+__global__ void k_merge_init(const uint32_t* lcp, const uint8_t* run_start, uint64_t n, uint32_t* ids, uint32_t* l) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    ids[o] = (uint32_t)o;
+    l[o] = run_start[o] ? 0u : lcp[o];
+}
+
+__global__ void k_merge_tags(const uint32_t* ids, const uint32_t* lcp_orig, const uint8_t* run_start,
+                             const uint32_t* run_of, const uint32_t* run_begin, const uint64_t* run_offset,
+                             uint32_t runs_per_recv, uint64_t n, uint32_t* old_lcp, uint32_t* perm_index,
+                             uint32_t* perm_pe) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const uint32_t e = ids[o];
+    if (old_lcp) old_lcp[o] = run_start[e] ? 0u : lcp_orig[e];
+    const uint32_t r = run_of[e];
+    if (perm_index) perm_index[o] = (uint32_t)(run_offset[r] + (e - run_begin[r]));
+    if (perm_pe) perm_pe[o] = r % runs_per_recv;
+}
+
+__global__ void k_run_marks(const uint32_t* run_begin, const uint32_t* run_len, uint32_t nruns, uint8_t* run_start,
+                            uint32_t* run_of) {
+    const uint32_t r = blockIdx.x;
+    if (r >= nruns) return;
+    for (uint32_t k = threadIdx.x; k < run_len[r]; k += blockDim.x) {
+        run_start[run_begin[r] + k] = k == 0 ? 1 : 0;
+        run_of[run_begin[r] + k] = r;
+    }
+}
+
+static int tree_levels(uint64_t n) {
+    int l = 1;
+    while ((n >> (l - 1)) > 1) ++l;
+    return l;
+}
+
+void layout_merge(Carve& c, MergeLayout& L, uint64_t n, uint64_t bytes, uint64_t full_bytes, uint32_t nruns) {
+    const uint64_t N = n ? n : 1;
+    L.start = c.take<uint32_t>(N);
+    L.flag = c.take<uint32_t>(bytes ? bytes : 1);
+    L.pos = c.take<uint32_t>(bytes ? bytes : 1);
+    L.flen = c.take<uint32_t>(N);
+    L.foff = c.take<uint64_t>(N);
+    L.tree = c.take<uint32_t>(2 * N + 64);
+    L.ids[0] = c.take<uint32_t>(N);
+    L.ids[1] = c.take<uint32_t>(N);
+    L.l[0] = c.take<uint32_t>(N);
+    L.l[1] = c.take<uint32_t>(N);
+    L.run_start = c.take<uint8_t>(N);
+    L.run_of = c.take<uint32_t>(N);
+    L.run_begin = c.take<uint32_t>(nruns + 1);
+    L.run_len = c.take<uint32_t>(nruns + 1);
+    L.run_offset = c.take<uint64_t>(nruns + 1);
+    L.jobs = c.take<MergeJob>(nruns + 1);
+    L.counters = c.take<uint32_t>(4);
+    L.total64 = c.take<uint64_t>(1);
+    L.scan = c.take<unsigned char>(scan_scratch_bytes(bytes > N ? bytes : N));
+    // Last: the second carve (once the decompressed size is known) must not
+    // move any array the first one handed out.
+    L.full = c.take<uint8_t>(full_bytes + 64);
+}
+
+int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* char_start, const uint32_t* lcp,
+              uint64_t n, uint32_t nrecv, uint32_t p, const uint64_t* counts, const uint64_t* offsets,
+              uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp, uint32_t* perm_index, uint32_t* perm_pe,
+              cudaStream_t st) {
+    if (n == 0) return DSSS_OK;
+    if (bytes >= (1ull << 32)) return fail(DSSS_ENOTSUP, "receive containers over 4 GiB per call");
+    const uint32_t nruns = nrecv * p;
+    uint64_t sum = 0;
+    for (uint32_t r = 0; r < nruns; ++r) sum += counts[r];
+    if (sum != n) return fail(DSSS_EINVAL, "recv_counts add up to %llu, not n = %llu", (unsigned long long)sum,
+                              (unsigned long long)n);
+    // sizes: decompressed bytes are known only after the lengths are summed,
+    // so lay out with a first pass that reserves them last.
+    Carve sz(nullptr);
+    MergeLayout L;
+    layout_merge(sz, L, n, bytes, 0, nruns);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c0(ctx->ws);
+    layout_merge(c0, L, n, bytes, 0, nruns);
+    uint32_t* pin = (uint32_t*)ctx->pin;
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 4 * sizeof(uint32_t), st));
+    const uint32_t* start = char_start;
+    if (!start) {
+        DSSS_LAUNCH("k_start_flags", st, k_start_flags<<<grid_for(bytes, 256), 256, 0, st>>>(chars, bytes, L.flag));
+        DSSS_TRY(exclusive_scan_u32(L.flag, L.pos, bytes, L.counters + 1, L.scan, st));
+        DSSS_LAUNCH("k_start_compact", st,
+                    k_start_compact<<<grid_for(bytes, 256), 256, 0, st>>>(L.flag, L.pos, bytes, n, L.start,
+                                                                         L.counters));
+        start = L.start;
+    }
+    // runs
+    std::vector<uint32_t> rb(nruns), rl(nruns);
+    std::vector<uint64_t> ro(nruns);
+    {
+        uint64_t b = 0;
+        for (uint32_t r = 0; r < nruns; ++r) {
+            rb[r] = (uint32_t)b;
+            rl[r] = (uint32_t)counts[r];
+            ro[r] = offsets ? offsets[r] : 0;
+            b += counts[r];
+        }
+    }
+    DSSS_CUDA(cudaMemcpyAsync(L.run_begin, rb.data(), nruns * 4, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.run_len, rl.data(), nruns * 4, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.run_offset, ro.data(), nruns * 8, cudaMemcpyHostToDevice, st));
+    DSSS_LAUNCH("k_run_marks", st, k_run_marks<<<nruns, 256, 0, st>>>(L.run_begin, L.run_len, nruns, L.run_start, L.run_of));
+    // LCPs with run starts forced to 0 (compute_ranges_and_set_lcp_at_start_of_range)
+    DSSS_LAUNCH("k_merge_init", st, k_merge_init<<<grid_for(n, 256), 256, 0, st>>>(lcp, L.run_start, n, L.ids[0], L.l[0]));
+    // decompression
+    DSSS_LAUNCH("k_full_len", st, k_full_len<<<grid_for(n, 256), 256, 0, st>>>(start, L.l[0], n, bytes, L.flen, L.counters));
+    DSSS_TRY(exclusive_scan_u32_to_u64(L.flen, L.foff, n, L.total64, L.scan, st));
+    MinTree tree;
+    tree.levels = tree_levels(n);
+    if (tree.levels > 40) return fail(DSSS_ENOTSUP, "merge: too many strings");
+    {
+        uint64_t off = 0, m = n;
+        for (int l = 0; l < tree.levels; ++l) {
+            tree.lv[l] = L.tree + off;
+            tree.sz[l] = m;
+            off += m;
+            m = (m + 1) / 2;
+        }
+    }
+    DSSS_CUDA(cudaMemcpyAsync((void*)tree.lv[0], L.l[0], n * 4, cudaMemcpyDeviceToDevice, st));
+    for (int l = 1; l < tree.levels; ++l)
+        DSSS_LAUNCH("k_min_level", st,
+                    k_min_level<<<grid_for(tree.sz[l], 256), 256, 0, st>>>(tree.lv[l - 1], tree.sz[l - 1],
+                                                                          (uint32_t*)tree.lv[l], tree.sz[l]));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaMemcpyAsync(pin + 4, L.total64, 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[0]) return fail(DSSS_EINVAL, "merge: string starts are not increasing offsets inside the buffer, "
+                                         "or the NUL layout holds more strings than n");
+    if (!char_start && pin[1] != n) return fail(DSSS_EINVAL, "merge: the NUL layout holds %u strings, not n", pin[1]);
+    const uint64_t full_bytes = *(const uint64_t*)(pin + 4);
+    // reserve the decompressed arena behind the layout
+    Carve sz2(nullptr);
+    layout_merge(sz2, L, n, bytes, full_bytes, nruns);
+    if (sz2.used > ctx->ws_cap) {
+        // grow: everything computed so far lives in the scratch, so recompute
+        // after growing (simplest correct path; the next call reuses the size)
+        DSSS_TRY(ensure_ws(ctx, sz2.used));
+        return lcp_merge(ctx, chars, bytes, char_start, lcp, n, nrecv, p, counts, offsets, order, merged_lcp,
+                         old_lcp, perm_index, perm_pe, st);
+    }
+    Carve c1(ctx->ws);
+    layout_merge(c1, L, n, bytes, full_bytes, nruns);
+    DSSS_LAUNCH("k_extend", st,
+                k_extend<<<grid_for(n, 256), 256, 0, st>>>(chars, start, L.l[0], tree, n, L.foff, L.flen, L.full,
+                                                          L.counters + 2));
+    FullView f{L.full, L.foff, L.flen};
+    // merge rounds: within each receiving PE, runs (2j, 2j+1) merge into one
+    struct Run { uint32_t beg, len; };
+    std::vector<std::vector<Run>> runs(nrecv);
+    for (uint32_t r = 0; r < nrecv; ++r)
+        for (uint32_t q = 0; q < p; ++q) runs[r].push_back({rb[(uint64_t)r * p + q], rl[(uint64_t)r * p + q]});
+    int cur = 0;
+    std::vector<MergeJob> jobs;
+    for (;;) {
+        bool more = false;
+        for (auto& v : runs) more |= v.size() > 1;
+        if (!more) break;
+        jobs.clear();
+        uint32_t tiles = 0;
+        for (auto& v : runs) {
+            std::vector<Run> next;
+            for (size_t k = 0; k < v.size(); k += 2) {
+                MergeJob J;
+                J.a_beg = v[k].beg;
+                J.a_len = v[k].len;
+                J.b_beg = k + 1 < v.size() ? v[k + 1].beg : v[k].beg + v[k].len;
+                J.b_len = k + 1 < v.size() ? v[k + 1].len : 0;
+                J.out_beg = J.a_beg;
+                J.tile0 = tiles;
+                const uint32_t tot = J.a_len + J.b_len;
+                if (tot) {
+                    tiles += (tot + MG_TILE - 1) / MG_TILE;
+                    jobs.push_back(J);
+                }
+                next.push_back({J.a_beg, tot});
+            }
+            v.swap(next);
+        }
+        if (!jobs.empty()) {
+            DSSS_CUDA(cudaMemcpyAsync(L.jobs, jobs.data(), jobs.size() * sizeof(MergeJob), cudaMemcpyHostToDevice, st));
+            DSSS_LAUNCH("k_merge_round", st,
+                        k_merge_round<<<tiles, MG_NT, 0, st>>>(f, L.jobs, (uint32_t)jobs.size(), L.ids[cur], L.l[cur],
+                                                              L.ids[cur ^ 1], L.l[cur ^ 1]));
+            DSSS_CUDA(cudaGetLastError());
+            // the job table is re-filled next round: wait for this round to read it
+            DSSS_CUDA(cudaStreamSynchronize(st));
+            cur ^= 1;
+        }
+    }
+    DSSS_CUDA(cudaMemcpyAsync(order, L.ids[cur], n * 4, cudaMemcpyDeviceToDevice, st));
+    if (merged_lcp) DSSS_CUDA(cudaMemcpyAsync(merged_lcp, L.l[cur], n * 4, cudaMemcpyDeviceToDevice, st));
+    DSSS_LAUNCH("k_merge_tags", st,
+                k_merge_tags<<<grid_for(n, 256), 256, 0, st>>>(L.ids[cur], lcp, L.run_start, L.run_of, L.run_begin,
+                                                              L.run_offset, p, n, old_lcp, perm_index, perm_pe));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[2]) return fail(DSSS_EINVAL, "merge: a source run does not start with LCP 0");
+    return DSSS_OK;
+}
+
+}  // namespace dsss

@@ -138,6 +138,17 @@ int dsss_dp_prefixes(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint
                      uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds,
                      dsss_stream_t stream);
 
+/* One round of BloomFilter<…>::filter (bloomfilter.hpp:1415-1489 round 0,
+ * :1491-1556 later rounds) over PEs whose strings are locally sorted
+ * (order/lcp as dsss_local_sort_lcp writes them, every PE's first LCP 0):
+ * candidates = ascending positions still undecided (NULL = every position,
+ * the first round); results[c] = depth (or the length at EOS) for each
+ * candidate (setDepth :1380-1411); next receives the positions that stay
+ * candidates, *m_next their count (host). */
+int dsss_dp_round(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, const uint32_t* lcp,
+                  const uint32_t* candidates, uint64_t m, uint32_t depth, uint32_t* results, uint32_t* next,
+                  uint64_t* m_next, dsss_stream_t stream);
+
 /* XXHasher::hash(str, depth, UINT64_MAX) (bloomfilter.hpp:1094-1102) over
  * xxh::hash_state_t<64> (hash/xxhash.hpp:508-706) for strings ids[0..m):
  * hash[j] = XXH64(seed 0) of the first min(depth, len) bytes of string ids[j]
@@ -152,6 +163,42 @@ int dsss_prefix_hash(const dsss_arena* in, const uint32_t* ids, uint64_t m, uint
 int dsss_partition(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                    const uint32_t* order, const uint32_t* dp, const dsss_opts* opts,
                    uint64_t* intervals, dsss_stream_t stream);
+
+/* AllToAllStringImplPrefixDoubling::alltoallv (mpi/alltoall.hpp:910-1008)
+ * with EmptyPrefixDoublingLcpByteEncoderMemCpy (mpi/byte_encoder.hpp:139-171)
+ * between p PEs of one GPU: builds every PE's receive container, back to
+ * back in PE order.  Inputs: the local sort (local_order/lcp per PE, as
+ * dsss_local_sort_lcp), dp in local order, intervals (HOST p*p, q*p + r).
+ * Each string contributes bytes [lcp', dp) and a NUL, lcp' = 0 at the first
+ * string of every interval (setLcpAtStartOfInterval :396-404).  Per received
+ * string (device, n): recv_char_start (optional) its byte offset, recv_lcp
+ * lcp', recv_index its index in the sender's local order, recv_pe the sender.
+ * HOST outputs: *char_total, recv_char_begin[p+1] (optional),
+ * recv_counts/recv_offsets [r*p + q] (optional): strings PE r got from q and
+ * q's bucket offset.  recv_chars == NULL: sizes and per-string arrays only. */
+int dsss_bucket_scatter(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                        const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, const uint64_t* intervals,
+                        uint8_t* recv_chars, uint64_t recv_capacity, uint64_t* char_total, uint64_t* recv_char_begin,
+                        uint32_t* recv_char_start, uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe,
+                        uint64_t* recv_counts, uint64_t* recv_offsets, dsss_stream_t stream);
+
+/* choose_merge<AllToAllStringImplPrefixDoubling> (merging.hpp:66-123) with
+ * LcpStringLoserTree_::writeElementsToStream(…, oldLcps)
+ * (merge/bingmann-lcp_losertree.hpp:375-428), for nrecv receive containers
+ * back to back (1 = one PE's container), each of p source runs:
+ * recv_chars holds the prefix-compressed NUL-terminated strings,
+ * recv_char_start (optional) their byte offsets, recv_lcp their sender-side
+ * LCPs; recv_counts/recv_offsets (HOST, nrecv*p, [r*p + q]) the strings of
+ * source q and q's bucket offset.  Outputs per merged position (device):
+ * order = index into the containers, merged_lcp (0 at each PE start),
+ * old_lcp (the sender-side LCP, 0 at run starts), perm_index/perm_pe (the
+ * (stringIndex, PEIndex) tag); all but order optional.  Byte-identical
+ * strings keep source order; the reference's loser tree orders them by
+ * tournament history. */
+int dsss_lcp_merge(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes, const uint32_t* recv_char_start,
+                   const uint32_t* recv_lcp, uint64_t n, uint32_t nrecv, uint32_t p, const uint64_t* recv_counts,
+                   const uint64_t* recv_offsets, uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp,
+                   uint32_t* perm_index, uint32_t* perm_pe, dsss_stream_t stream);
 
 /* calc_lcp of sorted neighbours (strings/stringtools.hpp:158-166): lcp[i] =
  * LCP(string order[i-1], string order[i]) for i >= 1, lcp[0] = 0. */
