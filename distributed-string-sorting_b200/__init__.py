@@ -64,6 +64,10 @@ _SIGS = {
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
                                _P]),
+    "dsss_pd_sort_batched": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
+                                  ctypes.POINTER(PdResult), _P]),
+    "dsss_pd_sort_batched_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
+                                       ctypes.POINTER(PdResult), _P]),
     "dsss_local_sort_lcp": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), _P, _P, _P]),
     "dsss_dp_prefixes": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "dsss_prefix_hash": (_I, [ctypes.POINTER(Arena), _P, _U64, _U32, _P, _P]),
@@ -221,6 +225,37 @@ def equal_parts(n: int, p: int) -> np.ndarray:
     return np.array([q * n // p for q in range(p + 1)], dtype=np.uint64)
 
 
+def concat_sets(sets, pinned: bool = False):
+    """One arena holding several string sets back to back; returns it and the
+    set bounds (len(sets) + 1 string ids)."""
+    n = sum(h.n for h in sets)
+    total = sum(h.char_bytes for h in sets)
+    chars = _alloc_host(total + PAD, np.uint8, pinned)
+    offs = _alloc_host(max(n, 1) * 8, np.uint64, pinned)[:n]
+    lens = _alloc_host(max(n, 1) * 4, np.uint32, pinned)[:n]
+    set_begin = np.zeros(len(sets) + 1, dtype=np.uint64)
+    cpos, spos = 0, 0
+    for k, h in enumerate(sets):
+        chars[cpos:cpos + h.char_bytes] = h.chars[:h.char_bytes]
+        offs[spos:spos + h.n] = h.offsets + np.uint64(cpos)
+        lens[spos:spos + h.n] = h.lengths
+        cpos += h.char_bytes
+        spos += h.n
+        set_begin[k + 1] = spos
+    chars[total:] = 0
+    return HostStrings(chars, offs, lens, total), set_begin
+
+
+def batched_parts(set_begin, p: int) -> np.ndarray:
+    """PE boundaries (nsets*p + 1) of p equal slices inside every set."""
+    sb = np.asarray(set_begin, dtype=np.uint64)
+    out = [0]
+    for s in range(len(sb) - 1):
+        n = int(sb[s + 1] - sb[s])
+        out.extend(int(sb[s]) + q * n // p for q in range(1, p + 1))
+    return np.array(out, dtype=np.uint64)
+
+
 # ------------------------------------------------------------------ device --
 class DeviceStrings:
     """A device copy of HostStrings (torch tensors; chars padded with zeros)."""
@@ -327,6 +362,45 @@ def pd_sort_host(ctx: Context, hs: HostStrings, p: int, part_begin=None, sampler
     o = _opts(sampler)
     check(lib().dsss_pd_sort_host(ctx.h, ctypes.byref(a), p, _ptr(pb), ctypes.byref(o), ctypes.byref(res),
                                   _stream_ptr(stream)))
+    out["part_begin"] = pb
+    return out
+
+
+def pd_sort_batched(ctx: Context, ds: DeviceStrings, nsets: int, p: int, part_begin, sampler: int = 0,
+                    merged_lcp: bool = True, local_lcp: bool = False, small_sort_max: int = 0, stream=None, out=None):
+    """dsss_pd_sort_batched: nsets independent sets of p PEs in one arena
+    (part_begin: nsets*p + 1 PE bounds, e.g. batched_parts)."""
+    n = ds.n
+    pb = np.asarray(part_begin, dtype=np.uint64)
+    npe = nsets * p
+    if out is None:
+        out = dict(local_order=_empty(n), dp=_empty(n), perm_index=_empty(n), perm_pe=_empty(n),
+                   merged_lcp=_empty(n) if merged_lcp else None, local_lcp=_empty(n) if local_lcp else None,
+                   intervals=np.zeros(npe * p, dtype=np.uint64), recv_counts=np.zeros(npe, dtype=np.uint64))
+    res = PdResult(_ptr(out["local_order"]), _ptr(out["local_lcp"]), _ptr(out["dp"]), _ptr(out["intervals"]),
+                   _ptr(out["perm_index"]), _ptr(out["perm_pe"]), _ptr(out["merged_lcp"]), _ptr(out["recv_counts"]))
+    o = _opts(sampler, 2, small_sort_max, FLAG_LOCAL_LCP if local_lcp else 0)
+    check(lib().dsss_pd_sort_batched(ctx.h, ctypes.byref(ds.arena()), nsets, p, _ptr(pb), ctypes.byref(o),
+                                     ctypes.byref(res), _stream_ptr(stream)))
+    out["part_begin"] = pb
+    return out
+
+
+def pd_sort_batched_host(ctx: Context, hs: HostStrings, nsets: int, p: int, part_begin, sampler: int = 0,
+                         merged_lcp: bool = True, out=None, pinned: bool = False, stream=None):
+    """dsss_pd_sort_batched_host: the batched path with host buffers."""
+    n = hs.n
+    pb = np.asarray(part_begin, dtype=np.uint64)
+    npe = nsets * p
+    if out is None:
+        mk = (lambda: _alloc_host(max(n, 1) * 4, np.uint32, pinned)[:max(n, 1)])
+        out = dict(local_order=mk(), dp=mk(), perm_index=mk(), perm_pe=mk(), merged_lcp=mk() if merged_lcp else None,
+                   local_lcp=None, intervals=np.zeros(npe * p, dtype=np.uint64),
+                   recv_counts=np.zeros(npe, dtype=np.uint64))
+    res = PdResult(_ptr(out["local_order"]), None, _ptr(out["dp"]), _ptr(out["intervals"]), _ptr(out["perm_index"]),
+                   _ptr(out["perm_pe"]), _ptr(out["merged_lcp"]), _ptr(out["recv_counts"]))
+    check(lib().dsss_pd_sort_batched_host(ctx.h, ctypes.byref(hs.arena()), nsets, p, _ptr(pb),
+                                          ctypes.byref(_opts(sampler)), ctypes.byref(res), _stream_ptr(stream)))
     out["part_begin"] = pb
     return out
 

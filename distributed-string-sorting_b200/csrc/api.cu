@@ -55,11 +55,15 @@ __global__ void k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uin
     pe[g] = lo;
 }
 
+// Receiving PE of every string: set s's PE q sends local positions
+// [bounds[(s*p+q)*(p+1) + r], … + r + 1) to the set's PE r; buckets are
+// numbered s*p + r.  pe_local (optional) receives q.
 __global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p, uint64_t n,
-                            uint32_t* bucket) {
+                            uint32_t* bucket, uint32_t* pe_local) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    const uint64_t* b = bounds + (uint64_t)pe[g] * (p + 1);
+    const uint32_t src = pe[g];
+    const uint64_t* b = bounds + (uint64_t)src * (p + 1);
     const uint64_t li = g2l[g];
     uint32_t lo = 0, hi = p;  // last r with b[r] <= li (b[0] = 0, b[p] = n_q > li)
     while (hi - lo > 1) {
@@ -67,7 +71,9 @@ __global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint6
         if (b[mid] <= li) lo = mid;
         else hi = mid;
     }
-    bucket[g] = lo;
+    const uint32_t set = src / p;
+    bucket[g] = set * p + lo;
+    if (pe_local) pe_local[g] = src - set * p;
 }
 
 __global__ void k_merged_lcp(const uint32_t* out2g, const uint32_t* lcpg, const uint64_t* recv_begin, uint32_t p,
@@ -97,7 +103,7 @@ __global__ void k_zero_starts(uint32_t* a, const uint64_t* pb, uint32_t p) {
 
 struct PdLayout {
     ulonglong2* handles;
-    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *out2g, *nlong, *err;
+    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *out2g, *pel, *nlong, *err;
     uint64_t *pb, *bounds, *recv_begin;
     void* ms;
     SortLayout sort;
@@ -105,8 +111,11 @@ struct PdLayout {
     PartitionLayout part;
 };
 
-static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t p, uint32_t factor, uint32_t small_max) {
+// n strings in nsets sets of p PEs each.
+static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t nsets, uint32_t p, uint32_t factor,
+                      uint32_t small_max) {
     uint64_t N = n ? n : 1;
+    const uint64_t npe = (uint64_t)nsets * p;
     L.handles = c.take<ulonglong2>(N);
     L.ord = c.take<uint32_t>(N);
     L.lcp = c.take<uint32_t>(N);
@@ -115,110 +124,122 @@ static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t p, uint32_t fa
     L.g2l = c.take<uint32_t>(N);
     L.tmp = c.take<uint32_t>(N);
     L.out2g = c.take<uint32_t>(N);
+    L.pel = nsets > 1 ? c.take<uint32_t>(N) : nullptr;
     L.nlong = c.take<uint32_t>(1);
     L.err = c.take<uint32_t>(1);
-    L.pb = c.take<uint64_t>(p + 1);
-    L.bounds = c.take<uint64_t>((uint64_t)p * (p + 1));
-    L.recv_begin = c.take<uint64_t>(p + 1);
-    L.ms = c.take<unsigned char>(multisplit_scratch_bytes(N, p));
-    layout_sort(c, L.sort, N, 1, small_max);
-    layout_dp(c, L.dp, N);
-    layout_partition(c, L.part, N, p, factor);
+    L.pb = c.take<uint64_t>(npe + 1);
+    L.bounds = c.take<uint64_t>(npe * (p + 1));
+    L.recv_begin = c.take<uint64_t>(npe + 1);
+    L.ms = c.take<unsigned char>(multisplit_scratch_bytes(N, (uint32_t)npe));
+    layout_sort(c, L.sort, N, nsets, small_max);
+    layout_dp(c, L.dp, N, nsets);
+    layout_partition(c, L.part, N, p, factor, nsets);
 }
 
-static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* pb, const dsss_opts* opts,
-                       dsss_pd_result* out, cudaStream_t st) {
+// The fused path over nsets independent string sets of p PEs each (PE q of
+// set s = part_begin[s*p + q] .. part_begin[s*p + q + 1]); every set's result
+// is the one a call on that set alone gives.  Per-string outputs keep the
+// arena's positions (set s's merged sequences fill the positions of its
+// strings), intervals and recv_counts are per set, one after the other.
+static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* pb,
+                       const dsss_opts* opts, dsss_pd_result* out, cudaStream_t st) {
     DSSS_TRY(check_arena(in));
-    DSSS_TRY(check_parts(p, pb, in->n));
+    if (nsets == 0) return fail(DSSS_EINVAL, "nsets must be >= 1");
+    if (p == 0) return fail(DSSS_EINVAL, "p must be >= 1");
+    if ((uint64_t)nsets * p > MAX_SPLIT_BUCKETS)
+        return fail(DSSS_ENOTSUP, "nsets * p > %u PEs per GPU is not supported", MAX_SPLIT_BUCKETS);
+    const uint32_t npe = nsets * p;
+    DSSS_TRY(check_parts(npe, pb, in->n));
     if (!out || !out->local_order || !out->recv_counts) return fail(DSSS_EINVAL, "result arrays missing");
     if (p > 1 && (!out->dp || !out->intervals || !out->perm_index || !out->perm_pe))
         return fail(DSSS_EINVAL, "result arrays missing");
-    if (p > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "p > %u PEs per GPU is not supported", MAX_SPLIT_BUCKETS);
     const uint64_t n = in->n;
     const uint32_t factor = factor_of(opts), smax = smallmax_of(opts);
     const bool want_local_lcp = opts && (opts->flags & DSSS_FLAG_LOCAL_LCP) && out->local_lcp;
     Carve sz(nullptr);
     PdLayout L;
-    layout_pd(sz, L, n, p, factor, smax);
+    layout_pd(sz, L, n, nsets, p, factor, smax);
     DSSS_TRY(ensure_ws(ctx, sz.used));
     DSSS_TRY(ensure_pin(ctx, 4096));
     Carve c(ctx->ws);
-    layout_pd(c, L, n, p, factor, smax);
+    layout_pd(c, L, n, nsets, p, factor, smax);
     uint32_t* pin = (uint32_t*)ctx->pin;  // re-read after any call that may grow it
     ArenaDev a = view(in);
     if (n == 0) {
-        for (uint32_t r = 0; r < p; ++r) out->recv_counts[r] = 0;
+        for (uint32_t r = 0; r < npe; ++r) out->recv_counts[r] = 0;
         if (p > 1)
-            for (uint64_t k = 0; k < (uint64_t)p * p; ++k) out->intervals[k] = 0;
+            for (uint64_t k = 0; k < (uint64_t)npe * p; ++k) out->intervals[k] = 0;
         return DSSS_OK;
     }
+    std::vector<uint64_t> set_begin(nsets + 1);
+    for (uint32_t s = 0; s <= nsets; ++s) set_begin[s] = pb[(uint64_t)s * p];
     make_handles(a, L.handles, st);
     a.h = L.handles;
     DSSS_CUDA(cudaMemsetAsync(L.err, 0, sizeof(uint32_t), st));
-    // 1. one sort of all strings
-    uint64_t all[2] = {0, n};
+    // 1. one sort per set, all sets in one segmented sort
     {
         StageTimer t("stage:sort", st);
-        DSSS_TRY(sort_strings(L.sort, a, n, 1, all, nullptr, L.ord, L.lcp, smax, pin, st));
+        DSSS_TRY(sort_strings(L.sort, a, n, nsets, set_begin.data(), nullptr, L.ord, L.lcp, smax, pin, st));
     }
     if (p == 1) {  // prefix_doubling.hpp:236: one PE sorts locally and returns no permutation
         DSSS_CUDA(cudaMemcpyAsync(out->local_order, L.ord, n * 4, cudaMemcpyDeviceToDevice, st));
         if (want_local_lcp) DSSS_CUDA(cudaMemcpyAsync(out->local_lcp, L.lcp, n * 4, cudaMemcpyDeviceToDevice, st));
-        out->recv_counts[0] = 0;
+        for (uint32_t r = 0; r < npe; ++r) out->recv_counts[r] = 0;
         return DSSS_OK;
     }
-    // 2. distinguishing prefixes over the global order
+    // 2. distinguishing prefixes over each set's sorted order
     {
         StageTimer t("stage:dp", st);
-        DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st));
+        DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st, nsets, set_begin.data()));
     }
     // 3. local orders per PE
     StageTimer t_local("stage:local", st);
-    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe));
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (npe + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, npe, L.pe));
     {
         // local order and DP per PE: out[dest] = (string id, dp); g2l = rank inside the PE
         const uint32_t* in[2] = {L.ord, L.dpg};
         uint32_t* outs[2] = {out->local_order, out->dp};
-        DSSS_TRY(multisplit_payload(L.pe, n, p, 2, in, outs, L.g2l, L.err, L.ms, st));
+        DSSS_TRY(multisplit_payload(L.pe, n, npe, 2, in, outs, L.g2l, L.err, L.ms, st));
     }
     DSSS_CUDA(cudaGetLastError());
     t_local.end();
     // 4. partition
     {
         StageTimer t("stage:partition", st);
-        DSSS_TRY(partition_pes(L.part, ctx, a, p, pb, out->local_order, out->dp, sampler_of(opts), factor,
-                               out->intervals, st));
+        DSSS_TRY(partition_sets(L.part, ctx, a, nsets, p, pb, out->local_order, out->dp, sampler_of(opts), factor,
+                                out->intervals, st));
     }
     StageTimer t_merge("stage:merge", st);
-    // 5. buckets and the merged sequences
-    std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), recv(p + 1, 0);
-    for (uint32_t q = 0; q < p; ++q) {
-        bounds[(uint64_t)q * (p + 1)] = 0;
+    // 5. buckets and the merged sequences; receiving PE (s, r) is bucket s*p + r
+    std::vector<uint64_t> bounds((uint64_t)npe * (p + 1)), recv(npe + 1, 0);
+    for (uint32_t g = 0; g < npe; ++g) {
+        const uint32_t s = g / p;
+        bounds[(uint64_t)g * (p + 1)] = 0;
         for (uint32_t r = 0; r < p; ++r) {
-            uint64_t v = out->intervals[(uint64_t)q * p + r];
-            bounds[(uint64_t)q * (p + 1) + r + 1] = bounds[(uint64_t)q * (p + 1) + r] + v;
-            recv[r + 1] += v;
+            uint64_t v = out->intervals[(uint64_t)g * p + r];
+            bounds[(uint64_t)g * (p + 1) + r + 1] = bounds[(uint64_t)g * (p + 1) + r] + v;
+            recv[(uint64_t)s * p + r + 1] += v;
         }
     }
-    for (uint32_t r = 0; r < p; ++r) {
+    for (uint32_t r = 0; r < npe; ++r) {
         out->recv_counts[r] = recv[r + 1];
         recv[r + 1] += recv[r];
     }
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
-    DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_bucket_of", st, k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp));
+    DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (npe + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_LAUNCH("k_bucket_of", st, k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp, L.pel));
     {
         // merged sequences: (index in sender's local order, sender PE, global position)
-        const uint32_t* in[3] = {L.g2l, L.pe, nullptr};
+        const uint32_t* in[3] = {L.g2l, nsets > 1 ? L.pel : L.pe, nullptr};
         uint32_t* outs[3] = {out->perm_index, out->perm_pe, L.out2g};
-        DSSS_TRY(multisplit_payload(L.tmp, n, p, 3, in, outs, nullptr, L.err, L.ms, st));
+        DSSS_TRY(multisplit_payload(L.tmp, n, npe, 3, in, outs, nullptr, L.err, L.ms, st));
     }
     if (out->merged_lcp)
-        DSSS_LAUNCH("k_merged_lcp", st, k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->merged_lcp));
+        DSSS_LAUNCH("k_merged_lcp", st, k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, npe, n, out->merged_lcp));
     if (want_local_lcp) {
         DSSS_TRY(adjacent_lcp(a, out->local_order, n, out->local_lcp, L.tmp, L.nlong, st));
-        DSSS_LAUNCH("k_zero_starts", st, k_zero_starts<<<grid_for(p, 128), 128, 0, st>>>(out->local_lcp, L.pb, p));
+        DSSS_LAUNCH("k_zero_starts", st, k_zero_starts<<<grid_for(npe, 128), 128, 0, st>>>(out->local_lcp, L.pb, npe));
     }
     DSSS_CUDA(cudaGetLastError());
     // The host vectors above were copied asynchronously; finish before they go.
@@ -240,7 +261,15 @@ int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
     ActiveCtx active(ctx);
     DSSS_CUDA(cudaSetDevice(ctx->device));
-    return pd_sort_dev(ctx, in, p, part_begin, opts, out, (cudaStream_t)stream);
+    return pd_sort_dev(ctx, in, 1, p, part_begin, opts, out, (cudaStream_t)stream);
+}
+
+int dsss_pd_sort_batched(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* part_begin,
+                         const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    return pd_sort_dev(ctx, in, nsets, p, part_begin, opts, out, (cudaStream_t)stream);
 }
 
 int dsss_local_sort_lcp(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
@@ -406,12 +435,13 @@ int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order
 
 // Host-memory variant: device copies of the arena and results live in a
 // second context buffer so repeated calls reuse it.
-int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
-                      const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
+static int pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* part_begin,
+                        const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
     ActiveCtx active(ctx);
     if (!in) return fail(DSSS_EINVAL, "arena is NULL");
-    DSSS_TRY(check_parts(p, part_begin, in->n));
+    if (nsets == 0 || p == 0) return fail(DSSS_EINVAL, "nsets and p must be >= 1");
+    DSSS_TRY(check_parts(nsets * p, part_begin, in->n));
     if (!out) return fail(DSSS_EINVAL, "result is NULL");
     DSSS_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
@@ -437,7 +467,7 @@ int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uin
     // The io buffer sits in front of the pipeline's own scratch.
     Carve pdsz(nullptr);
     PdLayout PL;
-    layout_pd(pdsz, PL, n, p, factor_of(opts), smallmax_of(opts));
+    layout_pd(pdsz, PL, n, nsets, p, factor_of(opts), smallmax_of(opts));
     const uint64_t io_bytes = (sz.used + 255) & ~255ull;
     DSSS_TRY(ensure_ws(ctx, io_bytes + pdsz.used));
     Carve c(ctx->ws);
@@ -453,7 +483,7 @@ int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uin
     sub.ws = (char*)ctx->ws + io_bytes;
     sub.ws_cap = ctx->ws_cap - io_bytes;
     sub.budget = 0;
-    int rc = pd_sort_dev(&sub, &da, p, part_begin, opts, &dr, st);
+    int rc = pd_sort_dev(&sub, &da, nsets, p, part_begin, opts, &dr, st);
     ctx->pin = sub.pin;
     ctx->pin_cap = sub.pin_cap;
     if (rc != DSSS_OK) return rc;
@@ -470,6 +500,17 @@ int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uin
     }
     DSSS_CUDA(cudaStreamSynchronize(st));
     return DSSS_OK;
+}
+
+int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                      const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream) {
+    return pd_sort_host(ctx, in, 1, p, part_begin, opts, out, stream);
+}
+
+int dsss_pd_sort_batched_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p,
+                              const uint64_t* part_begin, const dsss_opts* opts, dsss_pd_result* out,
+                              dsss_stream_t stream) {
+    return pd_sort_host(ctx, in, nsets, p, part_begin, opts, out, stream);
 }
 
 }  // extern "C"

@@ -37,6 +37,17 @@ __global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_
     if (i < n) lens[i] = a.len[order[i]];  // the 4-byte array caches better than 16-byte handles
 }
 
+// Index of the string set holding sorted position i (set_begin: nsets+1 bounds).
+__device__ __forceinline__ uint32_t set_of(const uint64_t* set_begin, uint32_t nsets, uint64_t i) {
+    uint32_t lo = 0, hi = nsets;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (set_begin[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Adds the block's number of true flags to *ctr with one atomic per block
 // (blockDim.x == 256, called by every thread of the block).
 __device__ __forceinline__ void block_count(uint32_t* ctr, bool flag) {
@@ -54,7 +65,8 @@ __device__ __forceinline__ void block_count(uint32_t* ctr, bool flag) {
 }
 
 __global__ void k_dp_classify(const uint8_t* st, int all, const uint32_t* lens, const uint32_t* lcp, uint64_t n,
-                              uint32_t depth, uint32_t* dp, uint8_t* st_next, uint8_t* kind, uint32_t* counters) {
+                              uint32_t depth, uint32_t* dp, uint8_t* st_next, uint8_t* kind, uint32_t* counters,
+                              const uint64_t* set_begin, uint32_t nsets, uint32_t* set_cnt) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool hashed = false, stays = false;
     if (i < n) {
@@ -80,14 +92,33 @@ __global__ void k_dp_classify(const uint8_t* st, int all, const uint32_t* lens, 
         st_next[i] = nx;
         stays = nx != 0;
     }
+    if (nsets > 1) {  // hashed strings per set size the per-set table regions
+        const int lane = threadIdx.x & 31;
+        const uint32_t sid = hashed ? set_of(set_begin, nsets, i) : 0xFFFFFFFFu - lane;
+        const uint32_t peers = __match_any_sync(FULLM, sid);
+        if (hashed && lane == __ffs(peers) - 1) atomicAdd(&set_cnt[sid], (uint32_t)__popc(peers));
+    }
     block_count(counters + 0, hashed);
     block_count(counters + 1, stays);
 }
 
+// Each string set owns a power-of-two region of the table (base, mask): equal
+// prefixes in different sets are not duplicates of each other.
 __global__ void k_dp_hash(ArenaDev a, const uint32_t* order, const uint8_t* kind, uint64_t n, uint32_t depth,
-                          unsigned long long* tkeys, uint8_t* tdup, uint32_t mask, uint32_t* slot, uint32_t* err) {
+                          unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1, const uint64_t* set_begin,
+                          uint32_t nsets, const uint64_t* set_base, const uint32_t* set_mask, uint32_t* slot,
+                          uint32_t* err) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || kind[i] < 2) return;
+    uint64_t base = 0;
+    uint32_t mask = mask1;
+    if (nsets > 1) {
+        const uint32_t sid = set_of(set_begin, nsets, i);
+        base = set_base[sid];
+        mask = set_mask[sid];
+        tkeys += base;
+        tdup += base;
+    }
     const unsigned long long h = filter_hash(xxh64_dev(a.chars + a.off[order[i]], depth));
     uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
     // Linear probing; the table always has free slots, so a free or matching
@@ -106,7 +137,7 @@ __global__ void k_dp_hash(ArenaDev a, const uint32_t* order, const uint8_t* kind
         }
         sl = (sl + 1) & mask;
     }
-    slot[i] = sl;
+    slot[i] = sl == NO_SLOT ? NO_SLOT : (uint32_t)(base + sl);
 }
 
 __global__ void k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup, uint64_t n,
@@ -137,14 +168,65 @@ static uint64_t table_slots(uint64_t n) {
     return t;
 }
 
-void layout_dp(Carve& c, DpLayout& L, uint64_t n) {
+// Per-set table regions, the same rule with 64 slots at least (none for a set
+// that hashes nothing).  Total <= 3 * hashed + 68 * nsets.
+__device__ __forceinline__ uint64_t set_slots(uint32_t c) {
+    if (c == 0) return 0;
+    uint64_t t = 64;
+    while (t < (uint64_t)c + c / 2 + 2) t <<= 1;
+    return t;
+}
+
+constexpr int SET_NT = 1024;
+
+// One block: region base and mask per set from the hashed counts, total slots
+// into counters[4..5] (lo, hi), counters[2] set if it exceeds cap.
+__global__ void __launch_bounds__(SET_NT) k_set_tables(const uint32_t* cnt, uint32_t nsets, uint64_t cap,
+                                                       uint64_t* base, uint32_t* mask, uint32_t* counters) {
+    __shared__ uint64_t part[SET_NT];
+    const uint32_t per = (nsets + SET_NT - 1) / SET_NT;
+    const uint32_t b = min(nsets, threadIdx.x * per), e = min(nsets, b + per);
+    uint64_t sum = 0;
+    for (uint32_t s = b; s < e; ++s) sum += set_slots(cnt[s]);
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < SET_NT; off <<= 1) {
+        const uint64_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint64_t run = part[threadIdx.x] - sum;
+    for (uint32_t s = b; s < e; ++s) {
+        const uint64_t sl = set_slots(cnt[s]);
+        base[s] = run;
+        mask[s] = sl ? (uint32_t)(sl - 1) : 0;
+        run += sl;
+    }
+    if (threadIdx.x == SET_NT - 1) {
+        const uint64_t total = part[SET_NT - 1];
+        if (total > cap) counters[2] = 1;
+        counters[4] = (uint32_t)total;
+        counters[5] = (uint32_t)(total >> 32);
+    }
+}
+
+void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     uint64_t N = n ? n : 1;
+    if (nsets == 0) nsets = 1;
+    L.nsets_cap = nsets;
+    L.set_begin = c.take<uint64_t>(nsets + 1);
+    L.set_base = c.take<uint64_t>(nsets + 1);
+    L.set_mask = c.take<uint32_t>(nsets);
+    L.set_cnt = c.take<uint32_t>(nsets);
     L.st[0] = c.take<uint8_t>(N);
     L.st[1] = c.take<uint8_t>(N);
     L.kind = c.take<uint8_t>(N);
     L.lens = c.take<uint32_t>(N);
     L.slot = c.take<uint32_t>(N);
-    L.slots = table_slots(N);
+    // one set: the table for n keys; several: room for every set's own
+    // power-of-two region (at most 3 slots per key plus 68 per set)
+    L.slots = nsets == 1 ? table_slots(N) : 3 * N + 128ull * (nsets + 1);
     L.tkeys = c.take<unsigned long long>(L.slots);
     L.tdup = c.take<uint8_t>(L.slots);
     L.counters = c.take<uint32_t>(8);
@@ -152,11 +234,17 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n) {
 
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
-              cudaStream_t st) {
+              cudaStream_t st, uint32_t nsets, const uint64_t* set_begin_host) {
     uint32_t r = 0;
     if (n == 0) {
         if (rounds) *rounds = 0;
         return DSSS_OK;
+    }
+    if (nsets == 0) nsets = 1;
+    if (nsets > 1) {
+        if (!set_begin_host || nsets > L.nsets_cap) return fail(DSSS_EINVAL, "string sets not planned");
+        DSSS_CUDA(cudaMemcpyAsync(L.set_begin, set_begin_host, (nsets + 1) * sizeof(uint64_t),
+                                  cudaMemcpyHostToDevice, st));
     }
     const unsigned grid = grid_for(n, 256);
     DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens));
@@ -166,19 +254,28 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
     for (uint64_t i = start * 2;; i *= 2) {
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
         DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
+        if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
         DSSS_LAUNCH("k_dp_classify", st,
                     k_dp_classify<<<grid, 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
-                                                       L.st[cur ^ 1], L.kind, L.counters));
-        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                                                       L.st[cur ^ 1], L.kind, L.counters, L.set_begin, nsets,
+                                                       L.set_cnt));
+        if (nsets > 1)
+            DSSS_LAUNCH("k_set_tables", st,
+                        k_set_tables<<<1, SET_NT, 0, st>>>(L.set_cnt, nsets, L.slots, L.set_base, L.set_mask,
+                                                           L.counters));
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 6 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
         const uint32_t hashed = pin[0];
+        if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table regions exceed the plan");
         if (hashed) {
-            const uint64_t slots = table_slots(hashed);
+            const uint64_t slots = nsets > 1 ? ((uint64_t)pin[5] << 32 | pin[4]) : table_slots(hashed);
+            if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
             DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
             DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
             DSSS_LAUNCH("k_dp_hash", st,
                         k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
-                                                       (uint32_t)(slots - 1), L.slot, L.counters + 2));
+                                                       (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
+                                                       L.set_mask, L.slot, L.counters + 2));
             DSSS_LAUNCH("k_dp_query", st,
                         k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
             DSSS_CUDA(cudaGetLastError());
@@ -244,7 +341,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
     }
     DSSS_LAUNCH("k_dp_classify", st,
                 k_dp_classify<<<grid, 256, 0, st>>>(L.st[0], all, L.lens, lcp, n, depth, dp, L.st[1], L.kind,
-                                                   L.counters));
+                                                   L.counters, nullptr, 1, nullptr));
     DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
     if (pin[3]) return fail(DSSS_EINVAL, "candidates must be ascending positions below n");
@@ -254,7 +351,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
         DSSS_LAUNCH("k_dp_hash", st,
                     k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
-                                                   L.slot, L.counters + 2));
+                                                   nullptr, 1, nullptr, nullptr, L.slot, L.counters + 2));
         DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
     }
     DSSS_LAUNCH("k_state_flags", st, k_state_flags<<<grid, 256, 0, st>>>(L.st[1], n, R.flag));

@@ -13,15 +13,25 @@ struct DpLayout {
     uint8_t* tdup;
     uint64_t slots;
     uint32_t* counters;
+    // independent string sets (batched sorts): sorted positions
+    // [set_begin[s], set_begin[s+1]) belong to set s; each set hashes into its
+    // own region [set_base[s], set_base[s] + set_mask[s] + 1) of the table
+    uint32_t nsets_cap;
+    uint64_t* set_begin;
+    uint64_t* set_base;
+    uint32_t* set_mask;
+    uint32_t* set_cnt;
 };
 
-void layout_dp(Carve& c, DpLayout& L, uint64_t n);
+void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets = 1);
 
 // order/lcp: strings in sorted order per PE (lcp 0 at every PE start); dp[i]
 // receives the distinguishing-prefix length of the string at position i.
+// set_begin_host (nsets + 1 bounds, NULL for one set): prefixes are only
+// duplicates of prefixes in the same set.
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
-              cudaStream_t st);
+              cudaStream_t st, uint32_t nsets = 1, const uint64_t* set_begin_host = nullptr);
 
 struct DpRoundLayout {
     DpLayout dp;

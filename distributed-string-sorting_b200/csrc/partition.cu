@@ -42,16 +42,22 @@ __device__ __forceinline__ int str_cmp(const uint8_t* chars, uint64_t oa, uint32
     }
 }
 
-__global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint64_t* pb, uint32_t p,
-                            uint32_t nspl, const uint64_t* spl_off, const uint32_t* spl_len,
+// One thread per (PE, splitter): PE g of set g / p searches the set's k-th
+// splitter (k < set_nspl[set]); splitters and positions are strided by p - 1.
+__global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint64_t* pb, uint32_t npe, uint32_t p,
+                            const uint32_t* set_nspl, const uint64_t* spl_off, const uint32_t* spl_len,
                             const uint64_t* spl_index, int indexed, uint64_t* pos) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)p * nspl) return;
-    const uint32_t q = (uint32_t)(t / nspl), k = (uint32_t)(t % nspl);
-    const uint64_t base = pb[q];
-    uint64_t left = 0, right = pb[q + 1] - base;
-    const uint64_t so = spl_off[k];
-    const uint32_t sl = spl_len[k];
+    const uint32_t stride = p - 1;
+    if (t >= (uint64_t)npe * stride) return;
+    const uint32_t g = (uint32_t)(t / stride), k = (uint32_t)(t % stride);
+    const uint32_t set = g / p;
+    if (k >= set_nspl[set]) return;
+    const uint64_t sp = (uint64_t)set * stride + k;
+    const uint64_t base = pb[g];
+    uint64_t left = 0, right = pb[g + 1] - base;
+    const uint64_t so = spl_off[sp];
+    const uint32_t sl = spl_len[sp];
     while (left != right) {
         const uint64_t d = (right - left) / 2;
         uint64_t off;
@@ -60,8 +66,9 @@ __global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint6
         int res = str_cmp(a.chars, off, len, so, sl);
         if (res == 0 && indexed) {
             // indexStringCompare (misc.hpp:335-345): equal bytes compare by the
-            // global index, as int64 narrowed to int.
-            res = (int)(int32_t)(uint32_t)((left + d + base) - spl_index[k]);
+            // global index, as int64 narrowed to int (both indices carry the
+            // same set offset, so their difference is the set-local one).
+            res = (int)(int32_t)(uint32_t)((left + d + base) - spl_index[sp]);
         }
         if (res < 0) {
             left = left + d + 1;
@@ -75,68 +82,70 @@ __global__ void k_binsearch(ArenaDev a, const uint32_t* local_order, const uint6
     pos[t] = left;
 }
 
-uint64_t partition_scratch_bytes(uint64_t n, uint32_t p, uint32_t factor) {
-    Carve c(nullptr);
-    PartitionLayout L;
-    layout_partition(c, L, n, p, factor);
-    return c.used;
+static uint64_t max_samples(uint64_t n, uint32_t nsets, uint32_t p, uint32_t factor) {
+    return std::min<uint64_t>((uint64_t)factor * (p ? p - 1 : 0) * p * nsets, n) + 1;
 }
 
-static uint64_t max_samples(uint64_t n, uint32_t p, uint32_t factor) {
-    return std::min<uint64_t>((uint64_t)factor * (p ? p - 1 : 0) * p, n) + 1;
-}
-
-void layout_partition(Carve& c, PartitionLayout& L, uint64_t n, uint32_t p, uint32_t factor) {
-    uint64_t S = max_samples(n, p, factor);
+void layout_partition(Carve& c, PartitionLayout& L, uint64_t n, uint32_t p, uint32_t factor, uint32_t nsets) {
+    if (nsets == 0) nsets = 1;
+    const uint64_t npe = (uint64_t)nsets * p;
+    uint64_t S = max_samples(n, nsets, p, factor);
     L.cap = S;
     L.sample_lp = c.take<uint64_t>(S);
     L.soff = c.take<uint64_t>(S);
     L.slen = c.take<uint32_t>(S);
     L.sorted = c.take<uint32_t>(S);
     L.slcp = c.take<uint32_t>(S);
-    L.spl_off = c.take<uint64_t>(p);
-    L.spl_len = c.take<uint32_t>(p);
-    L.spl_index = c.take<uint64_t>(p);
-    L.pos = c.take<uint64_t>((uint64_t)p * p + 1);
-    L.pb = c.take<uint64_t>(p + 1);
-    layout_sort(c, L.sort, S, 1, 0);
+    L.spl_off = c.take<uint64_t>(npe);
+    L.spl_len = c.take<uint32_t>(npe);
+    L.spl_index = c.take<uint64_t>(npe);
+    L.pos = c.take<uint64_t>(npe * p + 1);
+    L.pb = c.take<uint64_t>(npe + 1);
+    L.set_nspl = c.take<uint32_t>(nsets);
+    layout_sort(c, L.sort, S, nsets, 0);
 }
 
-int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_t p, const uint64_t* pb,
-                  const uint32_t* local_order, const uint32_t* dp, uint32_t sampler, uint32_t factor,
-                  uint64_t* intervals, cudaStream_t st) {
+int partition_sets(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_t nsets, uint32_t p,
+                   const uint64_t* pb, const uint32_t* local_order, const uint32_t* dp, uint32_t sampler,
+                   uint32_t factor, uint64_t* intervals, cudaStream_t st) {
     const bool indexed = sampler == DSSS_SAMPLER_INDEXED_NUM_STRINGS;
+    const uint64_t npe = (uint64_t)nsets * p;
     // sample positions (host, double arithmetic as getNumberSplitter/sample_splitters)
-    std::vector<uint64_t> lp, sindex;
-    for (uint32_t q = 0; q < p; ++q) {
-        const uint64_t nq = pb[q + 1] - pb[q];
-        const uint64_t nr = std::min<uint64_t>((uint64_t)factor * (p - 1), nq);
-        const double dist = (double)nq / (double)(nr + 1);
-        for (uint64_t i = 1; i <= nr; ++i) {
-            const uint64_t idx = (uint64_t)((double)i * dist);
-            lp.push_back(pb[q] + idx);
-            sindex.push_back(pb[q] + idx);
+    std::vector<uint64_t> lp, sbeg(nsets + 1, 0);
+    for (uint32_t s = 0; s < nsets; ++s) {
+        for (uint32_t q = 0; q < p; ++q) {
+            const uint64_t g = (uint64_t)s * p + q;
+            const uint64_t nq = pb[g + 1] - pb[g];
+            const uint64_t nr = std::min<uint64_t>((uint64_t)factor * (p - 1), nq);
+            const double dist = (double)nq / (double)(nr + 1);
+            for (uint64_t i = 1; i <= nr; ++i) lp.push_back(pb[g] + (uint64_t)((double)i * dist));
         }
+        sbeg[s + 1] = lp.size();
     }
     const uint64_t S = lp.size();
     if (S > L.cap) return fail(DSSS_EINVAL, "partition: sample larger than planned");
-    const uint64_t nspl = std::min<uint64_t>(p - 1, S);
-    if (nspl == 0) {
-        for (uint32_t q = 0; q < p; ++q)
-            for (uint32_t r = 0; r < p; ++r) intervals[(uint64_t)q * p + r] = r == 0 ? pb[q + 1] - pb[q] : 0;
+    // splitters per set: nr' = min(p - 1, the set's sample size)
+    std::vector<uint32_t> nspl(nsets);
+    uint64_t total_spl = 0;
+    for (uint32_t s = 0; s < nsets; ++s) {
+        nspl[s] = (uint32_t)std::min<uint64_t>(p - 1, sbeg[s + 1] - sbeg[s]);
+        total_spl += nspl[s];
+    }
+    if (total_spl == 0) {
+        for (uint64_t g = 0; g < npe; ++g)
+            for (uint32_t r = 0; r < p; ++r) intervals[g * p + r] = r == 0 ? pb[g + 1] - pb[g] : 0;
         return DSSS_OK;
     }
-    DSSS_TRY(ensure_pin(ctx, S * 16 + 64 + (uint64_t)p * p * 8));
+    DSSS_TRY(ensure_pin(ctx, S * 16 + 64 + npe * p * 8));
     uint64_t* hpin = (uint64_t*)ctx->pin;
     std::copy(lp.begin(), lp.end(), hpin);
     DSSS_CUDA(cudaMemcpyAsync(L.sample_lp, hpin, S * 8, cudaMemcpyHostToDevice, st));
     DSSS_LAUNCH("k_sample_gather", st, k_sample_gather<<<grid_for(S, 256), 256, 0, st>>>(a, local_order, dp, L.sample_lp, S, L.soff, L.slen));
     DSSS_CUDA(cudaGetLastError());
     ArenaDev sa{a.chars, L.soff, L.slen, S};
-    uint64_t one[2] = {0, S};
     // sort_strings synchronises on st before reading its counts back, so the
     // sample positions copied above are consumed before hpin is reused.
-    DSSS_TRY(sort_strings(L.sort, sa, S, 1, one, nullptr, L.sorted, L.slcp, 0, (uint32_t*)hpin, st));
+    DSSS_TRY(sort_strings(L.sort, sa, S, nsets, sbeg.data(), nullptr, L.sorted, L.slcp, 0, (uint32_t*)hpin, st));
     uint32_t* hsorted = (uint32_t*)hpin;
     uint64_t* hoff = (uint64_t*)(hpin + (S + 1) / 2 + 1);
     uint32_t* hlen = (uint32_t*)(hoff + S);
@@ -144,35 +153,48 @@ int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_
     DSSS_CUDA(cudaMemcpyAsync(hoff, L.soff, S * 8, cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaMemcpyAsync(hlen, L.slen, S * 4, cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
-    const uint64_t sd = S / (nspl + 1);
-    std::vector<uint64_t> so(nspl), si(nspl), pbv(pb, pb + p + 1);
-    std::vector<uint32_t> sl(nspl);
-    for (uint64_t k = 1; k <= nspl; ++k) {
-        const uint32_t sid = hsorted[k * sd];
-        so[k - 1] = hoff[sid];
-        sl[k - 1] = hlen[sid];
-        si[k - 1] = sindex[sid];
+    const uint32_t stride = p - 1;
+    std::vector<uint64_t> so((uint64_t)nsets * stride), si((uint64_t)nsets * stride), pbv(pb, pb + npe + 1);
+    std::vector<uint32_t> sl((uint64_t)nsets * stride);
+    for (uint32_t s = 0; s < nsets; ++s) {
+        if (!nspl[s]) continue;
+        const uint64_t sd = (sbeg[s + 1] - sbeg[s]) / (nspl[s] + 1);
+        for (uint64_t k = 1; k <= nspl[s]; ++k) {
+            const uint32_t sid = hsorted[sbeg[s] + k * sd];  // sorted ids are sample positions
+            so[(uint64_t)s * stride + k - 1] = hoff[sid];
+            sl[(uint64_t)s * stride + k - 1] = hlen[sid];
+            si[(uint64_t)s * stride + k - 1] = lp[sid];
+        }
     }
-    DSSS_CUDA(cudaMemcpyAsync(L.spl_off, so.data(), nspl * 8, cudaMemcpyHostToDevice, st));
-    DSSS_CUDA(cudaMemcpyAsync(L.spl_len, sl.data(), nspl * 4, cudaMemcpyHostToDevice, st));
-    DSSS_CUDA(cudaMemcpyAsync(L.spl_index, si.data(), nspl * 8, cudaMemcpyHostToDevice, st));
-    DSSS_CUDA(cudaMemcpyAsync(L.pb, pbv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_binsearch", st, k_binsearch<<<grid_for((uint64_t)p * nspl, 128), 128, 0, st>>>(a, local_order, L.pb, p, (uint32_t)nspl, L.spl_off,
-                                                                  L.spl_len, L.spl_index, indexed ? 1 : 0, L.pos));
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_off, so.data(), so.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_len, sl.data(), sl.size() * 4, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.spl_index, si.data(), si.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pbv.data(), (npe + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.set_nspl, nspl.data(), nsets * 4, cudaMemcpyHostToDevice, st));
+    const uint64_t tasks = npe * stride;
+    DSSS_LAUNCH("k_binsearch", st, k_binsearch<<<grid_for(tasks, 128), 128, 0, st>>>(a, local_order, L.pb, (uint32_t)npe, p, L.set_nspl,
+                                                                  L.spl_off, L.spl_len, L.spl_index, indexed ? 1 : 0, L.pos));
     DSSS_CUDA(cudaGetLastError());
-    std::vector<uint64_t> pos((uint64_t)p * nspl);
-    DSSS_CUDA(cudaMemcpyAsync(pos.data(), L.pos, pos.size() * 8, cudaMemcpyDeviceToHost, st));
+    std::vector<uint64_t> pos(tasks);
+    DSSS_CUDA(cudaMemcpyAsync(pos.data(), L.pos, tasks * 8, cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
     // compute_interval_binary (misc.hpp:376-395): differences of the positions
-    for (uint32_t q = 0; q < p; ++q) {
+    for (uint64_t g = 0; g < npe; ++g) {
+        const uint32_t ns = nspl[g / p];
         uint64_t prev = 0;
         for (uint32_t r = 0; r < p; ++r) {
-            uint64_t cur = r < nspl ? pos[(uint64_t)q * nspl + r] : pb[q + 1] - pb[q];
-            intervals[(uint64_t)q * p + r] = cur - prev;
+            uint64_t cur = r < ns ? pos[g * stride + r] : pb[g + 1] - pb[g];
+            intervals[g * p + r] = cur - prev;
             prev = cur;
         }
     }
     return DSSS_OK;
+}
+
+int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_t p, const uint64_t* pb,
+                  const uint32_t* local_order, const uint32_t* dp, uint32_t sampler, uint32_t factor,
+                  uint64_t* intervals, cudaStream_t st) {
+    return partition_sets(L, ctx, a, 1, p, pb, local_order, dp, sampler, factor, intervals, st);
 }
 
 }  // namespace dsss

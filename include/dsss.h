@@ -116,6 +116,22 @@ int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t
 int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                       const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream);
 
+/* Batched form (no reference counterpart: the reference sorts one string set
+ * per MPI job): nsets independent string sets of p PEs each in one arena, run
+ * through one pipeline.  part_begin has nsets*p + 1 entries; PE q of set s
+ * holds ids [part_begin[s*p + q], part_begin[s*p + q + 1]).  Each set's result
+ * is exactly what dsss_pd_sort gives for that set alone: local_order holds
+ * arena ids, perm_pe is the PE inside the set, and set s's merged sequences
+ * fill the positions [part_begin[s*p], part_begin[(s+1)*p]) of perm_index,
+ * perm_pe and merged_lcp.  intervals (HOST, nsets*p*p) and recv_counts (HOST,
+ * nsets*p) hold the sets one after the other.  nsets*p <= 1024. */
+int dsss_pd_sort_batched(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p,
+                         const uint64_t* part_begin, const dsss_opts* opts, dsss_pd_result* out,
+                         dsss_stream_t stream);
+int dsss_pd_sort_batched_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p,
+                              const uint64_t* part_begin, const dsss_opts* opts, dsss_pd_result* out,
+                              dsss_stream_t stream);
+
 /* ---- stages (one per reference seam) ------------------------------------ */
 
 /* tlx::sort_strings_detail::radixsort_CI3(StringLcpPtr, 0, 0)
