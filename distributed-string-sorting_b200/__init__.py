@@ -49,6 +49,24 @@ class PdResult(ctypes.Structure):
                 ("merged_lcp", ctypes.c_void_p), ("recv_counts", ctypes.c_void_p)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("p", ctypes.c_uint32),
+                ("max_sets", ctypes.c_uint32), ("max_batch_strings", ctypes.c_uint64),
+                ("hbm_budget", ctypes.c_uint64), ("opts", Opts)]
+
+
+class RequestStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("batch_sets", ctypes.c_uint32), ("batch_id", ctypes.c_uint64),
+                ("batch_strings", ctypes.c_uint64), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("error", ctypes.c_char * 160)]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_uint64), ("reserved_bytes", ctypes.c_uint64),
+                ("max_reserved_bytes", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("batched_requests", ctypes.c_uint64), ("hbm_budget", ctypes.c_uint64)]
+
+
 _P = ctypes.c_void_p
 _U64 = ctypes.c_uint64
 _U32 = ctypes.c_uint32
@@ -68,6 +86,13 @@ _SIGS = {
                                   ctypes.POINTER(PdResult), _P]),
     "dsss_pd_sort_batched_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
                                        ctypes.POINTER(PdResult), _P]),
+    "dsss_clock_now": (ctypes.c_double, []),
+    "dsss_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    "dsss_server_submit": (_I, [_P, ctypes.POINTER(Arena), _P, ctypes.POINTER(PdResult), ctypes.POINTER(_U64)]),
+    "dsss_server_wait": (_I, [_P, _U64, ctypes.c_int64, ctypes.POINTER(RequestStats)]),
+    "dsss_server_info": (_I, [_P, ctypes.POINTER(ServerInfo)]),
+    "dsss_server_footprint": (_U64, [_P, _U64, _U64]),
+    "dsss_server_destroy": (_I, [_P]),
     "dsss_local_sort_lcp": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), _P, _P, _P]),
     "dsss_dp_prefixes": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "dsss_prefix_hash": (_I, [ctypes.POINTER(Arena), _P, _U64, _U32, _P, _P]),
@@ -403,6 +428,75 @@ def pd_sort_batched_host(ctx: Context, hs: HostStrings, nsets: int, p: int, part
                                           ctypes.byref(_opts(sampler)), ctypes.byref(res), _stream_ptr(stream)))
     out["part_begin"] = pb
     return out
+
+
+def clock_now() -> float:
+    """The server's clock (steady, seconds)."""
+    return float(lib().dsss_clock_now())
+
+
+class Server:
+    """dsss_server: continuous batching of sort requests onto one GPU."""
+
+    def __init__(self, device: int = 0, p: int = 4, workers: int = 2, max_sets: int = 0, max_batch_strings: int = 0,
+                 hbm_budget: int = 0, sampler: int = 0, small_sort_max: int = 0):
+        cfg = ServerConfig(device, workers, p, max_sets, max_batch_strings, hbm_budget, _opts(sampler, 2, small_sort_max))
+        h = ctypes.c_void_p()
+        check(lib().dsss_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.p = p
+        self._live = {}
+
+    def submit(self, hs: HostStrings, part_begin=None, merged_lcp: bool = True, out=None):
+        """Queues one request; returns (ticket, out) with out's host arrays
+        filled once wait(ticket) returns."""
+        n, p = hs.n, self.p
+        if out is None:
+            mk = (lambda: np.empty(max(n, 1), np.uint32))
+            out = dict(local_order=mk(), dp=mk(), perm_index=mk(), perm_pe=mk(),
+                       merged_lcp=mk() if merged_lcp else None, intervals=np.zeros(p * p, np.uint64),
+                       recv_counts=np.zeros(p, np.uint64))
+        pb = None if part_begin is None else np.ascontiguousarray(part_begin, dtype=np.uint64)
+        res = PdResult(_ptr(out["local_order"]), None, _ptr(out["dp"]), _ptr(out["intervals"]),
+                       _ptr(out["perm_index"]), _ptr(out["perm_pe"]), _ptr(out["merged_lcp"]),
+                       _ptr(out["recv_counts"]))
+        a = hs.arena()
+        t = ctypes.c_uint64(0)
+        check(lib().dsss_server_submit(self.h, ctypes.byref(a), _ptr(pb), ctypes.byref(res), ctypes.byref(t)))
+        out["part_begin"] = pb if pb is not None else equal_parts(n, p)
+        self._live[t.value] = (hs, out, pb)
+        return t.value, out
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        st = RequestStats()
+        rc = lib().dsss_server_wait(self.h, ticket, timeout_ms, ctypes.byref(st))
+        if rc == -110:
+            check(rc)
+        self._live.pop(ticket, None)
+        check(rc)
+        return dict(batch_sets=st.batch_sets, batch_id=st.batch_id, batch_strings=st.batch_strings,
+                    t_submit=st.t_submit, t_admit=st.t_admit, t_done=st.t_done,
+                    latency=st.t_done - st.t_submit)
+
+    def info(self) -> dict:
+        i = ServerInfo()
+        check(lib().dsss_server_info(self.h, ctypes.byref(i)))
+        return {k: int(getattr(i, k)) for k, _ in ServerInfo._fields_}
+
+    def footprint(self, n: int, char_bytes: int) -> int:
+        return int(lib().dsss_server_footprint(self.h, n, char_bytes))
+
+    def close(self):
+        if self.h:
+            check(lib().dsss_server_destroy(self.h))
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def local_sort_lcp(ctx: Context, ds: DeviceStrings, p: int = 1, part_begin=None, small_sort_max: int = 0,

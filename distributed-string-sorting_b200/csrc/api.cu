@@ -22,6 +22,7 @@
 #include "internal.cuh"
 #include "merge.cuh"
 #include "partition.cuh"
+#include "pd.cuh"
 #include "strsort.cuh"
 #include "util.cuh"
 
@@ -141,8 +142,15 @@ static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t nsets, uint32_
 // is the one a call on that set alone gives.  Per-string outputs keep the
 // arena's positions (set s's merged sequences fill the positions of its
 // strings), intervals and recv_counts are per set, one after the other.
-static int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* pb,
-                       const dsss_opts* opts, dsss_pd_result* out, cudaStream_t st) {
+uint64_t pd_scratch_bytes(uint64_t n, uint32_t nsets, uint32_t p, const dsss_opts* opts) {
+    Carve sz(nullptr);
+    PdLayout L;
+    layout_pd(sz, L, n, nsets, p, factor_of(opts), smallmax_of(opts));
+    return sz.used;
+}
+
+int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* pb,
+                const dsss_opts* opts, dsss_pd_result* out, cudaStream_t st) {
     DSSS_TRY(check_arena(in));
     if (nsets == 0) return fail(DSSS_EINVAL, "nsets must be >= 1");
     if (p == 0) return fail(DSSS_EINVAL, "p must be >= 1");
@@ -482,7 +490,7 @@ static int pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uin
     Ctx sub = *ctx;
     sub.ws = (char*)ctx->ws + io_bytes;
     sub.ws_cap = ctx->ws_cap - io_bytes;
-    sub.budget = 0;
+    sub.fixed_ws = true;
     int rc = pd_sort_dev(&sub, &da, nsets, p, part_begin, opts, &dr, st);
     ctx->pin = sub.pin;
     ctx->pin_cap = sub.pin_cap;

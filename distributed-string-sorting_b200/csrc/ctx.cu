@@ -57,6 +57,9 @@ int fail(int code, const char* fmt, ...) {
 
 int ensure_ws(Ctx* c, uint64_t bytes) {
     if (bytes <= c->ws_cap) return DSSS_OK;
+    if (c->fixed_ws)
+        return fail(DSSS_ENOMEM, "scratch of %llu bytes exceeds the fixed block of %llu bytes",
+                    (unsigned long long)bytes, (unsigned long long)c->ws_cap);
     if (c->budget && bytes > c->budget)
         return fail(DSSS_ENOMEM, "scratch of %llu bytes exceeds the context budget of %llu bytes",
                     (unsigned long long)bytes, (unsigned long long)c->budget);

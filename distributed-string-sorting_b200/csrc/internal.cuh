@@ -1,6 +1,7 @@
 // Shared internals of libdsss: context, error reporting, scratch carving and
 // the device helpers every kernel uses (big-endian 8-byte key loads, XXH64).
 #pragma once
+#include <atomic>
 
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -51,6 +52,7 @@ struct Ctx {
     uint64_t budget = 0;     // 0 = unlimited
     void* ws = nullptr;      // device scratch, grown on demand
     uint64_t ws_cap = 0;
+    bool fixed_ws = false;   // ws is a block of someone else's buffer: never reallocated
     void* pin = nullptr;     // pinned host staging for small read-backs
     uint64_t pin_cap = 0;
     KernelTimes* times = nullptr;
@@ -108,6 +110,19 @@ struct Carve {
         return p;
     }
 };
+
+// Raises a kernel's dynamic shared-memory limit once per device.  Safe from
+// several host threads: concurrent first calls both set it, which is harmless.
+template <typename K>
+inline int set_smem_once(std::atomic<uint64_t>& done, K* kernel, int bytes) {
+    int dev = 0;
+    DSSS_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return DSSS_OK;
+    DSSS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.fetch_or(bit, std::memory_order_release);
+    return DSSS_OK;
+}
 
 int ensure_ws(Ctx* c, uint64_t bytes);
 int ensure_pin(Ctx* c, uint64_t bytes);

@@ -795,11 +795,8 @@ template <int CAP, int NT>
 static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, const char* name, cudaStream_t st) {
     if (!n) return DSSS_OK;
     constexpr size_t shm = seg_sort_smem<CAP>();
-    static bool configured = false;
-    if (!configured) {
-        DSSS_CUDA(cudaFuncSetAttribute(k_seg_sort<CAP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    DSSS_TRY(set_smem_once(configured, k_seg_sort<CAP, NT>, (int)shm));
     DSSS_LAUNCH(name, st, k_seg_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
@@ -863,11 +860,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.cap_tiles = L.cap_tiles;
     S.cap_chunks = L.cap_chunks;
 
-    static bool scatter_configured = false;
-    if (!scatter_configured) {
-        DSSS_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SCATTER_SMEM));
-        scatter_configured = true;
-    }
+    static std::atomic<uint64_t> scatter_configured{0};
+    DSSS_TRY(set_smem_once(scatter_configured, k_scatter, (int)SCATTER_SMEM));
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb_host, (p + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     DSSS_LAUNCH("k_init_ids", st, k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n));

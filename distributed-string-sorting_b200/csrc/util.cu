@@ -271,13 +271,9 @@ __global__ void __launch_bounds__(MS_NT) k_ms_scatter_pay(const uint32_t* bucket
 template <int NPAY>
 static int launch_ms_pay(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles, const uint32_t* off,
                          const Payload& pl, uint32_t* rank_out, uint32_t* err, cudaStream_t st) {
-    static uint32_t configured_p = 0;
+    static std::atomic<uint64_t> configured{0};
     const size_t sm = msp_smem<NPAY>(P);
-    if (configured_p < P) {
-        DSSS_CUDA(cudaFuncSetAttribute(k_ms_scatter_pay<NPAY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)msp_smem<NPAY>(MAX_SPLIT_BUCKETS)));
-        configured_p = MAX_SPLIT_BUCKETS;
-    }
+    DSSS_TRY(set_smem_once(configured, k_ms_scatter_pay<NPAY>, (int)msp_smem<NPAY>(MAX_SPLIT_BUCKETS)));
     DSSS_LAUNCH("k_ms_scatter_pay", st,
                 k_ms_scatter_pay<NPAY><<<(unsigned)tiles, MS_NT, sm, st>>>(bucket, n, P, tiles, off, pl, rank_out, err));
     return DSSS_OK;
@@ -327,12 +323,8 @@ int multisplit(const uint32_t* bucket, uint64_t n, uint32_t P, uint32_t* dest, v
     uint32_t* off = c.take<uint32_t>(cells);
     void* sc = c.take<unsigned char>(scan_scratch_bytes(cells));
     size_t sh1 = P * sizeof(uint32_t), sh2 = (size_t)P * (1 + MS_NT / 32) * sizeof(uint32_t);
-    static bool configured = false;
-    if (!configured) {
-        DSSS_CUDA(cudaFuncSetAttribute(k_ms_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(MAX_SPLIT_BUCKETS * (1 + MS_NT / 32) * sizeof(uint32_t))));
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    DSSS_TRY(set_smem_once(configured, k_ms_scatter, (int)(MAX_SPLIT_BUCKETS * (1 + MS_NT / 32) * sizeof(uint32_t))));
     DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, sh1, st>>>(bucket, n, P, tiles, hist));
     DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
     DSSS_LAUNCH("k_ms_scatter", st, k_ms_scatter<<<(unsigned)tiles, MS_NT, sh2, st>>>(bucket, n, P, tiles, off, dest));

@@ -237,6 +237,62 @@ int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order
 int dsss_adjacent_lcp_noalloc(const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
                               dsss_stream_t stream);
 
+/* ---- request server (no reference counterpart) ---------------------------
+ * Continuous batching of independent sort requests onto one GPU.  Requests
+ * (host arenas, p PEs each) are queued on submit; worker threads, each with
+ * its own stream, take the requests at the head of the queue that fit one
+ * batch and the device-memory budget and run them as one
+ * dsss_pd_sort_batched call, several batches in flight at once.  Device
+ * memory comes from a pool that keeps freed blocks resident up to the budget;
+ * a batch is admitted only if its exact footprint (arena, outputs, pipeline
+ * scratch) fits beside the batches in flight.  Each request's result equals
+ * dsss_pd_sort_host on that request alone.  Input and output host buffers
+ * must stay valid until dsss_server_wait returns for the ticket. */
+typedef struct dsss_server dsss_server;
+
+typedef struct {
+    int device;
+    uint32_t workers;           /* batches in flight at once; 0 -> 2 */
+    uint32_t p;                 /* PEs per request (1..1024) */
+    uint32_t max_sets;          /* requests per batch; 0 -> 1024 / p (also capped there) */
+    uint64_t max_batch_strings; /* strings per batch beyond its first request; 0 -> no limit */
+    uint64_t hbm_budget;        /* device bytes the server may hold; 0 -> 150e9 */
+    dsss_opts opts;
+} dsss_server_config;
+
+typedef struct {
+    int status;                 /* DSSS_OK or the batch's error */
+    uint32_t batch_sets;        /* requests in the batch this one ran in */
+    uint64_t batch_id;
+    uint64_t batch_strings;
+    double t_submit, t_admit, t_done; /* seconds, dsss_clock_now() */
+    char error[160];
+} dsss_request_stats;
+
+typedef struct {
+    uint64_t queued;
+    uint64_t reserved_bytes;     /* footprints of the batches in flight */
+    uint64_t max_reserved_bytes; /* the most ever reserved at once (<= hbm_budget) */
+    uint64_t batches;
+    uint64_t batched_requests;
+    uint64_t hbm_budget;
+} dsss_server_info_t;
+
+double dsss_clock_now(void);
+int dsss_server_create(const dsss_server_config* cfg, dsss_server** out);
+/* part_begin: p + 1 PE bounds of the request, or NULL for p equal slices.
+ * out: host arrays as for dsss_pd_sort_host. */
+int dsss_server_submit(dsss_server* s, const dsss_arena* in, const uint64_t* part_begin, dsss_pd_result* out,
+                       uint64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit; DSSS_ETIMEDOUT keeps the
+ * ticket valid), fills stats and releases the ticket; returns its status. */
+int dsss_server_wait(dsss_server* s, uint64_t ticket, int64_t timeout_ms, dsss_request_stats* stats);
+int dsss_server_info(dsss_server* s, dsss_server_info_t* info);
+/* Device bytes a request of n strings and char_bytes bytes needs alone. */
+uint64_t dsss_server_footprint(dsss_server* s, uint64_t n, uint64_t char_bytes);
+/* Finishes every queued request, then stops the workers. */
+int dsss_server_destroy(dsss_server* s);
+
 /* ---- synthetic inputs (host) --------------------------------------------- */
 
 /* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared():
     with open(os.path.join(ROOT, "include", "dsss.h")) as f:
         src = f.read()
-    return sorted(set(re.findall(r"^\s*(?:int|uint64_t|const char\*)\s+(dsss_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|uint64_t|double|const char\*)\s+(dsss_\w+)\s*\(", src, re.M)))
 
 
 def test_header_symbols_exported(dsss):
