@@ -111,6 +111,112 @@ def cpu_baseline_port(n_sample, L, k, p, seed):
     return hs.n / (time.perf_counter() - t)
 
 
+def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
+    """Suffix instances (all suffixes, truncated to 256 B, of seeded order-3
+    Markov ACGT texts with 1% copied 1-4 KiB blocks): nsets texts of `text`
+    bytes sorted as one dsss_pd_sort_batched call vs one dsss_pd_sort call per
+    instance, inputs resident in HBM, device-timed."""
+    sets = [d.gen_suffix_strings(text, 256, seed=100 + k) for k in range(nsets)]
+    hs, sb = d.concat_sets(sets)
+    pb = d.batched_parts(sb, p)
+    ds_all = d.DeviceStrings(hs)
+    ds_each = [d.DeviceStrings(h) for h in sets]
+    ctx = d.Context(torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    n = hs.n
+    out, outs = None, [None] * nsets
+
+    def batched():
+        nonlocal out
+        out = d.pd_sort_batched(ctx, ds_all, nsets, p, pb, out=out)
+
+    def plain():
+        for k in range(nsets):
+            outs[k] = d.pd_sort(ctx, ds_each[k], p, out=outs[k])
+
+    res = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / steps
+    # the batched result equals the per-instance results
+    same = all(np.array_equal(out["dp"][int(sb[k]):int(sb[k + 1])].cpu().numpy(),
+                              outs[k]["dp"][:sets[k].n].cpu().numpy()) for k in range(nsets))
+    char_bytes = int(hs.lengths.astype(np.uint64).sum()) + n
+    ctx.close()
+    return {
+        "workload": f"{nsets} x {text >> 20} MiB-text suffix instances (x 256 B max), p = {p} each",
+        "strings": n, "char_bytes": char_bytes, "steps": steps,
+        "plain_ms": res["plain"], "batched_ms": res["batched"],
+        "plain_strings_per_s": n / (res["plain"] * 1e-3), "batched_strings_per_s": n / (res["batched"] * 1e-3),
+        "batched_char_gbs": char_bytes / (res["batched"] * 1e-3) / 1e9,
+        "speedup": res["plain"] / res["batched"], "dp_identical": bool(same),
+    }
+
+
+def bench_serving(d, torch, p=8, n_req=48, rate=60.0, seed=2024):
+    """Sort requests through dsss_server: n log-uniform in [1e3, 4e6], lengths
+    Zipf(1.2) on [8, 256], bytes 0x21-0x7E after a shared random prefix; host
+    buffers pinned.  Saturated throughput (all requests queued at once) and
+    latency under seeded Poisson arrivals at `rate` requests/s, for continuous
+    batching (3 workers) and for the plain per-request path (1 worker, one
+    request per batch = dsss_pd_sort_host per request)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(4e6), size=n_req)).astype(np.int64)
+    reqs = [d.gen_request(int(n), seed=seed * 1000 + k, pinned=True) for k, n in enumerate(ns)]
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    total = int(ns.sum())
+    outs = []
+    for h in reqs:
+        mk = (lambda: d._alloc_host(max(h.n, 1) * 4, np.uint32, True)[:max(h.n, 1)])
+        outs.append(dict(local_order=mk(), dp=mk(), perm_index=mk(), perm_pe=mk(), merged_lcp=mk(),
+                         intervals=np.zeros(p * p, np.uint64), recv_counts=np.zeros(p, np.uint64)))
+
+    def run(workers, max_sets, paced):
+        srv = d.Server(torch.cuda.current_device(), p=p, workers=workers, max_sets=max_sets)
+        for h, o in list(zip(reqs, outs))[:4]:  # warm-up
+            srv.wait(srv.submit(h, out=o)[0])
+        t0 = d.clock_now()
+        tickets = []
+        for k, (h, o) in enumerate(zip(reqs, outs)):
+            if paced:
+                dt = t0 + arrivals[k] - d.clock_now()
+                if dt > 0:
+                    time.sleep(dt)
+            tickets.append(srv.submit(h, out=o)[0])
+        st = [srv.wait(t) for t in tickets]
+        info = srv.info()
+        srv.close()
+        lat = np.array([s["latency"] for s in st]) * 1e3
+        span = max(s["t_done"] for s in st) - min(s["t_submit"] for s in st)
+        return {"strings_per_s": total / span, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_batch": info["batched_requests"] / info["batches"],
+                "max_reserved_gb": info["max_reserved_bytes"] / 1e9}
+
+    served_sat = run(3, 0, False)
+    plain_sat = run(1, 1, False)
+    served = run(3, 0, True)
+    plain = run(1, 1, True)
+    return {
+        "workload": f"{n_req} requests, n log-uniform [1e3, 4e6] (total {total}), p = {p}, Poisson {rate}/s (seed {seed})",
+        "hbm_budget_gb": 150,
+        "served": {"saturated_strings_per_s": served_sat["strings_per_s"], "p50_ms": served["p50_ms"],
+                   "p99_ms": served["p99_ms"], "paced_strings_per_s": served["strings_per_s"],
+                   "mean_batch": served_sat["mean_batch"], "max_reserved_gb": served_sat["max_reserved_gb"]},
+        "plain": {"saturated_strings_per_s": plain_sat["strings_per_s"], "p50_ms": plain["p50_ms"],
+                  "p99_ms": plain["p99_ms"], "paced_strings_per_s": plain["strings_per_s"]},
+        "speedup_saturated": served_sat["strings_per_s"] / plain_sat["strings_per_s"],
+    }
+
+
 def run_reference(args, cfg):
     """--impl reference: the CPU port of the reference path on all host threads."""
     import __graft_entry__
@@ -159,6 +265,8 @@ def main():
     ap.add_argument("--config", default="dn32m", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
@@ -268,6 +376,17 @@ def main():
         cpu = {"value": cpu_baseline_port(sample, L, k, p, seed=1), "unit": "strings/s", "cores": 1, "kind": "port",
                "sample": f"{sample} strings of the same rule, p = {p}, oracle port single-threaded"}
 
+    ctx.close()
+    del ds, out
+    torch.cuda.empty_cache()
+    # batched and served forms: reported on the one-GPU line
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = bench_batched(d, torch, max(3, min(args.steps, 10)), 3)
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = bench_serving(d, torch)
+
     if rank == 0:
         line = {
             "metric": "strings/s", "value": value, "unit": "strings/s", "n_gpus": world, "steps": args.steps,
@@ -288,9 +407,10 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -12,6 +12,12 @@
 //   hist     : warp-aggregated 256-bin histogram of that byte per 4096-element tile;
 //   scan     : per segment, bucket starts and per-tile offsets (chunked);
 //   scatter  : stable scatter of ids (and keys of children that stay large).
+// A child that keeps more than half of its parent (a chain of long shared
+// prefixes, e.g. suffixes inside repeats or strings that share a long common
+// head) would lose one byte per pass; it is flagged for a pivot pass instead:
+// every string's LCP with the segment's first string (up to 127 bytes) and
+// the byte after it become a two-byte pseudo key whose order is the strings'
+// order, so one pass resolves up to 127 bytes of the chain.
 // Children of size <= small_max finish in one CTA (small_sort): bitonic sort
 // of (group, key, id) in shared memory, tie groups re-keyed 8 bytes deeper
 // until every group is a single string or byte-identical strings.
@@ -28,7 +34,10 @@ namespace dsss {
 constexpr int LT_NT = 256, LT_IPT = 16, LT_TILE = LT_NT * LT_IPT;
 constexpr int CHUNK_TILES = 32;
 constexpr uint32_t PREFIX_CAP = 256;
-constexpr uint32_t F_PARITY = 1u, F_KEYS = 2u;
+// F_KEYS: the key array holds the segment's keys at Seg.depth; F_PIVOT: the
+// next pass is a pivot pass; F_PSEUDO: the keys are pivot pseudo keys.
+constexpr uint32_t F_PARITY = 1u, F_KEYS = 2u, F_PIVOT = 4u, F_PSEUDO = 8u;
+constexpr uint32_t PIVOT_CAP = 127;  // pseudo key byte 0 holds codes 0 .. 2 * PIVOT_CAP
 
 struct Seg {
     uint32_t start, size, depth, flags;
@@ -147,7 +156,7 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
     Seg& sg = segs[si];
-    if (sg.flags & F_KEYS) return;
+    if (sg.flags & (F_KEYS | F_PIVOT)) return;
     const uint32_t par = sg.flags & F_PARITY;
     const uint32_t* ord = S.ord[par];
     const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
@@ -208,6 +217,7 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
     Seg& sg = segs[si];
+    if (sg.flags & F_PIVOT) return;  // keys and diff come from k_pivot
     const uint32_t par = sg.flags & F_PARITY;
     const bool valid = sg.flags & F_KEYS;
     const uint32_t depth = valid ? sg.depth : sg.newdepth;
@@ -253,6 +263,87 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
                 }
             }
         }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(0xffffffffu, df, o);
+    if ((threadIdx.x & 31) == 0 && df) atomicOr(&sg.diff, (unsigned long long)df);
+}
+
+// ----------------------------------------------------------------- pivot ----
+// Pivot pass of an F_PIVOT segment at depth d (all its strings share their
+// first d bytes) with s0 its first string.  For string x, l = LCP(x, s0)
+// counted from d and capped at PIVOT_CAP, and x's pseudo key holds
+//   byte 0: code = l            if x < s0 (x's byte at l is smaller: x ends
+//                               there or differs downwards),
+//                = PIVOT_CAP    if x matches s0 for PIVOT_CAP bytes or equals it,
+//                = 2*PIVOT_CAP - l  if x > s0;
+//   byte 1: x's byte at d + l (0 for the code PIVOT_CAP).
+// Ascending pseudo keys are ascending strings: two strings below s0 with
+// different l compare at the smaller l, where the one with the smaller l has
+// the smaller byte; above s0 the larger l comes first; equal codes compare by
+// the byte at d + l.  Strings with the same pseudo key share their first
+// d + l + 1 bytes (d + PIVOT_CAP for the middle code), and the LCP of two
+// strings with different codes is d + min(l, l').
+__device__ __forceinline__ uint32_t pivot_l(uint32_t code) { return code <= PIVOT_CAP ? code : 2 * PIVOT_CAP - code; }
+
+// Pseudo key of string (off, len) against the pivot (off0, len0), both
+// sharing their first d0 bytes.
+__device__ __forceinline__ uint64_t pivot_key(const uint8_t* chars, uint64_t off, uint32_t len, uint64_t off0,
+                                              uint32_t len0, uint32_t d0) {
+    uint32_t code = PIVOT_CAP, byte = 0;
+    bool done = false;
+    for (uint32_t c = 0; c < PIVOT_CAP && !done; c += 16) {
+        // 16 bytes per step: two independent 8-byte compares
+        uint64_t x[2], y[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            x[q] = key8(chars, off, len, d0 + c + 8 * q);
+            y[q] = key8(chars, off0, len0, d0 + c + 8 * q);
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (done) continue;
+            if (x[q] != y[q]) {
+                const uint32_t j = key_lcp(x[q], y[q]);
+                const uint32_t l = c + 8 * q + j;
+                if (l < PIVOT_CAP) {
+                    const uint32_t bx = (uint32_t)(x[q] >> (56 - 8 * j)) & 0xFFu;
+                    const uint32_t by = (uint32_t)(y[q] >> (56 - 8 * j)) & 0xFFu;
+                    code = bx < by ? l : 2 * PIVOT_CAP - l;
+                    byte = bx;
+                }
+                done = true;
+            } else if (zero_byte(x[q]) < 8) {
+                done = true;  // equal to the pivot
+            }
+        }
+    }
+    return (uint64_t)code << 56 | (uint64_t)byte << 48;
+}
+
+__global__ void __launch_bounds__(LT_NT) k_pivot(SortState S, Seg* segs, uint32_t nseg) {
+    const uint32_t t = blockIdx.x;
+    if (t >= S.counters[8]) return;
+    const uint32_t si = find_seg(S.tile0, nseg, t);
+    Seg& sg = segs[si];
+    if (!(sg.flags & F_PIVOT)) return;
+    const uint32_t par = sg.flags & F_PARITY;
+    const uint32_t* ord = S.ord[par];
+    unsigned long long* key = S.key[par];
+    const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
+    const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
+    uint64_t off0;
+    uint32_t len0;
+    str_of(S.a, ord[sg.start], off0, len0);
+    const uint64_t k0 = (uint64_t)PIVOT_CAP << 56;
+    uint64_t df = 0;
+    for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
+        uint64_t off;
+        uint32_t len;
+        str_of(S.a, ord[i], off, len);
+        const uint64_t k = pivot_key(S.a.chars, off, len, off0, len0, sg.depth);
+        key[i] = k;
+        df |= k ^ k0;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(0xffffffffu, df, o);
@@ -308,21 +399,41 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
     const uint32_t si = blockIdx.x;
     Seg& sg = segs[si];
     const uint32_t par = sg.flags & F_PARITY;
-    const uint32_t depth = (sg.flags & F_KEYS) ? sg.depth : sg.newdepth;
+    const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
+    const uint32_t depth = (sg.flags & (F_KEYS | F_PIVOT)) ? sg.depth : sg.newdepth;
     const uint32_t d = threadIdx.x;
     if (sg.diff == 0) {
-        // Every key equal: byte-identical strings if the key holds the end,
-        // else look 8 bytes deeper.
+        // Every key equal: byte-identical strings if the key holds their end,
+        // else continue deeper without keys.
         const uint64_t k0 = S.key[par][sg.start];
-        const uint32_t z = zero_byte(k0);
-        if (z < 8) {
-            const uint32_t* ord = S.ord[par];
+        const uint32_t* ord = S.ord[par];
+        uint32_t fin = 0xFFFFFFFFu, cont = 0, cflags = par;
+        if (pseudo) {
+            const uint32_t code = (uint32_t)(k0 >> 56), byte = (uint32_t)(k0 >> 48) & 0xFFu;
+            if (code == PIVOT_CAP) {
+                uint64_t o0;
+                uint32_t l0;
+                str_of(S.a, ord[sg.start], o0, l0);
+                if (l0 < depth + PIVOT_CAP) fin = l0;  // all equal the pivot
+                else cont = depth + PIVOT_CAP;
+            } else if (byte == 0) {
+                fin = depth + pivot_l(code);  // all end where they leave the pivot
+            } else {
+                cont = depth + pivot_l(code) + 1;
+            }
+            cflags |= F_PIVOT;
+        } else {
+            const uint32_t z = zero_byte(k0);
+            if (z < 8) fin = depth + z;
+            else cont = depth + 8;
+        }
+        if (fin != 0xFFFFFFFFu) {
             for (uint32_t i = threadIdx.x; i < sg.size; i += blockDim.x) {
                 S.ord_out[sg.start + i] = ord[sg.start + i];
-                if (i) S.lcp_out[sg.start + i] = depth + z;
+                if (i) S.lcp_out[sg.start + i] = fin;
             }
         } else if (threadIdx.x == 0) {
-            push_large(S, next, sg.start, sg.size, depth + 8, par);
+            push_large(S, next, sg.start, sg.size, cont, cflags);
         }
         return;
     }
@@ -361,11 +472,42 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
         sg.first_digit = s_first;
         sg.depth = depth;
     }
-    if (total >= 2 && d != 0) {
-        const uint32_t cs = sg.start + excl;
-        // children keep the parent's keys: their first b+1 key bytes are now common
-        if (total > S.small_max) push_large(S, next, cs, total, depth, (par ^ 1u) | F_KEYS);
-        else push_small(S, cs, total, depth, (par ^ 1u) | F_KEYS);
+    if (total < 2) return;
+    const uint32_t cs = sg.start + excl;
+    const uint32_t np = par ^ 1u;
+    if (!pseudo) {
+        if (d == 0) return;  // strings that end here: written by the scatter
+        // children keep the parent's keys: their first b+1 key bytes are now
+        // common; one that keeps most of the parent gets a pivot pass
+        if (total > S.small_max) {
+            if (2 * (uint64_t)total > sg.size) push_large(S, next, cs, total, depth + b + 1, np | F_PIVOT);
+            else push_large(S, next, cs, total, depth, np | F_KEYS);
+        } else {
+            push_small(S, cs, total, depth, np | F_KEYS);
+        }
+    } else if (b == 0) {
+        // split by pivot code (only the pivot pass's own segment, whose first
+        // string is the pivot): large children keep the pseudo keys, small
+        // ones restart from the depth their strings share
+        if (total > S.small_max) {
+            push_large(S, next, cs, total, depth, np | F_KEYS | F_PSEUDO);
+        } else {
+            uint32_t cd = depth + pivot_l(d);
+            if (d == PIVOT_CAP) {
+                uint64_t o0;
+                uint32_t l0;
+                str_of(S.a, S.ord[par][sg.start], o0, l0);
+                cd = min(depth + PIVOT_CAP, l0);
+            }
+            push_small(S, cs, total, cd, np);
+        }
+    } else {
+        // split by the byte after the shared d + l bytes; byte 0: strings that
+        // end there, written by the scatter
+        if (d == 0) return;
+        const uint32_t cd = depth + pivot_l((uint32_t)(S.key[par][sg.start] >> 56)) + 1;
+        if (total > S.small_max) push_large(S, next, cs, total, cd, np | (2 * (uint64_t)total > sg.size ? F_PIVOT : 0u));
+        else push_small(S, cs, total, cd, np);
     }
 }
 
@@ -394,6 +536,11 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
     const uint32_t b = (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t shift = 56 - 8 * b;
     const uint32_t depth = sg.depth;
+    const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
+    // LCP inside the group of strings that end here and at bucket starts
+    // (pivot code splits: d + min(l, l') from the two codes)
+    const bool code_split = pseudo && b == 0;
+    const uint32_t lcp_here = pseudo ? depth + pivot_l((uint32_t)(S.key[par][sg.start] >> 56)) : depth + b;
     const uint32_t tloc = t - S.tile0[si];
     const uint32_t c = S.chunk0[si] + tloc / CHUNK_TILES;
     const uint32_t tfirst = t - tloc % CHUNK_TILES;
@@ -487,14 +634,23 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
             continue;
         }
         const uint32_t oo = sord[x];
-        if (dg == 0 || cnt == 1) {
+        const bool ended = dg == 0 && !code_split;
+        if (ended || cnt == 1) {
             S.ord_out[dest] = oo;
-            if (dg == 0 && dest != bs) S.lcp_out[dest] = depth + b;
+            if (ended && dest != bs) S.lcp_out[dest] = lcp_here;
         } else {
             ord_dst[dest] = oo;
             key_dst[dest] = skey[x];
         }
-        if (dest == bs && dg != sg.first_digit) S.lcp_out[dest] = depth + b;
+        if (dest == bs && dg != sg.first_digit) {
+            uint32_t l = lcp_here;
+            if (code_split) {
+                uint32_t pd = dg - 1;  // previous non-empty code (exists: dg is not the first)
+                while (pd > 0 && bstart[pd] == bs) --pd;
+                l = depth + min(pivot_l(dg), pivot_l(pd));
+            }
+            S.lcp_out[dest] = l;
+        }
     }
 }
 
@@ -562,8 +718,29 @@ __device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint
         const bool unres = valid && multi && zero_byte(key) == 8;
         if (valid) grp = rs;
         if (!__any_sync(FULL, unres)) break;
+        // Every unresolved run shares its 8-byte key: jump to the first depth
+        // where a member differs from the run head (or ends), the minimum over
+        // the run of each member's LCP with the head.
+        const uint32_t hid = __shfl_sync(FULL, id, rs);
+        uint32_t l = 0xFFFFFFFFu;
+        if (unres && (uint32_t)lane != rs) {
+            uint64_t off, offh;
+            uint32_t len, lenh;
+            str_of(a, id, off, len);
+            str_of(a, hid, offh, lenh);
+            for (uint32_t d = dep + 8;; d += 16) {
+                const uint64_t x0 = key8(a.chars, off, len, d), y0 = key8(a.chars, offh, lenh, d);
+                const uint64_t x1 = key8(a.chars, off, len, d + 8), y1 = key8(a.chars, offh, lenh, d + 8);
+                if (x0 != y0) { l = d + key_lcp(x0, y0); break; }
+                if (zero_byte(x0) < 8) { l = d + zero_byte(x0); break; }
+                if (x1 != y1) { l = d + 8 + key_lcp(x1, y1); break; }
+                if (zero_byte(x1) < 8) { l = d + 8 + zero_byte(x1); break; }
+            }
+        }
+        const uint32_t run = __match_any_sync(FULL, unres ? rs : 32u + (uint32_t)lane);
+        const uint32_t nd = __reduce_min_sync(run, l);
         if (unres) {
-            dep += 8;
+            dep = nd;
             key = key8_of(a, id, dep);
         }
     }
@@ -592,6 +769,12 @@ constexpr size_t seg_sort_smem() {
     return (size_t)CAP * (8 + 8 + 4 + 4 + 4) + (size_t)(CAP / 2) * 3 * 4 * 2;
 }
 
+// Bucket flags inside k_seg_sort, packed above the 16-bit bucket size: the
+// keys must be gathered at the bucket depth first (SF_REKEY), a pivot pass is
+// due (SF_PIVOT), or the keys are pivot pseudo keys whose base depth is the
+// bucket depth (SF_PSEUDO).
+constexpr uint32_t SF_REKEY = 1u, SF_PIVOT = 2u, SF_PSEUDO = 4u;
+
 template <int CAP, int NT>
 __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg) {
     constexpr int NW = NT / 32;
@@ -601,8 +784,8 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     uint32_t* so = (uint32_t*)(tk + CAP);
     uint32_t* to = so + CAP;
     uint32_t* pk = to + CAP;  // digit << 24 | rank within the warp's chunk
-    uint32_t* stk = pk + CAP;  // (start, size, depth) of buckets > 32
-    uint32_t* wl = stk + 3 * (CAP / 2);  // (start, size, depth) of buckets <= 32
+    uint32_t* stk = pk + CAP;  // (start, size | flags << 16, depth) of buckets > 32
+    uint32_t* wl = stk + 3 * (CAP / 2);  // (start, size | flags << 16, depth) of buckets <= 32
     __shared__ uint32_t hist[256], bstart[256];
     __shared__ uint32_t wcnt[NW][256];
     __shared__ uint32_t s_top, s_nw, s_cur[3];
@@ -651,8 +834,27 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
             }
         }
         __syncthreads();
-        const uint32_t bs = s_cur[0], bn = s_cur[1], dep = s_cur[2];
+        const uint32_t bs = s_cur[0], bn = s_cur[1] & 0xFFFFu, dep = s_cur[2];
+        uint32_t fl = s_cur[1] >> 16;
         if (bn == 0) break;
+        if (fl & SF_REKEY) {
+            for (uint32_t i = threadIdx.x; i < bn; i += NT) sk[bs + i] = key8_of(S.a, so[bs + i], dep);
+            fl = 0;
+            __syncthreads();
+        } else if (fl & SF_PIVOT) {
+            uint64_t off0;
+            uint32_t len0;
+            str_of(S.a, so[bs], off0, len0);
+            for (uint32_t i = threadIdx.x; i < bn; i += NT) {
+                uint64_t off;
+                uint32_t len;
+                str_of(S.a, so[bs + i], off, len);
+                sk[bs + i] = pivot_key(S.a.chars, off, len, off0, len0, dep);
+            }
+            fl = SF_PSEUDO;
+            __syncthreads();
+        }
+        const bool pseudo = fl & SF_PSEUDO;
         const uint64_t k0 = sk[bs];
         uint64_t df = 0;
         for (uint32_t i = threadIdx.x; i < bn; i += NT) df |= sk[bs + i] ^ k0;
@@ -662,20 +864,35 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
         __syncthreads();
         df = s_diff;
         if (df == 0) {
-            const uint32_t z = zero_byte(k0);
-            if (z < 8) {
-                for (uint32_t i = threadIdx.x + 1; i < bn; i += NT) lcp[bs + i] = dep + z;
+            // one key for the whole bucket: byte-identical strings (their LCP
+            // is their length), or continue deeper
+            uint32_t fin = 0xFFFFFFFFu, cont = 0, cfl = SF_REKEY;
+            if (pseudo) {
+                const uint32_t code = (uint32_t)(k0 >> 56), byte = (uint32_t)(k0 >> 48) & 0xFFu;
+                if (code == PIVOT_CAP) {
+                    uint64_t o0;
+                    uint32_t l0;
+                    str_of(S.a, so[bs], o0, l0);
+                    if (l0 < dep + PIVOT_CAP) fin = l0;
+                    else cont = dep + PIVOT_CAP;
+                } else if (byte == 0) {
+                    fin = dep + pivot_l(code);
+                } else {
+                    cont = dep + pivot_l(code) + 1;
+                }
+                cfl = SF_PIVOT;
             } else {
-                for (uint32_t i = threadIdx.x; i < bn; i += NT) {
-                    const uint32_t o = so[bs + i];
-                    sk[bs + i] = key8_of(S.a, o, dep + 8);
-                }
-                if (threadIdx.x == 0) {
-                    stk[3 * s_top] = bs;
-                    stk[3 * s_top + 1] = bn;
-                    stk[3 * s_top + 2] = dep + 8;
-                    ++s_top;
-                }
+                const uint32_t z = zero_byte(k0);
+                if (z < 8) fin = dep + z;
+                else cont = dep + 8;
+            }
+            if (fin != 0xFFFFFFFFu) {
+                for (uint32_t i = threadIdx.x + 1; i < bn; i += NT) lcp[bs + i] = fin;
+            } else if (threadIdx.x == 0) {
+                stk[3 * s_top] = bs;
+                stk[3 * s_top + 1] = bn | (cfl << 16);
+                stk[3 * s_top + 2] = cont;
+                ++s_top;
             }
             __syncthreads();
             if (threadIdx.x == 0) s_diff = 0;
@@ -750,39 +967,81 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
             sk[bs + i] = tk[bs + i];
             so[bs + i] = to[bs + i];
         }
+        __syncthreads();
+        // split by pivot code, by the byte after a pivot code's shared
+        // prefix, or by a plain key byte
+        const bool code_split = pseudo && b == 0;
+        const uint32_t lin = pseudo ? dep + pivot_l((uint32_t)(k0 >> 56)) : dep + b;
         for (uint32_t d = threadIdx.x; d < 256; d += NT) {
             const uint32_t cnt = hist[d];
             if (!cnt) continue;
             const uint32_t c0 = bs + bstart[d];
-            if (c0 != bs) lcp[c0] = dep + b;  // boundary to the previous non-empty bucket
-            if (d == 0) {  // strings that end here: byte-identical
-                for (uint32_t k = 1; k < cnt; ++k) lcp[c0 + k] = dep + b;
-            } else if (cnt >= 2) {
-                uint32_t* dst;
-                uint32_t slot;
-                if (cnt <= 32) {
-                    slot = atomicAdd(&s_nw, 1u);
-                    dst = wl + 3 * slot;
-                } else {
-                    slot = atomicAdd(&s_top, 1u);
-                    dst = stk + 3 * slot;
+            if (c0 != bs) {  // boundary to the previous non-empty bucket
+                uint32_t l = lin;
+                if (code_split) {
+                    uint32_t pd = d - 1;
+                    while (pd > 0 && bstart[pd] == bstart[d]) --pd;
+                    l = dep + min(pivot_l(d), pivot_l(pd));
                 }
-                dst[0] = c0;
-                dst[1] = cnt;
-                dst[2] = dep;
+                lcp[c0] = l;
             }
+            if (d == 0 && !code_split) {  // strings that end here: byte-identical
+                for (uint32_t k = 1; k < cnt; ++k) lcp[c0 + k] = lin;
+                continue;
+            }
+            if (cnt < 2) continue;
+            uint32_t cd, cf;
+            if (!pseudo) {
+                if (cnt > 32 && 2 * cnt > bn) {
+                    cd = dep + b + 1;  // keeps most of the bucket: pivot pass next
+                    cf = SF_PIVOT;
+                } else {
+                    cd = dep;
+                    cf = 0;
+                }
+            } else if (code_split) {
+                if (cnt > 32) {
+                    cd = dep;
+                    cf = SF_PSEUDO;
+                } else {
+                    cd = dep + pivot_l(d);
+                    if (d == PIVOT_CAP) {
+                        uint64_t o0;
+                        uint32_t l0;
+                        str_of(S.a, so[c0], o0, l0);
+                        cd = min(dep + PIVOT_CAP, l0);
+                    }
+                    cf = SF_REKEY;
+                }
+            } else {
+                cd = lin + 1;
+                cf = (cnt > 32 && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
+            }
+            uint32_t* dst;
+            uint32_t slot;
+            if (cnt <= 32) {
+                slot = atomicAdd(&s_nw, 1u);
+                dst = wl + 3 * slot;
+            } else {
+                slot = atomicAdd(&s_top, 1u);
+                dst = stk + 3 * slot;
+            }
+            dst[0] = c0;
+            dst[1] = cnt | (cf << 16);
+            dst[2] = cd;
         }
         if (threadIdx.x == 0) s_diff = 0;
         __syncthreads();
     }
     const uint32_t nwl = s_nw;
     for (uint32_t e = w; e < nwl; e += NW) {
-        const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1], wd = wl[3 * e + 2];
+        const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1] & 0xFFFFu, wd = wl[3 * e + 2];
+        const bool rekey = (wl[3 * e + 1] >> 16) & SF_REKEY;
         uint64_t key = 0;
         uint32_t id = 0;
         if ((uint32_t)lane < wn) {
-            key = sk[ws + lane];
             id = so[ws + lane];
+            key = rekey ? key8_of(S.a, id, wd) : sk[ws + lane];
         }
         warp_sort(S.a, wn, wd, key, id, lcp + ws);
         if ((uint32_t)lane < wn) so[ws + lane] = id;
@@ -888,6 +1147,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
         S.large[0] = segs;
         DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        DSSS_LAUNCH("k_pivot", st, k_pivot<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_hist", st, k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));

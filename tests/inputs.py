@@ -31,6 +31,35 @@ def prefixes_of_each_other(n, seed=3):
     return [base[:int(rng.integers(0, 301))] for _ in range(n)]
 
 
+def shared_head(n, head_len=300, tail=20, seed=8):
+    """Strings that copy a random length of one shared head, then random tail
+    bytes: a chain of nested groups that each lose a few strings per byte."""
+    rng = np.random.default_rng(seed)
+    head = bytes(rng.integers(65, 91, size=head_len).astype(np.uint8))
+    out = []
+    for _ in range(n):
+        k = int(rng.integers(0, head_len + 1))
+        out.append(head[:k] + bytes(rng.integers(65, 91, size=int(rng.integers(0, tail + 1))).astype(np.uint8)))
+    return out
+
+
+def run_suffixes(seed=9, max_len=256):
+    """All suffixes (truncated) of a text with long single-letter and periodic
+    runs: suffixes inside a run share prefixes that end one byte apart."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for _ in range(12):
+        r = int(rng.integers(0, 3))
+        if r == 0:
+            parts.append(b"A" * int(rng.integers(100, 700)))
+        elif r == 1:
+            parts.append(b"CG" * int(rng.integers(50, 300)))
+        else:
+            parts.append(bytes(rng.integers(65, 69, size=int(rng.integers(5, 60))).astype(np.uint8)))
+    text = b"".join(parts)
+    return [text[i:i + max_len] for i in range(len(text))]
+
+
 def cases():
     """(name, list of byte strings) covering the edge cases the reference's tests touch."""
     return [
@@ -46,4 +75,6 @@ def cases():
         ("prefix_chain", prefixes_of_each_other(800)),
         ("long_strings", random_strings(400, 900, 2100, b"AB", 6)),
         ("wide_alphabet", random_strings(2000, 1, 64, bytes(range(1, 256)), 7)),
+        ("shared_head", shared_head(3000)),
+        ("run_suffixes", run_suffixes()),
     ]

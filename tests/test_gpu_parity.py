@@ -39,7 +39,7 @@ def test_prefix_hash(dsss, orc, depth):
         assert int(h[i]) == orc.xxh64(s[:depth]) % M, (i, len(s))
 
 
-@pytest.mark.parametrize("small_max", [0, 32, 300])
+@pytest.mark.parametrize("small_max", [0, 2, 32, 300])
 @pytest.mark.parametrize("p", [1, 3])
 @pytest.mark.parametrize("name,strs", CASES, ids=IDS)
 def test_local_sort(dsss, orc, ctx, name, strs, p, small_max):
@@ -182,6 +182,19 @@ def test_pd_sort_suffixes(dsss, orc, ctx, p):
     hs = dsss.gen_suffix_strings(150000, 256, seed=5)
     out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), p)
     check_pd(dsss, orc, hs, out, p)
+
+
+@pytest.mark.parametrize("which", ["suffix_1mib", "request_300k"])
+def test_local_sort_long_chains(dsss, orc, ctx, which):
+    """Inputs whose sort tree has long chains of large groups (repeats in a
+    suffix set; strings sharing a random-length common head): the pivot
+    passes of the sort, checked against the oracle's order and LCPs."""
+    hs = dsss.gen_suffix_strings(1 << 20, 256, seed=100) if which == "suffix_1mib" else dsss.gen_request(300000, seed=3)
+    n = hs.n
+    order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), 1)
+    ro, rl = orc.local_sort(orc.Strings.from_host(hs), np.array([0, n], np.uint64))
+    assert np.array_equal(u64(order, n), ro)
+    assert np.array_equal(u64(lcp, n), rl)
 
 
 def test_pd_sort_request(dsss, orc, ctx):
