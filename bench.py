@@ -161,13 +161,17 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
     }
 
 
-def bench_serving(d, torch, p=8, n_req=48, rate=60.0, seed=2024):
+def bench_serving(d, torch, p=8, n_req=48, rate=250.0, seed=2024, workers=4, max_batch=4_000_000,
+                  reserve=24 << 30):
     """Sort requests through dsss_server: n log-uniform in [1e3, 4e6], lengths
     Zipf(1.2) on [8, 256], bytes 0x21-0x7E after a shared random prefix; host
     buffers pinned.  Saturated throughput (all requests queued at once) and
     latency under seeded Poisson arrivals at `rate` requests/s, for continuous
-    batching (3 workers) and for the plain per-request path (1 worker, one
-    request per batch = dsss_pd_sort_host per request)."""
+    batching (`workers` batches in flight, up to `max_batch` strings per batch
+    beyond its first request) and for the plain per-request path (1 worker,
+    one request per batch = dsss_pd_sort_host per request).  Both servers map
+    `reserve` bytes into their memory pool at start; admission is against a
+    150 GB budget."""
     rng = np.random.default_rng(seed)
     ns = np.exp(rng.uniform(np.log(1e3), np.log(4e6), size=n_req)).astype(np.int64)
     reqs = [d.gen_request(int(n), seed=seed * 1000 + k, pinned=True) for k, n in enumerate(ns)]
@@ -180,8 +184,9 @@ def bench_serving(d, torch, p=8, n_req=48, rate=60.0, seed=2024):
         outs.append(dict(local_order=mk(), dp=mk(), perm_index=mk(), perm_pe=mk(), merged_lcp=mk(),
                          intervals=np.zeros(p * p, np.uint64), recv_counts=np.zeros(p, np.uint64)))
 
-    def run(workers, max_sets, paced):
-        srv = d.Server(torch.cuda.current_device(), p=p, workers=workers, max_sets=max_sets)
+    def run(workers, max_sets, paced, mbs=0):
+        srv = d.Server(torch.cuda.current_device(), p=p, workers=workers, max_sets=max_sets, max_batch_strings=mbs,
+                       reserve_bytes=reserve, hbm_budget=150_000_000_000)
         for h, o in list(zip(reqs, outs))[:4]:  # warm-up
             srv.wait(srv.submit(h, out=o)[0])
         t0 = d.clock_now()
@@ -201,13 +206,13 @@ def bench_serving(d, torch, p=8, n_req=48, rate=60.0, seed=2024):
                 "p99_ms": float(np.percentile(lat, 99)), "mean_batch": info["batched_requests"] / info["batches"],
                 "max_reserved_gb": info["max_reserved_bytes"] / 1e9}
 
-    served_sat = run(3, 0, False)
+    served_sat = run(workers, 0, False, max_batch)
     plain_sat = run(1, 1, False)
-    served = run(3, 0, True)
+    served = run(workers, 0, True, max_batch)
     plain = run(1, 1, True)
     return {
         "workload": f"{n_req} requests, n log-uniform [1e3, 4e6] (total {total}), p = {p}, Poisson {rate}/s (seed {seed})",
-        "hbm_budget_gb": 150,
+        "hbm_budget_gb": 150, "workers": workers, "max_batch_strings": max_batch,
         "served": {"saturated_strings_per_s": served_sat["strings_per_s"], "p50_ms": served["p50_ms"],
                    "p99_ms": served["p99_ms"], "paced_strings_per_s": served["strings_per_s"],
                    "mean_batch": served_sat["mean_batch"], "max_reserved_gb": served_sat["max_reserved_gb"]},

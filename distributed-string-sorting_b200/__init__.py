@@ -52,13 +52,15 @@ class PdResult(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("p", ctypes.c_uint32),
                 ("max_sets", ctypes.c_uint32), ("max_batch_strings", ctypes.c_uint64),
-                ("hbm_budget", ctypes.c_uint64), ("opts", Opts)]
+                ("hbm_budget", ctypes.c_uint64), ("opts", Opts), ("flags", ctypes.c_uint32),
+                ("reserve_bytes", ctypes.c_uint64)]
 
 
 class RequestStats(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("batch_sets", ctypes.c_uint32), ("batch_id", ctypes.c_uint64),
                 ("batch_strings", ctypes.c_uint64), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
-                ("t_done", ctypes.c_double), ("error", ctypes.c_char * 160)]
+                ("t_done", ctypes.c_double), ("t_copied", ctypes.c_double), ("t_sorted", ctypes.c_double),
+                ("error", ctypes.c_char * 160)]
 
 
 class ServerInfo(ctypes.Structure):
@@ -439,8 +441,10 @@ class Server:
     """dsss_server: continuous batching of sort requests onto one GPU."""
 
     def __init__(self, device: int = 0, p: int = 4, workers: int = 2, max_sets: int = 0, max_batch_strings: int = 0,
-                 hbm_budget: int = 0, sampler: int = 0, small_sort_max: int = 0):
-        cfg = ServerConfig(device, workers, p, max_sets, max_batch_strings, hbm_budget, _opts(sampler, 2, small_sort_max))
+                 hbm_budget: int = 0, sampler: int = 0, small_sort_max: int = 0, timestamps: bool = False,
+                 reserve_bytes: int = 0):
+        cfg = ServerConfig(device, workers, p, max_sets, max_batch_strings, hbm_budget, _opts(sampler, 2, small_sort_max),
+                           1 if timestamps else 0, reserve_bytes)
         h = ctypes.c_void_p()
         check(lib().dsss_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
@@ -475,7 +479,8 @@ class Server:
         self._live.pop(ticket, None)
         check(rc)
         return dict(batch_sets=st.batch_sets, batch_id=st.batch_id, batch_strings=st.batch_strings,
-                    t_submit=st.t_submit, t_admit=st.t_admit, t_done=st.t_done,
+                    t_submit=st.t_submit, t_admit=st.t_admit, t_done=st.t_done, t_copied=st.t_copied,
+                    t_sorted=st.t_sorted,
                     latency=st.t_done - st.t_submit)
 
     def info(self) -> dict:

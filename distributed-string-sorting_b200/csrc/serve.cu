@@ -158,7 +158,8 @@ static bool form_batch(Server* s, Batch& b) {
 }
 
 // Runs one batch on the worker's stream; returns a status for all its requests.
-static int run_batch(Server* s, Ctx* ctx, cudaStream_t st, Batch& b, uint64_t batch_id) {
+static int run_batch(Server* s, Ctx* ctx, cudaStream_t st, Batch& b, uint64_t batch_id, double* t_copied,
+                     double* t_sorted) {
     const uint32_t p = s->cfg.p, nsets = (uint32_t)b.reqs.size();
     const uint64_t n = b.n;
     void* block = nullptr;
@@ -201,6 +202,10 @@ static int run_batch(Server* s, Ctx* ctx, cudaStream_t st, Batch& b, uint64_t ba
     DSSS_CUDA(cudaMemcpyAsync(sb_d, sb.data(), (nsets + 1) * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(cb_d, cb.data(), (nsets + 1) * 8, cudaMemcpyHostToDevice, st));
     if (n) DSSS_LAUNCH("k_rebase_offsets", st, k_rebase_offsets<<<grid_for(n, 256), 256, 0, st>>>(off, n, sb_d, cb_d, nsets));
+    if (s->cfg.flags & DSSS_SERVER_TIMESTAMPS) {
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        *t_copied = now_s();
+    }
 
     dsss_arena a{chars, b.chars, off, len, n};
     std::vector<uint64_t> intervals((uint64_t)nsets * p * p), recv((uint64_t)nsets * p);
@@ -213,6 +218,7 @@ static int run_batch(Server* s, Ctx* ctx, cudaStream_t st, Batch& b, uint64_t ba
     ctx->pin = sub.pin;
     ctx->pin_cap = sub.pin_cap;
     if (rc != DSSS_OK) return rc;
+    *t_sorted = now_s();  // pd_sort_dev returns after its last read-back
     if (n) DSSS_LAUNCH("k_local_ids", st, k_local_ids<<<grid_for(n, 256), 256, 0, st>>>(lorder, n, sb_d, nsets));
     for (uint32_t k = 0; k < nsets; ++k) {
         Request* r = b.reqs[k];
@@ -264,9 +270,10 @@ static void worker_main(Server* s) {
             for (Request* r : b.reqs) r->st.t_admit = t;
         }
         int rc;
+        double t_copied = 0, t_sorted = 0;
         {
             ActiveCtx active(&ctx);
-            rc = run_batch(s, &ctx, st, b, batch_id);
+            rc = run_batch(s, &ctx, st, b, batch_id, &t_copied, &t_sorted);
         }
         char msg[sizeof(dsss_request_stats::error)] = "";
         if (rc != DSSS_OK) {
@@ -284,6 +291,8 @@ static void worker_main(Server* s) {
                 r->st.batch_sets = (uint32_t)b.reqs.size();
                 r->st.batch_strings = b.n;
                 r->st.t_done = t;
+                r->st.t_copied = t_copied;
+                r->st.t_sorted = t_sorted;
                 if (rc != DSSS_OK) snprintf(r->st.error, sizeof r->st.error, "%s", msg);
                 r->done = true;
             }
@@ -326,6 +335,23 @@ int dsss_server_create(const dsss_server_config* cfg, dsss_server** out) {
     DSSS_CUDA(cudaMemPoolCreate(&s.pool, &props));
     uint64_t keep = s.cfg.hbm_budget;  // freed blocks stay resident up to the budget
     DSSS_CUDA(cudaMemPoolSetAttribute(s.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    if (s.cfg.reserve_bytes) {
+        // map the reserve now: growing the pool later stalls the batches in flight
+        const uint64_t r = std::min(s.cfg.reserve_bytes, s.cfg.hbm_budget);
+        void* p = nullptr;
+        cudaStream_t st = nullptr;
+        DSSS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        cudaError_t e = cudaMallocFromPoolAsync(&p, r, s.pool, st);
+        if (e == cudaSuccess) e = cudaFreeAsync(p, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaMemPoolDestroy(s.pool);
+            return fail(DSSS_ENOMEM, "server: reserving %llu device bytes failed: %s", (unsigned long long)r,
+                        cudaGetErrorString(e));
+        }
+    }
     for (uint32_t w = 0; w < s.cfg.workers; ++w) s.workers.emplace_back(worker_main, &s);
     *out = h.release();
     return DSSS_OK;

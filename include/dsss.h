@@ -258,7 +258,12 @@ typedef struct {
     uint64_t max_batch_strings; /* strings per batch beyond its first request; 0 -> no limit */
     uint64_t hbm_budget;        /* device bytes the server may hold; 0 -> 150e9 */
     dsss_opts opts;
+    uint32_t flags;             /* DSSS_SERVER_* */
+    uint64_t reserve_bytes;     /* device memory mapped into the pool at start (kept resident) */
 } dsss_server_config;
+
+/* Record t_copied (one extra stream synchronisation per batch). */
+#define DSSS_SERVER_TIMESTAMPS 1u
 
 typedef struct {
     int status;                 /* DSSS_OK or the batch's error */
@@ -266,6 +271,7 @@ typedef struct {
     uint64_t batch_id;
     uint64_t batch_strings;
     double t_submit, t_admit, t_done; /* seconds, dsss_clock_now() */
+    double t_copied, t_sorted;        /* batch inputs on the device; batch sorted */
     char error[160];
 } dsss_request_stats;
 
