@@ -89,6 +89,8 @@ _SIGS = {
     "dsss_pd_sort_batched_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
                                        ctypes.POINTER(PdResult), _P]),
     "dsss_clock_now": (ctypes.c_double, []),
+    "dsss_tune_set": (_I, [ctypes.c_char_p, ctypes.c_int64]),
+    "dsss_tune_get": (_I, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
     "dsss_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
     "dsss_server_submit": (_I, [_P, ctypes.POINTER(Arena), _P, ctypes.POINTER(PdResult), ctypes.POINTER(_U64)]),
     "dsss_server_wait": (_I, [_P, _U64, ctypes.c_int64, ctypes.POINTER(RequestStats)]),
@@ -430,6 +432,37 @@ def pd_sort_batched_host(ctx: Context, hs: HostStrings, nsets: int, p: int, part
                                           ctypes.byref(_opts(sampler)), ctypes.byref(res), _stream_ptr(stream)))
     out["part_begin"] = pb
     return out
+
+
+TUNE_KNOBS = ("dp_filter_min", "dp_filter_bits", "sort_small_max", "sort_pivot")
+
+
+def tune_set(name: str, value: int):
+    """Sets a process-wide tuning knob (-1 restores its default)."""
+    check(lib().dsss_tune_set(name.encode(), int(value)))
+
+
+def tune_get(name: str) -> int:
+    v = ctypes.c_int64(0)
+    check(lib().dsss_tune_get(name.encode(), ctypes.byref(v)))
+    return int(v.value)
+
+
+class tuned:
+    """Context manager: knobs set for the block, defaults restored after."""
+
+    def __init__(self, **knobs):
+        self.knobs = knobs
+
+    def __enter__(self):
+        self.old = {k: tune_get(k) for k in self.knobs}
+        for k, v in self.knobs.items():
+            tune_set(k, v)
+        return self
+
+    def __exit__(self, *exc):
+        for k, v in self.old.items():
+            tune_set(k, v)
 
 
 def clock_now() -> float:

@@ -55,6 +55,28 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+// ------------------------------------------------------------- tuning ----
+struct KnobDef {
+    const char* name;
+    int64_t def, lo, hi;
+};
+static const KnobDef g_knob_defs[TUNE_COUNT] = {
+    {"dp_filter_min", 1ll << 40, 0, 1ll << 40},
+    {"dp_filter_bits", 16, 4, 64},
+    {"sort_small_max", 4096, 2, 4096},
+    {"sort_pivot", 1, 0, 1},
+};
+static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}};
+
+int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
+
+static int knob_index(const char* name) {
+    if (!name) return -1;
+    for (int k = 0; k < TUNE_COUNT; ++k)
+        if (!strcmp(name, g_knob_defs[k].name)) return k;
+    return -1;
+}
+
 int ensure_ws(Ctx* c, uint64_t bytes) {
     if (bytes <= c->ws_cap) return DSSS_OK;
     if (c->fixed_ws)
@@ -355,5 +377,23 @@ uint64_t dsss_ctx_scratch_bytes(const dsss_ctx* c) { return c ? c->ws_cap : 0; }
 const char* dsss_last_error(void) { return g_err; }
 
 int dsss_abi_version(void) { return DSSS_ABI_VERSION; }
+
+int dsss_tune_set(const char* name, int64_t value) {
+    const int k = knob_index(name);
+    if (k < 0) return fail(DSSS_EINVAL, "unknown tuning knob '%s'", name ? name : "(null)");
+    if (value < 0) value = g_knob_defs[k].def;
+    if (value < g_knob_defs[k].lo || value > g_knob_defs[k].hi)
+        return fail(DSSS_EINVAL, "knob %s takes %lld..%lld", name, (long long)g_knob_defs[k].lo,
+                    (long long)g_knob_defs[k].hi);
+    g_knobs[k].store(value, std::memory_order_relaxed);
+    return DSSS_OK;
+}
+
+int dsss_tune_get(const char* name, int64_t* value) {
+    const int k = knob_index(name);
+    if (k < 0 || !value) return fail(DSSS_EINVAL, "unknown tuning knob '%s'", name ? name : "(null)");
+    *value = g_knobs[k].load(std::memory_order_relaxed);
+    return DSSS_OK;
+}
 
 }  // extern "C"

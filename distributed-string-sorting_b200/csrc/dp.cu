@@ -32,9 +32,16 @@ constexpr unsigned FULLM = 0xffffffffu;
 // duplicate (stays), 2 hashed (stays iff its hash is shared), 3 hashed root
 // (stays; its hash is still inserted so others can collide with it).
 
-__global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_t* lens) {
+// Length and char offset of every sorted position, gathered once per call so
+// that the hash rounds read them in order.
+__global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_t* lens, uint64_t* soff) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) lens[i] = a.len[order[i]];  // the 4-byte array caches better than 16-byte handles
+    if (i >= n) return;
+    uint64_t off;
+    uint32_t len;
+    str_of(a, order[i], off, len);
+    lens[i] = len;
+    soff[i] = off;
 }
 
 // Index of the string set holding sorted position i (set_begin: nsets+1 bounds).
@@ -104,7 +111,7 @@ __global__ void k_dp_classify(const uint8_t* st, int all, const uint32_t* lens, 
 
 // Each string set owns a power-of-two region of the table (base, mask): equal
 // prefixes in different sets are not duplicates of each other.
-__global__ void k_dp_hash(ArenaDev a, const uint32_t* order, const uint8_t* kind, uint64_t n, uint32_t depth,
+__global__ void k_dp_hash(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
                           unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1, const uint64_t* set_begin,
                           uint32_t nsets, const uint64_t* set_base, const uint32_t* set_mask, uint32_t* slot,
                           uint32_t* err) {
@@ -119,7 +126,7 @@ __global__ void k_dp_hash(ArenaDev a, const uint32_t* order, const uint8_t* kind
         tkeys += base;
         tdup += base;
     }
-    const unsigned long long h = filter_hash(xxh64_dev(a.chars + a.off[order[i]], depth));
+    const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
     uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
     // Linear probing; the table always has free slots, so a free or matching
     // slot is reached within mask + 1 probes.
@@ -177,17 +184,28 @@ __device__ __forceinline__ uint64_t set_slots(uint32_t c) {
     return t;
 }
 
+// Per-set filter regions in 32-bit words: a power of two >= bpk bits per
+// hashed string, 1024 bits at least.
+__device__ __forceinline__ uint64_t set_filter_bits(uint32_t c, uint32_t bpk) {
+    if (c == 0) return 0;
+    uint64_t t = 1024;
+    while (t < (uint64_t)c * bpk) t <<= 1;
+    return t;
+}
+
 constexpr int SET_NT = 1024;
 
-// One block: region base and mask per set from the hashed counts, total slots
-// into counters[4..5] (lo, hi), counters[2] set if it exceeds cap.
-__global__ void __launch_bounds__(SET_NT) k_set_tables(const uint32_t* cnt, uint32_t nsets, uint64_t cap,
-                                                       uint64_t* base, uint32_t* mask, uint32_t* counters) {
+// One block: region base and mask per set from the per-set counts, total into
+// out[0..1] (lo, hi), *err set if it exceeds cap.  bpk == 0: hash-table
+// regions (slots); bpk > 0: filter regions (base in words, mask in bits).
+__global__ void __launch_bounds__(SET_NT) k_set_tables(const uint32_t* cnt, uint32_t nsets, uint64_t cap, uint32_t bpk,
+                                                       uint64_t* base, uint32_t* mask, uint32_t* out, uint32_t* err) {
     __shared__ uint64_t part[SET_NT];
     const uint32_t per = (nsets + SET_NT - 1) / SET_NT;
     const uint32_t b = min(nsets, threadIdx.x * per), e = min(nsets, b + per);
+    auto size_of = [&](uint32_t c) -> uint64_t { return bpk ? set_filter_bits(c, bpk) / 32 : set_slots(c); };
     uint64_t sum = 0;
-    for (uint32_t s = b; s < e; ++s) sum += set_slots(cnt[s]);
+    for (uint32_t s = b; s < e; ++s) sum += size_of(cnt[s]);
     part[threadIdx.x] = sum;
     __syncthreads();
     for (int off = 1; off < SET_NT; off <<= 1) {
@@ -198,17 +216,152 @@ __global__ void __launch_bounds__(SET_NT) k_set_tables(const uint32_t* cnt, uint
     }
     uint64_t run = part[threadIdx.x] - sum;
     for (uint32_t s = b; s < e; ++s) {
-        const uint64_t sl = set_slots(cnt[s]);
+        const uint64_t sl = size_of(cnt[s]);
         base[s] = run;
-        mask[s] = sl ? (uint32_t)(sl - 1) : 0;
+        mask[s] = sl ? (uint32_t)((bpk ? sl * 32 : sl) - 1) : 0;
         run += sl;
     }
     if (threadIdx.x == SET_NT - 1) {
         const uint64_t total = part[SET_NT - 1];
-        if (total > cap) counters[2] = 1;
-        counters[4] = (uint32_t)total;
-        counters[5] = (uint32_t)(total >> 32);
+        if (total > cap) *err = 1;
+        out[0] = (uint32_t)total;
+        out[1] = (uint32_t)(total >> 32);
     }
+}
+
+// ---------------------------------------------------- fingerprint filter ----
+// Rounds that hash many strings find duplicate hashes without a table entry
+// per string: each hashed string sets one bit, chosen by its hash, of a
+// bitmap small enough to stay in L2; a string whose bit was already set is a
+// candidate.  Every hash that occurs twice has a candidate (its later insert),
+// so an exact table over the candidates' hashes, in which every hashed string
+// then counts itself if its hash is there, gives the exact number of strings
+// per duplicated hash; a string whose hash is not in that table is unique.
+// The outcome is exactly that of one table over all hashes.
+__global__ void k_dp_filter(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
+                            uint32_t* bits, uint32_t bmask1, const uint64_t* set_begin, uint32_t nsets,
+                            const uint64_t* set_wbase, const uint32_t* set_bmask, unsigned long long* hbuf,
+                            uint32_t* cand, uint32_t* ncand, uint32_t* set_ccnt) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool c = false;
+    uint32_t sid = 0;
+    if (i < n && kind[i] >= 2) {
+        const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+        hbuf[i] = h;
+        uint64_t wbase = 0;
+        uint32_t bm = bmask1;
+        if (nsets > 1) {
+            sid = set_of(set_begin, nsets, i);
+            wbase = set_wbase[sid];
+            bm = set_bmask[sid];
+        }
+        const uint32_t b = (uint32_t)(h >> 32) & bm;
+        const uint32_t bit = 1u << (b & 31);
+        c = (atomicOr(&bits[wbase + (b >> 5)], bit) & bit) != 0;
+    }
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = __ballot_sync(FULLM, c);
+    if (m) {
+        uint32_t base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(ncand, (uint32_t)__popc(m));
+        base = __shfl_sync(FULLM, base, __ffs(m) - 1);
+        if (c) cand[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+        if (nsets > 1) {
+            const uint32_t key = c ? sid : 0xFFFFFFFFu - lane;
+            const uint32_t peers = __match_any_sync(FULLM, key);
+            if (c && lane == __ffs(peers) - 1) atomicAdd(&set_ccnt[sid], (uint32_t)__popc(peers));
+        }
+    }
+}
+
+// Table region of position i: (base, mask).
+__device__ __forceinline__ void table_region(const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
+                                             const uint32_t* set_mask, uint32_t mask1, uint64_t i, uint64_t& base,
+                                             uint32_t& mask) {
+    base = 0;
+    mask = mask1;
+    if (nsets > 1) {
+        const uint32_t sid = set_of(set_begin, nsets, i);
+        base = set_base[sid];
+        mask = set_mask[sid];
+    }
+}
+
+// Inserts the candidates' hashes (each distinct hash once).
+__global__ void k_cand_insert(const uint32_t* cand, uint32_t ncand, const unsigned long long* hbuf,
+                              unsigned long long* tkeys, uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
+                              const uint64_t* set_base, const uint32_t* set_mask, uint32_t* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ncand) return;
+    const uint32_t i = cand[j];
+    const unsigned long long h = hbuf[i];
+    uint64_t base;
+    uint32_t mask;
+    table_region(set_begin, nsets, set_base, set_mask, mask1, i, base, mask);
+    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
+    for (uint32_t probe = 0;; ++probe) {
+        if (probe > mask) {
+            atomicExch(err, 1u);
+            return;
+        }
+        const unsigned long long prev = atomicCAS(&tkeys[base + sl], EMPTY_KEY, h);
+        if (prev == EMPTY_KEY || prev == h) return;
+        sl = (sl + 1) & mask;
+    }
+}
+
+// Every hashed string whose hash is in the candidate table counts itself
+// there: tcnt byte bit 0 = seen, bit 1 = seen twice or more.
+__global__ void k_dp_count(const uint8_t* kind, uint64_t n, const unsigned long long* hbuf,
+                           const unsigned long long* tkeys, uint32_t* tcnt_words, uint32_t mask1,
+                           const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
+                           const uint32_t* set_mask, uint32_t* slot, uint32_t* err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    const unsigned long long h = hbuf[i];
+    uint64_t base;
+    uint32_t mask;
+    table_region(set_begin, nsets, set_base, set_mask, mask1, i, base, mask);
+    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
+    uint32_t found = NO_SLOT;
+    // a set without candidates has no region (mask 0): nothing to find
+    for (uint32_t probe = 0; mask != 0; ++probe) {
+        if (probe > mask) {
+            atomicExch(err, 1u);
+            break;
+        }
+        const unsigned long long k = tkeys[base + sl];
+        if (k == h) {
+            found = (uint32_t)(base + sl);
+            break;
+        }
+        if (k == EMPTY_KEY) break;
+        sl = (sl + 1) & mask;
+    }
+    slot[i] = found;
+    if (found != NO_SLOT) {
+        const uint32_t sh = 8 * (found & 3u);
+        const uint32_t old = atomicOr(&tcnt_words[found >> 2], 1u << sh);
+        if (old & (1u << sh)) atomicOr(&tcnt_words[found >> 2], 2u << sh);
+    }
+}
+
+__global__ void k_dp_query_cnt(const uint8_t* kind, const uint32_t* slot, const uint8_t* tcnt, uint64_t n,
+                               uint8_t* st_next, uint32_t* counters) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool stays = false;
+    if (i < n && kind[i] == 2) {
+        const uint32_t sl = slot[i];
+        stays = sl != NO_SLOT && (tcnt[sl] & 2);
+        st_next[i] = stays ? 1 : 0;
+    }
+    block_count(counters + 1, stays);
+}
+
+static uint64_t pow2_at_least(uint64_t x, uint64_t lo) {
+    uint64_t t = lo;
+    while (t < x) t <<= 1;
+    return t;
 }
 
 void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
@@ -223,13 +376,31 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.st[1] = c.take<uint8_t>(N);
     L.kind = c.take<uint8_t>(N);
     L.lens = c.take<uint32_t>(N);
+    L.soff = c.take<uint64_t>(N);
     L.slot = c.take<uint32_t>(N);
     // one set: the table for n keys; several: room for every set's own
     // power-of-two region (at most 3 slots per key plus 68 per set)
     L.slots = nsets == 1 ? table_slots(N) : 3 * N + 128ull * (nsets + 1);
     L.tkeys = c.take<unsigned long long>(L.slots);
-    L.tdup = c.take<uint8_t>(L.slots);
-    L.counters = c.take<uint32_t>(8);
+    L.tdup = c.take<uint8_t>(L.slots + 4);
+    L.counters = c.take<uint32_t>(16);
+    L.set_bbase = c.take<uint64_t>(nsets);
+    L.set_bmask = c.take<uint32_t>(nsets);
+    L.set_ccnt = c.take<uint32_t>(nsets);
+    // fingerprint filter: planned when a round may hash dp_filter_min strings
+    L.filter_min = (uint64_t)tune(TUNE_DP_FILTER_MIN);
+    L.filter_bpk = (uint32_t)tune(TUNE_DP_FILTER_BITS);
+    if (N >= L.filter_min) {
+        L.bm_words = (nsets == 1 ? pow2_at_least(N * L.filter_bpk, 1024) : 2 * N * L.filter_bpk + 1024ull * nsets) / 32;
+        L.bits = c.take<uint32_t>(L.bm_words);
+        L.hbuf = c.take<unsigned long long>(N);
+        L.cand = c.take<uint32_t>(N);
+    } else {
+        L.bm_words = 0;
+        L.bits = nullptr;
+        L.hbuf = nullptr;
+        L.cand = nullptr;
+    }
 }
 
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
@@ -247,33 +418,80 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                   cudaMemcpyHostToDevice, st));
     }
     const unsigned grid = grid_for(n, 256);
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
     int cur = 0;
     const uint64_t start = 8;
     uint64_t depth = start;
     for (uint64_t i = start * 2;; i *= 2) {
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
-        DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
+        DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
         if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
         DSSS_LAUNCH("k_dp_classify", st,
                     k_dp_classify<<<grid, 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
                                                        L.st[cur ^ 1], L.kind, L.counters, L.set_begin, nsets,
                                                        L.set_cnt));
-        if (nsets > 1)
+        if (nsets > 1) {
             DSSS_LAUNCH("k_set_tables", st,
-                        k_set_tables<<<1, SET_NT, 0, st>>>(L.set_cnt, nsets, L.slots, L.set_base, L.set_mask,
-                                                           L.counters));
-        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 6 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                        k_set_tables<<<1, SET_NT, 0, st>>>(L.set_cnt, nsets, L.slots, 0, L.set_base, L.set_mask,
+                                                           L.counters + 4, L.counters + 2));
+            if (L.bits)
+                DSSS_LAUNCH("k_set_tables", st,
+                            k_set_tables<<<1, SET_NT, 0, st>>>(L.set_cnt, nsets, L.bm_words, L.filter_bpk,
+                                                               L.set_bbase, L.set_bmask, L.counters + 6,
+                                                               L.counters + 2));
+        }
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
         const uint32_t hashed = pin[0];
         if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table regions exceed the plan");
-        if (hashed) {
+        if (hashed && L.bits && hashed >= L.filter_min) {
+            // fingerprint filter, then an exact table over the candidates only
+            const uint64_t words = nsets > 1 ? ((uint64_t)pin[7] << 32 | pin[6])
+                                             : pow2_at_least((uint64_t)hashed * L.filter_bpk, 1024) / 32;
+            if (words > L.bm_words) return fail(DSSS_EDEVICE, "distinguishing-prefix filter exceeds the plan");
+            DSSS_CUDA(cudaMemsetAsync(L.bits, 0, words * 4, st));
+            if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_ccnt, 0, nsets * sizeof(uint32_t), st));
+            DSSS_LAUNCH("k_dp_filter", st,
+                        k_dp_filter<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.bits,
+                                                         (uint32_t)(words * 32 - 1), L.set_begin, nsets, L.set_bbase,
+                                                         L.set_bmask, L.hbuf, L.cand, L.counters + 3, L.set_ccnt));
+            if (nsets > 1)
+                DSSS_LAUNCH("k_set_tables", st,
+                            k_set_tables<<<1, SET_NT, 0, st>>>(L.set_ccnt, nsets, L.slots, 0, L.set_base, L.set_mask,
+                                                               L.counters + 4, L.counters + 2));
+            DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            DSSS_CUDA(cudaStreamSynchronize(st));
+            if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table regions exceed the plan");
+            const uint32_t ncand = pin[3];
+            if (ncand) {  // else every hash is unique: no kind-2 string stays
+                const uint64_t slots = nsets > 1 ? ((uint64_t)pin[5] << 32 | pin[4]) : table_slots(ncand);
+                if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
+                DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+                DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, (slots + 3) & ~3ull, st));
+                DSSS_LAUNCH("k_cand_insert", st,
+                            k_cand_insert<<<grid_for(ncand, 256), 256, 0, st>>>(L.cand, ncand, L.hbuf, L.tkeys,
+                                                                                 (uint32_t)(slots - 1), L.set_begin,
+                                                                                 nsets, L.set_base, L.set_mask,
+                                                                                 L.counters + 2));
+                DSSS_LAUNCH("k_dp_count", st,
+                            k_dp_count<<<grid, 256, 0, st>>>(L.kind, n, L.hbuf, L.tkeys, (uint32_t*)L.tdup,
+                                                            (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
+                                                            L.set_mask, L.slot, L.counters + 2));
+                DSSS_LAUNCH("k_dp_query", st,
+                            k_dp_query_cnt<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1],
+                                                                L.counters));
+                DSSS_CUDA(cudaGetLastError());
+                DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                DSSS_CUDA(cudaStreamSynchronize(st));
+                if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table overflow");
+            }
+        } else if (hashed) {
             const uint64_t slots = nsets > 1 ? ((uint64_t)pin[5] << 32 | pin[4]) : table_slots(hashed);
             if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
             DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
             DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
             DSSS_LAUNCH("k_dp_hash", st,
-                        k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
+                        k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
                                                        (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
                                                        L.set_mask, L.slot, L.counters + 2));
             DSSS_LAUNCH("k_dp_query", st,
@@ -331,8 +549,8 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
     *m_next = 0;
     if (n == 0) return DSSS_OK;
     const unsigned grid = grid_for(n, 256);
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens));
-    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 8 * sizeof(uint32_t), st));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     const bool all = cand == nullptr;
     if (!all) {
         DSSS_CUDA(cudaMemsetAsync(L.st[0], 0, n, st));
@@ -350,7 +568,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
         DSSS_LAUNCH("k_dp_hash", st,
-                    k_dp_hash<<<grid, 256, 0, st>>>(a, order, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
+                    k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
                                                    nullptr, 1, nullptr, nullptr, L.slot, L.counters + 2));
         DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
     }

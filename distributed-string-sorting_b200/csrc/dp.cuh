@@ -8,6 +8,7 @@ struct DpLayout {
     uint8_t* st[2];
     uint8_t* kind;
     uint32_t* lens;
+    uint64_t* soff;
     uint32_t* slot;
     unsigned long long* tkeys;
     uint8_t* tdup;
@@ -21,6 +22,17 @@ struct DpLayout {
     uint64_t* set_base;
     uint32_t* set_mask;
     uint32_t* set_cnt;
+    // fingerprint filter (planned when n >= filter_min): bitmap words,
+    // per-position hashes, candidate positions, per-set filter regions
+    uint64_t filter_min;
+    uint32_t filter_bpk;
+    uint64_t bm_words;
+    uint32_t* bits;
+    unsigned long long* hbuf;
+    uint32_t* cand;
+    uint64_t* set_bbase;
+    uint32_t* set_bmask;
+    uint32_t* set_ccnt;
 };
 
 void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets = 1);

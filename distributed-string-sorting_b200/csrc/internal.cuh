@@ -124,6 +124,16 @@ inline int set_smem_once(std::atomic<uint64_t>& done, K* kernel, int bytes) {
     return DSSS_OK;
 }
 
+// Process-wide tuning knobs (dsss_tune_set / dsss_tune_get), read at call time.
+enum TuneKnob : int {
+    TUNE_DP_FILTER_MIN = 0,  // hashed strings per round from which the fingerprint filter is used
+    TUNE_DP_FILTER_BITS,     // filter bits per hashed string (rounded up to a power of two in total)
+    TUNE_SORT_SMALL_MAX,     // small-segment cutoff when the options give 0
+    TUNE_SORT_PIVOT,         // pivot passes on (1) or off (0)
+    TUNE_COUNT
+};
+int64_t tune(TuneKnob k);
+
 int ensure_ws(Ctx* c, uint64_t bytes);
 int ensure_pin(Ctx* c, uint64_t bytes);
 
@@ -263,8 +273,96 @@ struct WordStream {
     }
 };
 
+// XXH64 of m <= XXH_SHORT_MAX bytes at p with all of its 16-byte loads
+// issued before the first round, so that they are in flight together (the
+// streaming form below waits for each load in turn).  Same value as the
+// streaming form.  Reads up to 22 bytes past p + m.
+constexpr uint32_t XXH_SHORT_MAX = 88;
+__device__ __forceinline__ uint64_t xxh64_short(const uint8_t* p, uint32_t m) {
+    using namespace xxh;
+    const uintptr_t a = (uintptr_t)p;
+    const uint4* q = (const uint4*)(a & ~(uintptr_t)15);
+    const uint32_t skip = (uint32_t)(a & 15);
+    const uint32_t nq = (skip + m + 8 + 15) / 16;  // chunks up to byte p + m + 7
+    uint64_t w[14];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if ((uint32_t)k < nq) v = __ldg(q + k);
+        w[2 * k] = ((uint64_t)v.y << 32) | v.x;
+        w[2 * k + 1] = ((uint64_t)v.w << 32) | v.z;
+    }
+    const bool odd = skip >= 8;
+    const uint32_t sh = (skip & 7) * 8;
+    // input word j = bytes [p + 8j, p + 8j + 8), little-endian
+    auto word = [&](int j) -> uint64_t {
+        const uint64_t lo = odd ? w[j + 1] : w[j];
+        const uint64_t hi = odd ? w[j + 2] : w[j + 1];
+        return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+    };
+    const uint32_t ns = m >= 64 ? 2u : (m >= 32 ? 1u : 0u);  // 32-byte stripes
+    uint64_t v1 = P1 + P2, v2 = P2, v3 = 0, v4 = 0 - P1;
+    if (ns >= 1) {
+        v1 = round(v1, word(0));
+        v2 = round(v2, word(1));
+        v3 = round(v3, word(2));
+        v4 = round(v4, word(3));
+    }
+    if (ns >= 2) {
+        v1 = round(v1, word(4));
+        v2 = round(v2, word(5));
+        v3 = round(v3, word(6));
+        v4 = round(v4, word(7));
+    }
+    uint64_t h;
+    if (m > 32) {
+        h = rotl(v1, 1) + rotl(v2, 7) + rotl(v3, 12) + rotl(v4, 18);
+        h = merge(h, v1);
+        h = merge(h, v2);
+        h = merge(h, v3);
+        h = merge(h, v4);
+    } else {
+        h = v3 + P5;
+    }
+    h += m;
+    const uint32_t t0 = 4 * ns, t1 = t0 + (m - 32 * ns) / 8;  // 8-byte tail words [t0, t1)
+    uint32_t rem = (m - 32 * ns) & 7;
+    uint64_t last = 0;
+#pragma unroll
+    for (int j = 0; j < 11; ++j) {
+        const uint64_t x = word(j);
+        if ((uint32_t)j >= t0 && (uint32_t)j < t1) {
+            h ^= round(0, x);
+            h = rotl(h, 27) * P1 + P4;
+        }
+        if ((uint32_t)j == t1) last = x;
+    }
+    if (rem) {
+        uint64_t wv = last;  // bytes past m are ignored
+        if (rem >= 4) {
+            h ^= (uint64_t)(uint32_t)wv * P1;
+            h = rotl(h, 23) * P2 + P3;
+            wv >>= 32;
+            rem -= 4;
+        }
+        while (rem) {
+            h ^= (wv & 0xff) * P5;
+            h = rotl(h, 11) * P1;
+            wv >>= 8;
+            --rem;
+        }
+    }
+    h ^= h >> 33;
+    h *= P2;
+    h ^= h >> 29;
+    h *= P3;
+    h ^= h >> 32;
+    return h;
+}
+
 __device__ __forceinline__ uint64_t xxh64_dev(const uint8_t* p, uint32_t m) {
     using namespace xxh;
+    if (m <= XXH_SHORT_MAX) return xxh64_short(p, m);
     WordStream ws(p);
     uint64_t v1 = P1 + P2, v2 = P2, v3 = 0, v4 = 0 - P1;
     uint32_t rem = m;

@@ -70,6 +70,7 @@ struct SortState {
     uint32_t* bucket;  // 257 per large segment
     uint32_t* counters;
     uint32_t small_max;
+    uint32_t pivot;  // pivot passes enabled
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
 };
 
@@ -480,7 +481,7 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
         // children keep the parent's keys: their first b+1 key bytes are now
         // common; one that keeps most of the parent gets a pivot pass
         if (total > S.small_max) {
-            if (2 * (uint64_t)total > sg.size) push_large(S, next, cs, total, depth + b + 1, np | F_PIVOT);
+            if (S.pivot && 2 * (uint64_t)total > sg.size) push_large(S, next, cs, total, depth + b + 1, np | F_PIVOT);
             else push_large(S, next, cs, total, depth, np | F_KEYS);
         } else {
             push_small(S, cs, total, depth, np | F_KEYS);
@@ -506,7 +507,7 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
         // end there, written by the scatter
         if (d == 0) return;
         const uint32_t cd = depth + pivot_l((uint32_t)(S.key[par][sg.start] >> 56)) + 1;
-        if (total > S.small_max) push_large(S, next, cs, total, cd, np | (2 * (uint64_t)total > sg.size ? F_PIVOT : 0u));
+        if (total > S.small_max) push_large(S, next, cs, total, cd, np | (S.pivot && 2 * (uint64_t)total > sg.size ? F_PIVOT : 0u));
         else push_small(S, cs, total, cd, np);
     }
 }
@@ -992,7 +993,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
             if (cnt < 2) continue;
             uint32_t cd, cf;
             if (!pseudo) {
-                if (cnt > 32 && 2 * cnt > bn) {
+                if (S.pivot && cnt > 32 && 2 * cnt > bn) {
                     cd = dep + b + 1;  // keeps most of the bucket: pivot pass next
                     cf = SF_PIVOT;
                 } else {
@@ -1015,7 +1016,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                 }
             } else {
                 cd = lin + 1;
-                cf = (cnt > 32 && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
+                cf = (S.pivot && cnt > 32 && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
             }
             uint32_t* dst;
             uint32_t slot;
@@ -1063,6 +1064,7 @@ static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, cons
 
 // ------------------------------------------------------------------ host ----
 static uint32_t clamp_small_max(uint32_t m) {
+    if (m == 0) m = (uint32_t)tune(TUNE_SORT_SMALL_MAX);
     return (m == 0 || m > (uint32_t)bin_cap(NBINS - 1)) ? (uint32_t)bin_cap(NBINS - 1) : (m < 2 ? 2 : m);
 }
 
@@ -1114,6 +1116,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.bucket = L.bucket;
     S.counters = L.counters;
     S.small_max = clamp_small_max(small_max);
+    S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
     S.cap_large = L.cap_large;
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;

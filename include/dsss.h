@@ -101,6 +101,19 @@ int dsss_ctx_set_timing(dsss_ctx* ctx, int on);
 int dsss_ctx_kernel_times(dsss_ctx* ctx, char* buf, uint64_t len);
 int dsss_abi_version(void);
 
+/* Process-wide tuning knobs (no reference counterpart), read by every later
+ * call; value -1 restores the default.  Results never depend on them.
+ *   dp_filter_min   hashed strings in a distinguishing-prefix round from which
+ *                   duplicates are found through the fingerprint filter
+ *                   (default 2^40, i.e. off: on B200 the filter's L2
+ *                   atomics cost as much as the table's; 0 = always)
+ *   dp_filter_bits  filter bits per hashed string (default 16)
+ *   sort_small_max  small-segment cutoff of the string sort when dsss_opts
+ *                   gives 0 (2..4096, default 4096)
+ *   sort_pivot      pivot passes of the string sort on/off (default 1) */
+int dsss_tune_set(const char* name, int64_t value);
+int dsss_tune_get(const char* name, int64_t* value);
+
 /* ---- full path ---------------------------------------------------------- */
 
 /* DistributedPrefixDoublingSort<...>::sort (src/sorter/distributed/prefix_doubling.hpp:200-295):

@@ -108,3 +108,16 @@ def test_request_generator(dsss):
     assert 40 < float(hs.lengths.mean()) < 80
     body = np.concatenate([hs.chars[int(o):int(o) + int(l)] for o, l in zip(hs.offsets[:200], hs.lengths[:200])])
     assert body.min() >= 0x21 and body.max() <= 0x7E
+
+
+def test_knob_errors(dsss):
+    """Tuning knobs are host state: set, read back, range-checked, reset."""
+    with pytest.raises(dsss.DsssError):
+        dsss.tune_set("no_such_knob", 1)
+    with pytest.raises(dsss.DsssError):
+        dsss.tune_set("sort_small_max", 100000)
+    v = dsss.tune_get("dp_filter_bits")
+    dsss.tune_set("dp_filter_bits", 8)
+    assert dsss.tune_get("dp_filter_bits") == 8
+    dsss.tune_set("dp_filter_bits", -1)
+    assert dsss.tune_get("dp_filter_bits") == v == 16

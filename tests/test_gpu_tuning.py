@@ -1,0 +1,58 @@
+"""Tuning knobs change how the path runs, never its results: the fingerprint
+filter of the distinguishing-prefix rounds (forced on for small inputs), the
+pivot passes of the string sort (off), and the small-segment cutoff."""
+import numpy as np
+import pytest
+
+from inputs import cases
+from test_gpu_parity import check_pd, host_of, u64
+
+pytestmark = pytest.mark.gpu
+
+CASES = [c for c in cases() if len(c[1]) >= 8]
+IDS = [c[0] for c in CASES]
+
+
+@pytest.mark.parametrize("p", [2, 5])
+@pytest.mark.parametrize("name,strs", CASES, ids=IDS)
+def test_filter_forced(dsss, orc, ctx, name, strs, p):
+    hs = host_of(dsss, strs)
+    with dsss.tuned(dp_filter_min=0):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), p)
+    check_pd(dsss, orc, hs, out, p)
+
+
+@pytest.mark.parametrize("bits", [4, 64])
+def test_filter_bits(dsss, orc, ctx, bits):
+    """Few filter bits per key: many candidates (every one checked exactly)."""
+    hs = dsss.gen_suffix_strings(60000, 256, seed=3)
+    with dsss.tuned(dp_filter_min=0, dp_filter_bits=bits):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 4)
+    check_pd(dsss, orc, hs, out, 4)
+
+
+def test_filter_batched(dsss, ctx):
+    """Per-set filter regions: a batch with repeated sets gives each set its
+    single-set result."""
+    h1 = dsss.gen_dn(20000, 100, 50, seed=31)
+    h2 = dsss.gen_suffix_strings(30000, 256, seed=4)
+    hs, sb = dsss.concat_sets([h1, h2, h1, h2])
+    pb = dsss.batched_parts(sb, 4)
+    with dsss.tuned(dp_filter_min=0):
+        out = dsss.pd_sort_batched(ctx, dsss.DeviceStrings(hs), 4, 4, pb)
+    for s, h in enumerate([h1, h2, h1, h2]):
+        ref = dsss.pd_sort(ctx, dsss.DeviceStrings(h), 4)
+        b, e = int(sb[s]), int(sb[s + 1])
+        assert np.array_equal(u64(out["dp"], hs.n)[b:e], u64(ref["dp"], h.n)), s
+        assert np.array_equal(u64(out["perm_index"], hs.n)[b:e], u64(ref["perm_index"], h.n)), s
+
+
+@pytest.mark.parametrize("knobs", [dict(sort_pivot=0), dict(sort_small_max=64), dict(sort_small_max=2, sort_pivot=0)])
+def test_sort_knobs(dsss, orc, ctx, knobs):
+    hs = dsss.gen_suffix_strings(50000, 256, seed=6)
+    n = hs.n
+    with dsss.tuned(**knobs):
+        order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), 1)
+    ro, rl = orc.local_sort(orc.Strings.from_host(hs), np.array([0, n], np.uint64))
+    assert np.array_equal(u64(order, n), ro)
+    assert np.array_equal(u64(lcp, n), rl)
