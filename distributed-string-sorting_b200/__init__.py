@@ -89,6 +89,17 @@ _SIGS = {
     "dsss_pd_sort_batched_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
                                        ctypes.POINTER(PdResult), _P]),
     "dsss_clock_now": (ctypes.c_double, []),
+    "dsss_dp_classify_hash": (_I, [_P, ctypes.POINTER(Arena), _P, _P, _P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U64),
+                                   _P]),
+    "dsss_hash_route": (_I, [_P, _P, _P, _U64, _U32, _P, _P, _P, _P]),
+    "dsss_hash_dups": (_I, [_P, _P, _U64, _P, _P]),
+    "dsss_dp_apply": (_I, [_P, _P, _P, _U64, _P, _U64, ctypes.POINTER(_U64), _P]),
+    "dsss_pack_strings": (_I, [_P, ctypes.POINTER(Arena), _P, _P, _U64, _P, _U64, _P, _P, ctypes.POINTER(_U64), _P]),
+    "dsss_partition_search": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, ctypes.POINTER(Arena), _P, _U32, _P, _I,
+                                   _P, _P]),
+    "dsss_bucket_send": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _U32, _U32, _P, _P, _U64,
+                              ctypes.POINTER(_U64), _P, _P, _P, _P, _P, _P]),
+    "dsss_regroup": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _U64, _P]),
     "dsss_tune_set": (_I, [ctypes.c_char_p, ctypes.c_int64]),
     "dsss_tune_get": (_I, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
     "dsss_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),

@@ -20,6 +20,8 @@
 // The hash table is sized by the number of strings hashed in the round.
 #include "internal.cuh"
 #include "dp.cuh"
+#include "util.cuh"
+#include <algorithm>
 
 namespace dsss {
 
@@ -589,6 +591,201 @@ int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t dep
     if (m == 0) return DSSS_OK;
     DSSS_LAUNCH("k_prefix_hash", st, k_prefix_hash<<<grid_for(m, 256), 256, 0, st>>>(a, ids, m, depth, out));
     DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
+}
+
+// ------------------------------------------------- PEs on several GPUs ----
+// One distinguishing-prefix round split where the hashes cross GPUs: the
+// classification and the hashes of this GPU's candidates (dp_classify_hash),
+// the duplicate test on the hashes routed to this GPU (hash_route, hash_dups)
+// and the outcome applied to the candidate states (dp_apply).
+
+__global__ void k_hash_flags(const uint8_t* kind, uint64_t n, uint32_t* flag) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = kind[i] >= 2 ? 1u : 0u;
+}
+
+__global__ void k_hash_compact(ArenaDev a, const uint64_t* soff, const uint8_t* kind, const uint32_t* pos, uint64_t n,
+                               uint32_t depth, uint32_t* hpos, unsigned long long* hval) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    const uint32_t j = pos[i];
+    hpos[j] = (uint32_t)i;
+    hval[j] = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+}
+
+void layout_dp_split(Carve& c, DpSplitLayout& L, uint64_t n) {
+    const uint64_t N = n ? n : 1;
+    L.lens = c.take<uint32_t>(N);
+    L.soff = c.take<uint64_t>(N);
+    L.kind = c.take<uint8_t>(N);
+    L.flag = c.take<uint32_t>(N);
+    L.pos = c.take<uint32_t>(N);
+    L.counters = c.take<uint32_t>(16);
+    L.scan = c.take<unsigned char>(scan_scratch_bytes(N));
+}
+
+int dp_classify_hash(const DpSplitLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
+                     const uint8_t* state_in, uint32_t depth, uint32_t* dp, uint8_t* state_out, uint32_t* hpos,
+                     unsigned long long* hval, uint64_t* m, uint32_t* pin, cudaStream_t st) {
+    *m = 0;
+    if (n == 0) return DSSS_OK;
+    const unsigned grid = grid_for(n, 256);
+    DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    DSSS_LAUNCH("k_dp_classify", st,
+                k_dp_classify<<<grid, 256, 0, st>>>(state_in, state_in == nullptr, L.lens, lcp, n, depth, dp, state_out,
+                                                   L.kind, L.counters, nullptr, 1, nullptr));
+    DSSS_LAUNCH("k_hash_flags", st, k_hash_flags<<<grid, 256, 0, st>>>(L.kind, n, L.flag));
+    DSSS_TRY(exclusive_scan_u32(L.flag, L.pos, n, L.counters + 4, L.scan, st));
+    DSSS_LAUNCH("k_hash_compact", st,
+                k_hash_compact<<<grid, 256, 0, st>>>(a, L.soff, L.kind, L.pos, n, depth, hpos, hval));
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    *m = pin[4];
+    return DSSS_OK;
+}
+
+// Owner of a hash among nowner GPUs: equal slices of the 64-bit range.
+__device__ __forceinline__ uint32_t hash_owner(unsigned long long h, uint32_t nowner) {
+    return (uint32_t)__umul64hi(h, (unsigned long long)nowner);
+}
+
+__global__ void k_hash_owner(const unsigned long long* hval, uint64_t m, uint32_t nowner, uint32_t* owner,
+                             unsigned long long* counts) {
+    extern __shared__ uint32_t hcnt[];
+    for (uint32_t k = threadIdx.x; k < nowner; k += blockDim.x) hcnt[k] = 0;
+    __syncthreads();
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t o = hash_owner(hval[j], nowner);
+        owner[j] = o;
+        atomicAdd(&hcnt[o], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nowner; k += blockDim.x)
+        if (hcnt[k]) atomicAdd(&counts[k], (unsigned long long)hcnt[k]);
+}
+
+__global__ void k_route_scatter(const unsigned long long* hval, const uint32_t* hpos, const uint32_t* dest, uint64_t m,
+                                unsigned long long* out_hval, uint32_t* out_hpos) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint32_t d = dest[j];
+    out_hval[d] = hval[j];
+    out_hpos[d] = hpos[j];
+}
+
+void layout_hash_route(Carve& c, HashRouteLayout& L, uint64_t m, uint32_t nowner) {
+    const uint64_t M = m ? m : 1;
+    L.owner = c.take<uint32_t>(M);
+    L.dest = c.take<uint32_t>(M);
+    L.counts = c.take<unsigned long long>(nowner);
+    L.ms = c.take<unsigned char>(multisplit_scratch_bytes(M, nowner));
+}
+
+int hash_route(const HashRouteLayout& L, const unsigned long long* hval, const uint32_t* hpos, uint64_t m,
+               uint32_t nowner, unsigned long long* out_hval, uint32_t* out_hpos, uint64_t* counts_host,
+               cudaStream_t st) {
+    DSSS_CUDA(cudaMemsetAsync(L.counts, 0, nowner * sizeof(unsigned long long), st));
+    if (m) {
+        const unsigned g = (unsigned)std::min<uint64_t>(grid_for(m, 256), 148 * 8);
+        DSSS_LAUNCH("k_hash_owner", st,
+                    k_hash_owner<<<g, 256, nowner * sizeof(uint32_t), st>>>(hval, m, nowner, L.owner, L.counts));
+        DSSS_TRY(multisplit(L.owner, m, nowner, L.dest, L.ms, st));
+        DSSS_LAUNCH("k_route_scatter", st,
+                    k_route_scatter<<<grid_for(m, 256), 256, 0, st>>>(hval, hpos, L.dest, m, out_hval, out_hpos));
+    }
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(counts_host, L.counts, nowner * 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    return DSSS_OK;
+}
+
+__global__ void k_dup_insert(const unsigned long long* hval, uint64_t m, unsigned long long* tkeys, uint8_t* tdup,
+                             uint32_t mask, uint32_t* slot, uint32_t* err) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const unsigned long long h = hval[j];
+    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
+    for (uint32_t probe = 0;; ++probe) {
+        if (probe > mask) {
+            atomicExch(err, 1u);
+            sl = NO_SLOT;
+            break;
+        }
+        const unsigned long long prev = atomicCAS(&tkeys[sl], EMPTY_KEY, h);
+        if (prev == EMPTY_KEY) break;
+        if (prev == h) {
+            tdup[sl] = 1;
+            break;
+        }
+        sl = (sl + 1) & mask;
+    }
+    slot[j] = sl;
+}
+
+__global__ void k_dup_query(const uint32_t* slot, const uint8_t* tdup, uint64_t m, uint8_t* dup) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint32_t sl = slot[j];
+    dup[j] = (sl != NO_SLOT && tdup[sl]) ? 1 : 0;
+}
+
+void layout_hash_dups(Carve& c, HashDupLayout& L, uint64_t m) {
+    const uint64_t M = m ? m : 1;
+    L.slots = table_slots(M);
+    L.tkeys = c.take<unsigned long long>(L.slots);
+    L.tdup = c.take<uint8_t>(L.slots);
+    L.slot = c.take<uint32_t>(M);
+    L.err = c.take<uint32_t>(1);
+}
+
+int hash_dups(const HashDupLayout& L, const unsigned long long* hval, uint64_t m, uint8_t* dup, uint32_t* pin,
+              cudaStream_t st) {
+    if (m == 0) return DSSS_OK;
+    const uint64_t slots = table_slots(m);
+    DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+    DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
+    DSSS_CUDA(cudaMemsetAsync(L.err, 0, 4, st));
+    DSSS_LAUNCH("k_dup_insert", st,
+                k_dup_insert<<<grid_for(m, 256), 256, 0, st>>>(hval, m, L.tkeys, L.tdup, (uint32_t)(slots - 1), L.slot,
+                                                              L.err));
+    DSSS_LAUNCH("k_dup_query", st, k_dup_query<<<grid_for(m, 256), 256, 0, st>>>(L.slot, L.tdup, m, dup));
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.err, 4, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[0]) return fail(DSSS_EDEVICE, "duplicate test: hash table overflow");
+    return DSSS_OK;
+}
+
+__global__ void k_dp_apply(const uint32_t* hpos, const uint8_t* dup, uint64_t m, uint64_t n, uint8_t* state,
+                           uint32_t* err) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m || !dup[j]) return;
+    const uint32_t i = hpos[j];
+    if (i >= n) {
+        atomicExch(err, 1u);
+        return;
+    }
+    state[i] = 1;
+}
+
+__global__ void k_count_state(const uint8_t* state, uint64_t n, uint32_t* counters) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    block_count(counters, i < n && state[i]);
+}
+
+int dp_apply(uint32_t* counters, const uint32_t* hpos, const uint8_t* dup, uint64_t m, uint8_t* state, uint64_t n,
+             uint64_t* candidates, uint32_t* pin, cudaStream_t st) {
+    DSSS_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st));
+    if (m) DSSS_LAUNCH("k_dp_apply", st, k_dp_apply<<<grid_for(m, 256), 256, 0, st>>>(hpos, dup, m, n, state, counters + 1));
+    if (n) DSSS_LAUNCH("k_count_state", st, k_count_state<<<grid_for(n, 256), 256, 0, st>>>(state, n, counters));
+    DSSS_CUDA(cudaGetLastError());
+    DSSS_CUDA(cudaMemcpyAsync(pin, counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[1]) return fail(DSSS_EINVAL, "hash positions must be below n");
+    *candidates = pin[0];
     return DSSS_OK;
 }
 

@@ -65,4 +65,56 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
 int prefix_hash(const ArenaDev& a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out,
                 cudaStream_t st);
 
+// ---- PEs on several GPUs: one round split around the hash exchange ----
+struct DpSplitLayout {
+    uint32_t* lens;
+    uint64_t* soff;
+    uint8_t* kind;
+    uint32_t* flag;
+    uint32_t* pos;
+    uint32_t* counters;
+    unsigned char* scan;
+};
+void layout_dp_split(Carve& c, DpSplitLayout& L, uint64_t n);
+
+// Classifies the round at depth (state_in NULL: every position is a
+// candidate); dp gets the depth (or the length) of every candidate,
+// state_out the LCP duplicates and roots, and (hpos, hval)[0..*m) the
+// positions and hashes of every hashed candidate, in position order.
+int dp_classify_hash(const DpSplitLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
+                     const uint8_t* state_in, uint32_t depth, uint32_t* dp, uint8_t* state_out, uint32_t* hpos,
+                     unsigned long long* hval, uint64_t* m, uint32_t* pin, cudaStream_t st);
+
+struct HashRouteLayout {
+    uint32_t* owner;
+    uint32_t* dest;
+    unsigned long long* counts;
+    void* ms;
+};
+void layout_hash_route(Carve& c, HashRouteLayout& L, uint64_t m, uint32_t nowner);
+
+// Groups (hval, hpos) by owner GPU (equal slices of the hash range), stable;
+// counts_host[nowner] the group sizes.
+int hash_route(const HashRouteLayout& L, const unsigned long long* hval, const uint32_t* hpos, uint64_t m,
+               uint32_t nowner, unsigned long long* out_hval, uint32_t* out_hpos, uint64_t* counts_host,
+               cudaStream_t st);
+
+struct HashDupLayout {
+    uint64_t slots;
+    unsigned long long* tkeys;
+    uint8_t* tdup;
+    uint32_t* slot;
+    uint32_t* err;
+};
+void layout_hash_dups(Carve& c, HashDupLayout& L, uint64_t m);
+
+// dup[j] = 1 iff hval[j] occurs at least twice in hval[0..m).
+int hash_dups(const HashDupLayout& L, const unsigned long long* hval, uint64_t m, uint8_t* dup, uint32_t* pin,
+              cudaStream_t st);
+
+// state[hpos[j]] = 1 where dup[j]; *candidates = the positions with state 1.
+// counters: 2 device u32.
+int dp_apply(uint32_t* counters, const uint32_t* hpos, const uint8_t* dup, uint64_t m, uint8_t* state, uint64_t n,
+             uint64_t* candidates, uint32_t* pin, cudaStream_t st);
+
 }  // namespace dsss

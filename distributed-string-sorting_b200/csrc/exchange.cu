@@ -20,13 +20,15 @@
 
 namespace dsss {
 
+// ps sending PEs (this call's strings) and pr receiving PEs; the senders'
+// global PE ids start at q_first.
 __global__ void k_recv_slots(ArenaDev a, const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp,
-                             const uint64_t* pb, const uint64_t* bounds, const uint64_t* slot_base, uint32_t p,
-                             uint64_t n, uint32_t* cnt, uint32_t* rlcp, uint32_t* rindex, uint32_t* rpe,
-                             uint32_t* rsrc, uint32_t* err) {
+                             const uint64_t* pb, const uint64_t* bounds, const uint64_t* slot_base, uint32_t ps,
+                             uint32_t pr, uint32_t q_first, uint64_t n, uint32_t* cnt, uint32_t* rlcp,
+                             uint32_t* rindex, uint32_t* rpe, uint32_t* rsrc, uint32_t* err) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    uint32_t lo = 0, hi = p;  // PE of local position g: last q with pb[q] <= g
+    uint32_t lo = 0, hi = ps;  // PE of local position g: last q with pb[q] <= g
     while (hi - lo > 1) {
         uint32_t mid = (lo + hi) >> 1;
         if (pb[mid] <= g) lo = mid;
@@ -34,9 +36,9 @@ __global__ void k_recv_slots(ArenaDev a, const uint32_t* local_order, const uint
     }
     const uint32_t q = lo;
     const uint64_t i = g - pb[q];
-    const uint64_t* b = bounds + (uint64_t)q * (p + 1);
+    const uint64_t* b = bounds + (uint64_t)q * (pr + 1);
     lo = 0;
-    hi = p;  // bucket: last r with b[r] <= i
+    hi = pr;  // bucket: last r with b[r] <= i
     while (hi - lo > 1) {
         uint32_t mid = (lo + hi) >> 1;
         if (b[mid] <= i) lo = mid;
@@ -49,16 +51,29 @@ __global__ void k_recv_slots(ArenaDev a, const uint32_t* local_order, const uint
         atomicExch(err, 1u);
         return;
     }
-    const uint64_t o = slot_base[(uint64_t)r * p + q] + (i - b[r]);
+    const uint64_t o = slot_base[(uint64_t)r * ps + q] + (i - b[r]);
     if (o >= n) {
         atomicExch(err, 1u);
         return;
     }
     cnt[o] = d - l + 1;
     rlcp[o] = l;
-    rindex[o] = (uint32_t)i;
-    rpe[o] = q;
+    if (rindex) rindex[o] = (uint32_t)i;
+    if (rpe) rpe[o] = q_first + q;
     rsrc[o] = local_order[g];
+}
+
+// Char starts relative to each receiver's container (rbeg: pr + 1 slot bounds).
+__global__ void k_rel_starts(const uint32_t* cstart, uint64_t n, const uint64_t* rbeg, uint32_t pr, uint32_t* out) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    uint32_t lo = 0, hi = pr;  // receiver of slot o: last r with rbeg[r] <= o
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (rbeg[mid] <= o) lo = mid;
+        else hi = mid;
+    }
+    out[o] = cstart[o] - cstart[rbeg[lo]];
 }
 
 __global__ void k_sum_u32(const uint32_t* v, uint64_t n, unsigned long long* total) {
@@ -118,7 +133,8 @@ __global__ void k_recv_copy_warp(ArenaDev a, const uint32_t* cnt, const uint32_t
     }
 }
 
-void layout_exchange(Carve& c, ExchangeLayout& L, uint64_t n, uint32_t p) {
+void layout_exchange(Carve& c, ExchangeLayout& L, uint64_t n, uint32_t ps, uint32_t pr) {
+    if (pr == 0) pr = ps;
     uint64_t N = n ? n : 1;
     L.cnt = c.take<uint32_t>(N);
     L.cstart = c.take<uint32_t>(N);
@@ -126,53 +142,56 @@ void layout_exchange(Carve& c, ExchangeLayout& L, uint64_t n, uint32_t p) {
     L.longq = c.take<uint32_t>(N);
     L.counters = c.take<uint32_t>(4);
     L.total64 = c.take<unsigned long long>(1);
-    L.pb = c.take<uint64_t>(p + 1);
-    L.bounds = c.take<uint64_t>((uint64_t)p * (p + 1));
-    L.slot_base = c.take<uint64_t>((uint64_t)p * p);
+    L.pb = c.take<uint64_t>(ps + 1);
+    L.bounds = c.take<uint64_t>((uint64_t)ps * (pr + 1));
+    L.slot_base = c.take<uint64_t>((uint64_t)ps * pr);
+    L.rbeg = c.take<uint64_t>(pr + 1);
     L.scan = c.take<unsigned char>(scan_scratch_bytes(N));
 }
 
-int bucket_scatter(const ExchangeLayout& L, const ArenaDev& a, uint32_t p, const uint64_t* pb,
-                   const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, const uint64_t* intervals,
-                   uint64_t* char_total, uint8_t* recv_chars, uint64_t recv_capacity, uint64_t* recv_char_begin,
-                   uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe, uint64_t* recv_counts,
-                   uint64_t* recv_offsets, uint32_t* pin, cudaStream_t st) {
-    const uint64_t n = pb[p];
+int bucket_scatter_rect(const ExchangeLayout& L, const ArenaDev& a, uint32_t ps, uint32_t pr, uint32_t q_first,
+                        const uint64_t* pb, const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp,
+                        const uint64_t* intervals, uint64_t* char_total, uint8_t* recv_chars, uint64_t recv_capacity,
+                        uint64_t* recv_char_begin, uint32_t* recv_char_start, bool starts_per_receiver,
+                        uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe, uint64_t* recv_counts,
+                        uint64_t* recv_offsets, uint32_t* pin, cudaStream_t st) {
+    const uint64_t n = pb[ps];
     // interval bounds per sender, receive slots per (receiver, sender)
-    std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), slot((uint64_t)p * p), rbeg(p + 1, 0);
-    for (uint32_t q = 0; q < p; ++q) {
-        bounds[(uint64_t)q * (p + 1)] = 0;
+    std::vector<uint64_t> bounds((uint64_t)ps * (pr + 1)), slot((uint64_t)pr * ps), rbeg(pr + 1, 0);
+    for (uint32_t q = 0; q < ps; ++q) {
+        bounds[(uint64_t)q * (pr + 1)] = 0;
         uint64_t tot = 0;
-        for (uint32_t r = 0; r < p; ++r) {
-            tot += intervals[(uint64_t)q * p + r];
-            bounds[(uint64_t)q * (p + 1) + r + 1] = tot;
+        for (uint32_t r = 0; r < pr; ++r) {
+            tot += intervals[(uint64_t)q * pr + r];
+            bounds[(uint64_t)q * (pr + 1) + r + 1] = tot;
         }
         if (tot != pb[q + 1] - pb[q]) return fail(DSSS_EINVAL, "intervals of PE %u do not add up to its size", q);
     }
-    for (uint32_t r = 0; r < p; ++r) {
+    for (uint32_t r = 0; r < pr; ++r) {
         uint64_t run = rbeg[r];
-        for (uint32_t q = 0; q < p; ++q) {
-            slot[(uint64_t)r * p + q] = run;
-            if (recv_counts) recv_counts[(uint64_t)r * p + q] = intervals[(uint64_t)q * p + r];
-            if (recv_offsets) recv_offsets[(uint64_t)r * p + q] = bounds[(uint64_t)q * (p + 1) + r];
-            run += intervals[(uint64_t)q * p + r];
+        for (uint32_t q = 0; q < ps; ++q) {
+            slot[(uint64_t)r * ps + q] = run;
+            if (recv_counts) recv_counts[(uint64_t)r * ps + q] = intervals[(uint64_t)q * pr + r];
+            if (recv_offsets) recv_offsets[(uint64_t)r * ps + q] = bounds[(uint64_t)q * (pr + 1) + r];
+            run += intervals[(uint64_t)q * pr + r];
         }
         rbeg[r + 1] = run;
     }
     if (n == 0) {
         *char_total = 0;
         if (recv_char_begin)
-            for (uint32_t r = 0; r <= p; ++r) recv_char_begin[r] = 0;
+            for (uint32_t r = 0; r <= pr; ++r) recv_char_begin[r] = 0;
         return DSSS_OK;
     }
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 4 * sizeof(uint32_t), st));
-    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (ps + 1) * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.slot_base, slot.data(), slot.size() * 8, cudaMemcpyHostToDevice, st));
+    DSSS_CUDA(cudaMemcpyAsync(L.rbeg, rbeg.data(), rbeg.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_LAUNCH("k_recv_slots", st,
                 k_recv_slots<<<grid_for(n, 256), 256, 0, st>>>(a, local_order, lcp, dp, L.pb, L.bounds, L.slot_base,
-                                                              p, n, L.cnt, recv_lcp, recv_index, recv_pe, L.src,
-                                                              L.counters + 2));
+                                                              ps, pr, q_first, n, L.cnt, recv_lcp, recv_index, recv_pe,
+                                                              L.src, L.counters + 2));
     DSSS_TRY(exclusive_scan_u32(L.cnt, L.cstart, n, L.counters, L.scan, st));
     DSSS_CUDA(cudaMemsetAsync(L.total64, 0, 8, st));
     DSSS_LAUNCH("k_sum_u32", st, k_sum_u32<<<148 * 4, 256, 0, st>>>(L.cnt, n, L.total64));
@@ -184,14 +203,21 @@ int bucket_scatter(const ExchangeLayout& L, const ArenaDev& a, uint32_t p, const
     if (total64 >= (1ull << 32)) return fail(DSSS_ENOTSUP, "receive containers over 4 GiB per call");
     *char_total = pin[0];
     if (recv_char_begin) {
-        std::vector<uint32_t> cs(p + 1);
-        for (uint32_t r = 0; r < p; ++r) {
+        std::vector<uint32_t> cs(pr + 1);
+        for (uint32_t r = 0; r < pr; ++r) {
             if (rbeg[r] < n) DSSS_CUDA(cudaMemcpyAsync(&cs[r], L.cstart + rbeg[r], 4, cudaMemcpyDeviceToHost, st));
             else cs[r] = pin[0];
         }
         DSSS_CUDA(cudaStreamSynchronize(st));
-        for (uint32_t r = 0; r < p; ++r) recv_char_begin[r] = cs[r];
-        recv_char_begin[p] = pin[0];
+        for (uint32_t r = 0; r < pr; ++r) recv_char_begin[r] = cs[r];
+        recv_char_begin[pr] = pin[0];
+    }
+    if (recv_char_start) {
+        if (starts_per_receiver)
+            DSSS_LAUNCH("k_rel_starts", st,
+                        k_rel_starts<<<grid_for(n, 256), 256, 0, st>>>(L.cstart, n, L.rbeg, pr, recv_char_start));
+        else
+            DSSS_CUDA(cudaMemcpyAsync(recv_char_start, L.cstart, n * 4, cudaMemcpyDeviceToDevice, st));
     }
     if (!recv_chars) return DSSS_OK;
     if (recv_capacity < *char_total) return fail(DSSS_EINVAL, "receive buffer of %llu bytes < %llu needed",
@@ -204,6 +230,16 @@ int bucket_scatter(const ExchangeLayout& L, const ArenaDev& a, uint32_t p, const
                                                          L.counters + 1));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
+}
+
+int bucket_scatter(const ExchangeLayout& L, const ArenaDev& a, uint32_t p, const uint64_t* pb,
+                   const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, const uint64_t* intervals,
+                   uint64_t* char_total, uint8_t* recv_chars, uint64_t recv_capacity, uint64_t* recv_char_begin,
+                   uint32_t* recv_lcp, uint32_t* recv_index, uint32_t* recv_pe, uint64_t* recv_counts,
+                   uint64_t* recv_offsets, uint32_t* pin, cudaStream_t st) {
+    return bucket_scatter_rect(L, a, p, p, 0, pb, local_order, lcp, dp, intervals, char_total, recv_chars,
+                               recv_capacity, recv_char_begin, nullptr, false, recv_lcp, recv_index, recv_pe,
+                               recv_counts, recv_offsets, pin, st);
 }
 
 }  // namespace dsss

@@ -197,4 +197,92 @@ int partition_pes(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32_
     return partition_sets(L, ctx, a, 1, p, pb, local_order, dp, sampler, factor, intervals, st);
 }
 
+// ---- PEs on several GPUs: search splitters gathered from every GPU ----
+__device__ __forceinline__ int str_cmp2(const uint8_t* ca, uint64_t oa, uint32_t la, const uint8_t* cb, uint64_t ob,
+                                        uint32_t lb) {
+    for (uint32_t d = 0;; d += 8) {
+        uint64_t x = key8(ca, oa, la, d), y = key8(cb, ob, lb, d);
+        if (x != y) return x < y ? -1 : 1;
+        if (zero_byte(x) < 8) return 0;
+    }
+}
+
+// One thread per (local PE g, splitter k): the reference's binary search of
+// PE g's sorted strings for splitter k; goff[g]: the global index of PE g's
+// first string (indexed compare).
+__global__ void k_binsearch_ext(ArenaDev a, const uint32_t* local_order, const uint64_t* pb, const uint64_t* goff,
+                                uint32_t npe, ArenaDev sp, const uint64_t* spl_index, int indexed, uint64_t* pos) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nspl = (uint32_t)sp.n;
+    if (t >= (uint64_t)npe * nspl) return;
+    const uint32_t g = (uint32_t)(t / nspl), k = (uint32_t)(t % nspl);
+    const uint64_t base = pb[g];
+    uint64_t left = 0, right = pb[g + 1] - base;
+    uint64_t so;
+    uint32_t sl;
+    str_of(sp, k, so, sl);
+    while (left != right) {
+        const uint64_t d = (right - left) / 2;
+        uint64_t off;
+        uint32_t len;
+        str_of(a, local_order[base + left + d], off, len);
+        int res = str_cmp2(a.chars, off, len, sp.chars, so, sl);
+        if (res == 0 && indexed) res = (int)(int32_t)(uint32_t)((left + d + goff[g]) - spl_index[k]);
+        if (res < 0) {
+            left = left + d + 1;
+        } else if (res == 0) {
+            pos[t] = left + d;
+            return;
+        } else {
+            right = left + d;
+        }
+    }
+    pos[t] = left;
+}
+
+int partition_search(Ctx* ctx, const ArenaDev& a, uint32_t p_local, const uint64_t* pb, const uint32_t* local_order,
+                     const ArenaDev& sp, const uint64_t* spl_index_host, uint32_t p_global, const uint64_t* goff_host,
+                     int indexed, uint64_t* intervals, cudaStream_t st) {
+    const uint32_t nspl = (uint32_t)sp.n;
+    if (nspl + 1 > p_global) return fail(DSSS_EINVAL, "%u splitters for %u PEs", nspl, p_global);
+    const uint64_t tasks = (uint64_t)p_local * nspl;
+    Carve sz(nullptr);
+    sz.take<uint64_t>(p_local + 1);
+    sz.take<uint64_t>(p_local + 1);
+    sz.take<uint64_t>(nspl + 1);
+    sz.take<uint64_t>(tasks + 1);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    Carve c(ctx->ws);
+    uint64_t* d_pb = c.take<uint64_t>(p_local + 1);
+    uint64_t* d_goff = c.take<uint64_t>(p_local + 1);
+    uint64_t* d_si = c.take<uint64_t>(nspl + 1);
+    uint64_t* d_pos = c.take<uint64_t>(tasks + 1);
+    std::vector<uint64_t> gv(p_local + 1, 0), siv(nspl + 1, 0), pos(tasks);
+    if (indexed) {
+        for (uint32_t g = 0; g < p_local; ++g) gv[g] = goff_host[g];
+        for (uint32_t k = 0; k < nspl; ++k) siv[k] = spl_index_host[k];
+    }
+    if (tasks) {
+        DSSS_CUDA(cudaMemcpyAsync(d_pb, pb, (p_local + 1) * 8, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(d_goff, gv.data(), (p_local + 1) * 8, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(d_si, siv.data(), (nspl + 1) * 8, cudaMemcpyHostToDevice, st));
+        DSSS_LAUNCH("k_binsearch", st,
+                    k_binsearch_ext<<<grid_for(tasks, 128), 128, 0, st>>>(a, local_order, d_pb, d_goff, p_local, sp,
+                                                                          d_si, indexed, d_pos));
+        DSSS_CUDA(cudaGetLastError());
+        DSSS_CUDA(cudaMemcpyAsync(pos.data(), d_pos, tasks * 8, cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+    }
+    // compute_interval_binary (misc.hpp:376-395)
+    for (uint32_t g = 0; g < p_local; ++g) {
+        uint64_t prev = 0;
+        for (uint32_t r = 0; r < p_global; ++r) {
+            const uint64_t cur = r < nspl ? pos[(uint64_t)g * nspl + r] : pb[g + 1] - pb[g];
+            intervals[(uint64_t)g * p_global + r] = cur - prev;
+            prev = cur;
+        }
+    }
+    return DSSS_OK;
+}
+
 }  // namespace dsss

@@ -35,4 +35,12 @@ int partition_sets(const PartitionLayout& L, Ctx* ctx, const ArenaDev& a, uint32
                    const uint64_t* pb, const uint32_t* local_order, const uint32_t* dp, uint32_t sampler,
                    uint32_t factor, uint64_t* intervals, cudaStream_t st);
 
+// PEs on several GPUs: intervals (host, p_local x p_global) of this GPU's
+// p_local PEs against the nspl = sp.n <= p_global - 1 splitters in arena sp
+// (gathered from every GPU).  Indexed compare: goff_host[g] is the global
+// index of local PE g's first string, spl_index_host[k] the splitter's.
+int partition_search(Ctx* ctx, const ArenaDev& a, uint32_t p_local, const uint64_t* pb, const uint32_t* local_order,
+                     const ArenaDev& sp, const uint64_t* spl_index_host, uint32_t p_global, const uint64_t* goff_host,
+                     int indexed, uint64_t* intervals, cudaStream_t st);
+
 }  // namespace dsss

@@ -250,6 +250,66 @@ int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order
 int dsss_adjacent_lcp_noalloc(const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,
                               dsss_stream_t stream);
 
+/* ---- PEs on several GPUs ---------------------------------------------------
+ * One process per GPU, p_local PEs each (global PE ids q_first..); the caller
+ * runs the collectives between these calls (NCCL through torch.distributed in
+ * the Python package's dist.py).  Each entry is one piece of the reference's
+ * distributed path around one of its exchanges.
+ *
+ * One BloomFilter::filter round on this GPU's sorted PEs (order/lcp as from
+ * dsss_local_sort_lcp with the PE bounds): classification at depth (EOS, LCP
+ * duplicates, roots, hashed: bloomfilter.hpp:1162-1227, 1273-1331), dp of every
+ * candidate, state_out[i] = 1 for LCP duplicates and roots, and the positions
+ * and XXH64 filter hashes of every hashed candidate (hpos, hval, *m of them,
+ * in position order).  state_in NULL: the first round (all candidates). */
+int dsss_dp_classify_hash(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, const uint32_t* lcp,
+                          const uint8_t* state_in, uint32_t depth, uint32_t* dp, uint8_t* state_out, uint32_t* hpos,
+                          uint64_t* hval, uint64_t* m, dsss_stream_t stream);
+/* Groups (hval, hpos) by owning GPU, equal slices of the hash range as
+ * SendOnlyHashesToFilter::sendToFilter (bloomfilter.hpp:581-640) cuts it;
+ * counts (HOST, nowner): the group sizes, in owner order. */
+int dsss_hash_route(dsss_ctx* ctx, const uint64_t* hval, const uint32_t* hpos, uint64_t m, uint32_t nowner,
+                    uint64_t* out_hval, uint32_t* out_hpos, uint64_t* counts, dsss_stream_t stream);
+/* Owner side of FindDuplicates::findDuplicates (bloomfilter.hpp:662-765):
+ * dup[j] = 1 iff hval[j] occurs at least twice among the m received hashes. */
+int dsss_hash_dups(dsss_ctx* ctx, const uint64_t* hval, uint64_t m, uint8_t* dup, dsss_stream_t stream);
+/* state[hpos[j]] = 1 where dup[j] (the duplicates returned to their senders,
+ * bloomfilter.hpp:767-817); *candidates = positions with state 1. */
+int dsss_dp_apply(dsss_ctx* ctx, const uint32_t* hpos, const uint8_t* dup, uint64_t m, uint8_t* state, uint64_t n,
+                  uint64_t* candidates, dsss_stream_t stream);
+/* Packs strings ids[j] truncated to min(length, trunc[j]) (trunc NULL: whole)
+ * back to back with a NUL each (the splitter sample, samplingStrategies.hpp:
+ * 57-89); out_offsets/out_lengths (device, m); *bytes the packed size;
+ * out_chars NULL: sizes only. */
+int dsss_pack_strings(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* ids, const uint32_t* trunc, uint64_t m,
+                      uint8_t* out_chars, uint64_t capacity, uint64_t* out_offsets, uint32_t* out_lengths,
+                      uint64_t* bytes, dsss_stream_t stream);
+/* compute_interval_binary (misc.hpp:376-414) of this GPU's p_local PEs against
+ * splitters->n <= p_global - 1 splitters gathered from every GPU; intervals
+ * (HOST, p_local x p_global).  indexed: spl_index (HOST) the splitters' global
+ * indices and pe_index (HOST, p_local) the global index of each local PE's
+ * first string (indexStringCompare, misc.hpp:335-345). */
+int dsss_partition_search(dsss_ctx* ctx, const dsss_arena* in, uint32_t p_local, const uint64_t* part_begin,
+                          const uint32_t* local_order, const dsss_arena* splitters, const uint64_t* spl_index,
+                          uint32_t p_global, const uint64_t* pe_index, int indexed, uint64_t* intervals,
+                          dsss_stream_t stream);
+/* Sender side of AllToAllStringImplPrefixDoubling::alltoallv (alltoall.hpp:
+ * 910-1008): the receive container of every one of the p_global PEs, from this
+ * GPU's senders, back to back (bytes [lcp', dp) + NUL per string); per string
+ * char_start (relative to its receiver's container) and the sent LCP;
+ * recv_char_begin (HOST, p_global + 1), counts/offsets (HOST, [r*p_local + q]). */
+int dsss_bucket_send(dsss_ctx* ctx, const dsss_arena* in, uint32_t p_local, const uint64_t* part_begin,
+                     const uint32_t* local_order, const uint32_t* lcp, const uint32_t* dp, uint32_t p_global,
+                     uint32_t q_first, const uint64_t* intervals, uint8_t* send_chars, uint64_t capacity,
+                     uint64_t* char_total, uint64_t* recv_char_begin, uint32_t* char_start, uint32_t* send_lcp,
+                     uint64_t* counts, uint64_t* offsets, dsss_stream_t stream);
+/* Receiver side: copies blocks (HOST, nblocks x {src string, dst string,
+ * strings, src byte, dst byte, bytes}) of received containers into receiver
+ * order; dst_start = src_start + the block's dst byte. */
+int dsss_regroup(dsss_ctx* ctx, uint32_t nblocks, const uint64_t* blocks, const uint8_t* src_chars,
+                 uint8_t* dst_chars, const uint32_t* src_start, uint32_t* dst_start, const uint32_t* src_lcp,
+                 uint32_t* dst_lcp, uint64_t n, dsss_stream_t stream);
+
 /* ---- request server (no reference counterpart) ---------------------------
  * Continuous batching of independent sort requests onto one GPU.  Requests
  * (host arenas, p PEs each) are queued on submit; worker threads, each with
