@@ -1,0 +1,81 @@
+"""The distributed path (dist.py) on CPU ranks over gloo, with the host
+backend: collectives, routing of hashes, sample gathering, container exchange
+and regrouping, checked against the oracle's single-process run of the whole
+input.  test_gpu_dist.py runs the same flow with the CUDA backend."""
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+from inputs import random_strings, run_suffixes, shared_head, with_duplicates
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def run_ranks(world, inputs, backend):
+    import torch.multiprocessing as mp
+    from dist_worker import rank_main
+    with tempfile.TemporaryDirectory() as tmp:
+        mp.spawn(rank_main, args=(world, free_port(), tmp, inputs, backend), nprocs=world, join=True)
+        return [dict(np.load(os.path.join(tmp, f"rank{r}.npz"))) for r in range(world)]
+
+
+def check_against_oracle(orc, strs, pb, results, sampler, exact_ties=True):
+    from dist_oracle import pack_list
+    chars, offs, lens, _ = pack_list(strs)
+    s = orc.Strings(chars, offs.astype(np.uint64), lens.astype(np.uint32))
+    ref = orc.pd_sort(s, np.asarray(pb, np.uint64), indexed=sampler == 2)
+    p = len(pb) - 1
+    rb = np.concatenate([[0], np.cumsum(ref["recv_counts"])]).astype(np.int64)
+    for r in results:
+        q0, q1, s0 = int(r["q0"]), int(r["q1"]), int(r["s0"])
+        s1 = int(pb[q1])
+        assert np.array_equal(r["local_order"] + s0, ref["order"][s0:s1].astype(np.int64))
+        if p == 1:
+            continue
+        assert np.array_equal(r["dp"], ref["dp"][s0:s1].astype(np.int64))
+        assert np.array_equal(r["intervals"], ref["intervals"][q0:q1].astype(np.int64))
+        assert np.array_equal(r["recv_counts"], ref["recv_counts"][q0:q1].astype(np.int64))
+        b0, b1 = rb[q0], rb[q1]
+        gi, gp = r["perm_index"], r["perm_pe"]
+        ri, rp = ref["perm_index"][b0:b1].astype(np.int64), ref["perm_pe"][b0:b1].astype(np.int64)
+        assert np.array_equal(r["merged_lcp"], ref["merged_lcp"][b0:b1].astype(np.int64))
+        if exact_ties:
+            assert np.array_equal(gi, ri) and np.array_equal(gp, rp)
+        else:
+            assert sorted(zip(gp.tolist(), gi.tolist())) == sorted(zip(rp.tolist(), ri.tolist()))
+
+
+def cases():
+    a = random_strings(1500, 0, 30, b"ABC", seed=41)
+    b = with_duplicates(random_strings(1200, 0, 20, b"AB", seed=42), 0.3, seed=43)
+    c = shared_head(1000, 120, 10, seed=44)
+    d = run_suffixes(seed=45)[:1500]
+    return [("random", a), ("dups", b), ("shared_head", c), ("runs", d)]
+
+
+CASES = cases()
+
+
+@pytest.mark.parametrize("sampler", [0, 2])
+@pytest.mark.parametrize("name,strs", CASES, ids=[c[0] for c in CASES])
+def test_two_ranks_match_oracle(orc, name, strs, sampler):
+    n = len(strs)
+    pb = [0, n // 7, n // 3, n // 2, (4 * n) // 5, n]          # 5 PEs of uneven sizes
+    splits = [0, 2, 5]                                        # rank 0: PEs 0-1, rank 1: PEs 2-4
+    res = run_ranks(2, (strs, pb, splits, sampler), "oracle")
+    check_against_oracle(orc, strs, pb, res, sampler)
+
+
+def test_three_ranks_one_pe_each(orc):
+    strs = CASES[0][1]
+    n = len(strs)
+    pb = [0, n // 3, (2 * n) // 3, n]
+    res = run_ranks(3, (strs, pb, [0, 1, 2, 3], 0), "oracle")
+    check_against_oracle(orc, strs, pb, res, 0)

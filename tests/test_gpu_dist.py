@@ -1,0 +1,43 @@
+"""The distributed path with the CUDA backend: two or three ranks, each with
+its own context on the one GPU, exchanging through gloo (host memory); the
+ranks' kernels never wait on one another.  Checked against the oracle's
+single-process run of the whole input, as test_dist.py checks the host
+backend."""
+import pytest
+
+from inputs import random_strings, run_suffixes, shared_head, with_duplicates
+from test_dist import check_against_oracle, run_ranks
+
+pytestmark = pytest.mark.gpu
+
+
+def gen_inputs():
+    import __graft_entry__
+    d = __graft_entry__.load_package()
+    dn = d.gen_dn(12000, 60, 30, seed=7)
+    return [
+        ("dn", [dn.get(i) for i in range(dn.n)]),
+        ("dups", with_duplicates(random_strings(4000, 0, 24, b"ABC", seed=52), 0.3, seed=53)),
+        ("shared_head", shared_head(3000, 200, 12, seed=54)),
+        ("runs", run_suffixes(seed=55)),
+    ]
+
+
+CASES = gen_inputs()
+
+
+@pytest.mark.parametrize("sampler", [0, 2])
+@pytest.mark.parametrize("name,strs", CASES, ids=[c[0] for c in CASES])
+def test_gpu_ranks_match_oracle(orc, name, strs, sampler):
+    n = len(strs)
+    pb = [0, n // 9, n // 3, n // 2, (5 * n) // 6, n]
+    res = run_ranks(2, (strs, pb, [0, 3, 5], sampler), "gpu")
+    check_against_oracle(orc, strs, pb, res, sampler, exact_ties=False)
+
+
+def test_gpu_three_ranks(orc):
+    strs = CASES[0][1]
+    n = len(strs)
+    pb = [0, n // 4, n // 2, (3 * n) // 4, n]
+    res = run_ranks(3, (strs, pb, [0, 1, 3, 4], 0), "gpu")
+    check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
