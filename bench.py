@@ -222,6 +222,68 @@ def bench_serving(d, torch, p=8, n_req=48, rate=250.0, seed=2024, workers=4, max
     }
 
 
+def run_dist(args, cfg):
+    """--mode dist: one distributed sort over all ranks (dist.py), each rank
+    holding p PEs of n strings of the D/N rule (rank-seeded), exchanging over
+    NCCL; device-timed per step, max over ranks."""
+    import datetime
+    import torch
+    import torch.distributed as tdist
+    import __graft_entry__
+    d = __graft_entry__.load_package()
+    import dsss_b200.dist as D
+    n, L, k, p, desc = cfg
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world == 1:
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        tdist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                 timeout=datetime.timedelta(seconds=300))
+    else:
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    hs = d.gen_dn(n, L, k, seed=1 + rank)
+    ctx = d.Context(local)
+    be = D.GpuBackend(ctx)
+    ds = be.strings(hs)
+    pb = d.equal_parts(n, p).astype(np.int64)
+    comm = D.Comm()
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        res = D.sort(comm, be, ds, pb)
+    tdist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            res = D.sort(comm, be, ds, pb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    tdist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    ms = float(t.item())
+    if rank == 0:
+        line = {
+            "metric": "strings/s", "value": n * world / (ms * 1e-3), "unit": "strings/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded D/N generator)",
+            "config": {"workload": desc + f", {world} GPU(s) x {p} PEs, one distributed sort", "n_per_gpu": n,
+                       "len": L, "p_per_gpu": p, "parallelism": f"{world} ranks, NCCL exchanges (dist.py)",
+                       "l2": "inputs > L2, no flush"},
+            "mode": "dist", "dp_rounds": res.get("dp_rounds"), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    tdist.destroy_process_group()
+
+
 def run_reference(args, cfg):
     """--impl reference: the CPU port of the reference path on all host threads."""
     import __graft_entry__
@@ -272,6 +334,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "dist"],
+                    help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
@@ -282,6 +346,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args, cfg)
+        return
+    if args.mode == "dist":
+        run_dist(args, cfg)
         return
 
     import torch

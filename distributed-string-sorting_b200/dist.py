@@ -102,7 +102,7 @@ class Comm:
         import torch
         if isinstance(t, np.ndarray):
             return self.alltoallv(torch.from_numpy(np.ascontiguousarray(t)), send_counts, recv_counts).numpy()
-        dev = t.device if (self.device_ok and t.is_cuda) else torch.device("cpu")
+        dev = (t.device if t.is_cuda else self._home()) if self.device_ok else torch.device("cpu")
         src = t.to(dev)
         dt = src.dtype
         if dt == torch.uint64:

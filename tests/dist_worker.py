@@ -9,7 +9,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def rank_main(rank, world, port, outdir, inputs, backend):
+def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     sys.path.insert(0, ROOT)
@@ -21,7 +21,10 @@ def rank_main(rank, world, port, outdir, inputs, backend):
     d = __graft_entry__.load_package()
     import dsss_b200.dist as D
     strs, pb, splits, sampler = inputs
-    tdist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    if pg == "nccl":
+        import torch
+        torch.cuda.set_device(0)
+    tdist.init_process_group(pg, rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         q0, q1 = splits[rank], splits[rank + 1]
         s0, s1 = int(pb[q0]), int(pb[q1])

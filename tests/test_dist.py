@@ -18,11 +18,11 @@ def free_port():
         return s.getsockname()[1]
 
 
-def run_ranks(world, inputs, backend):
+def run_ranks(world, inputs, backend, pg="gloo"):
     import torch.multiprocessing as mp
     from dist_worker import rank_main
     with tempfile.TemporaryDirectory() as tmp:
-        mp.spawn(rank_main, args=(world, free_port(), tmp, inputs, backend), nprocs=world, join=True)
+        mp.spawn(rank_main, args=(world, free_port(), tmp, inputs, backend, pg), nprocs=world, join=True)
         return [dict(np.load(os.path.join(tmp, f"rank{r}.npz"))) for r in range(world)]
 
 

@@ -41,3 +41,13 @@ def test_gpu_three_ranks(orc):
     pb = [0, n // 4, n // 2, (3 * n) // 4, n]
     res = run_ranks(3, (strs, pb, [0, 1, 3, 4], 0), "gpu")
     check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
+
+
+def test_nccl_single_rank(orc):
+    """The NCCL code path of the collectives (payloads stay on the GPU), with
+    one rank holding all five PEs."""
+    strs = CASES[1][1]
+    n = len(strs)
+    pb = [0, n // 5, (2 * n) // 5, (3 * n) // 5, (4 * n) // 5, n]
+    res = run_ranks(1, (strs, pb, [0, 5], 0), "gpu", pg="nccl")
+    check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
