@@ -49,6 +49,11 @@ class PdResult(ctypes.Structure):
                 ("merged_lcp", ctypes.c_void_p), ("recv_counts", ctypes.c_void_p)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("sort_small_max", ctypes.c_int64), ("sort_pivot", ctypes.c_int64), ("dp_filter_min", ctypes.c_int64),
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("settings_tried", ctypes.c_uint32)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("p", ctypes.c_uint32),
                 ("max_sets", ctypes.c_uint32), ("max_batch_strings", ctypes.c_uint64),
@@ -102,6 +107,8 @@ _SIGS = {
     "dsss_regroup": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _U64, _P]),
     "dsss_tune_set": (_I, [ctypes.c_char_p, ctypes.c_int64]),
     "dsss_tune_get": (_I, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
+    "dsss_autotune": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts), _U32, ctypes.POINTER(Tuning),
+                           _P]),
     "dsss_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
     "dsss_server_submit": (_I, [_P, ctypes.POINTER(Arena), _P, ctypes.POINTER(PdResult), ctypes.POINTER(_U64)]),
     "dsss_server_wait": (_I, [_P, _U64, ctypes.c_int64, ctypes.POINTER(RequestStats)]),
@@ -474,6 +481,17 @@ class tuned:
     def __exit__(self, *exc):
         for k, v in self.old.items():
             tune_set(k, v)
+
+
+def autotune(ctx: Context, ds, p: int, part_begin=None, nsets: int = 1, sampler: int = 0, trials: int = 2,
+             stream=None) -> dict:
+    """dsss_autotune on this input: times the knob grid and leaves the fastest
+    setting in force; returns it with its time and the default's."""
+    pb = equal_parts(ds.n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    t = Tuning()
+    check(lib().dsss_autotune(ctx.h, ctypes.byref(ds.arena()), nsets, p, _ptr(pb), ctypes.byref(_opts(sampler)),
+                              trials, ctypes.byref(t), _stream_ptr(stream)))
+    return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
 
 def clock_now() -> float:

@@ -114,6 +114,20 @@ int dsss_abi_version(void);
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 
+/* Autotuner (no reference counterpart): runs the full path (as
+ * dsss_pd_sort_batched; nsets = 1 for one set) on the given device input
+ * under each setting of a grid of the knobs above (sort_small_max 256 / 1024 /
+ * 4096, sort_pivot on / off, the DP filter on / off), 1 + trials runs each,
+ * and leaves the fastest setting in force for later calls.  out: the chosen
+ * setting, its time (minimum over trials) and the default setting's time. */
+typedef struct {
+    int64_t sort_small_max, sort_pivot, dp_filter_min;
+    double best_ms, default_ms;
+    uint32_t settings_tried;
+} dsss_tuning;
+int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* part_begin,
+                  const dsss_opts* opts, uint32_t trials, dsss_tuning* out, dsss_stream_t stream);
+
 /* ---- full path ---------------------------------------------------------- */
 
 /* DistributedPrefixDoublingSort<...>::sort (src/sorter/distributed/prefix_doubling.hpp:200-295):

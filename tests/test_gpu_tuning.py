@@ -56,3 +56,18 @@ def test_sort_knobs(dsss, orc, ctx, knobs):
     ro, rl = orc.local_sort(orc.Strings.from_host(hs), np.array([0, n], np.uint64))
     assert np.array_equal(u64(order, n), ro)
     assert np.array_equal(u64(lcp, n), rl)
+
+
+def test_autotune_picks_a_grid_setting(dsss, orc, ctx):
+    """dsss_autotune leaves one setting of its grid in force; results stay exact."""
+    hs = dsss.gen_suffix_strings(80000, 256, seed=8)
+    ds = dsss.DeviceStrings(hs)
+    with dsss.tuned(sort_small_max=-1, sort_pivot=-1, dp_filter_min=-1):
+        t = dsss.autotune(ctx, ds, 4, trials=1)
+        assert t["settings_tried"] == 12
+        assert t["sort_small_max"] in (256, 1024, 4096) and t["sort_pivot"] in (0, 1)
+        assert t["dp_filter_min"] in (0, 1 << 40)
+        assert 0 < t["best_ms"] <= t["default_ms"]
+        assert dsss.tune_get("sort_small_max") == t["sort_small_max"]
+        out = dsss.pd_sort(ctx, ds, 4)
+        check_pd(dsss, orc, hs, out, 4)
