@@ -134,6 +134,7 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
         for k in range(nsets):
             outs[k] = d.pd_sort(ctx, ds_each[k], p, out=outs[k])
 
+    tuning = d.autotune(ctx, ds_all, p, part_begin=pb, nsets=nsets, trials=1)
     res = {}
     for name, fn in (("plain", plain), ("batched", batched)):
         for _ in range(warmup):
@@ -157,7 +158,7 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
         "plain_ms": res["plain"], "batched_ms": res["batched"],
         "plain_strings_per_s": n / (res["plain"] * 1e-3), "batched_strings_per_s": n / (res["batched"] * 1e-3),
         "batched_char_gbs": char_bytes / (res["batched"] * 1e-3) / 1e9,
-        "speedup": res["plain"] / res["batched"], "dp_identical": bool(same),
+        "speedup": res["plain"] / res["batched"], "dp_identical": bool(same), "tuning": tuning,
     }
 
 
@@ -334,6 +335,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dist"],
                     help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL)")
     args = ap.parse_args()
@@ -372,6 +374,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    # knobs picked by the autotuner on this input (results never depend on them)
+    tuning = None if args.no_autotune else d.autotune(ctx, ds, p, trials=1)
     for _ in range(args.warmup):
         out = d.pd_sort(ctx, ds, p, out=out)
     torch.cuda.synchronize()
@@ -473,6 +477,7 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": None, "algo_bytes": algo_bytes,
                          "algo_formula": "D + 20 n", "sort_ms": sort_ms, "sort_launches": sort_launches},
+            "tuning": tuning,
             "stages_ms": stages,
             "kernels_ms": {k2: round(v[1] / args.steps, 4) for k2, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
             "gpu_launches": int(round(launches_per_step * args.steps)),
