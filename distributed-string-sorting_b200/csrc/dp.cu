@@ -73,42 +73,69 @@ __device__ __forceinline__ void block_count(uint32_t* ctr, bool flag) {
     __syncthreads();
 }
 
-__global__ void k_dp_classify(const uint8_t* st, int all, const uint32_t* lens, const uint32_t* lcp, uint64_t n,
-                              uint32_t depth, uint32_t* dp, uint8_t* st_next, uint8_t* kind, uint32_t* counters,
-                              const uint64_t* set_begin, uint32_t nsets, uint32_t* set_cnt) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool hashed = false, stays = false;
-    if (i < n) {
-        uint8_t k = 0, nx = 0;
-        if (all || st[i]) {
-            const uint32_t L = lens[i];
-            if (depth > L) {
-                dp[i] = L;  // end of string before the depth (EOS)
-            } else {
-                dp[i] = depth;
-                if (i > 0 && (all || st[i - 1]) && lcp[i] >= depth) {
-                    k = 1;
-                    nx = 1;
+// Grid of the grid-stride kernels: up to eight 256-thread blocks per SM.
+static unsigned stride_grid(uint64_t n) { return (unsigned)std::min<uint64_t>(grid_for(n, 256), 148 * 8); }
+
+// Adds v (per thread) over the block to *ctr with one atomic per block
+// (blockDim.x == 256, called by every thread of the block).
+__device__ __forceinline__ void block_add(uint32_t* ctr, uint32_t v) {
+    __shared__ uint32_t part[8];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULLM, v, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += part[w];
+        if (t) atomicAdd(ctr, t);
+    }
+    __syncthreads();
+}
+
+// Grid-stride over positions (grid a few blocks per SM): one pair of counter
+// atomics per block instead of per 256 positions.
+__global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all, const uint32_t* lens,
+                                                     const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
+                                                     uint8_t* st_next, uint8_t* kind, uint32_t* counters,
+                                                     const uint64_t* set_begin, uint32_t nsets, uint32_t* set_cnt) {
+    uint32_t nhashed = 0, nstays = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x % 32 < n; i += stride) {
+        bool hashed = false;
+        if (i < n) {
+            uint8_t k = 0, nx = 0;
+            if (all || st[i]) {
+                const uint32_t L = lens[i];
+                if (depth > L) {
+                    dp[i] = L;  // end of string before the depth (EOS)
                 } else {
-                    const bool root = i + 1 < n && (all || st[i + 1]) && lcp[i + 1] >= depth;
-                    k = root ? 3 : 2;
-                    nx = root ? 1 : 0;
-                    hashed = true;
+                    dp[i] = depth;
+                    if (i > 0 && (all || st[i - 1]) && lcp[i] >= depth) {
+                        k = 1;
+                        nx = 1;
+                    } else {
+                        const bool root = i + 1 < n && (all || st[i + 1]) && lcp[i + 1] >= depth;
+                        k = root ? 3 : 2;
+                        nx = root ? 1 : 0;
+                        hashed = true;
+                    }
                 }
             }
+            kind[i] = k;
+            st_next[i] = nx;
+            nstays += nx;
+            nhashed += hashed;
         }
-        kind[i] = k;
-        st_next[i] = nx;
-        stays = nx != 0;
+        if (nsets > 1) {  // hashed strings per set size the per-set table regions
+            const int lane = threadIdx.x & 31;
+            const uint32_t sid = hashed ? set_of(set_begin, nsets, i) : 0xFFFFFFFFu - lane;
+            const uint32_t peers = __match_any_sync(FULLM, sid);
+            if (hashed && lane == __ffs(peers) - 1) atomicAdd(&set_cnt[sid], (uint32_t)__popc(peers));
+        }
     }
-    if (nsets > 1) {  // hashed strings per set size the per-set table regions
-        const int lane = threadIdx.x & 31;
-        const uint32_t sid = hashed ? set_of(set_begin, nsets, i) : 0xFFFFFFFFu - lane;
-        const uint32_t peers = __match_any_sync(FULLM, sid);
-        if (hashed && lane == __ffs(peers) - 1) atomicAdd(&set_cnt[sid], (uint32_t)__popc(peers));
-    }
-    block_count(counters + 0, hashed);
-    block_count(counters + 1, stays);
+    block_add(counters + 0, nhashed);
+    block_add(counters + 1, nstays);
 }
 
 // Each string set owns a power-of-two region of the table (base, mask): equal
@@ -149,16 +176,19 @@ __global__ void k_dp_hash(ArenaDev a, const uint64_t* soff, const uint8_t* kind,
     slot[i] = sl == NO_SLOT ? NO_SLOT : (uint32_t)(base + sl);
 }
 
-__global__ void k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup, uint64_t n,
-                           uint8_t* st_next, uint32_t* counters) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool stays = false;
-    if (i < n && kind[i] == 2) {
-        const uint32_t sl = slot[i];
-        stays = sl != NO_SLOT && tdup[sl];
-        st_next[i] = stays ? 1 : 0;
+__global__ void __launch_bounds__(256) k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup,
+                                                  uint64_t n, uint8_t* st_next, uint32_t* counters) {
+    uint32_t nstays = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (kind[i] == 2) {
+            const uint32_t sl = slot[i];
+            const bool stays = sl != NO_SLOT && tdup[sl];
+            st_next[i] = stays ? 1 : 0;
+            nstays += stays;
+        }
     }
-    block_count(counters + 1, stays);
+    block_add(counters + 1, nstays);
 }
 
 __global__ void k_prefix_hash(ArenaDev a, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* out) {
@@ -429,7 +459,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
         if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
         DSSS_LAUNCH("k_dp_classify", st,
-                    k_dp_classify<<<grid, 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
+                    k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
                                                        L.st[cur ^ 1], L.kind, L.counters, L.set_begin, nsets,
                                                        L.set_cnt));
         if (nsets > 1) {
@@ -497,7 +527,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                                        (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
                                                        L.set_mask, L.slot, L.counters + 2));
             DSSS_LAUNCH("k_dp_query", st,
-                        k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
+                        k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
             DSSS_CUDA(cudaGetLastError());
             DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             DSSS_CUDA(cudaStreamSynchronize(st));
@@ -560,7 +590,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
                            k_cand_to_state<<<grid_for(m, 256), 256, 0, st>>>(cand, m, n, L.st[0], L.counters + 3));
     }
     DSSS_LAUNCH("k_dp_classify", st,
-                k_dp_classify<<<grid, 256, 0, st>>>(L.st[0], all, L.lens, lcp, n, depth, dp, L.st[1], L.kind,
+                k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[0], all, L.lens, lcp, n, depth, dp, L.st[1], L.kind,
                                                    L.counters, nullptr, 1, nullptr));
     DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
@@ -572,7 +602,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         DSSS_LAUNCH("k_dp_hash", st,
                     k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
                                                    nullptr, 1, nullptr, nullptr, L.slot, L.counters + 2));
-        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<grid, 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
+        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
     }
     DSSS_LAUNCH("k_state_flags", st, k_state_flags<<<grid, 256, 0, st>>>(L.st[1], n, R.flag));
     DSSS_TRY(exclusive_scan_u32(R.flag, R.pos, n, R.total, R.scan, st));
@@ -634,7 +664,7 @@ int dp_classify_hash(const DpSplitLayout& L, const ArenaDev& a, uint64_t n, cons
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
     DSSS_LAUNCH("k_dp_classify", st,
-                k_dp_classify<<<grid, 256, 0, st>>>(state_in, state_in == nullptr, L.lens, lcp, n, depth, dp, state_out,
+                k_dp_classify<<<stride_grid(n), 256, 0, st>>>(state_in, state_in == nullptr, L.lens, lcp, n, depth, dp, state_out,
                                                    L.kind, L.counters, nullptr, 1, nullptr));
     DSSS_LAUNCH("k_hash_flags", st, k_hash_flags<<<grid, 256, 0, st>>>(L.kind, n, L.flag));
     DSSS_TRY(exclusive_scan_u32(L.flag, L.pos, n, L.counters + 4, L.scan, st));

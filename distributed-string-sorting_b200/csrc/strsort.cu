@@ -173,6 +173,8 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
         uint32_t len;
         str_of(S.a, ord[i], off, len);
         uint32_t d = d0, l;
+        // no need to compare past this thread's minimum so far
+        const uint32_t lim = min(cap, mn);
         for (;;) {
             // 16 bytes per step: two independent 8-byte compares
             uint64_t x[2], y[2];
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
             }
             if (done) break;
             d += 16;
-            if (d >= cap) {
+            if (d >= lim) {
                 l = d;
                 break;
             }
