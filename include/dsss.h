@@ -110,7 +110,9 @@ int dsss_abi_version(void);
  *   dp_filter_bits  filter bits per hashed string (default 16)
  *   sort_small_max  small-segment cutoff of the string sort when dsss_opts
  *                   gives 0 (2..4096, default 4096)
- *   sort_pivot      pivot passes of the string sort on/off (default 1) */
+ *   sort_pivot      pivot passes of the string sort on/off (default 1)
+ *   dp_table        hash-table slots per hashed string in a distinguishing-
+ *                   prefix round, rounded up to a power of two (2..8, default 2) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 
