@@ -162,7 +162,7 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
     }
 
 
-def bench_serving(d, torch, p=8, n_req=48, rate=250.0, seed=2024, workers=4, max_batch=4_000_000,
+def bench_serving(d, torch, p=8, n_req=48, rate=250.0, seed=2024, workers=6, max_batch=2_000_000,
                   reserve=24 << 30):
     """Sort requests through dsss_server: n log-uniform in [1e3, 4e6], lengths
     Zipf(1.2) on [8, 256], bytes 0x21-0x7E after a shared random prefix; host

@@ -131,6 +131,7 @@ enum TuneKnob : int {
     TUNE_SORT_SMALL_MAX,     // small-segment cutoff when the options give 0
     TUNE_SORT_PIVOT,         // pivot passes on (1) or off (0)
     TUNE_DP_TABLE,           // DP hash-table slots per hashed string (rounded up to a power of two)
+    TUNE_SORT_GRAPH,         // largest n sorted by the device-driven graph (0: never)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

@@ -153,6 +153,10 @@ __global__ void k_tile_counts(const Seg* segs, uint32_t nseg, uint32_t* tiles, u
 
 // ---------------------------------------------------------------- prefix ----
 __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -216,6 +220,10 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
 
 // ------------------------------------------------------------- keys/diff ----
 __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -325,6 +333,10 @@ __device__ __forceinline__ uint64_t pivot_key(const uint8_t* chars, uint64_t off
 }
 
 __global__ void __launch_bounds__(LT_NT) k_pivot(SortState S, Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -357,6 +369,10 @@ __global__ void __launch_bounds__(LT_NT) k_pivot(SortState S, Seg* segs, uint32_
 __device__ __forceinline__ uint32_t digit_of(uint64_t k, uint32_t shift) { return (uint32_t)(k >> shift) & 0xFFu; }
 
 __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     __shared__ uint32_t hist[256];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
@@ -382,6 +398,10 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
 
 // ------------------------------------------------------------ chunk sums ----
 __global__ void k_chunk_sum(SortState S, const Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     const uint32_t c = blockIdx.x;
     if (c >= S.counters[9]) return;
     const uint32_t si = find_seg(S.chunk0, nseg, c);
@@ -399,7 +419,14 @@ __global__ void k_chunk_sum(SortState S, const Seg* segs, uint32_t nseg) {
 __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32_t nseg, Seg* next) {
     __shared__ uint32_t sh[32];
     __shared__ uint32_t s_first;
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        const uint32_t c = S.counters[12];
+        segs = S.large[c];
+        next = S.large[c ^ 1u];
+        nseg = S.counters[13];
+    }
     const uint32_t si = blockIdx.x;
+    if (si >= nseg) return;
     Seg& sg = segs[si];
     const uint32_t par = sg.flags & F_PARITY;
     const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
@@ -521,6 +548,10 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
 constexpr size_t SCATTER_SMEM = (size_t)LT_TILE * (8 + 4 + 1);
 
 __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     extern __shared__ __align__(16) unsigned char sm_scatter[];
     unsigned long long* skey = (unsigned long long*)sm_scatter;
     uint32_t* sord = (uint32_t*)(skey + LT_TILE);
@@ -750,9 +781,10 @@ __device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint
 }
 
 // Segments of 2..32 strings: one warp each, four per CTA.
-__global__ void __launch_bounds__(128) k_warp_segs(SortState S, const Seg* segs, uint32_t nseg) {
-    const uint32_t si = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (si >= nseg) return;
+// dcount (graph mode): the segment count on the device; blocks stride over it.
+__global__ void __launch_bounds__(128) k_warp_segs(SortState S, const Seg* segs, uint32_t nseg, const uint32_t* dcount) {
+    if (dcount) nseg = *dcount;
+    for (uint32_t si = blockIdx.x * 4 + (threadIdx.x >> 5); si < nseg; si += gridDim.x * 4) {
     const int lane = threadIdx.x & 31;
     const Seg seg = segs[si];
     const uint32_t* src = S.ord[seg.flags & F_PARITY];
@@ -765,6 +797,7 @@ __global__ void __launch_bounds__(128) k_warp_segs(SortState S, const Seg* segs,
     }
     warp_sort(S.a, seg.size, seg.depth, key, id, S.lcp_out + seg.start);
     if ((uint32_t)lane < seg.size) S.ord_out[seg.start + lane] = id;
+    }
 }
 
 template <int CAP>
@@ -779,7 +812,7 @@ constexpr size_t seg_sort_smem() {
 constexpr uint32_t SF_REKEY = 1u, SF_PIVOT = 2u, SF_PSEUDO = 4u;
 
 template <int CAP, int NT>
-__global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg) {
+__global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg, const uint32_t* dcount) {
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* sk = (unsigned long long*)smem;
@@ -793,8 +826,8 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     __shared__ uint32_t wcnt[NW][256];
     __shared__ uint32_t s_top, s_nw, s_cur[3];
     __shared__ unsigned long long s_diff;
-    const uint32_t bi = blockIdx.x;
-    if (bi >= nseg) return;
+    if (dcount) nseg = *dcount;
+    for (uint32_t bi = blockIdx.x; bi < nseg; bi += gridDim.x) {
     const Seg seg = segs[bi];
     const uint32_t start = seg.start, size = seg.size;
     const uint32_t* src = S.ord[seg.flags & F_PARITY];
@@ -1051,6 +1084,8 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < size; i += NT) S.ord_out[start + i] = so[i];
+    __syncthreads();  // shared memory is reused by the next segment
+    }
 }
 
 template <int CAP, int NT>
@@ -1059,12 +1094,180 @@ static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, cons
     constexpr size_t shm = seg_sort_smem<CAP>();
     static std::atomic<uint64_t> configured{0};
     DSSS_TRY(set_smem_once(configured, k_seg_sort<CAP, NT>, (int)shm));
-    DSSS_LAUNCH(name, st, k_seg_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n));
+    DSSS_LAUNCH(name, st, k_seg_sort<CAP, NT><<<n, NT, shm, st>>>(S, segs, n, nullptr));
     DSSS_CUDA(cudaGetLastError());
     return DSSS_OK;
 }
 
+
+// ------------------------------------------------------- graph mode ----
+// For n up to sort_graph_max_n (off by default) the MSD passes run as one CUDA graph: the pass
+// is the body of a conditional WHILE node, the number of large segments and
+// the parity of their list live on the device (counters[13], [12]), grids are
+// the layout's capacities (blocks past the real tiles exit), and a one-thread
+// kernel at the end of each pass sets the loop condition — no host round trip
+// per pass.  The small-segment sorters then stride over the device counts.
+
+// One block: per large segment its first tile and chunk (exclusive prefix
+// over the list), totals into counters[8], [9]; resets the next-list count.
+__global__ void __launch_bounds__(1024) k_seg_offsets(SortState S) {
+    __shared__ uint32_t st_[1024], sc_[1024];
+    const Seg* segs = S.large[S.counters[12]];
+    const uint32_t nseg = S.counters[13];
+    const uint32_t per = (nseg + 1023) / 1024;
+    const uint32_t b = min(nseg, threadIdx.x * per), e = min(nseg, b + per);
+    uint32_t tt = 0, tc = 0;
+    for (uint32_t i = b; i < e; ++i) {
+        const uint32_t t = (segs[i].size + LT_TILE - 1) / LT_TILE;
+        tt += t;
+        tc += (t + CHUNK_TILES - 1) / CHUNK_TILES;
+    }
+    st_[threadIdx.x] = tt;
+    sc_[threadIdx.x] = tc;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const uint32_t vt = threadIdx.x >= (unsigned)off ? st_[threadIdx.x - off] : 0;
+        const uint32_t vc = threadIdx.x >= (unsigned)off ? sc_[threadIdx.x - off] : 0;
+        __syncthreads();
+        st_[threadIdx.x] += vt;
+        sc_[threadIdx.x] += vc;
+        __syncthreads();
+    }
+    uint32_t rt = st_[threadIdx.x] - tt, rc = sc_[threadIdx.x] - tc;
+    for (uint32_t i = b; i < e; ++i) {
+        const uint32_t t = (segs[i].size + LT_TILE - 1) / LT_TILE;
+        S.tile0[i] = rt;
+        S.chunk0[i] = rc;
+        rt += t;
+        rc += (t + CHUNK_TILES - 1) / CHUNK_TILES;
+    }
+    if (threadIdx.x == 1023) {
+        S.counters[8] = st_[1023];
+        S.counters[9] = sc_[1023];
+        if (st_[1023] > S.cap_tiles || sc_[1023] > S.cap_chunks) {
+            S.counters[8] = 0;  // nothing runs; the guard stops the loop
+            S.counters[9] = 0;
+            S.counters[10] = 1;
+        }
+        S.counters[0] = 0;  // large segments of the next pass
+    }
+}
+
+__global__ void k_loop_init(SortState S, cudaGraphConditionalHandle h) {
+    S.counters[12] = 0;
+    S.counters[13] = S.counters[0];
+    S.counters[14] = 0;
+    cudaGraphSetConditional(h, S.counters[13] > 0 ? 1u : 0u);
+}
+
+// Ends a pass: the next list becomes current; loop while it is not empty,
+// no guard tripped and the pass count stays sane.
+__global__ void k_pass_end(SortState S, cudaGraphConditionalHandle h) {
+    uint32_t next = S.counters[0];
+    if (next > S.cap_large) {
+        S.counters[10] = 1;
+        next = 0;
+    }
+    S.counters[12] ^= 1u;
+    S.counters[13] = next;
+    const uint32_t passes = ++S.counters[14];
+    if (passes > (1u << 20)) S.counters[10] = 1;
+    cudaGraphSetConditional(h, (next > 0 && S.counters[10] == 0) ? 1u : 0u);
+}
+
+// Two streams per host thread and device to capture on (the caller's stream
+// may be the legacy default stream, which cannot be captured); the graph is
+// then launched on the caller's stream.
+static int capture_streams(cudaStream_t* cap, cudaStream_t* body) {
+    constexpr int MAXDEV = 64;
+    thread_local cudaStream_t tl[MAXDEV][2] = {};
+    int dev = 0;
+    DSSS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAXDEV) return fail(DSSS_ENOTSUP, "device %d out of range", dev);
+    for (int k = 0; k < 2; ++k)
+        if (!tl[dev][k]) DSSS_CUDA(cudaStreamCreateWithFlags(&tl[dev][k], cudaStreamNonBlocking));
+    *cap = tl[dev][0];
+    *body = tl[dev][1];
+    return DSSS_OK;
+}
+
+static int sort_strings_graph(const SortLayout& L, SortState S, uint64_t n, uint32_t p, const uint32_t* ids_in,
+                              uint32_t* pin, cudaStream_t run_st) {
+    cudaStream_t st = nullptr, bst = nullptr;
+    DSSS_TRY(capture_streams(&st, &bst));
+    struct Res {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t x = nullptr;
+        ~Res() {
+            if (x) cudaGraphExecDestroy(x);
+            if (g) cudaGraphDestroy(g);
+        }
+    } res;
+    const unsigned tiles = (unsigned)L.cap_tiles, chunks = (unsigned)L.cap_chunks, large = (unsigned)L.cap_large;
+    DSSS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st);
+    k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n);
+    k_init_segs<<<grid_for(p, 128), 128, 0, st>>>(S, L.pb, p);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphConditionalHandle h{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+    if (e == cudaSuccess) k_loop_init<<<1, 1, 0, st>>>(S, h);
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t cond = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cond, g, deps, ndeps, &np);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &cond, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        // the loop body: one MSD pass, captured on a second stream into the body graph
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(bst, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            k_seg_offsets<<<1, 1024, 0, bst>>>(S);
+            k_prefix<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            k_pivot<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            k_keys_diff<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            k_hist<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            k_chunk_sum<<<chunks, 256, 0, bst>>>(S, nullptr, 0);
+            k_seg_scan<<<large, 256, 0, bst>>>(S, nullptr, 0, nullptr);
+            k_scatter<<<tiles, LT_NT, SCATTER_SMEM, bst>>>(S, nullptr, 0);
+            k_pass_end<<<1, 1, 0, bst>>>(S, h);
+            cudaGraph_t got = nullptr;
+            e = cudaStreamEndCapture(bst, &got);
+        }
+    }
+    if (e == cudaSuccess) {
+        // small segments, striding over the device counts
+        k_warp_segs<<<148 * 8, 128, 0, st>>>(S, S.small[0], 0, S.counters + 1);
+        k_seg_sort<256, 128><<<148 * 8, 128, seg_sort_smem<256>(), st>>>(S, S.small[1], 0, S.counters + 2);
+        k_seg_sort<1024, 256><<<148 * 4, 256, seg_sort_smem<1024>(), st>>>(S, S.small[2], 0, S.counters + 3);
+        k_seg_sort<4096, 256><<<148, 256, seg_sort_smem<4096>(), st>>>(S, S.small[3], 0, S.counters + 4);
+        cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    }
+    cudaGraph_t whole = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &whole);
+    res.g = whole;
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return fail(DSSS_EDEVICE, "string sort graph: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    DSSS_CUDA(cudaGraphInstantiate(&res.x, whole, 0));
+    {
+        StageTimer t("graph:sort", run_st);
+        DSSS_CUDA(cudaGraphLaunch(res.x, run_st));
+    }
+    DSSS_CUDA(cudaStreamSynchronize(run_st));
+    if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
+    return DSSS_OK;
+}
+
 // ------------------------------------------------------------------ host ----
+static Seg* large_list(const SortLayout& L, int k) { return (Seg*)L.large[k]; }
 static uint32_t clamp_small_max(uint32_t m) {
     if (m == 0) m = (uint32_t)tune(TUNE_SORT_SMALL_MAX);
     return (m == 0 || m > (uint32_t)bin_cap(NBINS - 1)) ? (uint32_t)bin_cap(NBINS - 1) : (m < 2 ? 2 : m);
@@ -1127,6 +1330,15 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     static std::atomic<uint64_t> scatter_configured{0};
     DSSS_TRY(set_smem_once(scatter_configured, k_scatter, (int)SCATTER_SMEM));
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb_host, (p + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (n <= (uint64_t)tune(TUNE_SORT_GRAPH)) {
+        static std::atomic<uint64_t> c256{0}, c1024{0}, c4096{0};
+        DSSS_TRY(set_smem_once(c256, k_seg_sort<256, 128>, (int)seg_sort_smem<256>()));
+        DSSS_TRY(set_smem_once(c1024, k_seg_sort<1024, 256>, (int)seg_sort_smem<1024>()));
+        DSSS_TRY(set_smem_once(c4096, k_seg_sort<4096, 256>, (int)seg_sort_smem<4096>()));
+        S.large[0] = large_list(L, 0);
+        S.large[1] = large_list(L, 1);
+        return sort_strings_graph(L, S, n, p, ids_in, pin, st);
+    }
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     DSSS_LAUNCH("k_init_ids", st, k_init_ids<<<grid_for(n, 256), 256, 0, st>>>(S.ord[0], ids_in, n));
     S.large[0] = large[0];
@@ -1169,7 +1381,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     for (int b = 0; b < NBINS; ++b)
         if (pin[1 + b] > L.cap_small) return fail(DSSS_EDEVICE, "string sort: small-segment list overflow");
     if (pin[1]) {
-        DSSS_LAUNCH("k_warp_segs", st, k_warp_segs<<<(pin[1] + 3) / 4, 128, 0, st>>>(S, S.small[0], pin[1]));
+        DSSS_LAUNCH("k_warp_segs", st, k_warp_segs<<<(pin[1] + 3) / 4, 128, 0, st>>>(S, S.small[0], pin[1], nullptr));
         DSSS_CUDA(cudaGetLastError());
     }
     DSSS_TRY((launch_seg_sort<256, 128>(S, S.small[1], pin[2], "k_seg_sort256", st)));

@@ -112,7 +112,12 @@ int dsss_abi_version(void);
  *                   gives 0 (2..4096, default 4096)
  *   sort_pivot      pivot passes of the string sort on/off (default 1)
  *   dp_table        hash-table slots per hashed string in a distinguishing-
- *                   prefix round, rounded up to a power of two (2..8, default 2) */
+ *                   prefix round, rounded up to a power of two (2..8, default 2)
+ *   sort_graph_max_n  largest n whose string sort runs as one CUDA graph with
+ *                   a device-side pass loop (default 0 = never: measured on
+ *                   B200 no faster than the host-driven loop, whose per-pass
+ *                   read-back costs less than the graph's capacity-sized grids
+ *                   and per-call instantiation) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 

@@ -47,7 +47,8 @@ def test_filter_batched(dsss, ctx):
         assert np.array_equal(u64(out["perm_index"], hs.n)[b:e], u64(ref["perm_index"], h.n)), s
 
 
-@pytest.mark.parametrize("knobs", [dict(sort_pivot=0), dict(sort_small_max=64), dict(sort_small_max=2, sort_pivot=0)])
+@pytest.mark.parametrize("knobs", [dict(sort_pivot=0), dict(sort_small_max=64), dict(sort_small_max=2, sort_pivot=0),
+                                   dict(sort_graph_max_n=0), dict(sort_graph_max_n=0, sort_small_max=64)])
 def test_sort_knobs(dsss, orc, ctx, knobs):
     hs = dsss.gen_suffix_strings(50000, 256, seed=6)
     n = hs.n
@@ -71,3 +72,18 @@ def test_autotune_picks_a_grid_setting(dsss, orc, ctx):
         assert dsss.tune_get("sort_small_max") == t["sort_small_max"]
         out = dsss.pd_sort(ctx, ds, 4)
         check_pd(dsss, orc, hs, out, 4)
+
+
+@pytest.mark.parametrize("graph", [0, 1 << 22])
+@pytest.mark.parametrize("name,strs", CASES, ids=IDS)
+def test_sort_host_loop_and_graph(dsss, orc, ctx, name, strs, graph):
+    """The MSD passes driven from the host (one read-back per pass) and as one
+    CUDA graph with a device-side loop condition give the same order and LCPs."""
+    hs = host_of(dsss, strs)
+    n = hs.n
+    with dsss.tuned(sort_graph_max_n=graph, sort_small_max=32):
+        order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), 3 if n >= 3 else 1)
+    pb = dsss.equal_parts(n, 3 if n >= 3 else 1)
+    ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
+    assert np.array_equal(u64(order, n), ro)
+    assert np.array_equal(u64(lcp, n), rl)
