@@ -1110,10 +1110,12 @@ static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, cons
 
 // One block: per large segment its first tile and chunk (exclusive prefix
 // over the list), totals into counters[8], [9]; resets the next-list count.
-__global__ void __launch_bounds__(1024) k_seg_offsets(SortState S) {
+__global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, const Seg* segs, uint32_t nseg) {
     __shared__ uint32_t st_[1024], sc_[1024];
-    const Seg* segs = S.large[S.counters[12]];
-    const uint32_t nseg = S.counters[13];
+    if (!segs) {
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
     const uint32_t per = (nseg + 1023) / 1024;
     const uint32_t b = min(nseg, threadIdx.x * per), e = min(nseg, b + per);
     uint32_t tt = 0, tc = 0;
@@ -1230,7 +1232,7 @@ static int sort_strings_graph(const SortLayout& L, SortState S, uint64_t n, uint
         cudaGraph_t body = np.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(bst, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            k_seg_offsets<<<1, 1024, 0, bst>>>(S);
+            k_seg_offsets<<<1, 1024, 0, bst>>>(S, nullptr, 0);
             k_prefix<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_pivot<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_keys_diff<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
@@ -1355,10 +1357,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         Seg* segs = large[cur];
         Seg* next = large[cur ^ 1];
         // tile / chunk indexing
-        DSSS_LAUNCH("k_tile_counts", st, k_tile_counts<<<grid_for(nlarge, 256), 256, 0, st>>>(segs, nlarge, S.tmp_counts, S.tmp_counts + L.cap_large));
-        DSSS_TRY(exclusive_scan_u32(S.tmp_counts, S.tile0, nlarge, S.counters + 8, L.scan, st));
-        DSSS_TRY(exclusive_scan_u32(S.tmp_counts + L.cap_large, S.chunk0, nlarge, S.counters + 9, L.scan, st));
-        DSSS_CUDA(cudaMemsetAsync(S.counters, 0, sizeof(uint32_t), st));  // n_large_next
+        // tile / chunk indexing (and the next list's count reset): one block
+        DSSS_LAUNCH("k_seg_offsets", st, k_seg_offsets<<<1, 1024, 0, st>>>(S, segs, nlarge));
         // upper bounds for the grids (kernels exit past the real counts)
         uint64_t max_tiles = std::min<uint64_t>(L.cap_tiles, n / LT_TILE + nlarge + 1);
         uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
