@@ -256,6 +256,8 @@ def run_dist(args, cfg):
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         res = D.sort(comm, be, ds, pb)
+    phases = {}
+    D.sort(comm, be, ds, pb, phases=phases)  # one call with per-phase wall-clock times
     tdist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -279,6 +281,7 @@ def run_dist(args, cfg):
                        "len": L, "p_per_gpu": p, "parallelism": f"{world} ranks, NCCL exchanges (dist.py)",
                        "l2": "inputs > L2, no flush"},
             "mode": "dist", "dp_rounds": res.get("dp_rounds"), "clocks": clk.summary(),
+            "phases_ms": {k: round(v, 3) for k, v in phases.items()},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -67,8 +67,9 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"sort_pivot", 1, 0, 1},
     {"dp_table", 2, 2, 8},
     {"sort_graph_max_n", 0, 0, 1ll << 32},
+    {"merge_by_sort", 1, 0, 1},
 };
-static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}};
+static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}};
 
 int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
 

@@ -132,6 +132,7 @@ enum TuneKnob : int {
     TUNE_SORT_PIVOT,         // pivot passes on (1) or off (0)
     TUNE_DP_TABLE,           // DP hash-table slots per hashed string (rounded up to a power of two)
     TUNE_SORT_GRAPH,         // largest n sorted by the device-driven graph (0: never)
+    TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1) or by merge rounds (0)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

@@ -20,6 +20,7 @@
 
 #include "internal.cuh"
 #include "merge.cuh"
+#include "strsort.cuh"
 
 namespace dsss {
 
@@ -384,9 +385,13 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
                                          "or the NUL layout holds more strings than n");
     if (!char_start && pin[1] != n) return fail(DSSS_EINVAL, "merge: the NUL layout holds %u strings, not n", pin[1]);
     const uint64_t full_bytes = *(const uint64_t*)(pin + 4);
-    // reserve the decompressed arena behind the layout
+    // reserve the decompressed arena behind the layout (and the string sort's
+    // scratch behind it when the runs are merged by sorting)
+    const bool by_sort = tune(TUNE_MERGE_SORT) != 0;
+    SortLayout SL;
     Carve sz2(nullptr);
     layout_merge(sz2, L, n, bytes, full_bytes, nruns);
+    if (by_sort) layout_sort(sz2, SL, n, nrecv, 0);
     if (sz2.used > ctx->ws_cap) {
         // grow: everything computed so far lives in the scratch, so recompute
         // after growing (simplest correct path; the next call reuses the size)
@@ -396,9 +401,29 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
     }
     Carve c1(ctx->ws);
     layout_merge(c1, L, n, bytes, full_bytes, nruns);
+    if (by_sort) layout_sort(c1, SL, n, nrecv, 0);
     DSSS_LAUNCH("k_extend", st,
                 k_extend<<<grid_for(n, 256), 256, 0, st>>>(chars, start, L.l[0], tree, n, L.foff, L.flen, L.full,
                                                           L.counters + 2));
+    if (by_sort) {
+        // Merging sorted runs by sorting their union: each receiving PE's
+        // strings are one segment of the string sort, with ids in run order so
+        // that byte-identical strings keep run order (lower source PE first),
+        // exactly as the merge rounds below leave them.
+        std::vector<uint64_t> rbnd(nrecv + 1, n);
+        for (uint32_t r = 0; r < nrecv; ++r) rbnd[r] = rb[(uint64_t)r * p];
+        ArenaDev fa{L.full, L.foff, L.flen, n};
+        uint32_t* mlcp = merged_lcp ? merged_lcp : L.l[1];
+        DSSS_TRY(sort_strings(SL, fa, n, nrecv, rbnd.data(), nullptr, order, mlcp, 0, (uint32_t*)ctx->pin, st));
+        DSSS_LAUNCH("k_merge_tags", st,
+                    k_merge_tags<<<grid_for(n, 256), 256, 0, st>>>(order, lcp, L.run_start, L.run_of, L.run_begin,
+                                                                  L.run_offset, p, n, old_lcp, perm_index, perm_pe));
+        pin = (uint32_t*)ctx->pin;
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        if (pin[2]) return fail(DSSS_EINVAL, "merge: a source run does not start with LCP 0");
+        return DSSS_OK;
+    }
     FullView f{L.full, L.foff, L.flen};
     // merge rounds: within each receiving PE, runs (2j, 2j+1) merge into one
     struct Run { uint32_t beg, len; };

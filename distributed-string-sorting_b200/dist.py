@@ -197,8 +197,12 @@ class GpuBackend:
         return int(c.value)
 
     def take(self, t, idx):
-        h = t.cpu().numpy()
-        return h[np.asarray(idx, np.int64)].astype(np.int64)
+        """Host copy of t at the (few) host positions idx."""
+        torch = self.torch
+        sel = t[torch.from_numpy(np.asarray(idx, np.int64)).to(t.device)].cpu().numpy()
+        if sel.dtype == np.int32:
+            sel = sel.view(np.uint32)
+        return sel.astype(np.int64)
 
     def pack(self, ds, ids, trunc=None):
         """Strings ids (host) truncated to trunc (host) -> (device chars, host offsets, host lengths, bytes)."""
@@ -308,9 +312,33 @@ def depths():
         i *= 2
 
 
-def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2):
+class _Phases:
+    """Wall-clock time per phase (after a device synchronisation), when asked."""
+
+    def __init__(self, out):
+        import time
+        self.out, self.time = out, time
+        self.t = time.perf_counter() if out is not None else 0.0
+
+    def mark(self, name):
+        if self.out is None:
+            return
+        try:
+            import torch
+            if torch.cuda.is_available():
+                torch.cuda.synchronize()
+        except ImportError:
+            pass
+        t = self.time.perf_counter()
+        self.out[name] = self.out.get(name, 0.0) + (t - self.t) * 1e3
+        self.t = t
+
+
+def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None):
     """This rank's part of DistributedPrefixDoublingSort::sort.  strings: the
-    backend's arena of this rank's strings; part_begin: p_local + 1 PE bounds."""
+    backend's arena of this rank's strings; part_begin: p_local + 1 PE bounds.
+    phases (dict, optional) receives milliseconds per phase."""
+    ph = _Phases(phases)
     indexed = sampler == 2
     pb = np.asarray(part_begin, np.int64)
     p_local = len(pb) - 1
@@ -325,8 +353,10 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2)
     res = dict(part_begin=pb, p_global=p, q_first=q_first)
 
     # local sort (prefix_doubling.hpp:228)
+    ph.mark("setup")
     order, lcp = be.local_sort(strings, pb)
     res["local_order"] = order
+    ph.mark("local_sort")
     if p == 1:  # prefix_doubling.hpp:236
         res["recv_counts"] = np.zeros(p_local, np.int64)
         return res
@@ -349,6 +379,7 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2)
             break
     res["dp"] = dp
     res["dp_rounds"] = rounds
+    ph.mark("dp")
 
     # 2. splitters (misc.hpp:531-587)
     pos = sample_positions(sizes_local, p, factor)
@@ -384,9 +415,11 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2)
                                    indexed)
     iv_all = np.concatenate(comm.allgather_np(np.asarray(iv_local).ravel())).reshape(p, p)
     res["intervals"] = np.asarray(iv_local, np.int64)
+    ph.mark("partition")
 
     # 3. string exchange (alltoall.hpp:910-1008) and merge (merging.hpp:66-123)
     snd = be.bucket_send(strings, pb, order, lcp, dp, p, q_first, iv_local)
+    ph.mark("bucket_send")
     per_r = snd["counts"].sum(axis=1)                    # strings per receiver from this rank
     rbeg = np.concatenate([[0], np.cumsum(per_r)])
     cbeg = snd["char_begin"]
@@ -403,6 +436,7 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2)
     rchars = comm.alltoallv(snd["chars"], s_byte, r_byte)
     rstart = comm.alltoallv(snd["char_start"], s_str, r_str)
     rlcp = comm.alltoallv(snd["lcp"], s_str, r_str)
+    ph.mark("exchange")
     # regroup [sender rank][receiver] -> [receiver][sender rank]
     src_str = np.concatenate([[0], np.cumsum(r_str)])
     src_byte = np.concatenate([[0], np.cumsum(r_byte)])
@@ -424,7 +458,9 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2)
     res["recv_total"] = nrecv
     if nrecv:
         mchars, mstart, mlcp = be.regroup(blocks, rchars, rstart, rlcp, nrecv, dbyte)
+        ph.mark("regroup")
         res.update(be.merge(mchars, dbyte, mstart, mlcp, counts, offsets))
+        ph.mark("merge")
     else:
         res.update(perm_index=np.zeros(0, np.int64), perm_pe=np.zeros(0, np.int64), merged_lcp=np.zeros(0, np.int64))
     return res

@@ -117,7 +117,10 @@ int dsss_abi_version(void);
  *                   a device-side pass loop (default 0 = never: measured on
  *                   B200 no faster than the host-driven loop, whose per-pass
  *                   read-back costs less than the graph's capacity-sized grids
- *                   and per-call instantiation) */
+ *                   and per-call instantiation)
+ *   merge_by_sort   dsss_lcp_merge: decompressed runs merged by one segmented
+ *                   string sort (1, default) or by pairwise merge-path rounds
+ *                   (0); identical results, ties in run order either way */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 

@@ -115,10 +115,17 @@ def string_runs_equal(strs_got, strs_ref, labels_got, labels_ref):
         k = e
 
 
-def test_lcp_merge_golden(dsss, ctx):
-    """merge_ref.json: the reference's LcpStringLoserTree_ on receive containers."""
+@pytest.mark.parametrize("by_sort", [1, 0])
+def test_lcp_merge_golden(dsss, ctx, by_sort):
+    """merge_ref.json: the reference's LcpStringLoserTree_ on receive containers
+    (runs merged by one segmented sort, or by merge-path rounds)."""
     with open(os.path.join(GOLDEN, "merge_ref.json")) as f:
         gold = json.load(f)
+    with dsss.tuned(merge_by_sort=by_sort):
+        _merge_golden(dsss, ctx, gold)
+
+
+def _merge_golden(dsss, ctx, gold):
     for name, v in gold.items():
         for pe in v["pes"]:
             raw = bytes.fromhex(pe["chars"])
@@ -155,8 +162,9 @@ def test_lcp_merge_golden(dsss, ctx):
             assert u64(out["merged_lcp"]).tolist() == pe["merged_lcp"], name
 
 
+@pytest.mark.parametrize("by_sort", [1, 0])
 @pytest.mark.parametrize("p", [2, 3, 4, 8, 16])
-def test_staged_pipeline_matches_oracle(dsss, orc, ctx, p):
+def test_staged_pipeline_matches_oracle(dsss, orc, ctx, p, by_sort):
     """The reference's stage order on the GPU: local sort, DP rounds, partition,
     bucket scatter, LCP merge of every PE's container."""
     strs = with_duplicates(random_strings(6000, 0, 40, b"ABC", 200 + p), 0.15, 201)
@@ -168,8 +176,9 @@ def test_staged_pipeline_matches_oracle(dsss, orc, ctx, p):
     dp, _ = dsss.dp_prefixes(ctx, ds, order, lcp, p)
     iv = dsss.partition(ctx, ds, order, dp, p)
     g = dsss.bucket_scatter(ctx, ds, p, order, lcp, dp, iv)
-    out = dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
-                         char_start=g["char_start"])
+    with dsss.tuned(merge_by_sort=by_sort):
+        out = dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
+                             char_start=g["char_start"])
     r = orc.pd_sort(orc.Strings.from_host(hs), pb)
     assert np.array_equal(iv, r["intervals"])
     local = u64(order)
@@ -185,3 +194,22 @@ def test_staged_pipeline_matches_oracle(dsss, orc, ctx, p):
                       list(zip(r["perm_pe"].tolist(), r["perm_index"].tolist())))
     # merged LCP restarts at 0 for every receiving PE
     assert np.array_equal(u64(out["merged_lcp"]), r["merged_lcp"])
+
+
+def test_lcp_merge_modes_identical(dsss, ctx):
+    """Sort-based and merge-path merging give the same order, LCPs and labels
+    (ties in run order) on containers with many byte-identical strings."""
+    hs = dsss.gen_suffix_strings(200000, 256, seed=12)
+    ds = dsss.DeviceStrings(hs)
+    p = 8
+    order, lcp = dsss.local_sort_lcp(ctx, ds, p)
+    dp, _ = dsss.dp_prefixes(ctx, ds, order, lcp, p)
+    iv = dsss.partition(ctx, ds, order, dp, p)
+    g = dsss.bucket_scatter(ctx, ds, p, order, lcp, dp, iv)
+    outs = []
+    for m in (1, 0):
+        with dsss.tuned(merge_by_sort=m):
+            outs.append(dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
+                                       char_start=g["char_start"]))
+    for k in ("order", "merged_lcp", "old_lcp", "perm_index", "perm_pe"):
+        assert np.array_equal(u64(outs[0][k]), u64(outs[1][k])), k
