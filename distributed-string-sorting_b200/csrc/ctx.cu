@@ -68,8 +68,9 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"dp_table", 2, 2, 8},
     {"sort_graph_max_n", 0, 0, 1ll << 32},
     {"merge_by_sort", 1, 0, 1},
+    {"merge_extend_lanes", 0, 0, 32},
 };
-static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}};
+static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}};
 
 int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
 
@@ -388,6 +389,8 @@ int dsss_tune_set(const char* name, int64_t value) {
     if (value < g_knob_defs[k].lo || value > g_knob_defs[k].hi)
         return fail(DSSS_EINVAL, "knob %s takes %lld..%lld", name, (long long)g_knob_defs[k].lo,
                     (long long)g_knob_defs[k].hi);
+    if (k == TUNE_MERGE_LANES && value && (value < 4 || (value & (value - 1))))
+        return fail(DSSS_EINVAL, "knob %s takes 0, 4, 8, 16 or 32", name);
     g_knobs[k].store(value, std::memory_order_relaxed);
     return DSSS_OK;
 }

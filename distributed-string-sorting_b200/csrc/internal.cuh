@@ -133,6 +133,7 @@ enum TuneKnob : int {
     TUNE_DP_TABLE,           // DP hash-table slots per hashed string (rounded up to a power of two)
     TUNE_SORT_GRAPH,         // largest n sorted by the device-driven graph (0: never)
     TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1) or by merge rounds (0)
+    TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

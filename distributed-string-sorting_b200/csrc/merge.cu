@@ -88,36 +88,165 @@ __device__ uint32_t prev_smaller(const MinTree& t, uint64_t o, uint32_t v) {
     return NONE32;
 }
 
+// G lanes decompress one string together (G = 1: one thread per string), so
+// that a warp's byte loads and stores fall on 32 / G strings' consecutive
+// bytes instead of 32 scattered ones; strings 0, step, 2 step, ...
+template <int G>
 __global__ void k_extend(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, MinTree tree, uint64_t n,
-                         const uint64_t* foff, const uint32_t* flen, uint8_t* full, uint32_t* err) {
-    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                         uint64_t step, const uint64_t* foff, const uint32_t* flen, uint8_t* full, uint32_t* err) {
+    const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G * step;
+    const uint32_t lane = threadIdx.x % G;
     if (o >= n) return;
     uint8_t* dst = full + foff[o];
     const uint32_t l0 = lcp[o];
-    if (flen[o] < l0) {
-        atomicExch(err, 1u);
+    const uint32_t fo = flen[o];
+    if (fo < l0) {
+        if (lane == 0) atomicExch(err, 1u);
         return;
     }
-    const uint32_t own = flen[o] - l0;
+    const uint32_t own = fo - l0;
     const uint8_t* src = chars + start[o];
-    for (uint32_t k = 0; k < own; ++k) dst[l0 + k] = src[k];
+#pragma unroll 4
+    for (uint32_t k = lane; k < own; k += G) dst[l0 + k] = src[k];
     uint32_t need = l0;
     uint64_t cur = o;
     while (need > 0) {
         const uint32_t j = prev_smaller(tree, cur, need);
         if (j == NONE32) {  // a run must start with LCP 0
-            atomicExch(err, 1u);
+            if (lane == 0) atomicExch(err, 1u);
             return;
         }
         const uint32_t lj = lcp[j];
         if (need - lj > flen[j] - lj) {  // the LCP claims more bytes than string j holds
-            atomicExch(err, 1u);
+            if (lane == 0) atomicExch(err, 1u);
             return;
         }
         const uint8_t* sj = chars + start[j];
-        for (uint32_t x = lj; x < need; ++x) dst[x] = sj[x - lj];
+#pragma unroll 4
+        for (uint32_t x = lj + lane; x < need; x += G) dst[x] = sj[x - lj];
         need = lj;
         cur = j;
+    }
+}
+
+// A group of G lanes decompresses a chunk of XT_CHUNK consecutive strings in
+// order.  The chunk's first string is decompressed beforehand (k_extend over
+// every XT_CHUNK-th string, through min-tree chains, all chunks in parallel);
+// every later string o copies bytes [0, lcp[o]) from string o - 1, whose first
+// 32 G bytes the group keeps in shared memory (longer prefixes are read back
+// from o - 1's decompressed bytes, which this group wrote before its
+// __syncwarp).  Bytes [0, lcp[o]) of the buffer already hold string o - 1's
+// prefix, so each string only writes its own bytes into it.  Several groups
+// per warp cut the per-string overhead of short strings.
+constexpr int XT_THREADS = 256, XT_CHUNK = 128;
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+template <int G>
+__global__ void __launch_bounds__(XT_THREADS, 8)
+    k_extend_chunks(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, uint64_t n, const uint64_t* foff,
+                    const uint32_t* flen, uint8_t* full, uint32_t* err) {
+    constexpr uint32_t GROUPS = XT_THREADS / G, BUF = 32 * G;
+    __shared__ uint8_t sbuf[GROUPS][BUF];
+    const uint32_t lane = threadIdx.x % G, grp = threadIdx.x / G;
+    const uint32_t mask = G == 32 ? 0xffffffffu : ((1u << G) - 1) << (threadIdx.x & 31 & ~(G - 1));
+    uint8_t* buf = sbuf[grp];
+    const uint32_t nchunks = (uint32_t)((n + XT_CHUNK - 1) / XT_CHUNK);  // n <= bytes < 2^32
+    for (uint32_t c = blockIdx.x * GROUPS + grp; c < nchunks; c += gridDim.x * GROUPS) {
+        const uint32_t b0 = c * XT_CHUNK, e0 = (uint64_t)b0 + XT_CHUNK < n ? b0 + XT_CHUNK : (uint32_t)n;
+        uint32_t prev_len = 0;
+        const uint8_t* prev = nullptr;
+        for (uint32_t g = b0; g < e0; g += G) {
+            const uint32_t mine = g + lane;
+            uint32_t ml = 0, mf = 0, ms = 0;
+            uint64_t mo = 0;
+            if (mine < e0) {
+                ml = lcp[mine];
+                mf = flen[mine];
+                ms = start[mine];
+                mo = foff[mine];
+                prefetch_l1(chars + ms);
+            }
+            const int cnt = e0 - g < G ? (int)(e0 - g) : G;
+            for (int i = 0; i < cnt; ++i) {
+                const uint32_t l0 = __shfl_sync(mask, ml, i, G);
+                const uint32_t fo = __shfl_sync(mask, mf, i, G);
+                const uint32_t so = __shfl_sync(mask, ms, i, G);
+                const uint64_t oo = __shfl_sync(mask, mo, i, G);
+                uint8_t* dst = full + oo;
+                if (fo < l0) {
+                    if (lane == 0) atomicExch(err, 1u);
+                    return;
+                }
+                if (g + i == b0) {  // decompressed by k_extend before this kernel
+                    const uint32_t m = fo < BUF ? fo : BUF;
+                    for (uint32_t x = lane; x < m; x += G) buf[x] = dst[x];
+                    __syncwarp(mask);
+                    prev_len = fo;
+                    prev = dst;
+                    continue;
+                }
+                if (l0 > prev_len) {  // the LCP claims more bytes than the previous string holds
+                    if (lane == 0) atomicExch(err, 1u);
+                    return;
+                }
+                for (uint32_t x = lane; x < l0; x += G) dst[x] = x < BUF ? buf[x] : prev[x];
+                const uint8_t* src = chars + so;
+                for (uint32_t x = l0 + lane; x < fo; x += G) {
+                    const uint8_t v = src[x - l0];
+                    dst[x] = v;
+                    if (x < BUF) buf[x] = v;
+                }
+                __syncwarp(mask);
+                prev_len = fo;
+                prev = dst;
+            }
+        }
+    }
+}
+
+template <int G>
+static int launch_chunks(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, uint64_t n,
+                         const uint64_t* foff, const uint32_t* flen, uint8_t* full, uint32_t* err, cudaStream_t st) {
+    const uint64_t chunks = (n + XT_CHUNK - 1) / XT_CHUNK;
+    const uint64_t groups = XT_THREADS / G;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((chunks + groups - 1) / groups, 148 * 8));
+    DSSS_LAUNCH("k_extend_chunks", st,
+                k_extend_chunks<G><<<grid, XT_THREADS, 0, st>>>(chars, start, lcp, n, foff, flen, full, err));
+    return DSSS_OK;
+}
+
+template <int G>
+static int launch_extend(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, const MinTree& tree,
+                         uint64_t n, const uint64_t* foff, const uint32_t* flen, uint8_t* full, uint32_t* err,
+                         cudaStream_t st, uint64_t step = 1) {
+    const uint64_t strings = (n + step - 1) / step;
+    DSSS_LAUNCH("k_extend", st,
+                k_extend<G><<<grid_for(strings * G, 256), 256, 0, st>>>(chars, start, lcp, tree, n, step, foff, flen,
+                                                                       full, err));
+    return DSSS_OK;
+}
+
+// Lanes per chunk group: the knob's value, or from the average decompressed
+// length (about two passes of the group over a string).
+static int extend_lanes(uint64_t n, uint64_t full_bytes) {
+    const int64_t k = tune(TUNE_MERGE_LANES);
+    if (k > 0) return (int)k;
+    const uint64_t avg = n ? full_bytes / n : 0;
+    return avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 128 ? 16 : 32;
+}
+
+static int run_extend(const uint8_t* chars, const uint32_t* start, const uint32_t* lcp, const MinTree& tree,
+                      uint64_t n, uint64_t full_bytes, const uint64_t* foff, const uint32_t* flen, uint8_t* full,
+                      uint32_t* err, cudaStream_t st) {
+    DSSS_TRY(launch_extend<4>(chars, start, lcp, tree, n, foff, flen, full, err, st, XT_CHUNK));
+    switch (extend_lanes(n, full_bytes)) {
+    case 4: return launch_chunks<4>(chars, start, lcp, n, foff, flen, full, err, st);
+    case 8: return launch_chunks<8>(chars, start, lcp, n, foff, flen, full, err, st);
+    case 16: return launch_chunks<16>(chars, start, lcp, n, foff, flen, full, err, st);
+    default: return launch_chunks<32>(chars, start, lcp, n, foff, flen, full, err, st);
     }
 }
 
@@ -402,9 +531,7 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
     Carve c1(ctx->ws);
     layout_merge(c1, L, n, bytes, full_bytes, nruns);
     if (by_sort) layout_sort(c1, SL, n, nrecv, 0);
-    DSSS_LAUNCH("k_extend", st,
-                k_extend<<<grid_for(n, 256), 256, 0, st>>>(chars, start, L.l[0], tree, n, L.foff, L.flen, L.full,
-                                                          L.counters + 2));
+    DSSS_TRY(run_extend(chars, start, L.l[0], tree, n, full_bytes, L.foff, L.flen, L.full, L.counters + 2, st));
     if (by_sort) {
         // Merging sorted runs by sorting their union: each receiving PE's
         // strings are one segment of the string sort, with ids in run order so

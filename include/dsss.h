@@ -120,7 +120,11 @@ int dsss_abi_version(void);
  *                   and per-call instantiation)
  *   merge_by_sort   dsss_lcp_merge: decompressed runs merged by one segmented
  *                   string sort (1, default) or by pairwise merge-path rounds
- *                   (0); identical results, ties in run order either way */
+ *                   (0); identical results, ties in run order either way
+ *   merge_extend_lanes  dsss_lcp_merge prefix decompression: threads that
+ *                   decompress a chunk of 128 consecutive strings in order
+ *                   (4, 8, 16 or 32; default 0 = from the average
+ *                   decompressed length) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 

@@ -116,6 +116,10 @@ def test_knob_errors(dsss):
         dsss.tune_set("no_such_knob", 1)
     with pytest.raises(dsss.DsssError):
         dsss.tune_set("sort_small_max", 100000)
+    with pytest.raises(dsss.DsssError):
+        dsss.tune_set("merge_extend_lanes", 3)
+    with pytest.raises(dsss.DsssError):
+        dsss.tune_set("merge_extend_lanes", 2)
     v = dsss.tune_get("dp_filter_bits")
     dsss.tune_set("dp_filter_bits", 8)
     assert dsss.tune_get("dp_filter_bits") == 8

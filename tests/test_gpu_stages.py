@@ -213,3 +213,28 @@ def test_lcp_merge_modes_identical(dsss, ctx):
                                        char_start=g["char_start"]))
     for k in ("order", "merged_lcp", "old_lcp", "perm_index", "perm_pe"):
         assert np.array_equal(u64(outs[0][k]), u64(outs[1][k])), k
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_lcp_merge_extend_lanes(dsss, ctx, lanes):
+    """Prefix decompression with 4..32 threads per chunk of strings gives the golden
+    merge results, and the same order as the automatic choice on long shared
+    prefixes (suffixes of a 256-byte-periodic text)."""
+    with open(os.path.join(GOLDEN, "merge_ref.json")) as f:
+        gold = json.load(f)
+    with dsss.tuned(merge_extend_lanes=lanes):
+        _merge_golden(dsss, ctx, gold)
+    hs = dsss.gen_suffix_strings(50000, 256, seed=13)
+    ds = dsss.DeviceStrings(hs)
+    p = 4
+    order, lcp = dsss.local_sort_lcp(ctx, ds, p)
+    dp, _ = dsss.dp_prefixes(ctx, ds, order, lcp, p)
+    iv = dsss.partition(ctx, ds, order, dp, p)
+    g = dsss.bucket_scatter(ctx, ds, p, order, lcp, dp, iv)
+    outs = []
+    for k in (0, lanes):
+        with dsss.tuned(merge_extend_lanes=k):
+            outs.append(dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
+                                       char_start=g["char_start"]))
+    for k in ("order", "merged_lcp", "old_lcp", "perm_index", "perm_pe"):
+        assert np.array_equal(u64(outs[0][k]), u64(outs[1][k])), k
