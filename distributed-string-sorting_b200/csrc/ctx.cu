@@ -69,8 +69,9 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"sort_graph_max_n", 0, 0, 1ll << 32},
     {"merge_by_sort", 1, 0, 1},
     {"merge_extend_lanes", 0, 0, 32},
+    {"dp_split", 0, 0, 1},
 };
-static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}};
+static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}, {0}};
 
 int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
 

@@ -138,6 +138,28 @@ __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all,
     block_add(counters + 1, nstays);
 }
 
+// Inserts h into the table region (base, mask) by linear probing; returns its
+// slot, NO_SLOT when the region is full.  The table always has free slots, so
+// a free or matching slot is reached within mask + 1 probes.
+__device__ __forceinline__ uint32_t table_insert(unsigned long long* tkeys, uint8_t* tdup, uint64_t base, uint32_t mask,
+                                                 unsigned long long h, uint32_t* err) {
+    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
+    for (uint32_t probe = 0;; ++probe) {
+        if (probe > mask) {
+            atomicExch(err, 1u);
+            return NO_SLOT;
+        }
+        const unsigned long long prev = atomicCAS(&tkeys[base + sl], EMPTY_KEY, h);
+        if (prev == EMPTY_KEY) break;
+        if (prev == h) {
+            tdup[base + sl] = 1;
+            break;
+        }
+        sl = (sl + 1) & mask;
+    }
+    return (uint32_t)(base + sl);
+}
+
 // Each string set owns a power-of-two region of the table (base, mask): equal
 // prefixes in different sets are not duplicates of each other.
 __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
@@ -152,28 +174,35 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* 
         const uint32_t sid = set_of(set_begin, nsets, i);
         base = set_base[sid];
         mask = set_mask[sid];
-        tkeys += base;
-        tdup += base;
     }
     const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
-    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
-    // Linear probing; the table always has free slots, so a free or matching
-    // slot is reached within mask + 1 probes.
-    for (uint32_t probe = 0;; ++probe) {
-        if (probe > mask) {
-            atomicExch(err, 1u);
-            sl = NO_SLOT;
-            break;
-        }
-        const unsigned long long prev = atomicCAS(&tkeys[sl], EMPTY_KEY, h);
-        if (prev == EMPTY_KEY) break;
-        if (prev == h) {
-            tdup[sl] = 1;
-            break;
-        }
-        sl = (sl + 1) & mask;
+    slot[i] = table_insert(tkeys, tdup, base, mask, h, err);
+}
+
+// Split form of k_dp_hash (knob dp_split): the hashes first, stored per
+// position, then the table inserts by a kernel of few registers, so that many
+// more inserts are in flight.
+__global__ void __launch_bounds__(256, 5) k_dp_hash_store(ArenaDev a, const uint64_t* soff, const uint8_t* kind,
+                                                          uint64_t n, uint32_t depth, unsigned long long* hbuf) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    hbuf[i] = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+}
+
+__global__ void __launch_bounds__(256) k_dp_insert(const uint8_t* kind, uint64_t n, const unsigned long long* hbuf,
+                                                   unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1,
+                                                   const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
+                                                   const uint32_t* set_mask, uint32_t* slot, uint32_t* err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    uint64_t base = 0;
+    uint32_t mask = mask1;
+    if (nsets > 1) {
+        const uint32_t sid = set_of(set_begin, nsets, i);
+        base = set_base[sid];
+        mask = set_mask[sid];
     }
-    slot[i] = sl == NO_SLOT ? NO_SLOT : (uint32_t)(base + sl);
+    slot[i] = table_insert(tkeys, tdup, base, mask, hbuf[i], err);
 }
 
 __global__ void __launch_bounds__(256) k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup,
@@ -424,15 +453,16 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     // fingerprint filter: planned when a round may hash dp_filter_min strings
     L.filter_min = (uint64_t)tune(TUNE_DP_FILTER_MIN);
     L.filter_bpk = (uint32_t)tune(TUNE_DP_FILTER_BITS);
-    if (N >= L.filter_min) {
+    L.split = tune(TUNE_DP_SPLIT) != 0;
+    const bool filter = N >= L.filter_min;
+    L.hbuf = (filter || L.split) ? c.take<unsigned long long>(N) : nullptr;
+    if (filter) {
         L.bm_words = (nsets == 1 ? pow2_at_least(N * L.filter_bpk, 1024) : 2 * N * L.filter_bpk + 1024ull * nsets) / 32;
         L.bits = c.take<uint32_t>(L.bm_words);
-        L.hbuf = c.take<unsigned long long>(N);
         L.cand = c.take<uint32_t>(N);
     } else {
         L.bm_words = 0;
         L.bits = nullptr;
-        L.hbuf = nullptr;
         L.cand = nullptr;
     }
 }
@@ -524,10 +554,19 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
             if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
             DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
             DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-            DSSS_LAUNCH("k_dp_hash", st,
-                        k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
-                                                       (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
-                                                       L.set_mask, L.slot, L.counters + 2));
+            if (L.split) {
+                DSSS_LAUNCH("k_dp_hash_store", st,
+                            k_dp_hash_store<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.hbuf));
+                DSSS_LAUNCH("k_dp_insert", st,
+                            k_dp_insert<<<grid, 256, 0, st>>>(L.kind, n, L.hbuf, L.tkeys, L.tdup, (uint32_t)(slots - 1),
+                                                             L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
+                                                             L.counters + 2));
+            } else {
+                DSSS_LAUNCH("k_dp_hash", st,
+                            k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
+                                                           (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
+                                                           L.set_mask, L.slot, L.counters + 2));
+            }
             DSSS_LAUNCH("k_dp_query", st,
                         k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
             DSSS_CUDA(cudaGetLastError());

@@ -28,8 +28,9 @@ struct DpLayout {
     uint32_t filter_bpk;
     uint64_t bm_words;
     uint32_t* bits;
-    unsigned long long* hbuf;
+    unsigned long long* hbuf;  // also the stored hashes of the split hash round
     uint32_t* cand;
+    bool split;  // hash round as k_dp_hash_store + k_dp_insert
     uint64_t* set_bbase;
     uint32_t* set_bmask;
     uint32_t* set_ccnt;

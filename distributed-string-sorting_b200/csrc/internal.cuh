@@ -134,6 +134,7 @@ enum TuneKnob : int {
     TUNE_SORT_GRAPH,         // largest n sorted by the device-driven graph (0: never)
     TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1) or by merge rounds (0)
     TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
+    TUNE_DP_SPLIT,           // hash round split into hashing and table inserts (1) or one kernel (0)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

@@ -691,9 +691,10 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
 // ------------------------------------------------------------ small sort ----
 // Segments of 2..small_max strings finish inside one CTA (the tail the MSD
 // passes hand over, like the reference's insertion-sort / multikey tail):
-//  - buckets of up to 32 strings: one warp, a bitonic network across the 32
-//    lanes on (group, key, id); groups of equal keys are re-keyed 8 bytes
-//    deeper until each group is one string or byte-identical strings;
+//  - buckets of up to 64 strings: one warp, a bitonic network across the 32
+//    lanes (two elements per lane above 32) on (group, key, id); groups of
+//    equal keys jump to the depth where a member leaves the group's head and
+//    are sorted again until each group is one string or byte-identical strings;
 //  - larger buckets: an MSD pass in shared memory on the first key byte that
 //    differs inside the bucket (warp-aggregated histogram, scan, stable
 //    scatter); children go on a shared-memory stack or to the warp list.
@@ -715,22 +716,41 @@ __device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint
         key = ~0ull;
         id = 0xFFFFFFFFu;
     }
-    for (;;) {
+    for (bool first = true;; first = false) {
+        if (first) {
+            // one group at one depth (invalid lanes carry the largest key
+            // and id, so they still sort last): (key, id) is the whole order
 #pragma unroll
-        for (int k = 2; k <= 32; k <<= 1) {
+            for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                const uint32_t pg = __shfl_xor_sync(FULL, grp, j);
-                const uint64_t pk = __shfl_xor_sync(FULL, key, j);
-                const uint32_t po = __shfl_xor_sync(FULL, id, j);
-                const uint32_t pd = __shfl_xor_sync(FULL, dep, j);
-                const bool want_min = ((lane & k) == 0) == ((lane & j) == 0);
-                const bool take = want_min ? lt3(pg, pk, po, grp, key, id) : lt3(grp, key, id, pg, pk, po);
-                if (take) {
-                    grp = pg;
-                    key = pk;
-                    id = po;
-                    dep = pd;
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint64_t pk = __shfl_xor_sync(FULL, key, j);
+                    const uint32_t po = __shfl_xor_sync(FULL, id, j);
+                    const bool want_min = ((lane & k) == 0) == ((lane & j) == 0);
+                    const bool less = pk < key || (pk == key && po < id);
+                    if (less == want_min) {
+                        key = pk;
+                        id = po;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint32_t pg = __shfl_xor_sync(FULL, grp, j);
+                    const uint64_t pk = __shfl_xor_sync(FULL, key, j);
+                    const uint32_t po = __shfl_xor_sync(FULL, id, j);
+                    const uint32_t pd = __shfl_xor_sync(FULL, dep, j);
+                    const bool want_min = ((lane & k) == 0) == ((lane & j) == 0);
+                    const bool take = want_min ? lt3(pg, pk, po, grp, key, id) : lt3(grp, key, id, pg, pk, po);
+                    if (take) {
+                        grp = pg;
+                        key = pk;
+                        id = po;
+                        dep = pd;
+                    }
                 }
             }
         }
@@ -780,6 +800,162 @@ __device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint
     }
 }
 
+// Buckets of 33..64 strings: lane l holds positions l and l + 32 (elements 0
+// and 1).  The same bitonic order on (group, key, id) over 64 positions (the
+// stage j = 32 compares a lane's two elements), the same run handling as
+// warp_sort; the run minima go through `scratch` (>= size words of shared
+// memory owned by this warp).
+__device__ __forceinline__ void cx_key_id(uint64_t& key, uint32_t& id, int j, bool want_min) {
+    const uint64_t pk = __shfl_xor_sync(FULL, key, j);
+    const uint32_t po = __shfl_xor_sync(FULL, id, j);
+    const bool less = pk < key || (pk == key && po < id);
+    if (less == want_min) {
+        key = pk;
+        id = po;
+    }
+}
+
+__device__ __forceinline__ void cx_full(uint32_t& grp, uint64_t& key, uint32_t& id, uint32_t& dep, int j,
+                                        bool want_min) {
+    const uint32_t pg = __shfl_xor_sync(FULL, grp, j);
+    const uint64_t pk = __shfl_xor_sync(FULL, key, j);
+    const uint32_t po = __shfl_xor_sync(FULL, id, j);
+    const uint32_t pd = __shfl_xor_sync(FULL, dep, j);
+    const bool take = want_min ? lt3(pg, pk, po, grp, key, id) : lt3(grp, key, id, pg, pk, po);
+    if (take) {
+        grp = pg;
+        key = pk;
+        id = po;
+        dep = pd;
+    }
+}
+
+__device__ void warp_sort64(const ArenaDev& a, uint32_t size, uint32_t depth, uint64_t (&key)[2], uint32_t (&id)[2],
+                            uint32_t* lcp, uint32_t* scratch) {
+    const uint32_t lane = threadIdx.x & 31;
+    bool valid[2];
+    uint32_t grp[2], dep[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        valid[h] = lane + 32 * h < size;
+        grp[h] = valid[h] ? 0u : 0xFFFFFFFFu;
+        dep[h] = depth;
+        if (!valid[h]) {
+            key[h] = ~0ull;
+            id[h] = 0xFFFFFFFFu;
+        }
+    }
+    for (bool first = true;; first = false) {
+#pragma unroll
+        for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                if (j == 32) {  // k == 64: ascending, element 0 takes the smaller
+                    // In the first network the group marks positions (valid
+                    // or padding) and the depth is uniform: only (key, id)
+                    // move, as in cx_key_id.
+                    const bool sw = first ? (key[1] < key[0] || (key[1] == key[0] && id[1] < id[0]))
+                                          : lt3(grp[1], key[1], id[1], grp[0], key[0], id[0]);
+                    if (sw) {
+                        uint64_t tk = key[0];
+                        key[0] = key[1];
+                        key[1] = tk;
+                        uint32_t t = id[0];
+                        id[0] = id[1];
+                        id[1] = t;
+                        if (!first) {
+                            t = grp[0];
+                            grp[0] = grp[1];
+                            grp[1] = t;
+                            t = dep[0];
+                            dep[0] = dep[1];
+                            dep[1] = t;
+                        }
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t pos = lane + 32 * h;
+                    const bool want_min = ((pos & k) == 0) == ((pos & j) == 0);
+                    if (first) cx_key_id(key[h], id[h], j, want_min);
+                    else cx_full(grp[h], key[h], id[h], dep[h], j, want_min);
+                }
+            }
+        }
+        // predecessor of each position: lane - 1 of the same half, lane 31 of
+        // half 0 for position 32
+        const uint64_t k31 = __shfl_sync(FULL, key[0], 31);
+        const uint32_t g31 = __shfl_sync(FULL, grp[0], 31);
+        bool head[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint64_t qu = __shfl_up_sync(FULL, key[h], 1);
+            const uint32_t gu = __shfl_up_sync(FULL, grp[h], 1);
+            const uint64_t qk = lane == 0 ? k31 : qu;
+            const uint32_t qg = lane == 0 ? g31 : gu;
+            const bool has_pred = h == 1 || lane > 0;
+            head[h] = !has_pred || qg != grp[h] || qk != key[h];
+            if (valid[h] && has_pred && qg == grp[h]) {
+                const uint32_t pos = lane + 32 * h;
+                if (qk != key[h]) {
+                    lcp[pos] = dep[h] + key_lcp(key[h], qk);
+                } else {
+                    const uint32_t z = zero_byte(key[h]);
+                    if (z < 8) lcp[pos] = dep[h] + z;  // byte-identical neighbours
+                }
+            }
+        }
+        const uint64_t heads = (uint64_t)__ballot_sync(FULL, head[0]) | (uint64_t)__ballot_sync(FULL, head[1]) << 32;
+        bool unres[2];
+        uint32_t rs[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t pos = lane + 32 * h;
+            rs[h] = 63u - (uint32_t)__clzll(heads & ((2ull << pos) - 1ull));
+            const bool next_head = pos == 63 ? true : ((heads >> (pos + 1)) & 1ull) != 0;
+            const bool multi = !head[h] || (!next_head && pos + 1 < size);
+            unres[h] = valid[h] && multi && zero_byte(key[h]) == 8;
+            if (valid[h]) grp[h] = rs[h];
+        }
+        if (!__any_sync(FULL, unres[0] || unres[1])) break;
+        // Every unresolved run shares its 8-byte key: jump to the first depth
+        // where a member differs from the run head (or ends).
+        for (uint32_t x = lane; x < size; x += 32) scratch[x] = 0xFFFFFFFFu;
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t h0 = __shfl_sync(FULL, id[0], rs[h] & 31), h1 = __shfl_sync(FULL, id[1], rs[h] & 31);
+            const uint32_t hid = rs[h] < 32 ? h0 : h1;
+            if (unres[h] && lane + 32 * h != rs[h]) {
+                uint64_t off, offh;
+                uint32_t len, lenh;
+                str_of(a, id[h], off, len);
+                str_of(a, hid, offh, lenh);
+                uint32_t l;
+                for (uint32_t d = dep[h] + 8;; d += 16) {
+                    const uint64_t x0 = key8(a.chars, off, len, d), y0 = key8(a.chars, offh, lenh, d);
+                    const uint64_t x1 = key8(a.chars, off, len, d + 8), y1 = key8(a.chars, offh, lenh, d + 8);
+                    if (x0 != y0) { l = d + key_lcp(x0, y0); break; }
+                    if (zero_byte(x0) < 8) { l = d + zero_byte(x0); break; }
+                    if (x1 != y1) { l = d + 8 + key_lcp(x1, y1); break; }
+                    if (zero_byte(x1) < 8) { l = d + 8 + zero_byte(x1); break; }
+                }
+                atomicMin(&scratch[rs[h]], l);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (unres[h]) {
+                dep[h] = scratch[rs[h]];
+                key[h] = key8_of(a, id[h], dep[h]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Segments of 2..32 strings: one warp each, four per CTA.
 // dcount (graph mode): the segment count on the device; blocks stride over it.
 __global__ void __launch_bounds__(128) k_warp_segs(SortState S, const Seg* segs, uint32_t nseg, const uint32_t* dcount) {
@@ -810,6 +986,7 @@ constexpr size_t seg_sort_smem() {
 // due (SF_PIVOT), or the keys are pivot pseudo keys whose base depth is the
 // bucket depth (SF_PSEUDO).
 constexpr uint32_t SF_REKEY = 1u, SF_PIVOT = 2u, SF_PSEUDO = 4u;
+constexpr uint32_t WL_MAX = 64;  // buckets up to this size go to the warp sorts
 
 template <int CAP, int NT>
 __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg, const uint32_t* dcount) {
@@ -821,7 +998,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     uint32_t* to = so + CAP;
     uint32_t* pk = to + CAP;  // digit << 24 | rank within the warp's chunk
     uint32_t* stk = pk + CAP;  // (start, size | flags << 16, depth) of buckets > 32
-    uint32_t* wl = stk + 3 * (CAP / 2);  // (start, size | flags << 16, depth) of buckets <= 32
+    uint32_t* wl = stk + 3 * (CAP / 2);  // (start, size | flags << 16, depth) of buckets <= WL_MAX
     __shared__ uint32_t hist[256], bstart[256];
     __shared__ uint32_t wcnt[NW][256];
     __shared__ uint32_t s_top, s_nw, s_cur[3];
@@ -849,11 +1026,11 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     if (threadIdx.x == 0) {
         s_top = 0;
         s_nw = 0;
-        uint32_t* dst = size <= 32 ? wl : stk;
+        uint32_t* dst = size <= WL_MAX ? wl : stk;
         dst[0] = 0;
         dst[1] = size;
         dst[2] = seg.depth;
-        if (size <= 32) s_nw = 1;
+        if (size <= WL_MAX) s_nw = 1;
         else s_top = 1;
         s_diff = 0;
     }
@@ -1026,9 +1203,11 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                 continue;
             }
             if (cnt < 2) continue;
+            // buckets for the warp list (<= WL_MAX) carry keys valid at their
+            // depth or SF_REKEY, never pivot flags or pseudo keys
             uint32_t cd, cf;
             if (!pseudo) {
-                if (S.pivot && cnt > 32 && 2 * cnt > bn) {
+                if (S.pivot && cnt > WL_MAX && 2 * cnt > bn) {
                     cd = dep + b + 1;  // keeps most of the bucket: pivot pass next
                     cf = SF_PIVOT;
                 } else {
@@ -1036,7 +1215,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                     cf = 0;
                 }
             } else if (code_split) {
-                if (cnt > 32) {
+                if (cnt > WL_MAX) {
                     cd = dep;
                     cf = SF_PSEUDO;
                 } else {
@@ -1051,11 +1230,11 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                 }
             } else {
                 cd = lin + 1;
-                cf = (S.pivot && cnt > 32 && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
+                cf = (S.pivot && cnt > WL_MAX && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
             }
             uint32_t* dst;
             uint32_t slot;
-            if (cnt <= 32) {
+            if (cnt <= WL_MAX) {
                 slot = atomicAdd(&s_nw, 1u);
                 dst = wl + 3 * slot;
             } else {
@@ -1073,14 +1252,36 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     for (uint32_t e = w; e < nwl; e += NW) {
         const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1] & 0xFFFFu, wd = wl[3 * e + 2];
         const bool rekey = (wl[3 * e + 1] >> 16) & SF_REKEY;
-        uint64_t key = 0;
-        uint32_t id = 0;
-        if ((uint32_t)lane < wn) {
-            id = so[ws + lane];
-            key = rekey ? key8_of(S.a, id, wd) : sk[ws + lane];
+        if (wn <= 32) {
+            uint64_t key = 0;
+            uint32_t id = 0;
+            if ((uint32_t)lane < wn) {
+                id = so[ws + lane];
+                key = rekey ? key8_of(S.a, id, wd) : sk[ws + lane];
+            }
+            warp_sort(S.a, wn, wd, key, id, lcp + ws);
+            if ((uint32_t)lane < wn) so[ws + lane] = id;
+        } else {
+            // pk of this bucket's positions is free once the block passes end
+            uint64_t key[2];
+            uint32_t id[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t pos = (uint32_t)lane + 32 * h;
+                id[h] = 0;
+                key[h] = 0;
+                if (pos < wn) {
+                    id[h] = so[ws + pos];
+                    key[h] = rekey ? key8_of(S.a, id[h], wd) : sk[ws + pos];
+                }
+            }
+            warp_sort64(S.a, wn, wd, key, id, lcp + ws, pk + ws);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t pos = (uint32_t)lane + 32 * h;
+                if (pos < wn) so[ws + pos] = id[h];
+            }
         }
-        warp_sort(S.a, wn, wd, key, id, lcp + ws);
-        if ((uint32_t)lane < wn) so[ws + lane] = id;
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < size; i += NT) S.ord_out[start + i] = so[i];

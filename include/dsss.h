@@ -124,7 +124,10 @@ int dsss_abi_version(void);
  *   merge_extend_lanes  dsss_lcp_merge prefix decompression: threads that
  *                   decompress a chunk of 128 consecutive strings in order
  *                   (4, 8, 16 or 32; default 0 = from the average
- *                   decompressed length) */
+ *                   decompressed length)
+ *   dp_split        distinguishing-prefix hash rounds as two kernels, hashes
+ *                   stored per position then inserted into the table (1), or
+ *                   hash and insert in one kernel (0, default) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 

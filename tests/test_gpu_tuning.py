@@ -1,6 +1,7 @@
 """Tuning knobs change how the path runs, never its results: the fingerprint
 filter of the distinguishing-prefix rounds (forced on for small inputs), the
-pivot passes of the string sort (off), and the small-segment cutoff."""
+pivot passes of the string sort (off), the small-segment cutoff, and the
+hash rounds split into hashing and insert kernels."""
 import numpy as np
 import pytest
 
@@ -41,6 +42,30 @@ def test_filter_batched(dsss, ctx):
     with dsss.tuned(dp_filter_min=0):
         out = dsss.pd_sort_batched(ctx, dsss.DeviceStrings(hs), 4, 4, pb)
     for s, h in enumerate([h1, h2, h1, h2]):
+        ref = dsss.pd_sort(ctx, dsss.DeviceStrings(h), 4)
+        b, e = int(sb[s]), int(sb[s + 1])
+        assert np.array_equal(u64(out["dp"], hs.n)[b:e], u64(ref["dp"], h.n)), s
+        assert np.array_equal(u64(out["perm_index"], hs.n)[b:e], u64(ref["perm_index"], h.n)), s
+
+
+@pytest.mark.parametrize("name,strs", CASES, ids=IDS)
+def test_dp_split(dsss, orc, ctx, name, strs):
+    """Hash rounds as separate hashing and insert kernels: the oracle's result."""
+    hs = host_of(dsss, strs)
+    with dsss.tuned(dp_split=1):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 3)
+    check_pd(dsss, orc, hs, out, 3)
+
+
+def test_dp_split_batched(dsss, ctx):
+    """Split hash rounds over per-set table regions: each set's own result."""
+    h1 = dsss.gen_dn(20000, 100, 50, seed=33)
+    h2 = dsss.gen_suffix_strings(30000, 256, seed=5)
+    hs, sb = dsss.concat_sets([h1, h2, h1])
+    pb = dsss.batched_parts(sb, 4)
+    with dsss.tuned(dp_split=1):
+        out = dsss.pd_sort_batched(ctx, dsss.DeviceStrings(hs), 3, 4, pb)
+    for s, h in enumerate([h1, h2, h1]):
         ref = dsss.pd_sort(ctx, dsss.DeviceStrings(h), 4)
         b, e = int(sb[s]), int(sb[s + 1])
         assert np.array_equal(u64(out["dp"], hs.n)[b:e], u64(ref["dp"], h.n)), s
