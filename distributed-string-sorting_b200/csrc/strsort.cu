@@ -152,7 +152,38 @@ __global__ void k_tile_counts(const Seg* segs, uint32_t nseg, uint32_t* tiles, u
 }
 
 // ---------------------------------------------------------------- prefix ----
-__global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32_t nseg) {
+// Big-endian key words [d, d + 8 W) of a string (0 past its end) from at most
+// W + 1 aligned 8-byte loads, all issued before any is used.  Words wholly
+// past the end are not loaded, so at most 15 bytes past a string are read
+// (the arena contract pads 32).
+template <int W>
+__device__ __forceinline__ void key_words(const uint8_t* chars, uint64_t off, uint32_t len, uint32_t d,
+                                          uint32_t want, uint64_t (&x)[W]) {
+    const uint32_t avail = d < len ? (len - d + 7) >> 3 : 0;
+    const uint32_t words = want < avail ? want : avail;
+    const uintptr_t p = (uintptr_t)(chars + off + d);
+    const unsigned long long* q = (const unsigned long long*)(p & ~(uintptr_t)7);
+    const unsigned sh = (unsigned)(p & 7) * 8;
+    uint64_t raw[W + 1];
+    const uint32_t loads = words ? words + (sh != 0) : 0;
+#pragma unroll
+    for (int w = 0; w <= W; ++w) raw[w] = (uint32_t)w < loads ? __ldg(q + w) : 0ull;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        uint64_t v = sh ? (raw[w] >> sh) | (raw[w + 1] << (64 - sh)) : raw[w];
+        const uint32_t at = d + 8 * w;
+        if ((uint32_t)w >= words || at >= len) {
+            v = 0;
+        } else if (len - at < 8) {
+            v &= (1ull << ((len - at) * 8)) - 1;
+        }
+        x[w] = bswap64(v);
+    }
+}
+
+constexpr int PF_W = 8;  // prefix words compared per batch (64 bytes)
+
+__global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
         segs = S.large[S.counters[12]];
         nseg = S.counters[13];
@@ -171,32 +202,66 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
     uint64_t off0;
     uint32_t len0;
     str_of(S.a, s0, off0, len0);
+    // the first string's first 64 bytes from d0, shared by the block
+    __shared__ unsigned long long y[PF_W];
+    if (threadIdx.x == 0) {
+        uint64_t v[PF_W];
+        key_words<PF_W>(S.a.chars, off0, len0, d0, PF_W, v);
+#pragma unroll
+        for (int w = 0; w < PF_W; ++w) y[w] = v[w];
+    }
+    __syncthreads();
     uint32_t mn = 0xFFFFFFFFu;
     for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
         uint64_t off;
         uint32_t len;
         str_of(S.a, ord[i], off, len);
-        uint32_t d = d0, l;
         // no need to compare past this thread's minimum so far
         const uint32_t lim = min(cap, mn);
-        for (;;) {
-            // 16 bytes per step: two independent 8-byte compares
-            uint64_t x[2], y[2];
+        uint32_t l = 0;
+        bool done = false;
+        // first batch: every word up to the limit loaded at once
+        {
+            const uint32_t want = lim > d0 ? min((lim - d0 + 7) >> 3, (uint32_t)PF_W) : 0u;
+            uint64_t x[PF_W];
+            key_words<PF_W>(S.a.chars, off, len, d0, want, x);
+#pragma unroll
+            for (int w = 0; w < PF_W; ++w) {
+                if (!done && (uint32_t)w < want) {
+                    if (x[w] != y[w]) {
+                        l = d0 + 8 * w + key_lcp(x[w], y[w]);
+                        done = true;
+                    } else {
+                        const uint32_t z = zero_byte(x[w]);
+                        if (z < 8) {
+                            l = d0 + 8 * w + z;
+                            done = true;
+                        }
+                    }
+                }
+            }
+            if (!done && d0 + 8 * want >= lim) {
+                l = d0 + 8 * want;
+                done = true;
+            }
+        }
+        // longer common prefixes: 16 bytes per step
+        for (uint32_t d = d0 + 8 * PF_W; !done;) {
+            uint64_t xx[2], yy[2];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                x[q] = key8(S.a.chars, off, len, d + 8 * q);
-                y[q] = key8(S.a.chars, off0, len0, d + 8 * q);
+                xx[q] = key8(S.a.chars, off, len, d + 8 * q);
+                yy[q] = key8(S.a.chars, off0, len0, d + 8 * q);
             }
-            bool done = false;
             l = d + 16;
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 if (!done) {
-                    if (x[q] != y[q]) {
-                        l = d + 8 * q + key_lcp(x[q], y[q]);
+                    if (xx[q] != yy[q]) {
+                        l = d + 8 * q + key_lcp(xx[q], yy[q]);
                         done = true;
                     } else {
-                        const uint32_t z = zero_byte(x[q]);
+                        const uint32_t z = zero_byte(xx[q]);
                         if (z < 8) {
                             l = d + 8 * q + z;
                             done = true;
@@ -219,6 +284,7 @@ __global__ void __launch_bounds__(LT_NT) k_prefix(SortState S, Seg* segs, uint32
 }
 
 // ------------------------------------------------------------- keys/diff ----
+constexpr int KD_ILP = 8;
 __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
         segs = S.large[S.counters[12]];
@@ -247,25 +313,25 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
     if (valid) {
         for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) df |= key[i] ^ k0;
     } else {
-        // four independent gathers in flight per thread
-        for (uint32_t i0 = tb + threadIdx.x; i0 < te; i0 += 4 * LT_NT) {
-            uint32_t s[4];
-            uint64_t off[4];
-            uint32_t len[4];
+        // KD_ILP independent gathers in flight per thread
+        for (uint32_t i0 = tb + threadIdx.x; i0 < te; i0 += KD_ILP * LT_NT) {
+            uint32_t s[KD_ILP];
+            uint64_t off[KD_ILP];
+            uint32_t len[KD_ILP];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < KD_ILP; ++q) {
                 const uint32_t i = i0 + q * LT_NT;
                 s[q] = i < te ? ord[i] : 0u;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < KD_ILP; ++q) {
                 const uint32_t i = i0 + q * LT_NT;
                 off[q] = 0;
                 len[q] = 0;
                 if (i < te) str_of(S.a, s[q], off[q], len[q]);
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < KD_ILP; ++q) {
                 const uint32_t i = i0 + q * LT_NT;
                 if (i < te) {
                     const uint64_t k = key8(S.a.chars, off[q], len[q], depth);
@@ -691,8 +757,9 @@ __global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs,
 // ------------------------------------------------------------ small sort ----
 // Segments of 2..small_max strings finish inside one CTA (the tail the MSD
 // passes hand over, like the reference's insertion-sort / multikey tail):
-//  - buckets of up to 64 strings: one warp, a bitonic network across the 32
-//    lanes (two elements per lane above 32) on (group, key, id); groups of
+//  - buckets of up to 32 strings, and of up to 64 from a wide split in the
+//    large variants: one warp, a bitonic network across the 32 lanes (two
+//    elements per lane above 32) on (group, key, id); groups of
 //    equal keys jump to the depth where a member leaves the group's head and
 //    are sorted again until each group is one string or byte-identical strings;
 //  - larger buckets: an MSD pass in shared memory on the first key byte that
@@ -986,11 +1053,14 @@ constexpr size_t seg_sort_smem() {
 // due (SF_PIVOT), or the keys are pivot pseudo keys whose base depth is the
 // bucket depth (SF_PSEUDO).
 constexpr uint32_t SF_REKEY = 1u, SF_PIVOT = 2u, SF_PSEUDO = 4u;
-constexpr uint32_t WL_MAX = 64;  // buckets up to this size go to the warp sorts
+constexpr uint32_t WL_MAX = 64;  // largest bucket a warp sort takes (wide splits only)
 
 template <int CAP, int NT>
 __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, uint32_t nseg, const uint32_t* dcount) {
     constexpr int NW = NT / 32;
+    // the 64-wide warp sort only where segments are large enough to split
+    // wide (its registers would cost the small variant occupancy)
+    constexpr uint32_t WIDE_WL = CAP >= 1024 ? WL_MAX : 32;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* sk = (unsigned long long*)smem;
     unsigned long long* tk = sk + CAP;
@@ -1026,11 +1096,11 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     if (threadIdx.x == 0) {
         s_top = 0;
         s_nw = 0;
-        uint32_t* dst = size <= WL_MAX ? wl : stk;
+        uint32_t* dst = size <= 32 ? wl : stk;
         dst[0] = 0;
         dst[1] = size;
         dst[2] = seg.depth;
-        if (size <= WL_MAX) s_nw = 1;
+        if (size <= 32) s_nw = 1;
         else s_top = 1;
         s_diff = 0;
     }
@@ -1203,11 +1273,9 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                 continue;
             }
             if (cnt < 2) continue;
-            // buckets for the warp list (<= WL_MAX) carry keys valid at their
-            // depth or SF_REKEY, never pivot flags or pseudo keys
             uint32_t cd, cf;
             if (!pseudo) {
-                if (S.pivot && cnt > WL_MAX && 2 * cnt > bn) {
+                if (S.pivot && cnt > 32 && 2 * cnt > bn) {
                     cd = dep + b + 1;  // keeps most of the bucket: pivot pass next
                     cf = SF_PIVOT;
                 } else {
@@ -1215,7 +1283,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                     cf = 0;
                 }
             } else if (code_split) {
-                if (cnt > WL_MAX) {
+                if (cnt > 32) {
                     cd = dep;
                     cf = SF_PSEUDO;
                 } else {
@@ -1230,11 +1298,18 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                 }
             } else {
                 cd = lin + 1;
-                cf = (S.pivot && cnt > WL_MAX && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
+                cf = (S.pivot && cnt > 32 && 2 * cnt > bn) ? SF_PIVOT : SF_REKEY;
             }
+            // Warp list: up to 32 strings, or up to WL_MAX with plain keys
+            // (valid or re-gathered) from a wide split (at most 1/8 of the
+            // bucket: the keys' remaining bytes are likely to tell the strings
+            // apart in one network).  Narrow splits and chains stay with the
+            // block: a deep 64-string bucket on one warp would work through
+            // all of its runs alone, where a block pass hands them to 8 warps,
+            // and a chain of long shared prefixes gets the pivot pass.
             uint32_t* dst;
             uint32_t slot;
-            if (cnt <= WL_MAX) {
+            if (cnt <= 32 || (cnt <= WIDE_WL && 8 * cnt <= bn && !(cf & (SF_PIVOT | SF_PSEUDO)))) {
                 slot = atomicAdd(&s_nw, 1u);
                 dst = wl + 3 * slot;
             } else {
@@ -1252,7 +1327,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     for (uint32_t e = w; e < nwl; e += NW) {
         const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1] & 0xFFFFu, wd = wl[3 * e + 2];
         const bool rekey = (wl[3 * e + 1] >> 16) & SF_REKEY;
-        if (wn <= 32) {
+        if (WIDE_WL == 32 || wn <= 32) {
             uint64_t key = 0;
             uint32_t id = 0;
             if ((uint32_t)lane < wn) {
@@ -1275,7 +1350,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
                     key[h] = rekey ? key8_of(S.a, id[h], wd) : sk[ws + pos];
                 }
             }
-            warp_sort64(S.a, wn, wd, key, id, lcp + ws, pk + ws);
+            if constexpr (WIDE_WL > 32) warp_sort64(S.a, wn, wd, key, id, lcp + ws, pk + ws);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const uint32_t pos = (uint32_t)lane + 32 * h;

@@ -293,14 +293,38 @@ class GpuBackend:
 def sample_positions(sizes, p_global: int, factor: int = 2):
     """Per PE of `sizes` strings: the local indices SampleSplittersNumStringsPolicy
     samples (nr = min(factor (p-1), n_q), index floor(i n_q / (nr + 1)) in double
-    arithmetic, samplingStrategies.hpp:57-89)."""
+    arithmetic, samplingStrategies.hpp:57-89), as int64 arrays."""
     out = []
     for nq in sizes:
         nq = int(nq)
         nr = min(factor * (p_global - 1), nq)
         dist = float(nq) / float(nr + 1)
-        out.append([int(float(i) * dist) for i in range(1, nr + 1)])
+        out.append(np.floor(np.arange(1, nr + 1, dtype=np.float64) * dist).astype(np.int64))
     return out
+
+
+def _pack_rows(*cols, blob=None):
+    """One int64 message: the column lengths, the columns, then the blob bytes
+    (padded to 8) viewed as int64 — one all-gather instead of one per column."""
+    blob = np.zeros(0, np.uint8) if blob is None else np.ascontiguousarray(blob, np.uint8)
+    padded = np.zeros((blob.size + 7) // 8 * 8, np.uint8)
+    padded[:blob.size] = blob
+    head = [len(cols), blob.size] + [int(np.asarray(c).size) for c in cols]
+    parts = [np.asarray(head, np.int64)] + [np.asarray(c, np.int64).ravel() for c in cols] + [padded.view(np.int64)]
+    return np.concatenate(parts)
+
+
+def _unpack_rows(msg):
+    """Inverse of _pack_rows: (list of int64 columns, uint8 blob)."""
+    msg = np.ascontiguousarray(msg, np.int64)
+    k, nb = int(msg[0]), int(msg[1])
+    sizes = [int(x) for x in msg[2:2 + k]]
+    at = 2 + k
+    cols = []
+    for m in sizes:
+        cols.append(msg[at:at + m])
+        at += m
+    return cols, msg[at:].view(np.uint8)[:nb]
 
 
 def depths():
@@ -383,30 +407,35 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
 
     # 2. splitters (misc.hpp:531-587)
     pos = sample_positions(sizes_local, p, factor)
-    flat = np.array([pb[q] + i for q in range(p_local) for i in pos[q]], np.int64)
-    gidx = np.array([pe_goff[q_first + q] + i for q in range(p_local) for i in pos[q]], np.int64)
+    if p_local:
+        flat = np.concatenate([pb[q] + pos[q] for q in range(p_local)])
+        gidx = np.concatenate([pe_goff[q_first + q] + pos[q] for q in range(p_local)])
+    else:
+        flat = gidx = np.zeros(0, np.int64)
     ids = be.take(order, flat) if flat.size else np.zeros(0, np.int64)
     tr = be.take(dp, flat) if flat.size else np.zeros(0, np.int64)
     schars, soffs, slens, sbytes = be.pack(strings, ids, tr)
-    all_chars = comm.allgather_np(np.asarray(be.chars_to_host(schars, sbytes), np.int64))
-    all_lens = comm.allgather_np(slens)
-    all_offs = comm.allgather_np(soffs)
-    all_gidx = comm.allgather_np(gidx)
-    base, offs = 0, []
-    for c, o in zip(all_chars, all_offs):
-        offs.append(o + base)
-        base += c.size
-    gchars = np.concatenate(all_chars).astype(np.uint8)
+    # every rank's (lengths, offsets, global indices, bytes) in one all-gather
+    msg = _pack_rows(slens, soffs, gidx, blob=np.asarray(be.chars_to_host(schars, sbytes), np.uint8))
+    base, offs, lens_l, gidx_l, chars_l = 0, [], [], [], []
+    for part in comm.allgather_np(msg):
+        (ln, of, gi), cb = _unpack_rows(part)
+        lens_l.append(ln)
+        offs.append(of + base)
+        gidx_l.append(gi)
+        chars_l.append(cb)
+        base += cb.size
+    gchars = np.concatenate(chars_l) if chars_l else np.zeros(0, np.uint8)
     goffs = np.concatenate(offs)
-    glens = np.concatenate(all_lens)
-    ggidx = np.concatenate(all_gidx)
+    glens = np.concatenate(lens_l)
+    ggidx = np.concatenate(gidx_l)
     S = int(glens.size)
     sample = be.arena_from(be.chars_from_host(gchars), goffs, glens, gchars.size)
     nspl = min(p - 1, S)
     if nspl:
-        sorted_ids = be.sort_arena(sample)
+        sorted_ids = np.asarray(be.sort_arena(sample), np.int64)
         step = S // (nspl + 1)
-        spl_ids = np.array([sorted_ids[k * step] for k in range(1, nspl + 1)], np.int64)
+        spl_ids = sorted_ids[np.arange(1, nspl + 1, dtype=np.int64) * step]
     else:
         spl_ids = np.zeros(0, np.int64)
     pchars, poffs, plens, pbytes = be.pack(sample, spl_ids, None)

@@ -79,3 +79,29 @@ def test_three_ranks_one_pe_each(orc):
     pb = [0, n // 3, (2 * n) // 3, n]
     res = run_ranks(3, (strs, pb, [0, 1, 2, 3], 0), "oracle")
     check_against_oracle(orc, strs, pb, res, 0)
+
+
+def test_pack_rows_round_trip(dsss):
+    """The one-message packing of the sample all-gather: columns of any
+    length (empty too) and a byte blob of any length come back unchanged."""
+    from dsss_b200 import dist
+    rng = np.random.default_rng(3)
+    for ncols, nb in ((3, 0), (3, 1), (3, 13), (1, 64), (0, 5)):
+        cols = [rng.integers(-2**40, 2**40, size=int(rng.integers(0, 9)), dtype=np.int64) for _ in range(ncols)]
+        if ncols:
+            cols[0] = np.zeros(0, np.int64)
+        blob = rng.integers(0, 256, size=nb, dtype=np.uint8)
+        got, gb = dist._unpack_rows(dist._pack_rows(*cols, blob=blob))
+        assert len(got) == ncols
+        for a, b in zip(cols, got):
+            assert np.array_equal(a, b)
+        assert np.array_equal(gb, blob)
+
+
+def test_sample_positions_match_reference_rule(dsss):
+    """floor(i * (n_q / (nr + 1))) in double arithmetic for i = 1..nr."""
+    from dsss_b200 import dist
+    for nq, p in ((0, 4), (1, 4), (5, 4), (1000, 64), (999_999, 64), (7, 2)):
+        nr = min(2 * (p - 1), nq)
+        want = [int(float(i) * (float(nq) / float(nr + 1))) for i in range(1, nr + 1)]
+        assert dist.sample_positions([nq], p)[0].tolist() == want
