@@ -7,10 +7,15 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   value     strings/s with the input resident in HBM (device-timed, max over ranks)
   e2e       the same metric through dsss_pd_sort_host: pinned host input copied
             in, results copied out, inside the timed region
-  roofline  the string sort (K3, the dominant stage) against HBM: algorithmic
-            bytes D + 20 n (D = sum of DP lengths: each distinguishing byte read
-            once, 8 B id read + 8 B id write + 4 B LCP write per string) over the
-            summed CUDA-event durations of its launches
+  roofline  the dominant kernel, k_dp_hash (the distinguishing-prefix hash
+            rounds), against HBM: algorithmic bytes d + 16 for every string
+            hashed at its final depth d (its prefix read once, the 8-byte hash
+            written and read; roots hashed in earlier rounds are not counted,
+            so this is a lower bound) over the summed CUDA-event durations of
+            its launches; traffic = DRAM bytes per hashed string from one ncu
+            capture (profiles/k_dp_hash_dn8m.md) times the strings hashed
+  roofline_sort  the string sort stage (K3) the same way: D + 20 n (D = sum of
+            DP lengths, 8 B id read + 8 B id write + 4 B LCP write per string)
   cpu_baseline  the oracle port of the reference path on the host
 
 --impl reference times the CPU port of the reference path (oracle/) on all
@@ -41,6 +46,12 @@ CONFIGS = {
     "dn8m": (8_000_000, 200, 50, 64, "8e6 strings x 200 B, D/N 0.25, p = 64 PEs (profiling size)"),
     "dn100m": (100_000_000, 100, 50, 64, "1e8 strings x 100 B, D/N 0.5, p = 64 PEs"),
 }
+
+
+# DRAM bytes (read + write) per hashed string of k_dp_hash's dense round, from
+# one ncu capture on 8e6 strings x 200 B (profiles/k_dp_hash_dn8m.md); the
+# traffic grows with the strings hashed.
+DP_HASH_DRAM_PER_STRING = 316.6
 
 
 def read_peaks():
@@ -422,6 +433,13 @@ def main():
     algo_bytes = D + 20 * n
     peak, peak_kind = read_peaks()
     achieved = algo_bytes / (sort_ms * 1e-3) / 1e9
+    # the hash rounds: strings hashed at their final depth (dp on the depth schedule)
+    sched = np.array([8] + [8 + (16 << j) for j in range(26)], np.uint64)
+    hashed_final = np.isin(dp, sched)
+    hash_bytes = int(dp[hashed_final].sum()) + 16 * int(hashed_final.sum())
+    hash_ms = kernels["k_dp_hash"][1] / args.steps if "k_dp_hash" in kernels else float("nan")
+    hash_launches = kernels["k_dp_hash"][0] / args.steps if "k_dp_hash" in kernels else 0
+    hash_achieved = hash_bytes / (hash_ms * 1e-3) / 1e9
     char_bytes = int(hs.lengths.astype(np.uint64).sum()) + n
     value = n * world / (ms * 1e-3)
 
@@ -476,10 +494,19 @@ def main():
                        "parallelism": "one GPU holds all p PEs" if world == 1 else
                        f"{world} ranks, one instance each (weak)"},
             "char_gbs": char_bytes / (ms * 1e-3) / 1e9 * world,
-            "roofline": {"bound": "hbm", "kernel": "string sort K3 (all launches of the sort stage)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": None, "algo_bytes": algo_bytes,
-                         "algo_formula": "D + 20 n", "sort_ms": sort_ms, "sort_launches": sort_launches},
+            "roofline": {"bound": "hbm", "kernel": "k_dp_hash (all launches of one step)",
+                         "achieved": hash_achieved, "peak": peak, "unit": "GB/s", "frac": hash_achieved / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": DP_HASH_DRAM_PER_STRING * int(hashed_final.sum()),
+                         "traffic_note": "ncu dram bytes read+write per hashed string of the dense round on 8e6 "
+                                         "strings (profiles/k_dp_hash_dn8m.md), times the strings hashed",
+                         "algo_bytes": hash_bytes,
+                         "algo_formula": "sum over strings hashed at their final depth d of (d + 16); lower bound",
+                         "kernel_ms": hash_ms, "launches": hash_launches},
+            "roofline_sort": {"bound": "hbm", "kernel": "string sort K3 (all launches of the sort stage)",
+                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                              "peak_kind": peak_kind, "traffic": None, "algo_bytes": algo_bytes,
+                              "algo_formula": "D + 20 n", "sort_ms": sort_ms, "sort_launches": sort_launches},
             "tuning": tuning,
             "stages_ms": stages,
             "kernels_ms": {k2: round(v[1] / args.steps, 4) for k2, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
