@@ -44,6 +44,10 @@ struct Seg {
     uint32_t newdepth;
     uint32_t first_digit;
     unsigned long long diff;
+    // speculated common-prefix depth + 1 (0: none) and the OR of key ^ key0
+    // over the keys k_prefix wrote at that depth (segments without keys)
+    uint32_t spec, spec_pad;
+    unsigned long long spec_diff;
 };
 
 constexpr int NBINS = 4;
@@ -101,6 +105,9 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
     s.newdepth = 0xFFFFFFFFu;
     s.first_digit = 0;
     s.diff = 0;
+    s.spec = 0;
+    s.spec_pad = 0;
+    s.spec_diff = 0;
     S.small[b][slot] = s;
 }
 
@@ -119,6 +126,9 @@ __device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_
     s.newdepth = 0xFFFFFFFFu;
     s.first_digit = 0;
     s.diff = 0;
+    s.spec = 0;
+    s.spec_pad = 0;
+    s.spec_diff = 0;
     dst[slot] = s;
 }
 
@@ -182,6 +192,53 @@ __device__ __forceinline__ void key_words(const uint8_t* chars, uint64_t off, ui
 }
 
 constexpr int PF_W = 8;  // prefix words compared per batch (64 bytes)
+constexpr uint32_t SPEC_MAX = 56;  // speculated depths stay below d0 + 56 (key inside 64 bytes)
+
+// Speculated common prefix of each segment without keys: the smallest LCP with
+// the segment's first string over up to 256 evenly spaced members, when it is
+// below d0 + SPEC_MAX.  k_prefix then reads each string once for both the
+// check (the segment's common prefix is exactly that depth iff no member
+// leaves the first string earlier) and the key at that depth; a wrong guess
+// only costs the usual key gather of k_keys_diff.  Segments whose samples all
+// share SPEC_MAX bytes keep the plain prefix search (long common prefixes).
+__global__ void __launch_bounds__(256) k_spec(SortState S, Seg* segs, uint32_t nseg) {
+    __shared__ uint32_t wmin[8];
+    for (uint32_t si = blockIdx.x; si < nseg; si += gridDim.x) {
+        Seg& sg = segs[si];
+        if (sg.flags & (F_KEYS | F_PIVOT)) continue;  // the same for the whole block
+        const uint32_t* ord = S.ord[sg.flags & F_PARITY];
+        const uint32_t d0 = sg.depth;
+        uint32_t l = 0xFFFFFFFFu;
+        const uint32_t m = sg.size < 256u ? sg.size : 256u;
+        if (threadIdx.x < m) {
+            uint64_t off0, off;
+            uint32_t len0, len;
+            str_of(S.a, ord[sg.start], off0, len0);
+            const uint32_t i = sg.start + (uint32_t)((uint64_t)threadIdx.x * sg.size / m);
+            str_of(S.a, ord[i], off, len);
+            uint64_t x[7], y[7];
+            key_words<7>(S.a.chars, off, len, d0, 7, x);
+            key_words<7>(S.a.chars, off0, len0, d0, 7, y);
+            l = d0 + SPEC_MAX;
+#pragma unroll
+            for (int w = 6; w >= 0; --w) {  // the first word that differs or ends wins
+                if (x[w] != y[w]) l = d0 + 8 * w + key_lcp(x[w], y[w]);
+                else if (zero_byte(x[w]) < 8) l = d0 + 8 * w + zero_byte(x[w]);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) l = min(l, __shfl_xor_sync(0xffffffffu, l, o));
+        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = l;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t v = wmin[0];
+            for (int w = 1; w < 8; ++w) v = min(v, wmin[w]);
+            sg.spec = v < d0 + SPEC_MAX ? v + 1 : 0u;
+            sg.spec_diff = 0;
+        }
+        __syncthreads();
+    }
+}
 
 __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
@@ -211,6 +268,52 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
         for (int w = 0; w < PF_W; ++w) y[w] = v[w];
     }
     __syncthreads();
+    if (sg.spec) {
+        // speculated depth D: LCP with the first string capped at D, and the
+        // key at D, from one load of the words covering [d0, D + 8)
+        const uint32_t D = sg.spec - 1, rel = D - d0;
+        const uint32_t want = (rel + 15) >> 3;
+        const uint32_t kw = rel >> 3, kr = (rel & 7) * 8;
+        const uint64_t key0 = kr ? (y[kw] << kr) | (y[kw + 1] >> (64 - kr)) : y[kw];
+        unsigned long long* key = S.key[par];
+        uint32_t mn = 0xFFFFFFFFu;
+        uint64_t df = 0;
+        for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
+            uint64_t off;
+            uint32_t len;
+            str_of(S.a, ord[i], off, len);
+            uint64_t x[PF_W];
+            key_words<PF_W>(S.a.chars, off, len, d0, want, x);
+            uint32_t l = D;
+#pragma unroll
+            for (int w = PF_W - 1; w >= 0; --w) {  // the first word that differs or ends wins
+                if ((uint32_t)(8 * w) < rel) {
+                    if (x[w] != y[w]) l = min(D, d0 + 8 * w + key_lcp(x[w], y[w]));
+                    else if (zero_byte(x[w]) < 8) l = min(D, d0 + 8 * w + zero_byte(x[w]));
+                }
+            }
+            uint64_t lo = 0, hi = 0;  // words kw and kw + 1, selected without indexing x at run time
+#pragma unroll
+            for (int w = 0; w < PF_W; ++w) {
+                if ((uint32_t)w == kw) lo = x[w];
+                if ((uint32_t)w == kw + 1) hi = x[w];
+            }
+            const uint64_t k = kr ? (lo << kr) | (hi >> (64 - kr)) : lo;
+            key[i] = k;
+            df |= k ^ key0;
+            mn = min(mn, l);
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            df |= __shfl_xor_sync(0xffffffffu, df, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (mn != 0xFFFFFFFFu) atomicMin(&sg.newdepth, mn);
+            if (df) atomicOr(&sg.spec_diff, (unsigned long long)df);
+        }
+        return;
+    }
     uint32_t mn = 0xFFFFFFFFu;
     for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
         uint64_t off;
@@ -295,6 +398,11 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
     const uint32_t si = find_seg(S.tile0, nseg, t);
     Seg& sg = segs[si];
     if (sg.flags & F_PIVOT) return;  // keys and diff come from k_pivot
+    if (!(sg.flags & F_KEYS) && sg.spec && sg.newdepth == sg.spec - 1) {
+        // the speculated depth was the common prefix: k_prefix wrote the keys
+        if (t == S.tile0[si] && threadIdx.x == 0) sg.diff = sg.spec_diff;
+        return;
+    }
     const uint32_t par = sg.flags & F_PARITY;
     const bool valid = sg.flags & F_KEYS;
     const uint32_t depth = valid ? sg.depth : sg.newdepth;
@@ -1639,6 +1747,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         uint64_t max_tiles = std::min<uint64_t>(L.cap_tiles, n / LT_TILE + nlarge + 1);
         uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
         S.large[0] = segs;
+        DSSS_LAUNCH("k_spec", st, k_spec<<<std::min<uint32_t>(nlarge, 148 * 16), 256, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_pivot", st, k_pivot<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));

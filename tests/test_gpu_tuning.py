@@ -112,3 +112,26 @@ def test_sort_host_loop_and_graph(dsss, orc, ctx, name, strs, graph):
     ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
     assert np.array_equal(u64(order, n), ro)
     assert np.array_equal(u64(lcp, n), rl)
+
+
+@pytest.mark.parametrize("early", [None, 1, 4999])
+def test_prefix_speculation(dsss, orc, ctx, early):
+    """The string sort guesses a segment's common prefix from 256 evenly
+    spaced members and writes the keys at that depth in the same pass; the
+    guess holds (early=None) or one member that the sample misses leaves the
+    shared head early (positions 1 and 4999 of 10000), and the sort falls back
+    to the exact depth.  Order and LCPs equal the oracle's either way."""
+    rng = np.random.default_rng(11)
+    head = b"XY" * 10
+    strs = [head + bytes(rng.integers(65, 91, size=int(rng.integers(0, 30)), dtype=np.uint8)) for _ in range(10000)]
+    if early is not None:
+        strs[early] = head[:5] + b"A" + strs[early][6:]
+    hs = host_of(dsss, strs)
+    n = hs.n
+    for p in (1, 3):
+        pb = np.linspace(0, n, p + 1).astype(np.uint64)
+        for small in (0, 64):  # 64: every segment above 64 strings takes the MSD passes
+            order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), p, part_begin=pb, small_sort_max=small)
+            ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
+            assert np.array_equal(u64(order, n), ro)
+            assert np.array_equal(u64(lcp, n), rl)
