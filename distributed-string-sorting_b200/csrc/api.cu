@@ -58,23 +58,43 @@ __global__ void k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uin
 
 // Receiving PE of every string: set s's PE q sends local positions
 // [bounds[(s*p+q)*(p+1) + r], … + r + 1) to the set's PE r; buckets are
-// numbered s*p + r.  pe_local (optional) receives q.
-__global__ void k_bucket_of(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p, uint64_t n,
-                            uint32_t* bucket, uint32_t* pe_local) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const uint32_t src = pe[g];
+// numbered s*p + r; src receives q's global PE number.
+__device__ __forceinline__ uint32_t bucket_at(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds,
+                                              uint32_t p, uint64_t g, uint32_t& src) {
+    src = pe[g];
     const uint64_t* b = bounds + (uint64_t)src * (p + 1);
     const uint64_t li = g2l[g];
-    uint32_t lo = 0, hi = p;  // last r with b[r] <= li (b[0] = 0, b[p] = n_q > li)
+    uint32_t lo = 0, hi = p;  // last r with b[r] <= li
     while (hi - lo > 1) {
         uint32_t mid = (lo + hi) >> 1;
         if (b[mid] <= li) lo = mid;
         else hi = mid;
     }
-    const uint32_t set = src / p;
-    bucket[g] = set * p + lo;
-    if (pe_local) pe_local[g] = src - set * p;
+    return (src / p) * p + lo;
+}
+
+// k_bucket_of plus, for the common case, the merged sequences themselves: when
+// the buckets never decrease along the global order (no equal strings that two
+// PEs cut on different sides of a splitter), the stable partition by bucket
+// is the identity, so position g of the merged sequences is global position g:
+// its (local index, sender PE) and, unless it starts a receiving PE's run, the
+// global LCP.  *viol is set when some bucket decreases; the caller then runs
+// the multisplit, which rewrites every output.
+__global__ void k_bucket_direct(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p,
+                                uint64_t n, int local_pe, const uint32_t* lcpg, uint32_t* bucket, uint32_t* pe_local,
+                                uint32_t* perm_index, uint32_t* perm_pe, uint32_t* merged, uint32_t* viol) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    uint32_t src, srcp;
+    const uint32_t b = bucket_at(pe, g2l, bounds, p, g, src);
+    const uint32_t bp = g ? bucket_at(pe, g2l, bounds, p, g - 1, srcp) : 0xFFFFFFFFu;
+    if (g && bp > b) atomicExch(viol, 1u);
+    const uint32_t ql = src - (src / p) * p;
+    bucket[g] = b;
+    if (pe_local) pe_local[g] = ql;
+    perm_index[g] = g2l[g];
+    perm_pe[g] = local_pe ? ql : src;
+    if (merged) merged[g] = (g == 0 || bp != b) ? 0u : lcpg[g];
 }
 
 __global__ void k_merged_lcp(const uint32_t* out2g, const uint32_t* lcpg, const uint64_t* recv_begin, uint32_t p,
@@ -104,7 +124,7 @@ __global__ void k_zero_starts(uint32_t* a, const uint64_t* pb, uint32_t p) {
 
 struct PdLayout {
     ulonglong2* handles;
-    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *out2g, *pel, *nlong, *err;
+    uint32_t *ord, *lcp, *dpg, *pe, *g2l, *tmp, *out2g, *pel, *nlong, *err, *viol;
     uint64_t *pb, *bounds, *recv_begin;
     void* ms;
     SortLayout sort;
@@ -128,6 +148,7 @@ static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t nsets, uint32_
     L.pel = nsets > 1 ? c.take<uint32_t>(N) : nullptr;
     L.nlong = c.take<uint32_t>(1);
     L.err = c.take<uint32_t>(1);
+    L.viol = c.take<uint32_t>(1);
     L.pb = c.take<uint64_t>(npe + 1);
     L.bounds = c.take<uint64_t>(npe * (p + 1));
     L.recv_begin = c.take<uint64_t>(npe + 1);
@@ -236,15 +257,24 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     }
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (npe + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_bucket_of", st, k_bucket_of<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, L.tmp, L.pel));
-    {
+    DSSS_CUDA(cudaMemsetAsync(L.viol, 0, sizeof(uint32_t), st));
+    DSSS_LAUNCH("k_bucket_direct", st,
+                k_bucket_direct<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, nsets > 1, L.lcp, L.tmp,
+                                                                 L.pel, out->perm_index, out->perm_pe,
+                                                                 out->merged_lcp, L.viol));
+    pin = (uint32_t*)ctx->pin;  // the partition step may have grown the staging buffer
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.viol, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[0]) {
         // merged sequences: (index in sender's local order, sender PE, global position)
         const uint32_t* in[3] = {L.g2l, nsets > 1 ? L.pel : L.pe, nullptr};
         uint32_t* outs[3] = {out->perm_index, out->perm_pe, L.out2g};
         DSSS_TRY(multisplit_payload(L.tmp, n, npe, 3, in, outs, nullptr, L.err, L.ms, st));
+        if (out->merged_lcp)
+            DSSS_LAUNCH("k_merged_lcp", st,
+                        k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, npe, n,
+                                                                      out->merged_lcp));
     }
-    if (out->merged_lcp)
-        DSSS_LAUNCH("k_merged_lcp", st, k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, npe, n, out->merged_lcp));
     if (want_local_lcp) {
         DSSS_TRY(adjacent_lcp(a, out->local_order, n, out->local_lcp, L.tmp, L.nlong, st));
         DSSS_LAUNCH("k_zero_starts", st, k_zero_starts<<<grid_for(npe, 128), 128, 0, st>>>(out->local_lcp, L.pb, npe));

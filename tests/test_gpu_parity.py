@@ -239,3 +239,26 @@ def test_budget_enomem(dsss):
         dsss.pd_sort(small, dsss.DeviceStrings(hs), 4)
     assert e.value.code == -12
     small.close()
+
+
+@pytest.mark.parametrize("kind", ["distinct", "ties"])
+def test_merged_sequences_direct_and_multisplit(dsss, orc, ctx, kind):
+    """When every bucket follows the previous one along the global order, the
+    merged sequences are written directly (one multisplit per call, the one by
+    PE); equal strings that PEs cut on different sides of a splitter force the
+    stable multisplit by bucket (two per call).  The oracle's full path either
+    way."""
+    rng = np.random.default_rng(21)
+    if kind == "distinct":
+        strs = [bytes(rng.integers(65, 91, size=12, dtype=np.uint8)) for _ in range(6000)]
+    else:
+        strs = [b"SAME" if rng.random() < 0.6 else bytes(rng.integers(65, 68, size=3, dtype=np.uint8))
+                for _ in range(6000)]
+    hs = host_of(dsss, strs)
+    p = 8
+    ctx.set_timing(True)
+    out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), p)
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    assert kt["k_ms_scatter_pay"][0] == (1 if kind == "distinct" else 2)
+    check_pd(dsss, orc, hs, out, p)
