@@ -36,15 +36,38 @@ constexpr unsigned FULLM = 0xffffffffu;
 
 // Length and char offset of every sorted position, gathered once per call so
 // that the hash rounds read them in order.
+// Four independent gathers in flight per thread (positions i, i + T, i + 2T,
+// i + 3T for T threads in the grid).
+constexpr int LENS_ILP = 4;
 __global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_t* lens, uint64_t* soff) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint64_t off;
-    uint32_t len;
-    str_of(a, order[i], off, len);
-    lens[i] = len;
-    soff[i] = off;
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t s[LENS_ILP];
+#pragma unroll
+    for (int q = 0; q < LENS_ILP; ++q) {
+        const uint64_t i = i0 + q * T;
+        s[q] = i < n ? order[i] : 0u;
+    }
+    uint64_t off[LENS_ILP];
+    uint32_t len[LENS_ILP];
+#pragma unroll
+    for (int q = 0; q < LENS_ILP; ++q) {
+        const uint64_t i = i0 + q * T;
+        off[q] = 0;
+        len[q] = 0;
+        if (i < n) str_of(a, s[q], off[q], len[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < LENS_ILP; ++q) {
+        const uint64_t i = i0 + q * T;
+        if (i < n) {
+            lens[i] = len[q];
+            soff[i] = off[q];
+        }
+    }
 }
+
+static unsigned lens_grid(uint64_t n) { return grid_for((n + LENS_ILP - 1) / LENS_ILP, 256); }
 
 // Index of the string set holding sorted position i (set_begin: nsets+1 bounds).
 __device__ __forceinline__ uint32_t set_of(const uint64_t* set_begin, uint32_t nsets, uint64_t i) {
@@ -137,6 +160,105 @@ __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all,
     block_add(counters + 0, nhashed);
     block_add(counters + 1, nstays);
 }
+
+// k_dp_classify for one string set over 16-byte-aligned arrays: four
+// consecutive positions per thread, read and written as vectors (the same
+// per-position rule; st of the neighbours i - 1 and i + 4 read singly).
+__global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all, const uint32_t* lens,
+                                                      const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
+                                                      uint8_t* st_next, uint8_t* kind, uint32_t* counters) {
+    uint32_t nhashed = 0, nstays = 0;
+    const uint64_t groups = n >> 2;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += stride) {
+        const uint64_t i0 = t * 4;
+        const uint4 L4 = reinterpret_cast<const uint4*>(lens)[t];
+        const uint4 C4 = reinterpret_cast<const uint4*>(lcp)[t];
+        const uint32_t Ls[4] = {L4.x, L4.y, L4.z, L4.w};
+        const uint32_t Cs[5] = {C4.x, C4.y, C4.z, C4.w, i0 + 4 < n ? lcp[i0 + 4] : 0u};
+        uint8_t S[6];  // st[i0 - 1 .. i0 + 4]
+        if (all) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) S[q] = 1;
+        } else {
+            const uchar4 s4 = reinterpret_cast<const uchar4*>(st)[t];
+            S[0] = i0 > 0 ? st[i0 - 1] : 0;
+            S[1] = s4.x;
+            S[2] = s4.y;
+            S[3] = s4.z;
+            S[4] = s4.w;
+            S[5] = i0 + 4 < n ? st[i0 + 4] : 0;
+        }
+        uint32_t D[4];
+        uint8_t K[4], X[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t i = i0 + q;
+            uint8_t k = 0, nx = 0;
+            D[q] = 0xFFFFFFFFu;  // untouched
+            if (S[q + 1]) {
+                const uint32_t L = Ls[q];
+                if (depth > L) {
+                    D[q] = L;
+                } else {
+                    D[q] = depth;
+                    if (i > 0 && S[q] && Cs[q] >= depth) {
+                        k = 1;
+                        nx = 1;
+                    } else {
+                        const bool root = i + 1 < n && S[q + 2] && Cs[q + 1] >= depth;
+                        k = root ? 3 : 2;
+                        nx = root ? 1 : 0;
+                        ++nhashed;
+                    }
+                }
+            }
+            K[q] = k;
+            X[q] = nx;
+            nstays += nx;
+        }
+        if (all) {
+            reinterpret_cast<uint4*>(dp)[t] = make_uint4(D[0], D[1], D[2], D[3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (D[q] != 0xFFFFFFFFu) dp[i0 + q] = D[q];
+        }
+        reinterpret_cast<uchar4*>(kind)[t] = make_uchar4(K[0], K[1], K[2], K[3]);
+        reinterpret_cast<uchar4*>(st_next)[t] = make_uchar4(X[0], X[1], X[2], X[3]);
+    }
+    // the last n % 4 positions, one thread each
+    const uint64_t tail = groups * 4;
+    const uint64_t tt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tt < n - tail) {
+        const uint64_t i = tail + tt;
+        uint8_t k = 0, nx = 0;
+        if (all || st[i]) {
+            const uint32_t L = lens[i];
+            if (depth > L) {
+                dp[i] = L;
+            } else {
+                dp[i] = depth;
+                if (i > 0 && (all || st[i - 1]) && lcp[i] >= depth) {
+                    k = 1;
+                    nx = 1;
+                } else {
+                    const bool root = i + 1 < n && (all || st[i + 1]) && lcp[i + 1] >= depth;
+                    k = root ? 3 : 2;
+                    nx = root ? 1 : 0;
+                    ++nhashed;
+                }
+            }
+        }
+        kind[i] = k;
+        st_next[i] = nx;
+        nstays += nx;
+    }
+    block_add(counters + 0, nhashed);
+    block_add(counters + 1, nstays);
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 // Inserts h into the table region (base, mask) by linear probing; returns its
 // slot, NO_SLOT when the region is full.  The table always has free slots, so
@@ -482,7 +604,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                   cudaMemcpyHostToDevice, st));
     }
     const unsigned grid = grid_for(n, 256);
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<lens_grid(n), 256, 0, st>>>(a, order, n, L.lens, L.soff));
     int cur = 0;
     const uint64_t start = 8;
     uint64_t depth = start;
@@ -490,10 +612,18 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
         DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
         if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
-        DSSS_LAUNCH("k_dp_classify", st,
-                    k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth, dp,
-                                                       L.st[cur ^ 1], L.kind, L.counters, L.set_begin, nsets,
-                                                       L.set_cnt));
+        if (nsets == 1 && aligned16(lcp) && aligned16(dp) && aligned16(L.lens) && aligned16(L.st[cur]) &&
+            aligned16(L.st[cur ^ 1]) && aligned16(L.kind)) {
+            DSSS_LAUNCH("k_dp_classify", st,
+                        k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n,
+                                                                                (uint32_t)depth, dp, L.st[cur ^ 1],
+                                                                                L.kind, L.counters));
+        } else {
+            DSSS_LAUNCH("k_dp_classify", st,
+                        k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth,
+                                                                     dp, L.st[cur ^ 1], L.kind, L.counters,
+                                                                     L.set_begin, nsets, L.set_cnt));
+        }
         if (nsets > 1) {
             DSSS_LAUNCH("k_set_tables", st,
                         k_set_tables<<<1, SET_NT, 0, st>>>(L.set_cnt, nsets, L.slots, 0, L.set_base, L.set_mask,
@@ -622,7 +752,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
     *m_next = 0;
     if (n == 0) return DSSS_OK;
     const unsigned grid = grid_for(n, 256);
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<lens_grid(n), 256, 0, st>>>(a, order, n, L.lens, L.soff));
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
     const bool all = cand == nullptr;
     if (!all) {
@@ -703,7 +833,7 @@ int dp_classify_hash(const DpSplitLayout& L, const ArenaDev& a, uint64_t n, cons
     if (n == 0) return DSSS_OK;
     const unsigned grid = grid_for(n, 256);
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<grid, 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<lens_grid(n), 256, 0, st>>>(a, order, n, L.lens, L.soff));
     DSSS_LAUNCH("k_dp_classify", st,
                 k_dp_classify<<<stride_grid(n), 256, 0, st>>>(state_in, state_in == nullptr, L.lens, lcp, n, depth, dp, state_out,
                                                    L.kind, L.counters, nullptr, 1, nullptr));
