@@ -90,7 +90,7 @@ void make_handles(const ArenaDev& a, ulonglong2* h, cudaStream_t st) {
 // buckets < b) + (elements of bucket b before i).  Histograms are stored
 // bucket-major per tile, so one flat exclusive scan yields every tile's
 // starting offset per bucket.
-constexpr int MS_NT = 256, MS_IPT = 16, MS_TILE = MS_NT * MS_IPT;
+constexpr int MS_NT = 256, MS_IPT = 8, MS_TILE = MS_NT * MS_IPT;
 
 __global__ void __launch_bounds__(MS_NT) k_ms_hist(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles,
                                                   uint32_t* hist) {
@@ -171,7 +171,7 @@ constexpr size_t msp_smem(uint32_t P) {
 }
 
 template <int NPAY>
-__global__ void __launch_bounds__(MS_NT) k_ms_scatter_pay(const uint32_t* bucket, uint64_t n, uint32_t P,
+__global__ void __launch_bounds__(MS_NT, 4) k_ms_scatter_pay(const uint32_t* bucket, uint64_t n, uint32_t P,
                                                          uint64_t tiles, const uint32_t* off, Payload pl,
                                                          uint32_t* rank_out, uint32_t* err) {
     extern __shared__ __align__(16) uint32_t smp[];
@@ -193,7 +193,15 @@ __global__ void __launch_bounds__(MS_NT) k_ms_scatter_pay(const uint32_t* bucket
     const uint64_t tb = (uint64_t)blockIdx.x * MS_TILE;
     const uint32_t tn = (uint32_t)min((uint64_t)MS_TILE, n - tb);
     const uint64_t wb = tb + (uint64_t)w * 32 * MS_IPT;
-    uint32_t rk[MS_IPT], bk[MS_IPT];
+    // the payloads are loaded with the buckets, so that a tile waits for
+    // DRAM once rather than once before and once after the ranking
+    uint32_t rk[MS_IPT], bk[MS_IPT], pv[NPAY][MS_IPT];
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        const uint64_t i = wb + j * 32 + lane;
+#pragma unroll
+        for (int k = 0; k < NPAY; ++k) pv[k][j] = i < n ? (pl.in[k] ? pl.in[k][i] : (uint32_t)i) : 0u;
+    }
 #pragma unroll
     for (int j = 0; j < MS_IPT; ++j) {
         const uint64_t i = wb + j * 32 + lane;
@@ -251,7 +259,7 @@ __global__ void __launch_bounds__(MS_NT) k_ms_scatter_pay(const uint32_t* bucket
             continue;
         }
 #pragma unroll
-        for (int k = 0; k < NPAY; ++k) spay[k * MS_TILE + lp] = pl.in[k] ? pl.in[k][i] : (uint32_t)i;
+        for (int k = 0; k < NPAY; ++k) spay[k * MS_TILE + lp] = pv[k][j];
         sbk[lp] = (uint16_t)d;
         if (rank_out) rank_out[i] = base[d] + wcnt[w * P + d] + rk[j] - b0[d];
     }
