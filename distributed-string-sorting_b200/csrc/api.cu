@@ -84,10 +84,16 @@ __global__ void k_bucket_direct(const uint32_t* pe, const uint32_t* g2l, const u
                                 uint64_t n, int local_pe, const uint32_t* lcpg, uint32_t* bucket, uint32_t* pe_local,
                                 uint32_t* perm_index, uint32_t* perm_pe, uint32_t* merged, uint32_t* viol) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    uint32_t src, srcp;
-    const uint32_t b = bucket_at(pe, g2l, bounds, p, g, src);
-    const uint32_t bp = g ? bucket_at(pe, g2l, bounds, p, g - 1, srcp) : 0xFFFFFFFFu;
+    const bool valid = g < n;
+    uint32_t src = 0, b = 0xFFFFFFFFu;
+    if (valid) b = bucket_at(pe, g2l, bounds, p, g, src);
+    // the previous position's bucket: from the lane below, or searched by lane 0
+    uint32_t bp = __shfl_up_sync(0xffffffffu, b, 1);
+    if ((threadIdx.x & 31) == 0) {
+        uint32_t srcp;
+        bp = valid && g ? bucket_at(pe, g2l, bounds, p, g - 1, srcp) : 0xFFFFFFFFu;
+    }
+    if (!valid) return;
     if (g && bp > b) atomicExch(viol, 1u);
     const uint32_t ql = src - (src / p) * p;
     bucket[g] = b;

@@ -31,7 +31,7 @@
 
 namespace dsss {
 
-constexpr int LT_NT = 256, LT_IPT = 16, LT_TILE = LT_NT * LT_IPT;
+constexpr int LT_NT = 256, LT_IPT = 8, LT_TILE = LT_NT * LT_IPT;
 constexpr int CHUNK_TILES = 32;
 constexpr uint32_t PREFIX_CAP = 256;
 // F_KEYS: the key array holds the segment's keys at Seg.depth; F_PIVOT: the
@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
 // digit's run are contiguous.
 constexpr size_t SCATTER_SMEM = (size_t)LT_TILE * (8 + 4 + 1);
 
-__global__ void __launch_bounds__(LT_NT) k_scatter(SortState S, const Seg* segs, uint32_t nseg) {
+__global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
         segs = S.large[S.counters[12]];
         nseg = S.counters[13];
