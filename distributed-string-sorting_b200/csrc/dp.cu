@@ -301,6 +301,47 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* 
     slot[i] = table_insert(tkeys, tdup, base, mask, h, err);
 }
 
+// k_dp_hash for rounds that hash few positions (e.g. only the roots of long
+// runs of LCP-local duplicates): a few blocks per SM stride over the kind
+// array instead of one thread per position.
+__global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n,
+                                                        uint32_t depth, unsigned long long* tkeys, uint8_t* tdup,
+                                                        uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
+                                                        const uint64_t* set_base, const uint32_t* set_mask,
+                                                        uint32_t* slot, uint32_t* err) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (kind[i] < 2) continue;
+        uint64_t base = 0;
+        uint32_t mask = mask1;
+        if (nsets > 1) {
+            const uint32_t sid = set_of(set_begin, nsets, i);
+            base = set_base[sid];
+            mask = set_mask[sid];
+        }
+        const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+        slot[i] = table_insert(tkeys, tdup, base, mask, h, err);
+    }
+}
+
+// One hash round's launch: the sparse form when fewer than 1/8 of the
+// positions hash.
+static int launch_dp_hash(const ArenaDev& a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
+                          uint64_t hashed, unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1,
+                          const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
+                          const uint32_t* set_mask, uint32_t* slot, uint32_t* err, cudaStream_t st) {
+    if (hashed * 8 < n) {
+        DSSS_LAUNCH("k_dp_hash", st,
+                    k_dp_hash_sparse<<<stride_grid(n), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1,
+                                                                     set_begin, nsets, set_base, set_mask, slot, err));
+    } else {
+        DSSS_LAUNCH("k_dp_hash", st,
+                    k_dp_hash<<<grid_for(n, 256), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1, set_begin,
+                                                               nsets, set_base, set_mask, slot, err));
+    }
+    return DSSS_OK;
+}
+
 // Split form of k_dp_hash (knob dp_split): the hashes first, stored per
 // position, then the table inserts by a kernel of few registers, so that many
 // more inserts are in flight.
@@ -692,10 +733,9 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                                              L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
                                                              L.counters + 2));
             } else {
-                DSSS_LAUNCH("k_dp_hash", st,
-                            k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.tkeys, L.tdup,
-                                                           (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
-                                                           L.set_mask, L.slot, L.counters + 2));
+                DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, (uint32_t)depth, hashed, L.tkeys, L.tdup,
+                                        (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
+                                        L.counters + 2, st));
             }
             DSSS_LAUNCH("k_dp_query", st,
                         k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
@@ -770,9 +810,8 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         const uint64_t slots = table_slots(pin[0]);
         DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-        DSSS_LAUNCH("k_dp_hash", st,
-                    k_dp_hash<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, depth, L.tkeys, L.tdup, (uint32_t)(slots - 1),
-                                                   nullptr, 1, nullptr, nullptr, L.slot, L.counters + 2));
+        DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, depth, pin[0], L.tkeys, L.tdup, (uint32_t)(slots - 1), nullptr,
+                                1, nullptr, nullptr, L.slot, L.counters + 2, st));
         DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
     }
     DSSS_LAUNCH("k_state_flags", st, k_state_flags<<<grid, 256, 0, st>>>(L.st[1], n, R.flag));
