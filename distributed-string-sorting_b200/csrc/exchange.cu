@@ -85,35 +85,31 @@ __global__ void k_sum_u32(const uint32_t* v, uint64_t n, unsigned long long* tot
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(total, s);
 }
 
-// Copies bytes [lcp, lcp + cnt - 1) of each source string and a NUL.  Strings
-// up to 64 bytes: one thread; longer: one warp (queued).
-constexpr uint32_t COPY_THREAD_MAX = 64;
-
-__device__ __forceinline__ void copy_bytes(uint8_t* dst, const uint8_t* src, uint32_t m) {
-    uint32_t k = 0;
-    for (; k + 8 <= m; k += 8) {
-        uint64_t w = load_le8(src + k);
-#pragma unroll
-        for (int b = 0; b < 8; ++b) dst[k + b] = (uint8_t)(w >> (8 * b));
-    }
-    for (; k < m; ++k) dst[k] = src[k];
-}
+// Copies bytes [lcp, lcp + cnt - 1) of each source string and a NUL.  Up to
+// COPY_GROUP_MAX bytes: a group of COPY_LANES lanes per string, so that one
+// warp instruction stores COPY_LANES consecutive bytes of each of 32 /
+// COPY_LANES strings instead of one byte of each of 32; longer strings: one
+// warp each (queued).
+constexpr uint32_t COPY_LANES = 8, COPY_GROUP_MAX = 256;
 
 __global__ void k_recv_copy(ArenaDev a, uint64_t n, const uint32_t* cnt, const uint32_t* cstart, const uint32_t* rlcp,
                             const uint32_t* rsrc, uint8_t* out, uint32_t* longq, uint32_t* nlong) {
-    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / COPY_LANES;
+    const uint32_t lane = threadIdx.x % COPY_LANES;
     if (o >= n) return;
     const uint32_t m = cnt[o] - 1;
     uint8_t* dst = out + cstart[o];
-    dst[m] = 0;
-    if (m > COPY_THREAD_MAX) {
-        longq[atomicAdd(nlong, 1u)] = (uint32_t)o;
+    if (lane == 0) dst[m] = 0;
+    if (m > COPY_GROUP_MAX) {
+        if (lane == 0) longq[atomicAdd(nlong, 1u)] = (uint32_t)o;
         return;
     }
     uint64_t off;
     uint32_t len;
     str_of(a, rsrc[o], off, len);
-    copy_bytes(dst, a.chars + off + rlcp[o], m);
+    const uint8_t* src = a.chars + off + rlcp[o];
+#pragma unroll 4
+    for (uint32_t k = lane; k < m; k += COPY_LANES) dst[k] = src[k];
 }
 
 __global__ void k_recv_copy_warp(ArenaDev a, const uint32_t* cnt, const uint32_t* cstart, const uint32_t* rlcp,
@@ -223,7 +219,7 @@ int bucket_scatter_rect(const ExchangeLayout& L, const ArenaDev& a, uint32_t ps,
     if (recv_capacity < *char_total) return fail(DSSS_EINVAL, "receive buffer of %llu bytes < %llu needed",
                                                  (unsigned long long)recv_capacity, (unsigned long long)*char_total);
     DSSS_LAUNCH("k_recv_copy", st,
-                k_recv_copy<<<grid_for(n, 256), 256, 0, st>>>(a, n, L.cnt, L.cstart, recv_lcp, L.src, recv_chars,
+                k_recv_copy<<<grid_for(n * COPY_LANES, 256), 256, 0, st>>>(a, n, L.cnt, L.cstart, recv_lcp, L.src, recv_chars,
                                                              L.longq, L.counters + 1));
     DSSS_LAUNCH("k_recv_copy_warp", st,
                 k_recv_copy_warp<<<148 * 8, 256, 0, st>>>(a, L.cnt, L.cstart, recv_lcp, L.src, recv_chars, L.longq,
