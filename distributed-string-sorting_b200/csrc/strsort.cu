@@ -560,10 +560,18 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
     const int lane = threadIdx.x & 31;
-    for (uint32_t base = tb + (threadIdx.x & ~31u); base < te; base += LT_NT) {
-        uint32_t i = base + lane;
-        uint32_t d = i < te ? digit_of(key[i], shift) : 0x100u + lane;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
+    // the tile's keys loaded before any is ranked (one DRAM wait, not LT_IPT)
+    uint64_t k[LT_IPT];
+#pragma unroll
+    for (int j = 0; j < LT_IPT; ++j) {
+        const uint32_t i = tb + (threadIdx.x & ~31u) + j * LT_NT + lane;
+        k[j] = i < te ? key[i] : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < LT_IPT; ++j) {
+        const uint32_t i = tb + (threadIdx.x & ~31u) + j * LT_NT + lane;
+        const uint32_t d = i < te ? digit_of(k[j], shift) : 0x100u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
     }
     __syncthreads();
