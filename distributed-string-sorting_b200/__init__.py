@@ -49,6 +49,13 @@ class PdResult(ctypes.Structure):
                 ("merged_lcp", ctypes.c_void_p), ("recv_counts", ctypes.c_void_p)]
 
 
+class MsResult(ctypes.Structure):
+    _fields_ = [("local_order", ctypes.c_void_p), ("intervals", ctypes.c_void_p), ("chars", ctypes.c_void_p),
+                ("chars_capacity", ctypes.c_uint64), ("offsets", ctypes.c_void_p), ("lengths", ctypes.c_void_p),
+                ("lcp", ctypes.c_void_p), ("source", ctypes.c_void_p), ("recv_counts", ctypes.c_void_p),
+                ("avg_lcp", ctypes.c_uint64)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("sort_small_max", ctypes.c_int64), ("sort_pivot", ctypes.c_int64), ("dp_filter_min", ctypes.c_int64),
                 ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("settings_tried", ctypes.c_uint32)]
@@ -87,6 +94,7 @@ _SIGS = {
     "dsss_ctx_kernel_times": (_I, [_P, ctypes.c_char_p, _U64]),
     "dsss_abi_version": (_I, []),
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
+    "dsss_ms_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(MsResult), _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
                                _P]),
     "dsss_pd_sort_batched": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
@@ -391,6 +399,30 @@ def pd_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, sampler: i
     check(lib().dsss_pd_sort(ctx.h, ctypes.byref(a), p, _ptr(pb), ctypes.byref(o), ctypes.byref(res),
                              _stream_ptr(stream)))
     out["part_begin"] = pb
+    return out
+
+
+def ms_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, small_sort_max: int = 0, stream=None):
+    """DistributedMergeSort::sort on the device: every receiving PE's strings,
+    whole and sorted, with LCPs.  Returns torch tensors (device: local_order,
+    chars, offsets, lengths, lcp, source) plus host numpy intervals /
+    recv_counts and the average LCP."""
+    import torch
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    cap = int(ds.lengths[:n].to(torch.int64).sum().item()) + n if n else 0
+    out = dict(local_order=_empty(n), chars=torch.zeros(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
+               offsets=torch.empty(max(n, 1), dtype=torch.int64, device="cuda"), lengths=_empty(n), lcp=_empty(n),
+               source=_empty(n), intervals=np.zeros(p * p, dtype=np.uint64), recv_counts=np.zeros(p, dtype=np.uint64))
+    res = MsResult(_ptr(out["local_order"]), _ptr(out["intervals"]), _ptr(out["chars"]), cap, _ptr(out["offsets"]),
+                   _ptr(out["lengths"]), _ptr(out["lcp"]), _ptr(out["source"]), _ptr(out["recv_counts"]), 0)
+    a = ds.arena()
+    o = _opts(0, 2, small_sort_max, 0)
+    check(lib().dsss_ms_sort(ctx.h, ctypes.byref(a), p, _ptr(pb), ctypes.byref(o), ctypes.byref(res),
+                             _stream_ptr(stream)))
+    out["part_begin"] = pb
+    out["avg_lcp"] = int(res.avg_lcp)
+    out["char_bytes"] = cap
     return out
 
 

@@ -300,6 +300,209 @@ using namespace dsss;
 
 extern "C" {
 
+// ------------------------------------------------------- merge-sort path ----
+// DistributedMergeSort::sort on one GPU holding every PE: the global sort, the
+// local orders (multisplit by PE) and their LCP arrays, getAvgLcp, the
+// partition with samples cut to 200 (avg + 5) bytes, then the receiving PEs'
+// sequences as a projection of the global order (written directly, or by the
+// multisplit by bucket when ties cross a splitter) and their strings copied
+// out whole.
+
+__global__ void k_sum_u32_to_u64(const uint32_t* v, uint64_t n, unsigned long long* total) {
+    unsigned long long s = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        s += v[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(total, s);
+}
+
+__global__ void k_fill_u32(uint32_t* a, uint64_t n, uint32_t v) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// Input index and length (+ 1 for the scan) of every output string.
+__global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, const uint32_t* perm_index,
+                            const uint32_t* perm_pe, ArenaDev a, uint64_t n, uint32_t* source, uint32_t* lengths,
+                            uint32_t* len1) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const uint32_t id = perm_pe ? local_order[pb[perm_pe[o]] + perm_index[o]] : local_order[o];
+    uint64_t off;
+    uint32_t len;
+    str_of(a, id, off, len);
+    source[o] = id;
+    lengths[o] = len;
+    len1[o] = len + 1;
+}
+
+// Whole output strings and their NULs: 8 lanes per string.
+constexpr uint32_t MS_COPY_LANES = 8;
+__global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* out_off, uint64_t n, uint8_t* out) {
+    const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MS_COPY_LANES;
+    const uint32_t lane = threadIdx.x % MS_COPY_LANES;
+    if (o >= n) return;
+    uint64_t off;
+    uint32_t len;
+    str_of(a, source[o], off, len);
+    const uint8_t* src = a.chars + off;
+    uint8_t* dst = out + out_off[o];
+#pragma unroll 4
+    for (uint32_t k = lane; k < len; k += MS_COPY_LANES) dst[k] = src[k];
+    if (lane == 0) dst[len] = 0;
+}
+
+static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* pb, const dsss_opts* opts,
+                       dsss_ms_result* out, cudaStream_t st) {
+    DSSS_TRY(check_arena(in));
+    if (p == 0) return fail(DSSS_EINVAL, "p must be >= 1");
+    if (p > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "p > %u PEs per GPU is not supported", MAX_SPLIT_BUCKETS);
+    DSSS_TRY(check_parts(p, pb, in->n));
+    if (!out || !out->local_order || !out->recv_counts || !out->intervals || !out->offsets || !out->lengths ||
+        !out->lcp || (in->n && !out->chars))
+        return fail(DSSS_EINVAL, "result arrays missing");
+    if (opts && opts->sampler != DSSS_SAMPLER_NUM_STRINGS)
+        return fail(DSSS_ENOTSUP, "the merge-sort path samples with SampleSplittersNumStringsPolicy only");
+    const uint64_t n = in->n;
+    const uint32_t factor = 2, smax = smallmax_of(opts);  // computePartition(..., 2): misc.hpp call in :238
+    const uint64_t N = n ? n : 1;
+    Carve sz(nullptr);
+    PdLayout L;
+    layout_pd(sz, L, n, 1, p, factor, smax);
+    uint32_t* src_tmp = sz.take<uint32_t>(N);
+    uint32_t* len1 = sz.take<uint32_t>(N);
+    unsigned long long* total = sz.take<unsigned long long>(2);
+    void* scan = sz.take<unsigned char>(scan_scratch_bytes(N));
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    DSSS_TRY(ensure_pin(ctx, 4096));
+    Carve c(ctx->ws);
+    layout_pd(c, L, n, 1, p, factor, smax);
+    src_tmp = c.take<uint32_t>(N);
+    len1 = c.take<uint32_t>(N);
+    total = c.take<unsigned long long>(2);
+    scan = c.take<unsigned char>(scan_scratch_bytes(N));
+    uint32_t* source = out->source ? out->source : src_tmp;
+    out->avg_lcp = 0;
+    if (n == 0) {
+        for (uint32_t r = 0; r < p; ++r) out->recv_counts[r] = 0;
+        for (uint64_t k = 0; k < (uint64_t)p * p; ++k) out->intervals[k] = 0;
+        return DSSS_OK;
+    }
+    ArenaDev a = view(in);
+    make_handles(a, L.handles, st);
+    a.h = L.handles;
+    uint32_t* pin = (uint32_t*)ctx->pin;
+    DSSS_CUDA(cudaMemsetAsync(L.err, 0, sizeof(uint32_t), st));
+    DSSS_CUDA(cudaMemsetAsync(total, 0, 2 * sizeof(unsigned long long), st));
+    const uint64_t set_begin[2] = {0, n};
+    {
+        StageTimer t("stage:sort", st);
+        DSSS_TRY(sort_strings(L.sort, a, n, 1, set_begin, nullptr, L.ord, L.lcp, smax, pin, st));
+    }
+    // local orders per PE and their LCP arrays (0 at each PE start)
+    StageTimer t_local("stage:local", st);
+    DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
+    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe));
+    {
+        const uint32_t* ins[1] = {L.ord};
+        uint32_t* outs[1] = {out->local_order};
+        DSSS_TRY(multisplit_payload(L.pe, n, p, 1, ins, outs, L.g2l, L.err, L.ms, st));
+    }
+    // L.dpg holds the local LCPs, then the sample cut
+    DSSS_TRY(adjacent_lcp(a, out->local_order, n, L.dpg, L.tmp, L.nlong, st));
+    DSSS_LAUNCH("k_zero_starts", st, k_zero_starts<<<grid_for(p, 128), 128, 0, st>>>(L.dpg, L.pb, p));
+    DSSS_LAUNCH("k_sum_u32_to_u64", st, k_sum_u32_to_u64<<<148 * 4, 256, 0, st>>>(L.dpg, n, total));
+    pin = (uint32_t*)ctx->pin;
+    DSSS_CUDA(cudaMemcpyAsync(pin, total, 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    const uint64_t avg = *(const uint64_t*)pin / n;  // getAvgLcp (misc.hpp:68-87)
+    out->avg_lcp = avg;
+    t_local.end();
+    if (p == 1) {  // lcp_aware_number_string_splitting.hpp:230-232: the local sort is the result
+        out->intervals[0] = n;
+        out->recv_counts[0] = n;
+        StageTimer t("stage:merge", st);
+        DSSS_CUDA(cudaMemcpyAsync(out->lcp, L.dpg, n * 4, cudaMemcpyDeviceToDevice, st));
+        DSSS_LAUNCH("k_ms_source", st,
+                    k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(out->local_order, L.pb, nullptr, nullptr, a, n,
+                                                                 source, out->lengths, len1));
+    } else {
+        {
+            StageTimer t("stage:partition", st);
+            const uint64_t cut = 2 * (100 * (avg + 5));  // misc.hpp:488 on 100 * globalLcpAvg (:238)
+            DSSS_LAUNCH("k_fill_u32", st,
+                        k_fill_u32<<<grid_for(n, 256), 256, 0, st>>>(L.dpg, n, cut > 0xFFFFFFFFull ? 0xFFFFFFFFu
+                                                                                                 : (uint32_t)cut));
+            DSSS_TRY(partition_sets(L.part, ctx, a, 1, p, pb, out->local_order, L.dpg, DSSS_SAMPLER_NUM_STRINGS,
+                                    factor, out->intervals, st));
+        }
+        StageTimer t_merge("stage:merge", st);
+        std::vector<uint64_t> bounds((uint64_t)p * (p + 1)), recv(p + 1, 0);
+        for (uint32_t q = 0; q < p; ++q) {
+            bounds[(uint64_t)q * (p + 1)] = 0;
+            for (uint32_t r = 0; r < p; ++r) {
+                const uint64_t v = out->intervals[(uint64_t)q * p + r];
+                bounds[(uint64_t)q * (p + 1) + r + 1] = bounds[(uint64_t)q * (p + 1) + r] + v;
+                recv[r + 1] += v;
+            }
+        }
+        for (uint32_t r = 0; r < p; ++r) {
+            out->recv_counts[r] = recv[r + 1];
+            recv[r + 1] += recv[r];
+        }
+        DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
+        // (local index, sender PE) of every output position: perm_index in L.dpg, perm_pe in len1
+        DSSS_CUDA(cudaMemsetAsync(L.viol, 0, sizeof(uint32_t), st));
+        DSSS_LAUNCH("k_bucket_direct", st,
+                    k_bucket_direct<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, 0, L.lcp, L.tmp,
+                                                                     nullptr, L.dpg, len1, out->lcp, L.viol));
+        pin = (uint32_t*)ctx->pin;
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.viol, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        if (pin[0]) {
+            const uint32_t* ins[3] = {L.g2l, L.pe, nullptr};
+            uint32_t* outs[3] = {L.dpg, len1, L.out2g};
+            DSSS_TRY(multisplit_payload(L.tmp, n, p, 3, ins, outs, nullptr, L.err, L.ms, st));
+            DSSS_LAUNCH("k_merged_lcp", st,
+                        k_merged_lcp<<<grid_for(n, 256), 256, 0, st>>>(L.out2g, L.lcp, L.recv_begin, p, n, out->lcp));
+        }
+        DSSS_LAUNCH("k_ms_source", st,
+                    k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(out->local_order, L.pb, L.dpg, len1, a, n, source,
+                                                                 out->lengths, src_tmp == source ? L.tmp : src_tmp));
+        len1 = src_tmp == source ? L.tmp : src_tmp;
+    }
+    // output layout and the strings themselves
+    {
+        StageTimer t("stage:copy", st);
+        DSSS_TRY(exclusive_scan_u32_to_u64(len1, out->offsets, n, (uint64_t*)(total + 1), scan, st));
+        pin = (uint32_t*)ctx->pin;
+        DSSS_CUDA(cudaMemcpyAsync(pin, total + 1, 8, cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        const uint64_t bytes = *(const uint64_t*)pin;
+        if (bytes > out->chars_capacity)
+            return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
+                        (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
+        DSSS_LAUNCH("k_ms_copy", st,
+                    k_ms_copy<<<grid_for(n * MS_COPY_LANES, 256), 256, 0, st>>>(a, source, out->offsets, n,
+                                                                                out->chars));
+    }
+    pin = (uint32_t*)ctx->pin;
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (pin[0]) return fail(DSSS_EDEVICE, "ms sort: internal consistency guard tripped");
+    return DSSS_OK;
+}
+
+int dsss_ms_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, const dsss_opts* opts,
+                 dsss_ms_result* out, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    return ms_sort_dev(ctx, in, p, part_begin, opts, out, (cudaStream_t)stream);
+}
+
 int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, const dsss_opts* opts,
                  dsss_pd_result* out, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");

@@ -160,6 +160,36 @@ int dsss_pd_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t
 int dsss_pd_sort_host(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                       const dsss_opts* opts, dsss_pd_result* out, dsss_stream_t stream);
 
+/* Outputs of the merge-sort path, device arrays of n entries unless noted.
+ * Receiving PEs back to back: PE r's recv_counts[r] strings, whole, in sorted
+ * order. */
+typedef struct dsss_ms_result {
+    uint32_t* local_order;    /* per PE, the input index of each locally sorted string */
+    uint64_t* intervals;      /* HOST [p*p]: strings PE q sends to PE r at [q*p + r] */
+    uint8_t* chars;           /* the output strings, each followed by a NUL */
+    uint64_t chars_capacity;  /* bytes at chars: at least the sum of (length + 1) */
+    uint64_t* offsets;        /* start of each output string in chars */
+    uint32_t* lengths;        /* length of each output string */
+    uint32_t* lcp;            /* LCP with the previous output string, 0 at each PE start */
+    uint32_t* source;         /* optional: input index of each output string */
+    uint64_t* recv_counts;    /* HOST [p]: strings per receiving PE */
+    uint64_t avg_lcp;         /* set by the call: getAvgLcp over all PEs */
+} dsss_ms_result;
+
+/* DistributedMergeSort<...>::sort (src/sorter/distributed/lcp_aware_number_string_splitting.hpp:184-290)
+ * with SampleSplittersNumStringsPolicy and AllToAllStringImpl with
+ * EmptyLcpByteEncoderMemCpy (mpi/alltoall.hpp:724-804): local sort; the
+ * average LCP (getAvgLcp, misc.hpp:68-87); splitters from samples cut to
+ * 200 (avg + 5) bytes (computePartition, misc.hpp:473-531;
+ * samplingStrategies.hpp:25-55); whole strings exchanged and merged; the
+ * output is every PE's received strings, whole and sorted, with LCPs (the
+ * reference's returned StringLcpContainer).  As in the reference, p == 1 returns
+ * the local sort (:230-232).  Byte-identical strings are indistinguishable in
+ * this output; `source` orders them by (sender PE, local index).  One GPU
+ * holds all PEs: the exchange and merge are a projection of one global sort. */
+int dsss_ms_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
+                 const dsss_opts* opts, dsss_ms_result* out, dsss_stream_t stream);
+
 /* Batched form (no reference counterpart: the reference sorts one string set
  * per MPI job): nsets independent string sets of p PEs each in one arena, run
  * through one pipeline.  part_begin has nsets*p + 1 entries; PE q of set s

@@ -55,6 +55,8 @@ def lib():
         L.oracle_merge.argtypes = [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P, _P]
         L.oracle_pd_sort.restype = _I
         L.oracle_pd_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.oracle_ms_sort.restype = _I
+        L.oracle_ms_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -205,6 +207,27 @@ def pd_sort(s: Strings, pb, indexed=False):
     for k in ("order", "lcp", "dp", "perm_index", "perm_pe", "merged_lcp", "old_lcp"):
         o[k] = o[k][:n]
     o["intervals"] = o["intervals"].reshape(p, p)
+    return o
+
+
+def ms_sort(s: Strings, pb):
+    """The merge-sort path (oracle_ms_sort): local sort, average LCP, splitters
+    from samples truncated to 200 (avg + 5) bytes, whole strings exchanged and
+    merged; source = string id of every output string, receiving PEs back to back."""
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    n = s.n
+    z = lambda: np.zeros(max(n, 1), np.uint64)
+    o = dict(order=z(), lcp=z(), intervals=np.zeros(p * p, np.uint64), source=z(), out_lcp=z(),
+             recv_counts=np.zeros(p, np.uint64))
+    avg = np.zeros(1, np.uint64)
+    rc = lib().oracle_ms_sort(*s.args(), p, _p(pb), _p(o["order"]), _p(o["lcp"]), _p(o["intervals"]),
+                              _p(o["source"]), _p(o["out_lcp"]), _p(o["recv_counts"]), _p(avg))
+    assert rc == 0
+    for k in ("order", "lcp", "source", "out_lcp"):
+        o[k] = o[k][:n]
+    o["intervals"] = o["intervals"].reshape(p, p)
+    o["avg_lcp"] = int(avg[0])
     return o
 
 

@@ -621,4 +621,55 @@ int oracle_pd_sort(const uint8_t* chars, const uint64_t* off, const uint32_t* le
     return 0;
 }
 
+// Merge-sort path: DistributedMergeSort::sort
+// (sorter/distributed/lcp_aware_number_string_splitting.hpp:184-290) with the
+// non-indexed sampler and AllToAllStringImpl<..., EmptyLcpByteEncoderMemCpy>
+// (mpi/alltoall.hpp:724-804).  Local sort; avg = getAvgLcp (misc.hpp:68-87:
+// the sum of every PE's local LCP array over the number of strings, integer
+// division); computePartition(ptr, 100 * (avg + 5), 2) (misc.hpp:473-531)
+// samples with SampleSplittersNumStringsPolicy's maxLength overload
+// (samplingStrategies.hpp:25-55), each sample truncated to 2 * that = 200 *
+// (avg + 5) bytes; the exchange sends whole strings LCP-compressed (bytes
+// [lcp, length) and a NUL); choose_merge outputs every received string, whole,
+// in order, with LCPs.  Outputs: order/lcp (local sort), intervals [p*p],
+// source [n] (string id of every output string, receiving PEs back to back),
+// out_lcp [n], recv_counts [p], *avg_lcp.  p == 1 returns the local sort
+// (lcp_aware_number_string_splitting.hpp:230-232).
+int oracle_ms_sort(const uint8_t* chars, const uint64_t* off, const uint32_t* len, uint64_t n, uint32_t p,
+                   const uint64_t* pb, uint64_t* order, uint64_t* lcp, uint64_t* intervals, uint64_t* source,
+                   uint64_t* out_lcp, uint64_t* recv_counts, uint64_t* avg_lcp) {
+    Arena a{chars, off, len, n};
+    local_sort(a, p, pb, order, lcp);
+    uint64_t lsum = 0;
+    for (uint64_t i = 0; i < n; ++i) lsum += lcp[i];
+    const uint64_t avg = n ? lsum / n : 0;
+    *avg_lcp = avg;
+    if (p == 1) {
+        for (uint64_t i = 0; i < n; ++i) {
+            source[i] = order[i];
+            out_lcp[i] = lcp[i];
+        }
+        intervals[0] = n;
+        recv_counts[0] = n;
+        return 0;
+    }
+    const uint64_t max_len = 2 * (100 * (avg + 5));
+    std::vector<uint64_t> trunc(n ? n : 1, max_len), whole(n ? n : 1);
+    for (uint64_t i = 0; i < n; ++i) whole[i] = len[order[i]];
+    partition(a, p, pb, order, trunc.data(), 2, false, intervals);
+    std::vector<Recv> rv = exchange(a, p, pb, order, lcp, whole.data(), intervals);
+    uint64_t o = 0;
+    for (uint32_t r = 0; r < p; ++r) {
+        const uint64_t m = rv[r].lcp.size();
+        recv_counts[r] = m;
+        std::vector<uint64_t> idx(m ? m : 1), pe(m ? m : 1), ml(m ? m : 1), old(m ? m : 1);
+        merge_one(rv[r], p, idx.data(), pe.data(), ml.data(), old.data());
+        for (uint64_t k = 0; k < m; ++k, ++o) {
+            source[o] = order[pb[pe[k]] + idx[k]];
+            out_lcp[o] = ml[k];
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"
