@@ -89,3 +89,42 @@ def test_full_size_properties(dsss, ctx, n, length):
     starts[1:] = ~same
     assert bool((ml[starts] == 0).all())
     assert bool((ml[1:][same] == lcp[same]).all())
+
+
+class _View:
+    """chars / offsets / lengths tensors shaped like DeviceStrings."""
+
+    def __init__(self, chars, offsets, lengths):
+        self.chars, self.offsets, self.lengths = chars, offsets, lengths
+
+
+def test_full_size_ms_sort(dsss, ctx):
+    """The merge-sort path on 32e6 strings x 200 B, p = 64: the output names
+    every string once, each receiving PE's strings are strictly increasing,
+    their bytes are the input strings', and the LCPs are the neighbours'."""
+    n, p = 32_000_000, 64
+    hs = dsss.gen_dn(n, 200, 50, seed=2)
+    ds = dsss.DeviceStrings(hs)
+    del hs
+    out = dsss.ms_sort(ctx, ds, p)
+    dev = ds.offsets.device
+    src = out["source"][:n].long() & 0xFFFFFFFF
+    assert bool((torch.sort(src).values == torch.arange(n, device=dev)).all())
+    lens = out["lengths"][:n].long() & 0xFFFFFFFF
+    assert bool((lens == ds.lengths[src].long()).all())
+    view = _View(out["chars"], out["offsets"][:n], out["lengths"][:n])
+    ids = torch.arange(n, device=dev)
+    # output bytes equal the input strings' (first W bytes, chunk by chunk)
+    for s in range(0, n, CHUNK):
+        e = min(n, s + CHUNK)
+        assert bool((prefix_bytes(view, ids[s:e]) == prefix_bytes(ds, src[s:e])).all())
+    rc = torch.from_numpy(np.asarray(out["recv_counts"], np.int64)).to(dev)
+    assert int(rc.sum()) == n
+    run = torch.repeat_interleave(torch.arange(p, device=dev), rc)
+    same = run[:-1] == run[1:]
+    lcp = pair_check(view, ids, same)
+    ml = out["lcp"][:n].long() & 0xFFFFFFFF
+    starts = torch.ones(n, dtype=torch.bool, device=dev)
+    starts[1:] = ~same
+    assert bool((ml[starts] == 0).all())
+    assert bool((ml[1:][same] == lcp[same]).all())
