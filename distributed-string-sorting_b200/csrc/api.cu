@@ -331,10 +331,8 @@ __global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, con
     len1[o] = len + 1;
 }
 
-// Whole output strings and their NULs, MS_COPY_LANES lanes per string: the
-// destination's aligned 8-byte words are stored whole (each from an unaligned
-// 8-byte load of the source, which reads at most 15 bytes past a string: the
-// arena pads 32), the at most 7 bytes before and after them one by one.
+// Whole output strings and their NULs, MS_COPY_LANES lanes per string
+// (copy_words: aligned 8-byte stores; 8 lanes measured faster than 4 or 32).
 constexpr uint32_t MS_COPY_LANES = 8;
 __global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* out_off, uint64_t n, uint8_t* out) {
     const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MS_COPY_LANES;
@@ -343,21 +341,8 @@ __global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* ou
     uint64_t off;
     uint32_t len;
     str_of(a, source[o], off, len);
-    const uint8_t* src = a.chars + off;
     uint8_t* dst = out + out_off[o];
-    const uintptr_t d0 = (uintptr_t)dst, e = d0 + len;
-    const uintptr_t a0 = (d0 + 7) & ~(uintptr_t)7, a1 = e & ~(uintptr_t)7;
-    if (a0 >= a1) {
-        for (uint32_t k = lane; k < len; k += MS_COPY_LANES) dst[k] = src[k];
-    } else {
-        const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(a1 - d0);
-        for (uint32_t k = lane; k < head; k += MS_COPY_LANES) dst[k] = src[k];
-        for (uint32_t k = tail + lane; k < len; k += MS_COPY_LANES) dst[k] = src[k];
-        const uint32_t nw = (uint32_t)((a1 - a0) >> 3);
-        unsigned long long* w = reinterpret_cast<unsigned long long*>(a0);
-#pragma unroll 4
-        for (uint32_t k = lane; k < nw; k += MS_COPY_LANES) w[k] = load_le8(src + head + 8 * k);
-    }
+    copy_words<MS_COPY_LANES>(dst, a.chars + off, len, lane);
     if (lane == 0) dst[len] = 0;
 }
 

@@ -188,6 +188,27 @@ __device__ __forceinline__ uint64_t load_le8(const uint8_t* p) {
     return (lo >> sh) | (hi << (64 - sh));
 }
 
+// Copies len bytes from src to dst with L lanes (lane = 0..L-1 of the
+// calling group): dst's aligned 8-byte words are stored whole, each from an
+// unaligned 8-byte load of src (reads at most 15 bytes past src + len; the
+// arena contract pads 32), the at most 7 bytes before and after them singly.
+template <uint32_t L>
+__device__ __forceinline__ void copy_words(uint8_t* dst, const uint8_t* src, uint32_t len, uint32_t lane) {
+    const uintptr_t d0 = (uintptr_t)dst, e = d0 + len;
+    const uintptr_t a0 = (d0 + 7) & ~(uintptr_t)7, a1 = e & ~(uintptr_t)7;
+    if (a0 >= a1) {
+        for (uint32_t k = lane; k < len; k += L) dst[k] = src[k];
+        return;
+    }
+    const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(a1 - d0);
+    for (uint32_t k = lane; k < head; k += L) dst[k] = src[k];
+    for (uint32_t k = tail + lane; k < len; k += L) dst[k] = src[k];
+    const uint32_t nw = (uint32_t)((a1 - a0) >> 3);
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(a0);
+#pragma unroll 4
+    for (uint32_t k = lane; k < nw; k += L) w[k] = load_le8(src + head + 8 * k);
+}
+
 // Bytes [depth, depth+8) of a string as a big-endian key; bytes at or past
 // the string's length are 0 (the NUL terminator and beyond), so unsigned key
 // order is the reference's byte-wise string order (scmp, stringtools.hpp:128).
