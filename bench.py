@@ -16,6 +16,7 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
             capture (profiles/k_dp_hash_dn8m.md) times the strings hashed
   roofline_sort  the string sort stage (K3) the same way: D + 20 n (D = sum of
             DP lengths, 8 B id read + 8 B id write + 4 B LCP write per string)
+  ms_path   the merge-sort path (dsss_ms_sort) on the same input, device-timed
   cpu_baseline  the oracle port of the reference path on the host
 
 --impl reference times the CPU port of the reference path (oracle/) on all
@@ -349,6 +350,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-ms", action="store_true", help="skip the merge-sort path line")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dist"],
                     help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL)")
@@ -473,6 +475,29 @@ def main():
         cpu = {"value": cpu_baseline_port(sample, L, k, p, seed=1), "unit": "strings/s", "cores": 1, "kind": "port",
                "sample": f"{sample} strings of the same rule, p = {p}, oracle port single-threaded"}
 
+    # the merge-sort path (dsss_ms_sort) on the same input, device-timed
+    ms_path = None
+    if world == 1 and not args.no_ms:
+        del out
+        torch.cuda.empty_cache()
+        mout = None
+        for _ in range(2):
+            mout = d.ms_sort(ctx, ds, p)
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        msteps = max(3, min(args.steps, 10))
+        for _ in range(msteps):
+            mout = d.ms_sort(ctx, ds, p)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        mms = m0.elapsed_time(m1) / msteps
+        ms_path = {"workload": desc + ", merge-sort path (whole strings and LCPs per receiving PE)",
+                   "steps": msteps, "ms_per_call": mms, "strings_per_s": n / (mms * 1e-3),
+                   "out_char_bytes": mout["char_bytes"], "avg_lcp": mout["avg_lcp"]}
+        del mout
+        out = None
+
     ctx.close()
     del ds, out
     torch.cuda.empty_cache()
@@ -514,6 +539,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "ms_path": ms_path,
             "batched": batched,
             "serving": serving,
         }
