@@ -198,6 +198,65 @@ private:
     Sampler sampler_;
 };
 
+// Results of DistributedMergeSort::sort for every PE.
+struct MsSortResult {
+    std::vector<std::vector<size_t>> local_order;     // per PE, as in PdSortResult
+    std::vector<std::vector<size_t>> interval_sizes;  // per PE: strings sent to each PE
+    // Per receiving PE: the returned StringLcpContainer's raw strings
+    // (NUL-terminated, in order) and LCPs (0 first).
+    std::vector<std::vector<unsigned char>> raw_strings;
+    std::vector<std::vector<size_t>> lcps;
+    size_t avg_lcp = 0;  // getAvgLcp over all PEs
+};
+
+// DistributedMergeSort<StringLcpPtr, SampleSplittersNumStringsPolicy,
+// AllToAllStringImpl<..., EmptyLcpByteEncoderMemCpy>, ...>::sort
+// (src/sorter/distributed/lcp_aware_number_string_splitting.hpp:184-290) for
+// all PEs at once.  As in the reference, p == 1 returns the local sort.
+class DistributedMergeSort {
+public:
+    MsSortResult sort(Context& ctx, const std::vector<std::vector<unsigned char>>& raw_per_pe,
+                      cudaStream_t stream = nullptr) const {
+        HostArena h(raw_per_pe);
+        DeviceArena d(h);
+        const size_t n = h.n();
+        const uint32_t p = h.p();
+        const uint64_t cap = h.chars.size() - 64;  // every string and its NUL
+        DeviceVec<uint32_t> order(n), lens(n), lcp(n);
+        DeviceVec<uint64_t> offs(n);
+        DeviceVec<uint8_t> chars(cap + 64);
+        std::vector<uint64_t> intervals((size_t)p * p), recv(p);
+        dsss_ms_result r{order.p, intervals.data(), chars.p, cap, offs.p, lens.p, lcp.p, nullptr, recv.data(), 0};
+        dsss_opts o{DSSS_SAMPLER_NUM_STRINGS, 2, 0, 0};
+        dsss_arena a = d.view();
+        check(dsss_ms_sort(ctx.get(), &a, p, h.part_begin.data(), &o, &r, (dsss_stream_t)stream));
+        check_cuda(cudaStreamSynchronize(stream));
+        const std::vector<uint32_t> ho = order.host(), hl = lcp.host();
+        const std::vector<uint8_t> hc = chars.host();
+        MsSortResult out;
+        out.avg_lcp = r.avg_lcp;
+        out.local_order.resize(p);
+        out.interval_sizes.resize(p);
+        for (uint32_t q = 0; q < p; ++q) {
+            for (uint64_t i = h.part_begin[q]; i < h.part_begin[q + 1]; ++i)
+                out.local_order[q].push_back(ho[i] - h.part_begin[q]);
+            out.interval_sizes[q].assign(intervals.begin() + (size_t)q * p, intervals.begin() + (size_t)(q + 1) * p);
+        }
+        out.raw_strings.resize(p);
+        out.lcps.resize(p);
+        size_t k = 0, byte = 0;
+        for (uint32_t q = 0; q < p; ++q)
+            for (uint64_t j = 0; j < recv[q]; ++j, ++k) {
+                size_t e = byte;
+                while (hc[e] != 0) ++e;
+                out.raw_strings[q].insert(out.raw_strings[q].end(), hc.begin() + byte, hc.begin() + e + 1);
+                out.lcps[q].push_back(hl[k]);
+                byte = e + 1;
+            }
+        return out;
+    }
+};
+
 // tlx::sort_strings_detail::radixsort_CI3(StringLcpPtr, 0, 0) for each PE:
 // order[q][i] = input position of the i-th smallest string of PE q,
 // lcp[q][i] = LCP with its predecessor (0 first).

@@ -1,6 +1,7 @@
 // Drives include/dsss_policies.hpp the way the reference's prefix_doubling
 // executable drives DistributedPrefixDoublingSort: strings per PE in, local
-// order / DP / intervals / permutation out.  Input (stdin): p, then for each
+// order / DP / intervals / permutation out, and DistributedMergeSort the way
+// the merge-sort executable does (strings and LCPs per receiving PE).  Input (stdin): p, then for each
 // PE a count and that many hex-encoded strings.  Output: one line per item.
 #include <iostream>
 #include <string>
@@ -47,6 +48,29 @@ int main(int argc, char** argv) {
             for (auto x : r.permutation[q]) std::cout << ' ' << x.stringIndex << ':' << x.PEIndex;
             std::cout << "\nlcp " << q;
             for (auto x : r.merged_lcp[q]) std::cout << ' ' << x;
+            std::cout << '\n';
+        }
+        // the merge-sort path: every receiving PE's strings (hex) and LCPs
+        dsss_gpu::DistributedMergeSort ms;
+        auto m = ms.sort(ctx, raw);
+        std::cout << "msavg 0 " << m.avg_lcp << '\n';
+        for (uint32_t q = 0; q < p; ++q) {
+            std::cout << "msintervals " << q;
+            for (auto x : m.interval_sizes[q]) std::cout << ' ' << x;
+            std::cout << "\nmsstr " << q;
+            std::string cur;
+            for (unsigned char c : m.raw_strings[q]) {
+                if (c == 0) {
+                    std::cout << ' ' << (cur.empty() ? std::string("-") : cur);
+                    cur.clear();
+                } else {
+                    static const char* hx = "0123456789abcdef";
+                    cur += hx[c >> 4];
+                    cur += hx[c & 15];
+                }
+            }
+            std::cout << "\nmslcp " << q;
+            for (auto x : m.lcps[q]) std::cout << ' ' << x;
             std::cout << '\n';
         }
         // the stage adaptors on PE 0

@@ -65,3 +65,22 @@ def test_policies_match_oracle(prog, orc, dsss, sampler):
     ro, rl = orc.local_sort(orc.Strings.from_host(dsss.from_bytes_list(per_pe[0])), np.array([0, 500], np.uint64))
     assert [int(x) for x in res["ci3order"][0]] == ro.tolist()
     assert [int(x) for x in res["ci3lcp"][0]] == rl.tolist()
+
+
+def test_merge_sort_policy_matches_oracle(prog, orc, dsss):
+    """dsss_gpu::DistributedMergeSort: every receiving PE's strings and LCPs,
+    the interval table and the average LCP, as the oracle's merge-sort path."""
+    p = 4
+    strs = with_duplicates(random_strings(2000, 1, 20, b"ABCDE", 79), 0.1, 80)
+    per_pe = [strs[q * 500:(q + 1) * 500] for q in range(p)]
+    res = run(prog, per_pe)
+    hs = dsss.from_bytes_list(strs)
+    s = orc.Strings.from_host(hs)
+    r = orc.ms_sort(s, dsss.equal_parts(len(strs), p))
+    assert int(res["msavg"][0][0]) == r["avg_lcp"]
+    iv = np.array([[int(x) for x in res["msintervals"][q]] for q in range(p)], np.uint64)
+    assert np.array_equal(iv, r["intervals"])
+    got = [bytes.fromhex(x) if x != "-" else b"" for q in range(p) for x in res["msstr"][q]]
+    assert got == [s.get(int(i)) for i in r["source"]]
+    lcp = np.concatenate([np.array(res["mslcp"][q], np.uint64) for q in range(p)])
+    assert np.array_equal(lcp, r["out_lcp"])
