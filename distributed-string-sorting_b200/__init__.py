@@ -95,6 +95,7 @@ _SIGS = {
     "dsss_abi_version": (_I, []),
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
     "dsss_ms_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(MsResult), _P]),
+    "dsss_distribute_lines": (_I, [_P, _P, _U64, _U64, _U32, _P, _U64, _P, _P, _U64, _P, _P, _P, _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
                                _P]),
     "dsss_pd_sort_batched": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
@@ -424,6 +425,29 @@ def ms_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, small_sort
     out["avg_lcp"] = int(res.avg_lcp)
     out["char_bytes"] = cap
     return out
+
+
+def distribute_lines(ctx: Context, data, p: int, max_size: int = 0, stream=None):
+    """distribute_strings on one GPU: the file bytes `data` (bytes or uint8
+    array) cut into p PEs' lines ('\\n' -> NUL).  Returns (DeviceStrings,
+    part_begin)."""
+    import torch
+    arr = np.frombuffer(data, np.uint8) if isinstance(data, (bytes, bytearray)) else np.ascontiguousarray(data, np.uint8)
+    size = int(arr.size)
+    S = min(size, max_size) if max_size else size
+    cap_n = int(np.count_nonzero(arr[:S] == 10) + np.count_nonzero(arr[:S] == 0)) + 1
+    cap = S + 1 + PAD
+    chars = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    offs = torch.empty(cap_n, dtype=torch.int64, device="cuda")
+    lens = torch.empty(cap_n, dtype=torch.int32, device="cuda")
+    n, cb = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    pb = np.zeros(p + 1, np.uint64)
+    check(lib().dsss_distribute_lines(ctx.h, _ptr(arr), size, max_size, p, _ptr(chars), cap, _ptr(offs), _ptr(lens),
+                                      cap_n, ctypes.byref(n), ctypes.byref(cb), _ptr(pb), _stream_ptr(stream)))
+    ds = DeviceStrings.__new__(DeviceStrings)
+    ds.chars, ds.offsets, ds.lengths = chars, offs[:max(n.value, 1)], lens[:max(n.value, 1)]
+    ds.char_bytes, ds.n = int(cb.value), int(n.value)
+    return ds, pb
 
 
 def pd_sort_host(ctx: Context, hs: HostStrings, p: int, part_begin=None, sampler: int = 0, merged_lcp: bool = True,

@@ -435,6 +435,21 @@ int dsss_server_destroy(dsss_server* s);
 
 /* ---- synthetic inputs (host) --------------------------------------------- */
 
+/* distribute_strings (src/mpi/readInput.hpp:40-104) for p PEs held by one
+ * GPU: the file's first S = min(size, max_size) bytes (max_size 0: all) in p
+ * byte slices (the first S % p one byte longer); every '\n' becomes a NUL;
+ * PE r > 0 starts just after the first '\n' of its slice (its first line goes
+ * to PE r - 1, as the reference's shift does); a NUL closes the file when it
+ * does not end with one.  file: host bytes.  Writes *char_bytes (S, + 1 for
+ * the closing NUL) and, when chars != NULL: chars (device, chars_cap >=
+ * char_bytes + 32, the tail zeroed), offsets / lengths (device, cap_n entries)
+ * of the *n lines in file order, part_begin (HOST, p + 1 line indices): an
+ * arena ready for dsss_pd_sort / dsss_ms_sort.  A slice of PE r > 0 without a
+ * '\n' (where the reference reads past its buffer) is an error. */
+int dsss_distribute_lines(dsss_ctx* ctx, const uint8_t* file, uint64_t size, uint64_t max_size, uint32_t p,
+                          uint8_t* chars, uint64_t chars_cap, uint64_t* offsets, uint32_t* lengths, uint64_t cap_n,
+                          uint64_t* n, uint64_t* char_bytes, uint64_t* part_begin, dsss_stream_t stream);
+
 /* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),
  * seeded and reproducible: string i is (k - d) 'A's, the d base-26 digits
  * ('A' = 0) of pi(i) for a seeded permutation pi of [0, n), then uniform

@@ -231,6 +231,48 @@ def ms_sort(s: Strings, pb):
     return o
 
 
+def distribute_strings(data: bytes, p: int, max_size: int = 0):
+    """distribute_strings (src/mpi/readInput.hpp:40-104) restated rank by rank:
+    the raw vector every rank ends with.  Raises ValueError where the reference
+    reads past a buffer (a rank r > 0 whose slice holds no newline, or an
+    empty last slice)."""
+    S = min(len(data), max_size) if max_size > 0 else len(data)
+    local, larger = S // p, S % p
+    sl = []
+    for r in range(p):  # :57-69
+        if r < larger:
+            ln = local + 1
+            off = ln * r
+        else:
+            ln = local
+            off = larger * (local + 1) + (r - larger) * local
+        res = bytearray(data[off:off + ln])
+        fe = 0  # :76-79
+        while fe < len(res) and res[fe] != 10:
+            fe += 1
+        for i in range(len(res)):  # :80-82
+            if res[i] == 10:
+                res[i] = 0
+        sl.append((res, fe))
+    out = []
+    for r in range(p):
+        res = bytearray(sl[r][0])
+        if r + 1 < p:  # :84-91, the next rank's shift_left of first_end + 1 bytes
+            nxt, nfe = sl[r + 1]
+            if nfe >= len(nxt):
+                raise ValueError("rank %d's slice holds no newline" % (r + 1))
+            res += nxt[:nfe + 1]
+        else:  # :92-96
+            if not res:
+                raise ValueError("empty last slice")
+            if res[-1] != 0:
+                res.append(0)
+        if r > 0:  # :97-99
+            res = res[sl[r][1] + 1:]
+        out.append(bytes(res))
+    return out
+
+
 # ------------------------------------------------------------ reference ----
 def ref_xxh64(data: bytes) -> int:
     buf = np.frombuffer(data + b"\0", dtype=np.uint8)
