@@ -96,6 +96,8 @@ _SIGS = {
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
     "dsss_ms_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(MsResult), _P]),
     "dsss_distribute_lines": (_I, [_P, _P, _U64, _U64, _U32, _P, _U64, _P, _P, _U64, _P, _P, _P, _P]),
+    "dsss_varint_encode": (_I, [_P, _P, _U64, _P, _U32, _P, _U64, _P, _P, _P]),
+    "dsss_varint_decode": (_I, [_P, _P, _U64, _P, _U64, _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
                                _P]),
     "dsss_pd_sort_batched": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
@@ -448,6 +450,33 @@ def distribute_lines(ctx: Context, data, p: int, max_size: int = 0, stream=None)
     ds.chars, ds.offsets, ds.lengths = chars, offs[:max(n.value, 1)], lens[:max(n.value, 1)]
     ds.char_bytes, ds.n = int(cb.value), int(n.value)
     return ds, pb
+
+
+def varint_encode(ctx: Context, values, range_counts=None, stream=None):
+    """LCPs (device uint32/int32 tensor) to their varint bytes (device uint8
+    tensor); with range_counts (values per destination) also the bytes per
+    range (host uint64), as writeRanges reports them."""
+    import torch
+    n = int(values.numel())
+    rc = np.zeros(0, np.uint64) if range_counts is None else np.asarray(range_counts, np.uint64)
+    rb = np.concatenate([[0], np.cumsum(rc)]).astype(np.uint64)
+    nr = int(rc.size)
+    tot = ctypes.c_uint64(0)
+    per = np.zeros(max(nr, 1), np.uint64)
+    check(lib().dsss_varint_encode(ctx.h, _ptr(values), n, _ptr(rb), nr, None, 0, ctypes.byref(tot), _ptr(per),
+                                   _stream_ptr(stream)))
+    out = torch.zeros(max(tot.value, 1), dtype=torch.uint8, device="cuda")
+    check(lib().dsss_varint_encode(ctx.h, _ptr(values), n, _ptr(rb), nr, _ptr(out), out.numel(), ctypes.byref(tot),
+                                   _ptr(per), _stream_ptr(stream)))
+    return out[:tot.value], per[:nr]
+
+
+def varint_decode(ctx: Context, data, n: int, stream=None):
+    """n varint-coded values (device uint8 tensor) to a device int32 tensor."""
+    out = _empty(n)
+    check(lib().dsss_varint_decode(ctx.h, _ptr(data) if data.numel() else None, int(data.numel()), _ptr(out), n,
+                                   _stream_ptr(stream)))
+    return out[:n]
 
 
 def pd_sort_host(ctx: Context, hs: HostStrings, p: int, part_begin=None, sampler: int = 0, merged_lcp: bool = True,

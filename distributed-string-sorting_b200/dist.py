@@ -30,7 +30,8 @@ import ctypes
 
 import numpy as np
 
-from . import Arena, DeviceStrings, PAD, _ptr, _stream_ptr, check, lcp_merge, lib, local_sort_lcp
+from . import (Arena, DeviceStrings, PAD, _ptr, _stream_ptr, check, lcp_merge, lib, local_sort_lcp, varint_decode,
+               varint_encode)
 
 
 # ------------------------------------------------------------- collectives --
@@ -277,6 +278,12 @@ class GpuBackend:
                                  _ptr(dstart), _ptr(lcps), _ptr(dlcp), n, self._s()))
         return dchars, dstart[:n], dlcp[:n]
 
+    def varint_encode(self, values, range_counts):
+        return varint_encode(self.ctx, values, range_counts, stream=self.stream)
+
+    def varint_decode(self, data, n):
+        return varint_decode(self.ctx, data, n, stream=self.stream)
+
     def merge(self, chars, nbytes, starts, lcps, counts, offsets):
         out = lcp_merge(self.ctx, chars, nbytes, lcps, counts, offsets, char_start=starts, stream=self.stream)
         return {k: out[k] for k in ("perm_index", "perm_pe", "merged_lcp")}
@@ -358,7 +365,8 @@ class _Phases:
         self.t = t
 
 
-def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None):
+def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None,
+         compress_lcps: bool = False):
     """This rank's part of DistributedPrefixDoublingSort::sort.  strings: the
     backend's arena of this rank's strings; part_begin: p_local + 1 PE bounds.
     phases (dict, optional) receives milliseconds per phase."""
@@ -464,7 +472,16 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
     r_byte = comm.alltoall_counts(s_byte)
     rchars = comm.alltoallv(snd["chars"], s_byte, r_byte)
     rstart = comm.alltoallv(snd["char_start"], s_str, r_str)
-    rlcp = comm.alltoallv(snd["lcp"], s_str, r_str)
+    if compress_lcps:
+        # sendLcps with compressLcps (alltoall.hpp:406-425): each rank's run of
+        # LCPs varint-coded (writeRanges), the bytes exchanged, and all that
+        # arrives decoded as one sequence (varint codes are self-delimiting)
+        lbytes, per_rank = be.varint_encode(snd["lcp"], s_str)
+        r_lb = comm.alltoall_counts([int(x) for x in per_rank])
+        got = comm.alltoallv(lbytes, [int(x) for x in per_rank], r_lb)
+        rlcp = be.varint_decode(got, int(sum(r_str)))
+    else:
+        rlcp = comm.alltoallv(snd["lcp"], s_str, r_str)
     ph.mark("exchange")
     # regroup [sender rank][receiver] -> [receiver][sender rank]
     src_str = np.concatenate([[0], np.cumsum(r_str)])

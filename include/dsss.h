@@ -450,6 +450,23 @@ int dsss_distribute_lines(dsss_ctx* ctx, const uint8_t* file, uint64_t size, uin
                           uint8_t* chars, uint64_t chars_cap, uint64_t* offsets, uint32_t* lengths, uint64_t cap_n,
                           uint64_t* n, uint64_t* char_bytes, uint64_t* part_begin, dsss_stream_t stream);
 
+/* Varint coding of LCP arrays, the wire format of the string exchange with
+ * compressLcps (sendLcps, src/mpi/alltoall.hpp:406-425; Writer::PutVarint,
+ * src/encoding/integer_compression.hpp:66-140: 7 bits per byte, least
+ * significant first, the high bit on every byte but the last).
+ * encode: values (device, n) to out (device, out_cap bytes); *out_bytes = the
+ * coded size (out == NULL: size query only); ranges [range_begin[r],
+ * range_begin[r+1]) (HOST, nranges + 1 value indices) get their byte counts
+ * in range_bytes (HOST, nranges), as IntegerCompression::writeRanges
+ * (src/mpi/byte_encoder.hpp:31-53) reports them.
+ * decode: nbytes coded bytes (device) holding exactly n values (device out);
+ * a cut-off, over-long or too large value is an error. */
+int dsss_varint_encode(dsss_ctx* ctx, const uint32_t* values, uint64_t n, const uint64_t* range_begin,
+                       uint32_t nranges, uint8_t* out, uint64_t out_cap, uint64_t* out_bytes, uint64_t* range_bytes,
+                       dsss_stream_t stream);
+int dsss_varint_decode(dsss_ctx* ctx, const uint8_t* in, uint64_t nbytes, uint32_t* values, uint64_t n,
+                       dsss_stream_t stream);
+
 /* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),
  * seeded and reproducible: string i is (k - d) 'A's, the d base-26 digits
  * ('A' = 0) of pi(i) for a seeded permutation pi of [0, n), then uniform

@@ -273,6 +273,39 @@ def distribute_strings(data: bytes, p: int, max_size: int = 0):
     return out
 
 
+def varint_encode(values, range_counts):
+    """Writer::PutVarint (src/encoding/integer_compression.hpp:66-140) for every
+    value: 7 bits per byte, least significant first, the high bit on every byte
+    but the last; ranges back to back with their byte counts
+    (IntegerCompression::writeRanges, src/mpi/byte_encoder.hpp:31-53)."""
+    out, per, k = bytearray(), [], 0
+    vals = np.asarray(values).astype(np.int64)
+    for c in range_counts:
+        start = len(out)
+        for v in vals[k:k + int(c)].tolist():
+            while v >= 128:
+                out.append((v & 0x7F) | 0x80)
+                v >>= 7
+            out.append(v)
+        per.append(len(out) - start)
+        k += int(c)
+    return np.frombuffer(bytes(out), np.uint8).copy(), np.asarray(per, np.uint64)
+
+
+def varint_decode(data, n):
+    """Reader::decode (src/encoding/integer_compression.hpp) of n values."""
+    vals, v, sh = [], 0, 0
+    for b in np.asarray(data, np.uint8).tolist():
+        v |= (b & 0x7F) << sh
+        sh += 7
+        if not b & 0x80:
+            vals.append(v)
+            v, sh = 0, 0
+    if len(vals) != n or sh != 0:
+        raise ValueError("not %d whole values" % n)
+    return np.asarray(vals, np.int64)
+
+
 # ------------------------------------------------------------ reference ----
 def ref_xxh64(data: bytes) -> int:
     buf = np.frombuffer(data + b"\0", dtype=np.uint8)

@@ -178,6 +178,12 @@ class OracleBackend:
             dlcp[do:do + ns] = np.asarray(lcps)[so:so + ns]
         return dchars, dstart, dlcp
 
+    def varint_encode(self, values, range_counts):
+        return self.orc.varint_encode(values, range_counts)
+
+    def varint_decode(self, data, n):
+        return self.orc.varint_decode(data, n)
+
     def merge(self, chars, nbytes, starts, lcps, counts, offsets):
         out = {k: [] for k in ("perm_index", "perm_pe", "merged_lcp")}
         k = 0

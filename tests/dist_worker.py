@@ -20,7 +20,8 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
     from dist_oracle import HostArena, OracleBackend, pack_list
     d = __graft_entry__.load_package()
     import dsss_b200.dist as D
-    strs, pb, splits, sampler = inputs
+    strs, pb, splits, sampler = inputs[:4]
+    compress = bool(inputs[4]) if len(inputs) > 4 else False
     if pg == "nccl":
         import torch
         torch.cuda.set_device(0)
@@ -40,7 +41,7 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
             ctx = d.Context(0)
             be = D.GpuBackend(ctx)
             arena = be.strings(d.from_bytes_list(mine))
-        res = D.sort(D.Comm(), be, arena, pb_local, sampler)
+        res = D.sort(D.Comm(), be, arena, pb_local, sampler, compress_lcps=compress)
         out = {"q0": q0, "q1": q1, "s0": s0}
         nrecv = int(res.get("recv_total", 0))
         for k in ("local_order", "dp", "perm_index", "perm_pe", "merged_lcp"):

@@ -73,6 +73,15 @@ def test_two_ranks_match_oracle(orc, name, strs, sampler):
     check_against_oracle(orc, strs, pb, res, sampler)
 
 
+@pytest.mark.parametrize("name,strs", CASES[:2] + CASES[3:], ids=["random", "dups", "runs"])
+def test_two_ranks_compressed_lcps(orc, name, strs):
+    """compressLcps: the LCPs cross as varint bytes; results unchanged."""
+    n = len(strs)
+    pb = [0, n // 4, n // 2, (3 * n) // 4, n]
+    res = run_ranks(2, (strs, pb, [0, 1, 4], 0, True), "oracle")
+    check_against_oracle(orc, strs, pb, res, 0)
+
+
 def test_three_ranks_one_pe_each(orc):
     strs = CASES[0][1]
     n = len(strs)
