@@ -119,6 +119,8 @@ int dsss_distribute_lines(dsss_ctx* ctx, const uint8_t* file, uint64_t size, uin
     // slices (readInput.hpp:57-69) and the boundary after each slice's first '\n'
     std::vector<uint64_t> bound(p + 1, 0);
     const uint64_t slice = S / p, larger = S % p;
+    if (slice == 0)  // the last slice is empty: the reference reads result.back() of an empty vector
+        return fail(DSSS_EINVAL, "the file has fewer bytes (%llu) than PEs (%u)", (unsigned long long)S, p);
     for (uint32_t r = 1; r < p; ++r) {
         const uint64_t len = slice + (r < larger ? 1 : 0);
         const uint64_t off = r < larger ? len * r : larger * (slice + 1) + (r - larger) * slice;

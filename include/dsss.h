@@ -444,8 +444,9 @@ int dsss_server_destroy(dsss_server* s);
  * the closing NUL) and, when chars != NULL: chars (device, chars_cap >=
  * char_bytes + 32, the tail zeroed), offsets / lengths (device, cap_n entries)
  * of the *n lines in file order, part_begin (HOST, p + 1 line indices): an
- * arena ready for dsss_pd_sort / dsss_ms_sort.  A slice of PE r > 0 without a
- * '\n' (where the reference reads past its buffer) is an error. */
+ * arena ready for dsss_pd_sort / dsss_ms_sort.  Where the reference reads
+ * past a buffer it is an error: a slice of PE r > 0 without a '\n', or fewer
+ * bytes than PEs (an empty last slice). */
 int dsss_distribute_lines(dsss_ctx* ctx, const uint8_t* file, uint64_t size, uint64_t max_size, uint32_t p,
                           uint8_t* chars, uint64_t chars_cap, uint64_t* offsets, uint32_t* lengths, uint64_t cap_n,
                           uint64_t* n, uint64_t* char_bytes, uint64_t* part_begin, dsss_stream_t stream);

@@ -376,7 +376,10 @@ void partition(const Arena& a, uint32_t p, const uint64_t* pb, const uint64_t* o
         }
         pos.push_back(nq);
         for (uint64_t k = pos.size() - 1; k > 0; --k) pos[k] -= pos[k - 1];
-        for (uint32_t r = 0; r < p; ++r) intervals[(uint64_t)q * p + r] = pos[r];
+        // fewer than p - 1 splitters (a sample smaller than p - 1): the last
+        // bucket that has a splitter bound takes the rest, later ones none
+        // (the reference's interval vector would be shorter than p there)
+        for (uint32_t r = 0; r < p; ++r) intervals[(uint64_t)q * p + r] = r < pos.size() ? pos[r] : 0;
     }
 }
 

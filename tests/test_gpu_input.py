@@ -75,3 +75,16 @@ def test_distributed_lines_through_the_path(dsss, orc, ctx, p):
     hs = dsss.from_bytes_list([bytes(x) for x in data.split(b"\n")[:-1]])
     assert hs.n == ds.n
     check_pd(dsss, orc, hs, out, p)
+
+
+@pytest.mark.parametrize("data,p", [(b"", 1), (b"x", 1), (b"\n", 1), (b"a\nb\n", 2), (b"\n\n\n\n", 4),
+                                    (b"ab\ncd", 2)])
+def test_distribute_edges(dsss, orc, ctx, data, p):
+    try:
+        want = orc.distribute_strings(data, p)
+    except ValueError:
+        with pytest.raises(dsss.DsssError):
+            dsss.distribute_lines(ctx, data, p)
+        return
+    ds, pb = dsss.distribute_lines(ctx, data, p)
+    assert per_pe(ds, pb) == want

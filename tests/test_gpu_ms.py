@@ -68,3 +68,17 @@ def test_ms_sort_truncated_splitter(dsss, orc, ctx):
     out = dsss.ms_sort(ctx, dsss.DeviceStrings(hs), 2, part_begin=pb)
     assert np.asarray(out["intervals"]).reshape(2, 2)[0].tolist() == [999, 2001]
     check_ms(dsss, orc, hs, out, pb)
+
+
+@pytest.mark.parametrize("strs,pb", [
+    ([], [0, 0, 0]),
+    ([b"solo"], [0, 1]),
+    ([b"solo"], [0, 0, 1, 1]),                       # empty PEs around one string
+    ([b"", b"", b"a", b""], [0, 2, 4]),              # empty strings
+    ([b"b", b"a", b"c"], [0, 1, 1, 2, 2, 3]),        # p = 5 > n with empty PEs
+])
+def test_ms_sort_edges(dsss, orc, ctx, strs, pb):
+    hs = host_of(dsss, strs)
+    pb = np.asarray(pb, np.uint64)
+    out = dsss.ms_sort(ctx, dsss.DeviceStrings(hs), len(pb) - 1, part_begin=pb)
+    check_ms(dsss, orc, hs, out, pb)
