@@ -56,6 +56,12 @@ class MsResult(ctypes.Structure):
                 ("avg_lcp", ctypes.c_uint64)]
 
 
+class HqResult(ctypes.Structure):
+    _fields_ = [("counts", ctypes.c_void_p), ("chars", ctypes.c_void_p), ("chars_capacity", ctypes.c_uint64),
+                ("offsets", ctypes.c_void_p), ("lengths", ctypes.c_void_p), ("source", ctypes.c_void_p),
+                ("levels", ctypes.c_uint32)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("sort_small_max", ctypes.c_int64), ("sort_pivot", ctypes.c_int64), ("dp_filter_min", ctypes.c_int64),
                 ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("settings_tried", ctypes.c_uint32)]
@@ -95,6 +101,7 @@ _SIGS = {
     "dsss_abi_version": (_I, []),
     "dsss_pd_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult), _P]),
     "dsss_ms_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(MsResult), _P]),
+    "dsss_hq_sort": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _U64, ctypes.POINTER(HqResult), _P]),
     "dsss_distribute_lines": (_I, [_P, _P, _U64, _U64, _U32, _P, _U64, _P, _P, _U64, _P, _P, _P, _P]),
     "dsss_varint_encode": (_I, [_P, _P, _U64, _P, _U32, _P, _U64, _P, _P, _P]),
     "dsss_varint_decode": (_I, [_P, _P, _U64, _P, _U64, _P]),
@@ -425,6 +432,31 @@ def ms_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, small_sort
                              _stream_ptr(stream)))
     out["part_begin"] = pb
     out["avg_lcp"] = int(res.avg_lcp)
+    out["char_bytes"] = cap
+    return out
+
+
+HQ_SEED = 3469931  # the hQuicksort executable's seed base: PE r seeds its generator with 3469931 + r
+
+
+def hq_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, seed: int = HQ_SEED, stream=None):
+    """RQuick::sort as hQuicksort runs it, on the device: every PE's strings,
+    whole and sorted, back to back in rank order.  Returns torch tensors
+    (device: chars, offsets, lengths, source) plus host numpy counts (strings
+    per PE) and the number of hypercube levels."""
+    import torch
+    n = ds.n
+    pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
+    cap = int(ds.lengths[:n].to(torch.int64).sum().item()) + n if n else 0
+    out = dict(chars=torch.zeros(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
+               offsets=torch.empty(max(n, 1), dtype=torch.int64, device="cuda"), lengths=_empty(n),
+               source=_empty(n), counts=np.zeros(p, dtype=np.uint64))
+    res = HqResult(_ptr(out["counts"]), _ptr(out["chars"]), cap, _ptr(out["offsets"]), _ptr(out["lengths"]),
+                   _ptr(out["source"]), 0)
+    a = ds.arena()
+    check(lib().dsss_hq_sort(ctx.h, ctypes.byref(a), p, _ptr(pb), seed, ctypes.byref(res), _stream_ptr(stream)))
+    out["part_begin"] = pb
+    out["levels"] = int(res.levels)
     out["char_bytes"] = cap
     return out
 

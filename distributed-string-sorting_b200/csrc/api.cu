@@ -15,6 +15,7 @@
 //      permutation (:282-290) and merged LCPs taken from the global LCPs.
 #include <algorithm>
 #include <cstring>
+#include <random>
 #include <vector>
 
 #include "dp.cuh"
@@ -488,11 +489,297 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     return DSSS_OK;
 }
 
+// ----------------------------------------------------------- hQuicksort ----
+// RQuick::sort (sorter/RQuick/RQuick.hpp:834-1104, sortRec :415-627) as the
+// hQuicksort executable runs it, on one GPU holding every PE.  Strings never
+// move between levels: after one global sort, PE q's sorted data at a level is
+// the ascending list of global positions it owns (equal strings are
+// byte-identical, so which of them a PE holds is immaterial), the pivot and
+// each PE's split are binary searches in those lists, the exchange relabels
+// owners, and the strings are written once at the end: the PEs' sorted data
+// in rank order is the global order.
+
+// The pivot's run: PE lists are searched for the first position of the run
+// of strings equal to the pivot and the first position past it.
+__global__ void k_hq_run_ends(const uint32_t* ord, const uint32_t* lcp, ArenaDev a, uint64_t n, uint32_t* tail) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    uint32_t t = 1;
+    if (g + 1 < n) {
+        uint64_t o0, o1;
+        uint32_t l0, l1;
+        str_of(a, ord[g], o0, l0);
+        str_of(a, ord[g + 1], o1, l1);
+        t = !(l0 == l1 && lcp[g + 1] == l0);
+    }
+    tail[g] = t;
+}
+
+__global__ void k_hq_fold(uint32_t* owner, uint64_t n, uint32_t pw) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n && owner[g] >= pw) owner[g] -= pw;
+}
+
+// Strings per owner (warp-aggregated: owners come in long runs).
+__global__ void k_hq_hist(const uint32_t* owner, uint64_t n, uint32_t P, uint32_t* cnt) {
+    extern __shared__ uint32_t h[];
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint64_t g = base + threadIdx.x;
+        const uint32_t o = g < n ? owner[g] : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, o);
+        if (o < P && lane == (uint32_t)__ffs(peers) - 1) atomicAdd(&h[o], __popc(peers));
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
+        if (h[b]) atomicAdd(&cnt[b], h[b]);
+}
+
+// One level's parameters of PE q, drawn on the host from its random bits.
+struct HqPe {
+    uint64_t begin;  // start of q's list in the positions grouped by owner
+    uint32_t cnt;    // strings q holds
+    uint32_t opt;    // locateSplitter's middle: cnt / 2, + 1 by a bit when cnt is odd
+    uint32_t piv;    // first PE of a subcube: index of the pivot in its list, HQ_NONE: the empty pivot
+    uint32_t cube;   // subcube size at this level
+};
+constexpr uint32_t HQ_NONE = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint64_t first_not_below(const uint32_t* v, uint64_t m, uint64_t x) {
+    uint64_t lo = 0, hi = m;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (v[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// locateSplitter (robust, RQuick.hpp:363-385) of every PE: the split index
+// in its list, as the position where its sent part starts (left half) or its
+// kept part starts (right half); HQ_NONE past the end.  dest: the partner,
+// bit 31 set for the left half.
+__global__ void k_hq_split(const HqPe* prm, const uint32_t* pos, const uint32_t* runx, const uint32_t* ord,
+                           ArenaDev a, uint64_t n, uint32_t pw, uint32_t* cut, uint32_t* dest, uint32_t* err) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= pw) return;
+    const HqPe m = prm[q];
+    const uint32_t P = m.cube, b = q & ~(P - 1), half = P >> 1;
+    const HqPe r = prm[b];
+    uint64_t lo = 0, hi = 0;
+    if (r.piv == HQ_NONE) {  // the empty string: every empty string equals it
+        uint64_t o;
+        uint32_t l;
+        str_of(a, ord[0], o, l);
+        hi = l == 0 ? first_not_below(runx, n, 1) : 0;
+    } else {
+        if (r.piv >= r.cnt) {
+            atomicExch(err, 1u);
+            return;
+        }
+        const uint32_t k = runx[pos[r.begin + r.piv]];
+        lo = first_not_below(runx, n, k);
+        hi = first_not_below(runx, n, (uint64_t)k + 1);
+    }
+    const uint32_t* v = pos + m.begin;
+    const uint64_t lb = first_not_below(v, m.cnt, lo), ub = first_not_below(v, m.cnt, hi);
+    const uint64_t sep = lb < m.opt ? min((uint64_t)m.opt, ub) : lb;
+    cut[q] = sep < m.cnt ? v[sep] : HQ_NONE;
+    const bool left = q - b < half;
+    dest[q] = (b + (q - b + half) % P) | (left ? 0x80000000u : 0u);
+}
+
+// The exchange: the left half sends its strings from the split on, the right
+// half those before it.
+__global__ void k_hq_move(uint32_t* owner, uint64_t n, uint32_t pw, const uint32_t* cut, const uint32_t* dest) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t q = owner[g];
+    if (q >= pw) return;
+    const uint32_t c = cut[q], d = dest[q];
+    const bool left = d >> 31;
+    if (left ? (c != HQ_NONE && g >= c) : (c == HQ_NONE || g < c)) owner[g] = d & 0x7FFFFFFFu;
+}
+
+// RandomBitStore (sorter/RQuick/RandomBitStore.hpp:27-52) on PE q's
+// std::mt19937_64.
+struct HqBits {
+    std::mt19937_64 gen;
+    uint64_t bits = 0;
+    int pos = 64;
+    uint32_t next() {
+        if (pos == 64) {
+            bits = gen();
+            pos = 0;
+        }
+        const uint32_t r = (uint32_t)(bits & 1);
+        bits >>= 1;
+        ++pos;
+        return r;
+    }
+};
+
+static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* pb, uint64_t seed,
+                       dsss_hq_result* out, cudaStream_t st) {
+    DSSS_TRY(check_arena(in));
+    if (p == 0) return fail(DSSS_EINVAL, "p must be >= 1");
+    if (p > MAX_SPLIT_BUCKETS) return fail(DSSS_ENOTSUP, "p > %u PEs per GPU is not supported", MAX_SPLIT_BUCKETS);
+    DSSS_TRY(check_parts(p, pb, in->n));
+    if (!out || !out->counts || !out->offsets || !out->lengths || (in->n && !out->chars))
+        return fail(DSSS_EINVAL, "result arrays missing");
+    const uint64_t n = in->n;
+    uint32_t pw = 1, levels = 0;
+    while (pw * 2 <= p) pw *= 2, ++levels;
+    out->levels = levels;
+    for (uint32_t q = 0; q < p; ++q) out->counts[q] = 0;
+    if (n == 0) return DSSS_OK;
+    const uint64_t N = n;
+    const uint32_t smax = 0;
+    auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint32_t*& owner, uint32_t*& pos,
+                    uint32_t*& runx, uint32_t*& cnt, HqPe*& prm, uint32_t*& cut, uint32_t*& dest, uint32_t*& err,
+                    uint64_t*& pbd, uint64_t*& total, void*& scan, void*& ms, SortLayout& sl) {
+        handles = c.take<ulonglong2>(N);
+        ord = c.take<uint32_t>(N);
+        lcp = c.take<uint32_t>(N);
+        owner = c.take<uint32_t>(N);
+        pos = c.take<uint32_t>(N);
+        runx = c.take<uint32_t>(N);
+        cnt = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
+        prm = c.take<HqPe>(MAX_SPLIT_BUCKETS);
+        cut = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
+        dest = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
+        err = c.take<uint32_t>(1);
+        pbd = c.take<uint64_t>(p + 1);
+        total = c.take<uint64_t>(2);
+        scan = c.take<unsigned char>(scan_scratch_bytes(N));
+        ms = c.take<unsigned char>(multisplit_scratch_bytes(N, pw));
+        layout_sort(c, sl, N, 1, smax);
+    };
+    ulonglong2* handles;
+    uint32_t *ord, *lcp, *owner, *pos, *runx, *cnt, *cut, *dest, *err;
+    HqPe* prm;
+    uint64_t *pbd, *total;
+    void *scan, *ms;
+    SortLayout sl;
+    Carve sz(nullptr);
+    plan(sz, handles, ord, lcp, owner, pos, runx, cnt, prm, cut, dest, err, pbd, total, scan, ms, sl);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    const uint64_t pin_bytes = MAX_SPLIT_BUCKETS * (sizeof(uint32_t) + sizeof(HqPe)) + 64;
+    DSSS_TRY(ensure_pin(ctx, pin_bytes < 4096 ? 4096 : pin_bytes));
+    Carve c(ctx->ws);
+    plan(c, handles, ord, lcp, owner, pos, runx, cnt, prm, cut, dest, err, pbd, total, scan, ms, sl);
+    ArenaDev a = view(in);
+    make_handles(a, handles, st);
+    a.h = handles;
+    DSSS_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+    const uint64_t set_begin[2] = {0, n};
+    {
+        StageTimer t("stage:sort", st);
+        DSSS_TRY(sort_strings(sl, a, n, 1, set_begin, nullptr, ord, lcp, smax, (uint32_t*)ctx->pin, st));
+    }
+    {
+        StageTimer t("stage:levels", st);
+        DSSS_CUDA(cudaMemcpyAsync(pbd, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
+        DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(ord, n, pbd, p, owner));
+        if (pw < p) DSSS_LAUNCH("k_hq_fold", st, k_hq_fold<<<grid_for(n, 256), 256, 0, st>>>(owner, n, pw));
+        if (levels) {
+            DSSS_LAUNCH("k_hq_run_ends", st, k_hq_run_ends<<<grid_for(n, 256), 256, 0, st>>>(ord, lcp, a, n, pos));
+            DSSS_TRY(exclusive_scan_u32(pos, runx, n, nullptr, scan, st));
+        }
+        std::vector<HqBits> bits(pw);
+        for (uint32_t q = 0; q < pw; ++q) bits[q].gen.seed(seed + q);  // HQuicksort.cpp:344-345
+        uint32_t* hcnt = (uint32_t*)ctx->pin;
+        HqPe* hprm = (HqPe*)((char*)ctx->pin + MAX_SPLIT_BUCKETS * sizeof(uint32_t));
+        const int hist_grid = 148 * 4;
+        for (uint32_t P = pw; P >= 2; P >>= 1) {
+            DSSS_CUDA(cudaMemsetAsync(cnt, 0, pw * sizeof(uint32_t), st));
+            DSSS_LAUNCH("k_hq_hist", st,
+                        k_hq_hist<<<hist_grid, 256, pw * sizeof(uint32_t), st>>>(owner, n, pw, cnt));
+            DSSS_CUDA(cudaMemcpyAsync(hcnt, cnt, pw * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            {
+                const uint32_t* ins[1] = {nullptr};
+                uint32_t* outs[1] = {pos};
+                DSSS_TRY(multisplit_payload(owner, n, pw, 1, ins, outs, nullptr, err, ms, st));
+            }
+            DSSS_CUDA(cudaStreamSynchronize(st));
+            // the bits in the reference's order per PE: middleMostElements
+            // (:273-314), the first PE's selectMedian
+            // (BinTreeMedianSelection.hpp:135-152), locateSplitter (:363-385)
+            uint64_t begin = 0;
+            for (uint32_t q = 0; q < pw; ++q) {
+                const uint32_t k = hcnt[q];
+                HqPe& m = hprm[q];
+                m.begin = begin;
+                m.cnt = k;
+                m.cube = P;
+                m.piv = HQ_NONE;
+                begin += k;
+                const uint32_t beg = k > 2 ? (k - 2) / 2 + (k % 2 == 1 ? bits[q].next() : 0u) : 0u;
+                if (q % P == 0) {
+                    const uint32_t nm = k < 2 ? k : 2;
+                    if (nm) m.piv = beg + (nm == 2 ? bits[q].next() : 0u);
+                }
+                m.opt = k / 2 + (k % 2 == 1 ? bits[q].next() : 0u);
+            }
+            if (begin != n) return fail(DSSS_EDEVICE, "hq sort: owner counts add up to %llu, not %llu",
+                                        (unsigned long long)begin, (unsigned long long)n);
+            DSSS_CUDA(cudaMemcpyAsync(prm, hprm, pw * sizeof(HqPe), cudaMemcpyHostToDevice, st));
+            DSSS_LAUNCH("k_hq_split", st,
+                        k_hq_split<<<grid_for(pw, 128), 128, 0, st>>>(prm, pos, runx, ord, a, n, pw, cut, dest, err));
+            DSSS_LAUNCH("k_hq_move", st, k_hq_move<<<grid_for(n, 256), 256, 0, st>>>(owner, n, pw, cut, dest));
+            // the pinned parameters are rewritten only after the next level's
+            // count read-back, which the stream orders after this copy
+        }
+        DSSS_CUDA(cudaMemsetAsync(cnt, 0, pw * sizeof(uint32_t), st));
+        DSSS_LAUNCH("k_hq_hist", st, k_hq_hist<<<hist_grid, 256, pw * sizeof(uint32_t), st>>>(owner, n, pw, cnt));
+        DSSS_CUDA(cudaMemcpyAsync(hcnt, cnt, pw * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        uint64_t sum = 0;
+        for (uint32_t q = 0; q < pw; ++q) sum += out->counts[q] = hcnt[q];
+        if (sum != n) return fail(DSSS_EDEVICE, "hq sort: final counts add up to %llu, not %llu",
+                                  (unsigned long long)sum, (unsigned long long)n);
+    }
+    // the strings in the global order, back to back
+    {
+        StageTimer t("stage:copy", st);
+        uint32_t* source = out->source ? out->source : lcp;
+        uint32_t* len1 = runx;
+        DSSS_LAUNCH("k_ms_source", st,
+                    k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(ord, nullptr, nullptr, nullptr, a, n, source,
+                                                                 out->lengths, len1));
+        DSSS_TRY(exclusive_scan_u32_to_u64(len1, out->offsets, n, total, scan, st));
+        DSSS_CUDA(cudaMemcpyAsync(ctx->pin, total, 8, cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        const uint64_t bytes = *(const uint64_t*)ctx->pin;
+        if (bytes > out->chars_capacity)
+            return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
+                        (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
+        DSSS_LAUNCH("k_ms_copy", st,
+                    k_ms_copy<<<grid_for(n * MS_COPY_LANES, 256), 256, 0, st>>>(a, source, out->offsets, n,
+                                                                                out->chars));
+    }
+    DSSS_CUDA(cudaMemcpyAsync(ctx->pin, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    if (*(const uint32_t*)ctx->pin) return fail(DSSS_EDEVICE, "hq sort: internal consistency guard tripped");
+    return DSSS_OK;
+}
+
 }  // namespace dsss
 
 using namespace dsss;
 
 extern "C" {
+
+int dsss_hq_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, uint64_t seed,
+                 dsss_hq_result* out, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    return hq_sort_dev(ctx, in, p, part_begin, seed, out, (cudaStream_t)stream);
+}
 
 int dsss_ms_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, const dsss_opts* opts,
                  dsss_ms_result* out, dsss_stream_t stream) {

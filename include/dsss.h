@@ -190,6 +190,33 @@ typedef struct dsss_ms_result {
 int dsss_ms_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin,
                  const dsss_opts* opts, dsss_ms_result* out, dsss_stream_t stream);
 
+/* Outputs of hQuicksort: the PEs' sorted strings back to back in rank order,
+ * device arrays of n entries unless noted. */
+typedef struct dsss_hq_result {
+    uint64_t* counts;         /* HOST [p]: strings PE r holds after the sort */
+    uint8_t* chars;           /* the output strings, each followed by a NUL */
+    uint64_t chars_capacity;  /* bytes at chars: at least the sum of (length + 1) */
+    uint64_t* offsets;        /* start of each output string in chars */
+    uint32_t* lengths;        /* length of each output string */
+    uint32_t* source;         /* optional: input index of each output string */
+    uint32_t levels;          /* set by the call: hypercube levels (log2 of the largest power of two <= p) */
+} dsss_hq_result;
+
+/* RQuick::sort (src/sorter/RQuick/RQuick.hpp:1109-1115 -> :834-1104, sortRec
+ * :415-627) as the hQuicksort executable runs it
+ * (src/executables/HQuicksort.cpp:307-358: robust, StringComparator, PE r's
+ * std::mt19937_64 seeded with seed + r; the executable passes 3469931): PEs
+ * past the largest power of two hand their strings to PE r - 2^k, each PE
+ * sorts, and every hypercube level splits each subcube at a pivot (one of the
+ * subcube's first PE's two middle strings) with random tie-breaking and
+ * exchanges halves with the partner PE.  The counts and the strings of every
+ * PE are the reference's, bit for bit.  Byte-identical strings are
+ * indistinguishable in this output; `source` names them in global order.
+ * One GPU holds all PEs: the levels relabel string owners on one global sort
+ * and the strings are written once. */
+int dsss_hq_sort(dsss_ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* part_begin, uint64_t seed,
+                 dsss_hq_result* out, dsss_stream_t stream);
+
 /* Batched form (no reference counterpart: the reference sorts one string set
  * per MPI job): nsets independent string sets of p PEs each in one arena, run
  * through one pipeline.  part_begin has nsets*p + 1 entries; PE q of set s

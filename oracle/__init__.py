@@ -57,6 +57,8 @@ def lib():
         L.oracle_pd_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.oracle_ms_sort.restype = _I
         L.oracle_ms_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.oracle_hq_sort.restype = _I
+        L.oracle_hq_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _U64, _P, _P]
         _lib = L
     return _lib
 
@@ -229,6 +231,22 @@ def ms_sort(s: Strings, pb):
     o["intervals"] = o["intervals"].reshape(p, p)
     o["avg_lcp"] = int(avg[0])
     return o
+
+
+HQ_SEED = 3469931  # HQuicksort.cpp:344: PE r seeds its generator with 3469931 + r
+
+
+def hq_sort(s: Strings, pb, seed: int = HQ_SEED):
+    """RQuick::sort as hQuicksort runs it (oracle_hq_sort): source = string id
+    of every output string, PEs back to back; counts = strings per PE."""
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    n = s.n
+    src = np.zeros(max(n, 1), np.uint64)
+    counts = np.zeros(p, np.uint64)
+    rc = lib().oracle_hq_sort(*s.args(), p, _p(pb), seed, _p(src), _p(counts))
+    assert rc == 0
+    return dict(source=src[:n], counts=counts)
 
 
 def distribute_strings(data: bytes, p: int, max_size: int = 0):

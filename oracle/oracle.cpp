@@ -11,6 +11,12 @@
 // BloomFilter/computeDistinguishingPrefixes at one PE, LcpStringLoserTree_)
 // and against the reference's PD-exchange known-answer test
 // (src/tests/alltoallStrings_tests.cpp:129-163) via tests/golden/.
+// oracle_hq_sort (RQuick, the hQuicksort competitor) is unpinned against the
+// reference's binary (RQuick needs MPI, not available here); its random bits
+// come from std::mt19937_64 as the reference's do, and the tests check it
+// against a second, pure-Python restatement with its own MT19937-64 (pinned
+// to the C++ standard's known answer) and against the reference
+// executable's own check (the PEs' outputs in rank order are the sorted input).
 //
 // Strings are (offset, length) views into one byte arena; bytes at or past a
 // string's length read as 0, which is exactly the NUL terminator the
@@ -19,6 +25,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <random>
 #include <vector>
 
 namespace {
@@ -671,6 +678,107 @@ int oracle_ms_sort(const uint8_t* chars, const uint64_t* off, const uint32_t* le
             source[o] = order[pb[pe[k]] + idx[k]];
             out_lcp[o] = ml[k];
         }
+    }
+    return 0;
+}
+
+// --------------------------------------------------------------- RQuick ----
+// RQuick::sort as the hQuicksort executable runs it
+// (src/executables/HQuicksort.cpp:307-358: robust, non-indexed strings, PE r's
+// std::mt19937_64 seeded with 3469931 + r at :344-345) on p simulated PEs:
+// sorter/RQuick/RQuick.hpp:834-1104 (sort) and :415-627 (sortRec).  The PEs'
+// string lists hold string ids; strings compare as the executable's
+// StringComparator (HQuicksort.cpp:27-42) does: bytes until the first
+// difference or NUL.
+int oracle_hq_sort(const uint8_t* chars, const uint64_t* off, const uint32_t* len, uint64_t n, uint32_t p,
+                   const uint64_t* pb, uint64_t seed, uint64_t* source, uint64_t* counts) {
+    (void)n;
+    // a string, or the empty pivot getRawString(-1) returns (stringcontainer.hpp:582-585)
+    struct Key { const uint8_t* c; uint32_t l; };
+    auto key = [&](uint64_t id) { return Key{chars + off[id], len[id]}; };
+    auto less = [](const Key& x, const Key& y) {
+        const uint32_t m = std::min(x.l, y.l);
+        const int c = m ? std::memcmp(x.c, y.c, m) : 0;
+        return c ? c < 0 : x.l < y.l;
+    };
+    auto id_less = [&](uint64_t x, uint64_t y) { return less(key(x), key(y)); };
+    std::vector<std::vector<uint64_t>> pe(p);
+    for (uint32_t q = 0; q < p; ++q)
+        for (uint64_t i = pb[q]; i < pb[q + 1]; ++i) pe[q].push_back(i);
+    uint32_t pw = 1;
+    while (pw * 2 <= p) pw *= 2;
+    // PEs past the largest power of two hand their strings down (RQuick.hpp:878-959)
+    for (uint32_t q = pw; q < p; ++q) {
+        pe[q - pw].insert(pe[q - pw].end(), pe[q].begin(), pe[q].end());
+        pe[q].clear();
+    }
+    for (uint32_t q = 0; q < pw; ++q) std::sort(pe[q].begin(), pe[q].end(), id_less);  // sortLocally
+    // RandomBitStore (RandomBitStore.hpp:27-52): 64 bits per draw, lowest first
+    struct Bits {
+        std::mt19937_64 gen;
+        uint64_t bits = 0;
+        int pos = 64;
+        uint64_t next() {
+            if (pos == 64) { bits = gen(); pos = 0; }
+            const uint64_t r = bits & 1;
+            bits >>= 1;
+            ++pos;
+            return r;
+        }
+    };
+    std::vector<Bits> bs(pw);
+    for (uint32_t q = 0; q < pw; ++q) bs[q].gen.seed(seed + q);
+    std::vector<uint64_t> beg(pw), sep(pw);
+    for (uint32_t P = pw; P >= 2; P /= 2) {  // one level per halving of the subcube (:600-623)
+        for (uint32_t b = 0; b < pw; b += P) {
+            // selectSplitter: every PE's two middle-most strings (middleMostElements, RQuick.hpp:273-314)
+            for (uint32_t q = b; q < b + P; ++q) {
+                const uint64_t c = pe[q].size();
+                beg[q] = c > 2 ? (c - 2) / 2 + (c % 2 == 1 ? bs[q].next() : 0) : 0;
+            }
+            // BinTreeMedianSelection::select (BinTreeMedianSelection.hpp:157-226):
+            // selectMedians builds both of its containers from its own input
+            // (:61-62; the second is the moved-from, empty vector), so the
+            // medians received are dropped and the subcube's first PE picks
+            // among its own (selectMedian :135-152: one of two by a bit)
+            const uint64_t m = std::min<uint64_t>(pe[b].size(), 2);
+            Key piv{chars, 0};
+            if (m) piv = key(pe[b][beg[b] + (m == 2 ? bs[b].next() : 0)]);
+            // locateSplitter, robust (RQuick.hpp:363-385)
+            for (uint32_t q = b; q < b + P; ++q) {
+                const std::vector<uint64_t>& v = pe[q];
+                const uint64_t c = v.size();
+                const uint64_t lo = std::lower_bound(v.begin(), v.end(), piv, [&](uint64_t x, const Key& k) {
+                                        return less(key(x), k);
+                                    }) - v.begin();
+                const uint64_t hi = std::upper_bound(v.begin() + lo, v.end(), piv, [&](const Key& k, uint64_t x) {
+                                        return less(k, key(x));
+                                    }) - v.begin();
+                const uint64_t opt = c / 2 + (c % 2 == 1 ? bs[q].next() : 0);
+                sep[q] = lo < opt ? std::min(opt, hi) : lo;
+            }
+            // the left half keeps the small strings, the right half the large;
+            // each merges what its partner sends after its own (RQuick.hpp:496-586)
+            std::vector<std::vector<uint64_t>> next(P);
+            for (uint32_t q = b; q < b + P; ++q) {
+                const uint32_t r = b + (q - b + P / 2) % P;
+                const bool left = q - b < P / 2;
+                const std::vector<uint64_t>& v = pe[q];
+                const std::vector<uint64_t>& w = pe[r];
+                std::vector<uint64_t> own = left ? std::vector<uint64_t>(v.begin(), v.begin() + sep[q])
+                                                 : std::vector<uint64_t>(v.begin() + sep[q], v.end());
+                std::vector<uint64_t> got = left ? std::vector<uint64_t>(w.begin(), w.begin() + sep[r])
+                                                 : std::vector<uint64_t>(w.begin() + sep[r], w.end());
+                next[q - b].resize(own.size() + got.size());
+                std::merge(own.begin(), own.end(), got.begin(), got.end(), next[q - b].begin(), id_less);
+            }
+            for (uint32_t q = b; q < b + P; ++q) pe[q] = std::move(next[q - b]);
+        }
+    }
+    uint64_t o = 0;
+    for (uint32_t q = 0; q < p; ++q) {
+        counts[q] = pe[q].size();
+        for (uint64_t id : pe[q]) source[o++] = id;
     }
     return 0;
 }
