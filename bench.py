@@ -17,6 +17,8 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   roofline_sort  the string sort stage (K3) the same way: D + 20 n (D = sum of
             DP lengths, 8 B id read + 8 B id write + 4 B LCP write per string)
   ms_path   the merge-sort path (dsss_ms_sort) on the same input, device-timed
+  hq_path   hQuicksort (dsss_hq_sort, the reference's RQuick competitor) on
+            the same input, device-timed
   cpu_baseline  the oracle port of the reference path on the host
 
 --impl reference times the CPU port of the reference path (oracle/) on all
@@ -351,6 +353,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-ms", action="store_true", help="skip the merge-sort path line")
+    ap.add_argument("--no-hq", action="store_true", help="skip the hQuicksort line")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dist"],
                     help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL)")
@@ -498,6 +501,40 @@ def main():
         del mout
         out = None
 
+    # hQuicksort (dsss_hq_sort) on the same input, device-timed
+    hq_path = None
+    if world == 1 and not args.no_hq:
+        out = None
+        torch.cuda.empty_cache()
+        hout = None
+        for _ in range(2):
+            hout = d.hq_sort(ctx, ds, p)
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        hsteps = max(3, min(args.steps, 10))
+        for _ in range(hsteps):
+            hout = d.hq_sort(ctx, ds, p)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        hms = h0.elapsed_time(h1) / hsteps
+        cnt = np.asarray(hout["counts"], np.int64)
+        ctx.set_timing(True)
+        for _ in range(3):
+            hout = d.hq_sort(ctx, ds, p)
+        torch.cuda.synchronize()
+        hkt = ctx.kernel_times()
+        ctx.set_timing(False)
+        hq_stages = {k2[6:]: round(v[1] / 3, 4) for k2, v in hkt.items() if k2.startswith("stage:")}
+        hq_kernels = {k2: round(v[1] / 3, 4) for k2, v in sorted(hkt.items(), key=lambda x: -x[1][1])
+                      if not k2.startswith("stage:")}
+        hq_path = {"workload": desc + ", hQuicksort (RQuick, seed 3469931 + rank; whole strings per PE)",
+                   "steps": hsteps, "ms_per_call": hms, "strings_per_s": n / (hms * 1e-3),
+                   "levels": hout["levels"], "out_char_bytes": hout["char_bytes"],
+                   "pe_strings_min": int(cnt.min()), "pe_strings_max": int(cnt.max()),
+                   "stages_ms": hq_stages, "kernels_ms": dict(list(hq_kernels.items())[:12])}
+        del hout
+
     ctx.close()
     del ds, out
     torch.cuda.empty_cache()
@@ -540,6 +577,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "ms_path": ms_path,
+            "hq_path": hq_path,
             "batched": batched,
             "serving": serving,
         }

@@ -570,7 +570,7 @@ def pd_sort_batched_host(ctx: Context, hs: HostStrings, nsets: int, p: int, part
 
 
 TUNE_KNOBS = ("dp_filter_min", "dp_filter_bits", "sort_small_max", "sort_pivot", "dp_table", "sort_graph_max_n", "merge_by_sort",
-              "merge_extend_lanes", "dp_split")
+              "merge_extend_lanes", "dp_split", "copy_word")
 
 
 def tune_set(name: str, value: int):

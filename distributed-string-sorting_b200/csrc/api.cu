@@ -333,8 +333,11 @@ __global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, con
 }
 
 // Whole output strings and their NULs, MS_COPY_LANES lanes per string
-// (copy_words: aligned 8-byte stores; 8 lanes measured faster than 4 or 32).
+// (copy_words16: aligned 16-byte stores, 3.5% faster on B200 than
+// copy_words' 8-byte ones, which the knob copy_word = 8 selects; 8 lanes
+// measured faster than 4 or 32).
 constexpr uint32_t MS_COPY_LANES = 8;
+template <uint32_t W>
 __global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* out_off, uint64_t n, uint8_t* out) {
     const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MS_COPY_LANES;
     const uint32_t lane = threadIdx.x % MS_COPY_LANES;
@@ -343,8 +346,19 @@ __global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* ou
     uint32_t len;
     str_of(a, source[o], off, len);
     uint8_t* dst = out + out_off[o];
-    copy_words<MS_COPY_LANES>(dst, a.chars + off, len, lane);
+    if (W == 16) copy_words16<MS_COPY_LANES>(dst, a.chars + off, len, lane);
+    else copy_words<MS_COPY_LANES>(dst, a.chars + off, len, lane);
     if (lane == 0) dst[len] = 0;
+}
+
+static int launch_ms_copy(const ArenaDev& a, const uint32_t* source, const uint64_t* out_off, uint64_t n,
+                          uint8_t* out, cudaStream_t st) {
+    const unsigned grid = grid_for(n * MS_COPY_LANES, 256);
+    if (tune(TUNE_COPY_WORD) == 16)
+        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<16><<<grid, 256, 0, st>>>(a, source, out_off, n, out));
+    else
+        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<8><<<grid, 256, 0, st>>>(a, source, out_off, n, out));
+    return DSSS_OK;
 }
 
 static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_t* pb, const dsss_opts* opts,
@@ -478,9 +492,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         if (bytes > out->chars_capacity)
             return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
                         (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
-        DSSS_LAUNCH("k_ms_copy", st,
-                    k_ms_copy<<<grid_for(n * MS_COPY_LANES, 256), 256, 0, st>>>(a, source, out->offsets, n,
-                                                                                out->chars));
+        DSSS_TRY(launch_ms_copy(a, source, out->offsets, n, out->chars, st));
     }
     pin = (uint32_t*)ctx->pin;
     DSSS_CUDA(cudaMemcpyAsync(pin, L.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -494,25 +506,23 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
 // hQuicksort executable runs it, on one GPU holding every PE.  Strings never
 // move between levels: after one global sort, PE q's sorted data at a level is
 // the ascending list of global positions it owns (equal strings are
-// byte-identical, so which of them a PE holds is immaterial), the pivot and
-// each PE's split are binary searches in those lists, the exchange relabels
-// owners, and the strings are written once at the end: the PEs' sorted data
-// in rank order is the global order.
+// byte-identical, so which of them a PE holds is immaterial), the exchange
+// relabels owners, and the strings are written once at the end: the PEs'
+// sorted data in rank order is the global order.  The lists are never built:
+// per-tile owner counts, scanned PE-major, give every list's start and the
+// rank of every tile in it, so the pivot and each PE's split are a binary
+// search over tiles plus a scan of one tile.
 
-// The pivot's run: PE lists are searched for the first position of the run
-// of strings equal to the pivot and the first position past it.
-__global__ void k_hq_run_ends(const uint32_t* ord, const uint32_t* lcp, ArenaDev a, uint64_t n, uint32_t* tail) {
+constexpr uint32_t HQ_NT = 256, HQ_IPT = 16, HQ_TILE = HQ_NT * HQ_IPT;
+constexpr uint32_t HQ_NONE = 0xFFFFFFFFu;
+
+// The pivot's run: lists are searched for the first position of the run of
+// strings equal to the pivot and the first position past it.
+// glen: lengths in the global order.
+__global__ void k_hq_run_ends(const uint32_t* glen, const uint32_t* lcp, uint64_t n, uint32_t* tail) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    uint32_t t = 1;
-    if (g + 1 < n) {
-        uint64_t o0, o1;
-        uint32_t l0, l1;
-        str_of(a, ord[g], o0, l0);
-        str_of(a, ord[g + 1], o1, l1);
-        t = !(l0 == l1 && lcp[g + 1] == l0);
-    }
-    tail[g] = t;
+    tail[g] = g + 1 < n ? !(glen[g] == glen[g + 1] && lcp[g + 1] == glen[g]) : 1u;
 }
 
 __global__ void k_hq_fold(uint32_t* owner, uint64_t n, uint32_t pw) {
@@ -520,33 +530,75 @@ __global__ void k_hq_fold(uint32_t* owner, uint64_t n, uint32_t pw) {
     if (g < n && owner[g] >= pw) owner[g] -= pw;
 }
 
-// Strings per owner (warp-aggregated: owners come in long runs).
-__global__ void k_hq_hist(const uint32_t* owner, uint64_t n, uint32_t P, uint32_t* cnt) {
+// Adds owner o of this lane to the shared histogram, one atomic per owner
+// and warp (owners come in long runs).
+__device__ __forceinline__ void hq_count(uint32_t* h, uint32_t o, uint32_t pw) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, o);
+    if (o < pw && (threadIdx.x & 31) == (uint32_t)__ffs(peers) - 1) atomicAdd(&h[o], __popc(peers));
+}
+
+// Owner counts of every tile, PE-major: tc[q * tiles + t].
+__global__ void __launch_bounds__(HQ_NT) k_hq_tile_hist(const uint32_t* owner, uint64_t n, uint32_t pw, uint64_t tiles,
+                                                        uint32_t* tc) {
     extern __shared__ uint32_t h[];
-    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) h[b] = 0;
+    for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) h[q] = 0;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const uint64_t g = base + threadIdx.x;
-        const uint32_t o = g < n ? owner[g] : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, o);
-        if (o < P && lane == (uint32_t)__ffs(peers) - 1) atomicAdd(&h[o], __popc(peers));
+    const uint64_t t0 = (uint64_t)blockIdx.x * HQ_TILE;
+#pragma unroll 4
+    for (uint32_t j = 0; j < HQ_IPT; ++j) {
+        const uint64_t g = t0 + j * HQ_NT + threadIdx.x;
+        hq_count(h, g < n ? owner[g] : HQ_NONE, pw);
     }
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
-        if (h[b]) atomicAdd(&cnt[b], h[b]);
+    for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) tc[(uint64_t)q * tiles + blockIdx.x] = h[q];
+}
+
+// The exchange (RQuick.hpp:496-586): the left half sends its strings from its
+// split on, the right half those before it; dest[q] is q's partner, bit 31 set
+// for the left half, cut[q] the position of q's split (HQ_NONE: past its
+// end).  The new owners' tile counts are those of the next level.
+__global__ void __launch_bounds__(HQ_NT) k_hq_move(uint32_t* owner, uint64_t n, uint32_t pw, uint64_t tiles,
+                                                   const uint32_t* cut, const uint32_t* dest, uint32_t* tc) {
+    extern __shared__ uint32_t h[];
+    for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) h[q] = 0;
+    __syncthreads();
+    const uint64_t t0 = (uint64_t)blockIdx.x * HQ_TILE;
+#pragma unroll 4
+    for (uint32_t j = 0; j < HQ_IPT; ++j) {
+        const uint64_t g = t0 + j * HQ_NT + threadIdx.x;
+        uint32_t o = HQ_NONE;
+        if (g < n) {
+            o = owner[g];
+            if (o < pw) {
+                const uint32_t c = cut[o], d = dest[o];
+                if ((d >> 31) ? (c != HQ_NONE && g >= c) : (c == HQ_NONE || g < c)) {
+                    o = d & 0x7FFFFFFFu;
+                    owner[g] = o;
+                }
+            }
+        }
+        hq_count(h, o, pw);
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) tc[(uint64_t)q * tiles + blockIdx.x] = h[q];
+}
+
+// Strings per PE from the scanned tile counts (off[pw * tiles] is not held:
+// the last PE ends at n).
+__global__ void k_hq_counts(const uint32_t* off, uint64_t tiles, uint32_t pw, uint64_t n, uint32_t* cnt) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= pw) return;
+    const uint64_t e = q + 1 < pw ? off[(uint64_t)(q + 1) * tiles] : n;
+    cnt[q] = (uint32_t)(e - off[(uint64_t)q * tiles]);
 }
 
 // One level's parameters of PE q, drawn on the host from its random bits.
 struct HqPe {
-    uint64_t begin;  // start of q's list in the positions grouped by owner
-    uint32_t cnt;    // strings q holds
-    uint32_t opt;    // locateSplitter's middle: cnt / 2, + 1 by a bit when cnt is odd
-    uint32_t piv;    // first PE of a subcube: index of the pivot in its list, HQ_NONE: the empty pivot
-    uint32_t cube;   // subcube size at this level
+    uint32_t cnt;   // strings q holds
+    uint32_t opt;   // locateSplitter's middle: cnt / 2, + 1 by a bit when cnt is odd
+    uint32_t piv;   // first PE of a subcube: index of the pivot in its list, HQ_NONE: the empty pivot
+    uint32_t cube;  // subcube size at this level
 };
-constexpr uint32_t HQ_NONE = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint64_t first_not_below(const uint32_t* v, uint64_t m, uint64_t x) {
     uint64_t lo = 0, hi = m;
@@ -558,14 +610,82 @@ __device__ __forceinline__ uint64_t first_not_below(const uint32_t* v, uint64_t 
     return lo;
 }
 
-// locateSplitter (robust, RQuick.hpp:363-385) of every PE: the split index
-// in its list, as the position where its sent part starts (left half) or its
-// kept part starts (right half); HQ_NONE past the end.  dest: the partner,
-// bit 31 set for the left half.
-__global__ void k_hq_split(const HqPe* prm, const uint32_t* pos, const uint32_t* runx, const uint32_t* ord,
-                           ArenaDev a, uint64_t n, uint32_t pw, uint32_t* cut, uint32_t* dest, uint32_t* err) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= pw) return;
+// Block sum and exclusive block scan (HQ_NT threads; sh: HQ_NT / 32 + 1 words).
+__device__ __forceinline__ uint32_t hq_block_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    uint32_t pre = x - v, tot = 0;
+    for (uint32_t k = 0; k < HQ_NT / 32; ++k) {
+        if (k < w) pre += sh[k];
+        tot += sh[k];
+    }
+    __syncthreads();
+    total = tot;
+    return pre;
+}
+
+// Strings of PE q at positions below x (its list's lower bound of x).
+__device__ uint32_t hq_rank(const uint32_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
+                            uint32_t cnt, uint64_t x, uint32_t* sh) {
+    if (x >= n) return cnt;
+    const uint64_t t = x / HQ_TILE, t0 = t * HQ_TILE;
+    uint32_t c = 0;
+    for (uint32_t j = 0; j < HQ_IPT; ++j) {
+        const uint64_t g = t0 + j * HQ_NT + threadIdx.x;
+        c += g < x && owner[g] == q;
+    }
+    uint32_t total;
+    hq_block_scan(c, sh, total);
+    return off[(uint64_t)q * tiles + t] - off[(uint64_t)q * tiles] + total;
+}
+
+// Position of the k-th string (from 0, k < its count) of PE q's list.
+__device__ uint32_t hq_select(const uint32_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
+                              uint32_t k, uint32_t* sh) {
+    const uint32_t* row = off + (uint64_t)q * tiles;
+    const uint32_t b = row[0];
+    uint64_t lo = 0, hi = tiles;  // the last tile whose list rank is <= k
+    while (hi - lo > 1) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (row[mid] - b <= k) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t r = k - (row[lo] - b);
+    const uint64_t g0 = lo * HQ_TILE + (uint64_t)threadIdx.x * HQ_IPT;
+    uint32_t c = 0;
+    for (uint32_t j = 0; j < HQ_IPT; ++j) c += g0 + j < n && owner[g0 + j] == q;
+    uint32_t total;
+    uint32_t pre = hq_block_scan(c, sh, total);
+    if (threadIdx.x == 0) sh[HQ_NT / 32] = HQ_NONE;
+    __syncthreads();
+    if (r >= pre && r < pre + c)
+        for (uint32_t j = 0; j < HQ_IPT; ++j)
+            if (g0 + j < n && owner[g0 + j] == q) {
+                if (pre == r) sh[HQ_NT / 32] = (uint32_t)(g0 + j);
+                ++pre;
+            }
+    __syncthreads();
+    const uint32_t v = sh[HQ_NT / 32];
+    __syncthreads();
+    return v;
+}
+
+// locateSplitter (robust, RQuick.hpp:363-385) of PE q = blockIdx.x: the
+// subcube's pivot, its run of equal strings, q's lower and upper bound of it,
+// the split, and the position where q's split falls.
+__global__ void __launch_bounds__(HQ_NT) k_hq_split(const HqPe* prm, const uint32_t* owner, const uint32_t* off,
+                                                    uint64_t tiles, const uint32_t* runx, const uint32_t* ord,
+                                                    ArenaDev a, uint64_t n, uint32_t pw, uint32_t* cut,
+                                                    uint32_t* dest, uint32_t* err) {
+    __shared__ uint32_t sh[HQ_NT / 32 + 1];
+    const uint32_t q = blockIdx.x;
     const HqPe m = prm[q];
     const uint32_t P = m.cube, b = q & ~(P - 1), half = P >> 1;
     const HqPe r = prm[b];
@@ -577,31 +697,27 @@ __global__ void k_hq_split(const HqPe* prm, const uint32_t* pos, const uint32_t*
         hi = l == 0 ? first_not_below(runx, n, 1) : 0;
     } else {
         if (r.piv >= r.cnt) {
-            atomicExch(err, 1u);
+            if (threadIdx.x == 0) atomicExch(err, 1u);
             return;
         }
-        const uint32_t k = runx[pos[r.begin + r.piv]];
+        const uint32_t pg = hq_select(owner, off, tiles, n, b, r.piv, sh);
+        if (pg >= n) {
+            if (threadIdx.x == 0) atomicExch(err, 1u);
+            return;
+        }
+        const uint32_t k = runx[pg];
         lo = first_not_below(runx, n, k);
         hi = first_not_below(runx, n, (uint64_t)k + 1);
     }
-    const uint32_t* v = pos + m.begin;
-    const uint64_t lb = first_not_below(v, m.cnt, lo), ub = first_not_below(v, m.cnt, hi);
-    const uint64_t sep = lb < m.opt ? min((uint64_t)m.opt, ub) : lb;
-    cut[q] = sep < m.cnt ? v[sep] : HQ_NONE;
-    const bool left = q - b < half;
-    dest[q] = (b + (q - b + half) % P) | (left ? 0x80000000u : 0u);
-}
-
-// The exchange: the left half sends its strings from the split on, the right
-// half those before it.
-__global__ void k_hq_move(uint32_t* owner, uint64_t n, uint32_t pw, const uint32_t* cut, const uint32_t* dest) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const uint32_t q = owner[g];
-    if (q >= pw) return;
-    const uint32_t c = cut[q], d = dest[q];
-    const bool left = d >> 31;
-    if (left ? (c != HQ_NONE && g >= c) : (c == HQ_NONE || g < c)) owner[g] = d & 0x7FFFFFFFu;
+    const uint32_t lb = hq_rank(owner, off, tiles, n, q, m.cnt, lo, sh);
+    const uint32_t ub = hq_rank(owner, off, tiles, n, q, m.cnt, hi, sh);
+    const uint32_t sep = lb < m.opt ? min(m.opt, ub) : lb;
+    const uint32_t c = sep < m.cnt ? hq_select(owner, off, tiles, n, q, sep, sh) : HQ_NONE;
+    if (threadIdx.x == 0) {
+        if (sep < m.cnt && c >= n) atomicExch(err, 1u);
+        cut[q] = c;
+        dest[q] = (b + (q - b + half) % P) | (q - b < half ? 0x80000000u : 0u);
+    }
 }
 
 // RandomBitStore (sorter/RQuick/RandomBitStore.hpp:27-52) on PE q's
@@ -636,17 +752,22 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     out->levels = levels;
     for (uint32_t q = 0; q < p; ++q) out->counts[q] = 0;
     if (n == 0) return DSSS_OK;
-    const uint64_t N = n;
+    const uint64_t N = n, tiles = (n + HQ_TILE - 1) / HQ_TILE, cells = tiles * pw;
+    if (cells >= (1ull << 32)) return fail(DSSS_ENOTSUP, "hq sort: too many tiles x PEs");
     const uint32_t smax = 0;
-    auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint32_t*& owner, uint32_t*& pos,
-                    uint32_t*& runx, uint32_t*& cnt, HqPe*& prm, uint32_t*& cut, uint32_t*& dest, uint32_t*& err,
-                    uint64_t*& pbd, uint64_t*& total, void*& scan, void*& ms, SortLayout& sl) {
+    auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint32_t*& owner, uint32_t*& tmp,
+                    uint32_t*& runx, uint32_t*& srcb, uint32_t*& tc, uint32_t*& off, uint32_t*& cnt, HqPe*& prm,
+                    uint32_t*& cut, uint32_t*& dest, uint32_t*& err, uint64_t*& pbd, uint64_t*& total, void*& scan,
+                    SortLayout& sl) {
         handles = c.take<ulonglong2>(N);
         ord = c.take<uint32_t>(N);
         lcp = c.take<uint32_t>(N);
         owner = c.take<uint32_t>(N);
-        pos = c.take<uint32_t>(N);
+        tmp = c.take<uint32_t>(N);
         runx = c.take<uint32_t>(N);
+        srcb = out->source ? nullptr : c.take<uint32_t>(N);
+        tc = c.take<uint32_t>(cells);
+        off = c.take<uint32_t>(cells);
         cnt = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
         prm = c.take<HqPe>(MAX_SPLIT_BUCKETS);
         cut = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
@@ -654,23 +775,22 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         err = c.take<uint32_t>(1);
         pbd = c.take<uint64_t>(p + 1);
         total = c.take<uint64_t>(2);
-        scan = c.take<unsigned char>(scan_scratch_bytes(N));
-        ms = c.take<unsigned char>(multisplit_scratch_bytes(N, pw));
+        scan = c.take<unsigned char>(scan_scratch_bytes(N > cells ? N : cells));
         layout_sort(c, sl, N, 1, smax);
     };
     ulonglong2* handles;
-    uint32_t *ord, *lcp, *owner, *pos, *runx, *cnt, *cut, *dest, *err;
+    uint32_t *ord, *lcp, *owner, *tmp, *runx, *srcb, *tc, *off, *cnt, *cut, *dest, *err;
     HqPe* prm;
     uint64_t *pbd, *total;
-    void *scan, *ms;
+    void* scan;
     SortLayout sl;
     Carve sz(nullptr);
-    plan(sz, handles, ord, lcp, owner, pos, runx, cnt, prm, cut, dest, err, pbd, total, scan, ms, sl);
+    plan(sz, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, sl);
     DSSS_TRY(ensure_ws(ctx, sz.used));
     const uint64_t pin_bytes = MAX_SPLIT_BUCKETS * (sizeof(uint32_t) + sizeof(HqPe)) + 64;
     DSSS_TRY(ensure_pin(ctx, pin_bytes < 4096 ? 4096 : pin_bytes));
     Carve c(ctx->ws);
-    plan(c, handles, ord, lcp, owner, pos, runx, cnt, prm, cut, dest, err, pbd, total, scan, ms, sl);
+    plan(c, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, sl);
     ArenaDev a = view(in);
     make_handles(a, handles, st);
     a.h = handles;
@@ -680,43 +800,55 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         StageTimer t("stage:sort", st);
         DSSS_TRY(sort_strings(sl, a, n, 1, set_begin, nullptr, ord, lcp, smax, (uint32_t*)ctx->pin, st));
     }
+    // the output layout: the PEs' sorted data in rank order is the global order
+    uint32_t* source = out->source ? out->source : srcb;
     {
+        StageTimer t("stage:layout", st);
+        DSSS_LAUNCH("k_ms_source", st,
+                    k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(ord, nullptr, nullptr, nullptr, a, n, source,
+                                                                 out->lengths, tmp));
+        DSSS_TRY(exclusive_scan_u32_to_u64(tmp, out->offsets, n, total, scan, st));
+        DSSS_CUDA(cudaMemcpyAsync(ctx->pin, total, 8, cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        const uint64_t bytes = *(const uint64_t*)ctx->pin;
+        if (bytes > out->chars_capacity)
+            return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
+                        (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
+    }
+    if (levels == 0) {  // one PE: the local sort is the result (RQuick.hpp:855-864)
+        out->counts[0] = n;
+    } else {
         StageTimer t("stage:levels", st);
         DSSS_CUDA(cudaMemcpyAsync(pbd, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
         DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(ord, n, pbd, p, owner));
         if (pw < p) DSSS_LAUNCH("k_hq_fold", st, k_hq_fold<<<grid_for(n, 256), 256, 0, st>>>(owner, n, pw));
-        if (levels) {
-            DSSS_LAUNCH("k_hq_run_ends", st, k_hq_run_ends<<<grid_for(n, 256), 256, 0, st>>>(ord, lcp, a, n, pos));
-            DSSS_TRY(exclusive_scan_u32(pos, runx, n, nullptr, scan, st));
-        }
+        DSSS_LAUNCH("k_hq_run_ends", st,
+                    k_hq_run_ends<<<grid_for(n, 256), 256, 0, st>>>(out->lengths, lcp, n, tmp));
+        DSSS_TRY(exclusive_scan_u32(tmp, runx, n, nullptr, scan, st));
+        const size_t hsm = pw * sizeof(uint32_t);
+        DSSS_LAUNCH("k_hq_tile_hist", st,
+                    k_hq_tile_hist<<<(unsigned)tiles, HQ_NT, hsm, st>>>(owner, n, pw, tiles, tc));
         std::vector<HqBits> bits(pw);
         for (uint32_t q = 0; q < pw; ++q) bits[q].gen.seed(seed + q);  // HQuicksort.cpp:344-345
         uint32_t* hcnt = (uint32_t*)ctx->pin;
         HqPe* hprm = (HqPe*)((char*)ctx->pin + MAX_SPLIT_BUCKETS * sizeof(uint32_t));
-        const int hist_grid = 148 * 4;
-        for (uint32_t P = pw; P >= 2; P >>= 1) {
-            DSSS_CUDA(cudaMemsetAsync(cnt, 0, pw * sizeof(uint32_t), st));
-            DSSS_LAUNCH("k_hq_hist", st,
-                        k_hq_hist<<<hist_grid, 256, pw * sizeof(uint32_t), st>>>(owner, n, pw, cnt));
+        for (uint32_t P = pw;; P >>= 1) {
+            DSSS_TRY(exclusive_scan_u32(tc, off, cells, nullptr, scan, st));
+            DSSS_LAUNCH("k_hq_counts", st, k_hq_counts<<<grid_for(pw, 128), 128, 0, st>>>(off, tiles, pw, n, cnt));
             DSSS_CUDA(cudaMemcpyAsync(hcnt, cnt, pw * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-            {
-                const uint32_t* ins[1] = {nullptr};
-                uint32_t* outs[1] = {pos};
-                DSSS_TRY(multisplit_payload(owner, n, pw, 1, ins, outs, nullptr, err, ms, st));
-            }
             DSSS_CUDA(cudaStreamSynchronize(st));
+            if (P < 2) break;  // the counts after the last level
             // the bits in the reference's order per PE: middleMostElements
             // (:273-314), the first PE's selectMedian
             // (BinTreeMedianSelection.hpp:135-152), locateSplitter (:363-385)
-            uint64_t begin = 0;
+            uint64_t sum = 0;
             for (uint32_t q = 0; q < pw; ++q) {
                 const uint32_t k = hcnt[q];
                 HqPe& m = hprm[q];
-                m.begin = begin;
+                sum += k;
                 m.cnt = k;
                 m.cube = P;
                 m.piv = HQ_NONE;
-                begin += k;
                 const uint32_t beg = k > 2 ? (k - 2) / 2 + (k % 2 == 1 ? bits[q].next() : 0u) : 0u;
                 if (q % P == 0) {
                     const uint32_t nm = k < 2 ? k : 2;
@@ -724,42 +856,24 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
                 }
                 m.opt = k / 2 + (k % 2 == 1 ? bits[q].next() : 0u);
             }
-            if (begin != n) return fail(DSSS_EDEVICE, "hq sort: owner counts add up to %llu, not %llu",
-                                        (unsigned long long)begin, (unsigned long long)n);
+            if (sum != n) return fail(DSSS_EDEVICE, "hq sort: owner counts add up to %llu, not %llu",
+                                      (unsigned long long)sum, (unsigned long long)n);
             DSSS_CUDA(cudaMemcpyAsync(prm, hprm, pw * sizeof(HqPe), cudaMemcpyHostToDevice, st));
             DSSS_LAUNCH("k_hq_split", st,
-                        k_hq_split<<<grid_for(pw, 128), 128, 0, st>>>(prm, pos, runx, ord, a, n, pw, cut, dest, err));
-            DSSS_LAUNCH("k_hq_move", st, k_hq_move<<<grid_for(n, 256), 256, 0, st>>>(owner, n, pw, cut, dest));
-            // the pinned parameters are rewritten only after the next level's
-            // count read-back, which the stream orders after this copy
+                        k_hq_split<<<pw, HQ_NT, 0, st>>>(prm, owner, off, tiles, runx, ord, a, n, pw, cut, dest, err));
+            DSSS_LAUNCH("k_hq_move", st,
+                        k_hq_move<<<(unsigned)tiles, HQ_NT, hsm, st>>>(owner, n, pw, tiles, cut, dest, tc));
+            // the pinned parameters are rewritten only after the next count
+            // read-back, which the stream orders after this copy
         }
-        DSSS_CUDA(cudaMemsetAsync(cnt, 0, pw * sizeof(uint32_t), st));
-        DSSS_LAUNCH("k_hq_hist", st, k_hq_hist<<<hist_grid, 256, pw * sizeof(uint32_t), st>>>(owner, n, pw, cnt));
-        DSSS_CUDA(cudaMemcpyAsync(hcnt, cnt, pw * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        DSSS_CUDA(cudaStreamSynchronize(st));
         uint64_t sum = 0;
         for (uint32_t q = 0; q < pw; ++q) sum += out->counts[q] = hcnt[q];
         if (sum != n) return fail(DSSS_EDEVICE, "hq sort: final counts add up to %llu, not %llu",
                                   (unsigned long long)sum, (unsigned long long)n);
     }
-    // the strings in the global order, back to back
     {
         StageTimer t("stage:copy", st);
-        uint32_t* source = out->source ? out->source : lcp;
-        uint32_t* len1 = runx;
-        DSSS_LAUNCH("k_ms_source", st,
-                    k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(ord, nullptr, nullptr, nullptr, a, n, source,
-                                                                 out->lengths, len1));
-        DSSS_TRY(exclusive_scan_u32_to_u64(len1, out->offsets, n, total, scan, st));
-        DSSS_CUDA(cudaMemcpyAsync(ctx->pin, total, 8, cudaMemcpyDeviceToHost, st));
-        DSSS_CUDA(cudaStreamSynchronize(st));
-        const uint64_t bytes = *(const uint64_t*)ctx->pin;
-        if (bytes > out->chars_capacity)
-            return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
-                        (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
-        DSSS_LAUNCH("k_ms_copy", st,
-                    k_ms_copy<<<grid_for(n * MS_COPY_LANES, 256), 256, 0, st>>>(a, source, out->offsets, n,
-                                                                                out->chars));
+        DSSS_TRY(launch_ms_copy(a, source, out->offsets, n, out->chars, st));
     }
     DSSS_CUDA(cudaMemcpyAsync(ctx->pin, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));

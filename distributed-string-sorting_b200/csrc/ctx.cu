@@ -70,8 +70,9 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"merge_by_sort", 1, 0, 1},
     {"merge_extend_lanes", 0, 0, 32},
     {"dp_split", 0, 0, 1},
+    {"copy_word", 16, 8, 16},
 };
-static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}, {0}};
+static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}, {0}, {16}};
 
 int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
 
@@ -392,6 +393,7 @@ int dsss_tune_set(const char* name, int64_t value) {
                     (long long)g_knob_defs[k].hi);
     if (k == TUNE_MERGE_LANES && value && (value < 4 || (value & (value - 1))))
         return fail(DSSS_EINVAL, "knob %s takes 0, 4, 8, 16 or 32", name);
+    if (k == TUNE_COPY_WORD && value != 8 && value != 16) return fail(DSSS_EINVAL, "knob %s takes 8 or 16", name);
     g_knobs[k].store(value, std::memory_order_relaxed);
     return DSSS_OK;
 }

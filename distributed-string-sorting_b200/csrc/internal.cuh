@@ -135,6 +135,7 @@ enum TuneKnob : int {
     TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1) or by merge rounds (0)
     TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
     TUNE_DP_SPLIT,           // hash round split into hashing and table inserts (1) or one kernel (0)
+    TUNE_COPY_WORD,          // bytes per store when whole strings are copied out (16, or 8)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);
@@ -207,6 +208,38 @@ __device__ __forceinline__ void copy_words(uint8_t* dst, const uint8_t* src, uin
     unsigned long long* w = reinterpret_cast<unsigned long long*>(a0);
 #pragma unroll 4
     for (uint32_t k = lane; k < nw; k += L) w[k] = load_le8(src + head + 8 * k);
+}
+
+// copy_words with dst's aligned 16-byte words stored whole, each from three
+// aligned 8-byte loads of src (reads at most 8 bytes past src + len), the at
+// most 15 bytes before and after them singly.
+template <uint32_t L>
+__device__ __forceinline__ void copy_words16(uint8_t* dst, const uint8_t* src, uint32_t len, uint32_t lane) {
+    const uintptr_t d0 = (uintptr_t)dst, e = d0 + len;
+    const uintptr_t a0 = (d0 + 15) & ~(uintptr_t)15, a1 = e & ~(uintptr_t)15;
+    if (a0 >= a1) {
+        for (uint32_t k = lane; k < len; k += L) dst[k] = src[k];
+        return;
+    }
+    const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(a1 - d0);
+    for (uint32_t k = lane; k < head; k += L) dst[k] = src[k];
+    for (uint32_t k = tail + lane; k < len; k += L) dst[k] = src[k];
+    const uint32_t nw = (uint32_t)((a1 - a0) >> 4);
+    uint4* w = reinterpret_cast<uint4*>(a0);
+    const uintptr_t sa = (uintptr_t)(src + head);
+    const unsigned long long* q = reinterpret_cast<const unsigned long long*>(sa & ~(uintptr_t)7);
+    const unsigned sh = (unsigned)(sa & 7) * 8;
+#pragma unroll 2
+    for (uint32_t k = lane; k < nw; k += L) {
+        const uint64_t x0 = __ldg(q + 2 * k), x1 = __ldg(q + 2 * k + 1);
+        uint64_t lo = x0, hi = x1;
+        if (sh) {
+            const uint64_t x2 = __ldg(q + 2 * k + 2);
+            lo = (x0 >> sh) | (x1 << (64 - sh));
+            hi = (x1 >> sh) | (x2 << (64 - sh));
+        }
+        w[k] = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+    }
 }
 
 // Bytes [depth, depth+8) of a string as a big-endian key; bytes at or past

@@ -127,7 +127,9 @@ int dsss_abi_version(void);
  *                   decompressed length)
  *   dp_split        distinguishing-prefix hash rounds as two kernels, hashes
  *                   stored per position then inserted into the table (1), or
- *                   hash and insert in one kernel (0, default) */
+ *                   hash and insert in one kernel (0, default)
+ *   copy_word       dsss_ms_sort / dsss_hq_sort: bytes per aligned store when
+ *                   the output strings are copied out (16, default, or 8) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 

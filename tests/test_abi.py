@@ -120,6 +120,9 @@ def test_knob_errors(dsss):
         dsss.tune_set("merge_extend_lanes", 3)
     with pytest.raises(dsss.DsssError):
         dsss.tune_set("merge_extend_lanes", 2)
+    with pytest.raises(dsss.DsssError):
+        dsss.tune_set("copy_word", 12)
+    assert dsss.tune_get("copy_word") == 16
     v = dsss.tune_get("dp_filter_bits")
     dsss.tune_set("dp_filter_bits", 8)
     assert dsss.tune_get("dp_filter_bits") == 8

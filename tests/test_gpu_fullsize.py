@@ -128,3 +128,28 @@ def test_full_size_ms_sort(dsss, ctx):
     starts[1:] = ~same
     assert bool((ml[starts] == 0).all())
     assert bool((ml[1:][same] == lcp[same]).all())
+
+
+def test_full_size_hq_sort(dsss, ctx):
+    """hQuicksort on 32e6 strings x 200 B, p = 64: the counts add up to n, the
+    output names every string once, is strictly increasing across all PEs
+    (the PEs in rank order are the global order), and its bytes are the input
+    strings'."""
+    n, p = 32_000_000, 64
+    hs = dsss.gen_dn(n, 200, 50, seed=3)
+    ds = dsss.DeviceStrings(hs)
+    del hs
+    out = dsss.hq_sort(ctx, ds, p)
+    dev = ds.offsets.device
+    cnt = np.asarray(out["counts"], np.int64)
+    assert int(cnt.sum()) == n and out["levels"] == 6
+    src = out["source"][:n].long() & 0xFFFFFFFF
+    assert bool((torch.sort(src).values == torch.arange(n, device=dev)).all())
+    lens = out["lengths"][:n].long() & 0xFFFFFFFF
+    assert bool((lens == ds.lengths[src].long()).all())
+    view = _View(out["chars"], out["offsets"][:n], out["lengths"][:n])
+    ids = torch.arange(n, device=dev)
+    for s in range(0, n, CHUNK):
+        e = min(n, s + CHUNK)
+        assert bool((prefix_bytes(view, ids[s:e]) == prefix_bytes(ds, src[s:e])).all())
+    pair_check(view, ids, torch.ones(n - 1, dtype=torch.bool, device=dev))

@@ -135,3 +135,33 @@ def test_prefix_speculation(dsss, orc, ctx, early):
             ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
             assert np.array_equal(u64(order, n), ro)
             assert np.array_equal(u64(lcp, n), rl)
+
+
+@pytest.mark.parametrize("w", [8, 16])
+@pytest.mark.parametrize("name,strs", CASES, ids=IDS)
+def test_copy_word(dsss, orc, ctx, name, strs, w):
+    """Output strings copied with 8- or 16-byte stores: the merge-sort path
+    and hQuicksort give the oracle's bytes either way."""
+    from test_gpu_hq import check_hq
+    from test_gpu_ms import check_ms
+    hs = host_of(dsss, strs)
+    pb = np.linspace(0, hs.n, 4).astype(np.uint64)
+    with dsss.tuned(copy_word=w):
+        ms = dsss.ms_sort(ctx, dsss.DeviceStrings(hs), 3, part_begin=pb)
+        hq = dsss.hq_sort(ctx, dsss.DeviceStrings(hs), 3, part_begin=pb)
+    check_ms(dsss, orc, hs, ms, pb)
+    check_hq(dsss, orc, hs, hq, pb)
+
+
+@pytest.mark.parametrize("w", [8, 16])
+def test_copy_word_lengths(dsss, orc, ctx, w):
+    """Every length from 0 to 80 at every alignment of the output: heads,
+    tails and strings shorter than one store word."""
+    from test_gpu_hq import check_hq
+    rng = np.random.default_rng(9)
+    strs = [bytes(rng.integers(65, 91, int(k)).astype(np.uint8)) for k in rng.integers(0, 81, 3000)]
+    hs = host_of(dsss, strs)
+    pb = np.array([0, 1000, 3000], np.uint64)
+    with dsss.tuned(copy_word=w):
+        hq = dsss.hq_sort(ctx, dsss.DeviceStrings(hs), 2, part_begin=pb)
+    check_hq(dsss, orc, hs, hq, pb)
