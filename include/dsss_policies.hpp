@@ -257,6 +257,47 @@ public:
     }
 };
 
+// RQuick::sort(generator, std::move(data), MPI_BYTE, tag, comm,
+// StringComparator(), true) (src/sorter/RQuick/RQuick.hpp:1109-1115) as the
+// hQuicksort executable calls it (src/executables/HQuicksort.cpp:344-356,
+// PE r's generator seeded with 3469931 + r) for all PEs at once: every PE's
+// returned container as raw NUL-terminated strings in sorted order.
+class RQuick {
+public:
+    explicit RQuick(uint64_t seed = 3469931) : seed_(seed) {}
+    std::vector<std::vector<unsigned char>> sort(Context& ctx,
+                                                 const std::vector<std::vector<unsigned char>>& raw_per_pe,
+                                                 cudaStream_t stream = nullptr) const {
+        HostArena h(raw_per_pe);
+        DeviceArena d(h);
+        const size_t n = h.n();
+        const uint32_t p = h.p();
+        const uint64_t cap = h.chars.size() - 64;  // every string and its NUL
+        DeviceVec<uint32_t> lens(n);
+        DeviceVec<uint64_t> offs(n);
+        DeviceVec<uint8_t> chars(cap + 64);
+        std::vector<uint64_t> counts(p);
+        dsss_hq_result r{counts.data(), chars.p, cap, offs.p, lens.p, nullptr, 0};
+        dsss_arena a = d.view();
+        check(dsss_hq_sort(ctx.get(), &a, p, h.part_begin.data(), seed_, &r, (dsss_stream_t)stream));
+        check_cuda(cudaStreamSynchronize(stream));
+        const std::vector<uint8_t> hc = chars.host();
+        std::vector<std::vector<unsigned char>> out(p);
+        size_t byte = 0;
+        for (uint32_t q = 0; q < p; ++q)
+            for (uint64_t j = 0; j < counts[q]; ++j) {
+                size_t e = byte;
+                while (hc[e] != 0) ++e;
+                out[q].insert(out[q].end(), hc.begin() + byte, hc.begin() + e + 1);
+                byte = e + 1;
+            }
+        return out;
+    }
+
+private:
+    uint64_t seed_;
+};
+
 // tlx::sort_strings_detail::radixsort_CI3(StringLcpPtr, 0, 0) for each PE:
 // order[q][i] = input position of the i-th smallest string of PE q,
 // lcp[q][i] = LCP with its predecessor (0 first).

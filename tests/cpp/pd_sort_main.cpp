@@ -1,6 +1,6 @@
 // Drives include/dsss_policies.hpp the way the reference's prefix_doubling
 // executable drives DistributedPrefixDoublingSort: strings per PE in, local
-// order / DP / intervals / permutation out, and DistributedMergeSort the way
+// order / DP / intervals / permutation out, DistributedMergeSort and RQuick the way
 // the merge-sort executable does (strings and LCPs per receiving PE).  Input (stdin): p, then for each
 // PE a count and that many hex-encoded strings.  Output: one line per item.
 #include <iostream>
@@ -71,6 +71,24 @@ int main(int argc, char** argv) {
             }
             std::cout << "\nmslcp " << q;
             for (auto x : m.lcps[q]) std::cout << ' ' << x;
+            std::cout << '\n';
+        }
+        // hQuicksort: every PE's strings (hex)
+        dsss_gpu::RQuick hq;
+        auto hqs = hq.sort(ctx, raw);
+        for (uint32_t q = 0; q < p; ++q) {
+            std::cout << "hqstr " << q;
+            std::string cur;
+            for (unsigned char c : hqs[q]) {
+                if (c == 0) {
+                    std::cout << ' ' << (cur.empty() ? std::string("-") : cur);
+                    cur.clear();
+                } else {
+                    static const char* hx = "0123456789abcdef";
+                    cur += hx[c >> 4];
+                    cur += hx[c & 15];
+                }
+            }
             std::cout << '\n';
         }
         // the stage adaptors on PE 0

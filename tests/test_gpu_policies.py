@@ -84,3 +84,21 @@ def test_merge_sort_policy_matches_oracle(prog, orc, dsss):
     assert got == [s.get(int(i)) for i in r["source"]]
     lcp = np.concatenate([np.array(res["mslcp"][q], np.uint64) for q in range(p)])
     assert np.array_equal(lcp, r["out_lcp"])
+
+
+def test_rquick_policy_matches_oracle(prog, orc, dsss):
+    """dsss_gpu::RQuick: every PE's strings after hQuicksort, as the
+    oracle's RQuick restatement (p = 4, seeds 3469931 + rank)."""
+    p = 4
+    strs = with_duplicates(random_strings(2000, 1, 20, b"ABCDE", 79), 0.1, 80)
+    per_pe = [strs[q * 500:(q + 1) * 500] for q in range(p)]
+    res = run(prog, per_pe)
+    hs = dsss.from_bytes_list(strs)
+    s = orc.Strings.from_host(hs)
+    r = orc.hq_sort(s, dsss.equal_parts(len(strs), p))
+    k = 0
+    for q in range(p):
+        got = [bytes.fromhex(x) if x != "-" else b"" for x in res["hqstr"].get(q, [])]
+        c = int(r["counts"][q])
+        assert got == [s.get(int(i)) for i in r["source"][k:k + c]], q
+        k += c
