@@ -317,10 +317,12 @@ __global__ void k_fill_u32(uint32_t* a, uint64_t n, uint32_t v) {
     if (i < n) a[i] = v;
 }
 
-// Input index and length (+ 1 for the scan) of every output string.
+// Input index, source offset and length (+ 1 for the scan) of every output
+// string: the copy then reads its string's place sequentially instead of
+// gathering it again.
 __global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, const uint32_t* perm_index,
                             const uint32_t* perm_pe, ArenaDev a, uint64_t n, uint32_t* source, uint32_t* lengths,
-                            uint32_t* len1) {
+                            uint32_t* len1, uint64_t* src_off) {
     const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     const uint32_t id = perm_pe ? local_order[pb[perm_pe[o]] + perm_index[o]] : local_order[o];
@@ -330,6 +332,7 @@ __global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, con
     source[o] = id;
     lengths[o] = len;
     len1[o] = len + 1;
+    src_off[o] = off;
 }
 
 // Whole output strings and their NULs, MS_COPY_LANES lanes per string
@@ -338,26 +341,25 @@ __global__ void k_ms_source(const uint32_t* local_order, const uint64_t* pb, con
 // measured faster than 4 or 32).
 constexpr uint32_t MS_COPY_LANES = 8;
 template <uint32_t W>
-__global__ void k_ms_copy(ArenaDev a, const uint32_t* source, const uint64_t* out_off, uint64_t n, uint8_t* out) {
+__global__ void k_ms_copy(const uint8_t* chars, const uint64_t* src_off, const uint32_t* lengths,
+                          const uint64_t* out_off, uint64_t n, uint8_t* out) {
     const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MS_COPY_LANES;
     const uint32_t lane = threadIdx.x % MS_COPY_LANES;
     if (o >= n) return;
-    uint64_t off;
-    uint32_t len;
-    str_of(a, source[o], off, len);
+    const uint32_t len = lengths[o];
     uint8_t* dst = out + out_off[o];
-    if (W == 16) copy_words16<MS_COPY_LANES>(dst, a.chars + off, len, lane);
-    else copy_words<MS_COPY_LANES>(dst, a.chars + off, len, lane);
+    if (W == 16) copy_words16<MS_COPY_LANES>(dst, chars + src_off[o], len, lane);
+    else copy_words<MS_COPY_LANES>(dst, chars + src_off[o], len, lane);
     if (lane == 0) dst[len] = 0;
 }
 
-static int launch_ms_copy(const ArenaDev& a, const uint32_t* source, const uint64_t* out_off, uint64_t n,
-                          uint8_t* out, cudaStream_t st) {
+static int launch_ms_copy(const uint8_t* chars, const uint64_t* src_off, const uint32_t* lengths,
+                          const uint64_t* out_off, uint64_t n, uint8_t* out, cudaStream_t st) {
     const unsigned grid = grid_for(n * MS_COPY_LANES, 256);
     if (tune(TUNE_COPY_WORD) == 16)
-        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<16><<<grid, 256, 0, st>>>(a, source, out_off, n, out));
+        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<16><<<grid, 256, 0, st>>>(chars, src_off, lengths, out_off, n, out));
     else
-        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<8><<<grid, 256, 0, st>>>(a, source, out_off, n, out));
+        DSSS_LAUNCH("k_ms_copy", st, k_ms_copy<8><<<grid, 256, 0, st>>>(chars, src_off, lengths, out_off, n, out));
     return DSSS_OK;
 }
 
@@ -380,6 +382,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     layout_pd(sz, L, n, 1, p, factor, smax);
     uint32_t* src_tmp = sz.take<uint32_t>(N);
     uint32_t* len1 = sz.take<uint32_t>(N);
+    uint64_t* srcoff = sz.take<uint64_t>(N);
     unsigned long long* total = sz.take<unsigned long long>(2);
     void* scan = sz.take<unsigned char>(scan_scratch_bytes(N));
     DSSS_TRY(ensure_ws(ctx, sz.used));
@@ -388,6 +391,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     layout_pd(c, L, n, 1, p, factor, smax);
     src_tmp = c.take<uint32_t>(N);
     len1 = c.take<uint32_t>(N);
+    srcoff = c.take<uint64_t>(N);
     total = c.take<unsigned long long>(2);
     scan = c.take<unsigned char>(scan_scratch_bytes(N));
     uint32_t* source = out->source ? out->source : src_tmp;
@@ -434,7 +438,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         DSSS_CUDA(cudaMemcpyAsync(out->lcp, L.dpg, n * 4, cudaMemcpyDeviceToDevice, st));
         DSSS_LAUNCH("k_ms_source", st,
                     k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(out->local_order, L.pb, nullptr, nullptr, a, n,
-                                                                 source, out->lengths, len1));
+                                                                 source, out->lengths, len1, srcoff));
     } else {
         {
             StageTimer t("stage:partition", st);
@@ -478,7 +482,8 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         }
         DSSS_LAUNCH("k_ms_source", st,
                     k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(out->local_order, L.pb, L.dpg, len1, a, n, source,
-                                                                 out->lengths, src_tmp == source ? L.tmp : src_tmp));
+                                                                 out->lengths, src_tmp == source ? L.tmp : src_tmp,
+                                                                 srcoff));
         len1 = src_tmp == source ? L.tmp : src_tmp;
     }
     // output layout and the strings themselves
@@ -492,7 +497,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         if (bytes > out->chars_capacity)
             return fail(DSSS_EINVAL, "chars_capacity %llu is below the %llu output bytes",
                         (unsigned long long)out->chars_capacity, (unsigned long long)bytes);
-        DSSS_TRY(launch_ms_copy(a, source, out->offsets, n, out->chars, st));
+        DSSS_TRY(launch_ms_copy(a.chars, srcoff, out->lengths, out->offsets, n, out->chars, st));
     }
     pin = (uint32_t*)ctx->pin;
     DSSS_CUDA(cudaMemcpyAsync(pin, L.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -758,7 +763,7 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint32_t*& owner, uint32_t*& tmp,
                     uint32_t*& runx, uint32_t*& srcb, uint32_t*& tc, uint32_t*& off, uint32_t*& cnt, HqPe*& prm,
                     uint32_t*& cut, uint32_t*& dest, uint32_t*& err, uint64_t*& pbd, uint64_t*& total, void*& scan,
-                    SortLayout& sl) {
+                    uint64_t*& srcoff, SortLayout& sl) {
         handles = c.take<ulonglong2>(N);
         ord = c.take<uint32_t>(N);
         lcp = c.take<uint32_t>(N);
@@ -766,6 +771,7 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         tmp = c.take<uint32_t>(N);
         runx = c.take<uint32_t>(N);
         srcb = out->source ? nullptr : c.take<uint32_t>(N);
+        srcoff = c.take<uint64_t>(N);
         tc = c.take<uint32_t>(cells);
         off = c.take<uint32_t>(cells);
         cnt = c.take<uint32_t>(MAX_SPLIT_BUCKETS);
@@ -781,16 +787,16 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     ulonglong2* handles;
     uint32_t *ord, *lcp, *owner, *tmp, *runx, *srcb, *tc, *off, *cnt, *cut, *dest, *err;
     HqPe* prm;
-    uint64_t *pbd, *total;
+    uint64_t *pbd, *total, *srcoff;
     void* scan;
     SortLayout sl;
     Carve sz(nullptr);
-    plan(sz, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, sl);
+    plan(sz, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, srcoff, sl);
     DSSS_TRY(ensure_ws(ctx, sz.used));
     const uint64_t pin_bytes = MAX_SPLIT_BUCKETS * (sizeof(uint32_t) + sizeof(HqPe)) + 64;
     DSSS_TRY(ensure_pin(ctx, pin_bytes < 4096 ? 4096 : pin_bytes));
     Carve c(ctx->ws);
-    plan(c, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, sl);
+    plan(c, handles, ord, lcp, owner, tmp, runx, srcb, tc, off, cnt, prm, cut, dest, err, pbd, total, scan, srcoff, sl);
     ArenaDev a = view(in);
     make_handles(a, handles, st);
     a.h = handles;
@@ -806,7 +812,7 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         StageTimer t("stage:layout", st);
         DSSS_LAUNCH("k_ms_source", st,
                     k_ms_source<<<grid_for(n, 256), 256, 0, st>>>(ord, nullptr, nullptr, nullptr, a, n, source,
-                                                                 out->lengths, tmp));
+                                                                 out->lengths, tmp, srcoff));
         DSSS_TRY(exclusive_scan_u32_to_u64(tmp, out->offsets, n, total, scan, st));
         DSSS_CUDA(cudaMemcpyAsync(ctx->pin, total, 8, cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
@@ -873,7 +879,7 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     }
     {
         StageTimer t("stage:copy", st);
-        DSSS_TRY(launch_ms_copy(a, source, out->offsets, n, out->chars, st));
+        DSSS_TRY(launch_ms_copy(a.chars, srcoff, out->lengths, out->offsets, n, out->chars, st));
     }
     DSSS_CUDA(cudaMemcpyAsync(ctx->pin, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
