@@ -21,6 +21,7 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
             the same input, device-timed
   cpu_baseline  the oracle port of the reference path on the host
 
+--mode ms / --mode hq time the merge-sort path or hQuicksort alone (one GPU).
 --impl reference times the CPU port of the reference path (oracle/) on all
 host cores: one independent sort of a 1e6-string sample of the same rule per
 thread, throughput = strings / wall time.
@@ -341,6 +342,56 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_path(args, cfg, which):
+    """--mode ms / hq: the merge-sort path (dsss_ms_sort) or hQuicksort
+    (dsss_hq_sort) alone on the same input, one GPU, device-timed, with its
+    stage and kernel times."""
+    import torch
+    import __graft_entry__
+    d = __graft_entry__.load_package()
+    n, L, k, p, desc = cfg
+    hs = d.gen_dn(n, L, k, seed=1)
+    ds = d.DeviceStrings(hs)
+    del hs
+    ctx = d.Context(0)
+    fn = d.ms_sort if which == "ms" else d.hq_sort
+    stream = torch.cuda.current_stream()
+    out = None
+    for _ in range(args.warmup):
+        out = None
+        out = fn(ctx, ds, p)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = None
+            out = fn(ctx, ds, p)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ctx.set_timing(True)
+    out = None
+    out = fn(ctx, ds, p)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    name = {"ms": "merge-sort path (dsss_ms_sort: whole strings and LCPs per receiving PE)",
+            "hq": "hQuicksort (dsss_hq_sort: RQuick, seed 3469931 + rank; whole strings per PE)"}[which]
+    line = {
+        "metric": "strings/s", "value": n / (ms * 1e-3), "unit": "strings/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded D/N generator)", "mode": which,
+        "config": {"workload": desc + ", " + name, "n": n, "len": L, "p": p,
+                   "l2": "inputs > L2 (126 MB), no flush"},
+        "out_char_bytes": out["char_bytes"], "clocks": clk.summary(),
+        "stages_ms": {k2[6:]: round(v[1], 4) for k2, v in kt.items() if k2.startswith("stage:")},
+        "kernels_ms": {k2: round(v[1], 4) for k2, v in sorted(kt.items(), key=lambda x: -x[1][1])
+                       if not k2.startswith("stage:")},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -355,8 +406,9 @@ def main():
     ap.add_argument("--no-ms", action="store_true", help="skip the merge-sort path line")
     ap.add_argument("--no-hq", action="store_true", help="skip the hQuicksort line")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
-    ap.add_argument("--mode", default="replicas", choices=["replicas", "dist"],
-                    help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL)")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "dist", "ms", "hq"],
+                    help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL); "
+                         "ms / hq: the merge-sort path or hQuicksort alone on one GPU")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
@@ -370,6 +422,10 @@ def main():
         return
     if args.mode == "dist":
         run_dist(args, cfg)
+        return
+    if args.mode in ("ms", "hq"):
+        if rank == 0:
+            run_path(args, cfg, args.mode)
         return
 
     import torch

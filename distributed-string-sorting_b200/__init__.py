@@ -421,7 +421,8 @@ def ms_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, small_sort
     n = ds.n
     pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
     cap = int(ds.lengths[:n].to(torch.int64).sum().item()) + n if n else 0
-    out = dict(local_order=_empty(n), chars=torch.zeros(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
+    # every output byte (strings and their NULs, back to back) is written by the call
+    out = dict(local_order=_empty(n), chars=torch.empty(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
                offsets=torch.empty(max(n, 1), dtype=torch.int64, device="cuda"), lengths=_empty(n), lcp=_empty(n),
                source=_empty(n), intervals=np.zeros(p * p, dtype=np.uint64), recv_counts=np.zeros(p, dtype=np.uint64))
     res = MsResult(_ptr(out["local_order"]), _ptr(out["intervals"]), _ptr(out["chars"]), cap, _ptr(out["offsets"]),
@@ -448,7 +449,8 @@ def hq_sort(ctx: Context, ds: DeviceStrings, p: int, part_begin=None, seed: int 
     n = ds.n
     pb = equal_parts(n, p) if part_begin is None else np.asarray(part_begin, dtype=np.uint64)
     cap = int(ds.lengths[:n].to(torch.int64).sum().item()) + n if n else 0
-    out = dict(chars=torch.zeros(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
+    # every output byte (strings and their NULs, back to back) is written by the call
+    out = dict(chars=torch.empty(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"),
                offsets=torch.empty(max(n, 1), dtype=torch.int64, device="cuda"), lengths=_empty(n),
                source=_empty(n), counts=np.zeros(p, dtype=np.uint64))
     res = HqResult(_ptr(out["counts"]), _ptr(out["chars"]), cap, _ptr(out["offsets"]), _ptr(out["lengths"]),
