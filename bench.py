@@ -19,6 +19,8 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   ms_path   the merge-sort path (dsss_ms_sort) on the same input, device-timed
   hq_path   hQuicksort (dsss_hq_sort, the reference's RQuick competitor) on
             the same input, device-timed
+  formats   the input side (dsss_distribute_lines on a 1.6 GB text) and the
+            varint LCP coding (32e6 values), device-timed
   cpu_baseline  the oracle port of the reference path on the host
 
 --mode ms / --mode hq time the merge-sort path or hQuicksort alone (one GPU).
@@ -238,6 +240,68 @@ def bench_serving(d, torch, p=8, n_req=48, rate=250.0, seed=2024, workers=6, max
     }
 
 
+def bench_formats(d, torch, steps):
+    """The input side and the LCP wire format on one GPU, device-timed:
+    dsss_distribute_lines on a 1.6 GB text (8e6 lines of the D/N rule, 200 B,
+    p = 64; the call takes host bytes, so its time includes the host-to-device
+    copy of the text, and the kernels alone are timed as well), and varint
+    coding of 32e6 LCP-like values (uniform 0..199, every 64th up to 2^20) over
+    64 destination ranges."""
+    hs = d.gen_dn(8_000_000, 200, 50, seed=7)
+    text = hs.chars[:hs.char_bytes].copy()
+    del hs
+    text[text == 0] = 10
+    ctx = d.Context(0)
+    stream = torch.cuda.current_stream()
+    out = {}
+    for _ in range(2):
+        ds, pb = d.distribute_lines(ctx, text, 64)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ds, pb = d.distribute_lines(ctx, text, 64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ctx.set_timing(True)
+    ds, pb = d.distribute_lines(ctx, text, 64)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    kms = sum(v[1] for k2, v in kt.items() if k2.startswith("k_lines") or k2.startswith("scan"))
+    out["distribute_lines"] = {"bytes": int(text.size), "lines": ds.n, "ms_per_call": ms,
+                               "gbs_e2e": text.size / (ms * 1e-3) / 1e9, "kernels_ms": round(kms, 4),
+                               "gbs_kernels": text.size / (kms * 1e-3) / 1e9}
+    del ds, text
+    n = 32_000_000
+    g = torch.Generator(device="cuda").manual_seed(11)
+    vals = torch.randint(0, 200, (n,), device="cuda", dtype=torch.int32, generator=g)
+    vals[::64] = torch.randint(0, 1 << 20, (n // 64,), device="cuda", dtype=torch.int32, generator=g)
+    rc = np.full(64, n // 64, np.uint64)
+    for _ in range(2):
+        enc, per = d.varint_encode(ctx, vals, rc)
+        dec = d.varint_decode(ctx, enc, n)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        enc, per = d.varint_encode(ctx, vals, rc)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / steps
+    e0.record(stream)
+    for _ in range(steps):
+        dec = d.varint_decode(ctx, enc, n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dms = e0.elapsed_time(e1) / steps
+    assert bool((dec.to(torch.int64) == vals.to(torch.int64)).all())
+    out["varint"] = {"values": n, "coded_bytes": int(enc.numel()), "encode_ms": ems, "decode_ms": dms,
+                     "encode_values_per_s": n / (ems * 1e-3), "decode_values_per_s": n / (dms * 1e-3)}
+    ctx.close()
+    return out
+
+
 def run_dist(args, cfg):
     """--mode dist: one distributed sort over all ranks (dist.py), each rank
     holding p PEs of n strings of the D/N rule (rank-seeded), exchanging over
@@ -405,6 +469,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-ms", action="store_true", help="skip the merge-sort path line")
     ap.add_argument("--no-hq", action="store_true", help="skip the hQuicksort line")
+    ap.add_argument("--no-formats", action="store_true", help="skip the line distribution and varint lines")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dist", "ms", "hq"],
                     help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL); "
@@ -601,6 +666,9 @@ def main():
     serving = None
     if world == 1 and not args.no_serving:
         serving = bench_serving(d, torch)
+    formats = None
+    if world == 1 and not args.no_formats:
+        formats = bench_formats(d, torch, max(3, min(args.steps, 10)))
 
     if rank == 0:
         line = {
@@ -636,6 +704,7 @@ def main():
             "hq_path": hq_path,
             "batched": batched,
             "serving": serving,
+            "formats": formats,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -473,7 +473,7 @@ def distribute_lines(ctx: Context, data, p: int, max_size: int = 0, stream=None)
     S = min(size, max_size) if max_size else size
     cap_n = int(np.count_nonzero(arr[:S] == 10) + np.count_nonzero(arr[:S] == 0)) + 1
     cap = S + 1 + PAD
-    chars = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    chars = torch.empty(cap, dtype=torch.uint8, device="cuda")  # the call copies the text and zeroes the rest
     offs = torch.empty(cap_n, dtype=torch.int64, device="cuda")
     lens = torch.empty(cap_n, dtype=torch.int32, device="cuda")
     n, cb = ctypes.c_uint64(0), ctypes.c_uint64(0)
