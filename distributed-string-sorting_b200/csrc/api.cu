@@ -530,11 +530,6 @@ __global__ void k_hq_run_ends(const uint32_t* glen, const uint32_t* lcp, uint64_
     tail[g] = g + 1 < n ? !(glen[g] == glen[g + 1] && lcp[g + 1] == glen[g]) : 1u;
 }
 
-__global__ void k_hq_fold(uint32_t* owner, uint64_t n, uint32_t pw) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < n && owner[g] >= pw) owner[g] -= pw;
-}
-
 // Adds owner o of this lane to the shared histogram, one atomic per owner
 // and warp (owners come in long runs).
 __device__ __forceinline__ void hq_count(uint32_t* h, uint32_t o, uint32_t pw) {
@@ -542,9 +537,11 @@ __device__ __forceinline__ void hq_count(uint32_t* h, uint32_t o, uint32_t pw) {
     if (o < pw && (threadIdx.x & 31) == (uint32_t)__ffs(peers) - 1) atomicAdd(&h[o], __popc(peers));
 }
 
-// Owner counts of every tile, PE-major: tc[q * tiles + t].
-__global__ void __launch_bounds__(HQ_NT) k_hq_tile_hist(const uint32_t* owner, uint64_t n, uint32_t pw, uint64_t tiles,
-                                                        uint32_t* tc) {
+// The first level's owners: the PE of the string at each global position,
+// PEs past the largest power of two pw folded onto PE q - pw (RQuick.hpp:878-959),
+// and the owner counts of every tile, PE-major: tc[q * tiles + t].
+__global__ void __launch_bounds__(HQ_NT) k_hq_owner0(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p,
+                                                     uint32_t pw, uint64_t tiles, uint16_t* owner, uint32_t* tc) {
     extern __shared__ uint32_t h[];
     for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) h[q] = 0;
     __syncthreads();
@@ -552,7 +549,19 @@ __global__ void __launch_bounds__(HQ_NT) k_hq_tile_hist(const uint32_t* owner, u
 #pragma unroll 4
     for (uint32_t j = 0; j < HQ_IPT; ++j) {
         const uint64_t g = t0 + j * HQ_NT + threadIdx.x;
-        hq_count(h, g < n ? owner[g] : HQ_NONE, pw);
+        uint32_t q = HQ_NONE;
+        if (g < n) {
+            const uint32_t s = ord[g];
+            uint32_t lo = 0, hi = p;  // last q with pb[q] <= s
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(&pb[mid]) <= s) lo = mid;
+                else hi = mid;
+            }
+            q = lo >= pw ? lo - pw : lo;
+            owner[g] = (uint16_t)q;
+        }
+        hq_count(h, q, pw);
     }
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) tc[(uint64_t)q * tiles + blockIdx.x] = h[q];
@@ -562,7 +571,7 @@ __global__ void __launch_bounds__(HQ_NT) k_hq_tile_hist(const uint32_t* owner, u
 // split on, the right half those before it; dest[q] is q's partner, bit 31 set
 // for the left half, cut[q] the position of q's split (HQ_NONE: past its
 // end).  The new owners' tile counts are those of the next level.
-__global__ void __launch_bounds__(HQ_NT) k_hq_move(uint32_t* owner, uint64_t n, uint32_t pw, uint64_t tiles,
+__global__ void __launch_bounds__(HQ_NT) k_hq_move(uint16_t* owner, uint64_t n, uint32_t pw, uint64_t tiles,
                                                    const uint32_t* cut, const uint32_t* dest, uint32_t* tc) {
     extern __shared__ uint32_t h[];
     for (uint32_t q = threadIdx.x; q < pw; q += HQ_NT) h[q] = 0;
@@ -578,7 +587,7 @@ __global__ void __launch_bounds__(HQ_NT) k_hq_move(uint32_t* owner, uint64_t n, 
                 const uint32_t c = cut[o], d = dest[o];
                 if ((d >> 31) ? (c != HQ_NONE && g >= c) : (c == HQ_NONE || g < c)) {
                     o = d & 0x7FFFFFFFu;
-                    owner[g] = o;
+                    owner[g] = (uint16_t)o;
                 }
             }
         }
@@ -637,7 +646,7 @@ __device__ __forceinline__ uint32_t hq_block_scan(uint32_t v, uint32_t* sh, uint
 }
 
 // Strings of PE q at positions below x (its list's lower bound of x).
-__device__ uint32_t hq_rank(const uint32_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
+__device__ uint32_t hq_rank(const uint16_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
                             uint32_t cnt, uint64_t x, uint32_t* sh) {
     if (x >= n) return cnt;
     const uint64_t t = x / HQ_TILE, t0 = t * HQ_TILE;
@@ -652,7 +661,7 @@ __device__ uint32_t hq_rank(const uint32_t* owner, const uint32_t* off, uint64_t
 }
 
 // Position of the k-th string (from 0, k < its count) of PE q's list.
-__device__ uint32_t hq_select(const uint32_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
+__device__ uint32_t hq_select(const uint16_t* owner, const uint32_t* off, uint64_t tiles, uint64_t n, uint32_t q,
                               uint32_t k, uint32_t* sh) {
     const uint32_t* row = off + (uint64_t)q * tiles;
     const uint32_t b = row[0];
@@ -685,7 +694,7 @@ __device__ uint32_t hq_select(const uint32_t* owner, const uint32_t* off, uint64
 // locateSplitter (robust, RQuick.hpp:363-385) of PE q = blockIdx.x: the
 // subcube's pivot, its run of equal strings, q's lower and upper bound of it,
 // the split, and the position where q's split falls.
-__global__ void __launch_bounds__(HQ_NT) k_hq_split(const HqPe* prm, const uint32_t* owner, const uint32_t* off,
+__global__ void __launch_bounds__(HQ_NT) k_hq_split(const HqPe* prm, const uint16_t* owner, const uint32_t* off,
                                                     uint64_t tiles, const uint32_t* runx, const uint32_t* ord,
                                                     ArenaDev a, uint64_t n, uint32_t pw, uint32_t* cut,
                                                     uint32_t* dest, uint32_t* err) {
@@ -760,14 +769,14 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     const uint64_t N = n, tiles = (n + HQ_TILE - 1) / HQ_TILE, cells = tiles * pw;
     if (cells >= (1ull << 32)) return fail(DSSS_ENOTSUP, "hq sort: too many tiles x PEs");
     const uint32_t smax = 0;
-    auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint32_t*& owner, uint32_t*& tmp,
+    auto plan = [&](Carve& c, ulonglong2*& handles, uint32_t*& ord, uint32_t*& lcp, uint16_t*& owner, uint32_t*& tmp,
                     uint32_t*& runx, uint32_t*& srcb, uint32_t*& tc, uint32_t*& off, uint32_t*& cnt, HqPe*& prm,
                     uint32_t*& cut, uint32_t*& dest, uint32_t*& err, uint64_t*& pbd, uint64_t*& total, void*& scan,
                     uint64_t*& srcoff, SortLayout& sl) {
         handles = c.take<ulonglong2>(N);
         ord = c.take<uint32_t>(N);
         lcp = c.take<uint32_t>(N);
-        owner = c.take<uint32_t>(N);
+        owner = c.take<uint16_t>(N);
         tmp = c.take<uint32_t>(N);
         runx = c.take<uint32_t>(N);
         srcb = out->source ? nullptr : c.take<uint32_t>(N);
@@ -785,7 +794,8 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         layout_sort(c, sl, N, 1, smax);
     };
     ulonglong2* handles;
-    uint32_t *ord, *lcp, *owner, *tmp, *runx, *srcb, *tc, *off, *cnt, *cut, *dest, *err;
+    uint32_t *ord, *lcp, *tmp, *runx, *srcb, *tc, *off, *cnt, *cut, *dest, *err;
+    uint16_t* owner;
     HqPe* prm;
     uint64_t *pbd, *total, *srcoff;
     void* scan;
@@ -826,14 +836,12 @@ static int hq_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     } else {
         StageTimer t("stage:levels", st);
         DSSS_CUDA(cudaMemcpyAsync(pbd, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
-        DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(ord, n, pbd, p, owner));
-        if (pw < p) DSSS_LAUNCH("k_hq_fold", st, k_hq_fold<<<grid_for(n, 256), 256, 0, st>>>(owner, n, pw));
         DSSS_LAUNCH("k_hq_run_ends", st,
                     k_hq_run_ends<<<grid_for(n, 256), 256, 0, st>>>(out->lengths, lcp, n, tmp));
         DSSS_TRY(exclusive_scan_u32(tmp, runx, n, nullptr, scan, st));
         const size_t hsm = pw * sizeof(uint32_t);
-        DSSS_LAUNCH("k_hq_tile_hist", st,
-                    k_hq_tile_hist<<<(unsigned)tiles, HQ_NT, hsm, st>>>(owner, n, pw, tiles, tc));
+        DSSS_LAUNCH("k_hq_owner0", st,
+                    k_hq_owner0<<<(unsigned)tiles, HQ_NT, hsm, st>>>(ord, n, pbd, p, pw, tiles, owner, tc));
         std::vector<HqBits> bits(pw);
         for (uint32_t q = 0; q < pw; ++q) bits[q].gen.seed(seed + q);  // HQuicksort.cpp:344-345
         uint32_t* hcnt = (uint32_t*)ctx->pin;
