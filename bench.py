@@ -46,11 +46,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    # name: (n, len, k, p, description)
-    "dn32m": (32_000_000, 200, 50, 64, "32e6 strings x 200 B, D/N 0.25, p = 64 PEs"),
-    "dn1m": (1_000_000, 100, 50, 4, "1e6 strings x 100 B, D/N 0.5, p = 4 PEs"),
-    "dn8m": (8_000_000, 200, 50, 64, "8e6 strings x 200 B, D/N 0.25, p = 64 PEs (profiling size)"),
-    "dn100m": (100_000_000, 100, 50, 64, "1e8 strings x 100 B, D/N 0.5, p = 64 PEs"),
+    # name: (n, len, k, p, description, further generator arguments)
+    "dn32m": (32_000_000, 200, 50, 64, "32e6 strings x 200 B, D/N 0.25, p = 64 PEs", {}),
+    "dn1m": (1_000_000, 100, 50, 4, "1e6 strings x 100 B, D/N 0.5, p = 4 PEs", {}),
+    "dn8m": (8_000_000, 200, 50, 64, "8e6 strings x 200 B, D/N 0.25, p = 64 PEs (profiling size)", {}),
+    "dn100m": (100_000_000, 100, 50, 64, "1e8 strings x 100 B, D/N 0.5, p = 64 PEs", {}),
+    "skew20m": (20_000_000, 100, 20, 64, "20e6 strings, 80 % x 100 B with k = 20 and 20 % x 500 B with k = 400 "
+                "(seeded choice), p = 64 PEs", dict(long_len=500, long_k=400, frac_long=0.2)),
 }
 
 
@@ -116,12 +118,12 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_port(n_sample, L, k, p, seed):
+def cpu_baseline_port(n_sample, L, k, p, seed, gk=None):
     """Oracle port, one thread, on a bounded sample of the workload."""
     import __graft_entry__
     import oracle
     d = __graft_entry__.load_package()
-    hs = d.gen_dn(n_sample, L, k, seed=seed)
+    hs = d.gen_dn(n_sample, L, k, seed=seed, **(gk or {}))
     s = oracle.Strings.from_host(hs)
     t = time.perf_counter()
     oracle.pd_sort(s, d.equal_parts(hs.n, p))
@@ -316,7 +318,7 @@ def run_dist(args, cfg):
     import __graft_entry__
     d = __graft_entry__.load_package()
     import dsss_b200.dist as D
-    n, L, k, p, desc = cfg
+    n, L, k, p, desc, gk = cfg
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -330,7 +332,7 @@ def run_dist(args, cfg):
                                  timeout=datetime.timedelta(seconds=300))
     else:
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    hs = d.gen_dn(n, L, k, seed=1 + rank)
+    hs = d.gen_dn(n, L, k, seed=1 + rank, **gk)
     ctx = d.Context(local)
     be = D.GpuBackend(ctx)
     ds = be.strings(hs)
@@ -376,10 +378,10 @@ def run_reference(args, cfg):
     import __graft_entry__
     import oracle
     d = __graft_entry__.load_package()
-    n, L, k, p, desc = cfg
+    n, L, k, p, desc, gk = cfg
     threads = os.cpu_count() or 1
     sample = 1_000_000
-    inputs = [d.gen_dn(sample, L, k, seed=100 + t) for t in range(threads)]
+    inputs = [d.gen_dn(sample, L, k, seed=100 + t, **gk) for t in range(threads)]
     strs = [oracle.Strings.from_host(h) for h in inputs]
     pb = d.equal_parts(sample, p)
     oracle.lib()
@@ -417,8 +419,8 @@ def run_path(args, cfg, which):
     import torch
     import __graft_entry__
     d = __graft_entry__.load_package()
-    n, L, k, p, desc = cfg
-    hs = d.gen_dn(n, L, k, seed=1)
+    n, L, k, p, desc, gk = cfg
+    hs = d.gen_dn(n, L, k, seed=1, **gk)
     ds = d.DeviceStrings(hs)
     del hs
     ctx = d.Context(0)
@@ -507,8 +509,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    n, L, k, p, desc = cfg
-    hs = d.gen_dn(n, L, k, seed=1 + rank, pinned=not args.no_e2e)
+    n, L, k, p, desc, gk = cfg
+    hs = d.gen_dn(n, L, k, seed=1 + rank, pinned=not args.no_e2e, **gk)
     ds = d.DeviceStrings(hs, f"cuda:{local}")
     ctx = d.Context(local)
     stream = torch.cuda.current_stream()
@@ -600,7 +602,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = min(n, 8_000_000)
-        cpu = {"value": cpu_baseline_port(sample, L, k, p, seed=1), "unit": "strings/s", "cores": 1, "kind": "port",
+        cpu = {"value": cpu_baseline_port(sample, L, k, p, seed=1, gk=gk), "unit": "strings/s", "cores": 1, "kind": "port",
                "sample": f"{sample} strings of the same rule, p = {p}, oracle port single-threaded"}
 
     # the merge-sort path (dsss_ms_sort) on the same input, device-timed
@@ -687,8 +689,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_dp_hash (all launches of one step)",
                          "achieved": hash_achieved, "peak": peak, "unit": "GB/s", "frac": hash_achieved / peak,
                          "peak_kind": peak_kind,
-                         "traffic": DP_HASH_DRAM_PER_STRING * int(hashed_final.sum()),
-                         "traffic_note": "ncu dram bytes read+write per hashed string of the dense round on 8e6 "
+                         "traffic": None if gk else DP_HASH_DRAM_PER_STRING * int(hashed_final.sum()),
+                         "traffic_note": "not measured for this string mix" if gk else
+                                         "ncu dram bytes read+write per hashed string of the dense round on 8e6 "
                                          "strings (profiles/k_dp_hash_dn8m.md), times the strings hashed",
                          "algo_bytes": hash_bytes,
                          "algo_formula": "sum over strings hashed at their final depth d of (d + 16); lower bound",
