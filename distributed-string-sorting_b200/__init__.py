@@ -140,6 +140,8 @@ _SIGS = {
     "dsss_bucket_scatter": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, _P, _P, _P, _U64, _P, _P, _P, _P, _P,
                                  _P, _P, _P, _P]),
     "dsss_lcp_merge": (_I, [_P, _P, _U64, _P, _P, _U64, _U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "dsss_lcp_merge_strings": (_I, [_P, _P, _U64, _P, _P, _U64, _U32, _U32, _P, _P, _P, _P, _P, _U64, _P, _P, _P,
+                                    _P]),
     "dsss_partition": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, _P, ctypes.POINTER(Opts), _P, _P]),
     "dsss_adjacent_lcp": (_I, [_P, ctypes.POINTER(Arena), _P, _U64, _P, _P]),
     "dsss_adjacent_lcp_noalloc": (_I, [ctypes.POINTER(Arena), _P, _U64, _P, _P]),
@@ -756,6 +758,34 @@ def lcp_merge(ctx: Context, chars, char_bytes: int, lcp, counts, offsets=None, c
                                _ptr(offs), _ptr(out["order"]), _ptr(out["merged_lcp"]), _ptr(out["old_lcp"]),
                                _ptr(out["perm_index"]), _ptr(out["perm_pe"]), _stream_ptr(stream)))
     return {k: v[:n] for k, v in out.items()}
+
+
+def lcp_merge_strings(ctx: Context, chars, char_bytes: int, lcp, counts, offsets=None, char_start=None,
+                      lcp_sum: int = None, stream=None):
+    """dsss_lcp_merge_strings: the merge of receive containers of whole strings
+    and every merged string whole, back to back in merged order.  lcp_sum (the
+    sum of lcp; read from the device when not given) sizes the output.
+    Returns device tensors chars, offsets, lengths, merged_lcp, order."""
+    import torch
+    counts = np.ascontiguousarray(np.asarray(counts, dtype=np.uint64))
+    nrecv, p = counts.shape
+    offs = None if offsets is None else np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+    n = int(lcp.shape[0])
+    if lcp_sum is None:
+        lcp_sum = int(lcp[:n].to(torch.int64).sum().item()) if n else 0
+    cap = char_bytes + lcp_sum
+    out = dict(order=_empty(n), merged_lcp=_empty(n), lengths=_empty(n),
+               offsets=torch.empty(max(n, 1), dtype=torch.int64, device="cuda"),
+               chars=torch.empty(max(cap, 1) + PAD, dtype=torch.uint8, device="cuda"))
+    nb = ctypes.c_uint64(0)
+    check(lib().dsss_lcp_merge_strings(ctx.h, _ptr(chars), char_bytes, _ptr(char_start), _ptr(lcp), n, nrecv, p,
+                                       _ptr(counts), _ptr(offs), _ptr(out["order"]), _ptr(out["merged_lcp"]),
+                                       _ptr(out["chars"]), cap, _ptr(out["offsets"]), _ptr(out["lengths"]),
+                                       ctypes.byref(nb), _stream_ptr(stream)))
+    res = {k: out[k][:n] for k in ("order", "merged_lcp", "lengths", "offsets")}
+    res["chars"] = out["chars"]
+    res["char_bytes"] = int(nb.value)
+    return res
 
 
 def prefix_hash(ds: DeviceStrings, ids, depth: int, stream=None):

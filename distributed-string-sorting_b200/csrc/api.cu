@@ -1050,6 +1050,22 @@ int dsss_lcp_merge(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes
     return rc;
 }
 
+int dsss_lcp_merge_strings(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes,
+                           const uint32_t* recv_char_start, const uint32_t* recv_lcp, uint64_t n, uint32_t nrecv,
+                           uint32_t p, const uint64_t* recv_counts, const uint64_t* recv_offsets, uint32_t* order,
+                           uint32_t* merged_lcp, uint8_t* out_chars, uint64_t out_capacity, uint64_t* out_offsets,
+                           uint32_t* out_lengths, uint64_t* out_bytes, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    if (nrecv == 0 || p == 0 || !recv_counts || !out_bytes) return fail(DSSS_EINVAL, "nrecv/p/recv_counts/out_bytes missing");
+    if (n && (!recv_chars || !recv_lcp || !order || !out_chars || !out_offsets || !out_lengths))
+        return fail(DSSS_EINVAL, "input or output arrays are NULL");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    return lcp_merge_strings(ctx, recv_chars, char_bytes, recv_char_start, recv_lcp, n, nrecv, p, recv_counts,
+                             recv_offsets, order, merged_lcp, nullptr, nullptr, nullptr, out_chars, out_capacity,
+                             out_offsets, out_lengths, out_bytes, (cudaStream_t)stream);
+}
+
 int dsss_prefix_hash(const dsss_arena* in, const uint32_t* ids, uint64_t m, uint32_t depth, uint64_t* hash,
                      dsss_stream_t stream) {
     DSSS_TRY(check_arena(in));

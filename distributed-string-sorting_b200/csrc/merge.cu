@@ -606,4 +606,60 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
     return DSSS_OK;
 }
 
+// ------------------------------------------------ whole merged strings ----
+// The merge-sort path's output on the receiving side: every merged string
+// whole (the decompressed arena of the merge, StringLcpContainer::extendPrefix,
+// stringcontainer.hpp:248-333), NUL-terminated, back to back in merged order.
+
+__global__ void k_merged_len1(const uint32_t* order, const uint32_t* flen, uint64_t n, uint32_t* len1) {
+    const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o < n) len1[o] = flen[order[o]] + 1;
+}
+
+constexpr uint32_t MG_COPY_LANES = 8;
+__global__ void k_merged_copy(const uint8_t* full, const uint64_t* foff, const uint32_t* flen, const uint32_t* order,
+                              const uint64_t* out_off, uint64_t n, uint8_t* out, uint32_t* out_len) {
+    const uint64_t o = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MG_COPY_LANES;
+    const uint32_t lane = threadIdx.x % MG_COPY_LANES;
+    if (o >= n) return;
+    const uint32_t id = order[o];
+    const uint32_t len = flen[id];
+    uint8_t* dst = out + out_off[o];
+    copy_words16<MG_COPY_LANES>(dst, full + foff[id], len, lane);
+    if (lane == 0) {
+        dst[len] = 0;
+        out_len[o] = len;
+    }
+}
+
+int lcp_merge_strings(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* char_start, const uint32_t* lcp,
+                      uint64_t n, uint32_t nrecv, uint32_t p, const uint64_t* counts, const uint64_t* offsets,
+                      uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp, uint32_t* perm_index,
+                      uint32_t* perm_pe, uint8_t* out_chars, uint64_t out_capacity, uint64_t* out_offsets,
+                      uint32_t* out_lengths, uint64_t* out_bytes, cudaStream_t st) {
+    *out_bytes = 0;
+    DSSS_TRY(lcp_merge(ctx, chars, bytes, char_start, lcp, n, nrecv, p, counts, offsets, order, merged_lcp, old_lcp,
+                       perm_index, perm_pe, st));
+    if (n == 0) return DSSS_OK;
+    // the merge's arrays are where its last carve put them: the decompressed
+    // arena is taken last, so a carve with its size unknown finds it too
+    Carve c(ctx->ws);
+    MergeLayout L;
+    layout_merge(c, L, n, bytes, 0, nrecv * p);
+    DSSS_LAUNCH("k_merged_len1", st, k_merged_len1<<<grid_for(n, 256), 256, 0, st>>>(order, L.flen, n, out_lengths));
+    DSSS_TRY(exclusive_scan_u32_to_u64(out_lengths, out_offsets, n, L.total64, L.scan, st));
+    uint64_t* pin = (uint64_t*)ctx->pin;
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.total64, 8, cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    *out_bytes = pin[0];
+    if (pin[0] > out_capacity)
+        return fail(DSSS_EINVAL, "out_capacity %llu is below the %llu output bytes", (unsigned long long)out_capacity,
+                    (unsigned long long)pin[0]);
+    DSSS_LAUNCH("k_merged_copy", st,
+                k_merged_copy<<<grid_for(n * MG_COPY_LANES, 256), 256, 0, st>>>(L.full, L.foff, L.flen, order,
+                                                                              out_offsets, n, out_chars,
+                                                                              out_lengths));
+    return DSSS_OK;
+}
+
 }  // namespace dsss

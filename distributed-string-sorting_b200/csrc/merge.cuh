@@ -39,4 +39,14 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
               uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp, uint32_t* perm_index, uint32_t* perm_pe,
               cudaStream_t st);
 
+// lcp_merge, then every merged string whole (prefixes decompressed),
+// NUL-terminated, back to back in merged order: out_offsets/out_lengths per
+// merged position, *out_bytes the bytes written (or needed: DSSS_EINVAL when
+// out_capacity is below them).
+int lcp_merge_strings(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* char_start, const uint32_t* lcp,
+                      uint64_t n, uint32_t nrecv, uint32_t p, const uint64_t* counts, const uint64_t* offsets,
+                      uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp, uint32_t* perm_index,
+                      uint32_t* perm_pe, uint8_t* out_chars, uint64_t out_capacity, uint64_t* out_offsets,
+                      uint32_t* out_lengths, uint64_t* out_bytes, cudaStream_t st);
+
 }  // namespace dsss

@@ -30,8 +30,8 @@ import ctypes
 
 import numpy as np
 
-from . import (Arena, DeviceStrings, PAD, _ptr, _stream_ptr, check, lcp_merge, lib, local_sort_lcp, varint_decode,
-               varint_encode)
+from . import (Arena, DeviceStrings, PAD, _ptr, _stream_ptr, check, lcp_merge, lcp_merge_strings, lib, local_sort_lcp,
+               varint_decode, varint_encode)
 
 
 # ------------------------------------------------------------- collectives --
@@ -288,6 +288,28 @@ class GpuBackend:
         out = lcp_merge(self.ctx, chars, nbytes, lcps, counts, offsets, char_start=starts, stream=self.stream)
         return {k: out[k] for k in ("perm_index", "perm_pe", "merged_lcp")}
 
+    def lcp_sum(self, lcp, n):
+        return int(lcp[:n].to(self.torch.int64).sum().item()) if n else 0
+
+    def lengths_in_order(self, ds, order):
+        """Whole strings as DP: the length of the string at every local position."""
+        n = ds.n
+        if n == 0:
+            return self._e(1, self.torch.int32)
+        return ds.lengths[:n][order[:n].to(self.torch.int64) & 0xFFFFFFFF].to(self.torch.int32).contiguous()
+
+    def merge_strings(self, chars, nbytes, starts, lcps, counts, offsets):
+        out = lcp_merge_strings(self.ctx, chars, nbytes, lcps, counts, offsets, char_start=starts,
+                                stream=self.stream)
+        return dict(chars=out["chars"], char_bytes=out["char_bytes"], offsets=out["offsets"], lengths=out["lengths"],
+                    lcp=out["merged_lcp"])
+
+    def no_strings(self):
+        torch = self.torch
+        return dict(chars=torch.zeros(1, dtype=torch.uint8, device=self.device), char_bytes=0,
+                    offsets=torch.zeros(0, dtype=torch.int64, device=self.device),
+                    lengths=self._e(0, torch.int32), lcp=self._e(0, torch.int32))
+
     def to_host(self, t, n=None):
         a = t.cpu().numpy() if hasattr(t, "cpu") else np.asarray(t)
         if a.dtype == np.int32:
@@ -365,6 +387,105 @@ class _Phases:
         self.t = t
 
 
+def _partition(comm, be, strings, pb, order, trunc, sizes_local, p, p_local, q_first, pe_goff, factor, indexed):
+    """Splitters from every PE's sample, each sample string cut to trunc(its
+    local positions), gathered on all ranks and sorted; this rank's interval
+    rows (computePartition, misc.hpp:531-587) and every rank's."""
+    pos = sample_positions(sizes_local, p, factor)
+    if p_local:
+        flat = np.concatenate([pb[q] + pos[q] for q in range(p_local)])
+        gidx = np.concatenate([pe_goff[q_first + q] + pos[q] for q in range(p_local)])
+    else:
+        flat = gidx = np.zeros(0, np.int64)
+    ids = be.take(order, flat) if flat.size else np.zeros(0, np.int64)
+    tr = trunc(flat) if flat.size else np.zeros(0, np.int64)
+    schars, soffs, slens, sbytes = be.pack(strings, ids, tr)
+    # every rank's (lengths, offsets, global indices, bytes) in one all-gather
+    msg = _pack_rows(slens, soffs, gidx, blob=np.asarray(be.chars_to_host(schars, sbytes), np.uint8))
+    base, offs, lens_l, gidx_l, chars_l = 0, [], [], [], []
+    for part in comm.allgather_np(msg):
+        (ln, of, gi), cb = _unpack_rows(part)
+        lens_l.append(ln)
+        offs.append(of + base)
+        gidx_l.append(gi)
+        chars_l.append(cb)
+        base += cb.size
+    gchars = np.concatenate(chars_l) if chars_l else np.zeros(0, np.uint8)
+    goffs = np.concatenate(offs)
+    glens = np.concatenate(lens_l)
+    ggidx = np.concatenate(gidx_l)
+    S = int(glens.size)
+    sample = be.arena_from(be.chars_from_host(gchars), goffs, glens, gchars.size)
+    nspl = min(p - 1, S)
+    if nspl:
+        sorted_ids = np.asarray(be.sort_arena(sample), np.int64)
+        step = S // (nspl + 1)
+        spl_ids = sorted_ids[np.arange(1, nspl + 1, dtype=np.int64) * step]
+    else:
+        spl_ids = np.zeros(0, np.int64)
+    pchars, poffs, plens, pbytes = be.pack(sample, spl_ids, None)
+    spl = be.arena_from(pchars, poffs, plens, pbytes)
+    iv_local = be.partition_search(strings, pb, order, spl, ggidx[spl_ids], p, pe_goff[q_first:q_first + p_local],
+                                   indexed)
+    iv_all = np.concatenate(comm.allgather_np(np.asarray(iv_local).ravel())).reshape(p, p)
+    return iv_local, iv_all
+
+
+def _exchange(comm, be, strings, pb, order, lcp, dp, p, p_all, p_local, q_first, iv_local, iv_all, compress_lcps,
+              ph):
+    """Receive containers of [lcp, dp) + NUL per string to every PE, across
+    ranks (alltoall.hpp:910-1008), regrouped by receiving PE; returns the
+    regroup plan, the received bytes, starts and LCPs, the strings and bytes
+    received, and per local receiving PE the strings and bucket offsets of
+    every source PE."""
+    snd = be.bucket_send(strings, pb, order, lcp, dp, p, q_first, iv_local)
+    ph.mark("bucket_send")
+    per_r = snd["counts"].sum(axis=1)                    # strings per receiver from this rank
+    rbeg = np.concatenate([[0], np.cumsum(per_r)])
+    cbeg = snd["char_begin"]
+    firsts = np.concatenate([[0], np.cumsum(p_all)])
+    s_str = [int(rbeg[firsts[t + 1]] - rbeg[firsts[t]]) for t in range(comm.world)]
+    s_byte = [int(cbeg[firsts[t + 1]] - cbeg[firsts[t]]) for t in range(comm.world)]
+    # to every rank: (strings, bytes) of each of its receivers from this rank
+    nbytes_r = np.diff(cbeg)
+    meta = [np.stack([per_r[firsts[t]:firsts[t + 1]], nbytes_r[firsts[t]:firsts[t + 1]]]).T.ravel()
+            for t in range(comm.world)]
+    rmeta = [m.reshape(-1, 2) for m in comm.alltoall_np(meta)]
+    r_str = comm.alltoall_counts(s_str)
+    r_byte = comm.alltoall_counts(s_byte)
+    rchars = comm.alltoallv(snd["chars"], s_byte, r_byte)
+    rstart = comm.alltoallv(snd["char_start"], s_str, r_str)
+    if compress_lcps:
+        # sendLcps with compressLcps (alltoall.hpp:406-425): each rank's run of
+        # LCPs varint-coded (writeRanges), the bytes exchanged, and all that
+        # arrives decoded as one sequence (varint codes are self-delimiting)
+        lbytes, per_rank = be.varint_encode(snd["lcp"], s_str)
+        r_lb = comm.alltoall_counts([int(x) for x in per_rank])
+        got = comm.alltoallv(lbytes, [int(x) for x in per_rank], r_lb)
+        rlcp = be.varint_decode(got, int(sum(r_str)))
+    else:
+        rlcp = comm.alltoallv(snd["lcp"], s_str, r_str)
+    ph.mark("exchange")
+    # regroup [sender rank][receiver] -> [receiver][sender rank]
+    src_str = np.concatenate([[0], np.cumsum(r_str)])
+    src_byte = np.concatenate([[0], np.cumsum(r_byte)])
+    blocks, dstr, dbyte = [], 0, 0
+    for r in range(p_local):
+        for s in range(comm.world):
+            ns_, nb_ = int(rmeta[s][r, 0]), int(rmeta[s][r, 1])
+            so = int(src_str[s] + rmeta[s][:r, 0].sum())
+            bo = int(src_byte[s] + rmeta[s][:r, 1].sum())
+            blocks.append([so, dstr, ns_, bo, dbyte, nb_])
+            dstr += ns_
+            dbyte += nb_
+    nrecv = dstr
+    my = slice(q_first, q_first + p_local)
+    counts = iv_all[:, my].T.copy()                                            # [r_local, q]
+    starts = np.concatenate([np.zeros((p, 1), np.int64), np.cumsum(iv_all, axis=1)], axis=1)
+    offsets = starts[:, my].T.copy()                                           # [r_local, q]
+    return blocks, rchars, rstart, rlcp, nrecv, dbyte, counts, offsets
+
+
 def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None,
          compress_lcps: bool = False):
     """This rank's part of DistributedPrefixDoublingSort::sort.  strings: the
@@ -414,92 +535,14 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
     ph.mark("dp")
 
     # 2. splitters (misc.hpp:531-587)
-    pos = sample_positions(sizes_local, p, factor)
-    if p_local:
-        flat = np.concatenate([pb[q] + pos[q] for q in range(p_local)])
-        gidx = np.concatenate([pe_goff[q_first + q] + pos[q] for q in range(p_local)])
-    else:
-        flat = gidx = np.zeros(0, np.int64)
-    ids = be.take(order, flat) if flat.size else np.zeros(0, np.int64)
-    tr = be.take(dp, flat) if flat.size else np.zeros(0, np.int64)
-    schars, soffs, slens, sbytes = be.pack(strings, ids, tr)
-    # every rank's (lengths, offsets, global indices, bytes) in one all-gather
-    msg = _pack_rows(slens, soffs, gidx, blob=np.asarray(be.chars_to_host(schars, sbytes), np.uint8))
-    base, offs, lens_l, gidx_l, chars_l = 0, [], [], [], []
-    for part in comm.allgather_np(msg):
-        (ln, of, gi), cb = _unpack_rows(part)
-        lens_l.append(ln)
-        offs.append(of + base)
-        gidx_l.append(gi)
-        chars_l.append(cb)
-        base += cb.size
-    gchars = np.concatenate(chars_l) if chars_l else np.zeros(0, np.uint8)
-    goffs = np.concatenate(offs)
-    glens = np.concatenate(lens_l)
-    ggidx = np.concatenate(gidx_l)
-    S = int(glens.size)
-    sample = be.arena_from(be.chars_from_host(gchars), goffs, glens, gchars.size)
-    nspl = min(p - 1, S)
-    if nspl:
-        sorted_ids = np.asarray(be.sort_arena(sample), np.int64)
-        step = S // (nspl + 1)
-        spl_ids = sorted_ids[np.arange(1, nspl + 1, dtype=np.int64) * step]
-    else:
-        spl_ids = np.zeros(0, np.int64)
-    pchars, poffs, plens, pbytes = be.pack(sample, spl_ids, None)
-    spl = be.arena_from(pchars, poffs, plens, pbytes)
-    iv_local = be.partition_search(strings, pb, order, spl, ggidx[spl_ids], p, pe_goff[q_first:q_first + p_local],
-                                   indexed)
-    iv_all = np.concatenate(comm.allgather_np(np.asarray(iv_local).ravel())).reshape(p, p)
+    iv_local, iv_all = _partition(comm, be, strings, pb, order, lambda flat: be.take(dp, flat), sizes_local, p,
+                                  p_local, q_first, pe_goff, factor, indexed)
     res["intervals"] = np.asarray(iv_local, np.int64)
     ph.mark("partition")
 
     # 3. string exchange (alltoall.hpp:910-1008) and merge (merging.hpp:66-123)
-    snd = be.bucket_send(strings, pb, order, lcp, dp, p, q_first, iv_local)
-    ph.mark("bucket_send")
-    per_r = snd["counts"].sum(axis=1)                    # strings per receiver from this rank
-    rbeg = np.concatenate([[0], np.cumsum(per_r)])
-    cbeg = snd["char_begin"]
-    firsts = np.concatenate([[0], np.cumsum(p_all)])
-    s_str = [int(rbeg[firsts[t + 1]] - rbeg[firsts[t]]) for t in range(comm.world)]
-    s_byte = [int(cbeg[firsts[t + 1]] - cbeg[firsts[t]]) for t in range(comm.world)]
-    # to every rank: (strings, bytes) of each of its receivers from this rank
-    nbytes_r = np.diff(cbeg)
-    meta = [np.stack([per_r[firsts[t]:firsts[t + 1]], nbytes_r[firsts[t]:firsts[t + 1]]]).T.ravel()
-            for t in range(comm.world)]
-    rmeta = [m.reshape(-1, 2) for m in comm.alltoall_np(meta)]
-    r_str = comm.alltoall_counts(s_str)
-    r_byte = comm.alltoall_counts(s_byte)
-    rchars = comm.alltoallv(snd["chars"], s_byte, r_byte)
-    rstart = comm.alltoallv(snd["char_start"], s_str, r_str)
-    if compress_lcps:
-        # sendLcps with compressLcps (alltoall.hpp:406-425): each rank's run of
-        # LCPs varint-coded (writeRanges), the bytes exchanged, and all that
-        # arrives decoded as one sequence (varint codes are self-delimiting)
-        lbytes, per_rank = be.varint_encode(snd["lcp"], s_str)
-        r_lb = comm.alltoall_counts([int(x) for x in per_rank])
-        got = comm.alltoallv(lbytes, [int(x) for x in per_rank], r_lb)
-        rlcp = be.varint_decode(got, int(sum(r_str)))
-    else:
-        rlcp = comm.alltoallv(snd["lcp"], s_str, r_str)
-    ph.mark("exchange")
-    # regroup [sender rank][receiver] -> [receiver][sender rank]
-    src_str = np.concatenate([[0], np.cumsum(r_str)])
-    src_byte = np.concatenate([[0], np.cumsum(r_byte)])
-    blocks, dstr, dbyte = [], 0, 0
-    for r in range(p_local):
-        for s in range(comm.world):
-            ns_, nb_ = int(rmeta[s][r, 0]), int(rmeta[s][r, 1])
-            so = int(src_str[s] + rmeta[s][:r, 0].sum())
-            bo = int(src_byte[s] + rmeta[s][:r, 1].sum())
-            blocks.append([so, dstr, ns_, bo, dbyte, nb_])
-            dstr += ns_
-            dbyte += nb_
-    nrecv = dstr
-    my = slice(q_first, q_first + p_local)
-    counts = iv_all[:, my].T.copy()                                            # [r_local, q]
-    starts = np.concatenate([np.zeros((p, 1), np.int64), np.cumsum(iv_all, axis=1)], axis=1)
-    offsets = starts[:, my].T.copy()                                           # [r_local, q]
+    blocks, rchars, rstart, rlcp, nrecv, dbyte, counts, offsets = _exchange(
+        comm, be, strings, pb, order, lcp, dp, p, p_all, p_local, q_first, iv_local, iv_all, compress_lcps, ph)
     res["recv_counts"] = counts.sum(axis=1)
     res["recv_total"] = nrecv
     if nrecv:
@@ -509,4 +552,55 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
         ph.mark("merge")
     else:
         res.update(perm_index=np.zeros(0, np.int64), perm_pe=np.zeros(0, np.int64), merged_lcp=np.zeros(0, np.int64))
+    return res
+
+
+def merge_sort(comm: Comm, be, strings, part_begin, factor: int = 2, phases=None, compress_lcps: bool = False):
+    """This rank's part of DistributedMergeSort::sort
+    (lcp_aware_number_string_splitting.hpp:184-290) with
+    SampleSplittersNumStringsPolicy: local sort, getAvgLcp over all PEs
+    (misc.hpp:68-87), splitters from samples cut to 200 (avg + 5) bytes
+    (misc.hpp:473-531 on 100 * avg, :238), whole strings exchanged
+    prefix-compressed (DP = length), merged and decompressed on the receiving
+    side (extendPrefix).  Returns per local receiving PE, back to back, the
+    strings whole (chars, offsets, lengths), their LCPs (0 at each PE start),
+    recv_counts, plus local_order, intervals and avg_lcp.  Byte-identical
+    strings are interchangeable in this output."""
+    ph = _Phases(phases)
+    pb = np.asarray(part_begin, np.int64)
+    p_local = len(pb) - 1
+    n = int(pb[-1])
+    sizes_local = np.diff(pb)
+    sizes_all = comm.allgather_np(sizes_local)
+    p_all = [len(x) for x in sizes_all]
+    p = sum(p_all)
+    q_first = sum(p_all[:comm.rank])
+    pe_goff = np.concatenate([[0], np.cumsum(np.concatenate(sizes_all))]).astype(np.int64)
+    res = dict(part_begin=pb, p_global=p, q_first=q_first)
+    ph.mark("setup")
+    order, lcp = be.local_sort(strings, pb)
+    res["local_order"] = order
+    ph.mark("local_sort")
+    # getAvgLcp: the local LCP arrays (0 at each PE start) over all strings
+    total_lcp = comm.allreduce_sum(be.lcp_sum(lcp, n))
+    total_n = comm.allreduce_sum(n)
+    avg = total_lcp // total_n if total_n else 0
+    res["avg_lcp"] = avg
+    cut = 2 * (100 * (avg + 5))
+    iv_local, iv_all = _partition(comm, be, strings, pb, order, lambda flat: np.full(flat.size, cut, np.int64),
+                                  sizes_local, p, p_local, q_first, pe_goff, factor, False)
+    res["intervals"] = np.asarray(iv_local, np.int64)
+    ph.mark("partition")
+    dp = be.lengths_in_order(strings, order)
+    blocks, rchars, rstart, rlcp, nrecv, dbyte, counts, offsets = _exchange(
+        comm, be, strings, pb, order, lcp, dp, p, p_all, p_local, q_first, iv_local, iv_all, compress_lcps, ph)
+    res["recv_counts"] = counts.sum(axis=1)
+    res["recv_total"] = nrecv
+    if nrecv:
+        mchars, mstart, mlcp = be.regroup(blocks, rchars, rstart, rlcp, nrecv, dbyte)
+        ph.mark("regroup")
+        res.update(be.merge_strings(mchars, dbyte, mstart, mlcp, counts, offsets))
+        ph.mark("merge")
+    else:
+        res.update(be.no_strings())
     return res

@@ -319,6 +319,20 @@ int dsss_lcp_merge(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes
                    const uint64_t* recv_offsets, uint32_t* order, uint32_t* merged_lcp, uint32_t* old_lcp,
                    uint32_t* perm_index, uint32_t* perm_pe, dsss_stream_t stream);
 
+/* The receiving side of DistributedMergeSort::sort
+ * (lcp_aware_number_string_splitting.hpp:184-290) for PEs on several GPUs:
+ * dsss_lcp_merge on receive containers of whole strings (sent with DP =
+ * length), then every merged string whole — its prefix restored as
+ * StringLcpContainer::extendPrefix does (strings/stringcontainer.hpp:248-333)
+ * — NUL-terminated, back to back in merged order (out_offsets, out_lengths:
+ * device, n each).  The output bytes are char_bytes + the sum of recv_lcp;
+ * *out_bytes gets them, and DSSS_EINVAL when out_capacity is below them. */
+int dsss_lcp_merge_strings(dsss_ctx* ctx, const uint8_t* recv_chars, uint64_t char_bytes,
+                           const uint32_t* recv_char_start, const uint32_t* recv_lcp, uint64_t n, uint32_t nrecv,
+                           uint32_t p, const uint64_t* recv_counts, const uint64_t* recv_offsets, uint32_t* order,
+                           uint32_t* merged_lcp, uint8_t* out_chars, uint64_t out_capacity, uint64_t* out_offsets,
+                           uint32_t* out_lengths, uint64_t* out_bytes, dsss_stream_t stream);
+
 /* calc_lcp of sorted neighbours (strings/stringtools.hpp:158-166): lcp[i] =
  * LCP(string order[i-1], string order[i]) for i >= 1, lcp[0] = 0. */
 int dsss_adjacent_lcp(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* order, uint64_t m, uint32_t* lcp,

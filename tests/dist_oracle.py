@@ -203,6 +203,43 @@ class OracleBackend:
             k += m
         return {key: (np.concatenate(v).astype(np.int64) if v else np.zeros(0, np.int64)) for key, v in out.items()}
 
+    def lcp_sum(self, lcp, n):
+        return int(np.asarray(lcp, np.int64)[:n].sum())
+
+    def lengths_in_order(self, a, order):
+        return np.asarray(a.lengths, np.int64)[np.asarray(order, np.int64)]
+
+    def merge_strings(self, chars, nbytes, starts, lcps, counts, offsets):
+        """The merge, then every run's strings with their prefixes restored
+        (extendPrefix, strings/stringcontainer.hpp:248-333), in merged order."""
+        m = self.merge(chars, nbytes, starts, lcps, counts, offsets)
+        chars, starts, lcps = np.asarray(chars), np.asarray(starts), np.asarray(lcps)
+        full, run_pos, k = [], {}, 0
+        for r in range(counts.shape[0]):
+            for q in range(counts.shape[1]):
+                run_pos[(r, q)] = k
+                prev = b""
+                for _ in range(int(counts[r, q])):
+                    b0 = b1 = int(starts[k])
+                    while chars[b1] != 0:
+                        b1 += 1
+                    cur = prev[:int(lcps[k])] + chars[b0:b1].tobytes()
+                    full.append(cur)
+                    prev = cur
+                    k += 1
+        out, t = [], 0
+        for r in range(counts.shape[0]):
+            for _ in range(int(counts[r].sum())):
+                q, i = int(m["perm_pe"][t]), int(m["perm_index"][t])
+                out.append(full[run_pos[(r, q)] + i - int(offsets[r, q])])
+                t += 1
+        oc, oo, ol, nb = pack_list(out)
+        return dict(chars=oc, char_bytes=nb, offsets=oo, lengths=ol, lcp=m["merged_lcp"])
+
+    def no_strings(self):
+        z = np.zeros(0, np.int64)
+        return dict(chars=np.zeros(1, np.uint8), char_bytes=0, offsets=z, lengths=z, lcp=z)
+
     def to_host(self, t, n=None):
         a = np.asarray(t).astype(np.int64)
         return a if n is None else a[:n]

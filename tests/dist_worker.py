@@ -22,6 +22,7 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
     import dsss_b200.dist as D
     strs, pb, splits, sampler = inputs[:4]
     compress = bool(inputs[4]) if len(inputs) > 4 else False
+    mode = inputs[5] if len(inputs) > 5 else "pd"
     if pg == "nccl":
         import torch
         torch.cuda.set_device(0)
@@ -41,8 +42,18 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
             ctx = d.Context(0)
             be = D.GpuBackend(ctx)
             arena = be.strings(d.from_bytes_list(mine))
-        res = D.sort(D.Comm(), be, arena, pb_local, sampler, compress_lcps=compress)
+        if mode == "ms":
+            res = D.merge_sort(D.Comm(), be, arena, pb_local, compress_lcps=compress)
+        else:
+            res = D.sort(D.Comm(), be, arena, pb_local, sampler, compress_lcps=compress)
         out = {"q0": q0, "q1": q1, "s0": s0}
+        if mode == "ms":
+            nrecv = int(res.get("recv_total", 0))
+            ch = res["chars"]
+            ch = ch.cpu().numpy() if hasattr(ch, "cpu") else np.asarray(ch)
+            out.update(avg_lcp=int(res["avg_lcp"]), out_chars=np.asarray(ch[:int(res["char_bytes"])], np.uint8),
+                       out_offsets=be.to_host(res["offsets"], nrecv), out_lengths=be.to_host(res["lengths"], nrecv),
+                       out_lcp=be.to_host(res["lcp"], nrecv))
         nrecv = int(res.get("recv_total", 0))
         for k in ("local_order", "dp", "perm_index", "perm_pe", "merged_lcp"):
             if k in res:

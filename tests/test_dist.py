@@ -114,3 +114,44 @@ def test_sample_positions_match_reference_rule(dsss):
         nr = min(2 * (p - 1), nq)
         want = [int(float(i) * (float(nq) / float(nr + 1))) for i in range(1, nr + 1)]
         assert dist.sample_positions([nq], p)[0].tolist() == want
+
+
+def check_ms_against_oracle(orc, strs, pb, results):
+    """DistributedMergeSort over ranks against the oracle's single-process
+    merge-sort path: average LCP, local orders, interval rows, strings per
+    receiving PE, every output string's bytes and its LCP."""
+    from dist_oracle import pack_list
+    chars, offs, lens, _ = pack_list(strs)
+    s = orc.Strings(chars, offs.astype(np.uint64), lens.astype(np.uint32))
+    ref = orc.ms_sort(s, np.asarray(pb, np.uint64))
+    rb = np.concatenate([[0], np.cumsum(ref["recv_counts"])]).astype(np.int64)
+    for r in results:
+        q0, q1, s0 = int(r["q0"]), int(r["q1"]), int(r["s0"])
+        s1 = int(pb[q1])
+        assert int(r["avg_lcp"]) == ref["avg_lcp"]
+        assert np.array_equal(r["local_order"] + s0, ref["order"][s0:s1].astype(np.int64))
+        assert np.array_equal(r["intervals"], ref["intervals"][q0:q1].astype(np.int64))
+        assert np.array_equal(r["recv_counts"], ref["recv_counts"][q0:q1].astype(np.int64))
+        b0, b1 = rb[q0], rb[q1]
+        oc, oo, ol = r["out_chars"], r["out_offsets"], r["out_lengths"]
+        got = [oc[o:o + l].tobytes() for o, l in zip(oo, ol)]
+        assert got == [s.get(int(i)) for i in ref["source"][b0:b1]]
+        assert np.array_equal(r["out_lcp"], ref["out_lcp"][b0:b1].astype(np.int64))
+
+
+@pytest.mark.parametrize("name,strs", CASES, ids=[c[0] for c in CASES])
+def test_two_ranks_merge_sort(orc, name, strs):
+    n = len(strs)
+    pb = [0, n // 7, n // 3, n // 2, (4 * n) // 5, n]
+    res = run_ranks(2, (strs, pb, [0, 2, 5], 0, False, "ms"), "oracle")
+    check_ms_against_oracle(orc, strs, pb, res)
+
+
+def test_merge_sort_compressed_lcps_three_ranks(orc):
+    """Three ranks, one with no PE's strings in its first PE, LCPs sent as
+    varint bytes."""
+    strs = CASES[1][1]
+    n = len(strs)
+    pb = [0, 0, n // 3, (2 * n) // 3, n]
+    res = run_ranks(3, (strs, pb, [0, 2, 3, 4], 0, True, "ms"), "oracle")
+    check_ms_against_oracle(orc, strs, pb, res)

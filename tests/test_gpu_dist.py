@@ -51,3 +51,23 @@ def test_nccl_single_rank(orc):
     pb = [0, n // 5, (2 * n) // 5, (3 * n) // 5, (4 * n) // 5, n]
     res = run_ranks(1, (strs, pb, [0, 5], 0), "gpu", pg="nccl")
     check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
+
+
+@pytest.mark.parametrize("name,strs", CASES, ids=[c[0] for c in CASES])
+def test_gpu_ranks_merge_sort(orc, name, strs):
+    """DistributedMergeSort with the CUDA backend (dsss_lcp_merge_strings on
+    the receiving side): every output string and LCP as the oracle's."""
+    from test_dist import check_ms_against_oracle
+    n = len(strs)
+    pb = [0, n // 9, n // 3, n // 2, (5 * n) // 6, n]
+    res = run_ranks(2, (strs, pb, [0, 3, 5], 0, False, "ms"), "gpu")
+    check_ms_against_oracle(orc, strs, pb, res)
+
+
+def test_nccl_single_rank_merge_sort(orc):
+    from test_dist import check_ms_against_oracle
+    strs = CASES[0][1]
+    n = len(strs)
+    pb = [0, n // 5, (2 * n) // 5, (3 * n) // 5, (4 * n) // 5, n]
+    res = run_ranks(1, (strs, pb, [0, 5], 0, True, "ms"), "gpu", pg="nccl")
+    check_ms_against_oracle(orc, strs, pb, res)
