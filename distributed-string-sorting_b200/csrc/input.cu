@@ -18,7 +18,25 @@ namespace dsss {
 
 constexpr int LN_NT = 256, LN_BPT = 16, LN_TILE = LN_NT * LN_BPT;
 
-__device__ __forceinline__ bool ln_term(uint8_t c) { return c == 0 || c == '\n'; }
+__device__ __forceinline__ bool ln_term(uint32_t c) { return c == 0 || c == '\n'; }
+
+// A thread's 16 bytes as one aligned load when the text is 16-byte aligned
+// and the chunk lies inside it (full), and the byte before them: the
+// previous lane's last byte by shuffle, lane 0's from memory (0 at position
+// 0, where a line starts).  Every lane of the warp calls it.
+__device__ __forceinline__ bool ln_chunk(const uint8_t* c, uint64_t S, uint64_t base, bool vec, uint32_t w[4],
+                                         uint32_t& prev) {
+    const bool full = vec && base + LN_BPT <= S;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (full) v = *reinterpret_cast<const uint4*>(c + base);
+    w[0] = v.x;
+    w[1] = v.y;
+    w[2] = v.z;
+    w[3] = v.w;
+    prev = __shfl_up_sync(0xffffffffu, v.w >> 24, 1);
+    if ((threadIdx.x & 31) == 0) prev = (base && base < S) ? c[base - 1] : 0u;
+    return full;
+}
 
 // Pass 1: '\n' -> NUL, and the number of line starts per tile (position 0 and
 // every position after a terminator).  A neighbour's byte read here is either
@@ -26,14 +44,30 @@ __device__ __forceinline__ bool ln_term(uint8_t c) { return c == 0 || c == '\n';
 __global__ void __launch_bounds__(LN_NT) k_lines_count(uint8_t* c, uint64_t S, uint32_t* tile_cnt) {
     __shared__ uint32_t part[LN_NT / 32];
     const uint64_t base = (uint64_t)blockIdx.x * LN_TILE + (uint64_t)threadIdx.x * LN_BPT;
-    uint32_t cnt = 0;
+    const bool vec = ((uintptr_t)c & 15) == 0;
+    uint32_t cnt = 0, w[4], prev;
+    if (ln_chunk(c, S, base, vec, w, prev)) {
+        bool nl = false;
 #pragma unroll
-    for (int j = 0; j < LN_BPT; ++j) {
-        const uint64_t b = base + j;
-        if (b >= S) break;
-        const uint8_t v = c[b];
-        if (b == 0 || ln_term(c[b - 1])) ++cnt;
-        if (v == '\n') c[b] = 0;
+        for (int j = 0; j < LN_BPT; ++j) {
+            const uint32_t v = (w[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+            cnt += ln_term(prev);
+            prev = v;
+            if (v == '\n') {
+                w[j >> 2] &= ~(0xFFu << (8 * (j & 3)));
+                nl = true;
+            }
+        }
+        if (nl) *reinterpret_cast<uint4*>(c + base) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < LN_BPT; ++j) {
+            const uint64_t b = base + j;
+            if (b >= S) break;
+            const uint8_t v = c[b];
+            if (b == 0 || ln_term(c[b - 1])) ++cnt;
+            if (v == '\n') c[b] = 0;
+        }
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -52,11 +86,20 @@ __global__ void __launch_bounds__(LN_NT) k_lines_offsets(const uint8_t* c, uint6
                                                          uint64_t* offsets) {
     __shared__ uint32_t wsum[LN_NT / 32];
     const uint64_t base = (uint64_t)blockIdx.x * LN_TILE + (uint64_t)threadIdx.x * LN_BPT;
-    uint32_t mask = 0;
+    const bool vec = ((uintptr_t)c & 15) == 0;
+    uint32_t mask = 0, wd[4], prev;
+    if (ln_chunk(c, S, base, vec, wd, prev)) {
 #pragma unroll
-    for (int j = 0; j < LN_BPT; ++j) {
-        const uint64_t b = base + j;
-        if (b < S && (b == 0 || c[b - 1] == 0)) mask |= 1u << j;
+        for (int j = 0; j < LN_BPT; ++j) {
+            if (prev == 0) mask |= 1u << j;
+            prev = (wd[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < LN_BPT; ++j) {
+            const uint64_t b = base + j;
+            if (b < S && (b == 0 || c[b - 1] == 0)) mask |= 1u << j;
+        }
     }
     const uint32_t cnt = __popc(mask);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
