@@ -155,3 +155,16 @@ def test_merge_sort_compressed_lcps_three_ranks(orc):
     pb = [0, 0, n // 3, (2 * n) // 3, n]
     res = run_ranks(3, (strs, pb, [0, 2, 3, 4], 0, True, "ms"), "oracle")
     check_ms_against_oracle(orc, strs, pb, res)
+
+
+@pytest.mark.parametrize("mode", ["pd", "ms"])
+def test_rank_without_pes(orc, mode):
+    """Rank 0 holds no PE: it still takes part in every collective."""
+    strs = CASES[0][1]
+    n = len(strs)
+    pb = [0, n // 3, (2 * n) // 3, n]
+    res = run_ranks(2, (strs, pb, [0, 0, 3], 0, False, mode), "oracle")
+    if mode == "ms":
+        check_ms_against_oracle(orc, strs, pb, res)
+    else:
+        check_against_oracle(orc, strs, pb, res, 0)
