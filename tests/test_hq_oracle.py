@@ -185,3 +185,18 @@ def test_seed_changes_split(orc):
     for seed in (HQ_SEED, HQ_SEED + 7):
         assert oracle_pes(orc, pes, seed) == rquick(pes, seed)
     assert len(seen) > 1 and all(sum(c) == 8 for c in seen)
+
+
+def test_oracle_matches_restatement_random_layouts(orc):
+    """Random PE layouts (empty PEs, few distinct strings, 1-12 PEs, random
+    seeds): the oracle and the pure-Python restatement agree exactly."""
+    from hypothesis import given, settings, strategies as st
+
+    word = st.binary(min_size=0, max_size=5).map(lambda b: bytes(65 + (x % 3) for x in b))
+
+    @settings(max_examples=150, deadline=None, derandomize=True)
+    @given(st.lists(st.lists(word, max_size=12), min_size=1, max_size=12), st.integers(0, 1 << 30))
+    def check(pes, seed):
+        assert oracle_pes(orc, pes, seed) == rquick(pes, seed)
+
+    check()
