@@ -184,3 +184,16 @@ def test_pd_sort_oracle_global_order(orc, dsss, p):
     assert merged == sorted(s.get(i) for i in range(hs.n))
     assert sorted(zip(r["perm_pe"].tolist(), r["perm_index"].tolist())) == \
         sorted((q, i) for q in range(p) for i in range(len(local[q])))
+
+
+def test_varint_reference_known_answer(orc):
+    """The reference's own test (src/tests/integerCompression_tests.cpp:11-60):
+    1, 2^8, 2^16, ..., 2^56 written twice as two ranges take 37 bytes each,
+    and read back unchanged."""
+    nums = [1 << (8 * i) for i in range(8)]
+    data, per = orc.varint_encode(nums + nums, [8, 8])
+    assert per.tolist() == [37, 37]
+    assert orc.varint_decode(data, 16).tolist() == nums + nums
+    # LEB128 bytes of single values (7 bits per byte, low first, high bit = more)
+    assert orc.varint_encode([300], [1])[0].tobytes() == b"\xac\x02"
+    assert orc.varint_encode([2**32 - 1], [1])[0].tobytes() == b"\xff\xff\xff\xff\x0f"
