@@ -373,41 +373,64 @@ def run_dist(args, cfg):
     tdist.destroy_process_group()
 
 
-def run_reference(args, cfg):
-    """--impl reference: the CPU port of the reference path on all host threads."""
-    import __graft_entry__
-    import oracle
-    d = __graft_entry__.load_package()
+def config_of(cfg):
+    """The line's `config`: identical on the GPU arm and the reference arm."""
     n, L, k, p, desc, gk = cfg
-    threads = os.cpu_count() or 1
-    sample = 1_000_000
-    inputs = [d.gen_dn(sample, L, k, seed=100 + t, **gk) for t in range(threads)]
-    strs = [oracle.Strings.from_host(h) for h in inputs]
-    pb = d.equal_parts(sample, p)
-    oracle.lib()
+    return {"workload": desc, "n": n, "len": L, "k": k, "p": p, "generator": dict(gk) or None, "seed": 1,
+            "l2": "inputs larger than L2 (126 MB), no flush"}
 
-    def step():
-        ths = [threading.Thread(target=oracle.pd_sort, args=(s, pb)) for s in strs]
-        t0 = time.perf_counter()
-        for t in ths:
-            t.start()
-        for t in ths:
-            t.join()
-        return time.perf_counter() - t0
 
-    for _ in range(args.warmup):
-        step()
-    times = [step() for _ in range(args.steps)]
-    sec = sum(times) / len(times)
-    value = threads * sample / sec
+def run_reference(args, cfg):
+    """--impl reference: the reference's own prefix_doubling executable
+    (src/executables/prefix_doubling.cpp with its default policies, compiled
+    from the reference's sources into oracle/_ref over the process-based MPI
+    stand-in oracle/shim_mpi) sorting the same input as the GPU arm with p
+    ranks = the configuration's p PEs on the host cores.  The input is made by
+    the oracle's restatement of the generator (no product code is loaded),
+    written one string per line and read by the executable's FileDistributer
+    (--generator 2 --path <file> --strongScaling).  One iteration of the
+    executable is one step; its time is the `sorting_overall` RESULT (the
+    slowest rank); W warm-up iterations are dropped and value = n / median of
+    the K timed ones."""
+    import shutil
+    import oracle
+    n, L, k, p, desc, gk = cfg
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    if not oracle.ref_exe_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/prefix_doubling was not built (the "
+                          "reference tree was absent when oracle/ was built)"}), flush=True)
+        return
+    s = oracle.gen_dn(n, L, k, seed=1, **gk)
+    tmpdir = "/dev/shm" if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > 3 * s.char_bytes \
+        else tempfile.gettempdir()
+    path = os.path.join(tmpdir, f"dsss_ref_input_{os.getpid()}.txt")
+    try:
+        oracle.write_lines(s, path)
+        char_bytes = int(s.char_bytes)
+        del s
+        iters = args.warmup + args.steps
+        times, _ = oracle.run_reference_pd(path, p, iters)
+    finally:
+        if os.path.exists(path):
+            os.unlink(path)
+    if len(times) != iters:
+        raise RuntimeError(f"expected {iters} iterations, parsed {len(times)}")
+    timed = times[args.warmup:]
+    sec = statistics.median(timed)
+    value = n / sec
     line = {
         "impl": "reference", "metric": "strings/s", "value": value, "unit": "strings/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded D/N generator)",
-        "config": {"workload": desc, "n": n, "len": L, "p": p, "parallelism": f"{threads} host threads"},
-        "cpu_baseline": {"value": value, "unit": "strings/s", "cores": threads, "kind": "port",
-                         "sample": f"{threads} independent sorts of 1e6 strings of the same rule, p = {p}"},
+        "config": config_of(cfg),
+        "char_gbs": char_bytes / sec / 1e9,
+        "cpu_baseline": {"value": value, "unit": "strings/s", "cores": cores, "kind": "reference",
+                         "sample": f"the whole input ({n} strings, {char_bytes} bytes): the reference's "
+                                   f"prefix_doubling with {p} ranks (processes) on {cores} host cores, "
+                                   f"default policies, median sorting_overall of {args.steps} iterations after "
+                                   f"{args.warmup}"},
         "e2e": {"value": value, "unit": "strings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iteration_ms": [round(t * 1e3, 2) for t in times],
     }
     print(json.dumps(line), flush=True)
 
@@ -681,10 +704,9 @@ def main():
             "metric": "strings/s", "value": value, "unit": "strings/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded D/N generator)",
-            "config": {"workload": desc, "n": n, "len": L, "k": k, "p": p, "char_bytes": char_bytes,
-                       "l2": "inputs of %.2f GB > L2 (126 MB), no flush" % (char_bytes / 1e9),
-                       "parallelism": "one GPU holds all p PEs" if world == 1 else
-                       f"{world} ranks, one instance each (weak)"},
+            "config": config_of(cfg),
+            "char_bytes": char_bytes,
+            "parallelism": "one GPU holds all p PEs" if world == 1 else f"{world} ranks, one instance each (weak)",
             "char_gbs": char_bytes / (ms * 1e-3) / 1e9 * world,
             "roofline": {"bound": "hbm", "kernel": "k_dp_hash (all launches of one step)",
                          "achieved": hash_achieved, "peak": peak, "unit": "GB/s", "frac": hash_achieved / peak,

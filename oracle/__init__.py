@@ -30,9 +30,27 @@ _ref = None
 _ref_dp = None
 
 
+REF_EXE = os.path.join(HERE, "_ref", "prefix_doubling")
+REF_MP = os.path.join(HERE, "_ref", "ref_mp")
+
+
+def reference_tree():
+    """The reference checkout to compile oracle/_ref from: $DSSS_REFERENCE, else
+    the read-only checkout this build container mounts, else None (a machine
+    without it uses the prebuilt oracle/_ref)."""
+    for cand in (os.environ.get("DSSS_REFERENCE"), "/root/reference"):
+        if cand and os.path.exists(os.path.join(cand, "src", "hash", "xxhash.hpp")):
+            return cand
+    return None
+
+
 def build():
     """Compiles liboracle.so (and oracle/_ref when the reference tree is present)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    cmd = ["make", "-s", "-C", HERE]
+    tree = reference_tree()
+    if tree:
+        cmd.append("REF=" + tree)
+    subprocess.run(cmd, check=True)
 
 
 def lib():
@@ -57,10 +75,110 @@ def lib():
         L.oracle_pd_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.oracle_ms_sort.restype = _I
         L.oracle_ms_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.oracle_gen_dn.restype = _I
+        L.oracle_gen_dn.argtypes = [_U64, _U32, _U32, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P]
         L.oracle_hq_sort.restype = _I
         L.oracle_hq_sort.argtypes = [_P, _P, _P, _U64, _U32, _P, _U64, _P, _P]
         _lib = L
     return _lib
+
+
+def gen_dn(n, L, k, seed, long_len=0, long_k=0, frac_long=0.0):
+    """The D/N-rule input, generated by the oracle's own restatement of the
+    rule (no product code): a Strings of n strings, NUL-terminated back to
+    back."""
+    L_ = lib()
+    tot = ctypes.c_uint64(0)
+    rc = L_.oracle_gen_dn(n, L, k, long_len, long_k, frac_long, seed, None, None, None, ctypes.byref(tot))
+    assert rc == 0, rc
+    chars = np.zeros(tot.value + 64, np.uint8)
+    offsets = np.zeros(max(n, 1), np.uint64)
+    lengths = np.zeros(max(n, 1), np.uint32)
+    rc = L_.oracle_gen_dn(n, L, k, long_len, long_k, frac_long, seed, _p(chars), _p(offsets), _p(lengths),
+                          ctypes.byref(tot))
+    assert rc == 0, rc
+    s = Strings(chars, offsets[:n], lengths[:n])
+    s.char_bytes = tot.value
+    return s
+
+
+def write_lines(s, path):
+    """Writes the strings one per line (the reference's --generator 2 input:
+    FileDistributer turns every newline into the NUL terminator).  The strings
+    must be back to back, NUL-terminated, as gen_dn makes them."""
+    chars = s.chars[:s.char_bytes].copy()
+    chars[chars == 0] = 10
+    with open(path, "wb") as f:
+        f.write(memoryview(chars))
+
+
+def ref_exe_available() -> bool:
+    return os.path.exists(REF_EXE)
+
+
+def run_reference_pd(path, np_ranks, iterations, extra=(), timeout=3600, env=None):
+    """Runs the reference's own prefix_doubling executable (compiled into
+    oracle/_ref over the process-based MPI stand-in) on a file of strings with
+    np_ranks ranks: ``--generator 2 --path <file> --strongScaling``.  Returns
+    the per-iteration `sorting_overall` time in seconds (its maxTime RESULT
+    value: the slowest rank, src/util/timer.hpp) and the output."""
+    e = dict(os.environ)
+    e.update(env or {})
+    e["DSSS_MPI_NP"] = str(np_ranks)
+    cmd = [REF_EXE, "--generator", "2", "--path", path, "--strongScaling", "--numberOfIterations",
+           str(iterations), *extra]
+    out = subprocess.run(cmd, env=e, capture_output=True, text=True, timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference prefix_doubling failed ({out.returncode}): {out.stderr[-2000:]}")
+    times = {}
+    for line in out.stdout.splitlines():
+        if not line.startswith("RESULT") or "operation=sorting_overall" not in line or "type=maxTime" not in line:
+            continue
+        kv = dict(t.split("=", 1) for t in line.split()[1:] if "=" in t)
+        times[int(kv["iteration"])] = int(kv["value"]) * 1e-9
+    return [times[i] for i in sorted(times)], out.stdout
+
+
+def ref_mp_available() -> bool:
+    return os.path.exists(REF_MP)
+
+
+def run_reference_mp(mode, s, pb, timeout=600):
+    """Runs the reference's own distributed sorter (oracle/ref_bridge_mp.cpp:
+    mode "pd", "pdi", "ms" or "hq") with one process per PE over the
+    process-based MPI stand-in, PE q holding strings pb[q]..pb[q+1] of `s`.
+    Returns one dict per rank with that mode's arrays (see the bridge)."""
+    import tempfile
+    pb = np.ascontiguousarray(pb, dtype=np.uint64)
+    p = len(pb) - 1
+    raw = s.raw()
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.bin")
+        with open(inp, "wb") as f:
+            f.write(np.array([s.n, p], np.uint64).tobytes())
+            f.write(pb.tobytes())
+            f.write(np.array([len(raw)], np.uint64).tobytes())
+            f.write(raw)
+        e = dict(os.environ)
+        e["DSSS_MPI_NP"] = str(p)
+        e.setdefault("DSSS_MPI_ARENA_GB", "2")
+        out = subprocess.run([REF_MP, mode, inp, os.path.join(td, "out")], env=e, capture_output=True, text=True,
+                             timeout=timeout)
+        if out.returncode != 0:
+            raise RuntimeError(f"ref_mp {mode} failed ({out.returncode}): {out.stderr[-2000:]}")
+        names = {"pd": ("order", "lcp", "dp", "intervals", "perm"), "pdi": ("order", "lcp", "dp", "intervals", "perm"),
+                 "ms": ("bytes", "lcp"), "hq": ("bytes",)}[mode]
+        res = []
+        for q in range(p):
+            with open(os.path.join(td, f"out.{q}"), "rb") as f:
+                buf = f.read()
+            pos, d = 0, {}
+            for nm in names:
+                c = int(np.frombuffer(buf, np.uint64, 1, pos)[0])
+                d[nm] = np.frombuffer(buf, np.uint64, c, pos + 8).copy()
+                pos += 8 + 8 * c
+            res.append(d)
+    return res
 
 
 def ref_available() -> bool:
