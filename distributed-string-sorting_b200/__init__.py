@@ -149,6 +149,9 @@ _SIGS = {
     "dsss_gen_markov_text": (_I, [_U64, ctypes.c_double, _U64, _P]),
     "dsss_gen_suffixes": (_I, [_U64, _U32, _P, _P]),
     "dsss_gen_request": (_I, [_U64, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P]),
+    "dsss_gen_dn_dev": (_I, [_P, _U64, _U32, _U32, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P, _P]),
+    "dsss_gen_suffixes_dev": (_I, [_U64, _U32, _P, _P, _P]),
+    "dsss_gen_request_dev": (_I, [_P, _U64, _U32, _U32, ctypes.c_double, _U64, _P, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -272,6 +275,56 @@ def gen_request(n: int, seed: int, min_len: int = 8, max_len: int = 256, zipf_s:
     return HostStrings(chars, offs, lens, total)
 
 
+def gen_dn_device(ctx, n: int, length: int, k: int, seed: int = 1, long_len: int = 0, long_k: int = 0,
+                  frac_long: float = 0.0, stream=None) -> "DeviceStrings":
+    """gen_dn generated in device memory (dsss_gen_dn_dev): the same bytes,
+    no host round trip."""
+    import torch
+    dev = f"cuda:{ctx.device}"
+    cb = ctypes.c_uint64(0)
+    check(lib().dsss_gen_dn_dev(ctx.h, n, length, k, long_len, long_k, frac_long, seed, None, None, None,
+                                ctypes.byref(cb), _stream_ptr(stream)))
+    total = cb.value
+    chars = torch.zeros(total + PAD, dtype=torch.uint8, device=dev)
+    offs = torch.empty(max(n, 1), dtype=torch.int64, device=dev)[:n]
+    lens = torch.empty(max(n, 1), dtype=torch.int32, device=dev)[:n]
+    check(lib().dsss_gen_dn_dev(ctx.h, n, length, k, long_len, long_k, frac_long, seed, chars.data_ptr(),
+                                offs.data_ptr(), lens.data_ptr(), ctypes.byref(cb), _stream_ptr(stream)))
+    return DeviceStrings(None, chars=chars, offsets=offs, lengths=lens, char_bytes=total)
+
+
+def gen_request_device(ctx, n: int, seed: int, min_len: int = 8, max_len: int = 256, zipf_s: float = 1.2,
+                       stream=None) -> "DeviceStrings":
+    """gen_request generated in device memory (dsss_gen_request_dev)."""
+    import torch
+    dev = f"cuda:{ctx.device}"
+    cb = ctypes.c_uint64(0)
+    check(lib().dsss_gen_request_dev(ctx.h, n, min_len, max_len, zipf_s, seed, None, None, None, ctypes.byref(cb),
+                                     _stream_ptr(stream)))
+    total = cb.value
+    chars = torch.zeros(total + PAD, dtype=torch.uint8, device=dev)
+    offs = torch.empty(max(n, 1), dtype=torch.int64, device=dev)[:n]
+    lens = torch.empty(max(n, 1), dtype=torch.int32, device=dev)[:n]
+    check(lib().dsss_gen_request_dev(ctx.h, n, min_len, max_len, zipf_s, seed, chars.data_ptr(), offs.data_ptr(),
+                                     lens.data_ptr(), ctypes.byref(cb), _stream_ptr(stream)))
+    return DeviceStrings(None, chars=chars, offsets=offs, lengths=lens, char_bytes=total)
+
+
+def gen_suffix_strings_device(text_len: int, max_len: int = 256, seed: int = 1, copy_prob: float = 0.01,
+                              device="cuda", stream=None) -> "DeviceStrings":
+    """gen_suffix_strings with the suffix views made on the device
+    (dsss_gen_suffixes_dev); only the text (text_len bytes) is made on the
+    host and copied in."""
+    import torch
+    text = np.zeros(text_len + PAD, np.uint8)
+    check(lib().dsss_gen_markov_text(text_len, copy_prob, seed, _ptr(text)))
+    chars = torch.from_numpy(text).to(device)
+    offs = torch.empty(max(text_len, 1), dtype=torch.int64, device=device)[:text_len]
+    lens = torch.empty(max(text_len, 1), dtype=torch.int32, device=device)[:text_len]
+    check(lib().dsss_gen_suffixes_dev(text_len, max_len, offs.data_ptr(), lens.data_ptr(), _stream_ptr(stream)))
+    return DeviceStrings(None, chars=chars, offsets=offs, lengths=lens, char_bytes=text_len)
+
+
 def from_bytes_list(strs) -> HostStrings:
     """Arena of Python byte strings laid out back to back with NULs."""
     n = len(strs)
@@ -325,10 +378,17 @@ def batched_parts(set_begin, p: int) -> np.ndarray:
 
 # ------------------------------------------------------------------ device --
 class DeviceStrings:
-    """A device copy of HostStrings (torch tensors; chars padded with zeros)."""
+    """A device copy of HostStrings (torch tensors; chars padded with zeros),
+    or device tensors made by the device-side generators (hs=None)."""
 
-    def __init__(self, hs: HostStrings, device="cuda"):
+    def __init__(self, hs: Optional[HostStrings], device="cuda", chars=None, offsets=None, lengths=None,
+                 char_bytes=0):
         import torch
+        if hs is None:
+            self.chars, self.offsets, self.lengths = chars, offsets, lengths
+            self.char_bytes = int(char_bytes)
+            self.n = int(offsets.numel())
+            return
         self.chars = torch.from_numpy(hs.chars).to(device)
         self.offsets = torch.from_numpy(hs.offsets.view(np.int64)).to(device)
         self.lengths = torch.from_numpy(hs.lengths.view(np.int32)).to(device)
@@ -810,6 +870,17 @@ def adjacent_lcp_noalloc(ds: DeviceStrings, order, lcp, stream=None):
     """dsss_adjacent_lcp_noalloc: writes into the caller's lcp tensor and
     allocates nothing (see include/dsss.h)."""
     m = int(order.shape[0])
+    # the entry point trusts its pointers: a short or host-side output would
+    # be written out of bounds on the device
+    if not (getattr(lcp, "is_cuda", False) and getattr(order, "is_cuda", False)):
+        raise ValueError("order and lcp must be CUDA tensors")
+    if lcp.device != order.device or ds.chars.device != order.device:
+        raise ValueError("order, lcp and the strings must be on one device")
+    import torch
+    if lcp.dtype != torch.int32 or order.dtype != torch.int32:
+        raise ValueError("order and lcp must be int32 tensors")
+    if lcp.numel() < m or not lcp.is_contiguous() or not order.is_contiguous():
+        raise ValueError("lcp needs at least len(order) contiguous entries")
     check(lib().dsss_adjacent_lcp_noalloc(ctypes.byref(ds.arena()), _ptr(order), m, _ptr(lcp), _stream_ptr(stream)))
     return lcp
 

@@ -264,7 +264,7 @@ static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 // slot, NO_SLOT when the region is full.  The table always has free slots, so
 // a free or matching slot is reached within mask + 1 probes.
 __device__ __forceinline__ uint32_t table_insert(unsigned long long* tkeys, uint8_t* tdup, uint64_t base, uint32_t mask,
-                                                 unsigned long long h, uint32_t* err) {
+                                                 unsigned long long h, uint32_t* err, uint32_t* ndup) {
     uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
     for (uint32_t probe = 0;; ++probe) {
         if (probe > mask) {
@@ -275,6 +275,7 @@ __device__ __forceinline__ uint32_t table_insert(unsigned long long* tkeys, uint
         if (prev == EMPTY_KEY) break;
         if (prev == h) {
             tdup[base + sl] = 1;
+            atomicAdd(ndup, 1u);
             break;
         }
         sl = (sl + 1) & mask;
@@ -287,7 +288,7 @@ __device__ __forceinline__ uint32_t table_insert(unsigned long long* tkeys, uint
 __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
                           unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1, const uint64_t* set_begin,
                           uint32_t nsets, const uint64_t* set_base, const uint32_t* set_mask, uint32_t* slot,
-                          uint32_t* err) {
+                          uint32_t* err, uint32_t* ndup) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || kind[i] < 2) return;
     uint64_t base = 0;
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* 
         mask = set_mask[sid];
     }
     const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
-    slot[i] = table_insert(tkeys, tdup, base, mask, h, err);
+    slot[i] = table_insert(tkeys, tdup, base, mask, h, err, ndup);
 }
 
 // k_dp_hash for rounds that hash few positions (e.g. only the roots of long
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64
                                                         uint32_t depth, unsigned long long* tkeys, uint8_t* tdup,
                                                         uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
                                                         const uint64_t* set_base, const uint32_t* set_mask,
-                                                        uint32_t* slot, uint32_t* err) {
+                                                        uint32_t* slot, uint32_t* err, uint32_t* ndup) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         if (kind[i] < 2) continue;
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64
             mask = set_mask[sid];
         }
         const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
-        slot[i] = table_insert(tkeys, tdup, base, mask, h, err);
+        slot[i] = table_insert(tkeys, tdup, base, mask, h, err, ndup);
     }
 }
 
@@ -329,15 +330,17 @@ __global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64
 static int launch_dp_hash(const ArenaDev& a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
                           uint64_t hashed, unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1,
                           const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
-                          const uint32_t* set_mask, uint32_t* slot, uint32_t* err, cudaStream_t st) {
+                          const uint32_t* set_mask, uint32_t* slot, uint32_t* err, uint32_t* ndup,
+                          cudaStream_t st) {
     if (hashed * 8 < n) {
         DSSS_LAUNCH("k_dp_hash", st,
                     k_dp_hash_sparse<<<stride_grid(n), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1,
-                                                                     set_begin, nsets, set_base, set_mask, slot, err));
+                                                                     set_begin, nsets, set_base, set_mask, slot, err,
+                                                                     ndup));
     } else {
         DSSS_LAUNCH("k_dp_hash", st,
                     k_dp_hash<<<grid_for(n, 256), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1, set_begin,
-                                                               nsets, set_base, set_mask, slot, err));
+                                                               nsets, set_base, set_mask, slot, err, ndup));
     }
     return DSSS_OK;
 }
@@ -355,7 +358,8 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash_store(ArenaDev a, const uint
 __global__ void __launch_bounds__(256) k_dp_insert(const uint8_t* kind, uint64_t n, const unsigned long long* hbuf,
                                                    unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1,
                                                    const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
-                                                   const uint32_t* set_mask, uint32_t* slot, uint32_t* err) {
+                                                   const uint32_t* set_mask, uint32_t* slot, uint32_t* err,
+                                                   uint32_t* ndup) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || kind[i] < 2) return;
     uint64_t base = 0;
@@ -365,11 +369,50 @@ __global__ void __launch_bounds__(256) k_dp_insert(const uint8_t* kind, uint64_t
         base = set_base[sid];
         mask = set_mask[sid];
     }
-    slot[i] = table_insert(tkeys, tdup, base, mask, hbuf[i], err);
+    slot[i] = table_insert(tkeys, tdup, base, mask, hbuf[i], err, ndup);
 }
 
+// Dense hash rounds (a large share of the positions hash): the d-byte prefix
+// hash of every string of length >= d, computed in arena order so that the
+// prefixes are read front to back, one string after the next, and stored per
+// string.  The sorted-order insert (k_dp_insert_dig) then gathers one 8-byte
+// hash per hashed position instead of its d-byte prefix.  Strings that do not
+// hash in the round are hashed too (their hashes are never read).
+__global__ void __launch_bounds__(256) k_dp_digest(ArenaDev a, uint32_t depth, unsigned long long* dig) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    uint64_t off;
+    uint32_t L;
+    str_of(a, (uint32_t)i, off, L);
+    if (L < depth) return;
+    dig[i] = filter_hash(xxh64_dev(a.chars + off, depth));
+}
+
+__global__ void __launch_bounds__(256) k_dp_insert_dig(const uint32_t* order, const uint8_t* kind, uint64_t n,
+                                                       const unsigned long long* dig, unsigned long long* tkeys,
+                                                       uint8_t* tdup, uint32_t mask1, const uint64_t* set_begin,
+                                                       uint32_t nsets, const uint64_t* set_base,
+                                                       const uint32_t* set_mask, uint32_t* slot, uint32_t* err,
+                                                       uint32_t* ndup) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || kind[i] < 2) return;
+    uint64_t base = 0;
+    uint32_t mask = mask1;
+    if (nsets > 1) {
+        const uint32_t sid = set_of(set_begin, nsets, i);
+        base = set_base[sid];
+        mask = set_mask[sid];
+    }
+    slot[i] = table_insert(tkeys, tdup, base, mask, dig[order[i]], err, ndup);
+}
+
+// Kind-2 positions whose hash was inserted twice stay candidates.  Nothing to
+// do when no insert of the round met its own hash (ndup == 0): classification
+// already left every kind-2 position retired.
 __global__ void __launch_bounds__(256) k_dp_query(const uint8_t* kind, const uint32_t* slot, const uint8_t* tdup,
-                                                  uint64_t n, uint8_t* st_next, uint32_t* counters) {
+                                                  uint64_t n, uint8_t* st_next, uint32_t* counters,
+                                                  const uint32_t* ndup) {
+    if (*ndup == 0) return;
     uint32_t nstays = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -617,6 +660,9 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.filter_min = (uint64_t)tune(TUNE_DP_FILTER_MIN);
     L.filter_bpk = (uint32_t)tune(TUNE_DP_FILTER_BITS);
     L.split = tune(TUNE_DP_SPLIT) != 0;
+    // arena-order hashes for dense rounds (every string of the arena)
+    L.digest_share = (uint32_t)tune(TUNE_DP_DIGEST);
+    L.dig = L.digest_share ? c.take<unsigned long long>(N) : nullptr;
     const bool filter = N >= L.filter_min;
     L.hbuf = (filter || L.split) ? c.take<unsigned long long>(N) : nullptr;
     if (filter) {
@@ -725,20 +771,28 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
             if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
             DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
             DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-            if (L.split) {
+            if (L.dig && a.n <= n && (uint64_t)hashed * L.digest_share >= n) {
+                DSSS_LAUNCH("k_dp_digest", st,
+                            k_dp_digest<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, L.dig));
+                DSSS_LAUNCH("k_dp_insert_dig", st,
+                            k_dp_insert_dig<<<grid, 256, 0, st>>>(order, L.kind, n, L.dig, L.tkeys, L.tdup,
+                                                                 (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
+                                                                 L.set_mask, L.slot, L.counters + 2, L.counters + 8));
+            } else if (L.split) {
                 DSSS_LAUNCH("k_dp_hash_store", st,
                             k_dp_hash_store<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.hbuf));
                 DSSS_LAUNCH("k_dp_insert", st,
                             k_dp_insert<<<grid, 256, 0, st>>>(L.kind, n, L.hbuf, L.tkeys, L.tdup, (uint32_t)(slots - 1),
                                                              L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
-                                                             L.counters + 2));
+                                                             L.counters + 2, L.counters + 8));
             } else {
                 DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, (uint32_t)depth, hashed, L.tkeys, L.tdup,
                                         (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
-                                        L.counters + 2, st));
+                                        L.counters + 2, L.counters + 8, st));
             }
             DSSS_LAUNCH("k_dp_query", st,
-                        k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters));
+                        k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters,
+                                                                  L.counters + 8));
             DSSS_CUDA(cudaGetLastError());
             DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             DSSS_CUDA(cudaStreamSynchronize(st));
@@ -811,8 +865,10 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
         DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, depth, pin[0], L.tkeys, L.tdup, (uint32_t)(slots - 1), nullptr,
-                                1, nullptr, nullptr, L.slot, L.counters + 2, st));
-        DSSS_LAUNCH("k_dp_query", st, k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters));
+                                1, nullptr, nullptr, L.slot, L.counters + 2, L.counters + 8, st));
+        DSSS_LAUNCH("k_dp_query", st,
+                    k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters,
+                                                              L.counters + 8));
     }
     DSSS_LAUNCH("k_state_flags", st, k_state_flags<<<grid, 256, 0, st>>>(L.st[1], n, R.flag));
     DSSS_TRY(exclusive_scan_u32(R.flag, R.pos, n, R.total, R.scan, st));

@@ -31,6 +31,10 @@ struct DpLayout {
     unsigned long long* hbuf;  // also the stored hashes of the split hash round
     uint32_t* cand;
     bool split;  // hash round as k_dp_hash_store + k_dp_insert
+    // dense rounds (hashed * digest_share >= positions): hashes computed per
+    // string in arena order (k_dp_digest), then gathered by sorted position
+    uint32_t digest_share;
+    unsigned long long* dig;
     uint64_t* set_bbase;
     uint32_t* set_bmask;
     uint32_t* set_ccnt;

@@ -136,6 +136,8 @@ enum TuneKnob : int {
     TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
     TUNE_DP_SPLIT,           // hash round split into hashing and table inserts (1) or one kernel (0)
     TUNE_COPY_WORD,          // bytes per store when whole strings are copied out (16, or 8)
+    TUNE_DP_DIGEST,          // hash rounds in which at least 1/k of the positions hash read the prefixes in
+                             // arena order (k_dp_digest); 0 turns the arena-order form off
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

@@ -87,6 +87,7 @@ int dsss_varint_encode(dsss_ctx* ctx, const uint32_t* values, uint64_t n, const 
     ActiveCtx active(ctx);
     if (!out_bytes || (nranges && (!range_begin || !range_bytes))) return fail(DSSS_EINVAL, "output pointers missing");
     if (n && !values) return fail(DSSS_EINVAL, "values is NULL");
+    if (nranges && range_begin[0] != 0) return fail(DSSS_EINVAL, "range_begin must start at 0");
     for (uint32_t r = 0; r < nranges; ++r)
         if (range_begin[r] > range_begin[r + 1] || range_begin[r + 1] > n)
             return fail(DSSS_EINVAL, "range_begin must rise from 0 to at most n");

@@ -129,7 +129,13 @@ int dsss_abi_version(void);
  *                   stored per position then inserted into the table (1), or
  *                   hash and insert in one kernel (0, default)
  *   copy_word       dsss_ms_sort / dsss_hq_sort: bytes per aligned store when
- *                   the output strings are copied out (16, default, or 8) */
+ *                   the output strings are copied out (16, default, or 8)
+ *   dp_digest       distinguishing-prefix hash rounds in which at least 1/k
+ *                   of the positions hash compute every string's prefix hash
+ *                   in arena order (prefixes read front to back) and gather
+ *                   one 8-byte hash per sorted position (k = 1..64, default
+ *                   4); 0 hashes every round by gathering the prefixes in
+ *                   sorted order */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 
@@ -536,6 +542,22 @@ int dsss_gen_suffixes(uint64_t text_len, uint32_t max_len, uint64_t* offsets, ui
  * uniform in [0, len/2].  Layout as dsss_gen_dn. */
 int dsss_gen_request(uint64_t n, uint32_t min_len, uint32_t max_len, double zipf_s, uint64_t seed,
                      uint8_t* chars, uint64_t* offsets, uint32_t* lengths, uint64_t* char_bytes);
+
+/* The same generators writing device memory, so that a configuration's input
+ * never crosses PCIe (the reference's generators build each PE's strings in
+ * place, util/random_string_generator.hpp:167-318, :432-509).  Byte for byte
+ * the host generators' output; chars, offsets and lengths are device
+ * pointers (chars 16-byte aligned), the call is asynchronous on `stream`
+ * except for the read-back of the total.  chars == NULL: *char_bytes only.
+ * Errors: DSSS_EINVAL (arguments, n >= 2^32), DSSS_ENOMEM (scratch). */
+int dsss_gen_dn_dev(dsss_ctx* ctx, uint64_t n, uint32_t len_short, uint32_t k_short, uint32_t len_long,
+                    uint32_t k_long, double frac_long, uint64_t seed, uint8_t* chars, uint64_t* offsets,
+                    uint32_t* lengths, uint64_t* char_bytes, dsss_stream_t stream);
+int dsss_gen_suffixes_dev(uint64_t text_len, uint32_t max_len, uint64_t* offsets, uint32_t* lengths,
+                          dsss_stream_t stream);
+int dsss_gen_request_dev(dsss_ctx* ctx, uint64_t n, uint32_t min_len, uint32_t max_len, double zipf_s,
+                         uint64_t seed, uint8_t* chars, uint64_t* offsets, uint32_t* lengths, uint64_t* char_bytes,
+                         dsss_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -165,3 +165,31 @@ def test_copy_word_lengths(dsss, orc, ctx, w):
     with dsss.tuned(copy_word=w):
         hq = dsss.hq_sort(ctx, dsss.DeviceStrings(hs), 2, part_begin=pb)
     check_hq(dsss, orc, hs, hq, pb)
+
+
+@pytest.mark.parametrize("share", [0, 1, 64])
+@pytest.mark.parametrize("name,strs", CASES, ids=IDS)
+def test_dp_digest(dsss, orc, ctx, name, strs, share):
+    """Dense hash rounds with the prefixes hashed in arena order (share 64:
+    nearly every round; 1: only rounds where every position hashes; 0: off):
+    the oracle's result."""
+    hs = host_of(dsss, strs)
+    with dsss.tuned(dp_digest=share):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 3)
+    check_pd(dsss, orc, hs, out, 3)
+
+
+def test_dp_digest_batched(dsss, ctx):
+    """Arena-order hashes over per-set table regions: each set's own result."""
+    h1 = dsss.gen_dn(20000, 100, 50, seed=35)
+    h2 = dsss.gen_suffix_strings(30000, 256, seed=7)
+    hs, sb = dsss.concat_sets([h1, h2, h1])
+    pb = dsss.batched_parts(sb, 4)
+    with dsss.tuned(dp_digest=64):
+        out = dsss.pd_sort_batched(ctx, dsss.DeviceStrings(hs), 3, 4, pb)
+    with dsss.tuned(dp_digest=0):
+        for s, h in enumerate([h1, h2, h1]):
+            ref = dsss.pd_sort(ctx, dsss.DeviceStrings(h), 4)
+            b, e = int(sb[s]), int(sb[s + 1])
+            assert np.array_equal(u64(out["dp"], hs.n)[b:e], u64(ref["dp"], h.n)), s
+            assert np.array_equal(u64(out["perm_index"], hs.n)[b:e], u64(ref["perm_index"], h.n)), s

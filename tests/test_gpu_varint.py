@@ -52,3 +52,16 @@ def test_dist_gpu_compressed_lcps(orc):
     pb = [0, n // 4, n // 2, (3 * n) // 4, n]
     res = run_ranks(2, (strs, pb, [0, 1, 4], 0, True), "gpu")
     check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
+
+
+def test_varint_encode_rejects_ranges_not_starting_at_zero(dsss, ctx):
+    """range_begin must start at 0: a first bound past 0 would leave values
+    before it coded but counted in no range."""
+    import ctypes
+    v = torch.arange(8, dtype=torch.int32, device="cuda")
+    rb = np.array([1, 5, 8], np.uint64)
+    tot = ctypes.c_uint64(0)
+    per = np.zeros(2, np.uint64)
+    rc = dsss.lib().dsss_varint_encode(ctx.h, v.data_ptr(), 8, rb.ctypes.data, 2, None, 0, ctypes.byref(tot),
+                                       per.ctypes.data, None)
+    assert rc == -22  # DSSS_EINVAL
