@@ -7,15 +7,17 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   value     strings/s with the input resident in HBM (device-timed, max over ranks)
   e2e       the same metric through dsss_pd_sort_host: pinned host input copied
             in, results copied out, inside the timed region
-  roofline  the dominant kernel, k_dp_hash (the distinguishing-prefix hash
-            rounds), against HBM: algorithmic bytes d + 16 for every string
-            hashed at its final depth d (its prefix read once, the 8-byte hash
-            written and read; roots hashed in earlier rounds are not counted,
-            so this is a lower bound) over the summed CUDA-event durations of
-            its launches; traffic = DRAM bytes per hashed string from one ncu
-            capture (profiles/k_dp_hash_dn8m.md) times the strings hashed
-  roofline_sort  the string sort stage (K3) the same way: D + 20 n (D = sum of
-            DP lengths, 8 B id read + 8 B id write + 4 B LCP write per string)
+  roofline  the dominant kernel of one sort against HBM: algorithmic bytes
+            per launch over its CUDA-event launch time (the formulas are
+            listed in ROOFLINE_BYTES); traffic = DRAM bytes per unit from one
+            ncu capture on 8e6 strings times the units of one launch (a
+            capture of the full launch is beyond the capture-size rule)
+  rooflines the same figure for every kernel with a formula, and for the
+            string sort stage (D + 20 n, D = sum of DP lengths: 8 B id read +
+            8 B id write + 4 B LCP write per string) and for the sort plus
+            merge stages (D + 20 n + sum(DP - lcp + 1) + 24 n)
+  dn100m    the same sort of 1e8 strings x 100 B (D/N 0.5, p = 64),
+            generated on the device, with its own rooflines
   ms_path   the merge-sort path (dsss_ms_sort) on the same input, device-timed
   hq_path   hQuicksort (dsss_hq_sort, the reference's RQuick competitor) on
             the same input, device-timed
@@ -56,10 +58,14 @@ CONFIGS = {
 }
 
 
-# DRAM bytes (read + write) per hashed string of k_dp_hash's dense round, from
-# one ncu capture on 8e6 strings x 200 B (profiles/k_dp_hash_dn8m.md); the
-# traffic grows with the strings hashed.
-DP_HASH_DRAM_PER_STRING = 316.6
+# DRAM bytes (read + write) per unit of the kernels that carry a roofline,
+# from one ncu capture each on 8e6 strings x 200 B (D/N 0.25, p = 64); the
+# traffic of a launch grows with its units.  None: not captured.
+DRAM_PER_UNIT = {
+    "k_dp_arena_insert": None,
+    "k_dp_hash": None,
+    "k_seg_sort1024": None,
+}
 
 
 def read_peaks():
@@ -485,6 +491,110 @@ def run_path(args, cfg, which):
     print(json.dumps(line), flush=True)
 
 
+# Algorithmic bytes of the kernels that carry a roofline, per step of one
+# sort (the units a step's launches process):
+#   DP hash round (k_dp_arena_insert in arena order, k_dp_hash in sorted
+#   order): d + 16 for every string hashed at its final depth d (its d-byte
+#   prefix read once, its 8-byte hash written to the table and read back);
+#   roots hashed in earlier rounds are not counted, so this is a lower bound.
+ROOFLINE_BYTES = {
+    "k_dp_arena_insert": "sum over strings hashed at their final depth d of (d + 16)",
+    "k_dp_hash": "sum over strings hashed at their final depth d of (d + 16)",
+}
+SORT_KERNELS = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
+                "k_scatter", "k_seg_sort", "k_warp_segs", "k_spec", "k_pivot", "k_seg_offsets", "scan_")
+
+
+def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True):
+    """Rooflines of one dsss_pd_sort step from its per-kernel event times."""
+    kernels = {k: v for k, v in kt.items() if not k.startswith("stage:")}
+    stages = {k[6:]: v[1] / steps for k, v in kt.items() if k.startswith("stage:")}
+    dp = out["dp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
+    lcp = out["merged_lcp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
+    D = int(dp.sum())
+    sched = np.array([8] + [8 + (16 << j) for j in range(26)], np.uint64)
+    hashed_final = np.isin(dp, sched)
+    hash_bytes = int(dp[hashed_final].sum()) + 16 * int(hashed_final.sum())
+    b_sort = D + 20 * n
+    b_merge = int((dp - np.minimum(lcp, dp) + 1).sum()) + 24 * n
+    sort_ms = sum(v[1] for k, v in kernels.items() if k.startswith(SORT_KERNELS)) / steps
+    sort_launches = sum(v[0] for k, v in kernels.items() if k.startswith(SORT_KERNELS)) / steps
+
+    def line(kernel, algo, ms, launches, formula, traffic=None, note=None):
+        ach = algo / (ms * 1e-3) / 1e9 if ms > 0 else float("nan")
+        r = {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+             "peak_kind": peak_kind, "traffic": traffic, "algo_bytes": algo, "algo_formula": formula,
+             "kernel_ms": ms, "launches": launches}
+        if note:
+            r["traffic_note"] = note
+        return r
+
+    per = {}
+    for k, formula in ROOFLINE_BYTES.items():
+        if k not in kernels:
+            continue
+        launches = kernels[k][0] / steps
+        ms = kernels[k][1] / steps
+        unit = DRAM_PER_UNIT.get(k)
+        traffic = unit * int(hashed_final.sum()) / max(launches, 1) if (unit and traffic_known) else None
+        # per launch: the step's bytes over its launches
+        per[k] = line(k, hash_bytes / max(launches, 1), ms / max(launches, 1), launches, formula + " (per launch)",
+                      traffic, "ncu DRAM bytes per hashed string on 8e6 strings x 200 B, times the strings hashed"
+                      if traffic is not None else "not captured for this string mix")
+    top = max(kernels.items(), key=lambda kv: kv[1][1])[0] if kernels else None
+    rl = {
+        "sort_stage": line("string sort K3 (all launches of the sort stage)", b_sort, sort_ms, sort_launches,
+                           "D + 20 n"),
+        "sort_merge": line("sort + merge stages (north-star target)", b_sort + b_merge,
+                           stages.get("sort", 0.0) + stages.get("merge", 0.0), None,
+                           "D + 20 n + sum(DP - lcp + 1) + 24 n"),
+    }
+    rl.update(per)
+    # the headline: the DP hash-round kernel that carries a formula, the
+    # largest kernel of the step
+    main = max(per.values(), key=lambda r: r["kernel_ms"] * (r["launches"] or 1)) if per else rl["sort_stage"]
+    return {"roofline": dict(main, top_kernel=top), "rooflines": rl, "stages_ms": stages,
+            "kernels_ms": {k: round(v[1] / steps, 4) for k, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
+            "launches_per_step": sum(v[0] for v in kernels.values()) / steps}
+
+
+def bench_config_device(d, torch, name, steps, warmup, peak, peak_kind):
+    """One configuration's dsss_pd_sort with its input generated on the
+    device (dsss_gen_dn_dev), device-timed, with its stage and kernel times
+    and rooflines."""
+    n, L, k, p, desc, gk = CONFIGS[name]
+    ctx = d.Context(torch.cuda.current_device())
+    ds = d.gen_dn_device(ctx, n, L, k, seed=1, **gk)
+    stream = torch.cuda.current_stream()
+    out = None
+    for _ in range(warmup):
+        out = d.pd_sort(ctx, ds, p, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = d.pd_sort(ctx, ds, p, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ctx.set_timing(True)
+    for _ in range(steps):
+        out = d.pd_sort(ctx, ds, p, out=out)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    lengths = ds.lengths.cpu().numpy().view(np.uint32)
+    roof = pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=False)
+    res = {"workload": desc + " (generated on the device)", "n": n, "len": L, "p": p, "steps": steps,
+           "ms_per_step": ms, "strings_per_s": n / (ms * 1e-3),
+           "char_gbs": (int(lengths.astype(np.uint64).sum()) + n) / (ms * 1e-3) / 1e9,
+           "roofline": roof["roofline"], "rooflines": roof["rooflines"], "stages_ms": roof["stages_ms"],
+           "kernels_ms": dict(list(roof["kernels_ms"].items())[:16])}
+    del out, ds
+    ctx.close()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,6 +609,7 @@ def main():
     ap.add_argument("--no-ms", action="store_true", help="skip the merge-sort path line")
     ap.add_argument("--no-hq", action="store_true", help="skip the hQuicksort line")
     ap.add_argument("--no-formats", action="store_true", help="skip the line distribution and varint lines")
+    ap.add_argument("--no-dn100m", action="store_true", help="skip the 1e8-string configuration")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
     ap.add_argument("--mode", default="replicas", choices=["replicas", "dist", "ms", "hq"],
                     help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL); "
@@ -574,29 +685,19 @@ def main():
     torch.cuda.synchronize()
     kt = ctx.kernel_times()
     ctx.set_timing(False)
-    kernels = {k2: v for k2, v in kt.items() if not k2.startswith("stage:")}
-    stages = {k2[6:]: v[1] / args.steps for k2, v in kt.items() if k2.startswith("stage:")}
-    launches_per_step = sum(v[0] for v in kernels.values()) / args.steps
-    sort_kernels = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
-                    "k_scatter", "k_seg_sort", "k_warp_segs", "scan_")
-    # sort launches of the partition's sample sort are tiny; all sort-kernel time counts
-    sort_ms = sum(v[1] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps
-    sort_launches = sum(v[0] for k2, v in kernels.items() if k2.startswith(sort_kernels)) / args.steps
-
-    dp = out["dp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
-    D = int(dp.sum())
-    algo_bytes = D + 20 * n
     peak, peak_kind = read_peaks()
-    achieved = algo_bytes / (sort_ms * 1e-3) / 1e9
-    # the hash rounds: strings hashed at their final depth (dp on the depth schedule)
-    sched = np.array([8] + [8 + (16 << j) for j in range(26)], np.uint64)
-    hashed_final = np.isin(dp, sched)
-    hash_bytes = int(dp[hashed_final].sum()) + 16 * int(hashed_final.sum())
-    hash_ms = kernels["k_dp_hash"][1] / args.steps if "k_dp_hash" in kernels else float("nan")
-    hash_launches = kernels["k_dp_hash"][0] / args.steps if "k_dp_hash" in kernels else 0
-    hash_achieved = hash_bytes / (hash_ms * 1e-3) / 1e9
+    roof = pd_rooflines(out, hs.lengths, n, kt, args.steps, peak, peak_kind, traffic_known=not gk)
     char_bytes = int(hs.lengths.astype(np.uint64).sum()) + n
     value = n * world / (ms * 1e-3)
+
+    # the 1e8-string configuration (generated on the device), one GPU
+    dn100m = None
+    if world == 1 and not args.no_dn100m and args.config != "dn100m":
+        del out
+        out = None
+        torch.cuda.empty_cache()
+        dn100m = bench_config_device(d, torch, "dn100m", max(3, min(args.steps, 10)), 3, peak, peak_kind)
+        torch.cuda.empty_cache()
 
     # e2e through the host entry point
     e2e = None
@@ -708,24 +809,13 @@ def main():
             "char_bytes": char_bytes,
             "parallelism": "one GPU holds all p PEs" if world == 1 else f"{world} ranks, one instance each (weak)",
             "char_gbs": char_bytes / (ms * 1e-3) / 1e9 * world,
-            "roofline": {"bound": "hbm", "kernel": "k_dp_hash (all launches of one step)",
-                         "achieved": hash_achieved, "peak": peak, "unit": "GB/s", "frac": hash_achieved / peak,
-                         "peak_kind": peak_kind,
-                         "traffic": None if gk else DP_HASH_DRAM_PER_STRING * int(hashed_final.sum()),
-                         "traffic_note": "not measured for this string mix" if gk else
-                                         "ncu dram bytes read+write per hashed string of the dense round on 8e6 "
-                                         "strings (profiles/k_dp_hash_dn8m.md), times the strings hashed",
-                         "algo_bytes": hash_bytes,
-                         "algo_formula": "sum over strings hashed at their final depth d of (d + 16); lower bound",
-                         "kernel_ms": hash_ms, "launches": hash_launches},
-            "roofline_sort": {"bound": "hbm", "kernel": "string sort K3 (all launches of the sort stage)",
-                              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                              "peak_kind": peak_kind, "traffic": None, "algo_bytes": algo_bytes,
-                              "algo_formula": "D + 20 n", "sort_ms": sort_ms, "sort_launches": sort_launches},
+            "roofline": roof["roofline"],
+            "rooflines": roof["rooflines"],
             "tuning": tuning,
-            "stages_ms": stages,
-            "kernels_ms": {k2: round(v[1] / args.steps, 4) for k2, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
-            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "stages_ms": roof["stages_ms"],
+            "kernels_ms": roof["kernels_ms"],
+            "gpu_launches": int(round(roof["launches_per_step"] * args.steps)),
+            "dn100m": dn100m,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "e2e": e2e,

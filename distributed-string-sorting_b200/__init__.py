@@ -105,6 +105,10 @@ _SIGS = {
     "dsss_distribute_lines": (_I, [_P, _P, _U64, _U64, _U32, _P, _U64, _P, _P, _U64, _P, _P, _P, _P]),
     "dsss_varint_encode": (_I, [_P, _P, _U64, _P, _U32, _P, _U64, _P, _P, _P]),
     "dsss_varint_decode": (_I, [_P, _P, _U64, _P, _U64, _P]),
+    "dsss_golomb_param": (_U64, [_U64, _U64]),
+    "dsss_golomb_param_hashes": (_U64, [_U64, _U32]),
+    "dsss_golomb_encode": (_I, [_P, _P, _P, _U32, _P, _P, _U64, ctypes.POINTER(_U64), _P, _P]),
+    "dsss_golomb_decode": (_I, [_P, _P, _U64, _P, _U64, ctypes.POINTER(_U64), _P, _U32, ctypes.POINTER(_U32), _P]),
     "dsss_pd_sort_host": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, ctypes.POINTER(Opts), ctypes.POINTER(PdResult),
                                _P]),
     "dsss_pd_sort_batched": (_I, [_P, ctypes.POINTER(Arena), _U32, _U32, _P, ctypes.POINTER(Opts),
@@ -116,6 +120,7 @@ _SIGS = {
                                    _P]),
     "dsss_hash_route": (_I, [_P, _P, _P, _U64, _U32, _P, _P, _P, _P]),
     "dsss_hash_dups": (_I, [_P, _P, _U64, _P, _P]),
+    "dsss_hash_sort": (_I, [_P, _P, _P, _U64, _P, _P, _P]),
     "dsss_dp_apply": (_I, [_P, _P, _P, _U64, _P, _U64, ctypes.POINTER(_U64), _P]),
     "dsss_pack_strings": (_I, [_P, ctypes.POINTER(Arena), _P, _P, _U64, _P, _U64, _P, _P, ctypes.POINTER(_U64), _P]),
     "dsss_partition_search": (_I, [_P, ctypes.POINTER(Arena), _U32, _P, _P, ctypes.POINTER(Arena), _P, _U32, _P, _I,
@@ -576,6 +581,50 @@ def varint_decode(ctx: Context, data, n: int, stream=None):
     check(lib().dsss_varint_decode(ctx.h, _ptr(data) if data.numel() else None, int(data.numel()), _ptr(out), n,
                                    _stream_ptr(stream)))
     return out[:n]
+
+
+def golomb_param(max_value: int, count: int) -> int:
+    """getB of the reference's Golomb coder (dsss_golomb_param)."""
+    return int(lib().dsss_golomb_param(max_value, count))
+
+
+def golomb_param_hashes(count: int, p: int) -> int:
+    """b of the hash exchange for count hashes sent to one of p PEs."""
+    return int(lib().dsss_golomb_param_hashes(count, p))
+
+
+def golomb_encode(ctx: Context, values, range_counts, b, stream=None):
+    """Golomb/delta blocks (dsss_golomb_encode) of ascending device uint64
+    values (a torch int64 tensor viewed as unsigned) in ranges of
+    range_counts values with parameters b: (device words, words per range)."""
+    import torch
+    rc = np.ascontiguousarray(range_counts, dtype=np.uint64)
+    bb = np.ascontiguousarray(b, dtype=np.uint64)
+    nw = ctypes.c_uint64(0)
+    rw = np.zeros(max(len(rc), 1), np.uint64)
+    vp = _ptr(values) if values.numel() else None
+    check(lib().dsss_golomb_encode(ctx.h, vp, _ptr(rc), len(rc), _ptr(bb), None, 0, ctypes.byref(nw), _ptr(rw),
+                                   _stream_ptr(stream)))
+    out = torch.empty(max(nw.value, 1), dtype=torch.int64, device=values.device)
+    check(lib().dsss_golomb_encode(ctx.h, vp, _ptr(rc), len(rc), _ptr(bb), _ptr(out), nw.value, ctypes.byref(nw),
+                                   _ptr(rw), _stream_ptr(stream)))
+    return out[:nw.value], rw[:len(rc)]
+
+
+def golomb_decode(ctx: Context, words, max_blocks: int = 1 << 16, stream=None):
+    """Values (device int64 tensor) and values per block of back-to-back
+    Golomb/delta blocks (dsss_golomb_decode)."""
+    import torch
+    n = ctypes.c_uint64(0)
+    nb = ctypes.c_uint32(0)
+    bc = np.zeros(max(max_blocks, 1), np.uint64)
+    wp = _ptr(words) if words.numel() else None
+    check(lib().dsss_golomb_decode(ctx.h, wp, int(words.numel()), None, 0, ctypes.byref(n), _ptr(bc), max_blocks,
+                                   ctypes.byref(nb), _stream_ptr(stream)))
+    out = torch.empty(max(n.value, 1), dtype=torch.int64, device=words.device)
+    check(lib().dsss_golomb_decode(ctx.h, wp, int(words.numel()), _ptr(out), n.value, ctypes.byref(n), _ptr(bc),
+                                   max_blocks, ctypes.byref(nb), _stream_ptr(stream)))
+    return out[:n.value], bc[:nb.value]
 
 
 def pd_sort_host(ctx: Context, hs: HostStrings, p: int, part_begin=None, sampler: int = 0, merged_lcp: bool = True,

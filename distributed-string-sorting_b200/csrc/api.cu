@@ -137,6 +137,7 @@ struct PdLayout {
     SortLayout sort;
     DpLayout dp;
     PartitionLayout part;
+    unsigned long long* rdig;  // prefix hashes at the first schedule depths, from the sort's first pass
 };
 
 // n strings in nsets sets of p PEs each.
@@ -163,6 +164,7 @@ static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t nsets, uint32_
     layout_sort(c, L.sort, N, nsets, small_max);
     layout_dp(c, L.dp, N, nsets);
     layout_partition(c, L.part, N, p, factor, nsets);
+    L.rdig = L.dp.hmask ? c.take<unsigned long long>(ROOT_DIGESTS * N) : nullptr;
 }
 
 // The fused path over nsets independent string sets of p PEs each (PE q of
@@ -213,9 +215,11 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     a.h = L.handles;
     DSSS_CUDA(cudaMemsetAsync(L.err, 0, sizeof(uint32_t), st));
     // 1. one sort per set, all sets in one segmented sort
+    bool rdig_done = false;
     {
         StageTimer t("stage:sort", st);
-        DSSS_TRY(sort_strings(L.sort, a, n, nsets, set_begin.data(), nullptr, L.ord, L.lcp, smax, pin, st));
+        DSSS_TRY(sort_strings(L.sort, a, n, nsets, set_begin.data(), nullptr, L.ord, L.lcp, smax, pin, st,
+                              p > 1 ? L.rdig : nullptr, &rdig_done));
     }
     if (p == 1) {  // prefix_doubling.hpp:236: one PE sorts locally and returns no permutation
         DSSS_CUDA(cudaMemcpyAsync(out->local_order, L.ord, n * 4, cudaMemcpyDeviceToDevice, st));
@@ -226,7 +230,8 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     // 2. distinguishing prefixes over each set's sorted order
     {
         StageTimer t("stage:dp", st);
-        DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st, nsets, set_begin.data()));
+        DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st, nsets, set_begin.data(),
+                           rdig_done ? L.rdig : nullptr));
     }
     // 3. local orders per PE
     StageTimer t_local("stage:local", st);

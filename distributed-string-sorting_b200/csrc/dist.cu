@@ -112,6 +112,25 @@ int dsss_hash_route(dsss_ctx* ctx, const uint64_t* hval, const uint32_t* hpos, u
                       counts, (cudaStream_t)stream);
 }
 
+int dsss_hash_sort(dsss_ctx* ctx, const uint64_t* hval, const uint32_t* hpos, uint64_t m, uint64_t* out_hval,
+                   uint32_t* out_hpos, dsss_stream_t stream) {
+    if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
+    ActiveCtx active(ctx);
+    if (m && (!hval || !hpos || !out_hval || !out_hpos)) return fail(DSSS_EINVAL, "array is NULL");
+    if (m && ((const void*)hval == (const void*)out_hval || (const void*)hpos == (const void*)out_hpos))
+        return fail(DSSS_EINVAL, "the output may not be the input");
+    if (m >= (1ull << 32)) return fail(DSSS_ENOTSUP, "2^32 or more hash records");
+    DSSS_CUDA(cudaSetDevice(ctx->device));
+    Carve sz(nullptr);
+    HashSortLayout L;
+    layout_hash_sort(sz, L, m);
+    DSSS_TRY(ensure_ws(ctx, sz.used));
+    Carve c(ctx->ws);
+    layout_hash_sort(c, L, m);
+    return hash_sort(L, (const unsigned long long*)hval, hpos, m, (unsigned long long*)out_hval, out_hpos,
+                     (cudaStream_t)stream);
+}
+
 int dsss_hash_dups(dsss_ctx* ctx, const uint64_t* hval, uint64_t m, uint8_t* dup, dsss_stream_t stream) {
     if (!ctx) return fail(DSSS_EINVAL, "ctx is NULL");
     ActiveCtx active(ctx);

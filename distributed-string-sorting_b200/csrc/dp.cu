@@ -116,12 +116,18 @@ __device__ __forceinline__ void block_add(uint32_t* ctr, uint32_t v) {
     __syncthreads();
 }
 
+// Sets string s's bit in an arena-order bitmap (the strings hashed by a
+// dense round, which runs in arena order).
+__device__ __forceinline__ void mark_string(uint32_t* m, uint32_t s) { atomicOr(&m[s >> 5], 1u << (s & 31)); }
+
 // Grid-stride over positions (grid a few blocks per SM): one pair of counter
-// atomics per block instead of per 256 positions.
+// atomics per block instead of per 256 positions.  hmask (with order): every
+// hashed string is marked for the arena-order form of the round.
 __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all, const uint32_t* lens,
                                                      const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
                                                      uint8_t* st_next, uint8_t* kind, uint32_t* counters,
-                                                     const uint64_t* set_begin, uint32_t nsets, uint32_t* set_cnt) {
+                                                     const uint64_t* set_begin, uint32_t nsets, uint32_t* set_cnt,
+                                                     const uint32_t* order = nullptr, uint32_t* hmask = nullptr) {
     uint32_t nhashed = 0, nstays = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x % 32 < n; i += stride) {
@@ -149,6 +155,7 @@ __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all,
             st_next[i] = nx;
             nstays += nx;
             nhashed += hashed;
+            if (hashed && hmask) mark_string(hmask, order[i]);
         }
         if (nsets > 1) {  // hashed strings per set size the per-set table regions
             const int lane = threadIdx.x & 31;
@@ -166,7 +173,8 @@ __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all,
 // per-position rule; st of the neighbours i - 1 and i + 4 read singly).
 __global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all, const uint32_t* lens,
                                                       const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
-                                                      uint8_t* st_next, uint8_t* kind, uint32_t* counters) {
+                                                      uint8_t* st_next, uint8_t* kind, uint32_t* counters,
+                                                      const uint32_t* order = nullptr, uint32_t* hmask = nullptr) {
     uint32_t nhashed = 0, nstays = 0;
     const uint64_t groups = n >> 2;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -216,6 +224,7 @@ __global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all
             K[q] = k;
             X[q] = nx;
             nstays += nx;
+            if (k >= 2 && hmask) mark_string(hmask, order[i]);
         }
         if (all) {
             reinterpret_cast<uint4*>(dp)[t] = make_uint4(D[0], D[1], D[2], D[3]);
@@ -247,6 +256,7 @@ __global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all
                     k = root ? 3 : 2;
                     nx = root ? 1 : 0;
                     ++nhashed;
+                    if (hmask) mark_string(hmask, order[i]);
                 }
             }
         }
@@ -304,24 +314,47 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* 
 
 // k_dp_hash for rounds that hash few positions (e.g. only the roots of long
 // runs of LCP-local duplicates): a few blocks per SM stride over the kind
-// array instead of one thread per position.
+// array, 16 positions per 16-byte load, instead of one thread per position.
 __global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n,
                                                         uint32_t depth, unsigned long long* tkeys, uint8_t* tdup,
                                                         uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
                                                         const uint64_t* set_base, const uint32_t* set_mask,
                                                         uint32_t* slot, uint32_t* err, uint32_t* ndup) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        if (kind[i] < 2) continue;
-        uint64_t base = 0;
-        uint32_t mask = mask1;
-        if (nsets > 1) {
-            const uint32_t sid = set_of(set_begin, nsets, i);
-            base = set_base[sid];
-            mask = set_mask[sid];
+    const uint64_t groups = (n + 15) / 16;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += stride) {
+        uint32_t w[4];
+        if (g * 16 + 16 <= n) {  // kind is 16-byte aligned (scratch carving)
+            const uint4 v = reinterpret_cast<const uint4*>(kind)[g];
+            w[0] = v.x;
+            w[1] = v.y;
+            w[2] = v.z;
+            w[3] = v.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                w[q] = 0;
+                for (int b = 0; b < 4; ++b) {
+                    const uint64_t i = g * 16 + 4 * q + b;
+                    if (i < n) w[q] |= (uint32_t)kind[i] << (8 * b);
+                }
+            }
         }
-        const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
-        slot[i] = table_insert(tkeys, tdup, base, mask, h, err, ndup);
+        // kinds are 0..3: bit 1 of a byte marks a hashed position
+        if (!((w[0] | w[1] | w[2] | w[3]) & 0x02020202u)) continue;
+        for (int b = 0; b < 16; ++b) {
+            if (!((w[b >> 2] >> (8 * (b & 3))) & 2u)) continue;
+            const uint64_t i = g * 16 + b;
+            uint64_t base = 0;
+            uint32_t mask = mask1;
+            if (nsets > 1) {
+                const uint32_t sid = set_of(set_begin, nsets, i);
+                base = set_base[sid];
+                mask = set_mask[sid];
+            }
+            const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+            slot[i] = table_insert(tkeys, tdup, base, mask, h, err, ndup);
+        }
     }
 }
 
@@ -334,7 +367,7 @@ static int launch_dp_hash(const ArenaDev& a, const uint64_t* soff, const uint8_t
                           cudaStream_t st) {
     if (hashed * 8 < n) {
         DSSS_LAUNCH("k_dp_hash", st,
-                    k_dp_hash_sparse<<<stride_grid(n), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1,
+                    k_dp_hash_sparse<<<stride_grid((n + 15) / 16), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1,
                                                                      set_begin, nsets, set_base, set_mask, slot, err,
                                                                      ndup));
     } else {
@@ -372,38 +405,205 @@ __global__ void __launch_bounds__(256) k_dp_insert(const uint8_t* kind, uint64_t
     slot[i] = table_insert(tkeys, tdup, base, mask, hbuf[i], err, ndup);
 }
 
-// Dense hash rounds (a large share of the positions hash): the d-byte prefix
-// hash of every string of length >= d, computed in arena order so that the
-// prefixes are read front to back, one string after the next, and stored per
-// string.  The sorted-order insert (k_dp_insert_dig) then gathers one 8-byte
-// hash per hashed position instead of its d-byte prefix.  Strings that do not
-// hash in the round are hashed too (their hashes are never read).
-__global__ void __launch_bounds__(256) k_dp_digest(ArenaDev a, uint32_t depth, unsigned long long* dig) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    uint64_t off;
-    uint32_t L;
-    str_of(a, (uint32_t)i, off, L);
-    if (L < depth) return;
-    dig[i] = filter_hash(xxh64_dev(a.chars + off, depth));
-}
+// Dense hash rounds (at least 1/dp_digest of the positions hash) run in arena
+// order.  The classification marks every hashed string (kinds 2 and 3) in the
+// arena-order bitmap hmask; k_dp_arena_insert walks the strings front to
+// back, so the d-byte prefixes are read in address order (at the first
+// schedule depths it reads the hashes the string sort's first pass stored
+// instead), and inserts the hash of every marked string into the table.  The first insert of a hash
+// owns its slot (tid); an equal later insert marks the slot shared and its
+// own string in the arena-order bitmap dmask.  k_dp_owner_dups then adds the
+// owners of shared slots to dmask, and k_dp_query_mask keeps every kind-2
+// position whose string is in dmask.  The table receives the same hashes as
+// in the sorted-order form, so every string gets the same outcome; no
+// per-string state is gathered by sorted position except the one bit read
+// back by the query.
+__device__ __forceinline__ bool bit_of(const uint32_t* m, uint64_t s) { return (m[s >> 5] >> (s & 31)) & 1u; }
 
-__global__ void __launch_bounds__(256) k_dp_insert_dig(const uint32_t* order, const uint8_t* kind, uint64_t n,
-                                                       const unsigned long long* dig, unsigned long long* tkeys,
-                                                       uint8_t* tdup, uint32_t mask1, const uint64_t* set_begin,
-                                                       uint32_t nsets, const uint64_t* set_base,
-                                                       const uint32_t* set_mask, uint32_t* slot, uint32_t* err,
-                                                       uint32_t* ndup) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || kind[i] < 2) return;
+__global__ void __launch_bounds__(256) k_dp_arena_insert(ArenaDev a, uint32_t depth, const unsigned long long* dig,
+                                                         const uint32_t* hmask,
+                                                         unsigned long long* tkeys, uint8_t* tdup, uint32_t* tid,
+                                                         uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
+                                                         const uint64_t* set_base, const uint32_t* set_mask,
+                                                         uint32_t* dmask, uint32_t* err, uint32_t* ndup,
+                                                         uint32_t check, uint32_t* bad) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n || !bit_of(hmask, s)) return;
+    unsigned long long h;
+    if (dig) {  // stored by the string sort's first pass
+        h = dig[s];
+        if (check) {
+            uint64_t off;
+            uint32_t L;
+            str_of(a, (uint32_t)s, off, L);
+            if (h != filter_hash(xxh64_dev(a.chars + off, depth))) atomicExch(bad, 1u);
+        }
+    } else {
+        uint64_t off;
+        uint32_t L;
+        str_of(a, (uint32_t)s, off, L);
+        h = filter_hash(xxh64_dev(a.chars + off, depth));
+    }
     uint64_t base = 0;
     uint32_t mask = mask1;
-    if (nsets > 1) {
-        const uint32_t sid = set_of(set_begin, nsets, i);
+    if (nsets > 1) {  // a set's strings occupy the same index range in the arena and in the order
+        const uint32_t sid = set_of(set_begin, nsets, s);
         base = set_base[sid];
         mask = set_mask[sid];
     }
-    slot[i] = table_insert(tkeys, tdup, base, mask, dig[order[i]], err, ndup);
+    uint32_t sl = (uint32_t)(h ^ (h >> 32)) & mask;
+    for (uint32_t probe = 0;; ++probe) {
+        if (probe > mask) {
+            atomicExch(err, 1u);
+            return;
+        }
+        const unsigned long long prev = atomicCAS(&tkeys[base + sl], EMPTY_KEY, h);
+        if (prev == EMPTY_KEY) {
+            tid[base + sl] = (uint32_t)s;
+            return;
+        }
+        if (prev == h) {
+            tdup[base + sl] = 1;
+            atomicAdd(ndup, 1u);
+            atomicOr(&dmask[s >> 5], 1u << (s & 31));
+            return;
+        }
+        sl = (sl + 1) & mask;
+    }
+}
+
+// Dense rounds without a hash table in DRAM (whose random atomics bound the
+// round): the hashed strings' (hash, string) pairs are scattered in arena
+// order into 2^B buckets by the hash's top B bits, PD_TARGET pairs per bucket
+// on average, each bucket in a region of PD_CAP pairs; one block per bucket
+// then finds the equal hashes of its bucket in shared memory.  A bucket that
+// overflows its region (PD_CAP is the mean plus 64 standard deviations for
+// uniform hashes; only many equal prefixes on different PEs can fill it)
+// sends the round to the table form.
+constexpr uint32_t PD_TARGET = 4096;
+constexpr uint32_t PD_CAP = 8192;
+constexpr uint32_t PD_TAB = 2 * PD_CAP;  // shared-memory slots per bucket (load <= 1/2)
+constexpr uint32_t PD_NT = 1024;
+constexpr size_t PD_SMEM = (size_t)PD_CAP * 8 + (size_t)PD_TAB * 4 + PD_CAP;
+
+static uint32_t pd_buckets(uint64_t hashed) {
+    uint32_t nb = 1;
+    while ((uint64_t)nb * PD_TARGET < hashed) nb <<= 1;
+    return nb;
+}
+
+__global__ void __launch_bounds__(256) k_dp_part(ArenaDev a, uint32_t depth, const unsigned long long* dig,
+                                                 const uint32_t* hmask, uint32_t bbits, uint32_t* cursor,
+                                                 unsigned long long* ph, uint32_t* ps, uint32_t* overflow,
+                                                 uint32_t check, uint32_t* bad) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n || !bit_of(hmask, s)) return;
+    unsigned long long h;
+    if (dig) {  // stored by the string sort's first pass
+        h = dig[s];
+        if (check) {
+            uint64_t off;
+            uint32_t L;
+            str_of(a, (uint32_t)s, off, L);
+            if (h != filter_hash(xxh64_dev(a.chars + off, depth))) atomicExch(bad, 1u);
+        }
+    } else {
+        uint64_t off;
+        uint32_t L;
+        str_of(a, (uint32_t)s, off, L);
+        h = filter_hash(xxh64_dev(a.chars + off, depth));
+    }
+    const uint32_t b = bbits ? (uint32_t)(h >> (64 - bbits)) : 0u;
+    const uint32_t at = atomicAdd(&cursor[b], 1u);
+    if (at >= PD_CAP) {
+        atomicExch(overflow, 1u);
+        return;
+    }
+    ph[(uint64_t)b * PD_CAP + at] = h;
+    ps[(uint64_t)b * PD_CAP + at] = (uint32_t)s;
+}
+
+// One block per bucket: every pair whose hash occurs again in the bucket
+// (in the same string set) has its string marked in dmask.
+__global__ void __launch_bounds__(PD_NT) k_dp_bucket_dups(const uint32_t* cursor, const unsigned long long* ph,
+                                                          const uint32_t* ps, uint32_t* dmask, uint32_t* ndup,
+                                                          const uint64_t* set_begin, uint32_t nsets) {
+    extern __shared__ __align__(16) unsigned char pd_sm[];
+    unsigned long long* key = (unsigned long long*)pd_sm;
+    uint32_t* tab = (uint32_t*)(key + PD_CAP);
+    uint8_t* dup = (uint8_t*)(tab + PD_TAB);
+    const uint32_t b = blockIdx.x;
+    const uint32_t m = min(cursor[b], PD_CAP);
+    const unsigned long long* bh = ph + (uint64_t)b * PD_CAP;
+    const uint32_t* bs = ps + (uint64_t)b * PD_CAP;
+    for (uint32_t j = threadIdx.x; j < m; j += PD_NT) {
+        key[j] = bh[j];
+        dup[j] = 0;
+    }
+    for (uint32_t j = threadIdx.x; j < PD_TAB; j += PD_NT) tab[j] = 0xFFFFFFFFu;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < m; j += PD_NT) {
+        const unsigned long long h = key[j];
+        uint32_t sl = (uint32_t)(h ^ (h >> 29)) & (PD_TAB - 1);
+        for (uint32_t probe = 0; probe < PD_TAB; ++probe) {
+            const uint32_t prev = atomicCAS(&tab[sl], 0xFFFFFFFFu, j);
+            if (prev == 0xFFFFFFFFu) break;
+            if (key[prev] == h &&
+                (nsets <= 1 || set_of(set_begin, nsets, bs[prev]) == set_of(set_begin, nsets, bs[j]))) {
+                dup[j] = 1;
+                dup[prev] = 1;
+                break;
+            }
+            sl = (sl + 1) & (PD_TAB - 1);
+        }
+    }
+    __syncthreads();
+    uint32_t c = 0;
+    for (uint32_t j = threadIdx.x; j < m; j += PD_NT) {
+        if (dup[j]) {
+            const uint32_t s = bs[j];
+            atomicOr(&dmask[s >> 5], 1u << (s & 31));
+            ++c;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(FULLM, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(ndup, c);
+}
+
+// The owner of every shared slot joins dmask (nothing to do when no insert
+// met its own hash).  slots is a multiple of 4: tdup is read a word at a time.
+__global__ void __launch_bounds__(256) k_dp_owner_dups(const uint32_t* tdup_words, const uint32_t* tid, uint64_t words,
+                                                       uint32_t* dmask, const uint32_t* ndup) {
+    if (*ndup == 0) return;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
+        const uint32_t v = tdup_words[w];
+        if (!v) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            if ((v >> (8 * b)) & 0xFFu) {
+                const uint32_t s = tid[4 * w + b];
+                atomicOr(&dmask[s >> 5], 1u << (s & 31));
+            }
+    }
+}
+
+// Kind-2 positions whose string's hash is shared stay candidates.
+__global__ void __launch_bounds__(256) k_dp_query_mask(const uint8_t* kind, const uint32_t* order,
+                                                       const uint32_t* dmask, uint64_t n, uint8_t* st_next,
+                                                       uint32_t* counters, const uint32_t* ndup) {
+    if (*ndup == 0) return;
+    uint32_t nstays = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (kind[i] == 2) {
+            const bool stays = bit_of(dmask, order[i]);
+            st_next[i] = stays ? 1 : 0;
+            nstays += stays;
+        }
+    }
+    block_add(counters + 1, nstays);
 }
 
 // Kind-2 positions whose hash was inserted twice stay candidates.  Nothing to
@@ -662,7 +862,15 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.split = tune(TUNE_DP_SPLIT) != 0;
     // arena-order hashes for dense rounds (every string of the arena)
     L.digest_share = (uint32_t)tune(TUNE_DP_DIGEST);
-    L.dig = L.digest_share ? c.take<unsigned long long>(N) : nullptr;
+    L.mask_words = (N + 31) / 32;
+    L.hmask = L.digest_share ? c.take<uint32_t>(L.mask_words) : nullptr;
+    L.dmask = L.digest_share ? c.take<uint32_t>(L.mask_words) : nullptr;
+    L.tid = L.digest_share ? c.take<uint32_t>(L.slots) : nullptr;
+    // bucket regions of the dense rounds (at most pd_buckets(N) buckets)
+    L.pd_nb = L.digest_share ? pd_buckets(N) : 0;
+    L.pd_cursor = L.digest_share ? c.take<uint32_t>(L.pd_nb) : nullptr;
+    L.pd_h = L.digest_share ? c.take<unsigned long long>((uint64_t)L.pd_nb * PD_CAP) : nullptr;
+    L.pd_s = L.digest_share ? c.take<uint32_t>((uint64_t)L.pd_nb * PD_CAP) : nullptr;
     const bool filter = N >= L.filter_min;
     L.hbuf = (filter || L.split) ? c.take<unsigned long long>(N) : nullptr;
     if (filter) {
@@ -678,7 +886,7 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
 
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
-              cudaStream_t st, uint32_t nsets, const uint64_t* set_begin_host) {
+              cudaStream_t st, uint32_t nsets, const uint64_t* set_begin_host, const unsigned long long* rdig) {
     uint32_t r = 0;
     if (n == 0) {
         if (rounds) *rounds = 0;
@@ -695,21 +903,27 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
     int cur = 0;
     const uint64_t start = 8;
     uint64_t depth = start;
+    uint64_t cands = n;  // candidates entering the round
     for (uint64_t i = start * 2;; i *= 2) {
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
         DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
         if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
+        // a round that may turn out dense marks its hashed strings for the
+        // arena-order form (every string of the arena must be in the order)
+        const bool mark = L.hmask && a.n <= n && cands * L.digest_share >= n;
+        if (mark) DSSS_CUDA(cudaMemsetAsync(L.hmask, 0, L.mask_words * sizeof(uint32_t), st));
+        uint32_t* hm = mark ? L.hmask : nullptr;
         if (nsets == 1 && aligned16(lcp) && aligned16(dp) && aligned16(L.lens) && aligned16(L.st[cur]) &&
             aligned16(L.st[cur ^ 1]) && aligned16(L.kind)) {
             DSSS_LAUNCH("k_dp_classify", st,
                         k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n,
                                                                                 (uint32_t)depth, dp, L.st[cur ^ 1],
-                                                                                L.kind, L.counters));
+                                                                                L.kind, L.counters, order, hm));
         } else {
             DSSS_LAUNCH("k_dp_classify", st,
                         k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth,
                                                                      dp, L.st[cur ^ 1], L.kind, L.counters,
-                                                                     L.set_begin, nsets, L.set_cnt));
+                                                                     L.set_begin, nsets, L.set_cnt, order, hm));
         }
         if (nsets > 1) {
             DSSS_LAUNCH("k_set_tables", st,
@@ -769,40 +983,81 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         } else if (hashed) {
             const uint64_t slots = nsets > 1 ? ((uint64_t)pin[5] << 32 | pin[4]) : table_slots(hashed);
             if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
-            DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
-            DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-            if (L.dig && a.n <= n && (uint64_t)hashed * L.digest_share >= n) {
-                DSSS_LAUNCH("k_dp_digest", st,
-                            k_dp_digest<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, L.dig));
-                DSSS_LAUNCH("k_dp_insert_dig", st,
-                            k_dp_insert_dig<<<grid, 256, 0, st>>>(order, L.kind, n, L.dig, L.tkeys, L.tdup,
+            const bool arena = mark && (uint64_t)hashed * L.digest_share >= n;
+            const uint32_t check = (uint32_t)tune(TUNE_DP_CHECK);
+            if (arena) {
+                const int dj = root_digest_index(depth);
+                const unsigned long long* dig = rdig && dj >= 0 ? rdig + (uint64_t)dj * a.n : nullptr;
+                // buckets in shared memory first; the table only if a bucket overflows
+                bool done = false;
+                const uint32_t nb = pd_buckets(hashed);
+                if (nb <= L.pd_nb) {
+                    static std::atomic<uint64_t> pd_configured{0};
+                    DSSS_TRY(set_smem_once(pd_configured, k_dp_bucket_dups, (int)PD_SMEM));
+                    uint32_t bbits = 0;
+                    while ((1u << bbits) < nb) ++bbits;
+                    DSSS_CUDA(cudaMemsetAsync(L.dmask, 0, L.mask_words * sizeof(uint32_t), st));
+                    DSSS_CUDA(cudaMemsetAsync(L.pd_cursor, 0, nb * sizeof(uint32_t), st));
+                    DSSS_LAUNCH("k_dp_part", st,
+                                k_dp_part<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, dig, L.hmask, bbits,
+                                                                             L.pd_cursor, L.pd_h, L.pd_s,
+                                                                             L.counters + 10, check, L.counters + 9));
+                    DSSS_LAUNCH("k_dp_bucket_dups", st,
+                                k_dp_bucket_dups<<<nb, PD_NT, PD_SMEM, st>>>(L.pd_cursor, L.pd_h, L.pd_s, L.dmask,
+                                                                            L.counters + 8, L.set_begin, nsets));
+                    DSSS_CUDA(cudaGetLastError());
+                    DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                    DSSS_CUDA(cudaStreamSynchronize(st));
+                    done = pin[10] == 0;
+                    if (!done) DSSS_CUDA(cudaMemsetAsync(L.counters + 8, 0, 4 * sizeof(uint32_t), st));
+                }
+                if (!done) {
+                    DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+                    DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
+                    DSSS_CUDA(cudaMemsetAsync(L.dmask, 0, L.mask_words * sizeof(uint32_t), st));
+                    DSSS_LAUNCH("k_dp_arena_insert", st,
+                                k_dp_arena_insert<<<grid_for(a.n, 256), 256, 0, st>>>(
+                                    a, (uint32_t)depth, dig, L.hmask, L.tkeys, L.tdup, L.tid, (uint32_t)(slots - 1),
+                                    L.set_begin, nsets, L.set_base, L.set_mask, L.dmask, L.counters + 2,
+                                    L.counters + 8, check, L.counters + 9));
+                    DSSS_LAUNCH("k_dp_owner_dups", st,
+                                k_dp_owner_dups<<<stride_grid(slots / 4), 256, 0, st>>>(
+                                    (const uint32_t*)L.tdup, L.tid, slots / 4, L.dmask, L.counters + 8));
+                }
+                DSSS_LAUNCH("k_dp_query", st,
+                            k_dp_query_mask<<<stride_grid(n), 256, 0, st>>>(L.kind, order, L.dmask, n, L.st[cur ^ 1],
+                                                                           L.counters, L.counters + 8));
+            } else {
+                DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
+                DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
+                if (L.split) {
+                    DSSS_LAUNCH("k_dp_hash_store", st,
+                                k_dp_hash_store<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.hbuf));
+                    DSSS_LAUNCH("k_dp_insert", st,
+                                k_dp_insert<<<grid, 256, 0, st>>>(L.kind, n, L.hbuf, L.tkeys, L.tdup,
                                                                  (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
                                                                  L.set_mask, L.slot, L.counters + 2, L.counters + 8));
-            } else if (L.split) {
-                DSSS_LAUNCH("k_dp_hash_store", st,
-                            k_dp_hash_store<<<grid, 256, 0, st>>>(a, L.soff, L.kind, n, (uint32_t)depth, L.hbuf));
-                DSSS_LAUNCH("k_dp_insert", st,
-                            k_dp_insert<<<grid, 256, 0, st>>>(L.kind, n, L.hbuf, L.tkeys, L.tdup, (uint32_t)(slots - 1),
-                                                             L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
-                                                             L.counters + 2, L.counters + 8));
-            } else {
-                DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, (uint32_t)depth, hashed, L.tkeys, L.tdup,
-                                        (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
-                                        L.counters + 2, L.counters + 8, st));
+                } else {
+                    DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, (uint32_t)depth, hashed, L.tkeys, L.tdup,
+                                            (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
+                                            L.counters + 2, L.counters + 8, st));
+                }
+                DSSS_LAUNCH("k_dp_query", st,
+                            k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1],
+                                                                      L.counters, L.counters + 8));
             }
-            DSSS_LAUNCH("k_dp_query", st,
-                        k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[cur ^ 1], L.counters,
-                                                                  L.counters + 8));
             DSSS_CUDA(cudaGetLastError());
-            DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 10 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             DSSS_CUDA(cudaStreamSynchronize(st));
             if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table overflow");
+            if (pin[9]) return fail(DSSS_EDEVICE, "a stored prefix hash differs from the string's (dp_check)");
         }
         const uint32_t m = pin[1];
         if (round_counts && r < max_rounds) round_counts[r] = m;
         ++r;
         cur ^= 1;
         if (m == 0) break;
+        cands = m;
         depth = start + i;
     }
     if (rounds) *rounds = r;
@@ -970,6 +1225,53 @@ __global__ void k_route_scatter(const unsigned long long* hval, const uint32_t* 
     const uint32_t d = dest[j];
     out_hval[d] = hval[j];
     out_hpos[d] = hpos[j];
+}
+
+// Hash records in hash order (ips4o::sort of the round's HashStringIndex
+// records, bloomfilter.hpp:1512): a stable LSD radix sort, eight passes of
+// one byte, each a stable multisplit of the records by that byte.
+__global__ void k_hash_byte(const unsigned long long* h, uint64_t m, uint32_t shift, uint32_t* dig) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < m) dig[j] = (uint32_t)(h[j] >> shift) & 0xFFu;
+}
+
+__global__ void k_hash_place(const unsigned long long* h, const uint32_t* pos, const uint32_t* dest, uint64_t m,
+                             unsigned long long* ho, uint32_t* po) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint32_t d = dest[j];
+    ho[d] = h[j];
+    po[d] = pos[j];
+}
+
+void layout_hash_sort(Carve& c, HashSortLayout& L, uint64_t m) {
+    const uint64_t M = m ? m : 1;
+    L.dig = c.take<uint32_t>(M);
+    L.dest = c.take<uint32_t>(M);
+    L.h = c.take<unsigned long long>(M);
+    L.pos = c.take<uint32_t>(M);
+    L.ms = c.take<unsigned char>(multisplit_scratch_bytes(M, 256));
+}
+
+int hash_sort(const HashSortLayout& L, const unsigned long long* hval, const uint32_t* hpos, uint64_t m,
+              unsigned long long* out_hval, uint32_t* out_hpos, cudaStream_t st) {
+    if (m == 0) return DSSS_OK;
+    // passes alternate between the output and L's buffers; eight passes end
+    // in the output
+    const unsigned long long* src_h = hval;
+    const uint32_t* src_p = hpos;
+    for (int pass = 0; pass < 8; ++pass) {
+        unsigned long long* dh = (pass & 1) ? out_hval : L.h;
+        uint32_t* dp = (pass & 1) ? out_hpos : L.pos;
+        DSSS_LAUNCH("k_hash_byte", st, k_hash_byte<<<grid_for(m, 256), 256, 0, st>>>(src_h, m, 8 * pass, L.dig));
+        DSSS_TRY(multisplit(L.dig, m, 256, L.dest, L.ms, st));
+        DSSS_LAUNCH("k_hash_place", st,
+                    k_hash_place<<<grid_for(m, 256), 256, 0, st>>>(src_h, src_p, L.dest, m, dh, dp));
+        src_h = dh;
+        src_p = dp;
+    }
+    DSSS_CUDA(cudaGetLastError());
+    return DSSS_OK;
 }
 
 void layout_hash_route(Carve& c, HashRouteLayout& L, uint64_t m, uint32_t nowner) {

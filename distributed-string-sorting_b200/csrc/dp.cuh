@@ -31,10 +31,22 @@ struct DpLayout {
     unsigned long long* hbuf;  // also the stored hashes of the split hash round
     uint32_t* cand;
     bool split;  // hash round as k_dp_hash_store + k_dp_insert
-    // dense rounds (hashed * digest_share >= positions): hashes computed per
-    // string in arena order (k_dp_digest), then gathered by sorted position
+    // dense rounds (hashed * digest_share >= positions) in arena order: the
+    // hashed strings (hmask), the strings whose hash is shared (dmask), both
+    // bitmaps over arena indices, and the first inserting string of every
+    // table slot (tid)
     uint32_t digest_share;
-    unsigned long long* dig;
+    uint32_t* hmask;
+    uint32_t* dmask;
+    uint64_t mask_words;
+    uint32_t* tid;
+    // dense rounds without the table: (hash, string) pairs bucketed by the
+    // hash's top bits, pd_nb buckets of PD_CAP pairs at most, deduplicated in
+    // shared memory
+    uint32_t pd_nb;
+    uint32_t* pd_cursor;
+    unsigned long long* pd_h;
+    uint32_t* pd_s;
     uint64_t* set_bbase;
     uint32_t* set_bmask;
     uint32_t* set_ccnt;
@@ -46,9 +58,13 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets = 1);
 // receives the distinguishing-prefix length of the string at position i.
 // set_begin_host (nsets + 1 bounds, NULL for one set): prefixes are only
 // duplicates of prefixes in the same set.
+// rdig (optional): the string sort's prefix hashes at the first schedule
+// depths (ROOT_DIGESTS arrays of a.n entries, array j for depth
+// root_digest_depth(j)), read by the arena-order rounds at those depths.
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
-              cudaStream_t st, uint32_t nsets = 1, const uint64_t* set_begin_host = nullptr);
+              cudaStream_t st, uint32_t nsets = 1, const uint64_t* set_begin_host = nullptr,
+              const unsigned long long* rdig = nullptr);
 
 struct DpRoundLayout {
     DpLayout dp;
@@ -103,6 +119,19 @@ void layout_hash_route(Carve& c, HashRouteLayout& L, uint64_t m, uint32_t nowner
 int hash_route(const HashRouteLayout& L, const unsigned long long* hval, const uint32_t* hpos, uint64_t m,
                uint32_t nowner, unsigned long long* out_hval, uint32_t* out_hpos, uint64_t* counts_host,
                cudaStream_t st);
+
+struct HashSortLayout {
+    uint32_t* dig;
+    uint32_t* dest;
+    unsigned long long* h;
+    uint32_t* pos;
+    void* ms;
+};
+void layout_hash_sort(Carve& c, HashSortLayout& L, uint64_t m);
+
+// (hval, hpos) in ascending hash order, stable (out may not alias in).
+int hash_sort(const HashSortLayout& L, const unsigned long long* hval, const uint32_t* hpos, uint64_t m,
+              unsigned long long* out_hval, uint32_t* out_hpos, cudaStream_t st);
 
 struct HashDupLayout {
     uint64_t slots;

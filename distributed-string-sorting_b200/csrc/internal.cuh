@@ -136,8 +136,10 @@ enum TuneKnob : int {
     TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
     TUNE_DP_SPLIT,           // hash round split into hashing and table inserts (1) or one kernel (0)
     TUNE_COPY_WORD,          // bytes per store when whole strings are copied out (16, or 8)
-    TUNE_DP_DIGEST,          // hash rounds in which at least 1/k of the positions hash read the prefixes in
-                             // arena order (k_dp_digest); 0 turns the arena-order form off
+    TUNE_DP_DIGEST,          // hash rounds in which at least 1/k of the positions hash run in arena order
+                             // (k_dp_arena_insert); 0 turns the arena-order form off
+    TUNE_DP_CHECK,           // 1: the arena-order rounds recompute every stored prefix hash from the string and
+                             // fail on a mismatch (a self-check)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);
@@ -477,6 +479,80 @@ __device__ __forceinline__ uint64_t xxh64_dev(const uint8_t* p, uint32_t m) {
 
 // XXHasher::hash with bloomFilterSize = UINT64_MAX (bloomfilter.hpp:1094-1102, :1135).
 __device__ __forceinline__ uint64_t filter_hash(uint64_t h) { return h == ~0ull ? 0 : h; }
+
+// The first four depths of the distinguishing-prefix schedule (8, 24, 40,
+// 72): the string sort's first pass, which reads every string's first bytes
+// in arena order anyway, stores each string's filter hashes at these depths
+// so that a dense hash round at one of them reads 8 bytes per string instead
+// of the prefix.
+constexpr int ROOT_DIGESTS = 4;
+__host__ __device__ constexpr uint32_t root_digest_depth(int j) { return j == 0 ? 8u : j == 1 ? 24u : j == 2 ? 40u : 72u; }
+__host__ __device__ inline int root_digest_index(uint64_t depth) {
+    return depth == 8 ? 0 : depth == 24 ? 1 : depth == 40 ? 2 : depth == 72 ? 3 : -1;
+}
+
+// filter_hash(XXH64(p, d)) for d = 8, 24, 40, 72 from one set of loads (the
+// words of the first 72 bytes); out[j] for depths beyond len is left as is.
+// The same values as xxh64_dev (one stripe feeds the 40-byte hash, two the
+// 72-byte one; both merge the lanes since their lengths exceed 32).
+__device__ __forceinline__ void root_digests(const uint8_t* p, uint32_t len, unsigned long long* out,
+                                             uint64_t stride) {
+    using namespace xxh;
+    if (len < 8) return;
+    const uintptr_t a = (uintptr_t)p;
+    const uint4* q = (const uint4*)(a & ~(uintptr_t)15);
+    const uint32_t skip = (uint32_t)(a & 15);
+    const uint32_t m = len < 72 ? len : 72;
+    const uint32_t nq = (skip + m + 15) / 16;  // chunks up to byte p + m - 1 (6 at most)
+    uint64_t w[12];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if ((uint32_t)k < nq) v = __ldg(q + k);
+        w[2 * k] = ((uint64_t)v.y << 32) | v.x;
+        w[2 * k + 1] = ((uint64_t)v.w << 32) | v.z;
+    }
+    const bool odd = skip >= 8;
+    const uint32_t sh = (skip & 7) * 8;
+    auto word = [&](int j) -> uint64_t {  // bytes [p + 8j, p + 8j + 8), little-endian
+        const uint64_t lo = odd ? w[j + 1] : w[j];
+        const uint64_t hi = (j + 2 < 12) ? (odd ? w[j + 2] : w[j + 1]) : 0ull;
+        return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+    };
+    auto tail8 = [&](uint64_t h, uint64_t x) -> uint64_t {
+        h ^= round(0, x);
+        return rotl(h, 27) * P1 + P4;
+    };
+    auto aval = [&](uint64_t h) -> uint64_t {
+        h ^= h >> 33;
+        h *= P2;
+        h ^= h >> 29;
+        h *= P3;
+        h ^= h >> 32;
+        return h;
+    };
+    auto merged = [&](uint64_t v1, uint64_t v2, uint64_t v3, uint64_t v4) -> uint64_t {
+        uint64_t h = rotl(v1, 1) + rotl(v2, 7) + rotl(v3, 12) + rotl(v4, 18);
+        h = merge(h, v1);
+        h = merge(h, v2);
+        h = merge(h, v3);
+        return merge(h, v4);
+    };
+    const uint64_t w0 = word(0);
+    out[0] = filter_hash(aval(tail8(P5 + 8, w0)));
+    if (len < 24) return;
+    const uint64_t w1 = word(1), w2 = word(2);
+    out[stride] = filter_hash(aval(tail8(tail8(tail8(P5 + 24, w0), w1), w2)));
+    if (len < 40) return;
+    uint64_t v1 = round(P1 + P2, w0), v2 = round(P2, w1), v3 = round(0, w2), v4 = round(0 - P1, word(3));
+    out[2 * stride] = filter_hash(aval(tail8(merged(v1, v2, v3, v4) + 40, word(4))));
+    if (len < 72) return;
+    v1 = round(v1, word(4));
+    v2 = round(v2, word(5));
+    v3 = round(v3, word(6));
+    v4 = round(v4, word(7));
+    out[3 * stride] = filter_hash(aval(tail8(merged(v1, v2, v3, v4) + 72, word(8))));
+}
 
 // ------------------------------------------------------------ utilities ----
 // Exclusive scan of u32 values; writes the total to *total (device).

@@ -76,6 +76,10 @@ struct SortState {
     uint32_t small_max;
     uint32_t pivot;  // pivot passes enabled
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
+    // first pass only: every string's prefix hashes at the first schedule
+    // depths (root_digests), ROOT_DIGESTS arrays of dig_n entries
+    unsigned long long* dig;
+    uint64_t dig_n;
 };
 
 __device__ __forceinline__ uint32_t find_seg(const uint32_t* first, uint32_t nseg, uint32_t t) {
@@ -281,7 +285,9 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
         for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
             uint64_t off;
             uint32_t len;
-            str_of(S.a, ord[i], off, len);
+            const uint32_t s = ord[i];
+            str_of(S.a, s, off, len);
+            if (S.dig) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n);
             uint64_t x[PF_W];
             key_words<PF_W>(S.a.chars, off, len, d0, want, x);
             uint32_t l = D;
@@ -318,7 +324,9 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
     for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) {
         uint64_t off;
         uint32_t len;
-        str_of(S.a, ord[i], off, len);
+        const uint32_t s = ord[i];
+        str_of(S.a, s, off, len);
+        if (S.dig) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n);
         // no need to compare past this thread's minimum so far
         const uint32_t lim = min(cap, mn);
         uint32_t l = 0;
@@ -547,7 +555,9 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
         segs = S.large[S.counters[12]];
         nseg = S.counters[13];
     }
-    __shared__ uint32_t hist[256];
+    // one 256-bin histogram per warp (shared-memory atomics contend only
+    // inside a warp), summed per digit at the end
+    __shared__ uint32_t hist[LT_NT / 32][256];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -555,27 +565,29 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     if (sg.diff == 0) return;
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
     const unsigned long long* key = S.key[sg.flags & F_PARITY];
-    hist[threadIdx.x] = 0;
+#pragma unroll
+    for (int w = 0; w < LT_NT / 32; ++w) hist[w][threadIdx.x] = 0;
     __syncthreads();
     const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
-    const int lane = threadIdx.x & 31;
-    // the tile's keys loaded before any is ranked (one DRAM wait, not LT_IPT)
+    uint32_t* wh = hist[threadIdx.x >> 5];
+    // the tile's keys loaded before any is counted (one DRAM wait, not LT_IPT)
     uint64_t k[LT_IPT];
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
-        const uint32_t i = tb + (threadIdx.x & ~31u) + j * LT_NT + lane;
+        const uint32_t i = tb + j * LT_NT + threadIdx.x;
         k[j] = i < te ? key[i] : 0;
     }
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
-        const uint32_t i = tb + (threadIdx.x & ~31u) + j * LT_NT + lane;
-        const uint32_t d = i < te ? digit_of(k[j], shift) : 0x100u + lane;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+        const uint32_t i = tb + j * LT_NT + threadIdx.x;
+        if (i < te) atomicAdd(&wh[digit_of(k[j], shift)], 1u);
     }
     __syncthreads();
-    S.tile_hist[(uint64_t)t * 256 + threadIdx.x] = hist[threadIdx.x];
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < LT_NT / 32; ++w) c += hist[w][threadIdx.x];
+    S.tile_hist[(uint64_t)t * 256 + threadIdx.x] = c;
 }
 
 // ------------------------------------------------------------ chunk sums ----
@@ -653,12 +665,18 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
     const uint32_t c0 = S.chunk0[si];
     const uint32_t ntiles = (sg.size + LT_TILE - 1) / LT_TILE;
     const uint32_t nch = (ntiles + CHUNK_TILES - 1) / CHUNK_TILES;
+    // the digit's column of chunk sums, eight loads in flight (a segment of
+    // n strings has n / 64 Ki chunks, walked by one block)
     uint32_t run = 0;
-    for (uint32_t c = 0; c < nch; ++c) {
-        uint64_t idx = (uint64_t)(c0 + c) * 256 + d;
-        uint32_t v = S.chunk_pre[idx];
-        S.chunk_pre[idx] = run;
-        run += v;
+    for (uint32_t c = 0; c < nch; c += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = c + q < nch ? S.chunk_pre[(uint64_t)(c0 + c + q) * 256 + d] : 0u;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (c + q < nch) S.chunk_pre[(uint64_t)(c0 + c + q) * 256 + d] = run;
+            run += v[q];
+        }
     }
     const uint32_t total = run;
     // block exclusive scan over the 256 digits
@@ -1695,7 +1713,8 @@ void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small
 
 int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p, const uint64_t* pb_host,
                  const uint32_t* ids_in, uint32_t* ord_out, uint32_t* lcp_out, uint32_t small_max,
-                 uint32_t* pin, cudaStream_t st) {
+                 uint32_t* pin, cudaStream_t st, unsigned long long* dig, bool* dig_done) {
+    if (dig_done) *dig_done = false;
     if (n == 0) return DSSS_OK;
     SortState S;
     S.a = a;
@@ -1720,6 +1739,13 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;
     S.cap_chunks = L.cap_chunks;
+    S.dig = nullptr;
+    S.dig_n = n;
+    // the first pass reads every string when every initial segment is large
+    // (none goes straight to the small sorts) and the ids are the arena's
+    bool dig_all = dig && !ids_in && n <= a.n;
+    for (uint32_t q = 0; dig_all && q < p; ++q)
+        if (pb_host[q + 1] - pb_host[q] <= (uint64_t)clamp_small_max(small_max)) dig_all = false;
 
     static std::atomic<uint64_t> scatter_configured{0};
     DSSS_TRY(set_smem_once(scatter_configured, k_scatter, (int)SCATTER_SMEM));
@@ -1744,6 +1770,10 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     uint32_t nlarge = pin[0];
     int cur = 0;
     uint32_t guard = 0;
+    if (dig_all) {
+        S.dig = dig;
+        if (dig_done) *dig_done = true;
+    }
     while (nlarge) {
         if (++guard > (1u << 24)) return fail(DSSS_EDEVICE, "string sort made no progress");
         Seg* segs = large[cur];
@@ -1770,6 +1800,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
         if (nlarge > L.cap_large) return fail(DSSS_EDEVICE, "string sort: large-segment list overflow");
         cur ^= 1;
+        S.dig = nullptr;
     }
     for (int b = 0; b < NBINS; ++b)
         if (pin[1 + b] > L.cap_small) return fail(DSSS_EDEVICE, "string sort: small-segment list overflow");

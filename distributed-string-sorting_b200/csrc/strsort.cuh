@@ -31,8 +31,12 @@ void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small
 // [pb[q], pb[q+1]) by the bytes of their strings.  ord_out gets the sorted ids,
 // lcp_out[i] the LCP with position i-1 (0 at segment starts).  pin: pinned
 // host buffer of >= 16 u32 for count read-backs (the call synchronises on st).
+// dig (optional, ROOT_DIGESTS * n entries): the first pass stores every
+// string's prefix hashes at the first schedule depths there (root_digests,
+// array j at dig + j * n); *dig_done tells whether it did (the ids are the
+// arena's and every string went through that pass).
 int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p, const uint64_t* pb_host,
                  const uint32_t* ids_in, uint32_t* ord_out, uint32_t* lcp_out, uint32_t small_max,
-                 uint32_t* pin, cudaStream_t st);
+                 uint32_t* pin, cudaStream_t st, unsigned long long* dig = nullptr, bool* dig_done = nullptr);
 
 }  // namespace dsss

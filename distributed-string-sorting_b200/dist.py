@@ -184,6 +184,27 @@ class GpuBackend:
                                     self._s()))
         return oh[:m], op[:m], [int(c) for c in counts]
 
+    def hash_sort(self, hval, hpos):
+        """The round's hash records in hash order (dsss_hash_sort)."""
+        torch = self.torch
+        m = int(hval.shape[0])
+        oh, op = self._e(m, torch.int64), self._e(m, torch.int32)
+        check(lib().dsss_hash_sort(self.ctx.h, _ptr(hval), _ptr(hpos), m, _ptr(oh), _ptr(op), self._s()))
+        return oh[:m], op[:m]
+
+    def golomb_param_hashes(self, count, p):
+        return int(lib().dsss_golomb_param_hashes(int(count), int(p)))
+
+    def golomb_encode(self, hval, counts, bs):
+        from . import golomb_encode
+        words, rw = golomb_encode(self.ctx, hval, counts, bs, stream=self.stream)
+        return words, [int(x) for x in rw]
+
+    def golomb_decode(self, words):
+        from . import golomb_decode
+        vals, bc = golomb_decode(self.ctx, words, max_blocks=max(1, int(words.shape[0])), stream=self.stream)
+        return vals, [int(x) for x in bc]
+
     def hash_dups(self, hval):
         m = int(hval.shape[0])
         dup = self._e(m, self.torch.uint8)
@@ -487,10 +508,15 @@ def _exchange(comm, be, strings, pb, order, lcp, dp, p, p_all, p_local, q_first,
 
 
 def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None,
-         compress_lcps: bool = False):
+         compress_lcps: bool = False, golomb: bool = False):
     """This rank's part of DistributedPrefixDoublingSort::sort.  strings: the
     backend's arena of this rank's strings; part_begin: p_local + 1 PE bounds.
-    phases (dict, optional) receives milliseconds per phase."""
+    phases (dict, optional) receives milliseconds per phase.  golomb: the
+    hashes of every round cross as Golomb/delta-coded blocks, the
+    sequentialGolombEncoding policy (AllToAllHashesGolomb,
+    bloomfilter.hpp:164-243): each rank's hash records sorted (ips4o::sort,
+    :1512), one block per owning rank with b = getB(2^64 - 1 / ranks, count),
+    read back block after block by the owner."""
     ph = _Phases(phases)
     indexed = sampler == 2
     pb = np.asarray(part_begin, np.int64)
@@ -520,9 +546,19 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
     rounds = 0
     for depth in depths():
         state_out, hpos, hval = be.dp_classify(strings, order, lcp, state, depth, dp)
+        if golomb:
+            hval, hpos = be.hash_sort(hval, hpos)  # the owner groups then hold ascending hashes
         r_hval, r_hpos, counts = be.hash_route(hval, hpos, comm.world)
         recv = comm.alltoall_counts(counts)
-        got = comm.alltoallv(r_hval, counts, recv)
+        if golomb:
+            bs = [be.golomb_param_hashes(c, comm.world) if c else 1 for c in counts]
+            words, rw = be.golomb_encode(r_hval, counts, bs)
+            wrecv = comm.alltoall_counts(rw)
+            got, bc = be.golomb_decode(comm.alltoallv(words, rw, wrecv))
+            if bc != [c for c in recv if c]:
+                raise RuntimeError("Golomb blocks do not match the hash counts sent")
+        else:
+            got = comm.alltoallv(r_hval, counts, recv)
         dup = be.hash_dups(got)
         back = comm.alltoallv(dup, recv, counts)
         cand = be.dp_apply(r_hpos, back, state_out)

@@ -131,11 +131,16 @@ int dsss_abi_version(void);
  *   copy_word       dsss_ms_sort / dsss_hq_sort: bytes per aligned store when
  *                   the output strings are copied out (16, default, or 8)
  *   dp_digest       distinguishing-prefix hash rounds in which at least 1/k
- *                   of the positions hash compute every string's prefix hash
- *                   in arena order (prefixes read front to back) and gather
- *                   one 8-byte hash per sorted position (k = 1..64, default
- *                   4); 0 hashes every round by gathering the prefixes in
- *                   sorted order */
+ *                   of the positions hash run in arena order: the hashed
+ *                   strings are marked in a bitmap, hashed and inserted into
+ *                   the table front to back (prefixes read in address order),
+ *                   and the outcome read back as one bit per sorted position
+ *                   (k = 1..64, default 4); 0 hashes every round by gathering
+ *                   the prefixes in sorted order
+ *   dp_check        1: the arena-order rounds at depths 8, 24, 40 and 72,
+ *                   which read the prefix hashes the string sort's first pass
+ *                   stored, recompute each from the string and fail with
+ *                   DSSS_EDEVICE on a mismatch (a self-check; default 0) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 
@@ -380,6 +385,12 @@ int dsss_dp_classify_hash(dsss_ctx* ctx, const dsss_arena* in, const uint32_t* o
  * counts (HOST, nowner): the group sizes, in owner order. */
 int dsss_hash_route(dsss_ctx* ctx, const uint64_t* hval, const uint32_t* hpos, uint64_t m, uint32_t nowner,
                     uint64_t* out_hval, uint32_t* out_hpos, uint64_t* counts, dsss_stream_t stream);
+/* The round's hash records in hash order, stable: ips4o::sort of the
+ * HashStringIndex records (bloomfilter.hpp:1512), which the Golomb-coded
+ * exchange needs (each destination's hashes ascending).  Since the owner of a
+ * hash is monotone in it, the sorted records are also grouped by owner. */
+int dsss_hash_sort(dsss_ctx* ctx, const uint64_t* hval, const uint32_t* hpos, uint64_t m, uint64_t* out_hval,
+                   uint32_t* out_hpos, dsss_stream_t stream);
 /* Owner side of FindDuplicates::findDuplicates (bloomfilter.hpp:662-765):
  * dup[j] = 1 iff hval[j] occurs at least twice among the m received hashes. */
 int dsss_hash_dups(dsss_ctx* ctx, const uint64_t* hval, uint64_t m, uint8_t* dup, dsss_stream_t stream);
@@ -515,6 +526,37 @@ int dsss_varint_encode(dsss_ctx* ctx, const uint32_t* values, uint64_t n, const 
                        uint32_t nranges, uint8_t* out, uint64_t out_cap, uint64_t* out_bytes, uint64_t* range_bytes,
                        dsss_stream_t stream);
 int dsss_varint_decode(dsss_ctx* ctx, const uint8_t* in, uint64_t nbytes, uint32_t* values, uint64_t n,
+                       dsss_stream_t stream);
+
+/* Golomb/delta coding of sorted 64-bit values, the wire format of the hash
+ * exchange with sequentialGolombEncoding (AllToAllHashesGolomb,
+ * src/sorter/distributed/bloomfilter.hpp:164-313, over getDeltaEncoding /
+ * getDeltaDecoding, src/encoding/golomb_encoding.hpp:50-110, and thrill's
+ * GolombBitStreamWriter / Reader, src/encoding/golomb_bit_stream.hpp).  A
+ * range of c > 0 ascending values becomes the block [S, b, v_0, bit words]
+ * (S = words after S); the bit words hold, most significant bit first, each
+ * gap v_i - v_{i-1} as q = gap / b ones, a zero and gap mod b in truncated
+ * binary; the unused bits of the last word are ones.  An empty range takes
+ * no words.
+ * param: getB(max_value, count) (golomb_encoding.hpp:50-59); param_hashes:
+ * the hash exchange's b for count hashes sent to one of p PEs
+ * (bloomfilter.hpp:194-197: getB over 2^64 - 1 / p, 1 replaced by 2e10).
+ * encode: values (device) in nranges ranges of range_counts[r] values (HOST),
+ * parameters b[r] (HOST, >= 1) into out (device, out_cap words);
+ * *out_words = the total and range_words[r] (HOST) each range's words
+ * (out == NULL: size query only).  Values must ascend inside a range; a gap
+ * of more than 2^31 b is rejected.
+ * decode: nwords words (device) of back-to-back blocks, read block after
+ * block as the receiving PE does (bloomfilter.hpp:230-242); *n_values values
+ * to values (device, cap_values; NULL: size query), block_counts[j] (HOST,
+ * max_blocks) the values of block j, *nblocks the blocks. */
+uint64_t dsss_golomb_param(uint64_t max_value, uint64_t count);
+uint64_t dsss_golomb_param_hashes(uint64_t count, uint32_t p);
+int dsss_golomb_encode(dsss_ctx* ctx, const uint64_t* values, const uint64_t* range_counts, uint32_t nranges,
+                       const uint64_t* b, uint64_t* out, uint64_t out_cap, uint64_t* out_words, uint64_t* range_words,
+                       dsss_stream_t stream);
+int dsss_golomb_decode(dsss_ctx* ctx, const uint64_t* words, uint64_t nwords, uint64_t* values, uint64_t cap_values,
+                       uint64_t* n_values, uint64_t* block_counts, uint32_t max_blocks, uint32_t* nblocks,
                        dsss_stream_t stream);
 
 /* D/N-ratio strings (the role of DNRatioGenerator, util/random_string_generator.hpp:166-318),

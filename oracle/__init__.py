@@ -199,6 +199,12 @@ def ref():
         L.ref_radixsort_ci3.argtypes = [_P, _U64, _U64, _P, _P]
         L.ref_lcp_merge.restype = _I
         L.ref_lcp_merge.argtypes = [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P, _P]
+        L.ref_golomb_param.restype = _U64
+        L.ref_golomb_param.argtypes = [_U64, _U64]
+        L.ref_golomb_block.restype = ctypes.c_int64
+        L.ref_golomb_block.argtypes = [_P, _U64, _U64, _P, _U64]
+        L.ref_golomb_unblock.restype = ctypes.c_int64
+        L.ref_golomb_unblock.argtypes = [_P, _U64, _P, _U64]
         _ref = L
     return _ref
 
@@ -484,3 +490,90 @@ def ref_lcp_merge(chars, lcps, recv_counts, recv_offsets):
                              *(_p(x) for x in o))
     assert rc == 0, rc
     return tuple(x[:n] for x in o)
+
+
+# ------------------------------------------------------------------ Golomb ----
+def _golomb_lib():
+    L = lib()
+    if not hasattr(L, "_golomb_set"):
+        L.oracle_golomb_param.restype = _U64
+        L.oracle_golomb_param.argtypes = [_U64, _U64]
+        L.oracle_golomb_param_hashes.restype = _U64
+        L.oracle_golomb_param_hashes.argtypes = [_U64, _U32]
+        L.oracle_golomb_encode.restype = ctypes.c_int64
+        L.oracle_golomb_encode.argtypes = [_P, _P, _U32, _P, _P, _U64, _P]
+        L.oracle_golomb_decode.restype = ctypes.c_int64
+        L.oracle_golomb_decode.argtypes = [_P, _U64, _P, _U64, _P, _U32, ctypes.POINTER(_U32)]
+        L._golomb_set = True
+    return L
+
+
+def golomb_param(max_value: int, count: int) -> int:
+    """getB (golomb_encoding.hpp:50-59)."""
+    return int(_golomb_lib().oracle_golomb_param(max_value, count))
+
+
+def golomb_param_hashes(count: int, p: int) -> int:
+    """b of the hash exchange to one of p PEs that receives count hashes."""
+    return int(_golomb_lib().oracle_golomb_param_hashes(count, p))
+
+
+def golomb_encode(values, counts, bs):
+    """Golomb/delta blocks of sorted ranges (the hash exchange's format):
+    returns (words u64, words per range)."""
+    v = np.ascontiguousarray(values, dtype=np.uint64)
+    c = np.ascontiguousarray(counts, dtype=np.uint64)
+    b = np.ascontiguousarray(bs, dtype=np.uint64)
+    cap = int(3 * len(c) + 2 * len(v) + 8 + sum(int(x) for x in golomb_unary_words(v, c, b)))
+    out = np.zeros(cap, np.uint64)
+    rw = np.zeros(len(c), np.uint64)
+    n = _golomb_lib().oracle_golomb_encode(v.ctypes.data, c.ctypes.data, len(c), b.ctypes.data, out.ctypes.data,
+                                           cap, rw.ctypes.data)
+    if n < 0:
+        raise RuntimeError("golomb_encode: output larger than planned")
+    return out[:n], rw
+
+
+def golomb_unary_words(v, c, b):
+    """Upper bound of the words the unary parts of each range take."""
+    off = 0
+    for cnt, bb in zip(c.tolist(), b.tolist()):
+        seg = v[off:off + cnt]
+        off += cnt
+        yield 0 if cnt < 2 else int(((seg[-1] - seg[0]) // np.uint64(bb))) // 64 + 2
+
+
+def golomb_decode(words, max_blocks=1 << 20, cap=None):
+    """Values and per-block counts of back-to-back blocks."""
+    w = np.ascontiguousarray(words, dtype=np.uint64)
+    cap = cap if cap is not None else int(64 * len(w) + 8)
+    out = np.zeros(max(cap, 1), np.uint64)
+    bc = np.zeros(max_blocks, np.uint64)
+    nb = _U32(0)
+    n = _golomb_lib().oracle_golomb_decode(w.ctypes.data, len(w), out.ctypes.data, cap, bc.ctypes.data, max_blocks,
+                                           ctypes.byref(nb))
+    if n < 0:
+        raise ValueError("golomb_decode: malformed block")
+    return out[:n], bc[:nb.value]
+
+
+def ref_golomb_block(values, b):
+    """The reference's own coder (compiled from src/encoding/golomb_encoding.hpp)
+    on one block, framed as AllToAllHashesGolomb frames it."""
+    v = np.ascontiguousarray(values, dtype=np.uint64)
+    cap = int(3 + 2 * len(v) + 8 + (int((v[-1] - v[0]) // np.uint64(b)) // 64 + 2 if len(v) > 1 else 0))
+    out = np.zeros(cap, np.uint64)
+    n = ref().ref_golomb_block(v.ctypes.data, len(v), b, out.ctypes.data, cap)
+    if n < 0:
+        raise RuntimeError("ref_golomb_block: output larger than planned")
+    return out[:n]
+
+
+def ref_golomb_unblock(words, cap):
+    w = np.ascontiguousarray(words, dtype=np.uint64)
+    out = np.zeros(max(cap, 1), np.uint64)
+    n = ref().ref_golomb_unblock(w.ctypes.data, len(w), out.ctypes.data, cap)
+    if n < 0:
+        raise RuntimeError("ref_golomb_unblock failed")
+    return out[:n]
+

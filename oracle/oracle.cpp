@@ -22,6 +22,7 @@
 // string's length read as 0, which is exactly the NUL terminator the
 // reference's StringSets rely on.  Strings must not contain byte 0.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
@@ -781,6 +782,165 @@ int oracle_hq_sort(const uint8_t* chars, const uint64_t* off, const uint32_t* le
         for (uint64_t id : pe[q]) source[o++] = id;
     }
     return 0;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------- Golomb ----
+// The Golomb/delta coding of sorted 64-bit values that the reference's
+// sequentialGolombEncoding policy applies to the hash exchange
+// (AllToAllHashesGolomb, src/sorter/distributed/bloomfilter.hpp:164-313):
+// per destination with c > 0 values the block is
+//   [S, b, v_0, bit words...]   S = number of words after S,
+// the bit words holding, for i = 1..c-1, the Golomb code of v_i - v_{i-1}
+// most significant bit first (getDeltaEncoding, encoding/golomb_encoding.hpp:
+// 61-80; DeltaStreamWriter, delta_stream.hpp:24-48; GolombBitStreamWriter::
+// PutGolomb, golomb_bit_stream.hpp:59-115; BitStreamWriter::PutBits,
+// bit_stream.hpp:52-83): q = delta / b ones, a zero, then r = delta mod b in
+// truncated binary (k = ceil(log2 b) bits when r >= 2^k - b, stored as
+// r + 2^k - b, else k - 1 bits); the last word's unused bits are ones (the
+// writer's destructor, golomb_bit_stream.hpp:48-56).  A destination with no
+// values gets no words.
+static uint64_t golomb_param(uint64_t max_value, uint64_t count) {  // getB, golomb_encoding.hpp:50-59
+    if (count == 0) return 1;
+    const uint64_t avg = max_value / count;
+    if (avg < 1) return 1;
+    const uint64_t k = static_cast<uint64_t>(std::floor(std::log2(static_cast<double>(avg))));
+    return 1ull << k;
+}
+
+static unsigned ceil_log2(uint64_t b) {  // tlx::integer_log2_ceil
+    unsigned k = 0;
+    while (k < 64 && (1ull << k) < b) ++k;
+    return k;
+}
+
+namespace {
+struct BitSink {  // most significant bit first into 64-bit words
+    std::vector<uint64_t>& out;
+    uint64_t cur = 0;
+    unsigned used = 0;
+    explicit BitSink(std::vector<uint64_t>& o) : out(o) {}
+    void bit(unsigned v) {
+        cur |= (uint64_t)(v & 1u) << (63 - used);
+        if (++used == 64) {
+            out.push_back(cur);
+            cur = 0;
+            used = 0;
+        }
+    }
+    void bits(uint64_t v, unsigned k) {
+        for (unsigned j = k; j-- > 0;) bit((unsigned)(v >> j) & 1u);
+    }
+    void ones(uint64_t q) {
+        while (q && used) { bit(1); --q; }
+        while (q >= 64) { out.push_back(~0ull); q -= 64; }
+        while (q) { bit(1); --q; }
+    }
+    void finish() {  // the rest of a started word: ones
+        if (used) {
+            cur |= used ? (~0ull >> used) : 0;
+            out.push_back(cur);
+            cur = 0;
+            used = 0;
+        }
+    }
+};
+}  // namespace
+
+static void golomb_block(const uint64_t* v, uint64_t c, uint64_t b, std::vector<uint64_t>& out) {
+    const size_t at = out.size();
+    out.push_back(0);  // S, filled below
+    out.push_back(b);
+    out.push_back(v[0]);  // the first value is not coded
+    const unsigned k = ceil_log2(b);
+    const uint64_t little = (k >= 64 ? 0ull : (1ull << k)) - b;
+    BitSink w(out);
+    for (uint64_t i = 1; i < c; ++i) {
+        const uint64_t d = v[i] - v[i - 1];
+        const uint64_t q = d / b, r = d - q * b;
+        w.ones(q);
+        w.bit(0);
+        if (r >= little) w.bits(r + little, k);
+        else w.bits(r, k - 1);
+    }
+    w.finish();
+    out[at] = out.size() - at - 1;
+}
+
+extern "C" {
+
+uint64_t oracle_golomb_param(uint64_t max_value, uint64_t count) { return golomb_param(max_value, count); }
+
+// b of the hash exchange to one of p PEs holding count hashes
+// (bloomfilter.hpp:194-197: getB over the PE's slice of the 64-bit filter,
+// bloomFilterSize = 2^64 - 1 at :1135, and 1 replaced by 20000000000).
+uint64_t oracle_golomb_param_hashes(uint64_t count, uint32_t p) {
+    const uint64_t b = golomb_param(~0ull / p, count);
+    return b == 1 ? 20000000000ull : b;
+}
+
+// Blocks of nranges ranges (counts[r] sorted values each, back to back in
+// values) with parameters b[r]; range_words[r] = the block's words (0 for an
+// empty range).  Returns the total, -1 when it exceeds cap.
+int64_t oracle_golomb_encode(const uint64_t* values, const uint64_t* counts, uint32_t nranges, const uint64_t* b,
+                             uint64_t* out, uint64_t cap, uint64_t* range_words) {
+    std::vector<uint64_t> w;
+    uint64_t off = 0;
+    for (uint32_t r = 0; r < nranges; ++r) {
+        const size_t before = w.size();
+        if (counts[r]) golomb_block(values + off, counts[r], b[r], w);
+        range_words[r] = w.size() - before;
+        off += counts[r];
+    }
+    if (w.size() > cap) return -1;
+    std::copy(w.begin(), w.end(), out);
+    return (int64_t)w.size();
+}
+
+// Decodes back-to-back blocks (nwords words) as the receiving side does
+// (bloomfilter.hpp:230-242: per block S, b, then getDeltaDecoding until the
+// bit reader finds no further zero); block_counts[k] = values of block k
+// (at most max_blocks blocks).  Returns the values written, -1 on a
+// malformed block or more than cap values.
+int64_t oracle_golomb_decode(const uint64_t* words, uint64_t nwords, uint64_t* out, uint64_t cap,
+                             uint64_t* block_counts, uint32_t max_blocks, uint32_t* nblocks) {
+    uint64_t pos = 0, n = 0;
+    uint32_t blk = 0;
+    while (pos < nwords) {
+        if (blk >= max_blocks) return -1;
+        const uint64_t S = words[pos];
+        if (S < 2 || S > nwords - pos - 1) return -1;
+        const uint64_t end = pos + 1 + S, b = words[pos + 1];
+        if (b == 0) return -1;
+        const unsigned k = ceil_log2(b);
+        const uint64_t little = (k >= 64 ? 0ull : (1ull << k)) - b;
+        const uint64_t base = n;
+        if (n >= cap) return -1;
+        uint64_t v = words[pos + 2];
+        out[n++] = v;
+        const uint64_t bit0 = (pos + 3) * 64, bit1 = end * 64;
+        auto get = [&](uint64_t t) -> unsigned { return (unsigned)(words[t >> 6] >> (63 - (t & 63))) & 1u; };
+        uint64_t t = bit0;
+        for (;;) {
+            uint64_t q = 0;
+            while (t < bit1 && get(t)) { ++q; ++t; }
+            if (t >= bit1) break;  // only ones left: the padding
+            ++t;  // the zero
+            uint64_t r = 0;
+            const unsigned lo = k ? k - 1 : 0;
+            for (unsigned j = 0; j < lo; ++j) r = (r << 1) | (t < bit1 ? get(t++) : (t++, 0u));
+            if (k && r >= little) r = ((r << 1) | (t < bit1 ? get(t++) : (t++, 0u))) - little;
+            if (t > bit1) return -1;
+            if (n >= cap) return -1;
+            v += q * b + r;
+            out[n++] = v;
+        }
+        block_counts[blk++] = n - base;
+        pos = end;
+    }
+    *nblocks = blk;
+    return (int64_t)n;
 }
 
 }  // extern "C"

@@ -10,6 +10,10 @@
 //   src/merge/bingmann-lcp_losertree.hpp:203-480  LcpStringLoserTree_ (compressed-prefix merge)
 //   src/sorter/distributed/merging.hpp:23-63  range padding of merge<K> (restated: the
 //   header itself pulls in MPI)
+//   src/encoding/golomb_encoding.hpp:50-110   getB, getDeltaEncoding / getDeltaDecoding over
+//   thrill's Golomb bit streams (golomb_bit_stream.hpp, bit_stream.hpp, delta_stream.hpp);
+//   the [S, b] block framing of AllToAllHashesGolomb (bloomfilter.hpp:199-209) is restated
+//   here, since that struct's header pulls in MPI
 #include <cstdint>
 #include <cstring>
 #include <algorithm>
@@ -20,6 +24,7 @@
 #include "strings/stringcontainer.hpp"
 #include "strings/stringset.hpp"
 #include "merge/bingmann-lcp_losertree.hpp"
+#include "encoding/golomb_encoding.hpp"
 #include <tlx/sort/strings/radix_sort.hpp>
 
 extern "C" {
@@ -127,6 +132,36 @@ int ref_lcp_merge(const uint8_t* raw, uint64_t raw_bytes, const uint64_t* lcps, 
     default: return -95;
     }
     return 0;
+}
+
+// getB (golomb_encoding.hpp:50-59).
+uint64_t ref_golomb_param(uint64_t max_value, uint64_t count) { return getB(max_value, count); }
+
+// One block as AllToAllHashesGolomb frames it: [S, b, getDeltaEncoding of
+// the c values with parameter b].  Returns its words, -1 past cap.
+int64_t ref_golomb_block(const uint64_t* values, uint64_t c, uint64_t b, uint64_t* out, uint64_t cap) {
+    std::vector<size_t> enc;
+    enc.push_back(0);
+    enc.push_back(b);
+    std::vector<size_t> v(values, values + c);
+    getDeltaEncoding(v.begin(), v.end(), std::back_inserter(enc), b);
+    enc[0] = enc.size() - 1;
+    if (enc.size() > cap) return -1;
+    std::copy(enc.begin(), enc.end(), out);
+    return (int64_t)enc.size();
+}
+
+// One block's values: getDeltaDecoding over the words after S and b.
+int64_t ref_golomb_unblock(const uint64_t* words, uint64_t nwords, uint64_t* out, uint64_t cap) {
+    if (nwords < 3) return -1;
+    std::vector<size_t> w(words, words + nwords);
+    const size_t S = w[0], b = w[1];
+    if (S + 1 != nwords) return -1;
+    std::vector<size_t> dec;
+    getDeltaDecoding(w.begin() + 2, w.end(), std::back_inserter(dec), b);
+    if (dec.size() > cap) return -1;
+    std::copy(dec.begin(), dec.end(), out);
+    return (int64_t)dec.size();
 }
 
 } // extern "C"

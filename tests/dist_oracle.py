@@ -71,6 +71,21 @@ class OracleBackend:
         counts = np.bincount(owner, minlength=nowner) if owner.size else np.zeros(nowner, np.int64)
         return hval[perm], hpos[perm], [int(c) for c in counts]
 
+    def hash_sort(self, hval, hpos):
+        perm = np.argsort(np.asarray(hval, np.uint64), kind="stable")
+        return np.asarray(hval, np.uint64)[perm], np.asarray(hpos)[perm]
+
+    def golomb_param_hashes(self, count, p):
+        return self.orc.golomb_param_hashes(int(count), int(p))
+
+    def golomb_encode(self, hval, counts, bs):
+        words, rw = self.orc.golomb_encode(np.asarray(hval, np.uint64), counts, bs)
+        return words, [int(x) for x in rw]
+
+    def golomb_decode(self, words):
+        vals, bc = self.orc.golomb_decode(np.asarray(words, np.uint64))
+        return vals, [int(x) for x in bc]
+
     def hash_dups(self, got):
         got = np.asarray(got)
         if got.size == 0:

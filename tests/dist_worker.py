@@ -23,6 +23,7 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
     strs, pb, splits, sampler = inputs[:4]
     compress = bool(inputs[4]) if len(inputs) > 4 else False
     mode = inputs[5] if len(inputs) > 5 else "pd"
+    golomb = bool(inputs[6]) if len(inputs) > 6 else False
     if pg == "nccl":
         import torch
         torch.cuda.set_device(0)
@@ -45,7 +46,7 @@ def rank_main(rank, world, port, outdir, inputs, backend, pg="gloo"):
         if mode == "ms":
             res = D.merge_sort(D.Comm(), be, arena, pb_local, compress_lcps=compress)
         else:
-            res = D.sort(D.Comm(), be, arena, pb_local, sampler, compress_lcps=compress)
+            res = D.sort(D.Comm(), be, arena, pb_local, sampler, compress_lcps=compress, golomb=golomb)
         out = {"q0": q0, "q1": q1, "s0": s0}
         if mode == "ms":
             nrecv = int(res.get("recv_total", 0))

@@ -18,6 +18,11 @@ Fixtures (JSON, small):
                         DP lengths and send counts, and the expected receive
                         bytes and LCPs of getExpectedRawStringsForPrefixDoubling
                         (:62-72), ..._Duplicates... (:74-84), getExpectedLcpValues (:86-93).
+  golomb_ref.json       the reference's Golomb/delta coder (getDeltaEncoding of
+                        src/encoding/golomb_encoding.hpp over thrill's bit
+                        streams, via oracle/_ref/libref.so) on seeded sorted
+                        blocks, framed [S, b, ...] as AllToAllHashesGolomb
+                        frames them, and getB on a few (max, count) pairs.
 """
 import json
 import os
@@ -133,6 +138,40 @@ def make_kat():
     return cases
 
 
+def golomb_blocks():
+    rng = np.random.default_rng(2024)
+    cases = []
+    for k in range(24):
+        c = int(rng.integers(1, 120))
+        kind = k % 4
+        if kind == 0:  # hashes: the 64-bit range
+            v = np.sort(rng.integers(0, 2**64 - 1, c, dtype=np.uint64))
+            b = int(oracle.golomb_param_hashes(c, 4))
+        elif kind == 1:  # duplicate positions plus an offset: b >= 8
+            v = np.sort(rng.choice(5000, c, replace=False)).astype(np.uint64) + np.uint64(123456)
+            b = max(8, oracle.golomb_param(5000, c))
+        elif kind == 2:  # small gaps, b not a power of two
+            v = np.cumsum(rng.integers(0, 40, c)).astype(np.uint64)
+            b = [3, 5, 7, 1000, 20000000000][k % 5]
+        else:  # a gap that needs more than 64 unary bits
+            v = np.cumsum(rng.integers(0, 3, c)).astype(np.uint64)
+            v[c // 2:] += np.uint64(100000)
+            b = 8
+        cases.append((v, b))
+    return cases
+
+
+def make_golomb():
+    blocks = []
+    for v, b in golomb_blocks():
+        w = oracle.ref_golomb_block(v, b)
+        blocks.append({"values": [str(x) for x in v.tolist()], "b": int(b), "words": [str(x) for x in w.tolist()]})
+    params = [[str(m), str(c), str(int(oracle.ref().ref_golomb_param(m, c)))]
+              for m, c in [(2**64 - 1, 1), (2**64 - 1, 3), ((2**64 - 1) // 4, 1000), (100, 7), (7, 100),
+                           (2**63, 2**62 + 1), (10**12, 999), (0, 5), (5, 0)]]
+    return {"blocks": blocks, "params": params}
+
+
 def main():
     if not oracle.ref_available() or not oracle.ref_dp_available():
         sys.exit("oracle/_ref is not built: run `make -C oracle` where the reference tree is present")
@@ -144,6 +183,8 @@ def main():
         json.dump(make_merge(), f)
     with open(os.path.join(HERE, "pd_exchange_kat.json"), "w") as f:
         json.dump(make_kat(), f)
+    with open(os.path.join(HERE, "golomb_ref.json"), "w") as f:
+        json.dump(make_golomb(), f)
 
 
 if __name__ == "__main__":

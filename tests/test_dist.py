@@ -82,6 +82,18 @@ def test_two_ranks_compressed_lcps(orc, name, strs):
     check_against_oracle(orc, strs, pb, res, 0)
 
 
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("name,strs", CASES[:2] + CASES[3:], ids=["random", "dups", "runs"])
+def test_golomb_coded_hashes(orc, name, strs, world):
+    """sequentialGolombEncoding: every round's hashes cross sorted and
+    Golomb/delta-coded, one block per owning rank; results unchanged."""
+    n = len(strs)
+    pb = [0, n // 5, n // 3, n // 2, (3 * n) // 4, n]
+    splits = [0, 2, 5] if world == 2 else [0, 1, 3, 5]
+    res = run_ranks(world, (strs, pb, splits, 0, False, "pd", True), "oracle")
+    check_against_oracle(orc, strs, pb, res, 0)
+
+
 def test_three_ranks_one_pe_each(orc):
     strs = CASES[0][1]
     n = len(strs)

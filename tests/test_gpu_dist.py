@@ -71,3 +71,15 @@ def test_nccl_single_rank_merge_sort(orc):
     pb = [0, n // 5, (2 * n) // 5, (3 * n) // 5, (4 * n) // 5, n]
     res = run_ranks(1, (strs, pb, [0, 5], 0, True, "ms"), "gpu", pg="nccl")
     check_ms_against_oracle(orc, strs, pb, res)
+
+
+def test_gpu_ranks_golomb_coded_hashes(orc):
+    """The Golomb/delta-coded hash exchange with the CUDA backend: records
+    sorted by dsss_hash_sort, blocks by dsss_golomb_encode, read back by
+    dsss_golomb_decode on the owning rank; results equal the oracle's."""
+    strs = CASES[1][1]
+    n = len(strs)
+    pb = [0, n // 6, n // 3, n // 2, (3 * n) // 4, n]
+    res = run_ranks(2, (strs, pb, [0, 3, 5], 0, False, "pd", True), "gpu")
+    check_against_oracle(orc, strs, pb, res, 0)
+

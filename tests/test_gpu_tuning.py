@@ -193,3 +193,59 @@ def test_dp_digest_batched(dsss, ctx):
             b, e = int(sb[s]), int(sb[s + 1])
             assert np.array_equal(u64(out["dp"], hs.n)[b:e], u64(ref["dp"], h.n)), s
             assert np.array_equal(u64(out["perm_index"], hs.n)[b:e], u64(ref["perm_index"], h.n)), s
+
+
+@pytest.mark.parametrize("share", [0, 1, 64])
+@pytest.mark.parametrize("p", [3, 16])
+def test_dp_digest_per_pe_orders(dsss, orc, ctx, share, p):
+    """The distinguishing-prefix stage on per-PE local orders, where equal
+    prefixes on different PEs are separate roots whose hashes meet in the
+    table: the arena-order form (share 1 / 64) finds the same duplicates
+    (shared slots, their owners, the kind-2 strings kept) as the sorted-order
+    form (share 0) and the oracle."""
+    import torch
+    from inputs import long_prefix, random_strings, with_duplicates
+    strs = with_duplicates(long_prefix(3000, 90, 12, 71) + random_strings(3000, 0, 40, b"AB", 72), 0.3, 73)
+    hs = host_of(dsss, strs)
+    s = orc.Strings.from_host(hs)
+    pb = dsss.equal_parts(hs.n, p)
+    ro, rl = orc.local_sort(s, pb)
+    rdp, rcounts = orc.dp_rounds(s, pb, ro, rl)
+    ds = dsss.DeviceStrings(hs)
+    order = torch.from_numpy(ro.astype(np.int32)).cuda()
+    lcp = torch.from_numpy(rl.astype(np.int32)).cuda()
+    with dsss.tuned(dp_digest=share):
+        dp, counts = dsss.dp_prefixes(ctx, ds, order, lcp, p)
+    assert np.array_equal(u64(dp, hs.n), rdp)
+    assert counts.tolist() == rcounts.tolist()
+
+
+def _depth_families():
+    """Inputs whose dense hash round falls at each of the depths the string
+    sort's first pass hashes (8, 24, 40, 72), with lengths around each."""
+    rng = np.random.default_rng(77)
+    fams = []
+    for common in (0, 12, 30, 60):
+        strs = []
+        for k in range(4000):
+            L = int(rng.choice([common + 3, common + 8, common + 20, 7, 8, 9, 23, 24, 25, 39, 40, 41, 71, 72, 73,
+                                100, 200]))
+            body = bytes(rng.integers(65, 91, L).astype(np.uint8))
+            strs.append((b"Q" * common + body)[:max(L, 1)])
+        fams.append(strs)
+    return fams
+
+
+@pytest.mark.parametrize("fam", range(4), ids=["dense8", "dense24", "dense40", "dense72"])
+def test_root_digests_checked(dsss, orc, ctx, fam):
+    """The prefix hashes stored by the string sort's first pass equal XXH64 of
+    the prefix at every depth where a dense round reads them (dp_check
+    recomputes each one and fails the call on a mismatch), and the result is
+    the oracle's."""
+    hs = host_of(dsss, _depth_families()[fam])
+    with dsss.tuned(dp_check=1, dp_digest=64):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 3)
+    check_pd(dsss, orc, hs, out, 3)
+    with dsss.tuned(dp_check=1, dp_digest=64):
+        out = dsss.pd_sort(ctx, dsss.gen_dn_device(ctx, 60000, 200, 50, seed=5), 4)
+    assert (out["dp"][:60000] == 72).all()

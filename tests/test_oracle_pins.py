@@ -197,3 +197,65 @@ def test_varint_reference_known_answer(orc):
     # LEB128 bytes of single values (7 bits per byte, low first, high bit = more)
     assert orc.varint_encode([300], [1])[0].tobytes() == b"\xac\x02"
     assert orc.varint_encode([2**32 - 1], [1])[0].tobytes() == b"\xff\xff\xff\xff\x0f"
+
+
+def _golomb_fixture():
+    with open(os.path.join(GOLDEN, "golomb_ref.json")) as f:
+        return json.load(f)
+
+
+def test_golomb_golden(orc):
+    """The oracle's Golomb/delta coder writes, block for block, the words the
+    reference's coder wrote (getDeltaEncoding over thrill's bit streams,
+    framed as AllToAllHashesGolomb frames a destination's hashes), and reads
+    them back; getB agrees on every pair."""
+    g = _golomb_fixture()
+    for blk in g["blocks"]:
+        v = np.array([int(x) for x in blk["values"]], np.uint64)
+        want = np.array([int(x) for x in blk["words"]], np.uint64)
+        got, rw = orc.golomb_encode(v, [len(v)], [blk["b"]])
+        assert np.array_equal(got, want)
+        assert int(rw[0]) == len(want)
+        dec, counts = orc.golomb_decode(want)
+        assert np.array_equal(dec, v) and counts.tolist() == [len(v)]
+    for m, c, b in g["params"]:
+        assert orc.golomb_param(int(m), int(c)) == int(b)
+
+
+def test_golomb_blocks_back_to_back(orc):
+    """Several destinations in one buffer, empty ones taking no words, as the
+    exchange sends them; the receiver reads block after block."""
+    rng = np.random.default_rng(3)
+    counts = [5, 0, 1, 40, 0, 0, 17]
+    vals = np.concatenate([np.sort(rng.integers(0, 2**64 - 1, c, dtype=np.uint64)) for c in counts])
+    bs = [orc.golomb_param_hashes(c, len(counts)) for c in counts]
+    words, rw = orc.golomb_encode(vals, counts, bs)
+    assert [int(x) == 0 for x in rw] == [c == 0 for c in counts]
+    dec, bc = orc.golomb_decode(words)
+    assert np.array_equal(dec, vals)
+    assert bc.tolist() == [c for c in counts if c]
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="oracle/_ref not built")
+def test_golomb_vs_reference_coder(orc):
+    """Random sorted blocks (64-bit hashes, offsets, small gaps, b a power of
+    two or not): the oracle's words equal the reference coder's and both read
+    back to the values."""
+    rng = np.random.default_rng(11)
+    for trial in range(120):
+        c = int(rng.integers(1, 200))
+        mode = trial % 3
+        if mode == 0:
+            v = np.sort(rng.integers(0, 2**64 - 1, c, dtype=np.uint64))
+            choices = [orc.golomb_param_hashes(c, 8), 1 << 54]
+        elif mode == 1:
+            v = np.sort(rng.integers(0, 10**6, c, dtype=np.uint64))
+            choices = [8, 16, 3, 5, 1000, 20000000000, max(8, orc.golomb_param(10**6, c))]
+        else:
+            v = np.cumsum(rng.integers(0, 9, c)).astype(np.uint64)
+            choices = [3, 7, 8, 64]
+        for b in choices:
+            want = orc.ref_golomb_block(v, b)
+            got, _ = orc.golomb_encode(v, [c], [b])
+            assert np.array_equal(got, want), (trial, b)
+            assert np.array_equal(orc.ref_golomb_unblock(want, c + 4), v)
