@@ -164,7 +164,9 @@ static void layout_pd(Carve& c, PdLayout& L, uint64_t n, uint32_t nsets, uint32_
     layout_sort(c, L.sort, N, nsets, small_max);
     layout_dp(c, L.dp, N, nsets);
     layout_partition(c, L.part, N, p, factor, nsets);
-    L.rdig = L.dp.hmask ? c.take<unsigned long long>(ROOT_DIGESTS * N) : nullptr;
+    // decided by a value both carving passes see (the sizing pass hands out
+    // null pointers)
+    L.rdig = L.dp.digest_share ? c.take<unsigned long long>(ROOT_DIGESTS * N) : nullptr;
 }
 
 // The fused path over nsets independent string sets of p PEs each (PE q of

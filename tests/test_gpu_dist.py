@@ -81,5 +81,5 @@ def test_gpu_ranks_golomb_coded_hashes(orc):
     n = len(strs)
     pb = [0, n // 6, n // 3, n // 2, (3 * n) // 4, n]
     res = run_ranks(2, (strs, pb, [0, 3, 5], 0, False, "pd", True), "gpu")
-    check_against_oracle(orc, strs, pb, res, 0)
+    check_against_oracle(orc, strs, pb, res, 0, exact_ties=False)
 
