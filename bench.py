@@ -62,9 +62,10 @@ CONFIGS = {
 # from one ncu capture each on 8e6 strings x 200 B (D/N 0.25, p = 64); the
 # traffic of a launch grows with its units.  None: not captured.
 DRAM_PER_UNIT = {
-    "k_dp_arena_insert": None,
-    "k_dp_hash": None,
-    "k_seg_sort1024": None,
+    "k_prefix": None,
+    "k_dp_part": None,
+    "k_dp_bucket_dups": None,
+    "k_dp_lens": None,
 }
 
 
@@ -136,12 +137,21 @@ def cpu_baseline_port(n_sample, L, k, p, seed, gk=None):
     return hs.n / (time.perf_counter() - t)
 
 
-def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
+def uneven_sizes(nsets, lo, hi, seed):
+    """Seeded log-uniform sizes in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in np.exp(rng.uniform(np.log(lo), np.log(hi), size=nsets))]
+
+
+def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20, sizes=None):
     """Suffix instances (all suffixes, truncated to 256 B, of seeded order-3
     Markov ACGT texts with 1% copied 1-4 KiB blocks): nsets texts of `text`
-    bytes sorted as one dsss_pd_sort_batched call vs one dsss_pd_sort call per
-    instance, inputs resident in HBM, device-timed."""
-    sets = [d.gen_suffix_strings(text, 256, seed=100 + k) for k in range(nsets)]
+    bytes (or of the given uneven sizes) sorted as one dsss_pd_sort_batched
+    call vs one dsss_pd_sort call per instance, inputs resident in HBM,
+    device-timed."""
+    texts = sizes if sizes is not None else [text] * nsets
+    nsets = len(texts)
+    sets = [d.gen_suffix_strings(t, 256, seed=100 + k) for k, t in enumerate(texts)]
     hs, sb = d.concat_sets(sets)
     pb = d.batched_parts(sb, p)
     ds_all = d.DeviceStrings(hs)
@@ -177,8 +187,11 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20):
                               outs[k]["dp"][:sets[k].n].cpu().numpy()) for k in range(nsets))
     char_bytes = int(hs.lengths.astype(np.uint64).sum()) + n
     ctx.close()
+    desc = (f"{nsets} x {text >> 20} MiB-text suffix instances (x 256 B max), p = {p} each" if sizes is None else
+            f"{nsets} suffix instances (x 256 B max) of uneven texts, log-uniform {min(texts)}..{max(texts)} bytes "
+            f"(seed 77), p = {p} each")
     return {
-        "workload": f"{nsets} x {text >> 20} MiB-text suffix instances (x 256 B max), p = {p} each",
+        "workload": desc, "text_bytes": texts,
         "strings": n, "char_bytes": char_bytes, "steps": steps,
         "plain_ms": res["plain"], "batched_ms": res["batched"],
         "plain_strings_per_s": n / (res["plain"] * 1e-3), "batched_strings_per_s": n / (res["batched"] * 1e-3),
@@ -492,14 +505,22 @@ def run_path(args, cfg, which):
 
 
 # Algorithmic bytes of the kernels that carry a roofline, per step of one
-# sort (the units a step's launches process):
-#   DP hash round (k_dp_arena_insert in arena order, k_dp_hash in sorted
-#   order): d + 16 for every string hashed at its final depth d (its d-byte
-#   prefix read once, its 8-byte hash written to the table and read back);
-#   roots hashed in earlier rounds are not counted, so this is a lower bound.
+# sort (n strings, lengths L, DP lengths dp, schedule depths 8, 24, 40, 72, ...):
+#   k_prefix   the string sort's first pass over the arena: each string's
+#              first min(L + 1, 72) bytes read once, its 8-byte key and the
+#              four 8-byte prefix hashes of the dense rounds written, its id
+#              and handle read (16 + 4 B): min(L + 1, 72) + 60 per string
+#   k_dp_part  the dense hash round's partition: for every string hashed at
+#              its final depth, the stored 8-byte hash read and the 12-byte
+#              (hash, string) pair written: 20 per string
+#   k_dp_bucket_dups  the pairs read back: 12 per string
+#   k_dp_lens  per sorted position the 4-byte id read, the 16-byte handle
+#              gathered and 12 bytes written: 32 per string
 ROOFLINE_BYTES = {
-    "k_dp_arena_insert": "sum over strings hashed at their final depth d of (d + 16)",
-    "k_dp_hash": "sum over strings hashed at their final depth d of (d + 16)",
+    "k_prefix": "sum over strings of (min(L + 1, 72) + 60)",
+    "k_dp_part": "20 per string hashed at its final depth",
+    "k_dp_bucket_dups": "12 per string hashed at its final depth",
+    "k_dp_lens": "32 per string",
 }
 SORT_KERNELS = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
                 "k_scatter", "k_seg_sort", "k_warp_segs", "k_spec", "k_pivot", "k_seg_offsets", "scan_")
@@ -511,10 +532,16 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
     stages = {k[6:]: v[1] / steps for k, v in kt.items() if k.startswith("stage:")}
     dp = out["dp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
     lcp = out["merged_lcp"][:n].cpu().numpy().view(np.uint32).astype(np.uint64)
+    L = np.asarray(lengths, np.uint64)
     D = int(dp.sum())
     sched = np.array([8] + [8 + (16 << j) for j in range(26)], np.uint64)
-    hashed_final = np.isin(dp, sched)
-    hash_bytes = int(dp[hashed_final].sum()) + 16 * int(hashed_final.sum())
+    hashed = int(np.isin(dp, sched).sum())
+    per_step = {
+        "k_prefix": int(np.minimum(L + 1, 72).sum()) + 60 * n,
+        "k_dp_part": 20 * hashed,
+        "k_dp_bucket_dups": 12 * hashed,
+        "k_dp_lens": 32 * n,
+    }
     b_sort = D + 20 * n
     b_merge = int((dp - np.minimum(lcp, dp) + 1).sum()) + 24 * n
     sort_ms = sum(v[1] for k, v in kernels.items() if k.startswith(SORT_KERNELS)) / steps
@@ -536,12 +563,14 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
         launches = kernels[k][0] / steps
         ms = kernels[k][1] / steps
         unit = DRAM_PER_UNIT.get(k)
-        traffic = unit * int(hashed_final.sum()) / max(launches, 1) if (unit and traffic_known) else None
-        # per launch: the step's bytes over its launches
-        per[k] = line(k, hash_bytes / max(launches, 1), ms / max(launches, 1), launches, formula + " (per launch)",
-                      traffic, "ncu DRAM bytes per hashed string on 8e6 strings x 200 B, times the strings hashed"
+        units = n if k in ("k_prefix", "k_dp_lens") else hashed
+        traffic = unit * units if (unit and traffic_known) else None
+        # the step's bytes over the step's time of the kernel (all its launches)
+        per[k] = line(k, per_step[k], ms, launches, formula + " (per step: all launches)", traffic,
+                      "ncu DRAM bytes per string on 8e6 strings x 200 B (D/N 0.25), times the strings"
                       if traffic is not None else "not captured for this string mix")
-    top = max(kernels.items(), key=lambda kv: kv[1][1])[0] if kernels else None
+    ranked = sorted(kernels.items(), key=lambda kv: -kv[1][1])
+    top = ranked[0][0] if ranked else None
     rl = {
         "sort_stage": line("string sort K3 (all launches of the sort stage)", b_sort, sort_ms, sort_launches,
                            "D + 20 n"),
@@ -550,11 +579,10 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
                            "D + 20 n + sum(DP - lcp + 1) + 24 n"),
     }
     rl.update(per)
-    # the headline: the DP hash-round kernel that carries a formula, the
-    # largest kernel of the step
-    main = max(per.values(), key=lambda r: r["kernel_ms"] * (r["launches"] or 1)) if per else rl["sort_stage"]
+    # the headline: the step's largest kernel among those with a formula
+    main = next((per[k] for k, _ in ranked if k in per), rl["sort_stage"])
     return {"roofline": dict(main, top_kernel=top), "rooflines": rl, "stages_ms": stages,
-            "kernels_ms": {k: round(v[1] / steps, 4) for k, v in sorted(kernels.items(), key=lambda x: -x[1][1])},
+            "kernels_ms": {k: round(v[1] / steps, 4) for k, v in ranked},
             "launches_per_step": sum(v[0] for v in kernels.values()) / steps}
 
 
@@ -793,6 +821,8 @@ def main():
     batched = None
     if world == 1 and not args.no_batched:
         batched = bench_batched(d, torch, max(3, min(args.steps, 10)), 3)
+        batched["uneven"] = bench_batched(d, torch, max(3, min(args.steps, 10)), 3,
+                                          sizes=uneven_sizes(32, 1 << 14, 4 << 20, 77))
     serving = None
     if world == 1 and not args.no_serving:
         serving = bench_serving(d, torch)

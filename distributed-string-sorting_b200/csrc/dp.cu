@@ -523,6 +523,39 @@ __global__ void __launch_bounds__(256) k_dp_part(ArenaDev a, uint32_t depth, con
     ps[(uint64_t)b * PD_CAP + at] = (uint32_t)s;
 }
 
+// k_dp_part when the hashes are stored (the string sort's first pass): four
+// consecutive strings per thread, their bucket slots claimed by independent
+// atomics before any pair is written, in few registers so that many threads
+// keep atomics in flight.
+constexpr int PD_ILP = 4;
+__global__ void __launch_bounds__(256) k_dp_part_dig(uint64_t n, const unsigned long long* dig,
+                                                     const uint32_t* hmask, uint32_t bbits, uint32_t* cursor,
+                                                     unsigned long long* ph, uint32_t* ps, uint32_t* overflow) {
+    const uint64_t s0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * PD_ILP;
+    if (s0 >= n) return;
+    const uint32_t bits = (hmask[s0 >> 5] >> (s0 & 31)) & ((1u << PD_ILP) - 1u);  // s0 is a multiple of 4
+    if (!bits) return;
+    unsigned long long h[PD_ILP];
+    uint32_t b[PD_ILP], at[PD_ILP];
+#pragma unroll
+    for (int q = 0; q < PD_ILP; ++q) h[q] = ((bits >> q) & 1u) ? dig[s0 + q] : 0ull;
+#pragma unroll
+    for (int q = 0; q < PD_ILP; ++q) {
+        b[q] = bbits ? (uint32_t)(h[q] >> (64 - bbits)) : 0u;
+        at[q] = ((bits >> q) & 1u) ? atomicAdd(&cursor[b[q]], 1u) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < PD_ILP; ++q) {
+        if (!((bits >> q) & 1u)) continue;
+        if (at[q] >= PD_CAP) {
+            atomicExch(overflow, 1u);
+            continue;
+        }
+        ph[(uint64_t)b[q] * PD_CAP + at[q]] = h[q];
+        ps[(uint64_t)b[q] * PD_CAP + at[q]] = (uint32_t)(s0 + q);
+    }
+}
+
 // One block per bucket: every pair whose hash occurs again in the bucket
 // (in the same string set) has its string marked in dmask.
 __global__ void __launch_bounds__(PD_NT) k_dp_bucket_dups(const uint32_t* cursor, const unsigned long long* ph,
@@ -998,10 +1031,17 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                     while ((1u << bbits) < nb) ++bbits;
                     DSSS_CUDA(cudaMemsetAsync(L.dmask, 0, L.mask_words * sizeof(uint32_t), st));
                     DSSS_CUDA(cudaMemsetAsync(L.pd_cursor, 0, nb * sizeof(uint32_t), st));
-                    DSSS_LAUNCH("k_dp_part", st,
-                                k_dp_part<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, dig, L.hmask, bbits,
-                                                                             L.pd_cursor, L.pd_h, L.pd_s,
-                                                                             L.counters + 10, check, L.counters + 9));
+                    if (dig && !check) {
+                        DSSS_LAUNCH("k_dp_part", st,
+                                    k_dp_part_dig<<<grid_for((a.n + PD_ILP - 1) / PD_ILP, 256), 256, 0, st>>>(
+                                        a.n, dig, L.hmask, bbits, L.pd_cursor, L.pd_h, L.pd_s, L.counters + 10));
+                    } else {
+                        DSSS_LAUNCH("k_dp_part", st,
+                                    k_dp_part<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, dig, L.hmask,
+                                                                                 bbits, L.pd_cursor, L.pd_h, L.pd_s,
+                                                                                 L.counters + 10, check,
+                                                                                 L.counters + 9));
+                    }
                     DSSS_LAUNCH("k_dp_bucket_dups", st,
                                 k_dp_bucket_dups<<<nb, PD_NT, PD_SMEM, st>>>(L.pd_cursor, L.pd_h, L.pd_s, L.dmask,
                                                                             L.counters + 8, L.set_begin, nsets));
