@@ -26,11 +26,15 @@ split into p = 64 contiguous equal PEs, sorted on one B200 by dsss_pd_sort.
   cpu_baseline  the oracle port of the reference path on the host
 
 --mode ms / --mode hq time the merge-sort path or hQuicksort alone (one GPU).
---impl reference times the CPU port of the reference path (oracle/) on all
-host cores: one independent sort of a 1e6-string sample of the same rule per
-thread, throughput = strings / wall time.
-Under torchrun (N > 1) every rank sorts its own instance (weak scaling; the
-cross-GPU exchange is not used by this benchmark).
+--impl reference times the reference's own prefix_doubling executable
+(compiled from its sources into oracle/_ref over a process-based MPI stand-in)
+on the same input with p ranks on the host cores: the median of its
+`sorting_overall` times (run_reference).
+Under torchrun (N > 1) the default is --mode dist: one distributed sort over
+all ranks, each rank holding p PEs of its own 32e6-string share (weak
+scaling), with the hash exchange of every round, the sample all-gather and
+the string all-to-all over NCCL; --mode replicas runs one independent sort
+per GPU instead.
 """
 import argparse
 import json
@@ -351,10 +355,9 @@ def run_dist(args, cfg):
                                  timeout=datetime.timedelta(seconds=300))
     else:
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    hs = d.gen_dn(n, L, k, seed=1 + rank, **gk)
     ctx = d.Context(local)
     be = D.GpuBackend(ctx)
-    ds = be.strings(hs)
+    ds = d.gen_dn_device(ctx, n, L, k, seed=1 + rank, **gk)  # each rank's share, made on its GPU
     pb = d.equal_parts(n, p).astype(np.int64)
     comm = D.Comm()
     stream = torch.cuda.current_stream()
@@ -376,6 +379,64 @@ def run_dist(args, cfg):
     t = torch.tensor([ms], device=f"cuda:{local}")
     tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
     ms = float(t.item())
+    clocks = clk.summary()
+    # the library's kernel launches of one step (CUDA-event timing on)
+    ctx.set_timing(True)
+    D.sort(comm, be, ds, pb)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    launches = sum(v[0] for k2, v in kt.items() if not k2.startswith("stage:"))
+    # end to end: each step copies the rank's strings in from pinned host
+    # memory and its merged permutation and LCPs out
+    hchars = ds.chars.cpu().pin_memory()
+    hoffs = ds.offsets.cpu().pin_memory()
+    hlens = ds.lengths.cpu().pin_memory()
+    dchars, doffs, dlens = torch.empty_like(ds.chars), torch.empty_like(ds.offsets), torch.empty_like(ds.lengths)
+    dse = d.DeviceStrings(None, chars=dchars, offsets=doffs, lengths=dlens, char_bytes=ds.char_bytes)
+    outs = [torch.empty(n, dtype=torch.int32, pin_memory=True) for _ in range(3)]
+
+    def e2e_step():
+        dchars.copy_(hchars, non_blocking=True)
+        doffs.copy_(hoffs, non_blocking=True)
+        dlens.copy_(hlens, non_blocking=True)
+        r = D.sort(comm, be, dse, pb)
+        m = int(r.get("recv_total", 0))
+        for o, key in zip(outs, ("perm_index", "perm_pe", "merged_lcp")):
+            if m:
+                o[:m].copy_(r[key][:m], non_blocking=True)
+        return m
+
+    e2e_step()
+    tdist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    recv = 0
+    for _ in range(args.steps):
+        recv = e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tdist.barrier()
+    ems = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ems], device=f"cuda:{local}")
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    ems = float(t.item())
+    # one rank: the staged path too (local sort, DP rounds with their
+    # exchanges, partition, bucket send, all-to-all, regroup, merge), with the
+    # receive containers merged by one sort and by co-ranked tiles
+    staged = None
+    if world == 1:
+        staged = {}
+        for mode in (1, 2):
+            with d.tuned(merge_by_sort=mode):
+                D.sort(comm, be, ds, pb, fused=False)
+                torch.cuda.synchronize()
+                ph2 = {}
+                t0 = time.perf_counter()
+                D.sort(comm, be, ds, pb, fused=False, phases=ph2)
+                torch.cuda.synchronize()
+                staged[f"merge_by_sort={mode}"] = {"ms_per_call": (time.perf_counter() - t0) * 1e3,
+                                                   "phases_ms": {k: round(v, 3) for k, v in ph2.items()}}
     if rank == 0:
         line = {
             "metric": "strings/s", "value": n * world / (ms * 1e-3), "unit": "strings/s", "n_gpus": world,
@@ -384,8 +445,13 @@ def run_dist(args, cfg):
             "config": {"workload": desc + f", {world} GPU(s) x {p} PEs, one distributed sort", "n_per_gpu": n,
                        "len": L, "p_per_gpu": p, "parallelism": f"{world} ranks, NCCL exchanges (dist.py)",
                        "l2": "inputs > L2, no flush"},
-            "mode": "dist", "dp_rounds": res.get("dp_rounds"), "clocks": clk.summary(),
+            "mode": "dist", "dp_rounds": res.get("dp_rounds"), "clocks": clocks,
+            "gpu_launches": int(launches * args.steps),
+            "e2e": {"value": n * world / (ems * 1e-3), "unit": "strings/s",
+                    "h2d_bytes_per_step": int(ds.char_bytes + d.PAD + 12 * n), "d2h_bytes_per_step": 12 * recv,
+                    "ms_per_step": ems},
             "phases_ms": {k: round(v, 3) for k, v in phases.items()},
+            "staged_one_rank": staged,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -639,15 +705,18 @@ def main():
     ap.add_argument("--no-formats", action="store_true", help="skip the line distribution and varint lines")
     ap.add_argument("--no-dn100m", action="store_true", help="skip the 1e8-string configuration")
     ap.add_argument("--no-autotune", action="store_true", help="skip dsss_autotune before the warm-up")
-    ap.add_argument("--mode", default="replicas", choices=["replicas", "dist", "ms", "hq"],
-                    help="replicas: one independent sort per GPU; dist: one sort over all GPUs (NCCL); "
-                         "ms / hq: the merge-sort path or hQuicksort alone on one GPU")
+    ap.add_argument("--mode", default=None, choices=["replicas", "dist", "ms", "hq"],
+                    help="replicas: one independent sort per GPU (the default on one GPU); dist: one sort over "
+                         "all GPUs with the exchanges over NCCL (the default on several GPUs); ms / hq: the "
+                         "merge-sort path or hQuicksort alone on one GPU")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.mode is None:
+        args.mode = "dist" if world > 1 else "replicas"
 
     if args.impl == "reference":
         if rank == 0:
@@ -822,7 +891,7 @@ def main():
     if world == 1 and not args.no_batched:
         batched = bench_batched(d, torch, max(3, min(args.steps, 10)), 3)
         batched["uneven"] = bench_batched(d, torch, max(3, min(args.steps, 10)), 3,
-                                          sizes=uneven_sizes(32, 1 << 14, 4 << 20, 77))
+                                          sizes=uneven_sizes(16, 1 << 14, 4 << 20, 77))
     serving = None
     if world == 1 and not args.no_serving:
         serving = bench_serving(d, torch)

@@ -217,11 +217,11 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     a.h = L.handles;
     DSSS_CUDA(cudaMemsetAsync(L.err, 0, sizeof(uint32_t), st));
     // 1. one sort per set, all sets in one segmented sort
-    bool rdig_done = false;
+    uint32_t rdig_mask = 0;
     {
         StageTimer t("stage:sort", st);
         DSSS_TRY(sort_strings(L.sort, a, n, nsets, set_begin.data(), nullptr, L.ord, L.lcp, smax, pin, st,
-                              p > 1 ? L.rdig : nullptr, &rdig_done));
+                              p > 1 ? L.rdig : nullptr, &rdig_mask));
     }
     if (p == 1) {  // prefix_doubling.hpp:236: one PE sorts locally and returns no permutation
         DSSS_CUDA(cudaMemcpyAsync(out->local_order, L.ord, n * 4, cudaMemcpyDeviceToDevice, st));
@@ -233,7 +233,7 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     {
         StageTimer t("stage:dp", st);
         DSSS_TRY(dp_rounds(L.dp, a, n, L.ord, L.lcp, L.dpg, nullptr, 0, nullptr, pin, st, nsets, set_begin.data(),
-                           rdig_done ? L.rdig : nullptr));
+                           rdig_mask ? L.rdig : nullptr, rdig_mask));
     }
     // 3. local orders per PE
     StageTimer t_local("stage:local", st);

@@ -69,6 +69,20 @@ __global__ void k_dp_lens(ArenaDev a, const uint32_t* order, uint64_t n, uint32_
 
 static unsigned lens_grid(uint64_t n) { return grid_for((n + LENS_ILP - 1) / LENS_ILP, 256); }
 
+// The shortest string of the arena into *out (set to ~0 beforehand): rounds
+// at depths up to it retire no string at its end, so they need no lengths in
+// sorted order.
+__global__ void __launch_bounds__(256) k_min_len(const uint32_t* len, const ulonglong2* h, uint64_t n,
+                                                 uint32_t* out) {
+    uint32_t m = 0xFFFFFFFFu;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        m = min(m, h ? (uint32_t)h[i].y : len[i]);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m != 0xFFFFFFFFu) atomicMin(out, m);
+}
+
 // Index of the string set holding sorted position i (set_begin: nsets+1 bounds).
 __device__ __forceinline__ uint32_t set_of(const uint64_t* set_begin, uint32_t nsets, uint64_t i) {
     uint32_t lo = 0, hi = nsets;
@@ -122,7 +136,8 @@ __device__ __forceinline__ void mark_string(uint32_t* m, uint32_t s) { atomicOr(
 
 // Grid-stride over positions (grid a few blocks per SM): one pair of counter
 // atomics per block instead of per 256 positions.  hmask (with order): every
-// hashed string is marked for the arena-order form of the round.
+// hashed string is marked for the arena-order form of the round.  lens (the
+// lengths in sorted order) may be null when every string reaches depth.
 __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all, const uint32_t* lens,
                                                      const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
                                                      uint8_t* st_next, uint8_t* kind, uint32_t* counters,
@@ -135,7 +150,7 @@ __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all,
         if (i < n) {
             uint8_t k = 0, nx = 0;
             if (all || st[i]) {
-                const uint32_t L = lens[i];
+                const uint32_t L = lens ? lens[i] : 0xFFFFFFFFu;  // no lengths: none ends before depth
                 if (depth > L) {
                     dp[i] = L;  // end of string before the depth (EOS)
                 } else {
@@ -180,7 +195,7 @@ __global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += stride) {
         const uint64_t i0 = t * 4;
-        const uint4 L4 = reinterpret_cast<const uint4*>(lens)[t];
+        const uint4 L4 = lens ? reinterpret_cast<const uint4*>(lens)[t] : make_uint4(~0u, ~0u, ~0u, ~0u);
         const uint4 C4 = reinterpret_cast<const uint4*>(lcp)[t];
         const uint32_t Ls[4] = {L4.x, L4.y, L4.z, L4.w};
         const uint32_t Cs[5] = {C4.x, C4.y, C4.z, C4.w, i0 + 4 < n ? lcp[i0 + 4] : 0u};
@@ -243,7 +258,7 @@ __global__ void __launch_bounds__(256) k_dp_classify4(const uint8_t* st, int all
         const uint64_t i = tail + tt;
         uint8_t k = 0, nx = 0;
         if (all || st[i]) {
-            const uint32_t L = lens[i];
+            const uint32_t L = lens ? lens[i] : 0xFFFFFFFFu;
             if (depth > L) {
                 dp[i] = L;
             } else {
@@ -315,7 +330,10 @@ __global__ void __launch_bounds__(256, 5) k_dp_hash(ArenaDev a, const uint64_t* 
 // k_dp_hash for rounds that hash few positions (e.g. only the roots of long
 // runs of LCP-local duplicates): a few blocks per SM stride over the kind
 // array, 16 positions per 16-byte load, instead of one thread per position.
-__global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64_t* soff, const uint8_t* kind, uint64_t n,
+// Without the gathered offsets (soff null) each hashed position finds its
+// string through order.
+__global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64_t* soff, const uint32_t* order,
+                                                        const uint8_t* kind, uint64_t n,
                                                         uint32_t depth, unsigned long long* tkeys, uint8_t* tdup,
                                                         uint32_t mask1, const uint64_t* set_begin, uint32_t nsets,
                                                         const uint64_t* set_base, const uint32_t* set_mask,
@@ -352,22 +370,34 @@ __global__ void __launch_bounds__(256) k_dp_hash_sparse(ArenaDev a, const uint64
                 base = set_base[sid];
                 mask = set_mask[sid];
             }
-            const unsigned long long h = filter_hash(xxh64_dev(a.chars + soff[i], depth));
+            uint64_t off;
+            if (soff) {
+                off = soff[i];
+            } else {
+                uint32_t len;
+                str_of(a, order[i], off, len);
+            }
+            const unsigned long long h = filter_hash(xxh64_dev(a.chars + off, depth));
             slot[i] = table_insert(tkeys, tdup, base, mask, h, err, ndup);
         }
     }
 }
 
 // One hash round's launch: the sparse form when fewer than 1/8 of the
-// positions hash.
-static int launch_dp_hash(const ArenaDev& a, const uint64_t* soff, const uint8_t* kind, uint64_t n, uint32_t depth,
+// positions hash (soff may then be null: offsets through order), else the
+// dense form (soff required).
+static bool sparse_round(uint64_t hashed, uint64_t n) { return hashed * 8 < n; }
+
+static int launch_dp_hash(const ArenaDev& a, const uint64_t* soff, const uint32_t* order, const uint8_t* kind,
+                          uint64_t n, uint32_t depth,
                           uint64_t hashed, unsigned long long* tkeys, uint8_t* tdup, uint32_t mask1,
                           const uint64_t* set_begin, uint32_t nsets, const uint64_t* set_base,
                           const uint32_t* set_mask, uint32_t* slot, uint32_t* err, uint32_t* ndup,
                           cudaStream_t st) {
-    if (hashed * 8 < n) {
+    if (sparse_round(hashed, n)) {
         DSSS_LAUNCH("k_dp_hash", st,
-                    k_dp_hash_sparse<<<stride_grid((n + 15) / 16), 256, 0, st>>>(a, soff, kind, n, depth, tkeys, tdup, mask1,
+                    k_dp_hash_sparse<<<stride_grid((n + 15) / 16), 256, 0, st>>>(a, soff, order, kind, n, depth, tkeys,
+                                                                     tdup, mask1,
                                                                      set_begin, nsets, set_base, set_mask, slot, err,
                                                                      ndup));
     } else {
@@ -473,18 +503,22 @@ __global__ void __launch_bounds__(256) k_dp_arena_insert(ArenaDev a, uint32_t de
 }
 
 // Dense rounds without a hash table in DRAM (whose random atomics bound the
-// round): the hashed strings' (hash, string) pairs are scattered in arena
+// round): the hashed strings' (hash, string) pairs are partitioned in arena
 // order into 2^B buckets by the hash's top B bits, PD_TARGET pairs per bucket
-// on average, each bucket in a region of PD_CAP pairs; one block per bucket
-// then finds the equal hashes of its bucket in shared memory.  A bucket that
-// overflows its region (PD_CAP is the mean plus 64 standard deviations for
-// uniform hashes; only many equal prefixes on different PEs can fill it)
-// sends the round to the table form.
+// on average, by two radix passes (top b1 <= 8 bits, then the next b2 = B - b1
+// bits inside each coarse bucket): per tile a shared-memory histogram, one
+// exclusive scan over the bucket-major (bucket, tile) counts, and a scatter
+// to each (bucket, tile)'s range with shared-memory cursors — no global
+// atomic per pair.  One block per bucket then finds the equal hashes of its
+// bucket in shared memory.  A bucket of more than PD_CAP pairs (the mean
+// plus 64 standard deviations for uniform hashes; only many equal prefixes on
+// different PEs can reach it) sends the round to the table form.
 constexpr uint32_t PD_TARGET = 4096;
 constexpr uint32_t PD_CAP = 8192;
 constexpr uint32_t PD_TAB = 2 * PD_CAP;  // shared-memory slots per bucket (load <= 1/2)
 constexpr uint32_t PD_NT = 1024;
 constexpr size_t PD_SMEM = (size_t)PD_CAP * 8 + (size_t)PD_TAB * 4 + PD_CAP;
+constexpr int PP_NT = 256, PP_IPT = 16, PP_TILE = PP_NT * PP_IPT;  // positions or pairs per tile
 
 static uint32_t pd_buckets(uint64_t hashed) {
     uint32_t nb = 1;
@@ -492,83 +526,170 @@ static uint32_t pd_buckets(uint64_t hashed) {
     return nb;
 }
 
-__global__ void __launch_bounds__(256) k_dp_part(ArenaDev a, uint32_t depth, const unsigned long long* dig,
-                                                 const uint32_t* hmask, uint32_t bbits, uint32_t* cursor,
-                                                 unsigned long long* ph, uint32_t* ps, uint32_t* overflow,
-                                                 uint32_t check, uint32_t* bad) {
+// The round's hashes of the hashed strings, in arena order, when the string
+// sort's first pass did not store them (or, check, to compare with them).
+__global__ void __launch_bounds__(256) k_dp_arena_hash(ArenaDev a, uint32_t depth, const unsigned long long* dig,
+                                                       const uint32_t* hmask, unsigned long long* out, uint32_t* bad) {
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.n || !bit_of(hmask, s)) return;
-    unsigned long long h;
-    if (dig) {  // stored by the string sort's first pass
-        h = dig[s];
-        if (check) {
-            uint64_t off;
-            uint32_t L;
-            str_of(a, (uint32_t)s, off, L);
-            if (h != filter_hash(xxh64_dev(a.chars + off, depth))) atomicExch(bad, 1u);
-        }
-    } else {
-        uint64_t off;
-        uint32_t L;
-        str_of(a, (uint32_t)s, off, L);
-        h = filter_hash(xxh64_dev(a.chars + off, depth));
-    }
-    const uint32_t b = bbits ? (uint32_t)(h >> (64 - bbits)) : 0u;
-    const uint32_t at = atomicAdd(&cursor[b], 1u);
-    if (at >= PD_CAP) {
-        atomicExch(overflow, 1u);
-        return;
-    }
-    ph[(uint64_t)b * PD_CAP + at] = h;
-    ps[(uint64_t)b * PD_CAP + at] = (uint32_t)s;
+    uint64_t off;
+    uint32_t L;
+    str_of(a, (uint32_t)s, off, L);
+    const unsigned long long h = filter_hash(xxh64_dev(a.chars + off, depth));
+    if (dig && h != dig[s]) atomicExch(bad, 1u);
+    out[s] = h;
 }
 
-// k_dp_part when the hashes are stored (the string sort's first pass): four
-// consecutive strings per thread, their bucket slots claimed by independent
-// atomics before any pair is written, in few registers so that many threads
-// keep atomics in flight.
-constexpr int PD_ILP = 4;
-__global__ void __launch_bounds__(256) k_dp_part_dig(uint64_t n, const unsigned long long* dig,
-                                                     const uint32_t* hmask, uint32_t bbits, uint32_t* cursor,
-                                                     unsigned long long* ph, uint32_t* ps, uint32_t* overflow) {
-    const uint64_t s0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * PD_ILP;
-    if (s0 >= n) return;
-    const uint32_t bits = (hmask[s0 >> 5] >> (s0 & 31)) & ((1u << PD_ILP) - 1u);  // s0 is a multiple of 4
-    if (!bits) return;
-    unsigned long long h[PD_ILP];
-    uint32_t b[PD_ILP], at[PD_ILP];
-#pragma unroll
-    for (int q = 0; q < PD_ILP; ++q) h[q] = ((bits >> q) & 1u) ? dig[s0 + q] : 0ull;
-#pragma unroll
-    for (int q = 0; q < PD_ILP; ++q) {
-        b[q] = bbits ? (uint32_t)(h[q] >> (64 - bbits)) : 0u;
-        at[q] = ((bits >> q) & 1u) ? atomicAdd(&cursor[b[q]], 1u) : 0u;
+// Pass 1 counts: per tile of PP_TILE arena positions, the hashed strings per
+// coarse bucket (top b1 bits), stored bucket-major: hist[b * ntiles + tile].
+__global__ void __launch_bounds__(PP_NT) k_pp_hist1(uint64_t n, const unsigned long long* dig, const uint32_t* hmask,
+                                                   uint32_t b1, uint32_t ntiles, uint32_t* hist) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t t0 = (uint64_t)blockIdx.x * PP_TILE;
+#pragma unroll 4
+    for (int j = 0; j < PP_IPT; ++j) {
+        const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
+        if (s < n && bit_of(hmask, s)) atomicAdd(&h[(uint32_t)(dig[s] >> (64 - b1))], 1u);
     }
-#pragma unroll
-    for (int q = 0; q < PD_ILP; ++q) {
-        if (!((bits >> q) & 1u)) continue;
-        if (at[q] >= PD_CAP) {
-            atomicExch(overflow, 1u);
-            continue;
+    __syncthreads();
+    hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Pass 1 scatter: each hashed string's pair to its (bucket, tile) range.
+__global__ void __launch_bounds__(PP_NT) k_pp_scatter1(uint64_t n, const unsigned long long* dig,
+                                                      const uint32_t* hmask, uint32_t b1, uint32_t ntiles,
+                                                      const uint32_t* off, unsigned long long* oh, uint32_t* os) {
+    __shared__ uint32_t cur[256];
+    cur[threadIdx.x] = off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+    __syncthreads();
+    const uint64_t t0 = (uint64_t)blockIdx.x * PP_TILE;
+#pragma unroll 4
+    for (int j = 0; j < PP_IPT; ++j) {
+        const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
+        if (s < n && bit_of(hmask, s)) {
+            const unsigned long long h = dig[s];
+            const uint32_t at = atomicAdd(&cur[(uint32_t)(h >> (64 - b1))], 1u);
+            oh[at] = h;
+            os[at] = (uint32_t)s;
         }
-        ph[(uint64_t)b[q] * PD_CAP + at[q]] = h[q];
-        ps[(uint64_t)b[q] * PD_CAP + at[q]] = (uint32_t)(s0 + q);
+    }
+}
+
+// Between the passes, one block of 256 threads, thread c for coarse bucket c
+// (mid layout: start[256], count[256], first pass-2 tile[257], count base
+// [256]): the coarse bucket's range from the pass-1 scan, its pass-2 tiles
+// (PP_TILE pairs each) and where its bucket-major counts go.
+__global__ void __launch_bounds__(256) k_pp_mid(const uint32_t* off1, uint32_t ntiles1, const uint32_t* total1,
+                                               uint32_t b1, uint32_t b2, uint32_t* mid) {
+    __shared__ uint32_t sc[256], sh[256];
+    const uint32_t c = threadIdx.x;
+    const uint32_t nc = 1u << b1;
+    uint32_t start = 0, cnt = 0;
+    if (c < nc) {
+        start = off1[(uint64_t)c * ntiles1];
+        cnt = (c + 1 < nc ? off1[(uint64_t)(c + 1) * ntiles1] : *total1) - start;
+    }
+    const uint32_t nt = (cnt + PP_TILE - 1) / PP_TILE;
+    sc[c] = nt;
+    sh[c] = nt << b2;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {  // inclusive scans (Hillis-Steele)
+        const uint32_t a = c >= (uint32_t)o ? sc[c - o] : 0u, b = c >= (uint32_t)o ? sh[c - o] : 0u;
+        __syncthreads();
+        sc[c] += a;
+        sh[c] += b;
+        __syncthreads();
+    }
+    mid[c] = start;
+    mid[256 + c] = cnt;
+    mid[512 + c] = sc[c] - nt;
+    mid[769 + c] = sh[c] - (nt << b2);
+    if (c == 255) mid[512 + 256] = sc[255];
+}
+
+__device__ __forceinline__ uint32_t pp_coarse_of(const uint32_t* tile0, uint32_t t) {
+    uint32_t lo = 0, hi = 256;  // last c with tile0[c] <= t
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (tile0[m] <= t) lo = m;
+        else hi = m;
+    }
+    return lo;
+}
+
+// Pass 2 counts: per tile of a coarse bucket, its pairs per fine bucket (the
+// next b2 bits), bucket-major inside the coarse bucket's count block.
+__global__ void __launch_bounds__(PP_NT) k_pp_hist2(const unsigned long long* h1, const uint32_t* mid, uint32_t b1,
+                                                   uint32_t b2, uint32_t* hist) {
+    __shared__ uint32_t h[256];
+    const uint32_t t = blockIdx.x;
+    if (t >= mid[512 + 256]) return;
+    const uint32_t c = pp_coarse_of(mid + 512, t);
+    const uint32_t lt = t - mid[512 + c], nt = mid[512 + c + 1] - mid[512 + c];
+    const uint32_t b = mid[c] + lt * PP_TILE, e = mid[c] + min(mid[256 + c], (lt + 1) * PP_TILE);
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = b + threadIdx.x; i < e; i += PP_NT) atomicAdd(&h[(uint32_t)((h1[i] << b1) >> (64 - b2))], 1u);
+    __syncthreads();
+    if (threadIdx.x < (1u << b2)) hist[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(PP_NT) k_pp_scatter2(const unsigned long long* h1, const uint32_t* s1,
+                                                      const uint32_t* mid, uint32_t b1, uint32_t b2,
+                                                      const uint32_t* off, unsigned long long* oh, uint32_t* os) {
+    __shared__ uint32_t cur[256];
+    const uint32_t t = blockIdx.x;
+    if (t >= mid[512 + 256]) return;
+    const uint32_t c = pp_coarse_of(mid + 512, t);
+    const uint32_t lt = t - mid[512 + c], nt = mid[512 + c + 1] - mid[512 + c];
+    const uint32_t b = mid[c] + lt * PP_TILE, e = mid[c] + min(mid[256 + c], (lt + 1) * PP_TILE);
+    if (threadIdx.x < (1u << b2)) cur[threadIdx.x] = off[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt];
+    __syncthreads();
+    for (uint32_t i = b + threadIdx.x; i < e; i += PP_NT) {
+        const unsigned long long h = h1[i];
+        const uint32_t at = atomicAdd(&cur[(uint32_t)((h << b1) >> (64 - b2))], 1u);
+        oh[at] = h;
+        os[at] = s1[i];
+    }
+}
+
+// Start of every fine bucket f = (coarse c, fine f2) and the end at [nb].
+// With b2 = 0 the coarse buckets are the fine ones.
+__global__ void k_pp_starts(const uint32_t* off1, uint32_t ntiles1, const uint32_t* total1, const uint32_t* mid,
+                            const uint32_t* off2, uint32_t b2, uint32_t nb, uint32_t* fstart) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f > nb) return;
+    if (f == nb) {
+        fstart[f] = *total1;
+    } else if (b2 == 0) {
+        fstart[f] = off1[(uint64_t)f * ntiles1];
+    } else {
+        const uint32_t c = f >> b2, f2 = f & ((1u << b2) - 1u);
+        const uint32_t nt = mid[512 + c + 1] - mid[512 + c];
+        fstart[f] = nt ? off2[mid[769 + c] + (uint64_t)f2 * nt] : mid[c];
     }
 }
 
 // One block per bucket: every pair whose hash occurs again in the bucket
 // (in the same string set) has its string marked in dmask.
-__global__ void __launch_bounds__(PD_NT) k_dp_bucket_dups(const uint32_t* cursor, const unsigned long long* ph,
+__global__ void __launch_bounds__(PD_NT) k_dp_bucket_dups(const uint32_t* fstart, const unsigned long long* ph,
                                                           const uint32_t* ps, uint32_t* dmask, uint32_t* ndup,
-                                                          const uint64_t* set_begin, uint32_t nsets) {
+                                                          const uint64_t* set_begin, uint32_t nsets,
+                                                          uint32_t* overflow) {
     extern __shared__ __align__(16) unsigned char pd_sm[];
     unsigned long long* key = (unsigned long long*)pd_sm;
     uint32_t* tab = (uint32_t*)(key + PD_CAP);
     uint8_t* dup = (uint8_t*)(tab + PD_TAB);
     const uint32_t b = blockIdx.x;
-    const uint32_t m = min(cursor[b], PD_CAP);
-    const unsigned long long* bh = ph + (uint64_t)b * PD_CAP;
-    const uint32_t* bs = ps + (uint64_t)b * PD_CAP;
+    const uint32_t m = fstart[b + 1] - fstart[b];
+    if (m > PD_CAP) {  // the same for the whole block
+        if (threadIdx.x == 0) atomicExch(overflow, 1u);
+        return;
+    }
+    const unsigned long long* bh = ph + fstart[b];
+    const uint32_t* bs = ps + fstart[b];
     for (uint32_t j = threadIdx.x; j < m; j += PD_NT) {
         key[j] = bh[j];
         dup[j] = 0;
@@ -879,6 +1000,7 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.kind = c.take<uint8_t>(N);
     L.lens = c.take<uint32_t>(N);
     L.soff = c.take<uint64_t>(N);
+    L.minlen = c.take<uint32_t>(1);
     L.slot = c.take<uint32_t>(N);
     // one set: the table for n keys; several: room for every set's own
     // power-of-two region (at most 3 slots per key plus 68 per set)
@@ -900,10 +1022,36 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.dmask = L.digest_share ? c.take<uint32_t>(L.mask_words) : nullptr;
     L.tid = L.digest_share ? c.take<uint32_t>(L.slots) : nullptr;
     // bucket regions of the dense rounds (at most pd_buckets(N) buckets)
-    L.pd_nb = L.digest_share ? pd_buckets(N) : 0;
-    L.pd_cursor = L.digest_share ? c.take<uint32_t>(L.pd_nb) : nullptr;
-    L.pd_h = L.digest_share ? c.take<unsigned long long>((uint64_t)L.pd_nb * PD_CAP) : nullptr;
-    L.pd_s = L.digest_share ? c.take<uint32_t>((uint64_t)L.pd_nb * PD_CAP) : nullptr;
+    L.pd_nb = L.digest_share ? std::max<uint32_t>(pd_buckets(N), 2) : 0;
+    if (L.digest_share) {
+        L.pd_start = c.take<uint32_t>(L.pd_nb + 1);
+        L.pd_h = c.take<unsigned long long>(N);
+        L.pd_s = c.take<uint32_t>(N);
+        L.pp_h1 = c.take<unsigned long long>(N);
+        L.pp_s1 = c.take<uint32_t>(N);
+        L.pp_dig = c.take<unsigned long long>(N);
+        // pass-1 counts: 256 per tile of positions; pass 2: at most 256 per
+        // tile of pairs plus one partial tile per coarse bucket
+        L.pp_hcap = 256ull * ((N + PP_TILE - 1) / PP_TILE + 257);
+        L.pp_hist = c.take<uint32_t>(L.pp_hcap);
+        L.pp_off = c.take<uint32_t>(2 * L.pp_hcap);
+        L.pp_mid = c.take<uint32_t>(1032);
+        L.pp_total = c.take<uint32_t>(4);
+        L.pp_scan = c.take<unsigned char>(scan_scratch_bytes(L.pp_hcap));
+    } else {
+        L.pd_start = nullptr;
+        L.pd_h = nullptr;
+        L.pd_s = nullptr;
+        L.pp_h1 = nullptr;
+        L.pp_s1 = nullptr;
+        L.pp_dig = nullptr;
+        L.pp_hcap = 0;
+        L.pp_hist = nullptr;
+        L.pp_off = nullptr;
+        L.pp_mid = nullptr;
+        L.pp_total = nullptr;
+        L.pp_scan = nullptr;
+    }
     const bool filter = N >= L.filter_min;
     L.hbuf = (filter || L.split) ? c.take<unsigned long long>(N) : nullptr;
     if (filter) {
@@ -919,7 +1067,8 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
 
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
-              cudaStream_t st, uint32_t nsets, const uint64_t* set_begin_host, const unsigned long long* rdig) {
+              cudaStream_t st, uint32_t nsets, const uint64_t* set_begin_host, const unsigned long long* rdig,
+              uint32_t rdig_mask) {
     uint32_t r = 0;
     if (n == 0) {
         if (rounds) *rounds = 0;
@@ -932,7 +1081,24 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                   cudaMemcpyHostToDevice, st));
     }
     const unsigned grid = grid_for(n, 256);
-    DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<lens_grid(n), 256, 0, st>>>(a, order, n, L.lens, L.soff));
+    // lengths and offsets in sorted order are gathered (k_dp_lens, one random
+    // handle read per position) only once a round needs them: a depth past
+    // the shortest string of the arena, or hashes taken in sorted order
+    DSSS_CUDA(cudaMemsetAsync(L.minlen, 0xFF, sizeof(uint32_t), st));
+    DSSS_LAUNCH("k_min_len", st,
+                k_min_len<<<(unsigned)std::min<uint64_t>(grid_for(a.n, 256), 148 * 8), 256, 0, st>>>(
+                    a.len, a.h, a.n, L.minlen));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.minlen, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_CUDA(cudaStreamSynchronize(st));
+    const uint64_t min_len = pin[0];
+    bool lens_ready = false;
+    auto need_lens = [&]() -> int {
+        if (!lens_ready) {
+            DSSS_LAUNCH("k_dp_lens", st, k_dp_lens<<<lens_grid(n), 256, 0, st>>>(a, order, n, L.lens, L.soff));
+            lens_ready = true;
+        }
+        return DSSS_OK;
+    };
     int cur = 0;
     const uint64_t start = 8;
     uint64_t depth = start;
@@ -946,15 +1112,17 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         const bool mark = L.hmask && a.n <= n && cands * L.digest_share >= n;
         if (mark) DSSS_CUDA(cudaMemsetAsync(L.hmask, 0, L.mask_words * sizeof(uint32_t), st));
         uint32_t* hm = mark ? L.hmask : nullptr;
+        if (depth > min_len) DSSS_TRY(need_lens());
+        const uint32_t* lens = lens_ready ? L.lens : nullptr;  // nullptr: every string reaches the depth
         if (nsets == 1 && aligned16(lcp) && aligned16(dp) && aligned16(L.lens) && aligned16(L.st[cur]) &&
             aligned16(L.st[cur ^ 1]) && aligned16(L.kind)) {
             DSSS_LAUNCH("k_dp_classify", st,
-                        k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n,
+                        k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], r == 0, lens, lcp, n,
                                                                                 (uint32_t)depth, dp, L.st[cur ^ 1],
                                                                                 L.kind, L.counters, order, hm));
         } else {
             DSSS_LAUNCH("k_dp_classify", st,
-                        k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, L.lens, lcp, n, (uint32_t)depth,
+                        k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, lens, lcp, n, (uint32_t)depth,
                                                                      dp, L.st[cur ^ 1], L.kind, L.counters,
                                                                      L.set_begin, nsets, L.set_cnt, order, hm));
         }
@@ -974,6 +1142,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         if (pin[2]) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table regions exceed the plan");
         if (hashed && L.bits && hashed >= L.filter_min) {
             // fingerprint filter, then an exact table over the candidates only
+            DSSS_TRY(need_lens());
             const uint64_t words = nsets > 1 ? ((uint64_t)pin[7] << 32 | pin[6])
                                              : pow2_at_least((uint64_t)hashed * L.filter_bpk, 1024) / 32;
             if (words > L.bm_words) return fail(DSSS_EDEVICE, "distinguishing-prefix filter exceeds the plan");
@@ -1020,31 +1189,61 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
             const uint32_t check = (uint32_t)tune(TUNE_DP_CHECK);
             if (arena) {
                 const int dj = root_digest_index(depth);
-                const unsigned long long* dig = rdig && dj >= 0 ? rdig + (uint64_t)dj * a.n : nullptr;
+                const unsigned long long* dig =
+                    rdig && dj >= 0 && ((rdig_mask >> dj) & 1u) ? rdig + (uint64_t)dj * a.n : nullptr;
                 // buckets in shared memory first; the table only if a bucket overflows
                 bool done = false;
-                const uint32_t nb = pd_buckets(hashed);
-                if (nb <= L.pd_nb) {
+                uint32_t bbits = 1;  // at least two buckets (both radix shifts stay below 64)
+                while ((1ull << bbits) < pd_buckets(hashed)) ++bbits;
+                const uint32_t nb = 1u << bbits;
+                if (nb <= L.pd_nb && bbits <= 16) {
                     static std::atomic<uint64_t> pd_configured{0};
                     DSSS_TRY(set_smem_once(pd_configured, k_dp_bucket_dups, (int)PD_SMEM));
-                    uint32_t bbits = 0;
-                    while ((1u << bbits) < nb) ++bbits;
                     DSSS_CUDA(cudaMemsetAsync(L.dmask, 0, L.mask_words * sizeof(uint32_t), st));
-                    DSSS_CUDA(cudaMemsetAsync(L.pd_cursor, 0, nb * sizeof(uint32_t), st));
-                    if (dig && !check) {
-                        DSSS_LAUNCH("k_dp_part", st,
-                                    k_dp_part_dig<<<grid_for((a.n + PD_ILP - 1) / PD_ILP, 256), 256, 0, st>>>(
-                                        a.n, dig, L.hmask, bbits, L.pd_cursor, L.pd_h, L.pd_s, L.counters + 10));
-                    } else {
-                        DSSS_LAUNCH("k_dp_part", st,
-                                    k_dp_part<<<grid_for(a.n, 256), 256, 0, st>>>(a, (uint32_t)depth, dig, L.hmask,
-                                                                                 bbits, L.pd_cursor, L.pd_h, L.pd_s,
-                                                                                 L.counters + 10, check,
-                                                                                 L.counters + 9));
+                    const unsigned long long* hd = dig;
+                    if (!dig || check) {  // this round's hashes, in arena order
+                        DSSS_LAUNCH("k_dp_arena_hash", st,
+                                    k_dp_arena_hash<<<grid_for(a.n, 256), 256, 0, st>>>(
+                                        a, (uint32_t)depth, check ? dig : nullptr, L.hmask, L.pp_dig, L.counters + 9));
+                        hd = L.pp_dig;
                     }
+                    // two radix passes: top b1 bits, then the next b2 inside each coarse bucket
+                    const uint32_t b1 = std::min<uint32_t>(bbits, 8), b2 = bbits - b1;
+                    const uint32_t nt1 = (uint32_t)((a.n + PP_TILE - 1) / PP_TILE);
+                    DSSS_LAUNCH("k_pp_hist1", st,
+                                k_pp_hist1<<<nt1, PP_NT, 0, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_hist));
+                    DSSS_TRY(exclusive_scan_u32(L.pp_hist, L.pp_off, 256ull * nt1, L.pp_total, L.pp_scan, st));
+                    const unsigned long long* ph = L.pp_h1;
+                    const uint32_t* ps = L.pp_s1;
+                    DSSS_LAUNCH("k_pp_scatter1", st,
+                                k_pp_scatter1<<<nt1, PP_NT, 0, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_off, L.pp_h1,
+                                                                     L.pp_s1));
+                    uint32_t* off2 = nullptr;
+                    if (b2) {
+                        // pass-2 tiles: at most one partial tile per coarse bucket beyond hashed / PP_TILE
+                        const uint64_t nt2 = hashed / PP_TILE + 257;
+                        const uint64_t h2 = nt2 << b2;
+                        if (h2 > L.pp_hcap) return fail(DSSS_EDEVICE, "distinguishing-prefix partition exceeds the plan");
+                        off2 = L.pp_off + L.pp_hcap;  // the second pass's offsets beside the first's
+                        DSSS_LAUNCH("k_pp_mid", st,
+                                    k_pp_mid<<<1, 256, 0, st>>>(L.pp_off, nt1, L.pp_total, b1, b2, L.pp_mid));
+                        DSSS_CUDA(cudaMemsetAsync(L.pp_hist, 0, h2 * sizeof(uint32_t), st));
+                        DSSS_LAUNCH("k_pp_hist2", st,
+                                    k_pp_hist2<<<(unsigned)nt2, PP_NT, 0, st>>>(L.pp_h1, L.pp_mid, b1, b2, L.pp_hist));
+                        DSSS_TRY(exclusive_scan_u32(L.pp_hist, off2, h2, L.pp_total + 1, L.pp_scan, st));
+                        DSSS_LAUNCH("k_pp_scatter2", st,
+                                    k_pp_scatter2<<<(unsigned)nt2, PP_NT, 0, st>>>(L.pp_h1, L.pp_s1, L.pp_mid, b1, b2,
+                                                                                   off2, L.pd_h, L.pd_s));
+                        ph = L.pd_h;
+                        ps = L.pd_s;
+                    }
+                    DSSS_LAUNCH("k_pp_starts", st,
+                                k_pp_starts<<<grid_for(nb + 1, 256), 256, 0, st>>>(L.pp_off, nt1, L.pp_total, L.pp_mid,
+                                                                                  off2, b2, nb, L.pd_start));
                     DSSS_LAUNCH("k_dp_bucket_dups", st,
-                                k_dp_bucket_dups<<<nb, PD_NT, PD_SMEM, st>>>(L.pd_cursor, L.pd_h, L.pd_s, L.dmask,
-                                                                            L.counters + 8, L.set_begin, nsets));
+                                k_dp_bucket_dups<<<nb, PD_NT, PD_SMEM, st>>>(L.pd_start, ph, ps, L.dmask,
+                                                                            L.counters + 8, L.set_begin, nsets,
+                                                                            L.counters + 10));
                     DSSS_CUDA(cudaGetLastError());
                     DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
                     DSSS_CUDA(cudaStreamSynchronize(st));
@@ -1068,6 +1267,9 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                             k_dp_query_mask<<<stride_grid(n), 256, 0, st>>>(L.kind, order, L.dmask, n, L.st[cur ^ 1],
                                                                            L.counters, L.counters + 8));
             } else {
+                // hashes in sorted order read the offsets: gathered for all
+                // positions unless few hash (those find theirs through order)
+                if (L.split || !sparse_round(hashed, n)) DSSS_TRY(need_lens());
                 DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
                 DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
                 if (L.split) {
@@ -1078,7 +1280,8 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                                                  (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base,
                                                                  L.set_mask, L.slot, L.counters + 2, L.counters + 8));
                 } else {
-                    DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, (uint32_t)depth, hashed, L.tkeys, L.tdup,
+                    DSSS_TRY(launch_dp_hash(a, lens_ready ? L.soff : nullptr, order, L.kind, n, (uint32_t)depth, hashed,
+                                            L.tkeys, L.tdup,
                                             (uint32_t)(slots - 1), L.set_begin, nsets, L.set_base, L.set_mask, L.slot,
                                             L.counters + 2, L.counters + 8, st));
                 }
@@ -1159,7 +1362,7 @@ int dp_one_round(const DpRoundLayout& R, const ArenaDev& a, uint64_t n, const ui
         const uint64_t slots = table_slots(pin[0]);
         DSSS_CUDA(cudaMemsetAsync(L.tkeys, 0xFF, slots * sizeof(unsigned long long), st));
         DSSS_CUDA(cudaMemsetAsync(L.tdup, 0, slots, st));
-        DSSS_TRY(launch_dp_hash(a, L.soff, L.kind, n, depth, pin[0], L.tkeys, L.tdup, (uint32_t)(slots - 1), nullptr,
+        DSSS_TRY(launch_dp_hash(a, L.soff, order, L.kind, n, depth, pin[0], L.tkeys, L.tdup, (uint32_t)(slots - 1), nullptr,
                                 1, nullptr, nullptr, L.slot, L.counters + 2, L.counters + 8, st));
         DSSS_LAUNCH("k_dp_query", st,
                     k_dp_query<<<stride_grid(n), 256, 0, st>>>(L.kind, L.slot, L.tdup, n, L.st[1], L.counters,

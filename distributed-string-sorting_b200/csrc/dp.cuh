@@ -9,6 +9,7 @@ struct DpLayout {
     uint8_t* kind;
     uint32_t* lens;
     uint64_t* soff;
+    uint32_t* minlen;  // the shortest string of the arena (one word)
     uint32_t* slot;
     unsigned long long* tkeys;
     uint8_t* tdup;
@@ -40,13 +41,27 @@ struct DpLayout {
     uint32_t* dmask;
     uint64_t mask_words;
     uint32_t* tid;
-    // dense rounds without the table: (hash, string) pairs bucketed by the
-    // hash's top bits, pd_nb buckets of PD_CAP pairs at most, deduplicated in
-    // shared memory
+    // dense rounds without the table: (hash, string) pairs partitioned by
+    // the hash's top bits in two radix passes into at most pd_nb buckets,
+    // each deduplicated in shared memory: the pairs after the first pass
+    // (pp_h1 / pp_s1) and after the second (pd_h / pd_s), the buckets' starts
+    // (pd_start, pd_nb + 1), the round's hashes in arena order when the sort
+    // did not store them (pp_dig), per-tile counts and their scan (pp_hist,
+    // pp_off: pp_hcap and 2 pp_hcap entries), the coarse buckets' layout
+    // (pp_mid) and the passes' totals (pp_total)
     uint32_t pd_nb;
-    uint32_t* pd_cursor;
+    uint32_t* pd_start;
     unsigned long long* pd_h;
     uint32_t* pd_s;
+    unsigned long long* pp_h1;
+    uint32_t* pp_s1;
+    unsigned long long* pp_dig;
+    uint32_t* pp_hist;
+    uint32_t* pp_off;
+    uint64_t pp_hcap;
+    uint32_t* pp_mid;
+    uint32_t* pp_total;
+    unsigned char* pp_scan;
     uint64_t* set_bbase;
     uint32_t* set_bmask;
     uint32_t* set_ccnt;
@@ -60,11 +75,12 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets = 1);
 // duplicates of prefixes in the same set.
 // rdig (optional): the string sort's prefix hashes at the first schedule
 // depths (ROOT_DIGESTS arrays of a.n entries, array j for depth
-// root_digest_depth(j)), read by the arena-order rounds at those depths.
+// root_digest_depth(j), valid where bit j of rdig_mask is set), read by the
+// arena-order rounds at those depths.
 int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* order, const uint32_t* lcp,
               uint32_t* dp, uint64_t* round_counts, uint32_t max_rounds, uint32_t* rounds, uint32_t* pin,
               cudaStream_t st, uint32_t nsets = 1, const uint64_t* set_begin_host = nullptr,
-              const unsigned long long* rdig = nullptr);
+              const unsigned long long* rdig = nullptr, uint32_t rdig_mask = 0);
 
 struct DpRoundLayout {
     DpLayout dp;

@@ -132,7 +132,8 @@ enum TuneKnob : int {
     TUNE_SORT_PIVOT,         // pivot passes on (1) or off (0)
     TUNE_DP_TABLE,           // DP hash-table slots per hashed string (rounded up to a power of two)
     TUNE_SORT_GRAPH,         // largest n sorted by the device-driven graph (0: never)
-    TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1) or by merge rounds (0)
+    TUNE_MERGE_SORT,         // receive containers merged by sorting their union (1), by merge rounds (0) or
+                             // by co-ranked tiles of all runs at once (2)
     TUNE_MERGE_LANES,        // threads per chunk of strings in the prefix decompression (0: from the length)
     TUNE_DP_SPLIT,           // hash round split into hashing and table inserts (1) or one kernel (0)
     TUNE_COPY_WORD,          // bytes per store when whole strings are copied out (16, or 8)
@@ -140,6 +141,8 @@ enum TuneKnob : int {
                              // (k_dp_arena_insert); 0 turns the arena-order form off
     TUNE_DP_CHECK,           // 1: the arena-order rounds recompute every stored prefix hash from the string and
                              // fail on a mismatch (a self-check)
+    TUNE_SORT_SPLIT_MIN,     // smallest large segment that may split by sampled splitters instead of a key
+                             // byte (0: never; values below 4096 count as 4096)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);
@@ -491,14 +494,15 @@ __host__ __device__ inline int root_digest_index(uint64_t depth) {
     return depth == 8 ? 0 : depth == 24 ? 1 : depth == 40 ? 2 : depth == 72 ? 3 : -1;
 }
 
-// filter_hash(XXH64(p, d)) for d = 8, 24, 40, 72 from one set of loads (the
-// words of the first 72 bytes); out[j] for depths beyond len is left as is.
-// The same values as xxh64_dev (one stripe feeds the 40-byte hash, two the
-// 72-byte one; both merge the lanes since their lengths exceed 32).
+// filter_hash(XXH64(p, d)) for the depths d = 8, 24, 40, 72 whose bit is set
+// in want, from one set of loads (the words of the first 72 bytes); out[j]
+// for depths beyond len, or not wanted, is left as is.  The same values as
+// xxh64_dev (one stripe feeds the 40-byte hash, two the 72-byte one; both
+// merge the lanes since their lengths exceed 32).
 __device__ __forceinline__ void root_digests(const uint8_t* p, uint32_t len, unsigned long long* out,
-                                             uint64_t stride) {
+                                             uint64_t stride, uint32_t want) {
     using namespace xxh;
-    if (len < 8) return;
+    if (len < 8 || !want) return;
     const uintptr_t a = (uintptr_t)p;
     const uint4* q = (const uint4*)(a & ~(uintptr_t)15);
     const uint32_t skip = (uint32_t)(a & 15);
@@ -539,14 +543,14 @@ __device__ __forceinline__ void root_digests(const uint8_t* p, uint32_t len, uns
         return merge(h, v4);
     };
     const uint64_t w0 = word(0);
-    out[0] = filter_hash(aval(tail8(P5 + 8, w0)));
+    if (want & 1u) out[0] = filter_hash(aval(tail8(P5 + 8, w0)));
     if (len < 24) return;
     const uint64_t w1 = word(1), w2 = word(2);
-    out[stride] = filter_hash(aval(tail8(tail8(tail8(P5 + 24, w0), w1), w2)));
-    if (len < 40) return;
+    if (want & 2u) out[stride] = filter_hash(aval(tail8(tail8(tail8(P5 + 24, w0), w1), w2)));
+    if (len < 40 || !(want & 12u)) return;
     uint64_t v1 = round(P1 + P2, w0), v2 = round(P2, w1), v3 = round(0, w2), v4 = round(0 - P1, word(3));
-    out[2 * stride] = filter_hash(aval(tail8(merged(v1, v2, v3, v4) + 40, word(4))));
-    if (len < 72) return;
+    if (want & 4u) out[2 * stride] = filter_hash(aval(tail8(merged(v1, v2, v3, v4) + 40, word(4))));
+    if (len < 72 || !(want & 8u)) return;
     v1 = round(v1, word(4));
     v2 = round(v2, word(5));
     v3 = round(v3, word(6));

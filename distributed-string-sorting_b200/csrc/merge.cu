@@ -376,6 +376,169 @@ __global__ void __launch_bounds__(MG_NT) k_merge_round(FullView f, const MergeJo
     }
 }
 
+// ------------------------------------------------------------ K-way merge ----
+// The p runs of each receiving PE merged at once by co-ranked tiles (knob
+// merge_by_sort = 2): every KW_GAP-th string of every run is a sample; the
+// samples of each receiving PE are sorted; every KW_STEP-th sorted sample B
+// bounds a tile, and its rank in each run q (the number of q's strings
+// before B in the merged order: bytes, then position, so that byte-identical
+// strings keep run order) is found by a binary search inside the window of
+// KW_GAP strings that the samples leave (the run's samples before B are
+// counted from their sorted positions).  Every tile thus holds, from each
+// run, the strings between two consecutive bounds: about KW_GAP * KW_STEP
+// strings, at most (KW_STEP + p) * KW_GAP.  The tiles' strings are gathered
+// in run order and each tile is sorted on its own from the LCP of its two
+// bounds (the segment sorter, in shared memory for tiles up to 4096
+// strings); the LCP at each tile's first string, with the previous tile's
+// last, is computed last.
+constexpr uint32_t KW_GAP = 32;
+constexpr uint32_t KW_STEP = 32;
+
+// x before y in the merged order: bytes, then position.
+__device__ __forceinline__ bool kw_before(const FullView& f, uint32_t x, uint32_t y) {
+    uint32_t l;
+    const int c = cmp_from(f, x, y, 0, &l);
+    return c < 0 || (c == 0 && x < y);
+}
+
+// Run r's samples: positions 0, KW_GAP, 2 KW_GAP, ... (one block per run).
+__global__ void k_kw_samples(const uint32_t* run_begin, const uint32_t* run_len, const uint32_t* sbase, uint32_t* samp) {
+    const uint32_t r = blockIdx.x;
+    const uint32_t cnt = sbase[r + 1] - sbase[r];
+    for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) samp[sbase[r] + k] = run_begin[r] + k * KW_GAP;
+}
+
+// Sorted position of every sample, stored at the sample's place (run, k).
+__global__ void k_kw_posof(const uint32_t* sorted, uint64_t ns, const uint32_t* run_of, const uint32_t* run_begin,
+                           const uint32_t* sbase, uint32_t* pos) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const uint32_t x = sorted[j];
+    const uint32_t r = run_of[x];
+    pos[sbase[r] + (x - run_begin[r]) / KW_GAP] = (uint32_t)j;
+}
+
+// One thread per (bound, run of the bound's receiving PE): the run's
+// strings before the bound.  bb: first bound of each receiving PE (nrecv + 1);
+// sb: first sorted sample of each receiving PE.
+__global__ void k_kw_corank(FullView f, const uint32_t* sorted, const uint32_t* pos, const uint32_t* sbase,
+                            const uint32_t* run_begin, const uint32_t* run_len, const uint32_t* bb, const uint64_t* sb,
+                            uint32_t nrecv, uint32_t p, uint32_t* split) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nb = bb[nrecv];
+    if (g >= nb * p) return;
+    const uint32_t b = (uint32_t)(g / p), q = (uint32_t)(g % p);
+    uint32_t lo = 0, hi = nrecv;  // receiving PE: last R with bb[R] <= b
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (bb[m] <= b) lo = m;
+        else hi = m;
+    }
+    const uint32_t R = lo;
+    const uint64_t j = sb[R] + (uint64_t)KW_STEP * (b - bb[R] + 1);  // the bound's sorted position
+    const uint32_t B = sorted[j];
+    const uint32_t rq = R * p + q;
+    // samples of run rq sorted before the bound (their sorted positions rise)
+    uint32_t a = sbase[rq], e = sbase[rq + 1];
+    while (a < e) {
+        const uint32_t m = (a + e) >> 1;
+        if (pos[m] < j) a = m + 1;
+        else e = m;
+    }
+    const uint32_t c = a - sbase[rq];
+    uint32_t s = 0;
+    if (c > 0) {
+        // sample c - 1 (position (c - 1) KW_GAP) is before B, sample c (if any) is not
+        uint32_t l2 = (c - 1) * KW_GAP + 1, h2 = min(c * KW_GAP, run_len[rq]);
+        while (l2 < h2) {
+            const uint32_t m = (l2 + h2) >> 1;
+            if (kw_before(f, run_begin[rq] + m, B)) l2 = m + 1;
+            else h2 = m;
+        }
+        s = l2;
+    }
+    split[g] = s;
+}
+
+// One block per tile: its strings gathered in run order (the tile's range of
+// every run), its first output position and its strings' shared prefix (the
+// LCP of its two bounds; 0 for a receiving PE's first and last tile).
+// tb: first tile of each receiving PE (nrecv + 1).
+__global__ void __launch_bounds__(256) k_kw_gather(FullView f, const uint32_t* sorted, const uint32_t* split,
+                                                  const uint32_t* run_begin, const uint32_t* run_len,
+                                                  const uint32_t* tb, const uint32_t* bb, const uint64_t* sb,
+                                                  uint32_t nrecv, uint32_t p, uint32_t* gathered, uint64_t* tstart,
+                                                  uint32_t* tdepth) {
+    extern __shared__ uint32_t kw_sm[];  // lo[p], pre[p + 1]
+    uint32_t* lo_s = kw_sm;
+    uint32_t* pre = kw_sm + p;
+    const uint32_t t = blockIdx.x;
+    uint32_t lo = 0, hi = nrecv;  // receiving PE: last R with tb[R] <= t
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (tb[m] <= t) lo = m;
+        else hi = m;
+    }
+    const uint32_t R = lo, lt = t - tb[R], nbR = bb[R + 1] - bb[R];
+    for (uint32_t q = threadIdx.x; q < p; q += blockDim.x) {
+        const uint32_t rq = R * p + q;
+        const uint32_t a = lt == 0 ? 0u : split[(uint64_t)(bb[R] + lt - 1) * p + q];
+        const uint32_t e = lt == nbR ? run_len[rq] : split[(uint64_t)(bb[R] + lt) * p + q];
+        lo_s[q] = a;
+        pre[q + 1] = e - a;
+    }
+    __syncthreads();
+    __shared__ unsigned long long s_first;
+    if (threadIdx.x == 0) {
+        pre[0] = 0;
+        uint64_t first = run_begin[R * p];  // the receiving PE's first output position
+        for (uint32_t q = 0; q < p; ++q) {
+            first += lo_s[q];
+            pre[q + 1] += pre[q];
+        }
+        s_first = first;
+        tstart[t] = first;
+        uint32_t d = 0;
+        if (lt > 0 && lt < nbR) {
+            uint32_t l;
+            cmp_from(f, sorted[sb[R] + (uint64_t)KW_STEP * lt], sorted[sb[R] + (uint64_t)KW_STEP * (lt + 1)], 0, &l);
+            d = l;
+        }
+        tdepth[t] = d;
+    }
+    __syncthreads();
+    const uint64_t first = s_first;
+    const uint32_t size = pre[p];
+    for (uint32_t o = threadIdx.x; o < size; o += blockDim.x) {
+        uint32_t a = 0, e = p;  // run: last q with pre[q] <= o
+        while (e - a > 1) {
+            const uint32_t m = (a + e) >> 1;
+            if (pre[m] <= o) a = m;
+            else e = m;
+        }
+        gathered[first + o] = run_begin[R * p + a] + lo_s[a] + (o - pre[a]);
+    }
+}
+
+// The LCP at every tile's first string but a receiving PE's first.
+__global__ void k_kw_lcp_fix(FullView f, const uint64_t* tstart, const uint32_t* tb, uint32_t nrecv,
+                             const uint32_t* order, uint32_t* mlcp) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tb[nrecv]) return;
+    uint32_t lo = 0, hi = nrecv;
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (tb[m] <= t) lo = m;
+        else hi = m;
+    }
+    if (t == tb[lo]) return;  // a receiving PE's first tile: LCP 0 there
+    const uint64_t at = tstart[t];
+    if (at == tstart[t + 1]) return;  // an empty tile: the next one's start is the same place
+    uint32_t l;
+    cmp_from(f, order[at - 1], order[at], 0, &l);
+    mlcp[at] = l;
+}
+
 __global__ void k_merge_init(const uint32_t* lcp, const uint8_t* run_start, uint64_t n, uint32_t* ids, uint32_t* l) {
     const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
@@ -404,6 +567,58 @@ __global__ void k_run_marks(const uint32_t* run_begin, const uint32_t* run_len, 
         run_start[run_begin[r] + k] = k == 0 ? 1 : 0;
         run_of[run_begin[r] + k] = r;
     }
+}
+
+// Scratch of the K-way merge (sizes from the run lengths, on the host).
+struct KwLayout {
+    uint32_t *samp, *ssort, *slcp, *pos, *sbase, *split, *gathered, *tdepth, *bb, *tb;
+    uint64_t *tstart, *sb;
+    SortLayout SL;
+};
+
+struct KwPlan {
+    std::vector<uint32_t> sbase, bb, tb;
+    std::vector<uint64_t> sb;
+    uint64_t ns = 0, nb = 0, nt = 0;
+};
+
+static KwPlan kw_plan(const std::vector<uint32_t>& rl, uint32_t nrecv, uint32_t p) {
+    KwPlan P;
+    const uint32_t nruns = nrecv * p;
+    P.sbase.assign(nruns + 1, 0);
+    for (uint32_t r = 0; r < nruns; ++r) P.sbase[r + 1] = P.sbase[r] + (rl[r] + KW_GAP - 1) / KW_GAP;
+    P.sb.assign(nrecv + 1, 0);
+    P.bb.assign(nrecv + 1, 0);
+    P.tb.assign(nrecv + 1, 0);
+    for (uint32_t R = 0; R < nrecv; ++R) {
+        P.sb[R] = P.sbase[(uint64_t)R * p];
+        const uint64_t ms = P.sbase[(uint64_t)(R + 1) * p] - P.sbase[(uint64_t)R * p];
+        const uint32_t nbR = ms ? (uint32_t)((ms - 1) / KW_STEP) : 0u;
+        P.bb[R + 1] = P.bb[R] + nbR;
+        P.tb[R + 1] = P.tb[R] + nbR + 1;
+    }
+    P.sb[nrecv] = P.sbase[nruns];
+    P.ns = P.sbase[nruns];
+    P.nb = P.bb[nrecv];
+    P.nt = P.tb[nrecv];
+    return P;
+}
+
+static void layout_kw(Carve& c, KwLayout& K, const KwPlan& P, uint64_t n, uint32_t nrecv, uint32_t p) {
+    const uint64_t ns = P.ns ? P.ns : 1;
+    K.samp = c.take<uint32_t>(ns);
+    K.ssort = c.take<uint32_t>(ns);
+    K.slcp = c.take<uint32_t>(ns);
+    K.pos = c.take<uint32_t>(ns);
+    K.sbase = c.take<uint32_t>((uint64_t)nrecv * p + 1);
+    K.split = c.take<uint32_t>(P.nb * p + 1);
+    K.gathered = c.take<uint32_t>(n ? n : 1);
+    K.tstart = c.take<uint64_t>(P.nt + 1);
+    K.tdepth = c.take<uint32_t>(P.nt + 1);
+    K.bb = c.take<uint32_t>(nrecv + 1);
+    K.tb = c.take<uint32_t>(nrecv + 1);
+    K.sb = c.take<uint64_t>(nrecv + 1);
+    layout_sort(c, K.SL, n, (uint32_t)std::max<uint64_t>(P.nt, nrecv), 0);
 }
 
 static int tree_levels(uint64_t n) {
@@ -516,11 +731,17 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
     const uint64_t full_bytes = *(const uint64_t*)(pin + 4);
     // reserve the decompressed arena behind the layout (and the string sort's
     // scratch behind it when the runs are merged by sorting)
-    const bool by_sort = tune(TUNE_MERGE_SORT) != 0;
+    const int64_t mode = tune(TUNE_MERGE_SORT);  // 0 pairwise rounds, 1 one sort, 2 K-way tiles
+    const bool by_sort = mode == 1;
+    const bool kway = mode == 2;
     SortLayout SL;
+    KwLayout K;
+    KwPlan P;
+    if (kway) P = kw_plan(rl, nrecv, p);
     Carve sz2(nullptr);
     layout_merge(sz2, L, n, bytes, full_bytes, nruns);
     if (by_sort) layout_sort(sz2, SL, n, nrecv, 0);
+    if (kway) layout_kw(sz2, K, P, n, nrecv, p);
     if (sz2.used > ctx->ws_cap) {
         // grow: everything computed so far lives in the scratch, so recompute
         // after growing (simplest correct path; the next call reuses the size)
@@ -531,7 +752,50 @@ int lcp_merge(Ctx* ctx, const uint8_t* chars, uint64_t bytes, const uint32_t* ch
     Carve c1(ctx->ws);
     layout_merge(c1, L, n, bytes, full_bytes, nruns);
     if (by_sort) layout_sort(c1, SL, n, nrecv, 0);
+    if (kway) layout_kw(c1, K, P, n, nrecv, p);
     DSSS_TRY(run_extend(chars, start, L.l[0], tree, n, full_bytes, L.foff, L.flen, L.full, L.counters + 2, st));
+    if (kway) {
+        ArenaDev fa{L.full, L.foff, L.flen, n};
+        const FullView f{L.full, L.foff, L.flen};
+        uint32_t* mlcp = merged_lcp ? merged_lcp : L.l[1];
+        DSSS_CUDA(cudaMemcpyAsync(K.sbase, P.sbase.data(), P.sbase.size() * 4, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(K.sb, P.sb.data(), P.sb.size() * 8, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(K.bb, P.bb.data(), P.bb.size() * 4, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(K.tb, P.tb.data(), P.tb.size() * 4, cudaMemcpyHostToDevice, st));
+        DSSS_CUDA(cudaMemcpyAsync(K.tstart + P.nt, &n, 8, cudaMemcpyHostToDevice, st));
+        // samples of every run, sorted per receiving PE
+        DSSS_LAUNCH("k_kw_samples", st, k_kw_samples<<<nruns, 256, 0, st>>>(L.run_begin, L.run_len, K.sbase, K.samp));
+        DSSS_TRY(sort_strings(K.SL, fa, P.ns, nrecv, P.sb.data(), K.samp, K.ssort, K.slcp, 0, (uint32_t*)ctx->pin, st));
+        if (P.ns)
+            DSSS_LAUNCH("k_kw_posof", st,
+                        k_kw_posof<<<grid_for(P.ns, 256), 256, 0, st>>>(K.ssort, P.ns, L.run_of, L.run_begin, K.sbase,
+                                                                       K.pos));
+        // every bound's rank in every run of its receiving PE, then the tiles
+        if (P.nb)
+            DSSS_LAUNCH("k_kw_corank", st,
+                        k_kw_corank<<<grid_for(P.nb * p, 256), 256, 0, st>>>(f, K.ssort, K.pos, K.sbase, L.run_begin,
+                                                                            L.run_len, K.bb, K.sb, nrecv, p, K.split));
+        DSSS_LAUNCH("k_kw_gather", st,
+                    k_kw_gather<<<(unsigned)P.nt, 256, (2 * p + 1) * sizeof(uint32_t), st>>>(
+                        f, K.ssort, K.split, L.run_begin, L.run_len, K.tb, K.bb, K.sb, nrecv, p, K.gathered, K.tstart,
+                        K.tdepth));
+        std::vector<uint64_t> ts(P.nt + 1);
+        DSSS_CUDA(cudaMemcpyAsync(ts.data(), K.tstart, (P.nt + 1) * 8, cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        // every tile sorted on its own, from its strings' shared prefix
+        DSSS_TRY(sort_strings(K.SL, fa, n, (uint32_t)P.nt, ts.data(), K.gathered, order, mlcp, 0, (uint32_t*)ctx->pin,
+                              st, nullptr, nullptr, K.tdepth));
+        DSSS_LAUNCH("k_kw_lcp_fix", st,
+                    k_kw_lcp_fix<<<grid_for(P.nt, 256), 256, 0, st>>>(f, K.tstart, K.tb, nrecv, order, mlcp));
+        DSSS_LAUNCH("k_merge_tags", st,
+                    k_merge_tags<<<grid_for(n, 256), 256, 0, st>>>(order, lcp, L.run_start, L.run_of, L.run_begin,
+                                                                  L.run_offset, p, n, old_lcp, perm_index, perm_pe));
+        pin = (uint32_t*)ctx->pin;
+        DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        DSSS_CUDA(cudaStreamSynchronize(st));
+        if (pin[2]) return fail(DSSS_EINVAL, "merge: a source run does not start with LCP 0");
+        return DSSS_OK;
+    }
     if (by_sort) {
         // Merging sorted runs by sorting their union: each receiving PE's
         // strings are one segment of the string sort, with ids in run order so

@@ -46,9 +46,32 @@ struct Seg {
     unsigned long long diff;
     // speculated common-prefix depth + 1 (0: none) and the OR of key ^ key0
     // over the keys k_prefix wrote at that depth (segments without keys)
-    uint32_t spec, spec_pad;
+    uint32_t spec;
+    // this pass's digit: the key byte at the first difference (nspl = 0), or
+    // the bucket among nspl sampled splitters (table spl_slot; bucket-start
+    // LCPs into the fix list from fix0)
+    uint32_t nspl;
     unsigned long long spec_diff;
+    uint32_t spl_slot, fix0;
 };
+
+// Sampled splitters.  Where the key byte at a large segment's first
+// difference takes few values (letters, DNA), a byte digit splits the segment
+// only a few ways per pass.  Instead, the distinct keys among every 8th of an
+// evenly spaced, sorted sample of SPL_SAMPLE keys become m <= 255 splitters.
+// With more than SPL_EQ_MAX of them a key's bucket is the number of
+// splitters below it (about 1/256 of the segment each; two splitters are
+// keys of the segment in different buckets, so it splits).  With fewer (few
+// distinct keys: frequent ones), bucket 2j holds the keys between splitters
+// j-1 and j and bucket 2j+1 the keys equal to splitter j, so every sampled
+// key lands in an equality bucket and the others elsewhere.  Equal keys
+// always share a bucket, and two neighbours across a bucket boundary have
+// different keys, so their LCP is the depth plus the LCP of the two keys; it
+// is written once the final order is known (k_lcp_fix).
+constexpr int SPL_SAMPLE = 2048;
+constexpr uint32_t SPL_MAX = 255, SPL_STRIDE = 256, SPL_EQ_MAX = 127;
+constexpr uint32_t SPL_MIN_FLOOR = 4096;  // smallest sort_split_min other than 0 (off)
+constexpr uint32_t FIX_NONE = 0xFFFFFFFFu;
 
 constexpr int NBINS = 4;
 __host__ __device__ constexpr int bin_cap(int b) { return b == 0 ? 32 : b == 1 ? 256 : b == 2 ? 1024 : 4096; }
@@ -56,8 +79,9 @@ __device__ __forceinline__ int bin_of(uint32_t size) {
     return size <= 32 ? 0 : size <= 256 ? 1 : size <= 1024 ? 2 : 3;
 }
 
-// Counters block (device): [0] n_large_next, [1..4] n_small per bin,
-// [8] total tiles, [9] total chunks, [10] error flag (a guard tripped).
+// Counters block (device): [0] n_large_next, [1..4] n_small per bin, [5]
+// fix-list slots reserved, [6] splitter tables of the pass, [8] total tiles,
+// [9] total chunks, [10] error flag (a guard tripped).
 struct SortState {
     ArenaDev a;
     uint32_t* ord[2];
@@ -80,6 +104,14 @@ struct SortState {
     // depths (root_digests), ROOT_DIGESTS arrays of dig_n entries
     unsigned long long* dig;
     uint64_t dig_n;
+    // sampled splitters: segments of at least split_min strings (0: never);
+    // cap_spl tables of SPL_STRIDE keys per pass; the fix list holds
+    // (position, depth) pairs of bucket starts whose LCP k_lcp_fix writes
+    uint32_t split_min;
+    const uint32_t* seg_depth;  // optional: each segment's shared prefix length
+    unsigned long long* spl;
+    uint32_t* fix;
+    uint64_t cap_spl, cap_fix;
 };
 
 __device__ __forceinline__ uint32_t find_seg(const uint32_t* first, uint32_t nseg, uint32_t t) {
@@ -110,7 +142,9 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
     s.first_digit = 0;
     s.diff = 0;
     s.spec = 0;
-    s.spec_pad = 0;
+    s.nspl = 0;
+    s.spl_slot = 0;
+    s.fix0 = 0;
     s.spec_diff = 0;
     S.small[b][slot] = s;
 }
@@ -131,7 +165,9 @@ __device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_
     s.first_digit = 0;
     s.diff = 0;
     s.spec = 0;
-    s.spec_pad = 0;
+    s.nspl = 0;
+    s.spl_slot = 0;
+    s.fix0 = 0;
     s.spec_diff = 0;
     dst[slot] = s;
 }
@@ -152,8 +188,10 @@ __global__ void k_init_segs(SortState S, const uint64_t* pb, uint32_t p) {
         S.ord_out[start] = S.ord[0][start];
         return;
     }
-    if (size > S.small_max) push_large(S, S.large[0], start, size, 0, 0);
-    else push_small(S, start, size, 0, 0);
+    // a segment whose strings are known to share their first bytes starts there
+    const uint32_t d = S.seg_depth ? S.seg_depth[q] : 0u;
+    if (size > S.small_max) push_large(S, S.large[0], start, size, d, 0);
+    else push_small(S, start, size, d, 0);
 }
 
 // --------------------------------------------------------- tile indexing ----
@@ -260,6 +298,18 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
     const uint32_t d0 = sg.depth, cap = d0 + PREFIX_CAP;
     const uint32_t s0 = ord[sg.start];
+    // prefix hashes (first pass only) at the schedule depths past the common
+    // prefix this segment is expected to have: at or below it every string of
+    // the segment shares its prefix with the others, so a round there hashes
+    // one root per segment and never reads stored hashes; a depth skipped
+    // here is marked so that the rounds hash it from the strings
+    uint32_t dmask = 0;
+    if (S.dig) {
+        const uint32_t shared = sg.spec ? sg.spec - 1 : d0 + SPEC_MAX;
+        for (int j = 0; j < ROOT_DIGESTS; ++j)
+            if (root_digest_depth(j) > shared) dmask |= 1u << j;
+        if (dmask != (1u << ROOT_DIGESTS) - 1 && threadIdx.x == 0) atomicOr(&S.counters[15], ~dmask & 15u);
+    }
     uint64_t off0;
     uint32_t len0;
     str_of(S.a, s0, off0, len0);
@@ -287,7 +337,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
             uint32_t len;
             const uint32_t s = ord[i];
             str_of(S.a, s, off, len);
-            if (S.dig) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n);
+            if (dmask) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n, dmask);
             uint64_t x[PF_W];
             key_words<PF_W>(S.a.chars, off, len, d0, want, x);
             uint32_t l = D;
@@ -326,7 +376,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_prefix(SortState S, Seg* segs, uin
         uint32_t len;
         const uint32_t s = ord[i];
         str_of(S.a, s, off, len);
-        if (S.dig) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n);
+        if (dmask) root_digests(S.a.chars + off, len, S.dig + s, S.dig_n, dmask);
         // no need to compare past this thread's minimum so far
         const uint32_t lim = min(cap, mn);
         uint32_t l = 0;
@@ -427,7 +477,15 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
     }
     uint64_t df = 0;
     if (valid) {
-        for (uint32_t i = tb + threadIdx.x; i < te; i += LT_NT) df |= key[i] ^ k0;
+        // the tile's keys all in flight before any is used
+        uint64_t k[LT_IPT];
+#pragma unroll
+        for (int j = 0; j < LT_IPT; ++j) {
+            const uint32_t i = tb + j * LT_NT + threadIdx.x;
+            k[j] = i < te ? key[i] : k0;
+        }
+#pragma unroll
+        for (int j = 0; j < LT_IPT; ++j) df |= k[j] ^ k0;
     } else {
         // KD_ILP independent gathers in flight per thread
         for (uint32_t i0 = tb + threadIdx.x; i0 < te; i0 += KD_ILP * LT_NT) {
@@ -460,6 +518,127 @@ __global__ void __launch_bounds__(LT_NT) k_keys_diff(SortState S, Seg* segs, uin
 #pragma unroll
     for (int o = 16; o; o >>= 1) df |= __shfl_xor_sync(0xffffffffu, df, o);
     if ((threadIdx.x & 31) == 0 && df) atomicOr(&sg.diff, (unsigned long long)df);
+}
+
+// ------------------------------------------------------ sampled splitters ----
+// Per large segment with keys (not a pivot pass) of at least split_min
+// strings: the sample's byte-digit histogram at the first difference decides
+// whether splitters pay (its largest bucket holds more than 1/64 of the
+// sample, four times what a splitter bucket holds); if so, the sorted
+// sample's every 8th key, distinct, become the splitters.  One block of
+// SPL_SAMPLE / 2 threads per segment.
+__global__ void __launch_bounds__(SPL_SAMPLE / 2) k_split_sample(SortState S, Seg* segs, uint32_t nseg) {
+    if (!segs) {  // graph mode: this pass's list and count live on the device
+        segs = S.large[S.counters[12]];
+        nseg = S.counters[13];
+    }
+    __shared__ unsigned long long sk[SPL_SAMPLE];
+    __shared__ uint32_t bcnt[256];
+    __shared__ uint32_t s_fix0, s_nres;
+    for (uint32_t si = blockIdx.x; si < nseg; si += gridDim.x) {
+        Seg& sg = segs[si];
+        const bool use = S.split_min && sg.size >= S.split_min && sg.diff != 0 && !(sg.flags & (F_PIVOT | F_PSEUDO));
+        if (!use) {  // the same for the whole block
+            if (threadIdx.x == 0) sg.nspl = 0;
+            continue;
+        }
+        const unsigned long long* key = S.key[sg.flags & F_PARITY];
+        const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
+        if (threadIdx.x < 256) bcnt[threadIdx.x] = 0;
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < (uint32_t)SPL_SAMPLE; j += blockDim.x) {
+            const unsigned long long k = key[sg.start + (uint32_t)((uint64_t)j * sg.size / SPL_SAMPLE)];
+            sk[j] = k;
+            atomicAdd(&bcnt[(uint32_t)(k >> shift) & 0xFFu], 1u);
+        }
+        __syncthreads();
+        // bitonic sort of the sample, ascending: thread t compares index i
+        // (bit j clear) with i | j
+        for (uint32_t k = 2; k <= (uint32_t)SPL_SAMPLE; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                const uint32_t i = ((threadIdx.x & ~(j - 1)) << 1) | (threadIdx.x & (j - 1));
+                const unsigned long long a = sk[i], b = sk[i | j];
+                if ((a > b) == ((i & k) == 0)) {
+                    sk[i] = b;
+                    sk[i | j] = a;
+                }
+                __syncthreads();
+            }
+        }
+        if (threadIdx.x == 0) {
+            uint32_t mx = 0;
+            for (int d = 0; d < 256; ++d) mx = max(mx, bcnt[d]);
+            uint32_t m = 0, slot = 0, fix0 = 0, nres = 0;
+            if (64 * mx > (uint32_t)SPL_SAMPLE) {
+                slot = atomicAdd(&S.counters[6], 1u);
+                if (slot < S.cap_spl) {
+                    unsigned long long* spl = S.spl + (uint64_t)slot * SPL_STRIDE;
+                    for (uint32_t q = 0; q < SPL_MAX; ++q) {
+                        const unsigned long long c = sk[(q + 1) * (SPL_SAMPLE / SPL_STRIDE) - 1];
+                        if (m == 0 || c != spl[m - 1]) spl[m++] = c;
+                    }
+                    for (uint32_t q = m; q < SPL_STRIDE; ++q) spl[q] = ~0ull;
+                    // bucket-start slots in the fix list, one per bucket
+                    nres = m > SPL_EQ_MAX ? m + 1 : 2 * m + 1;
+                    fix0 = atomicAdd(&S.counters[5], nres);
+                    if ((uint64_t)fix0 + nres > S.cap_fix) m = 0;
+                }
+            }
+            s_fix0 = fix0;
+            s_nres = nres;
+            sg.nspl = m;
+            sg.spl_slot = slot;
+            sg.fix0 = fix0;
+        }
+        __syncthreads();
+        // every reserved fix slot starts empty (also a reservation past the
+        // list's end, as far as the list goes)
+        if (s_nres) {
+            const uint64_t e = min((uint64_t)s_fix0 + s_nres, S.cap_fix);
+            for (uint64_t f = (uint64_t)s_fix0 + threadIdx.x; f < e; f += blockDim.x) S.fix[2 * f] = FIX_NONE;
+        }
+        __syncthreads();  // the sample buffer is reused by the next segment
+    }
+}
+
+// Bucket of key k among m sorted splitters (the table padded to SPL_STRIDE
+// with ~0): j = the number of splitters below k (at most m, eight fixed
+// steps); with more than SPL_EQ_MAX splitters j, else 2j, or 2j + 1 when k
+// equals splitter j.
+__device__ __forceinline__ uint32_t spl_bucket(const unsigned long long* spl, uint32_t m, unsigned long long k) {
+    uint32_t j = 0;
+#pragma unroll
+    for (uint32_t step = SPL_STRIDE / 2; step; step >>= 1)
+        if (spl[j + step - 1] < k) j += step;
+    if (m > SPL_EQ_MAX) return j;
+    return 2 * j + (j < m && spl[j] == k ? 1u : 0u);
+}
+
+// LCPs at the bucket starts of splitter passes, once the order is final: the
+// two neighbours have different keys at depth d.
+__global__ void __launch_bounds__(256) k_lcp_fix(SortState S) {
+    const uint64_t m = min((uint64_t)S.counters[5], S.cap_fix);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t f = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; f < m; f += stride) {
+        const uint32_t pos = S.fix[2 * f];
+        if (pos == FIX_NONE) continue;
+        uint32_t l = S.fix[2 * f + 1];
+        const uint32_t x = S.ord_out[pos - 1], y = S.ord_out[pos];
+        for (;;) {
+            const uint64_t kx = key8_of(S.a, x, l), ky = key8_of(S.a, y, l);
+            if (kx != ky) {
+                l += key_lcp(kx, ky);
+                break;
+            }
+            const uint32_t z = zero_byte(kx);
+            if (z < 8) {
+                l += z;
+                break;
+            }
+            l += 8;
+        }
+        S.lcp_out[pos] = l;
+    }
 }
 
 // ----------------------------------------------------------------- pivot ----
@@ -558,15 +737,19 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     // one 256-bin histogram per warp (shared-memory atomics contend only
     // inside a warp), summed per digit at the end
     __shared__ uint32_t hist[LT_NT / 32][256];
+    __shared__ unsigned long long s_spl[SPL_STRIDE];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
     const Seg sg = segs[si];
     if (sg.diff == 0) return;
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
+    const uint32_t m = sg.nspl;
     const unsigned long long* key = S.key[sg.flags & F_PARITY];
 #pragma unroll
     for (int w = 0; w < LT_NT / 32; ++w) hist[w][threadIdx.x] = 0;
+    if (m)
+        for (uint32_t q = threadIdx.x; q < SPL_STRIDE; q += LT_NT) s_spl[q] = S.spl[(uint64_t)sg.spl_slot * SPL_STRIDE + q];
     __syncthreads();
     const uint32_t tb = sg.start + (t - S.tile0[si]) * LT_TILE;
     const uint32_t te = min(sg.start + sg.size, tb + LT_TILE);
@@ -581,7 +764,7 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = tb + j * LT_NT + threadIdx.x;
-        if (i < te) atomicAdd(&wh[digit_of(k[j], shift)], 1u);
+        if (i < te) atomicAdd(&wh[m ? spl_bucket(s_spl, m, k[j]) : digit_of(k[j], shift)], 1u);
     }
     __syncthreads();
     uint32_t c = 0;
@@ -604,8 +787,19 @@ __global__ void k_chunk_sum(SortState S, const Seg* segs, uint32_t nseg) {
     const uint32_t ntiles = (sg.size + LT_TILE - 1) / LT_TILE;
     const uint32_t t0 = S.tile0[si] + (c - S.chunk0[si]) * CHUNK_TILES;
     const uint32_t t1 = min(S.tile0[si] + ntiles, t0 + CHUNK_TILES);
+    // each tile's count becomes its exclusive prefix inside the chunk (one
+    // read for the scatter instead of the chunk's earlier tiles); every load
+    // of the chunk in flight before the first store
+    uint32_t v[CHUNK_TILES];
+#pragma unroll
+    for (int q = 0; q < CHUNK_TILES; ++q)
+        v[q] = t0 + q < t1 ? S.tile_hist[(uint64_t)(t0 + q) * 256 + threadIdx.x] : 0u;
     uint32_t s = 0;
-    for (uint32_t t = t0; t < t1; ++t) s += S.tile_hist[(uint64_t)t * 256 + threadIdx.x];
+#pragma unroll
+    for (int q = 0; q < CHUNK_TILES; ++q) {
+        if (t0 + q < t1) S.tile_hist[(uint64_t)(t0 + q) * 256 + threadIdx.x] = s;
+        s += v[q];
+    }
     S.chunk_pre[(uint64_t)c * 256 + threadIdx.x] = s;
 }
 
@@ -705,7 +899,12 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
     if (total < 2) return;
     const uint32_t cs = sg.start + excl;
     const uint32_t np = par ^ 1u;
-    if (!pseudo) {
+    if (sg.nspl) {
+        // splitter buckets: children keep the keys at this depth (an
+        // equality bucket's keys are all equal: its next pass goes deeper)
+        if (total > S.small_max) push_large(S, next, cs, total, depth, np | F_KEYS);
+        else push_small(S, cs, total, depth, np | F_KEYS);
+    } else if (!pseudo) {
         if (d == 0) return;  // strings that end here: written by the scatter
         // children keep the parent's keys: their first b+1 key bytes are now
         // common; one that keeps most of the parent gets a pivot pass
@@ -761,6 +960,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     __shared__ uint32_t tloff[256];
     __shared__ uint32_t wcnt[LT_NT / 32][256];
     __shared__ uint32_t wsum[LT_NT / 32];
+    __shared__ unsigned long long s_spl[SPL_STRIDE];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
     const uint32_t si = find_seg(S.tile0, nseg, t);
@@ -770,6 +970,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     const uint32_t b = (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t shift = 56 - 8 * b;
     const uint32_t depth = sg.depth;
+    const uint32_t m = sg.nspl;  // splitter buckets (0: the byte digit)
     const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
     // LCP inside the group of strings that end here and at bucket starts
     // (pivot code splits: d + min(l, l') from the two codes)
@@ -777,17 +978,17 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     const uint32_t lcp_here = pseudo ? depth + pivot_l((uint32_t)(S.key[par][sg.start] >> 56)) : depth + b;
     const uint32_t tloc = t - S.tile0[si];
     const uint32_t c = S.chunk0[si] + tloc / CHUNK_TILES;
-    const uint32_t tfirst = t - tloc % CHUNK_TILES;
     {
         const uint32_t d = threadIdx.x;
         const uint32_t* bk = S.bucket + (uint64_t)si * 257;
-        uint32_t o = bk[d] + S.chunk_pre[(uint64_t)c * 256 + d];
-        for (uint32_t u = tfirst; u < t; ++u) o += S.tile_hist[(uint64_t)u * 256 + d];
-        base[d] = o;
+        // k_chunk_sum left the tile's prefix inside its chunk in tile_hist
+        base[d] = bk[d] + S.chunk_pre[(uint64_t)c * 256 + d] + S.tile_hist[(uint64_t)t * 256 + d];
         bstart[d] = bk[d];
         if (d == 0) bstart[256] = bk[256];
 #pragma unroll
         for (int w = 0; w < LT_NT / 32; ++w) wcnt[w][d] = 0;
+        if (m)
+            for (uint32_t q = d; q < SPL_STRIDE; q += LT_NT) s_spl[q] = S.spl[(uint64_t)sg.spl_slot * SPL_STRIDE + q];
     }
     __syncthreads();
     const uint32_t* ord = S.ord[par];
@@ -811,14 +1012,14 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = wb + j * 32 + lane;
-        const uint32_t dg = i < te ? digit_of(k[j], shift) : 0x100u + lane;
+        const uint32_t dg = i < te ? (m ? spl_bucket(s_spl, m, k[j]) : digit_of(k[j], shift)) : 0x100u + lane;
         const uint32_t peers = __match_any_sync(0xffffffffu, dg);
         const uint32_t r = __popc(peers & ((1u << lane) - 1));
         const uint32_t prev = dg < 256 ? wcnt[w][dg] : 0;
         __syncwarp();
         if (dg < 256 && lane == __ffs(peers) - 1) wcnt[w][dg] = prev + __popc(peers);
         __syncwarp();
-        rk[j] = prev + r;
+        rk[j] = (dg & 0xFFu) << 24 | (prev + r);  // the digit kept for the placement below
     }
     __syncthreads();
     {
@@ -848,8 +1049,8 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = wb + j * 32 + lane;
         if (i >= te) continue;
-        const uint32_t dg = digit_of(k[j], shift);
-        const uint32_t lp = tloff[dg] + wcnt[w][dg] + rk[j];
+        const uint32_t dg = rk[j] >> 24;
+        const uint32_t lp = tloff[dg] + wcnt[w][dg] + (rk[j] & 0xFFFFFFu);
         if (lp >= tn) {  // never taken when the counts agree
             atomicExch(&S.counters[10], 1u);
             continue;
@@ -868,7 +1069,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
             continue;
         }
         const uint32_t oo = sord[x];
-        const bool ended = dg == 0 && !code_split;
+        const bool ended = !m && dg == 0 && !code_split;
         if (ended || cnt == 1) {
             S.ord_out[dest] = oo;
             if (ended && dest != bs) S.lcp_out[dest] = lcp_here;
@@ -876,7 +1077,13 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
             ord_dst[dest] = oo;
             key_dst[dest] = skey[x];
         }
-        if (dest == bs && dg != sg.first_digit) {
+        if (m) {
+            // a splitter bucket's start: its LCP once the order is final
+            if (dest == bs && dg != sg.first_digit) {
+                S.fix[2 * ((uint64_t)sg.fix0 + dg)] = dest;
+                S.fix[2 * ((uint64_t)sg.fix0 + dg) + 1] = depth;
+            }
+        } else if (dest == bs && dg != sg.first_digit) {
             uint32_t l = lcp_here;
             if (code_split) {
                 uint32_t pd = dg - 1;  // previous non-empty code (exists: dg is not the first)
@@ -1562,6 +1769,7 @@ __global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, const Seg* se
             S.counters[10] = 1;
         }
         S.counters[0] = 0;  // large segments of the next pass
+        S.counters[6] = 0;  // splitter tables of this pass
     }
 }
 
@@ -1646,6 +1854,7 @@ static int sort_strings_graph(const SortLayout& L, SortState S, uint64_t n, uint
             k_prefix<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_pivot<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_keys_diff<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            if (S.split_min) k_split_sample<<<148, SPL_SAMPLE / 2, 0, bst>>>(S, nullptr, 0);
             k_hist<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_chunk_sum<<<chunks, 256, 0, bst>>>(S, nullptr, 0);
             k_seg_scan<<<large, 256, 0, bst>>>(S, nullptr, 0, nullptr);
@@ -1661,6 +1870,7 @@ static int sort_strings_graph(const SortLayout& L, SortState S, uint64_t n, uint
         k_seg_sort<256, 128><<<148 * 8, 128, seg_sort_smem<256>(), st>>>(S, S.small[1], 0, S.counters + 2);
         k_seg_sort<1024, 256><<<148 * 4, 256, seg_sort_smem<1024>(), st>>>(S, S.small[2], 0, S.counters + 3);
         k_seg_sort<4096, 256><<<148, 256, seg_sort_smem<4096>(), st>>>(S, S.small[3], 0, S.counters + 4);
+        if (S.split_min) k_lcp_fix<<<148 * 4, 256, 0, st>>>(S);
         cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     }
     cudaGraph_t whole = nullptr;
@@ -1708,13 +1918,21 @@ void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small
     L.counters = c.take<uint32_t>(16);
     L.pb = c.take<uint64_t>(p + 1);
     L.scan = c.take<unsigned char>(scan_scratch_bytes(L.cap_large));
+    // splitter tables: segments of at least SPL_MIN_FLOOR strings per pass;
+    // fix list: (position, depth) pairs (when it runs short, passes keep the
+    // byte digit)
+    L.cap_spl = N / SPL_MIN_FLOOR + p + 1;
+    L.spl = c.take<unsigned long long>(L.cap_spl * SPL_STRIDE);
+    L.cap_fix = N / 16 + 65536;
+    L.fix = c.take<uint32_t>(2 * L.cap_fix);
     L.pin = nullptr;
 }
 
 int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p, const uint64_t* pb_host,
                  const uint32_t* ids_in, uint32_t* ord_out, uint32_t* lcp_out, uint32_t small_max,
-                 uint32_t* pin, cudaStream_t st, unsigned long long* dig, bool* dig_done) {
-    if (dig_done) *dig_done = false;
+                 uint32_t* pin, cudaStream_t st, unsigned long long* dig, uint32_t* dig_mask,
+                 const uint32_t* seg_depth) {
+    if (dig_mask) *dig_mask = 0;
     if (n == 0) return DSSS_OK;
     SortState S;
     S.a = a;
@@ -1739,6 +1957,15 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;
     S.cap_chunks = L.cap_chunks;
+    {
+        const int64_t v = tune(TUNE_SORT_SPLIT_MIN);
+        S.split_min = v <= 0 ? 0u : (uint32_t)std::min<int64_t>(std::max<int64_t>(v, SPL_MIN_FLOOR), 0xFFFFFFFFll);
+    }
+    S.seg_depth = seg_depth;
+    S.spl = L.spl;
+    S.fix = L.fix;
+    S.cap_spl = L.cap_spl;
+    S.cap_fix = L.cap_fix;
     S.dig = nullptr;
     S.dig_n = n;
     // the first pass reads every string when every initial segment is large
@@ -1770,10 +1997,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     uint32_t nlarge = pin[0];
     int cur = 0;
     uint32_t guard = 0;
-    if (dig_all) {
-        S.dig = dig;
-        if (dig_done) *dig_done = true;
-    }
+    S.dig = dig_all ? dig : nullptr;
+    bool first_pass = true;
     while (nlarge) {
         if (++guard > (1u << 24)) return fail(DSSS_EDEVICE, "string sort made no progress");
         Seg* segs = large[cur];
@@ -1789,6 +2014,9 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_pivot", st, k_pivot<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        if (S.split_min)
+            DSSS_LAUNCH("k_split_sample", st,
+                        k_split_sample<<<std::min<uint32_t>(nlarge, 148 * 2), SPL_SAMPLE / 2, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_hist", st, k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_seg_scan", st, k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next));
@@ -1800,6 +2028,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
         if (nlarge > L.cap_large) return fail(DSSS_EDEVICE, "string sort: large-segment list overflow");
         cur ^= 1;
+        if (first_pass && S.dig && dig_mask) *dig_mask = 15u & ~pin[15];  // depths no segment skipped
+        first_pass = false;
         S.dig = nullptr;
     }
     for (int b = 0; b < NBINS; ++b)
@@ -1811,6 +2041,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     DSSS_TRY((launch_seg_sort<256, 128>(S, S.small[1], pin[2], "k_seg_sort256", st)));
     DSSS_TRY((launch_seg_sort<1024, 256>(S, S.small[2], pin[3], "k_seg_sort1024", st)));
     DSSS_TRY((launch_seg_sort<4096, 256>(S, S.small[3], pin[4], "k_seg_sort4096", st)));
+    if (pin[5]) DSSS_LAUNCH("k_lcp_fix", st, k_lcp_fix<<<grid_for(std::min<uint64_t>(pin[5], L.cap_fix), 256), 256, 0, st>>>(S));
     DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
     if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");

@@ -1,9 +1,10 @@
 // Autotuner: times the full path on the caller's input under every setting of
 // the tuning knobs in a small grid (small-segment cutoff of the string sort,
-// pivot passes, the DP fingerprint filter) and leaves the fastest setting in
-// force.  Results never depend on the knobs, so tuning only changes speed.
-// The radix digit (one byte) and the scatter tile (4096 strings) are fixed in
-// this build: the 256-bin shared-memory histograms and the 13-byte-per-string
+// pivot passes, the MSD digit: sampled splitters where a key byte splits
+// poorly, or one key byte always) and leaves the fastest setting in force.
+// Results never depend on the knobs, so tuning only changes speed.  The
+// digit's bucket count (256) and the scatter tile (2048 strings) are fixed in
+// this build: the shared-memory histograms and the 13-byte-per-string
 // staging of the scatter are sized for them.
 #include <cstdio>
 #include <vector>
@@ -16,14 +17,14 @@ using namespace dsss;
 namespace {
 
 struct Setting {
-    int64_t small_max, pivot, filter_min;
+    int64_t small_max, pivot, split_min;
 };
 
 struct Knobs {
     int64_t v[3];
 };
 
-const char* const kNames[3] = {"sort_small_max", "sort_pivot", "dp_filter_min"};
+const char* const kNames[3] = {"sort_small_max", "sort_pivot", "sort_split_min"};
 
 Knobs get_knobs() {
     Knobs k;
@@ -57,14 +58,14 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const Knobs saved = get_knobs();
-    const Setting grid[] = {{4096, 1, 1ll << 40}, {1024, 1, 1ll << 40}, {256, 1, 1ll << 40}, {4096, 0, 1ll << 40},
-                            {1024, 0, 1ll << 40}, {256, 0, 1ll << 40}, {4096, 1, 0},         {1024, 1, 0},
-                            {256, 1, 0},          {4096, 0, 0},         {1024, 0, 0},         {256, 0, 0}};
+    const Setting grid[] = {{4096, 1, 65536}, {1024, 1, 65536}, {256, 1, 65536}, {4096, 0, 65536},
+                            {1024, 0, 65536}, {256, 0, 65536}, {4096, 1, 0},     {1024, 1, 0},
+                            {256, 1, 0},      {4096, 0, 0},     {1024, 0, 0},     {256, 0, 0}};
     double best = 1e300, first = 0;
     int best_i = -1, rc = DSSS_OK;
     uint32_t tried = 0;
     for (int i = 0; i < (int)(sizeof grid / sizeof grid[0]) && rc == DSSS_OK; ++i) {
-        const int64_t v[3] = {grid[i].small_max, grid[i].pivot, grid[i].filter_min};
+        const int64_t v[3] = {grid[i].small_max, grid[i].pivot, grid[i].split_min};
         set_knobs(v);
         ActiveCtx active(ctx);
         rc = pd_sort_dev(ctx, in, nsets, p, part_begin, opts, &r, st);  // warm: scratch grows here
@@ -93,11 +94,12 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
         set_knobs(saved.v);
         return rc != DSSS_OK ? rc : fail(DSSS_EDEVICE, "autotune: no setting ran");
     }
-    const int64_t v[3] = {grid[best_i].small_max, grid[best_i].pivot, grid[best_i].filter_min};
+    const int64_t v[3] = {grid[best_i].small_max, grid[best_i].pivot, grid[best_i].split_min};
     set_knobs(v);
     out->sort_small_max = v[0];
     out->sort_pivot = v[1];
-    out->dp_filter_min = v[2];
+    out->sort_split_min = v[2];
+    dsss_tune_get("dp_filter_min", &out->dp_filter_min);
     out->best_ms = best;
     out->default_ms = first;
     out->settings_tried = tried;

@@ -159,6 +159,16 @@ class GpuBackend:
                                     stream=self.stream)
         return order, lcp
 
+    def fused_sort(self, ds, pb, sampler):
+        """Every PE on this GPU: the one-GPU path (dsss_pd_sort)."""
+        from . import pd_sort
+        pb = np.asarray(pb, np.uint64)
+        p = len(pb) - 1
+        out = pd_sort(self.ctx, ds, p, part_begin=pb, sampler=sampler, stream=self.stream)
+        return dict(local_order=out["local_order"], dp=out["dp"], intervals=np.asarray(out["intervals"], np.int64)
+                    .reshape(p, p), recv_counts=np.asarray(out["recv_counts"], np.int64), perm_index=out["perm_index"],
+                    perm_pe=out["perm_pe"], merged_lcp=out["merged_lcp"])
+
     def new_dp(self, n):
         return self._e(n, self.torch.int32)
 
@@ -508,10 +518,12 @@ def _exchange(comm, be, strings, pb, order, lcp, dp, p, p_all, p_local, q_first,
 
 
 def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2, phases=None,
-         compress_lcps: bool = False, golomb: bool = False):
+         compress_lcps: bool = False, golomb: bool = False, fused: bool = True):
     """This rank's part of DistributedPrefixDoublingSort::sort.  strings: the
     backend's arena of this rank's strings; part_begin: p_local + 1 PE bounds.
-    phases (dict, optional) receives milliseconds per phase.  golomb: the
+    phases (dict, optional) receives milliseconds per phase.  fused: with one
+    rank, the one-GPU path (False: the staged path with its exchanges, as
+    with several ranks).  golomb: the
     hashes of every round cross as Golomb/delta-coded blocks, the
     sequentialGolombEncoding policy (AllToAllHashesGolomb,
     bloomfilter.hpp:164-243): each rank's hash records sorted (ips4o::sort,
@@ -531,8 +543,18 @@ def sort(comm: Comm, be, strings, part_begin, sampler: int = 0, factor: int = 2,
     pe_goff = np.concatenate([[0], np.cumsum(pe_sizes)]).astype(np.int64)
     res = dict(part_begin=pb, p_global=p, q_first=q_first)
 
-    # local sort (prefix_doubling.hpp:228)
     ph.mark("setup")
+    if fused and comm.world == 1 and p > 1 and factor == 2 and hasattr(be, "fused_sort"):
+        # one rank holds every PE: nothing crosses GPUs, so the one-GPU path
+        # (one global sort, DP rounds over it, projections for the exchange)
+        # gives this rank's results directly
+        out = be.fused_sort(strings, pb, sampler)
+        res.update(out)
+        res["recv_total"] = int(np.asarray(out["recv_counts"]).sum())
+        ph.mark("fused")
+        return res
+
+    # local sort (prefix_doubling.hpp:228)
     order, lcp = be.local_sort(strings, pb)
     res["local_order"] = order
     ph.mark("local_sort")

@@ -119,8 +119,13 @@ int dsss_abi_version(void);
  *                   read-back costs less than the graph's capacity-sized grids
  *                   and per-call instantiation)
  *   merge_by_sort   dsss_lcp_merge: decompressed runs merged by one segmented
- *                   string sort (1, default) or by pairwise merge-path rounds
- *                   (0); identical results, ties in run order either way
+ *                   string sort (1, default), by pairwise merge-path rounds
+ *                   (0), or all p runs at once by co-ranked tiles (2: every
+ *                   32nd string of every run sampled, the samples sorted, every
+ *                   32nd sorted sample ranked in each run by binary search,
+ *                   each tile of the runs' strings between two such bounds
+ *                   sorted on its own from the bounds' common prefix);
+ *                   identical results, ties in run order in every mode
  *   merge_extend_lanes  dsss_lcp_merge prefix decompression: threads that
  *                   decompress a chunk of 128 consecutive strings in order
  *                   (4, 8, 16 or 32; default 0 = from the average
@@ -137,6 +142,11 @@ int dsss_abi_version(void);
  *                   and the outcome read back as one bit per sorted position
  *                   (k = 1..64, default 4); 0 hashes every round by gathering
  *                   the prefixes in sorted order
+ *   sort_split_min  smallest segment of the string sort's MSD passes that
+ *                   may split by up to 255 splitters sampled from its keys
+ *                   instead of by one key byte, where that byte takes few
+ *                   values (letters, DNA; default 65536; 0 = never; values
+ *                   below 4096 count as 4096)
  *   dp_check        1: the arena-order rounds at depths 8, 24, 40 and 72,
  *                   which read the prefix hashes the string sort's first pass
  *                   stored, recompute each from the string and fail with
@@ -147,13 +157,17 @@ int dsss_tune_get(const char* name, int64_t* value);
 /* Autotuner (no reference counterpart): runs the full path (as
  * dsss_pd_sort_batched; nsets = 1 for one set) on the given device input
  * under each setting of a grid of the knobs above (sort_small_max 256 / 1024 /
- * 4096, sort_pivot on / off, the DP filter on / off), 1 + trials runs each,
- * and leaves the fastest setting in force for later calls.  out: the chosen
- * setting, its time (minimum over trials) and the default setting's time. */
+ * 4096, sort_pivot on / off, sort_split_min 65536 / 0: the MSD digit as
+ * sampled splitters where a key byte splits poorly, or always one key byte),
+ * 1 + trials runs each, and leaves the fastest setting in force for later
+ * calls.  out: the chosen setting (dp_filter_min: the value in force, not
+ * searched), its time (minimum over trials) and the default setting's
+ * time. */
 typedef struct {
     int64_t sort_small_max, sort_pivot, dp_filter_min;
     double best_ms, default_ms;
     uint32_t settings_tried;
+    int64_t sort_split_min;
 } dsss_tuning;
 int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* part_begin,
                   const dsss_opts* opts, uint32_t trials, dsss_tuning* out, dsss_stream_t stream);

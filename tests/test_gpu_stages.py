@@ -115,10 +115,11 @@ def string_runs_equal(strs_got, strs_ref, labels_got, labels_ref):
         k = e
 
 
-@pytest.mark.parametrize("by_sort", [1, 0])
+@pytest.mark.parametrize("by_sort", [1, 0, 2])
 def test_lcp_merge_golden(dsss, ctx, by_sort):
     """merge_ref.json: the reference's LcpStringLoserTree_ on receive containers
-    (runs merged by one segmented sort, or by merge-path rounds)."""
+    (runs merged by one segmented sort, by merge-path rounds, or all at once
+    by co-ranked tiles)."""
     with open(os.path.join(GOLDEN, "merge_ref.json")) as f:
         gold = json.load(f)
     with dsss.tuned(merge_by_sort=by_sort):
@@ -162,7 +163,7 @@ def _merge_golden(dsss, ctx, gold):
             assert u64(out["merged_lcp"]).tolist() == pe["merged_lcp"], name
 
 
-@pytest.mark.parametrize("by_sort", [1, 0])
+@pytest.mark.parametrize("by_sort", [1, 0, 2])
 @pytest.mark.parametrize("p", [2, 3, 4, 8, 16])
 def test_staged_pipeline_matches_oracle(dsss, orc, ctx, p, by_sort):
     """The reference's stage order on the GPU: local sort, DP rounds, partition,
@@ -207,7 +208,42 @@ def test_lcp_merge_modes_identical(dsss, ctx):
     iv = dsss.partition(ctx, ds, order, dp, p)
     g = dsss.bucket_scatter(ctx, ds, p, order, lcp, dp, iv)
     outs = []
-    for m in (1, 0):
+    for m in (1, 0, 2):
+        with dsss.tuned(merge_by_sort=m):
+            outs.append(dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
+                                       char_start=g["char_start"]))
+    for k in ("order", "merged_lcp", "old_lcp", "perm_index", "perm_pe"):
+        for o in outs[1:]:
+            assert np.array_equal(u64(outs[0][k]), u64(o[k])), k
+
+
+@pytest.mark.parametrize("which", ["dn", "suffix", "equal", "skewed"])
+def test_lcp_merge_kway_many_runs(dsss, ctx, which):
+    """The K-way merge by co-ranked tiles on receive containers of 16 to 64
+    runs each, with tiles that cut runs of byte-identical strings (suffixes,
+    all-equal strings) and runs of very different lengths: the same order,
+    LCPs and labels as the merge by one sort."""
+    if which == "dn":
+        hs, p = dsss.gen_dn(1500000, 60, 30, seed=14), 64
+    elif which == "suffix":
+        hs, p = dsss.gen_suffix_strings(400000, 256, seed=15), 16
+    elif which == "equal":
+        hs, p = dsss.from_bytes_list([b"SAME" * 5] * 300000), 32
+    else:
+        rng = np.random.default_rng(16)
+        hs, p = dsss.from_bytes_list([bytes(rng.integers(65, 70, int(k)).astype(np.uint8))
+                                      for k in rng.integers(0, 12, 200000)]), 24
+    ds = dsss.DeviceStrings(hs)
+    n = hs.n
+    # uneven PEs (an empty one among them when two cuts meet)
+    cuts = np.sort(np.random.default_rng(17).integers(0, n, p - 1))
+    pb = np.concatenate([[0], cuts, [n]]).astype(np.uint64)
+    order, lcp = dsss.local_sort_lcp(ctx, ds, p, part_begin=pb)
+    dp, _ = dsss.dp_prefixes(ctx, ds, order, lcp, p, part_begin=pb)
+    iv = dsss.partition(ctx, ds, order, dp, p, part_begin=pb)
+    g = dsss.bucket_scatter(ctx, ds, p, order, lcp, dp, iv, part_begin=pb)
+    outs = []
+    for m in (1, 2):
         with dsss.tuned(merge_by_sort=m):
             outs.append(dsss.lcp_merge(ctx, g["chars"], g["char_total"], g["lcp"], g["counts"], g["offsets"],
                                        char_start=g["char_start"]))

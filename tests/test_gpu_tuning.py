@@ -88,11 +88,12 @@ def test_autotune_picks_a_grid_setting(dsss, orc, ctx):
     """dsss_autotune leaves one setting of its grid in force; results stay exact."""
     hs = dsss.gen_suffix_strings(80000, 256, seed=8)
     ds = dsss.DeviceStrings(hs)
-    with dsss.tuned(sort_small_max=-1, sort_pivot=-1, dp_filter_min=-1):
+    with dsss.tuned(sort_small_max=-1, sort_pivot=-1, sort_split_min=-1):
         t = dsss.autotune(ctx, ds, 4, trials=1)
         assert t["settings_tried"] == 12
         assert t["sort_small_max"] in (256, 1024, 4096) and t["sort_pivot"] in (0, 1)
-        assert t["dp_filter_min"] in (0, 1 << 40)
+        assert t["sort_split_min"] in (0, 65536)
+        assert dsss.tune_get("sort_split_min") == t["sort_split_min"]
         assert 0 < t["best_ms"] <= t["default_ms"]
         assert dsss.tune_get("sort_small_max") == t["sort_small_max"]
         out = dsss.pd_sort(ctx, ds, 4)
@@ -249,3 +250,47 @@ def test_root_digests_checked(dsss, orc, ctx, fam):
     with dsss.tuned(dp_check=1, dp_digest=64):
         out = dsss.pd_sort(ctx, dsss.gen_dn_device(ctx, 60000, 200, 50, seed=5), 4)
     assert (out["dp"][:60000] == 72).all()
+
+
+def _split_inputs():
+    """String families for the sampled-splitter passes, 60-80k strings each."""
+    rng = np.random.default_rng(21)
+    letters = [bytes(rng.integers(65, 91, int(k)).astype(np.uint8)) for k in rng.integers(0, 40, 80000)]
+    dna = [bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), int(k))) for k in rng.integers(1, 60, 80000)]
+    # keys of all-0xFF bytes (the splitter table's padding value) next to 0xFE ones
+    ff = [bytes([255]) * int(k) + bytes(rng.integers(254, 256, int(j)).astype(np.uint8))
+          for k, j in zip(rng.integers(0, 20, 60000), rng.integers(0, 12, 60000))]
+    base = [bytes(rng.integers(97, 100, 12).astype(np.uint8)) for _ in range(5)]
+    frequent = [base[int(rng.integers(0, 5))] if rng.random() < 0.9 else
+                bytes(rng.integers(97, 123, int(rng.integers(1, 16))).astype(np.uint8)) for _ in range(70000)]
+    prefixes = [b"P" * int(k) for k in rng.integers(0, 600, 70000)]
+    anybyte = [bytes(rng.integers(1, 256, int(k)).astype(np.uint8)) for k in rng.integers(0, 24, 70000)]
+    return [("letters", letters), ("dna", dna), ("ff", ff), ("frequent", frequent), ("prefixes", prefixes),
+            ("anybyte", anybyte)]
+
+
+@pytest.mark.parametrize("small", [0, 64])
+@pytest.mark.parametrize("split_min", [0, 4096])
+@pytest.mark.parametrize("name,strs", _split_inputs(), ids=[c[0] for c in _split_inputs()])
+def test_sort_split(dsss, orc, ctx, name, strs, split_min, small):
+    """Large segments split by sampled splitters (sort_split_min 4096: every
+    segment from 4096 strings whose next key byte takes few values) or by key
+    bytes only (0): the oracle's order and LCPs, in one segment and in three."""
+    hs = host_of(dsss, strs)
+    n = hs.n
+    for p in (1, 3):
+        pb = np.linspace(0, n, p + 1).astype(np.uint64)
+        with dsss.tuned(sort_split_min=split_min):
+            order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), p, part_begin=pb, small_sort_max=small)
+        ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
+        assert np.array_equal(u64(order, n), ro)
+        assert np.array_equal(u64(lcp, n), rl)
+
+
+@pytest.mark.parametrize("graph", [0, 1 << 22])
+def test_sort_split_pd(dsss, orc, ctx, graph):
+    """The full path with splitter passes, host-driven and as one graph."""
+    hs = dsss.gen_dn(200000, 60, 30, seed=41)
+    with dsss.tuned(sort_split_min=4096, sort_graph_max_n=graph):
+        out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 4)
+    check_pd(dsss, orc, hs, out, 4)
