@@ -65,12 +65,8 @@ CONFIGS = {
 # DRAM bytes (read + write) per unit of the kernels that carry a roofline,
 # from one ncu capture each on 8e6 strings x 200 B (D/N 0.25, p = 64); the
 # traffic of a launch grows with its units.  None: not captured.
-DRAM_PER_UNIT = {
-    "k_prefix": None,
-    "k_dp_part": None,
-    "k_dp_bucket_dups": None,
-    "k_dp_lens": None,
-}
+DRAM_PER_UNIT = {k: None for k in ("k_prefix", "k_pp_hist1", "k_pp_scatter1", "k_pp_hist2", "k_pp_scatter2",
+                                     "k_dp_bucket_dups", "k_dp_lens")}
 
 
 def read_peaks():
@@ -435,8 +431,16 @@ def run_dist(args, cfg):
                 t0 = time.perf_counter()
                 D.sort(comm, be, ds, pb, fused=False, phases=ph2)
                 torch.cuda.synchronize()
-                staged[f"merge_by_sort={mode}"] = {"ms_per_call": (time.perf_counter() - t0) * 1e3,
-                                                   "phases_ms": {k: round(v, 3) for k, v in ph2.items()}}
+                wall = (time.perf_counter() - t0) * 1e3
+                ctx.set_timing(True)
+                D.sort(comm, be, ds, pb, fused=False)
+                torch.cuda.synchronize()
+                kt2 = ctx.kernel_times()
+                ctx.set_timing(False)
+                top = sorted(((k2, v[1]) for k2, v in kt2.items() if not k2.startswith("stage:")), key=lambda x: -x[1])
+                staged[f"merge_by_sort={mode}"] = {"ms_per_call": wall,
+                                                   "phases_ms": {k: round(v, 3) for k, v in ph2.items()},
+                                                   "kernels_ms": {k2: round(v, 3) for k2, v in top[:16]}}
     if rank == 0:
         line = {
             "metric": "strings/s", "value": n * world / (ms * 1e-3), "unit": "strings/s", "n_gpus": world,
@@ -583,13 +587,17 @@ def run_path(args, cfg, which):
 #   k_dp_lens  per sorted position the 4-byte id read, the 16-byte handle
 #              gathered and 12 bytes written: 32 per string
 ROOFLINE_BYTES = {
-    "k_prefix": "sum over strings of (min(L + 1, 72) + 60)",
-    "k_dp_part": "20 per string hashed at its final depth",
+    "k_prefix": "sum over strings of (min(L + 1, 72) + 36)",
+    "k_pp_hist1": "8 per string hashed at its final depth",
+    "k_pp_scatter1": "20 per string hashed at its final depth",
+    "k_pp_hist2": "8 per string hashed at its final depth",
+    "k_pp_scatter2": "24 per string hashed at its final depth",
     "k_dp_bucket_dups": "12 per string hashed at its final depth",
     "k_dp_lens": "32 per string",
 }
 SORT_KERNELS = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
-                "k_scatter", "k_seg_sort", "k_warp_segs", "k_spec", "k_pivot", "k_seg_offsets", "scan_")
+                "k_scatter", "k_seg_sort", "k_warp_segs", "k_spec", "k_pivot", "k_seg_offsets", "k_split_sample",
+                "k_lcp_fix", "scan_")
 
 
 def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True):
@@ -603,8 +611,11 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
     sched = np.array([8] + [8 + (16 << j) for j in range(26)], np.uint64)
     hashed = int(np.isin(dp, sched).sum())
     per_step = {
-        "k_prefix": int(np.minimum(L + 1, 72).sum()) + 60 * n,
-        "k_dp_part": 20 * hashed,
+        "k_prefix": int(np.minimum(L + 1, 72).sum()) + 36 * n,
+        "k_pp_hist1": 8 * hashed,
+        "k_pp_scatter1": 20 * hashed,
+        "k_pp_hist2": 8 * hashed,
+        "k_pp_scatter2": 24 * hashed,
         "k_dp_bucket_dups": 12 * hashed,
         "k_dp_lens": 32 * n,
     }
@@ -709,6 +720,8 @@ def main():
                     help="replicas: one independent sort per GPU (the default on one GPU); dist: one sort over "
                          "all GPUs with the exchanges over NCCL (the default on several GPUs); ms / hq: the "
                          "merge-sort path or hQuicksort alone on one GPU")
+    ap.add_argument("--tune", action="append", default=[], metavar="KNOB=VALUE",
+                    help="set a tuning knob (dsss_tune_set) before the run; repeatable")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
@@ -733,6 +746,9 @@ def main():
     import torch
     import __graft_entry__
     d = __graft_entry__.load_package()
+    for kv in args.tune:
+        name, value = kv.split("=", 1)
+        d.tune_set(name, int(value))
     torch.cuda.set_device(local)
     dist = None
     if world > 1:

@@ -73,10 +73,10 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"copy_word", 16, 8, 16},
     {"dp_digest", 4, 0, 64},
     {"dp_check", 0, 0, 1},
-    {"sort_split_min", 65536, 0, 1ll << 32},
+    {"sort_split_min", 0, 0, 1ll << 32},
 };
 static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}, {0}, {16}, {4},
-                                                   {0}, {65536}};
+                                                   {0}, {0}};
 
 int64_t tune(TuneKnob k) { return g_knobs[k].load(std::memory_order_relaxed); }
 

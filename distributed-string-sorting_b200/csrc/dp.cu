@@ -557,23 +557,76 @@ __global__ void __launch_bounds__(PP_NT) k_pp_hist1(uint64_t n, const unsigned l
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Exclusive scan of v over the 256 threads of a block (v of thread t is
+// bucket t's count); returns thread t's start.  Uses ws[8] of shared memory.
+__device__ __forceinline__ uint32_t pp_block_scan256(uint32_t v, uint32_t* ws) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    uint32_t pre = 0;
+    for (int k = 0; k < w; ++k) pre += ws[k];
+    return pre + x - v;
+}
+
+// Pairs of a tile in bucket order in shared memory, so that each bucket's
+// run is written to global memory contiguously.
+constexpr size_t PP_SMEM = (size_t)PP_TILE * (8 + 4);
+
 // Pass 1 scatter: each hashed string's pair to its (bucket, tile) range.
 __global__ void __launch_bounds__(PP_NT) k_pp_scatter1(uint64_t n, const unsigned long long* dig,
                                                       const uint32_t* hmask, uint32_t b1, uint32_t ntiles,
                                                       const uint32_t* off, unsigned long long* oh, uint32_t* os) {
-    __shared__ uint32_t cur[256];
-    cur[threadIdx.x] = off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+    extern __shared__ __align__(16) unsigned char pp_sm[];
+    unsigned long long* sh = (unsigned long long*)pp_sm;
+    uint32_t* ss = (uint32_t*)(sh + PP_TILE);
+    __shared__ uint32_t cnt[256], beg[256], cur[256], gbase[256], ws[8];
+    cnt[threadIdx.x] = 0;
+    gbase[threadIdx.x] = off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
     __syncthreads();
     const uint64_t t0 = (uint64_t)blockIdx.x * PP_TILE;
-#pragma unroll 4
+    unsigned long long h[PP_IPT];
+    uint32_t bk[PP_IPT];
+#pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
         const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
+        bk[j] = 256;
+        h[j] = 0;
         if (s < n && bit_of(hmask, s)) {
-            const unsigned long long h = dig[s];
-            const uint32_t at = atomicAdd(&cur[(uint32_t)(h >> (64 - b1))], 1u);
-            oh[at] = h;
-            os[at] = (uint32_t)s;
+            h[j] = dig[s];
+            bk[j] = (uint32_t)(h[j] >> (64 - b1));
         }
+    }
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j)
+        if (bk[j] < 256) atomicAdd(&cnt[bk[j]], 1u);
+    __syncthreads();
+    const uint32_t c = cnt[threadIdx.x];
+    const uint32_t e = pp_block_scan256(c, ws);
+    beg[threadIdx.x] = e;
+    cur[threadIdx.x] = e;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j) {
+        if (bk[j] < 256) {
+            const uint32_t lp = atomicAdd(&cur[bk[j]], 1u);
+            sh[lp] = h[j];
+            ss[lp] = (uint32_t)(t0 + (uint64_t)j * PP_NT + threadIdx.x);
+        }
+    }
+    __syncthreads();
+    const uint32_t total = beg[255] + cnt[255];
+    for (uint32_t x = threadIdx.x; x < total; x += PP_NT) {
+        const unsigned long long hv = sh[x];
+        const uint32_t b = (uint32_t)(hv >> (64 - b1));
+        const uint32_t dst = gbase[b] + (x - beg[b]);
+        oh[dst] = hv;
+        os[dst] = ss[x];
     }
 }
 
@@ -639,19 +692,55 @@ __global__ void __launch_bounds__(PP_NT) k_pp_hist2(const unsigned long long* h1
 __global__ void __launch_bounds__(PP_NT) k_pp_scatter2(const unsigned long long* h1, const uint32_t* s1,
                                                       const uint32_t* mid, uint32_t b1, uint32_t b2,
                                                       const uint32_t* off, unsigned long long* oh, uint32_t* os) {
-    __shared__ uint32_t cur[256];
+    extern __shared__ __align__(16) unsigned char pp_sm[];
+    unsigned long long* sh = (unsigned long long*)pp_sm;
+    uint32_t* ss = (uint32_t*)(sh + PP_TILE);
+    __shared__ uint32_t cnt[256], beg[256], cur[256], gbase[256], ws[8];
     const uint32_t t = blockIdx.x;
     if (t >= mid[512 + 256]) return;
     const uint32_t c = pp_coarse_of(mid + 512, t);
     const uint32_t lt = t - mid[512 + c], nt = mid[512 + c + 1] - mid[512 + c];
     const uint32_t b = mid[c] + lt * PP_TILE, e = mid[c] + min(mid[256 + c], (lt + 1) * PP_TILE);
-    if (threadIdx.x < (1u << b2)) cur[threadIdx.x] = off[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt];
+    cnt[threadIdx.x] = 0;
+    gbase[threadIdx.x] = threadIdx.x < (1u << b2) ? off[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt] : 0u;
     __syncthreads();
-    for (uint32_t i = b + threadIdx.x; i < e; i += PP_NT) {
-        const unsigned long long h = h1[i];
-        const uint32_t at = atomicAdd(&cur[(uint32_t)((h << b1) >> (64 - b2))], 1u);
-        oh[at] = h;
-        os[at] = s1[i];
+    unsigned long long h[PP_IPT];
+    uint32_t bk[PP_IPT];
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j) {
+        const uint32_t i = b + j * PP_NT + threadIdx.x;
+        bk[j] = 256;
+        h[j] = 0;
+        if (i < e) {
+            h[j] = h1[i];
+            bk[j] = (uint32_t)((h[j] << b1) >> (64 - b2));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j)
+        if (bk[j] < 256) atomicAdd(&cnt[bk[j]], 1u);
+    __syncthreads();
+    const uint32_t cv = cnt[threadIdx.x];
+    const uint32_t ex = pp_block_scan256(cv, ws);
+    beg[threadIdx.x] = ex;
+    cur[threadIdx.x] = ex;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j) {
+        if (bk[j] < 256) {
+            const uint32_t lp = atomicAdd(&cur[bk[j]], 1u);
+            sh[lp] = h[j];
+            ss[lp] = s1[b + j * PP_NT + threadIdx.x];
+        }
+    }
+    __syncthreads();
+    const uint32_t total = e - b;
+    for (uint32_t x = threadIdx.x; x < total; x += PP_NT) {
+        const unsigned long long hv = sh[x];
+        const uint32_t f2 = (uint32_t)((hv << b1) >> (64 - b2));
+        const uint32_t dst = gbase[f2] + (x - beg[f2]);
+        oh[dst] = hv;
+        os[dst] = ss[x];
     }
 }
 
@@ -1215,9 +1304,12 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                     DSSS_TRY(exclusive_scan_u32(L.pp_hist, L.pp_off, 256ull * nt1, L.pp_total, L.pp_scan, st));
                     const unsigned long long* ph = L.pp_h1;
                     const uint32_t* ps = L.pp_s1;
+                    static std::atomic<uint64_t> pp1_configured{0}, pp2_configured{0};
+                    DSSS_TRY(set_smem_once(pp1_configured, k_pp_scatter1, (int)PP_SMEM));
+                    DSSS_TRY(set_smem_once(pp2_configured, k_pp_scatter2, (int)PP_SMEM));
                     DSSS_LAUNCH("k_pp_scatter1", st,
-                                k_pp_scatter1<<<nt1, PP_NT, 0, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_off, L.pp_h1,
-                                                                     L.pp_s1));
+                                k_pp_scatter1<<<nt1, PP_NT, PP_SMEM, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_off, L.pp_h1,
+                                                                           L.pp_s1));
                     uint32_t* off2 = nullptr;
                     if (b2) {
                         // pass-2 tiles: at most one partial tile per coarse bucket beyond hashed / PP_TILE
@@ -1232,8 +1324,8 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                                     k_pp_hist2<<<(unsigned)nt2, PP_NT, 0, st>>>(L.pp_h1, L.pp_mid, b1, b2, L.pp_hist));
                         DSSS_TRY(exclusive_scan_u32(L.pp_hist, off2, h2, L.pp_total + 1, L.pp_scan, st));
                         DSSS_LAUNCH("k_pp_scatter2", st,
-                                    k_pp_scatter2<<<(unsigned)nt2, PP_NT, 0, st>>>(L.pp_h1, L.pp_s1, L.pp_mid, b1, b2,
-                                                                                   off2, L.pd_h, L.pd_s));
+                                    k_pp_scatter2<<<(unsigned)nt2, PP_NT, PP_SMEM, st>>>(L.pp_h1, L.pp_s1, L.pp_mid, b1,
+                                                                                         b2, off2, L.pd_h, L.pd_s));
                         ph = L.pd_h;
                         ps = L.pd_s;
                     }

@@ -142,7 +142,7 @@ enum TuneKnob : int {
     TUNE_DP_CHECK,           // 1: the arena-order rounds recompute every stored prefix hash from the string and
                              // fail on a mismatch (a self-check)
     TUNE_SORT_SPLIT_MIN,     // smallest large segment that may split by sampled splitters instead of a key
-                             // byte (0: never; values below 4096 count as 4096)
+                             // byte (0: never, the default; values below 4096 count as 4096)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

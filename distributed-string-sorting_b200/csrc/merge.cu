@@ -448,14 +448,29 @@ __global__ void k_kw_corank(FullView f, const uint32_t* sorted, const uint32_t* 
     const uint32_t c = a - sbase[rq];
     uint32_t s = 0;
     if (c > 0) {
-        // sample c - 1 (position (c - 1) KW_GAP) is before B, sample c (if any) is not
-        uint32_t l2 = (c - 1) * KW_GAP + 1, h2 = min(c * KW_GAP, run_len[rq]);
-        while (l2 < h2) {
+        // sample c - 1 (position (c - 1) KW_GAP) is before B, sample c (if
+        // any) is not; every string between two strings shares with B at
+        // least the smaller of their LCPs with B, so each comparison starts
+        // there (the LCP-aware binary search)
+        const uint32_t rb0 = run_begin[rq], len = run_len[rq];
+        uint32_t l2 = (c - 1) * KW_GAP, h2 = min(c * KW_GAP, len);
+        uint32_t llo, lhi = 0;
+        cmp_from(f, rb0 + l2, B, 0, &llo);
+        if (h2 < len) cmp_from(f, rb0 + h2, B, 0, &lhi);
+        // without an upper string nothing bounds the LCP from below until one is found
+        while (h2 - l2 > 1) {
             const uint32_t m = (l2 + h2) >> 1;
-            if (kw_before(f, run_begin[rq] + m, B)) l2 = m + 1;
-            else h2 = m;
+            uint32_t l;
+            const int cm = cmp_from(f, rb0 + m, B, min(llo, lhi), &l);
+            if (cm < 0 || (cm == 0 && rb0 + m < B)) {
+                l2 = m;
+                llo = l;
+            } else {
+                h2 = m;
+                lhi = l;
+            }
         }
-        s = l2;
+        s = h2;
     }
     split[g] = s;
 }

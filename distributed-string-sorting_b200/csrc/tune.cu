@@ -58,9 +58,9 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const Knobs saved = get_knobs();
-    const Setting grid[] = {{4096, 1, 65536}, {1024, 1, 65536}, {256, 1, 65536}, {4096, 0, 65536},
-                            {1024, 0, 65536}, {256, 0, 65536}, {4096, 1, 0},     {1024, 1, 0},
-                            {256, 1, 0},      {4096, 0, 0},     {1024, 0, 0},     {256, 0, 0}};
+    const Setting grid[] = {{4096, 1, 0},     {1024, 1, 0},     {256, 1, 0},     {4096, 0, 0},
+                            {1024, 0, 0},     {256, 0, 0},      {4096, 1, 65536}, {1024, 1, 65536},
+                            {256, 1, 65536},  {4096, 0, 65536}, {1024, 0, 65536}, {256, 0, 65536}};
     double best = 1e300, first = 0;
     int best_i = -1, rc = DSSS_OK;
     uint32_t tried = 0;

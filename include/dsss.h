@@ -145,8 +145,10 @@ int dsss_abi_version(void);
  *   sort_split_min  smallest segment of the string sort's MSD passes that
  *                   may split by up to 255 splitters sampled from its keys
  *                   instead of by one key byte, where that byte takes few
- *                   values (letters, DNA; default 65536; 0 = never; values
- *                   below 4096 count as 4096)
+ *                   values (letters, DNA; default 0 = never: on B200 the
+ *                   fewer passes cost more in the small-segment sorts, whose
+ *                   buckets then cut across key bytes; values below 4096
+ *                   count as 4096)
  *   dp_check        1: the arena-order rounds at depths 8, 24, 40 and 72,
  *                   which read the prefix hashes the string sort's first pass
  *                   stored, recompute each from the string and fail with
@@ -157,7 +159,7 @@ int dsss_tune_get(const char* name, int64_t* value);
 /* Autotuner (no reference counterpart): runs the full path (as
  * dsss_pd_sort_batched; nsets = 1 for one set) on the given device input
  * under each setting of a grid of the knobs above (sort_small_max 256 / 1024 /
- * 4096, sort_pivot on / off, sort_split_min 65536 / 0: the MSD digit as
+ * 4096, sort_pivot on / off, sort_split_min 0 / 65536: the MSD digit as
  * sampled splitters where a key byte splits poorly, or always one key byte),
  * 1 + trials runs each, and leaves the fastest setting in force for later
  * calls.  out: the chosen setting (dp_filter_min: the value in force, not
