@@ -44,32 +44,62 @@ static uint32_t factor_of(const dsss_opts* o) { return (o && o->sampling_factor)
 static uint32_t sampler_of(const dsss_opts* o) { return o ? o->sampler : DSSS_SAMPLER_NUM_STRINGS; }
 static uint32_t smallmax_of(const dsss_opts* o) { return o ? o->small_sort_max : 0; }
 
-__global__ void k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p, uint32_t* pe) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const uint32_t s = ord[g];
-    uint32_t lo = 0, hi = p;  // last q with pb[q] <= s
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (pb[mid] <= s) lo = mid;
-        else hi = mid;
+// PE of every sorted position: the last q with pb[q] <= ord[g], searched in
+// a shared-memory copy of the PE bounds (npe + 1 <= 1025 entries), PE_IPT
+// positions per thread with their ids loaded before the searches.
+constexpr int PE_NT = 256, PE_IPT = 8;
+__global__ void __launch_bounds__(PE_NT) k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p,
+                                                 uint32_t* pe) {
+    extern __shared__ unsigned long long spb[];
+    for (uint32_t q = threadIdx.x; q <= p; q += PE_NT) spb[q] = pb[q];
+    const uint64_t g0 = (uint64_t)blockIdx.x * (PE_NT * PE_IPT) + threadIdx.x;
+    uint32_t s[PE_IPT];
+#pragma unroll
+    for (int j = 0; j < PE_IPT; ++j) {
+        const uint64_t g = g0 + (uint64_t)j * PE_NT;
+        s[j] = g < n ? ord[g] : 0u;
     }
-    pe[g] = lo;
+    __syncthreads();
+    // the last q < p with pb[q] <= s: the same fixed steps for every
+    // position, the PE_IPT searches interleaved
+    uint32_t lo[PE_IPT];
+#pragma unroll
+    for (int j = 0; j < PE_IPT; ++j) lo[j] = 0;
+    for (uint32_t step = 1u << (31 - __clz(p | 1u)); step; step >>= 1) {
+#pragma unroll
+        for (int j = 0; j < PE_IPT; ++j) {
+            const uint32_t m = lo[j] + step;
+            if (m < p && spb[m] <= s[j]) lo[j] = m;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PE_IPT; ++j) {
+        const uint64_t g = g0 + (uint64_t)j * PE_NT;
+        if (g < n) pe[g] = lo[j];
+    }
+}
+
+static int launch_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p, uint32_t* pe,
+                        cudaStream_t st) {
+    const uint64_t per = (uint64_t)PE_NT * PE_IPT;
+    DSSS_LAUNCH("k_pe_of", st,
+                k_pe_of<<<(unsigned)((n + per - 1) / per), PE_NT, (p + 1) * sizeof(unsigned long long), st>>>(
+                    ord, n, pb, p, pe));
+    return DSSS_OK;
 }
 
 // Receiving PE of every string: set s's PE q sends local positions
 // [bounds[(s*p+q)*(p+1) + r], … + r + 1) to the set's PE r; buckets are
-// numbered s*p + r; src receives q's global PE number.
-__device__ __forceinline__ uint32_t bucket_at(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds,
-                                              uint32_t p, uint64_t g, uint32_t& src) {
-    src = pe[g];
-    const uint64_t* b = bounds + (uint64_t)src * (p + 1);
-    const uint64_t li = g2l[g];
-    uint32_t lo = 0, hi = p;  // last r with b[r] <= li
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (b[mid] <= li) lo = mid;
-        else hi = mid;
+// numbered s*p + r.  src is q's global PE number, li the string's index in
+// q's local order; B is the bound table (u64 in global memory, or a u32 copy
+// in shared memory).
+template <typename B>
+__device__ __forceinline__ uint32_t bucket_of(const B* bounds, uint32_t p, uint32_t src, uint32_t li) {
+    const B* b = bounds + (uint64_t)src * (p + 1);
+    uint32_t lo = 0;  // the last r < p with b[r] <= li (b[0] = 0), in fixed steps
+    for (uint32_t step = 1u << (31 - __clz(p | 1u)); step; step >>= 1) {
+        const uint32_t m = lo + step;
+        if (m < p && b[m] <= li) lo = m;
     }
     return (src / p) * p + lo;
 }
@@ -80,28 +110,97 @@ __device__ __forceinline__ uint32_t bucket_at(const uint32_t* pe, const uint32_t
 // is the identity, so position g of the merged sequences is global position g:
 // its (local index, sender PE) and, unless it starts a receiving PE's run, the
 // global LCP.  *viol is set when some bucket decreases; the caller then runs
-// the multisplit, which rewrites every output.
-__global__ void k_bucket_direct(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p,
-                                uint64_t n, int local_pe, const uint32_t* lcpg, uint32_t* bucket, uint32_t* pe_local,
-                                uint32_t* perm_index, uint32_t* perm_pe, uint32_t* merged, uint32_t* viol) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = g < n;
-    uint32_t src = 0, b = 0xFFFFFFFFu;
-    if (valid) b = bucket_at(pe, g2l, bounds, p, g, src);
-    // the previous position's bucket: from the lane below, or searched by lane 0
-    uint32_t bp = __shfl_up_sync(0xffffffffu, b, 1);
-    if ((threadIdx.x & 31) == 0) {
-        uint32_t srcp;
-        bp = valid && g ? bucket_at(pe, g2l, bounds, p, g - 1, srcp) : 0xFFFFFFFFu;
+// the multisplit, which rewrites every output (bucket, when given, receives
+// every position's bucket for it).  BD_IPT positions per thread, their inputs
+// loaded before the searches; with SMEM the bound table is searched in a u32
+// copy in shared memory; each position's predecessor bucket comes from the
+// tile's bucket row in shared memory.
+constexpr int BD_NT = 256, BD_IPT = 8, BD_TILE = BD_NT * BD_IPT;
+constexpr uint32_t BD_SMEM_BOUNDS = 8192;  // bound entries kept in shared memory (32 KiB)
+template <bool SMEM>
+__global__ void __launch_bounds__(BD_NT, 4) k_bucket_direct(const uint32_t* pe, const uint32_t* g2l,
+                                                         const uint64_t* bounds, uint32_t p, uint32_t npe, uint64_t n,
+                                                         int local_pe, const uint32_t* lcpg, uint32_t* bucket,
+                                                         uint32_t* pe_local, uint32_t* perm_index, uint32_t* perm_pe,
+                                                         uint32_t* merged, uint32_t* viol) {
+    extern __shared__ uint32_t sbd[];
+    uint32_t* sb = sbd;                  // the tile's buckets, after the one of the position before it
+    uint32_t* tab = sbd + BD_TILE + 1;   // SMEM: npe * (p + 1) bounds
+    const uint64_t t0 = (uint64_t)blockIdx.x * BD_TILE;
+    if (SMEM)
+        for (uint32_t k = threadIdx.x; k < npe * (p + 1); k += BD_NT) tab[k] = (uint32_t)bounds[k];
+    uint32_t src[BD_IPT], li[BD_IPT], lc[BD_IPT];
+#pragma unroll
+    for (int j = 0; j < BD_IPT; ++j) {
+        const uint64_t g = t0 + (uint64_t)j * BD_NT + threadIdx.x;
+        const bool v = g < n;
+        src[j] = v ? pe[g] : 0u;
+        li[j] = v ? g2l[g] : 0u;
+        lc[j] = v && merged ? lcpg[g] : 0u;
     }
-    if (!valid) return;
-    if (g && bp > b) atomicExch(viol, 1u);
-    const uint32_t ql = src - (src / p) * p;
-    bucket[g] = b;
-    if (pe_local) pe_local[g] = ql;
-    perm_index[g] = g2l[g];
-    perm_pe[g] = local_pe ? ql : src;
-    if (merged) merged[g] = (g == 0 || bp != b) ? 0u : lcpg[g];
+    __syncthreads();
+    // the BD_IPT searches interleaved, in the fixed steps of bucket_of
+    uint32_t bk[BD_IPT];
+#pragma unroll
+    for (int j = 0; j < BD_IPT; ++j) bk[j] = 0;
+    for (uint32_t step = 1u << (31 - __clz(p | 1u)); step; step >>= 1) {
+#pragma unroll
+        for (int j = 0; j < BD_IPT; ++j) {
+            const uint32_t m = bk[j] + step;
+            const uint64_t at = (uint64_t)src[j] * (p + 1) + m;
+            if (m < p && (SMEM ? (uint64_t)tab[at] : bounds[at]) <= li[j]) bk[j] = m;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < BD_IPT; ++j) {
+        bk[j] += (src[j] / p) * p;
+        sb[1 + j * BD_NT + threadIdx.x] = bk[j];
+    }
+    if (threadIdx.x == 0) {
+        uint32_t b = 0xFFFFFFFFu;
+        if (t0 && t0 <= n) {
+            const uint32_t s0 = pe[t0 - 1], l0 = g2l[t0 - 1];
+            b = SMEM ? bucket_of(tab, p, s0, l0) : bucket_of(bounds, p, s0, l0);
+        }
+        sb[0] = b;
+    }
+    __syncthreads();
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < BD_IPT; ++j) {
+        const uint64_t g = t0 + (uint64_t)j * BD_NT + threadIdx.x;
+        if (g >= n) continue;
+        const uint32_t b = bk[j], bp = sb[j * BD_NT + threadIdx.x];
+        if (g && bp > b) bad = true;
+        const uint32_t ql = src[j] - (src[j] / p) * p;
+        if (bucket) bucket[g] = b;
+        if (pe_local) pe_local[g] = ql;
+        perm_index[g] = li[j];
+        perm_pe[g] = local_pe ? ql : src[j];
+        if (merged) merged[g] = (g == 0 || bp != b) ? 0u : lc[j];
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(viol, 1u);
+}
+
+static int launch_bucket_direct(const uint32_t* pe, const uint32_t* g2l, const uint64_t* bounds, uint32_t p,
+                                uint32_t npe, uint64_t n, int local_pe, const uint32_t* lcpg, uint32_t* bucket,
+                                uint32_t* pe_local, uint32_t* perm_index, uint32_t* perm_pe, uint32_t* merged,
+                                uint32_t* viol, cudaStream_t st) {
+    const unsigned grid = (unsigned)((n + BD_TILE - 1) / BD_TILE);
+    const uint64_t entries = (uint64_t)npe * (p + 1);
+    if (entries <= BD_SMEM_BOUNDS) {
+        const size_t sm = (BD_TILE + 1 + entries) * sizeof(uint32_t);
+        DSSS_LAUNCH("k_bucket_direct", st,
+                    k_bucket_direct<true><<<grid, BD_NT, sm, st>>>(pe, g2l, bounds, p, npe, n, local_pe, lcpg, bucket,
+                                                                   pe_local, perm_index, perm_pe, merged, viol));
+    } else {
+        const size_t sm = (BD_TILE + 1) * sizeof(uint32_t);
+        DSSS_LAUNCH("k_bucket_direct", st,
+                    k_bucket_direct<false><<<grid, BD_NT, sm, st>>>(pe, g2l, bounds, p, npe, n, local_pe, lcpg,
+                                                                    bucket, pe_local, perm_index, perm_pe, merged,
+                                                                    viol));
+    }
+    return DSSS_OK;
 }
 
 __global__ void k_merged_lcp(const uint32_t* out2g, const uint32_t* lcpg, const uint64_t* recv_begin, uint32_t p,
@@ -238,7 +337,7 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     // 3. local orders per PE
     StageTimer t_local("stage:local", st);
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (npe + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, npe, L.pe));
+    DSSS_TRY(launch_pe_of(L.ord, n, L.pb, npe, L.pe, st));
     {
         // local order and DP per PE: out[dest] = (string id, dp); g2l = rank inside the PE
         const uint32_t* in[2] = {L.ord, L.dpg};
@@ -272,14 +371,15 @@ int pd_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, cons
     DSSS_CUDA(cudaMemcpyAsync(L.bounds, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (npe + 1) * 8, cudaMemcpyHostToDevice, st));
     DSSS_CUDA(cudaMemsetAsync(L.viol, 0, sizeof(uint32_t), st));
-    DSSS_LAUNCH("k_bucket_direct", st,
-                k_bucket_direct<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, nsets > 1, L.lcp, L.tmp,
-                                                                 L.pel, out->perm_index, out->perm_pe,
-                                                                 out->merged_lcp, L.viol));
+    DSSS_TRY(launch_bucket_direct(L.pe, L.g2l, L.bounds, p, npe, n, nsets > 1, L.lcp, nullptr, L.pel,
+                                  out->perm_index, out->perm_pe, out->merged_lcp, L.viol, st));
     pin = (uint32_t*)ctx->pin;  // the partition step may have grown the staging buffer
     DSSS_CUDA(cudaMemcpyAsync(pin, L.viol, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
     if (pin[0]) {
+        // every position's bucket for the multisplit (the outputs are rewritten by it)
+        DSSS_TRY(launch_bucket_direct(L.pe, L.g2l, L.bounds, p, npe, n, nsets > 1, L.lcp, L.tmp, L.pel,
+                                      out->perm_index, out->perm_pe, nullptr, L.viol, st));
         // merged sequences: (index in sender's local order, sender PE, global position)
         const uint32_t* in[3] = {L.g2l, nsets > 1 ? L.pel : L.pe, nullptr};
         uint32_t* outs[3] = {out->perm_index, out->perm_pe, L.out2g};
@@ -422,7 +522,7 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
     // local orders per PE and their LCP arrays (0 at each PE start)
     StageTimer t_local("stage:local", st);
     DSSS_CUDA(cudaMemcpyAsync(L.pb, pb, (p + 1) * 8, cudaMemcpyHostToDevice, st));
-    DSSS_LAUNCH("k_pe_of", st, k_pe_of<<<grid_for(n, 256), 256, 0, st>>>(L.ord, n, L.pb, p, L.pe));
+    DSSS_TRY(launch_pe_of(L.ord, n, L.pb, p, L.pe, st));
     {
         const uint32_t* ins[1] = {L.ord};
         uint32_t* outs[1] = {out->local_order};
@@ -474,13 +574,14 @@ static int ms_sort_dev(Ctx* ctx, const dsss_arena* in, uint32_t p, const uint64_
         DSSS_CUDA(cudaMemcpyAsync(L.recv_begin, recv.data(), (p + 1) * 8, cudaMemcpyHostToDevice, st));
         // (local index, sender PE) of every output position: perm_index in L.dpg, perm_pe in len1
         DSSS_CUDA(cudaMemsetAsync(L.viol, 0, sizeof(uint32_t), st));
-        DSSS_LAUNCH("k_bucket_direct", st,
-                    k_bucket_direct<<<grid_for(n, 256), 256, 0, st>>>(L.pe, L.g2l, L.bounds, p, n, 0, L.lcp, L.tmp,
-                                                                     nullptr, L.dpg, len1, out->lcp, L.viol));
+        DSSS_TRY(launch_bucket_direct(L.pe, L.g2l, L.bounds, p, p, n, 0, L.lcp, nullptr, nullptr, L.dpg, len1,
+                                      out->lcp, L.viol, st));
         pin = (uint32_t*)ctx->pin;
         DSSS_CUDA(cudaMemcpyAsync(pin, L.viol, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
         if (pin[0]) {
+            DSSS_TRY(launch_bucket_direct(L.pe, L.g2l, L.bounds, p, p, n, 0, L.lcp, L.tmp, nullptr, L.dpg, len1,
+                                          nullptr, L.viol, st));
             const uint32_t* ins[3] = {L.g2l, L.pe, nullptr};
             uint32_t* outs[3] = {L.dpg, len1, L.out2g};
             DSSS_TRY(multisplit_payload(L.tmp, n, p, 3, ins, outs, nullptr, L.err, L.ms, st));

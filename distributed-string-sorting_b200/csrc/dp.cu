@@ -76,8 +76,18 @@ __global__ void __launch_bounds__(256) k_min_len(const uint32_t* len, const ulon
                                                  uint32_t* out) {
     uint32_t m = 0xFFFFFFFFu;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        m = min(m, h ? (uint32_t)h[i].y : len[i]);
+    const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (len) {  // the 4-byte lengths, four loads in flight per thread
+        for (uint64_t i = i0; i < n; i += 4 * stride) {
+            uint32_t v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] = i + q * stride < n ? len[i + q * stride] : 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) m = min(m, v[q]);
+        }
+    } else {
+        for (uint64_t i = i0; i < n; i += stride) m = min(m, (uint32_t)h[i].y);
+    }
 #pragma unroll
     for (int o = 16; o; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0 && m != 0xFFFFFFFFu) atomicMin(out, m);
@@ -136,7 +146,9 @@ __device__ __forceinline__ void mark_string(uint32_t* m, uint32_t s) { atomicOr(
 
 // Grid-stride over positions (grid a few blocks per SM): one pair of counter
 // atomics per block instead of per 256 positions.  hmask (with order): every
-// hashed string is marked for the arena-order form of the round.  lens (the
+// hashed string is marked for the arena-order form of the round (an atomic
+// OR into a bitmap of n bits, which stays in L2; random byte stores into a
+// byte per string measured slower).  lens (the
 // lengths in sorted order) may be null when every string reaches depth.
 __global__ void __launch_bounds__(256) k_dp_classify(const uint8_t* st, int all, const uint32_t* lens,
                                                      const uint32_t* lcp, uint64_t n, uint32_t depth, uint32_t* dp,
@@ -548,10 +560,16 @@ __global__ void __launch_bounds__(PP_NT) k_pp_hist1(uint64_t n, const unsigned l
     h[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t t0 = (uint64_t)blockIdx.x * PP_TILE;
+    // the mask words and the hashes loaded together (every position has a
+    // hash slot; only marked ones count)
 #pragma unroll 4
     for (int j = 0; j < PP_IPT; ++j) {
         const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
-        if (s < n && bit_of(hmask, s)) atomicAdd(&h[(uint32_t)(dig[s] >> (64 - b1))], 1u);
+        if (s < n) {
+            const uint32_t mw = hmask[s >> 5];
+            const unsigned long long hv = dig[s];
+            if ((mw >> (s & 31)) & 1u) atomicAdd(&h[(uint32_t)(hv >> (64 - b1))], 1u);
+        }
     }
     __syncthreads();
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
@@ -579,7 +597,7 @@ __device__ __forceinline__ uint32_t pp_block_scan256(uint32_t v, uint32_t* ws) {
 constexpr size_t PP_SMEM = (size_t)PP_TILE * (8 + 4);
 
 // Pass 1 scatter: each hashed string's pair to its (bucket, tile) range.
-__global__ void __launch_bounds__(PP_NT) k_pp_scatter1(uint64_t n, const unsigned long long* dig,
+__global__ void __launch_bounds__(PP_NT, 4) k_pp_scatter1(uint64_t n, const unsigned long long* dig,
                                                       const uint32_t* hmask, uint32_t b1, uint32_t ntiles,
                                                       const uint32_t* off, unsigned long long* oh, uint32_t* os) {
     extern __shared__ __align__(16) unsigned char pp_sm[];
@@ -590,21 +608,25 @@ __global__ void __launch_bounds__(PP_NT) k_pp_scatter1(uint64_t n, const unsigne
     gbase[threadIdx.x] = off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
     __syncthreads();
     const uint64_t t0 = (uint64_t)blockIdx.x * PP_TILE;
+    // mask words and hashes loaded together, before any is used; a bit of
+    // `marked` per position, the bucket recomputed from the hash
     unsigned long long h[PP_IPT];
-    uint32_t bk[PP_IPT];
+    uint32_t mw[PP_IPT];
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
         const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
-        bk[j] = 256;
-        h[j] = 0;
-        if (s < n && bit_of(hmask, s)) {
-            h[j] = dig[s];
-            bk[j] = (uint32_t)(h[j] >> (64 - b1));
+        mw[j] = s < n ? hmask[s >> 5] : 0u;
+        h[j] = s < n ? dig[s] : 0ull;
+    }
+    uint32_t marked = 0;
+#pragma unroll
+    for (int j = 0; j < PP_IPT; ++j) {
+        const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
+        if ((mw[j] >> (s & 31)) & 1u) {
+            marked |= 1u << j;
+            atomicAdd(&cnt[(uint32_t)(h[j] >> (64 - b1))], 1u);
         }
     }
-#pragma unroll
-    for (int j = 0; j < PP_IPT; ++j)
-        if (bk[j] < 256) atomicAdd(&cnt[bk[j]], 1u);
     __syncthreads();
     const uint32_t c = cnt[threadIdx.x];
     const uint32_t e = pp_block_scan256(c, ws);
@@ -613,8 +635,8 @@ __global__ void __launch_bounds__(PP_NT) k_pp_scatter1(uint64_t n, const unsigne
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
-        if (bk[j] < 256) {
-            const uint32_t lp = atomicAdd(&cur[bk[j]], 1u);
+        if ((marked >> j) & 1u) {
+            const uint32_t lp = atomicAdd(&cur[(uint32_t)(h[j] >> (64 - b1))], 1u);
             sh[lp] = h[j];
             ss[lp] = (uint32_t)(t0 + (uint64_t)j * PP_NT + threadIdx.x);
         }
@@ -689,7 +711,7 @@ __global__ void __launch_bounds__(PP_NT) k_pp_hist2(const unsigned long long* h1
     if (threadIdx.x < (1u << b2)) hist[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt] = h[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(PP_NT) k_pp_scatter2(const unsigned long long* h1, const uint32_t* s1,
+__global__ void __launch_bounds__(PP_NT, 4) k_pp_scatter2(const unsigned long long* h1, const uint32_t* s1,
                                                       const uint32_t* mid, uint32_t b1, uint32_t b2,
                                                       const uint32_t* off, unsigned long long* oh, uint32_t* os) {
     extern __shared__ __align__(16) unsigned char pp_sm[];
@@ -704,21 +726,19 @@ __global__ void __launch_bounds__(PP_NT) k_pp_scatter2(const unsigned long long*
     cnt[threadIdx.x] = 0;
     gbase[threadIdx.x] = threadIdx.x < (1u << b2) ? off[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt] : 0u;
     __syncthreads();
+    // hashes and strings loaded together, before any is used; the fine
+    // bucket recomputed from the hash
     unsigned long long h[PP_IPT];
-    uint32_t bk[PP_IPT];
+    uint32_t sv[PP_IPT];
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
         const uint32_t i = b + j * PP_NT + threadIdx.x;
-        bk[j] = 256;
-        h[j] = 0;
-        if (i < e) {
-            h[j] = h1[i];
-            bk[j] = (uint32_t)((h[j] << b1) >> (64 - b2));
-        }
+        h[j] = i < e ? h1[i] : 0ull;
+        sv[j] = i < e ? s1[i] : 0u;
     }
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j)
-        if (bk[j] < 256) atomicAdd(&cnt[bk[j]], 1u);
+        if (b + j * PP_NT + threadIdx.x < e) atomicAdd(&cnt[(uint32_t)((h[j] << b1) >> (64 - b2))], 1u);
     __syncthreads();
     const uint32_t cv = cnt[threadIdx.x];
     const uint32_t ex = pp_block_scan256(cv, ws);
@@ -727,10 +747,10 @@ __global__ void __launch_bounds__(PP_NT) k_pp_scatter2(const unsigned long long*
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
-        if (bk[j] < 256) {
-            const uint32_t lp = atomicAdd(&cur[bk[j]], 1u);
+        if (b + j * PP_NT + threadIdx.x < e) {
+            const uint32_t lp = atomicAdd(&cur[(uint32_t)((h[j] << b1) >> (64 - b2))], 1u);
             sh[lp] = h[j];
-            ss[lp] = s1[b + j * PP_NT + threadIdx.x];
+            ss[lp] = sv[j];
         }
     }
     __syncthreads();

@@ -53,6 +53,10 @@ struct Seg {
     uint32_t nspl;
     unsigned long long spec_diff;
     uint32_t spl_slot, fix0;
+    // OR and AND of the keys the previous pass's scatter wrote for this
+    // segment (children with keys, when the child table is kept): the bits
+    // that differ among its keys are kor ^ kand
+    unsigned long long kor, kand;
 };
 
 // Sampled splitters.  Where the key byte at a large segment's first
@@ -81,7 +85,8 @@ __device__ __forceinline__ int bin_of(uint32_t size) {
 
 // Counters block (device): [0] n_large_next, [1..4] n_small per bin, [5]
 // fix-list slots reserved, [6] splitter tables of the pass, [8] total tiles,
-// [9] total chunks, [10] error flag (a guard tripped).
+// [9] total chunks, [10] error flag (a guard tripped), [11] large segments of
+// the next pass without keys or with a pivot pass.
 struct SortState {
     ArenaDev a;
     uint32_t* ord[2];
@@ -97,6 +102,11 @@ struct SortState {
     uint32_t* chunk_pre;
     uint32_t* bucket;  // 257 per large segment
     uint32_t* counters;
+    // child table (optional, 256 per large segment): the next list's slot of
+    // digit d's child when it is large and keeps the keys (~0u otherwise); the
+    // scatter then folds the keys it writes into that child's kor / kand
+    uint32_t* child;
+    Seg* nxt;  // the next pass's list (the scatter's children)
     uint32_t small_max;
     uint32_t pivot;  // pivot passes enabled
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
@@ -146,16 +156,20 @@ __device__ __forceinline__ void push_small(const SortState& S, uint32_t start, u
     s.spl_slot = 0;
     s.fix0 = 0;
     s.spec_diff = 0;
+    s.kor = 0;
+    s.kand = ~0ull;
     S.small[b][slot] = s;
 }
 
-__device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_t start, uint32_t size,
-                                           uint32_t depth, uint32_t flags) {
+// Returns the segment's slot in dst (~0u when the list is full).
+__device__ __forceinline__ uint32_t push_large(const SortState& S, Seg* dst, uint32_t start, uint32_t size,
+                                               uint32_t depth, uint32_t flags) {
     uint32_t slot = atomicAdd(&S.counters[0], 1u);
     if (slot >= S.cap_large) {
         atomicExch(&S.counters[10], 1u);
-        return;
+        return 0xFFFFFFFFu;
     }
+    if (!(flags & F_KEYS) || (flags & F_PIVOT)) atomicAdd(&S.counters[11], 1u);
     Seg s;
     s.start = start;
     s.size = size;
@@ -169,7 +183,10 @@ __device__ __forceinline__ void push_large(const SortState& S, Seg* dst, uint32_
     s.spl_slot = 0;
     s.fix0 = 0;
     s.spec_diff = 0;
+    s.kor = 0;
+    s.kand = ~0ull;
     dst[slot] = s;
+    return slot;
 }
 
 // ------------------------------------------------------------------ init ----
@@ -896,21 +913,31 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
         sg.first_digit = s_first;
         sg.depth = depth;
     }
+    uint32_t* child = S.child ? S.child + (uint64_t)si * 256 + d : nullptr;
+    if (child) *child = 0xFFFFFFFFu;  // set below for a large child that keeps the keys
     if (total < 2) return;
     const uint32_t cs = sg.start + excl;
     const uint32_t np = par ^ 1u;
     if (sg.nspl) {
         // splitter buckets: children keep the keys at this depth (an
         // equality bucket's keys are all equal: its next pass goes deeper)
-        if (total > S.small_max) push_large(S, next, cs, total, depth, np | F_KEYS);
-        else push_small(S, cs, total, depth, np | F_KEYS);
+        if (total > S.small_max) {
+            const uint32_t slot = push_large(S, next, cs, total, depth, np | F_KEYS);
+            if (child) *child = slot;
+        } else {
+            push_small(S, cs, total, depth, np | F_KEYS);
+        }
     } else if (!pseudo) {
         if (d == 0) return;  // strings that end here: written by the scatter
         // children keep the parent's keys: their first b+1 key bytes are now
         // common; one that keeps most of the parent gets a pivot pass
         if (total > S.small_max) {
-            if (S.pivot && 2 * (uint64_t)total > sg.size) push_large(S, next, cs, total, depth + b + 1, np | F_PIVOT);
-            else push_large(S, next, cs, total, depth, np | F_KEYS);
+            if (S.pivot && 2 * (uint64_t)total > sg.size) {
+                push_large(S, next, cs, total, depth + b + 1, np | F_PIVOT);
+            } else {
+                const uint32_t slot = push_large(S, next, cs, total, depth, np | F_KEYS);
+                if (child) *child = slot;
+            }
         } else {
             push_small(S, cs, total, depth, np | F_KEYS);
         }
@@ -919,7 +946,8 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
         // string is the pivot): large children keep the pseudo keys, small
         // ones restart from the depth their strings share
         if (total > S.small_max) {
-            push_large(S, next, cs, total, depth, np | F_KEYS | F_PSEUDO);
+            const uint32_t slot = push_large(S, next, cs, total, depth, np | F_KEYS | F_PSEUDO);
+            if (child) *child = slot;
         } else {
             uint32_t cd = depth + pivot_l(d);
             if (d == PIVOT_CAP) {
@@ -960,6 +988,8 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     __shared__ uint32_t tloff[256];
     __shared__ uint32_t wcnt[LT_NT / 32][256];
     __shared__ uint32_t wsum[LT_NT / 32];
+    __shared__ uint32_t schild[256];
+    __shared__ uint32_t actm[LT_NT / 32];  // per warp: the digits (d & 7 == warp) whose keys it folds
     __shared__ unsigned long long s_spl[SPL_STRIDE];
     const uint32_t t = blockIdx.x;
     if (t >= S.counters[8]) return;
@@ -985,6 +1015,8 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
         base[d] = bk[d] + S.chunk_pre[(uint64_t)c * 256 + d] + S.tile_hist[(uint64_t)t * 256 + d];
         bstart[d] = bk[d];
         if (d == 0) bstart[256] = bk[256];
+        if (S.child) schild[d] = S.child[(uint64_t)si * 256 + d];
+        if (d < LT_NT / 32) actm[d] = 0;
 #pragma unroll
         for (int w = 0; w < LT_NT / 32; ++w) wcnt[w][d] = 0;
         if (m)
@@ -1043,6 +1075,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
         uint32_t wpre = 0;
         for (int ww = 0; ww < w; ++ww) wpre += wsum[ww];
         tloff[d] = wpre + x - run;
+        if (S.child && run && schild[d] < S.cap_large) atomicOr(&actm[d & 7], 1u << (d >> 3));
     }
     __syncthreads();
 #pragma unroll
@@ -1060,6 +1093,31 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
         sdig[lp] = (uint8_t)dg;
     }
     __syncthreads();
+    if (S.child) {
+        // the OR and AND of the keys each large child that keeps them gets
+        // from this tile (one warp per digit, over the digit's run in shared
+        // memory): its next pass needs no key read to find the byte where its
+        // keys differ
+        for (uint32_t m = actm[w]; m; m &= m - 1) {
+            const uint32_t dg = ((uint32_t)(__ffs(m) - 1) << 3) | (uint32_t)w;
+            const uint32_t r0 = tloff[dg], r1 = dg < 255 ? tloff[dg + 1] : tn;
+            unsigned long long vo = 0, va = ~0ull;
+            for (uint32_t x = r0 + lane; x < r1; x += 32) {
+                const unsigned long long v = skey[x];
+                vo |= v;
+                va &= v;
+            }
+            const uint32_t olo = __reduce_or_sync(0xffffffffu, (uint32_t)vo);
+            const uint32_t ohi = __reduce_or_sync(0xffffffffu, (uint32_t)(vo >> 32));
+            const uint32_t alo = __reduce_and_sync(0xffffffffu, (uint32_t)va);
+            const uint32_t ahi = __reduce_and_sync(0xffffffffu, (uint32_t)(va >> 32));
+            if (lane == 0) {
+                const uint32_t slot = schild[dg];
+                atomicOr(&S.nxt[slot].kor, ((unsigned long long)ohi << 32) | olo);
+                atomicAnd(&S.nxt[slot].kand, ((unsigned long long)ahi << 32) | alo);
+            }
+        }
+    }
     for (uint32_t x = threadIdx.x; x < tn; x += LT_NT) {
         const uint32_t dg = sdig[x];
         const uint32_t dest = base[dg] + (x - tloff[dg]);
@@ -1727,7 +1785,7 @@ static int launch_seg_sort(const SortState& S, const Seg* segs, uint32_t n, cons
 
 // One block: per large segment its first tile and chunk (exclusive prefix
 // over the list), totals into counters[8], [9]; resets the next-list count.
-__global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, const Seg* segs, uint32_t nseg) {
+__global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, Seg* segs, uint32_t nseg) {
     __shared__ uint32_t st_[1024], sc_[1024];
     if (!segs) {
         segs = S.large[S.counters[12]];
@@ -1755,6 +1813,8 @@ __global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, const Seg* se
     uint32_t rt = st_[threadIdx.x] - tt, rc = sc_[threadIdx.x] - tc;
     for (uint32_t i = b; i < e; ++i) {
         const uint32_t t = (segs[i].size + LT_TILE - 1) / LT_TILE;
+        // keys folded by the previous scatter: the bits where they differ
+        if (S.child && (segs[i].flags & (F_KEYS | F_PIVOT)) == F_KEYS) segs[i].diff = segs[i].kor ^ segs[i].kand;
         S.tile0[i] = rt;
         S.chunk0[i] = rc;
         rt += t;
@@ -1768,8 +1828,9 @@ __global__ void __launch_bounds__(1024) k_seg_offsets(SortState S, const Seg* se
             S.counters[9] = 0;
             S.counters[10] = 1;
         }
-        S.counters[0] = 0;  // large segments of the next pass
-        S.counters[6] = 0;  // splitter tables of this pass
+        S.counters[0] = 0;   // large segments of the next pass
+        S.counters[11] = 0;  // of them, without keys or with a pivot pass
+        S.counters[6] = 0;   // splitter tables of this pass
     }
 }
 
@@ -1915,6 +1976,10 @@ void layout_sort(Carve& c, SortLayout& L, uint64_t n, uint32_t p, uint32_t small
     L.tile_hist = c.take<uint32_t>(L.cap_tiles * 256);
     L.chunk_pre = c.take<uint32_t>(L.cap_chunks * 256);
     L.bucket = c.take<uint32_t>(L.cap_large * 257);
+    // the child table: 256 slots per large segment, about 4 bytes per string
+    // once large segments hold more than 256 strings (smaller cut-offs keep
+    // the per-pass key reads instead)
+    L.child = small_max >= 256 ? c.take<uint32_t>(L.cap_large * 256) : nullptr;
     L.counters = c.take<uint32_t>(16);
     L.pb = c.take<uint64_t>(p + 1);
     L.scan = c.take<unsigned char>(scan_scratch_bytes(L.cap_large));
@@ -1951,6 +2016,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.chunk_pre = L.chunk_pre;
     S.bucket = L.bucket;
     S.counters = L.counters;
+    S.child = L.child;
+    S.nxt = nullptr;
     S.small_max = clamp_small_max(small_max);
     S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
     S.cap_large = L.cap_large;
@@ -1984,6 +2051,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         DSSS_TRY(set_smem_once(c4096, k_seg_sort<4096, 256>, (int)seg_sort_smem<4096>()));
         S.large[0] = large_list(L, 0);
         S.large[1] = large_list(L, 1);
+        S.child = nullptr;  // every pass of the graph reads the keys itself
         return sort_strings_graph(L, S, n, p, ids_in, pin, st);
     }
     DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
@@ -1999,6 +2067,10 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     uint32_t guard = 0;
     S.dig = dig_all ? dig : nullptr;
     bool first_pass = true;
+    // whether the list holds a segment without keys folded by the previous
+    // scatter (no keys, a pivot pass, or the first pass): only then the
+    // prefix, pivot and key passes run
+    bool keyless = true;
     while (nlarge) {
         if (++guard > (1u << 24)) return fail(DSSS_EDEVICE, "string sort made no progress");
         Seg* segs = large[cur];
@@ -2010,10 +2082,13 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         uint64_t max_tiles = std::min<uint64_t>(L.cap_tiles, n / LT_TILE + nlarge + 1);
         uint64_t max_chunks = std::min<uint64_t>(L.cap_chunks, max_tiles / CHUNK_TILES + nlarge + 1);
         S.large[0] = segs;
-        DSSS_LAUNCH("k_spec", st, k_spec<<<std::min<uint32_t>(nlarge, 148 * 16), 256, 0, st>>>(S, segs, nlarge));
-        DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
-        DSSS_LAUNCH("k_pivot", st, k_pivot<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
-        DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        S.nxt = next;
+        if (keyless) {
+            DSSS_LAUNCH("k_spec", st, k_spec<<<std::min<uint32_t>(nlarge, 148 * 16), 256, 0, st>>>(S, segs, nlarge));
+            DSSS_LAUNCH("k_prefix", st, k_prefix<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+            DSSS_LAUNCH("k_pivot", st, k_pivot<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+            DSSS_LAUNCH("k_keys_diff", st, k_keys_diff<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        }
         if (S.split_min)
             DSSS_LAUNCH("k_split_sample", st,
                         k_split_sample<<<std::min<uint32_t>(nlarge, 148 * 2), SPL_SAMPLE / 2, 0, st>>>(S, segs, nlarge));
@@ -2025,6 +2100,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         DSSS_CUDA(cudaMemcpyAsync(pin, L.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         DSSS_CUDA(cudaStreamSynchronize(st));
         nlarge = pin[0];
+        keyless = !S.child || pin[11] != 0;
         if (pin[10]) return fail(DSSS_EDEVICE, "string sort: internal consistency guard tripped");
         if (nlarge > L.cap_large) return fail(DSSS_EDEVICE, "string sort: large-segment list overflow");
         cur ^= 1;

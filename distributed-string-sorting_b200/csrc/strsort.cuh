@@ -15,6 +15,7 @@ struct SortLayout {
     uint32_t* tile_hist;
     uint32_t* chunk_pre;
     uint32_t* bucket;
+    uint32_t* child;  // 256 per large segment (NULL: the passes read the keys themselves)
     uint32_t* counters;
     uint64_t* pb;
     unsigned char* scan;

@@ -92,21 +92,33 @@ void make_handles(const ArenaDev& a, ulonglong2* h, cudaStream_t st) {
 // starting offset per bucket.
 constexpr int MS_NT = 256, MS_IPT = 8, MS_TILE = MS_NT * MS_IPT;
 
+// Counts per warp in its own row of shared memory (P x MS_NT / 32 words):
+// plain shared atomics, no match, no contention between warps.
 __global__ void __launch_bounds__(MS_NT) k_ms_hist(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles,
                                                   uint32_t* hist) {
     extern __shared__ uint32_t h[];
-    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) h[b] = 0;
+    constexpr int NW = MS_NT / 32;
+    for (uint32_t b = threadIdx.x; b < P * NW; b += MS_NT) h[b] = 0;
     __syncthreads();
     const uint64_t tb = (uint64_t)blockIdx.x * MS_TILE;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t base = tb + (threadIdx.x & ~31u); base < tb + MS_TILE; base += MS_NT) {
-        uint64_t i = base + lane;
-        uint32_t d = i < n ? bucket[i] : 0xFFFFFFFFu - lane;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (i < n && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    uint32_t* hw = h + (threadIdx.x >> 5) * P;
+    // every bucket id of the thread loaded before the first is counted
+    uint32_t dv[MS_IPT];
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j) {
+        const uint64_t i = tb + (uint64_t)j * MS_NT + threadIdx.x;
+        dv[j] = i < n ? bucket[i] : 0xFFFFFFFFu;
     }
+#pragma unroll
+    for (int j = 0; j < MS_IPT; ++j)
+        if (dv[j] < P) atomicAdd(&hw[dv[j]], 1u);
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) hist[(uint64_t)b * tiles + blockIdx.x] = h[b];
+    for (uint32_t b = threadIdx.x; b < P; b += MS_NT) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) t += h[w * P + b];
+        hist[(uint64_t)b * tiles + blockIdx.x] = t;
+    }
 }
 
 __global__ void __launch_bounds__(MS_NT) k_ms_scatter(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles,
@@ -276,6 +288,13 @@ __global__ void __launch_bounds__(MS_NT, 4) k_ms_scatter_pay(const uint32_t* buc
     }
 }
 
+static int launch_ms_hist(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles, uint32_t* hist,
+                          cudaStream_t st) {
+    const size_t sm = (size_t)P * (MS_NT / 32) * sizeof(uint32_t);  // at most 32 KiB
+    DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, sm, st>>>(bucket, n, P, tiles, hist));
+    return DSSS_OK;
+}
+
 template <int NPAY>
 static int launch_ms_pay(const uint32_t* bucket, uint64_t n, uint32_t P, uint64_t tiles, const uint32_t* off,
                          const Payload& pl, uint32_t* rank_out, uint32_t* err, cudaStream_t st) {
@@ -304,7 +323,7 @@ int multisplit_payload(const uint32_t* bucket, uint64_t n, uint32_t P, int npay,
         pl.in[k] = k < npay ? in[k] : nullptr;
         pl.out[k] = k < npay ? out[k] : nullptr;
     }
-    DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, P * sizeof(uint32_t), st>>>(bucket, n, P, tiles, hist));
+    DSSS_TRY(launch_ms_hist(bucket, n, P, tiles, hist, st));
     DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
     if (npay == 1) DSSS_TRY(launch_ms_pay<1>(bucket, n, P, tiles, off, pl, rank_out, err, st));
     else if (npay == 2) DSSS_TRY(launch_ms_pay<2>(bucket, n, P, tiles, off, pl, rank_out, err, st));
@@ -330,10 +349,10 @@ int multisplit(const uint32_t* bucket, uint64_t n, uint32_t P, uint32_t* dest, v
     uint32_t* hist = c.take<uint32_t>(cells);
     uint32_t* off = c.take<uint32_t>(cells);
     void* sc = c.take<unsigned char>(scan_scratch_bytes(cells));
-    size_t sh1 = P * sizeof(uint32_t), sh2 = (size_t)P * (1 + MS_NT / 32) * sizeof(uint32_t);
+    const size_t sh2 = (size_t)P * (1 + MS_NT / 32) * sizeof(uint32_t);
     static std::atomic<uint64_t> configured{0};
     DSSS_TRY(set_smem_once(configured, k_ms_scatter, (int)(MAX_SPLIT_BUCKETS * (1 + MS_NT / 32) * sizeof(uint32_t))));
-    DSSS_LAUNCH("k_ms_hist", st, k_ms_hist<<<(unsigned)tiles, MS_NT, sh1, st>>>(bucket, n, P, tiles, hist));
+    DSSS_TRY(launch_ms_hist(bucket, n, P, tiles, hist, st));
     DSSS_TRY(exclusive_scan_u32(hist, off, cells, nullptr, sc, st));
     DSSS_LAUNCH("k_ms_scatter", st, k_ms_scatter<<<(unsigned)tiles, MS_NT, sh2, st>>>(bucket, n, P, tiles, off, dest));
     DSSS_CUDA(cudaGetLastError());
