@@ -147,8 +147,11 @@ __global__ void __launch_bounds__(BD_NT, 4) k_bucket_direct(const uint32_t* pe, 
 #pragma unroll
         for (int j = 0; j < BD_IPT; ++j) {
             const uint32_t m = bk[j] + step;
-            const uint64_t at = (uint64_t)src[j] * (p + 1) + m;
-            if (m < p && (SMEM ? (uint64_t)tab[at] : bounds[at]) <= li[j]) bk[j] = m;
+            if (m < p) {
+                const bool le = SMEM ? tab[src[j] * (p + 1) + m] <= li[j]
+                                     : bounds[(uint64_t)src[j] * (p + 1) + m] <= li[j];
+                if (le) bk[j] = m;
+            }
         }
     }
 #pragma unroll

@@ -698,11 +698,14 @@ __device__ __forceinline__ uint32_t pp_coarse_of(const uint32_t* tile0, uint32_t
 // next b2 bits), bucket-major inside the coarse bucket's count block.
 __global__ void __launch_bounds__(PP_NT) k_pp_hist2(const unsigned long long* h1, const uint32_t* mid, uint32_t b1,
                                                    uint32_t b2, uint32_t* hist) {
-    __shared__ uint32_t h[256];
+    __shared__ uint32_t h[256], tile0[257];
     const uint32_t t = blockIdx.x;
     if (t >= mid[512 + 256]) return;
-    const uint32_t c = pp_coarse_of(mid + 512, t);
-    const uint32_t lt = t - mid[512 + c], nt = mid[512 + c + 1] - mid[512 + c];
+    tile0[threadIdx.x] = mid[512 + threadIdx.x];  // searched in shared memory
+    if (threadIdx.x == 0) tile0[256] = mid[512 + 256];
+    __syncthreads();
+    const uint32_t c = pp_coarse_of(tile0, t);
+    const uint32_t lt = t - tile0[c], nt = tile0[c + 1] - tile0[c];
     const uint32_t b = mid[c] + lt * PP_TILE, e = mid[c] + min(mid[256 + c], (lt + 1) * PP_TILE);
     h[threadIdx.x] = 0;
     __syncthreads();
@@ -717,11 +720,14 @@ __global__ void __launch_bounds__(PP_NT, 4) k_pp_scatter2(const unsigned long lo
     extern __shared__ __align__(16) unsigned char pp_sm[];
     unsigned long long* sh = (unsigned long long*)pp_sm;
     uint32_t* ss = (uint32_t*)(sh + PP_TILE);
-    __shared__ uint32_t cnt[256], beg[256], cur[256], gbase[256], ws[8];
+    __shared__ uint32_t cnt[256], beg[256], cur[256], gbase[256], ws[8], tile0[257];
     const uint32_t t = blockIdx.x;
     if (t >= mid[512 + 256]) return;
-    const uint32_t c = pp_coarse_of(mid + 512, t);
-    const uint32_t lt = t - mid[512 + c], nt = mid[512 + c + 1] - mid[512 + c];
+    tile0[threadIdx.x] = mid[512 + threadIdx.x];  // searched in shared memory
+    if (threadIdx.x == 0) tile0[256] = mid[512 + 256];
+    __syncthreads();
+    const uint32_t c = pp_coarse_of(tile0, t);
+    const uint32_t lt = t - tile0[c], nt = tile0[c + 1] - tile0[c];
     const uint32_t b = mid[c] + lt * PP_TILE, e = mid[c] + min(mid[256 + c], (lt + 1) * PP_TILE);
     cnt[threadIdx.x] = 0;
     gbase[threadIdx.x] = threadIdx.x < (1u << b2) ? off[mid[769 + c] + (uint64_t)threadIdx.x * nt + lt] : 0u;

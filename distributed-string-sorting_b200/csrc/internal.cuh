@@ -143,6 +143,8 @@ enum TuneKnob : int {
                              // fail on a mismatch (a self-check)
     TUNE_SORT_SPLIT_MIN,     // smallest large segment that may split by sampled splitters instead of a key
                              // byte (0: never, the default; values below 4096 count as 4096)
+    TUNE_SORT_BITS,          // 1: passes over plain keys split on the keys' eight most significant differing
+                             // bits (several key bytes over small alphabets); 0: on one key byte (default)
     TUNE_COUNT
 };
 int64_t tune(TuneKnob k);

@@ -109,6 +109,7 @@ struct SortState {
     Seg* nxt;  // the next pass's list (the scatter's children)
     uint32_t small_max;
     uint32_t pivot;  // pivot passes enabled
+    uint32_t bits;   // plain keys split on their top differing bits (0: on a key byte)
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
     // first pass only: every string's prefix hashes at the first schedule
     // depths (root_digests), ROOT_DIGESTS arrays of dig_n entries
@@ -746,6 +747,90 @@ __global__ void __launch_bounds__(LT_NT) k_pivot(SortState S, Seg* segs, uint32_
 // ------------------------------------------------------------------ hist ----
 __device__ __forceinline__ uint32_t digit_of(uint64_t k, uint32_t shift) { return (uint32_t)(k >> shift) & 0xFFu; }
 
+// The digit of a pass over plain keys: the (up to) eight most significant
+// bits in which the segment's keys differ, packed in key order.  Every bit
+// above the lowest of them that is not one of them is the same in all keys,
+// so the digit orders the keys as their first bytes do.  Where the key byte
+// at the first difference varies in all eight bits this is that byte; over a
+// small alphabet (letters vary in 5 or 6 bits of a byte, DNA in 4) a digit
+// covers more than one key byte, and a pass splits up to 256 ways instead of
+// as many ways as the byte has values.  sh[j]: the right shift that brings
+// digit bit j (most significant first) to bit 0.
+struct BitDigit {
+    uint32_t nb;     // bits in the digit (1..8)
+    uint32_t sh[8];
+    bool whole;      // one whole key byte: (k >> sh[7]) & 0xFF
+};
+
+__device__ __forceinline__ BitDigit bit_digit_spec(uint64_t diff) {
+    BitDigit d;
+    d.nb = 0;
+    uint64_t x = diff;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        d.sh[j] = 0;
+        if (x) {
+            const uint32_t at = 63u - (uint32_t)__clzll(x);
+            d.sh[j] = at;
+            x &= ~(1ull << at);
+            ++d.nb;
+        }
+    }
+    d.whole = d.nb == 8 && (d.sh[0] & 7u) == 7u && d.sh[7] + 7u == d.sh[0];
+    return d;
+}
+
+// Digit lookup in shared memory: for each key byte that holds digit bits,
+// tab[q][v] is the digit bits of byte value v, packed and moved to their place
+// in the digit; a key's digit is the OR over those bytes (usually two).
+struct BitTables {
+    uint8_t tab[8][256];
+    uint32_t n;      // key bytes holding digit bits
+    uint32_t sh[8];  // right shift of each such byte
+};
+
+// Builds the tables of digit d; every thread of a 256-thread block calls it,
+// and a barrier follows before the first lookup.
+__device__ __forceinline__ void bit_tables_build(BitTables& T, const BitDigit& d) {
+    uint64_t chosen = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if ((uint32_t)j < d.nb) chosen |= 1ull << d.sh[j];
+    const uint32_t v = threadIdx.x;
+    uint32_t q = 0, below = (uint32_t)__popcll(chosen);
+    for (int J = 0; J < 8; ++J) {
+        const uint32_t sh = 56u - 8u * (uint32_t)J;
+        const uint32_t sel = (uint32_t)(chosen >> sh) & 0xFFu;
+        if (!sel) continue;
+        below -= (uint32_t)__popc(sel);  // digit bits in later key bytes
+        uint32_t x = 0;                  // the bits of v that sel selects, packed
+        for (int bit = 7; bit >= 0; --bit)
+            if ((sel >> bit) & 1u) x = (x << 1) | ((v >> bit) & 1u);
+        T.tab[q][v] = (uint8_t)(x << below);
+        if (v == 0) T.sh[q] = sh;
+        ++q;
+    }
+    if (v == 0) T.n = q;
+}
+
+__device__ __forceinline__ uint32_t bit_digit(uint64_t k, const BitDigit& d, const BitTables& T) {
+    if (d.whole) return (uint32_t)(k >> d.sh[7]) & 0xFFu;
+    uint32_t v = 0;
+    for (uint32_t q = 0; q < T.n; ++q) v |= T.tab[q][(uint32_t)(k >> T.sh[q]) & 0xFFu];
+    return v;
+}
+
+// Key byte (from the key's first byte) that holds digit bit h (0: least
+// significant): two keys whose digits first differ in bit h share exactly
+// that many bytes past the segment depth.
+__device__ __forceinline__ uint32_t bit_digit_byte(const BitDigit& d, uint32_t h) {
+    uint32_t byte = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if ((uint32_t)j + 1 + h == d.nb) byte = (63u - d.sh[j]) >> 3;
+    return byte;
+}
+
 __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
         segs = S.large[S.counters[12]];
@@ -762,6 +847,11 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     if (sg.diff == 0) return;
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t m = sg.nspl;
+    // plain keys split on their top differing bits, pivot pseudo keys on a byte
+    const bool bits = S.bits && !m && !(sg.flags & (F_PIVOT | F_PSEUDO));
+    const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
+    __shared__ BitTables bt;
+    if (!bd.whole) bit_tables_build(bt, bd);
     const unsigned long long* key = S.key[sg.flags & F_PARITY];
 #pragma unroll
     for (int w = 0; w < LT_NT / 32; ++w) hist[w][threadIdx.x] = 0;
@@ -781,7 +871,7 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = tb + j * LT_NT + threadIdx.x;
-        if (i < te) atomicAdd(&wh[m ? spl_bucket(s_spl, m, k[j]) : digit_of(k[j], shift)], 1u);
+        if (i < te) atomicAdd(&wh[m ? spl_bucket(s_spl, m, k[j]) : bit_digit(k[j], bd, bt)], 1u);
     }
     __syncthreads();
     uint32_t c = 0;
@@ -928,7 +1018,16 @@ __global__ void __launch_bounds__(256) k_seg_scan(SortState S, Seg* segs, uint32
             push_small(S, cs, total, depth, np | F_KEYS);
         }
     } else if (!pseudo) {
-        if (d == 0) return;  // strings that end here: written by the scatter
+        // digit 0 holds the strings that end at byte b, unless byte b has a
+        // constant nonzero part (then no string ends there and digit 0 is an
+        // ordinary bucket)
+        bool ended_ok = true;
+        if (S.bits) {
+            const uint32_t shift = 56 - 8 * b;
+            const uint64_t k0 = S.key[par][sg.start];
+            ended_ok = (((k0 >> shift) & 0xFFu) & ~((sg.diff >> shift) & 0xFFu)) == 0;
+        }
+        if (d == 0 && ended_ok) return;  // strings that end here: written by the scatter
         // children keep the parent's keys: their first b+1 key bytes are now
         // common; one that keeps most of the parent gets a pivot pass
         if (total > S.small_max) {
@@ -1002,6 +1101,18 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     const uint32_t depth = sg.depth;
     const uint32_t m = sg.nspl;  // splitter buckets (0: the byte digit)
     const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
+    // plain keys split on their top differing bits, pivot pseudo keys on a byte
+    const bool bits = S.bits && !m && !pseudo;
+    const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
+    __shared__ BitTables bt;
+    if (!bd.whole) bit_tables_build(bt, bd);  // the barrier after the block's set-up follows
+    // digit 0 holds the strings that end at byte b unless byte b has a
+    // constant nonzero part
+    bool ended_ok = true;
+    if (bits) {
+        const uint64_t k0 = S.key[par][sg.start];
+        ended_ok = (((k0 >> shift) & 0xFFu) & ~((sg.diff >> shift) & 0xFFu)) == 0;
+    }
     // LCP inside the group of strings that end here and at bucket starts
     // (pivot code splits: d + min(l, l') from the two codes)
     const bool code_split = pseudo && b == 0;
@@ -1044,7 +1155,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = wb + j * 32 + lane;
-        const uint32_t dg = i < te ? (m ? spl_bucket(s_spl, m, k[j]) : digit_of(k[j], shift)) : 0x100u + lane;
+        const uint32_t dg = i < te ? (m ? spl_bucket(s_spl, m, k[j]) : bit_digit(k[j], bd, bt)) : 0x100u + lane;
         const uint32_t peers = __match_any_sync(0xffffffffu, dg);
         const uint32_t r = __popc(peers & ((1u << lane) - 1));
         const uint32_t prev = dg < 256 ? wcnt[w][dg] : 0;
@@ -1127,7 +1238,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
             continue;
         }
         const uint32_t oo = sord[x];
-        const bool ended = !m && dg == 0 && !code_split;
+        const bool ended = !m && dg == 0 && !code_split && ended_ok;
         if (ended || cnt == 1) {
             S.ord_out[dest] = oo;
             if (ended && dest != bs) S.lcp_out[dest] = lcp_here;
@@ -1143,10 +1254,13 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
             }
         } else if (dest == bs && dg != sg.first_digit) {
             uint32_t l = lcp_here;
-            if (code_split) {
-                uint32_t pd = dg - 1;  // previous non-empty code (exists: dg is not the first)
+            if (code_split || !bd.whole) {
+                uint32_t pd = dg - 1;  // previous non-empty bucket (exists: dg is not the first)
                 while (pd > 0 && bstart[pd] == bs) --pd;
-                l = depth + min(pivot_l(dg), pivot_l(pd));
+                // pivot codes: d + min(l, l'); bit digits: the byte of the
+                // highest bit in which the two buckets' digits differ
+                l = code_split ? depth + min(pivot_l(dg), pivot_l(pd))
+                               : depth + bit_digit_byte(bd, 31u - (uint32_t)__clz(dg ^ pd));
             }
             S.lcp_out[dest] = l;
         }
@@ -2020,6 +2134,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.nxt = nullptr;
     S.small_max = clamp_small_max(small_max);
     S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
+    S.bits = tune(TUNE_SORT_BITS) ? 1u : 0u;
     S.cap_large = L.cap_large;
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;
