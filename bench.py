@@ -65,8 +65,9 @@ CONFIGS = {
 # DRAM bytes (read + write) per unit of the kernels that carry a roofline,
 # from one ncu capture each on 8e6 strings x 200 B (D/N 0.25, p = 64); the
 # traffic of a launch grows with its units.  None: not captured.
-DRAM_PER_UNIT = {k: None for k in ("k_prefix", "k_pp_hist1", "k_pp_scatter1", "k_pp_hist2", "k_pp_scatter2",
-                                     "k_dp_bucket_dups", "k_dp_lens")}
+DRAM_PER_UNIT = {"k_prefix": 234.6, "k_pp_hist1": None, "k_pp_scatter1": 13.5, "k_pp_hist2": None,
+                 "k_pp_scatter2": 18.8, "k_dp_bucket_dups": 8.1, "k_dp_lens": None, "k_bucket_direct": 18.1,
+                 "k_ms_scatter_pay": 18.2}
 
 
 def read_peaks():
@@ -169,7 +170,7 @@ def bench_batched(d, torch, steps, warmup, p=64, nsets=16, text=4 << 20, sizes=N
         for k in range(nsets):
             outs[k] = d.pd_sort(ctx, ds_each[k], p, out=outs[k])
 
-    tuning = d.autotune(ctx, ds_all, p, part_begin=pb, nsets=nsets, trials=1)
+    tuning = d.autotune(ctx, ds_all, p, part_begin=pb, nsets=nsets, trials=2)
     res = {}
     for name, fn in (("plain", plain), ("batched", batched)):
         for _ in range(warmup):
@@ -594,6 +595,8 @@ ROOFLINE_BYTES = {
     "k_pp_scatter2": "24 per string hashed at its final depth",
     "k_dp_bucket_dups": "12 per string hashed at its final depth",
     "k_dp_lens": "32 per string",
+    "k_bucket_direct": "24 per string",
+    "k_ms_scatter_pay": "24 per string (the multisplit by PE)",
 }
 SORT_KERNELS = ("k_init", "k_tile_counts", "k_prefix", "k_keys_diff", "k_hist", "k_chunk_sum", "k_seg_scan",
                 "k_scatter", "k_seg_sort", "k_warp_segs", "k_spec", "k_pivot", "k_seg_offsets", "k_split_sample",
@@ -618,6 +621,8 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
         "k_pp_scatter2": 24 * hashed,
         "k_dp_bucket_dups": 12 * hashed,
         "k_dp_lens": 32 * n,
+        "k_bucket_direct": 24 * n,
+        "k_ms_scatter_pay": 24 * n,
     }
     b_sort = D + 20 * n
     b_merge = int((dp - np.minimum(lcp, dp) + 1).sum()) + 24 * n
@@ -640,7 +645,7 @@ def pd_rooflines(out, lengths, n, kt, steps, peak, peak_kind, traffic_known=True
         launches = kernels[k][0] / steps
         ms = kernels[k][1] / steps
         unit = DRAM_PER_UNIT.get(k)
-        units = n if k in ("k_prefix", "k_dp_lens") else hashed
+        units = n if k in ("k_prefix", "k_dp_lens", "k_bucket_direct", "k_ms_scatter_pay") else hashed
         traffic = unit * units if (unit and traffic_known) else None
         # the step's bytes over the step's time of the kernel (all its launches)
         per[k] = line(k, per_step[k], ms, launches, formula + " (per step: all launches)", traffic,
@@ -768,7 +773,7 @@ def main():
             dist.barrier()
 
     # knobs picked by the autotuner on this input (results never depend on them)
-    tuning = None if args.no_autotune else d.autotune(ctx, ds, p, trials=1)
+    tuning = None if args.no_autotune else d.autotune(ctx, ds, p, trials=2)
     for _ in range(args.warmup):
         out = d.pd_sort(ctx, ds, p, out=out)
     torch.cuda.synchronize()

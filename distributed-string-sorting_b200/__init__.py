@@ -65,7 +65,8 @@ class HqResult(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("sort_small_max", ctypes.c_int64), ("sort_pivot", ctypes.c_int64), ("dp_filter_min", ctypes.c_int64),
                 ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("settings_tried", ctypes.c_uint32),
-                ("sort_split_min", ctypes.c_int64), ("sort_bits", ctypes.c_int64)]
+                ("sort_split_min", ctypes.c_int64), ("sort_bits", ctypes.c_int64),
+                ("sort_seg_bits", ctypes.c_int64)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -687,7 +688,8 @@ def pd_sort_batched_host(ctx: Context, hs: HostStrings, nsets: int, p: int, part
 
 
 TUNE_KNOBS = ("dp_filter_min", "dp_filter_bits", "sort_small_max", "sort_pivot", "dp_table", "sort_graph_max_n", "merge_by_sort",
-              "merge_extend_lanes", "dp_split", "copy_word", "dp_digest", "dp_check", "sort_split_min", "sort_bits")
+              "merge_extend_lanes", "dp_split", "copy_word", "dp_digest", "dp_check", "sort_split_min", "sort_bits",
+              "sort_seg_bits")
 
 
 def tune_set(name: str, value: int):

@@ -144,6 +144,14 @@ __device__ __forceinline__ void block_add(uint32_t* ctr, uint32_t v) {
 // dense round, which runs in arena order).
 __device__ __forceinline__ void mark_string(uint32_t* m, uint32_t s) { atomicOr(&m[s >> 5], 1u << (s & 31)); }
 
+// Marks every hashed string of a dense round (kinds 2 and 3) in the
+// arena-order bitmap, when not every string of the arena is hashed.
+__global__ void __launch_bounds__(256) k_dp_mark(const uint8_t* kind, const uint32_t* order, uint64_t n,
+                                                 uint32_t* hmask) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && kind[i] >= 2) mark_string(hmask, order[i]);
+}
+
 // Grid-stride over positions (grid a few blocks per SM): one pair of counter
 // atomics per block instead of per 256 positions.  hmask (with order): every
 // hashed string is marked for the arena-order form of the round (an atomic
@@ -470,7 +478,7 @@ __global__ void __launch_bounds__(256) k_dp_arena_insert(ArenaDev a, uint32_t de
                                                          uint32_t* dmask, uint32_t* err, uint32_t* ndup,
                                                          uint32_t check, uint32_t* bad) {
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.n || !bit_of(hmask, s)) return;
+    if (s >= a.n || (hmask && !bit_of(hmask, s))) return;
     unsigned long long h;
     if (dig) {  // stored by the string sort's first pass
         h = dig[s];
@@ -522,13 +530,14 @@ __global__ void __launch_bounds__(256) k_dp_arena_insert(ArenaDev a, uint32_t de
 // exclusive scan over the bucket-major (bucket, tile) counts, and a scatter
 // to each (bucket, tile)'s range with shared-memory cursors — no global
 // atomic per pair.  One block per bucket then finds the equal hashes of its
-// bucket in shared memory.  A bucket of more than PD_CAP pairs (the mean
-// plus 64 standard deviations for uniform hashes; only many equal prefixes on
-// different PEs can reach it) sends the round to the table form.
-constexpr uint32_t PD_TARGET = 4096;
-constexpr uint32_t PD_CAP = 8192;
+// bucket in shared memory (68 KiB: three blocks per SM).  A bucket of more
+// than PD_CAP pairs (the mean plus 45 standard deviations for uniform
+// hashes; only many equal prefixes on different PEs can reach it) sends the
+// round to the table form.
+constexpr uint32_t PD_TARGET = 2048;
+constexpr uint32_t PD_CAP = 4096;
 constexpr uint32_t PD_TAB = 2 * PD_CAP;  // shared-memory slots per bucket (load <= 1/2)
-constexpr uint32_t PD_NT = 1024;
+constexpr uint32_t PD_NT = 512;
 constexpr size_t PD_SMEM = (size_t)PD_CAP * 8 + (size_t)PD_TAB * 4 + PD_CAP;
 constexpr int PP_NT = 256, PP_IPT = 16, PP_TILE = PP_NT * PP_IPT;  // positions or pairs per tile
 
@@ -543,7 +552,7 @@ static uint32_t pd_buckets(uint64_t hashed) {
 __global__ void __launch_bounds__(256) k_dp_arena_hash(ArenaDev a, uint32_t depth, const unsigned long long* dig,
                                                        const uint32_t* hmask, unsigned long long* out, uint32_t* bad) {
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.n || !bit_of(hmask, s)) return;
+    if (s >= a.n || (hmask && !bit_of(hmask, s))) return;
     uint64_t off;
     uint32_t L;
     str_of(a, (uint32_t)s, off, L);
@@ -566,7 +575,7 @@ __global__ void __launch_bounds__(PP_NT) k_pp_hist1(uint64_t n, const unsigned l
     for (int j = 0; j < PP_IPT; ++j) {
         const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
         if (s < n) {
-            const uint32_t mw = hmask[s >> 5];
+            const uint32_t mw = hmask ? hmask[s >> 5] : ~0u;
             const unsigned long long hv = dig[s];
             if ((mw >> (s & 31)) & 1u) atomicAdd(&h[(uint32_t)(hv >> (64 - b1))], 1u);
         }
@@ -615,7 +624,7 @@ __global__ void __launch_bounds__(PP_NT, 4) k_pp_scatter1(uint64_t n, const unsi
 #pragma unroll
     for (int j = 0; j < PP_IPT; ++j) {
         const uint64_t s = t0 + (uint64_t)j * PP_NT + threadIdx.x;
-        mw[j] = s < n ? hmask[s >> 5] : 0u;
+        mw[j] = s < n ? (hmask ? hmask[s >> 5] : ~0u) : 0u;
         h[j] = s < n ? dig[s] : 0ull;
     }
     uint32_t marked = 0;
@@ -1225,8 +1234,9 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         // a round that may turn out dense marks its hashed strings for the
         // arena-order form (every string of the arena must be in the order)
         const bool mark = L.hmask && a.n <= n && cands * L.digest_share >= n;
-        if (mark) DSSS_CUDA(cudaMemsetAsync(L.hmask, 0, L.mask_words * sizeof(uint32_t), st));
-        uint32_t* hm = mark ? L.hmask : nullptr;
+        // the hashed strings are marked after the count, only when not every
+        // string of the arena is hashed (a null mask then stands for all)
+        uint32_t* hm = nullptr;
         if (depth > min_len) DSSS_TRY(need_lens());
         const uint32_t* lens = lens_ready ? L.lens : nullptr;  // nullptr: every string reaches the depth
         if (nsets == 1 && aligned16(lcp) && aligned16(dp) && aligned16(L.lens) && aligned16(L.st[cur]) &&
@@ -1302,6 +1312,13 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
             if (slots > L.slots) return fail(DSSS_EDEVICE, "distinguishing-prefix hash table exceeds the plan");
             const bool arena = mark && (uint64_t)hashed * L.digest_share >= n;
             const uint32_t check = (uint32_t)tune(TUNE_DP_CHECK);
+            const uint32_t* hmask = nullptr;  // every string of the arena hashed
+            if (arena && hashed < a.n) {
+                DSSS_CUDA(cudaMemsetAsync(L.hmask, 0, L.mask_words * sizeof(uint32_t), st));
+                DSSS_LAUNCH("k_dp_mark", st,
+                            k_dp_mark<<<grid_for(n, 256), 256, 0, st>>>(L.kind, order, n, L.hmask));
+                hmask = L.hmask;
+            }
             if (arena) {
                 const int dj = root_digest_index(depth);
                 const unsigned long long* dig =
@@ -1319,14 +1336,14 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                     if (!dig || check) {  // this round's hashes, in arena order
                         DSSS_LAUNCH("k_dp_arena_hash", st,
                                     k_dp_arena_hash<<<grid_for(a.n, 256), 256, 0, st>>>(
-                                        a, (uint32_t)depth, check ? dig : nullptr, L.hmask, L.pp_dig, L.counters + 9));
+                                        a, (uint32_t)depth, check ? dig : nullptr, hmask, L.pp_dig, L.counters + 9));
                         hd = L.pp_dig;
                     }
                     // two radix passes: top b1 bits, then the next b2 inside each coarse bucket
                     const uint32_t b1 = std::min<uint32_t>(bbits, 8), b2 = bbits - b1;
                     const uint32_t nt1 = (uint32_t)((a.n + PP_TILE - 1) / PP_TILE);
                     DSSS_LAUNCH("k_pp_hist1", st,
-                                k_pp_hist1<<<nt1, PP_NT, 0, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_hist));
+                                k_pp_hist1<<<nt1, PP_NT, 0, st>>>(a.n, hd, hmask, b1, nt1, L.pp_hist));
                     DSSS_TRY(exclusive_scan_u32(L.pp_hist, L.pp_off, 256ull * nt1, L.pp_total, L.pp_scan, st));
                     const unsigned long long* ph = L.pp_h1;
                     const uint32_t* ps = L.pp_s1;
@@ -1334,7 +1351,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                     DSSS_TRY(set_smem_once(pp1_configured, k_pp_scatter1, (int)PP_SMEM));
                     DSSS_TRY(set_smem_once(pp2_configured, k_pp_scatter2, (int)PP_SMEM));
                     DSSS_LAUNCH("k_pp_scatter1", st,
-                                k_pp_scatter1<<<nt1, PP_NT, PP_SMEM, st>>>(a.n, hd, L.hmask, b1, nt1, L.pp_off, L.pp_h1,
+                                k_pp_scatter1<<<nt1, PP_NT, PP_SMEM, st>>>(a.n, hd, hmask, b1, nt1, L.pp_off, L.pp_h1,
                                                                            L.pp_s1));
                     uint32_t* off2 = nullptr;
                     if (b2) {
@@ -1374,7 +1391,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
                     DSSS_CUDA(cudaMemsetAsync(L.dmask, 0, L.mask_words * sizeof(uint32_t), st));
                     DSSS_LAUNCH("k_dp_arena_insert", st,
                                 k_dp_arena_insert<<<grid_for(a.n, 256), 256, 0, st>>>(
-                                    a, (uint32_t)depth, dig, L.hmask, L.tkeys, L.tdup, L.tid, (uint32_t)(slots - 1),
+                                    a, (uint32_t)depth, dig, hmask, L.tkeys, L.tdup, L.tid, (uint32_t)(slots - 1),
                                     L.set_begin, nsets, L.set_base, L.set_mask, L.dmask, L.counters + 2,
                                     L.counters + 8, check, L.counters + 9));
                     DSSS_LAUNCH("k_dp_owner_dups", st,

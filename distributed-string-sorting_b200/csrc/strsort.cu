@@ -110,6 +110,7 @@ struct SortState {
     uint32_t small_max;
     uint32_t pivot;  // pivot passes enabled
     uint32_t bits;   // plain keys split on their top differing bits (0: on a key byte)
+    uint32_t seg_bits;  // the same inside the segment sorter
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
     // first pass only: every string's prefix hashes at the first schedule
     // depths (root_digests), ROOT_DIGESTS arrays of dig_n entries
@@ -789,28 +790,29 @@ struct BitTables {
     uint32_t sh[8];  // right shift of each such byte
 };
 
-// Builds the tables of digit d; every thread of a 256-thread block calls it,
-// and a barrier follows before the first lookup.
+// Builds the tables of digit d; every thread of the block calls it, and a
+// barrier follows before the first lookup.
 __device__ __forceinline__ void bit_tables_build(BitTables& T, const BitDigit& d) {
     uint64_t chosen = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j)
         if ((uint32_t)j < d.nb) chosen |= 1ull << d.sh[j];
-    const uint32_t v = threadIdx.x;
-    uint32_t q = 0, below = (uint32_t)__popcll(chosen);
-    for (int J = 0; J < 8; ++J) {
-        const uint32_t sh = 56u - 8u * (uint32_t)J;
-        const uint32_t sel = (uint32_t)(chosen >> sh) & 0xFFu;
-        if (!sel) continue;
-        below -= (uint32_t)__popc(sel);  // digit bits in later key bytes
-        uint32_t x = 0;                  // the bits of v that sel selects, packed
-        for (int bit = 7; bit >= 0; --bit)
-            if ((sel >> bit) & 1u) x = (x << 1) | ((v >> bit) & 1u);
-        T.tab[q][v] = (uint8_t)(x << below);
-        if (v == 0) T.sh[q] = sh;
-        ++q;
+    for (uint32_t v = threadIdx.x; v < 256; v += blockDim.x) {
+        uint32_t q = 0, below = (uint32_t)__popcll(chosen);
+        for (int J = 0; J < 8; ++J) {
+            const uint32_t sh = 56u - 8u * (uint32_t)J;
+            const uint32_t sel = (uint32_t)(chosen >> sh) & 0xFFu;
+            if (!sel) continue;
+            below -= (uint32_t)__popc(sel);  // digit bits in later key bytes
+            uint32_t x = 0;                  // the bits of v that sel selects, packed
+            for (int bit = 7; bit >= 0; --bit)
+                if ((sel >> bit) & 1u) x = (x << 1) | ((v >> bit) & 1u);
+            T.tab[q][v] = (uint8_t)(x << below);
+            if (v == 0) T.sh[q] = sh;
+            ++q;
+        }
+        if (v == 0) T.n = q;
     }
-    if (v == 0) T.n = q;
 }
 
 __device__ __forceinline__ uint32_t bit_digit(uint64_t k, const BitDigit& d, const BitTables& T) {
@@ -831,6 +833,9 @@ __device__ __forceinline__ uint32_t bit_digit_byte(const BitDigit& d, uint32_t h
     return byte;
 }
 
+// BITS: the bit-digit form (its tables and registers only where the knob asks
+// for it; the byte form keeps the occupancy of a 32-register kernel).
+template <bool BITS>
 __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, uint32_t nseg) {
     if (!segs) {  // graph mode: this pass's list and count live on the device
         segs = S.large[S.counters[12]];
@@ -848,10 +853,10 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t m = sg.nspl;
     // plain keys split on their top differing bits, pivot pseudo keys on a byte
-    const bool bits = S.bits && !m && !(sg.flags & (F_PIVOT | F_PSEUDO));
+    const bool bits = BITS && !m && !(sg.flags & (F_PIVOT | F_PSEUDO));
     const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
     __shared__ BitTables bt;
-    if (!bd.whole) bit_tables_build(bt, bd);
+    if (BITS && !bd.whole) bit_tables_build(bt, bd);
     const unsigned long long* key = S.key[sg.flags & F_PARITY];
 #pragma unroll
     for (int w = 0; w < LT_NT / 32; ++w) hist[w][threadIdx.x] = 0;
@@ -871,7 +876,8 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
 #pragma unroll
     for (int j = 0; j < LT_IPT; ++j) {
         const uint32_t i = tb + j * LT_NT + threadIdx.x;
-        if (i < te) atomicAdd(&wh[m ? spl_bucket(s_spl, m, k[j]) : bit_digit(k[j], bd, bt)], 1u);
+        if (i < te)
+            atomicAdd(&wh[m ? spl_bucket(s_spl, m, k[j]) : BITS ? bit_digit(k[j], bd, bt) : digit_of(k[j], shift)], 1u);
     }
     __syncthreads();
     uint32_t c = 0;
@@ -1380,6 +1386,58 @@ __device__ __forceinline__ void warp_sort(const ArenaDev& a, uint32_t size, uint
     }
 }
 
+// A bucket of at most T strings whose keys are in shared memory, sorted by
+// one thread: an odd-even transposition network on (key, id) in registers
+// (absent slots carry the largest pair, so they sort last), then the LCPs of
+// neighbours.  Returns false,
+// writing nothing, when two keys are equal and neither string ends inside
+// them (a warp sort then goes deeper).
+template <int T>
+__device__ __forceinline__ bool tiny_sort(const unsigned long long* sk, uint32_t* so, uint32_t* lcp, uint32_t ws,
+                                          uint32_t wn, uint32_t wd) {
+    uint64_t k[T];
+    uint32_t o[T];
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+        o[i] = 0xFFFFFFFFu;
+        k[i] = ~0ull;
+        if ((uint32_t)i < wn) {
+            o[i] = so[ws + i];
+            k[i] = sk[ws + i];
+        }
+    }
+#pragma unroll
+    for (int pass = 0; pass < T; ++pass) {
+#pragma unroll
+        for (int i = pass & 1; i + 1 < T; i += 2) {
+            if (k[i + 1] < k[i] || (k[i + 1] == k[i] && o[i + 1] < o[i])) {
+                const uint64_t tk = k[i];
+                k[i] = k[i + 1];
+                k[i + 1] = tk;
+                const uint32_t to = o[i];
+                o[i] = o[i + 1];
+                o[i + 1] = to;
+            }
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int i = 1; i < T; ++i)
+        if ((uint32_t)i < wn && k[i - 1] == k[i] && zero_byte(k[i]) == 8) ok = false;
+    if (!ok) return false;
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+        if ((uint32_t)i < wn) {
+            so[ws + i] = o[i];
+            if (i) lcp[ws + i] = k[i - 1] != k[i] ? wd + key_lcp(k[i - 1], k[i]) : wd + zero_byte(k[i]);
+        }
+    }
+    return true;
+}
+
+constexpr uint32_t WL_DONE = 1u << 31;  // warp-list entry finished by one thread
+constexpr uint32_t TINY_MAX = 8;       // largest bucket one thread sorts
+
 // Buckets of 33..64 strings: lane l holds positions l and l + 32 (elements 0
 // and 1).  The same bitonic order on (group, key, id) over 64 positions (the
 // stage j = 32 compares a lane's two elements), the same run handling as
@@ -1586,6 +1644,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
     __shared__ uint32_t wcnt[NW][256];
     __shared__ uint32_t s_top, s_nw, s_cur[3];
     __shared__ unsigned long long s_diff;
+    __shared__ BitTables sbt;
     if (dcount) nseg = *dcount;
     for (uint32_t bi = blockIdx.x; bi < nseg; bi += gridDim.x) {
     const Seg seg = segs[bi];
@@ -1697,6 +1756,13 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
         }
         const uint32_t b = (uint32_t)(__clzll(df) >> 3);
         const uint32_t shift = 56 - 8 * b;
+        // plain keys split on their top eight differing bits (seg_bits), pivot
+        // pseudo keys on a byte; digit 0 holds strings that end at byte b only
+        // when that byte has no constant nonzero part
+        const bool bits = S.seg_bits && !pseudo;
+        const BitDigit bd = bit_digit_spec(bits ? df : (0xFFull << shift));
+        if (!bd.whole) bit_tables_build(sbt, bd);  // ordered by the barrier below
+        const bool ended_ok = !bits || (((k0 >> shift) & 0xFFu) & ~((df >> shift) & 0xFFu)) == 0;
         for (uint32_t x = threadIdx.x; x < NW * 256; x += NT) (&wcnt[0][0])[x] = 0;
         __syncthreads();
         // stable ranks: warp w owns the contiguous chunk [w*cs, min((w+1)*cs, bn))
@@ -1705,7 +1771,7 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
         for (uint32_t base = (uint32_t)w * cs; base < ce; base += 32) {
             const uint32_t i = base + lane;
             const bool v = i < ce;
-            const uint32_t d = v ? digit_of(sk[bs + i], shift) : 0x100u + lane;
+            const uint32_t d = v ? bit_digit(sk[bs + i], bd, sbt) : 0x100u + lane;
             const uint32_t peers = __match_any_sync(FULL, d);
             const uint32_t r = __popc(peers & ((1u << lane) - 1u));
             const uint32_t prev = v ? wcnt[w][d] : 0u;
@@ -1774,14 +1840,17 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
             const uint32_t c0 = bs + bstart[d];
             if (c0 != bs) {  // boundary to the previous non-empty bucket
                 uint32_t l = lin;
-                if (code_split) {
+                if (code_split || !bd.whole) {
                     uint32_t pd = d - 1;
                     while (pd > 0 && bstart[pd] == bstart[d]) --pd;
-                    l = dep + min(pivot_l(d), pivot_l(pd));
+                    // pivot codes: d + min(l, l'); bit digits: the byte of the
+                    // highest bit in which the two buckets' digits differ
+                    l = code_split ? dep + min(pivot_l(d), pivot_l(pd))
+                                   : dep + bit_digit_byte(bd, 31u - (uint32_t)__clz(d ^ pd));
                 }
                 lcp[c0] = l;
             }
-            if (d == 0 && !code_split) {  // strings that end here: byte-identical
+            if (d == 0 && !code_split && ended_ok) {  // strings that end here: byte-identical
                 for (uint32_t k = 1; k < cnt; ++k) lcp[c0 + k] = lin;
                 continue;
             }
@@ -1837,7 +1906,17 @@ __global__ void __launch_bounds__(NT) k_seg_sort(SortState S, const Seg* segs, u
         __syncthreads();
     }
     const uint32_t nwl = s_nw;
+    // buckets of up to TINY_MAX strings: one thread each
+    for (uint32_t e = threadIdx.x; e < nwl; e += NT) {
+        const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1] & 0xFFFFu, wd = wl[3 * e + 2];
+        // keys that must be gathered first stay with a warp (32 gathers at once)
+        if (wn > TINY_MAX || ((wl[3 * e + 1] >> 16) & SF_REKEY)) continue;
+        const bool done = wn <= 4 ? tiny_sort<4>(sk, so, lcp, ws, wn, wd) : tiny_sort<8>(sk, so, lcp, ws, wn, wd);
+        if (done) wl[3 * e + 1] |= WL_DONE;
+    }
+    __syncthreads();
     for (uint32_t e = w; e < nwl; e += NW) {
+        if (wl[3 * e + 1] & WL_DONE) continue;
         const uint32_t ws = wl[3 * e], wn = wl[3 * e + 1] & 0xFFFFu, wd = wl[3 * e + 2];
         const bool rekey = (wl[3 * e + 1] >> 16) & SF_REKEY;
         if (WIDE_WL == 32 || wn <= 32) {
@@ -2030,7 +2109,8 @@ static int sort_strings_graph(const SortLayout& L, SortState S, uint64_t n, uint
             k_pivot<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_keys_diff<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             if (S.split_min) k_split_sample<<<148, SPL_SAMPLE / 2, 0, bst>>>(S, nullptr, 0);
-            k_hist<<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            if (S.bits) k_hist<true><<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
+            else k_hist<false><<<tiles, LT_NT, 0, bst>>>(S, nullptr, 0);
             k_chunk_sum<<<chunks, 256, 0, bst>>>(S, nullptr, 0);
             k_seg_scan<<<large, 256, 0, bst>>>(S, nullptr, 0, nullptr);
             k_scatter<<<tiles, LT_NT, SCATTER_SMEM, bst>>>(S, nullptr, 0);
@@ -2135,6 +2215,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.small_max = clamp_small_max(small_max);
     S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
     S.bits = tune(TUNE_SORT_BITS) ? 1u : 0u;
+    S.seg_bits = tune(TUNE_SORT_SEG_BITS) ? 1u : 0u;
     S.cap_large = L.cap_large;
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;
@@ -2207,7 +2288,8 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         if (S.split_min)
             DSSS_LAUNCH("k_split_sample", st,
                         k_split_sample<<<std::min<uint32_t>(nlarge, 148 * 2), SPL_SAMPLE / 2, 0, st>>>(S, segs, nlarge));
-        DSSS_LAUNCH("k_hist", st, k_hist<<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        if (S.bits) DSSS_LAUNCH("k_hist", st, k_hist<true><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        else DSSS_LAUNCH("k_hist", st, k_hist<false><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_seg_scan", st, k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next));
         DSSS_LAUNCH("k_scatter", st, k_scatter<<<(unsigned)max_tiles, LT_NT, SCATTER_SMEM, st>>>(S, segs, nlarge));

@@ -1,8 +1,9 @@
 // Autotuner: times the full path on the caller's input under every setting of
 // the tuning knobs in a small grid (small-segment cutoff of the string sort,
 // pivot passes, the MSD digit: one key byte, sampled splitters where a key
-// byte splits poorly, or the keys' top differing bits) and leaves the fastest
-// setting in force.
+// byte splits poorly, the keys' top differing bits in the passes over the
+// arena or inside the segment sorter) and leaves the fastest setting in
+// force.
 // Results never depend on the knobs, so tuning only changes speed.  The
 // digit's bucket count (256) and the scatter tile (2048 strings) are fixed in
 // this build: the shared-memory histograms and the 13-byte-per-string
@@ -17,17 +18,17 @@ using namespace dsss;
 
 namespace {
 
-constexpr int NKNOBS = 4;
+constexpr int NKNOBS = 5;
 
 struct Setting {
-    int64_t small_max, pivot, split_min, bits;
+    int64_t small_max, pivot, split_min, bits, seg_bits;
 };
 
 struct Knobs {
     int64_t v[NKNOBS];
 };
 
-const char* const kNames[NKNOBS] = {"sort_small_max", "sort_pivot", "sort_split_min", "sort_bits"};
+const char* const kNames[NKNOBS] = {"sort_small_max", "sort_pivot", "sort_split_min", "sort_bits", "sort_seg_bits"};
 
 Knobs get_knobs() {
     Knobs k;
@@ -61,20 +62,22 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const Knobs saved = get_knobs();
-    Setting grid[3 * 3 * 2];
+    Setting grid[4 * 3 * 2];
     {
         const int64_t smalls[3] = {4096, 1024, 256};
-        const int64_t digits[3][2] = {{0, 0}, {65536, 0}, {0, 1}};  // (split_min, bits)
+        const int64_t digits[4][3] = {{0, 0, 0}, {65536, 0, 0}, {0, 1, 0}, {0, 0, 1}};  // (split_min, bits, seg_bits)
         int g = 0;
-        for (int dgt = 0; dgt < 3; ++dgt)
+        for (int dgt = 0; dgt < 4; ++dgt)
             for (int pv = 1; pv >= 0; --pv)
-                for (int sm = 0; sm < 3; ++sm) grid[g++] = {smalls[sm], pv, digits[dgt][0], digits[dgt][1]};
+                for (int sm = 0; sm < 3; ++sm)
+                    grid[g++] = {smalls[sm], pv, digits[dgt][0], digits[dgt][1], digits[dgt][2]};
     }
     double best = 1e300, first = 0;
     int best_i = -1, rc = DSSS_OK;
     uint32_t tried = 0;
     for (int i = 0; i < (int)(sizeof grid / sizeof grid[0]) && rc == DSSS_OK; ++i) {
-        const int64_t v[NKNOBS] = {grid[i].small_max, grid[i].pivot, grid[i].split_min, grid[i].bits};
+        const int64_t v[NKNOBS] = {grid[i].small_max, grid[i].pivot, grid[i].split_min, grid[i].bits,
+                                   grid[i].seg_bits};
         set_knobs(v);
         ActiveCtx active(ctx);
         rc = pd_sort_dev(ctx, in, nsets, p, part_begin, opts, &r, st);  // warm: scratch grows here
@@ -103,12 +106,14 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
         set_knobs(saved.v);
         return rc != DSSS_OK ? rc : fail(DSSS_EDEVICE, "autotune: no setting ran");
     }
-    const int64_t v[NKNOBS] = {grid[best_i].small_max, grid[best_i].pivot, grid[best_i].split_min, grid[best_i].bits};
+    const int64_t v[NKNOBS] = {grid[best_i].small_max, grid[best_i].pivot, grid[best_i].split_min, grid[best_i].bits,
+                               grid[best_i].seg_bits};
     set_knobs(v);
     out->sort_small_max = v[0];
     out->sort_pivot = v[1];
     out->sort_split_min = v[2];
     out->sort_bits = v[3];
+    out->sort_seg_bits = v[4];
     dsss_tune_get("dp_filter_min", &out->dp_filter_min);
     out->best_ms = best;
     out->default_ms = first;

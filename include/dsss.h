@@ -156,7 +156,10 @@ int dsss_abi_version(void);
  *   sort_bits       1: MSD passes over plain keys split on the eight most
  *                   significant bits in which a segment's keys differ (over
  *                   small alphabets one pass then covers more than a key
- *                   byte); 0: on the first differing key byte (default) */
+ *                   byte); 0: on the first differing key byte (default)
+ *   sort_seg_bits   the same for the shared-memory passes of the segment
+ *                   sorter (segments up to the small-segment cutoff; 0:
+ *                   one key byte, the default) */
 int dsss_tune_set(const char* name, int64_t value);
 int dsss_tune_get(const char* name, int64_t* value);
 
@@ -164,8 +167,9 @@ int dsss_tune_get(const char* name, int64_t* value);
  * dsss_pd_sort_batched; nsets = 1 for one set) on the given device input
  * under each setting of a grid of the knobs above (sort_small_max 256 / 1024 /
  * 4096, sort_pivot on / off, and the MSD digit: one key byte, sampled
- * splitters where a key byte splits poorly (sort_split_min 65536), or the
- * keys' top differing bits (sort_bits 1)),
+ * splitters where a key byte splits poorly (sort_split_min 65536), the keys'
+ * top differing bits in the passes over the arena (sort_bits 1) or inside the
+ * segment sorter (sort_seg_bits 1)),
  * 1 + trials runs each, and leaves the fastest setting in force for later
  * calls.  out: the chosen setting (dp_filter_min: the value in force, not
  * searched), its time (minimum over trials) and the default setting's
@@ -174,7 +178,7 @@ typedef struct {
     int64_t sort_small_max, sort_pivot, dp_filter_min;
     double best_ms, default_ms;
     uint32_t settings_tried;
-    int64_t sort_split_min, sort_bits;
+    int64_t sort_split_min, sort_bits, sort_seg_bits;
 } dsss_tuning;
 int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets, uint32_t p, const uint64_t* part_begin,
                   const dsss_opts* opts, uint32_t trials, dsss_tuning* out, dsss_stream_t stream);

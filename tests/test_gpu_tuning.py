@@ -88,11 +88,13 @@ def test_autotune_picks_a_grid_setting(dsss, orc, ctx):
     """dsss_autotune leaves one setting of its grid in force; results stay exact."""
     hs = dsss.gen_suffix_strings(80000, 256, seed=8)
     ds = dsss.DeviceStrings(hs)
-    with dsss.tuned(sort_small_max=-1, sort_pivot=-1, sort_split_min=-1, sort_bits=-1):
+    with dsss.tuned(sort_small_max=-1, sort_pivot=-1, sort_split_min=-1, sort_bits=-1, sort_seg_bits=-1):
         t = dsss.autotune(ctx, ds, 4, trials=1)
-        assert t["settings_tried"] == 18
+        assert t["settings_tried"] == 24
         assert t["sort_small_max"] in (256, 1024, 4096) and t["sort_pivot"] in (0, 1)
-        assert (t["sort_split_min"], t["sort_bits"]) in ((0, 0), (65536, 0), (0, 1))
+        assert (t["sort_split_min"], t["sort_bits"], t["sort_seg_bits"]) in ((0, 0, 0), (65536, 0, 0), (0, 1, 0),
+                                                                             (0, 0, 1))
+        assert dsss.tune_get("sort_seg_bits") == t["sort_seg_bits"]
         assert dsss.tune_get("sort_split_min") == t["sort_split_min"]
         assert dsss.tune_get("sort_bits") == t["sort_bits"]
         assert 0 < t["best_ms"] <= t["default_ms"]
@@ -297,32 +299,36 @@ def test_sort_split_pd(dsss, orc, ctx, graph):
     check_pd(dsss, orc, hs, out, 4)
 
 
+@pytest.mark.parametrize("bits,seg_bits", [(1, 1), (1, 0), (0, 0)])
 @pytest.mark.parametrize("small", [0, 64])
 @pytest.mark.parametrize("name,strs", CASES + _split_inputs(), ids=IDS + [c[0] for c in _split_inputs()])
-def test_sort_bits(dsss, orc, ctx, name, strs, small):
+def test_sort_bits(dsss, orc, ctx, name, strs, small, bits, seg_bits):
     """MSD passes that split plain keys on their eight most significant
-    differing bits (sort_bits 1; several key bytes per pass over letters and
-    DNA, strings that end inside a digit, bytes with a constant nonzero part):
-    the oracle's order and LCPs, in one segment and in three."""
+    differing bits (sort_bits 1 for the passes over the arena, sort_seg_bits
+    1 inside the segment sorter; several key bytes per pass over letters and
+    DNA, strings that end inside a digit, bytes with a constant nonzero part)
+    or on one key byte: the oracle's order and LCPs, in one segment and in
+    three."""
     hs = host_of(dsss, strs)
     n = hs.n
     for p in (1, 3):
         if n < p:
             continue
         pb = np.linspace(0, n, p + 1).astype(np.uint64)
-        with dsss.tuned(sort_bits=1):
+        with dsss.tuned(sort_bits=bits, sort_seg_bits=seg_bits):
             order, lcp = dsss.local_sort_lcp(ctx, dsss.DeviceStrings(hs), p, part_begin=pb, small_sort_max=small)
         ro, rl = orc.local_sort(orc.Strings.from_host(hs), pb)
         assert np.array_equal(u64(order, n), ro)
         assert np.array_equal(u64(lcp, n), rl)
 
 
+@pytest.mark.parametrize("seg_bits", [0, 1])
 @pytest.mark.parametrize("graph", [0, 1 << 22])
 @pytest.mark.parametrize("gen", ["dn", "suffix"])
-def test_sort_bits_pd(dsss, orc, ctx, graph, gen):
+def test_sort_bits_pd(dsss, orc, ctx, graph, gen, seg_bits):
     """The full path with bit-digit passes (D/N strings over letters and DNA
     suffixes), host-driven and as one graph, against the oracle."""
     hs = dsss.gen_dn(200000, 60, 30, seed=43) if gen == "dn" else dsss.gen_suffix_strings(120000, 256, seed=9)
-    with dsss.tuned(sort_bits=1, sort_graph_max_n=graph, sort_small_max=256):
+    with dsss.tuned(sort_bits=1, sort_seg_bits=seg_bits, sort_graph_max_n=graph, sort_small_max=256):
         out = dsss.pd_sort(ctx, dsss.DeviceStrings(hs), 4)
     check_pd(dsss, orc, hs, out, 4)
