@@ -183,7 +183,7 @@ constexpr size_t msp_smem(uint32_t P) {
 }
 
 template <int NPAY>
-__global__ void __launch_bounds__(MS_NT, 4) k_ms_scatter_pay(const uint32_t* bucket, uint64_t n, uint32_t P,
+__global__ void __launch_bounds__(MS_NT, 5) k_ms_scatter_pay(const uint32_t* bucket, uint64_t n, uint32_t P,
                                                          uint64_t tiles, const uint32_t* off, Payload pl,
                                                          uint32_t* rank_out, uint32_t* err) {
     extern __shared__ __align__(16) uint32_t smp[];
