@@ -44,9 +44,12 @@ static uint32_t factor_of(const dsss_opts* o) { return (o && o->sampling_factor)
 static uint32_t sampler_of(const dsss_opts* o) { return o ? o->sampler : DSSS_SAMPLER_NUM_STRINGS; }
 static uint32_t smallmax_of(const dsss_opts* o) { return o ? o->small_sort_max : 0; }
 
-// PE of every sorted position: the last q with pb[q] <= ord[g], searched in
-// a shared-memory copy of the PE bounds (npe + 1 <= 1025 entries), PE_IPT
-// positions per thread with their ids loaded before the searches.
+// PE of every sorted position: the q with pb[q] <= ord[g] < pb[q + 1] in a
+// shared-memory copy of the PE bounds (npe + 1 <= 1025 entries), PE_IPT
+// positions per thread with their ids loaded before the lookups.  The first
+// guess is the PE that equal parts would give (id * p / n), moved by up to
+// two steps; a guess that is still off (PEs of very uneven sizes) falls back
+// to a binary search.
 constexpr int PE_NT = 256, PE_IPT = 8;
 __global__ void __launch_bounds__(PE_NT) k_pe_of(const uint32_t* ord, uint64_t n, const uint64_t* pb, uint32_t p,
                                                  uint32_t* pe) {
@@ -60,22 +63,29 @@ __global__ void __launch_bounds__(PE_NT) k_pe_of(const uint32_t* ord, uint64_t n
         s[j] = g < n ? ord[g] : 0u;
     }
     __syncthreads();
-    // the last q < p with pb[q] <= s: the same fixed steps for every
-    // position, the PE_IPT searches interleaved
-    uint32_t lo[PE_IPT];
+    const float scale = (float)p / (float)(spb[p] ? spb[p] : 1ull);
+    uint32_t q[PE_IPT];
 #pragma unroll
-    for (int j = 0; j < PE_IPT; ++j) lo[j] = 0;
-    for (uint32_t step = 1u << (31 - __clz(p | 1u)); step; step >>= 1) {
+    for (int j = 0; j < PE_IPT; ++j) q[j] = min(p - 1, (uint32_t)((float)s[j] * scale));
+#pragma unroll
+    for (int step = 0; step < 2; ++step) {
 #pragma unroll
         for (int j = 0; j < PE_IPT; ++j) {
-            const uint32_t m = lo[j] + step;
-            if (m < p && spb[m] <= s[j]) lo[j] = m;
+            if (spb[q[j]] > s[j]) --q[j];                        // q[j] > 0 here: spb[0] = 0
+            else if (spb[q[j] + 1] <= s[j]) ++q[j];              // q[j] + 1 < p here: spb[p] = n > s
         }
     }
 #pragma unroll
     for (int j = 0; j < PE_IPT; ++j) {
         const uint64_t g = g0 + (uint64_t)j * PE_NT;
-        if (g < n) pe[g] = lo[j];
+        if (g >= n) continue;
+        uint32_t r = q[j];
+        if (spb[r] > s[j] || spb[r + 1] <= s[j]) {  // still off: the last r < p with pb[r] <= s
+            r = 0;
+            for (uint32_t st = 1u << (31 - __clz(p | 1u)); st; st >>= 1)
+                if (r + st < p && spb[r + st] <= s[j]) r += st;
+        }
+        pe[g] = r;
     }
 }
 
