@@ -144,7 +144,8 @@ enum TuneKnob : int {
     TUNE_SORT_SPLIT_MIN,     // smallest large segment that may split by sampled splitters instead of a key
                              // byte (0: never, the default; values below 4096 count as 4096)
     TUNE_SORT_BITS,          // 1: passes over plain keys split on the keys' eight most significant differing
-                             // bits (several key bytes over small alphabets); 0: on one key byte (default)
+                             // bits (several key bytes over small alphabets); 2: only where the first
+                             // differing byte varies in at most four bits; 0: on one key byte (default)
     TUNE_SORT_SEG_BITS,      // the same for the shared-memory passes of the segment sorter (default 0)
     TUNE_COUNT
 };

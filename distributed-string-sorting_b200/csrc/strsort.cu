@@ -109,7 +109,7 @@ struct SortState {
     Seg* nxt;  // the next pass's list (the scatter's children)
     uint32_t small_max;
     uint32_t pivot;  // pivot passes enabled
-    uint32_t bits;   // plain keys split on their top differing bits (0: on a key byte)
+    uint32_t bits;   // plain keys split on their top differing bits: 0 never, 1 always, 2 on narrow bytes
     uint32_t seg_bits;  // the same inside the segment sorter
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
     // first pass only: every string's prefix hashes at the first schedule
@@ -763,6 +763,18 @@ struct BitDigit {
     bool whole;      // one whole key byte: (k >> sh[7]) & 0xFF
 };
 
+// Whether a pass over plain keys splits on bits: knob sort_bits 1 always, 2
+// where the first differing key byte varies in at most four bits (DNA, or a
+// leading digit with few values), 0 never; and only for segments of more
+// than four times the small-segment cutoff (a 256-way split of a segment
+// just above the cutoff leaves children of a few strings each, whose segment
+// records cost more than sorting them).
+__device__ __forceinline__ bool use_bits(uint32_t mode, uint64_t diff, uint32_t shift, uint32_t size,
+                                         uint32_t small_max) {
+    if ((uint64_t)size <= 4ull * small_max) return false;
+    return mode == 1 || (mode == 2 && __popc((uint32_t)(diff >> shift) & 0xFFu) <= 4);
+}
+
 __device__ __forceinline__ BitDigit bit_digit_spec(uint64_t diff) {
     BitDigit d;
     d.nb = 0;
@@ -853,7 +865,7 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t m = sg.nspl;
     // plain keys split on their top differing bits, pivot pseudo keys on a byte
-    const bool bits = BITS && !m && !(sg.flags & (F_PIVOT | F_PSEUDO));
+    const bool bits = BITS && !m && !(sg.flags & (F_PIVOT | F_PSEUDO)) && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max);
     const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
     __shared__ BitTables bt;
     if (BITS && !bd.whole) bit_tables_build(bt, bd);
@@ -1108,7 +1120,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     const uint32_t m = sg.nspl;  // splitter buckets (0: the byte digit)
     const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
     // plain keys split on their top differing bits, pivot pseudo keys on a byte
-    const bool bits = S.bits && !m && !pseudo;
+    const bool bits = S.bits && !m && !pseudo && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max);
     const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
     __shared__ BitTables bt;
     if (!bd.whole) bit_tables_build(bt, bd);  // the barrier after the block's set-up follows
@@ -2214,7 +2226,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.nxt = nullptr;
     S.small_max = clamp_small_max(small_max);
     S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
-    S.bits = tune(TUNE_SORT_BITS) ? 1u : 0u;
+    S.bits = (uint32_t)tune(TUNE_SORT_BITS);
     S.seg_bits = tune(TUNE_SORT_SEG_BITS) ? 1u : 0u;
     S.cap_large = L.cap_large;
     S.cap_small = L.cap_small;

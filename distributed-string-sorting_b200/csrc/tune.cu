@@ -62,12 +62,13 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const Knobs saved = get_knobs();
-    Setting grid[4 * 3 * 2];
+    Setting grid[5 * 3 * 2];
     {
         const int64_t smalls[3] = {4096, 1024, 256};
-        const int64_t digits[4][3] = {{0, 0, 0}, {65536, 0, 0}, {0, 1, 0}, {0, 0, 1}};  // (split_min, bits, seg_bits)
+        // (split_min, bits, seg_bits)
+        const int64_t digits[5][3] = {{0, 0, 0}, {65536, 0, 0}, {0, 2, 0}, {0, 0, 1}, {0, 2, 1}};
         int g = 0;
-        for (int dgt = 0; dgt < 4; ++dgt)
+        for (int dgt = 0; dgt < 5; ++dgt)
             for (int pv = 1; pv >= 0; --pv)
                 for (int sm = 0; sm < 3; ++sm)
                     grid[g++] = {smalls[sm], pv, digits[dgt][0], digits[dgt][1], digits[dgt][2]};
