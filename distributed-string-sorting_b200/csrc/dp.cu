@@ -93,6 +93,22 @@ __global__ void __launch_bounds__(256) k_min_len(const uint32_t* len, const ulon
     if ((threadIdx.x & 31) == 0 && m != 0xFFFFFFFFu) atomicMin(out, m);
 }
 
+// The smallest over sorted positions of max(lcp[i], lcp[i + 1]) (lcp[0] and
+// lcp[n] taken as 0)
+// into *out (set to ~0 beforehand): while every string is a candidate, a
+// round at a depth up to it and up to the shortest string finds every string
+// an LCP-local duplicate or a root, so all stay and nothing it hashes can
+// matter (no string's survival rests on a hash).
+__global__ void __launch_bounds__(256) k_min_nbr_lcp(const uint32_t* lcp, uint64_t n, uint32_t* out) {
+    uint32_t m = 0xFFFFFFFFu;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        m = min(m, max(i ? lcp[i] : 0u, i + 1 < n ? lcp[i + 1] : 0u));  // position 0 has no predecessor
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m != 0xFFFFFFFFu) atomicMin(out, m);
+}
+
 // Index of the string set holding sorted position i (set_begin: nsets+1 bounds).
 __device__ __forceinline__ uint32_t set_of(const uint64_t* set_begin, uint32_t nsets, uint64_t i) {
     uint32_t lo = 0, hi = nsets;
@@ -1124,7 +1140,7 @@ void layout_dp(Carve& c, DpLayout& L, uint64_t n, uint32_t nsets) {
     L.kind = c.take<uint8_t>(N);
     L.lens = c.take<uint32_t>(N);
     L.soff = c.take<uint64_t>(N);
-    L.minlen = c.take<uint32_t>(1);
+    L.minlen = c.take<uint32_t>(2);  // shortest string, smallest neighbour LCP
     L.slot = c.take<uint32_t>(N);
     // one set: the table for n keys; several: room for every set's own
     // power-of-two region (at most 3 slots per key plus 68 per set)
@@ -1208,13 +1224,20 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
     // lengths and offsets in sorted order are gathered (k_dp_lens, one random
     // handle read per position) only once a round needs them: a depth past
     // the shortest string of the arena, or hashes taken in sorted order
-    DSSS_CUDA(cudaMemsetAsync(L.minlen, 0xFF, sizeof(uint32_t), st));
+    DSSS_CUDA(cudaMemsetAsync(L.minlen, 0xFF, 2 * sizeof(uint32_t), st));
     DSSS_LAUNCH("k_min_len", st,
                 k_min_len<<<(unsigned)std::min<uint64_t>(grid_for(a.n, 256), 148 * 8), 256, 0, st>>>(
                     a.len, a.h, a.n, L.minlen));
-    DSSS_CUDA(cudaMemcpyAsync(pin, L.minlen, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DSSS_LAUNCH("k_min_nbr_lcp", st,
+                k_min_nbr_lcp<<<(unsigned)std::min<uint64_t>(grid_for(n, 256), 148 * 8), 256, 0, st>>>(lcp, n,
+                                                                                                      L.minlen + 1));
+    DSSS_CUDA(cudaMemcpyAsync(pin, L.minlen, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DSSS_CUDA(cudaStreamSynchronize(st));
     const uint64_t min_len = pin[0];
+    // rounds up to this depth, while every string is a candidate, keep every
+    // string and are not run (their candidate counts are recorded as n)
+    const uint64_t trivial_to = std::min<uint64_t>(min_len, pin[1]);
+    bool all_cands = true;
     bool lens_ready = false;
     auto need_lens = [&]() -> int {
         if (!lens_ready) {
@@ -1229,6 +1252,12 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
     uint64_t cands = n;  // candidates entering the round
     for (uint64_t i = start * 2;; i *= 2) {
         if (depth > 0xFFFFFFFFull) return fail(DSSS_EINVAL, "distinguishing-prefix depth overflow");
+        if (all_cands && depth <= trivial_to) {
+            if (round_counts && r < max_rounds) round_counts[r] = n;
+            ++r;
+            depth = start + i;
+            continue;
+        }
         DSSS_CUDA(cudaMemsetAsync(L.counters, 0, 16 * sizeof(uint32_t), st));
         if (nsets > 1) DSSS_CUDA(cudaMemsetAsync(L.set_cnt, 0, nsets * sizeof(uint32_t), st));
         // a round that may turn out dense marks its hashed strings for the
@@ -1242,12 +1271,12 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         if (nsets == 1 && aligned16(lcp) && aligned16(dp) && aligned16(L.lens) && aligned16(L.st[cur]) &&
             aligned16(L.st[cur ^ 1]) && aligned16(L.kind)) {
             DSSS_LAUNCH("k_dp_classify", st,
-                        k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], r == 0, lens, lcp, n,
+                        k_dp_classify4<<<stride_grid((n + 3) / 4), 256, 0, st>>>(L.st[cur], all_cands, lens, lcp, n,
                                                                                 (uint32_t)depth, dp, L.st[cur ^ 1],
                                                                                 L.kind, L.counters, order, hm));
         } else {
             DSSS_LAUNCH("k_dp_classify", st,
-                        k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], r == 0, lens, lcp, n, (uint32_t)depth,
+                        k_dp_classify<<<stride_grid(n), 256, 0, st>>>(L.st[cur], all_cands, lens, lcp, n, (uint32_t)depth,
                                                                      dp, L.st[cur ^ 1], L.kind, L.counters,
                                                                      L.set_begin, nsets, L.set_cnt, order, hm));
         }
@@ -1434,6 +1463,7 @@ int dp_rounds(const DpLayout& L, const ArenaDev& a, uint64_t n, const uint32_t* 
         if (round_counts && r < max_rounds) round_counts[r] = m;
         ++r;
         cur ^= 1;
+        all_cands = false;
         if (m == 0) break;
         cands = m;
         depth = start + i;
