@@ -74,7 +74,7 @@ static const KnobDef g_knob_defs[TUNE_COUNT] = {
     {"dp_digest", 4, 0, 64},
     {"dp_check", 0, 0, 1},
     {"sort_split_min", 0, 0, 1ll << 32},
-    {"sort_bits", 0, 0, 2},
+    {"sort_bits", 0, 0, 3},
     {"sort_seg_bits", 0, 0, 1},
 };
 static std::atomic<int64_t> g_knobs[TUNE_COUNT] = {{1ll << 40}, {16}, {4096}, {1}, {2}, {0}, {1}, {0}, {0}, {16}, {4},

@@ -145,7 +145,8 @@ enum TuneKnob : int {
                              // byte (0: never, the default; values below 4096 count as 4096)
     TUNE_SORT_BITS,          // 1: passes over plain keys split on the keys' eight most significant differing
                              // bits (several key bytes over small alphabets); 2: only where the first
-                             // differing byte varies in at most four bits; 0: on one key byte (default)
+                             // differing byte varies in at most four bits; 3: the same in the first pass
+                             // only; 0: on one key byte (default)
     TUNE_SORT_SEG_BITS,      // the same for the shared-memory passes of the segment sorter (default 0)
     TUNE_COUNT
 };

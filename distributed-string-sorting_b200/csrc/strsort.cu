@@ -111,6 +111,7 @@ struct SortState {
     uint32_t pivot;  // pivot passes enabled
     uint32_t bits;   // plain keys split on their top differing bits: 0 never, 1 always, 2 on narrow bytes
     uint32_t seg_bits;  // the same inside the segment sorter
+    uint32_t first;     // the first pass over the arena (host-driven passes)
     uint64_t cap_large, cap_small, cap_tiles, cap_chunks;
     // first pass only: every string's prefix hashes at the first schedule
     // depths (root_digests), ROOT_DIGESTS arrays of dig_n entries
@@ -765,14 +766,15 @@ struct BitDigit {
 
 // Whether a pass over plain keys splits on bits: knob sort_bits 1 always, 2
 // where the first differing key byte varies in at most four bits (DNA, or a
-// leading digit with few values), 0 never; and only for segments of more
-// than four times the small-segment cutoff (a 256-way split of a segment
-// just above the cutoff leaves children of a few strings each, whose segment
-// records cost more than sorting them).
+// leading digit with few values), 3 the same in the first pass only, 0
+// never; and only for segments of more than four times the small-segment
+// cutoff (a 256-way split of a segment just above the cutoff leaves children
+// of a few strings each, whose segment records cost more than sorting them).
 __device__ __forceinline__ bool use_bits(uint32_t mode, uint64_t diff, uint32_t shift, uint32_t size,
-                                         uint32_t small_max) {
+                                         uint32_t small_max, uint32_t first) {
     if ((uint64_t)size <= 4ull * small_max) return false;
-    return mode == 1 || (mode == 2 && __popc((uint32_t)(diff >> shift) & 0xFFu) <= 4);
+    const bool narrow = __popc((uint32_t)(diff >> shift) & 0xFFu) <= 4;
+    return mode == 1 || (mode == 2 && narrow) || (mode == 3 && first && narrow);
 }
 
 __device__ __forceinline__ BitDigit bit_digit_spec(uint64_t diff) {
@@ -865,7 +867,7 @@ __global__ void __launch_bounds__(LT_NT) k_hist(SortState S, const Seg* segs, ui
     const uint32_t shift = 56 - 8 * (uint32_t)(__clzll(sg.diff) >> 3);
     const uint32_t m = sg.nspl;
     // plain keys split on their top differing bits, pivot pseudo keys on a byte
-    const bool bits = BITS && !m && !(sg.flags & (F_PIVOT | F_PSEUDO)) && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max);
+    const bool bits = BITS && !m && !(sg.flags & (F_PIVOT | F_PSEUDO)) && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max, S.first);
     const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
     __shared__ BitTables bt;
     if (BITS && !bd.whole) bit_tables_build(bt, bd);
@@ -1120,7 +1122,7 @@ __global__ void __launch_bounds__(LT_NT, 4) k_scatter(SortState S, const Seg* se
     const uint32_t m = sg.nspl;  // splitter buckets (0: the byte digit)
     const bool pseudo = (sg.flags & (F_PIVOT | F_PSEUDO)) != 0;
     // plain keys split on their top differing bits, pivot pseudo keys on a byte
-    const bool bits = S.bits && !m && !pseudo && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max);
+    const bool bits = S.bits && !m && !pseudo && use_bits(S.bits, sg.diff, shift, sg.size, S.small_max, S.first);
     const BitDigit bd = bit_digit_spec(bits ? (uint64_t)sg.diff : (0xFFull << shift));
     __shared__ BitTables bt;
     if (!bd.whole) bit_tables_build(bt, bd);  // the barrier after the block's set-up follows
@@ -2228,6 +2230,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     S.pivot = tune(TUNE_SORT_PIVOT) ? 1u : 0u;
     S.bits = (uint32_t)tune(TUNE_SORT_BITS);
     S.seg_bits = tune(TUNE_SORT_SEG_BITS) ? 1u : 0u;
+    S.first = 0;
     S.cap_large = L.cap_large;
     S.cap_small = L.cap_small;
     S.cap_tiles = L.cap_tiles;
@@ -2275,6 +2278,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
     uint32_t guard = 0;
     S.dig = dig_all ? dig : nullptr;
     bool first_pass = true;
+    S.first = 1;
     // whether the list holds a segment without keys folded by the previous
     // scatter (no keys, a pivot pass, or the first pass): only then the
     // prefix, pivot and key passes run
@@ -2300,8 +2304,12 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         if (S.split_min)
             DSSS_LAUNCH("k_split_sample", st,
                         k_split_sample<<<std::min<uint32_t>(nlarge, 148 * 2), SPL_SAMPLE / 2, 0, st>>>(S, segs, nlarge));
-        if (S.bits) DSSS_LAUNCH("k_hist", st, k_hist<true><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
-        else DSSS_LAUNCH("k_hist", st, k_hist<false><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        // the bit-digit histogram only in passes that can split on bits (its
+        // tables and registers cost the byte form's occupancy)
+        if (S.bits && (S.bits != 3 || S.first))
+            DSSS_LAUNCH("k_hist", st, k_hist<true><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
+        else
+            DSSS_LAUNCH("k_hist", st, k_hist<false><<<(unsigned)max_tiles, LT_NT, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_chunk_sum", st, k_chunk_sum<<<(unsigned)max_chunks, 256, 0, st>>>(S, segs, nlarge));
         DSSS_LAUNCH("k_seg_scan", st, k_seg_scan<<<nlarge, 256, 0, st>>>(S, segs, nlarge, next));
         DSSS_LAUNCH("k_scatter", st, k_scatter<<<(unsigned)max_tiles, LT_NT, SCATTER_SMEM, st>>>(S, segs, nlarge));
@@ -2315,6 +2323,7 @@ int sort_strings(const SortLayout& L, const ArenaDev& a, uint64_t n, uint32_t p,
         cur ^= 1;
         if (first_pass && S.dig && dig_mask) *dig_mask = 15u & ~pin[15];  // depths no segment skipped
         first_pass = false;
+        S.first = 0;
         S.dig = nullptr;
     }
     for (int b = 0; b < NBINS; ++b)

@@ -66,7 +66,7 @@ extern "C" int dsss_autotune(dsss_ctx* ctx, const dsss_arena* in, uint32_t nsets
     {
         const int64_t smalls[3] = {4096, 1024, 256};
         // (split_min, bits, seg_bits)
-        const int64_t digits[5][3] = {{0, 0, 0}, {65536, 0, 0}, {0, 2, 0}, {0, 0, 1}, {0, 2, 1}};
+        const int64_t digits[5][3] = {{0, 0, 0}, {65536, 0, 0}, {0, 2, 0}, {0, 0, 1}, {0, 3, 1}};
         int g = 0;
         for (int dgt = 0; dgt < 5; ++dgt)
             for (int pv = 1; pv >= 0; --pv)

@@ -157,8 +157,8 @@ int dsss_abi_version(void);
  *                   significant bits in which a segment's keys differ (over
  *                   small alphabets one pass then covers more than a key
  *                   byte); 2: only where the first differing key byte varies
- *                   in at most four bits; 0: on the first differing key byte
- *                   (default)
+ *                   in at most four bits; 3: the same in the first pass only;
+ *                   0: on the first differing key byte (default)
  *   sort_seg_bits   the same for the shared-memory passes of the segment
  *                   sorter (segments up to the small-segment cutoff; 0:
  *                   one key byte, the default) */
@@ -171,8 +171,9 @@ int dsss_tune_get(const char* name, int64_t* value);
  * 4096, sort_pivot on / off, and the MSD digit: one key byte, sampled
  * splitters where a key byte splits poorly (sort_split_min 65536), the keys'
  * top differing bits in the passes over the arena where a byte varies in at
- * most four bits (sort_bits 2), also inside the segment sorter (sort_bits 2,
- * sort_seg_bits 1), or inside the segment sorter only (sort_seg_bits 1)),
+ * most four bits (sort_bits 2), in the first pass and inside the segment
+ * sorter (sort_bits 3, sort_seg_bits 1), or inside the segment sorter only
+ * (sort_seg_bits 1)),
  * 1 + trials runs each, and leaves the fastest setting in force for later
  * calls.  out: the chosen setting (dp_filter_min: the value in force, not
  * searched), its time (minimum over trials) and the default setting's

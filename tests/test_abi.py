@@ -131,15 +131,15 @@ def test_knob_errors(dsss):
 
 
 def test_digit_knobs(dsss):
-    """The MSD digit knobs: bit digits over the arena 0 / 1 / 2 and inside the
+    """The MSD digit knobs: bit digits over the arena 0 / 1 / 2 / 3 and inside the
     segment sorter 0 / 1, both off by default; every knob the package lists
     can be read."""
     assert dsss.tune_get("sort_bits") == 0 and dsss.tune_get("sort_seg_bits") == 0
-    for v in (1, 2, 0):
+    for v in (1, 2, 3, 0):
         dsss.tune_set("sort_bits", v)
         assert dsss.tune_get("sort_bits") == v
     with pytest.raises(dsss.DsssError):
-        dsss.tune_set("sort_bits", 3)
+        dsss.tune_set("sort_bits", 4)
     with pytest.raises(dsss.DsssError):
         dsss.tune_set("sort_seg_bits", 2)
     dsss.tune_set("sort_seg_bits", 1)

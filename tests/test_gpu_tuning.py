@@ -93,7 +93,7 @@ def test_autotune_picks_a_grid_setting(dsss, orc, ctx):
         assert t["settings_tried"] == 30
         assert t["sort_small_max"] in (256, 1024, 4096) and t["sort_pivot"] in (0, 1)
         assert (t["sort_split_min"], t["sort_bits"], t["sort_seg_bits"]) in ((0, 0, 0), (65536, 0, 0), (0, 2, 0),
-                                                                             (0, 0, 1), (0, 2, 1))
+                                                                             (0, 0, 1), (0, 3, 1))
         assert dsss.tune_get("sort_seg_bits") == t["sort_seg_bits"]
         assert dsss.tune_get("sort_split_min") == t["sort_split_min"]
         assert dsss.tune_get("sort_bits") == t["sort_bits"]
@@ -299,7 +299,7 @@ def test_sort_split_pd(dsss, orc, ctx, graph):
     check_pd(dsss, orc, hs, out, 4)
 
 
-@pytest.mark.parametrize("bits,seg_bits", [(1, 1), (1, 0), (2, 1), (0, 0)])
+@pytest.mark.parametrize("bits,seg_bits", [(1, 1), (1, 0), (2, 1), (3, 1), (0, 0)])
 @pytest.mark.parametrize("small", [0, 64])
 @pytest.mark.parametrize("name,strs", CASES + _split_inputs(), ids=IDS + [c[0] for c in _split_inputs()])
 def test_sort_bits(dsss, orc, ctx, name, strs, small, bits, seg_bits):
